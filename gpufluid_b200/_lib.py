@@ -1,0 +1,118 @@
+"""ctypes binding of libgfb200.so (the C ABI declared in include/gfb200.h).
+
+The shared library is loaded from this package directory; it is built by
+``python -m gpufluid_b200.build``.  There is no fallback: if the library is
+missing or no sm_100 device is present, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgfb200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "gfb200.h")
+
+GF_OK, GF_INVALID_ARG, GF_CUDA_ERROR, GF_NOT_CONVERGED = 0, 1, 2, 3
+GF_NAN, GF_BREAKDOWN, GF_TIMEOUT, GF_NO_DEVICE = 4, 5, 6, 7
+STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "CUDA_ERROR", 3: "NOT_CONVERGED", 4: "NAN",
+                5: "BREAKDOWN", 6: "TIMEOUT", 7: "NO_DEVICE"}
+
+GF_FLIP, GF_PIC, GF_APIC = 0, 1, 2
+GF_JACOBI, GF_GSRB, GF_PCG, GF_PCG_REFINED = 0, 1, 2, 3
+TRANSFER = {"flip": GF_FLIP, "pic": GF_PIC, "apic": GF_APIC}
+SOLVER = {"jacobi": GF_JACOBI, "gsrb": GF_GSRB, "pcg": GF_PCG, "pcg_refined": GF_PCG_REFINED}
+
+
+class GfError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"gfb200 {STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+_fp = ctypes.POINTER(ctypes.c_float)
+_vp = ctypes.c_void_p
+
+
+class GridDesc(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+                ("dx", ctypes.c_float), ("dom", ctypes.c_float * 3)]
+
+
+class Fields(ctypes.Structure):
+    _fields_ = [(n, _vp) for n in ("u", "v", "w", "uw", "vw", "ww", "us", "vs", "ws", "p",
+                                   "div", "label", "solid_u", "solid_v", "solid_w")]
+
+
+class Particles(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("pos", _vp), ("vel", _vp), ("C", _vp), ("pid", _vp)]
+
+
+class StepParams(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_float), ("gravity", ctypes.c_float), ("rho", ctypes.c_float),
+                ("flip_blend", ctypes.c_float), ("transfer", ctypes.c_int32),
+                ("solver", ctypes.c_int32), ("max_iters", ctypes.c_int32),
+                ("check_every", ctypes.c_int32), ("tol", ctypes.c_double),
+                ("rhs_sign", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+_SIGS = {
+    "gf_create": ([ctypes.POINTER(GridDesc), ctypes.c_int64, ctypes.POINTER(_vp)], ctypes.c_int),
+    "gf_destroy": ([_vp], ctypes.c_int),
+    "gf_reserve_particles": ([_vp, ctypes.c_int64], ctypes.c_int),
+    "gf_bind": ([_vp, ctypes.POINTER(Fields), ctypes.POINTER(Particles)], ctypes.c_int),
+    "gf_set_stream": ([_vp, _vp], ctypes.c_int),
+    "gf_last_error": ([_vp], ctypes.c_char_p),
+    "gf_launch_count": ([_vp], ctypes.c_int64),
+    "gf_bin": ([_vp, ctypes.c_int32], ctypes.c_int),
+    "gf_p2g": ([_vp, ctypes.c_int32], ctypes.c_int),
+    "gf_forces_div": ([_vp, ctypes.c_float, ctypes.c_float, ctypes.c_float], ctypes.c_int),
+    "gf_pressure": ([_vp, ctypes.POINTER(StepParams), ctypes.POINTER(ctypes.c_int32)],
+                    ctypes.c_int),
+    "gf_project": ([_vp, ctypes.c_float, ctypes.c_float], ctypes.c_int),
+    "gf_g2p": ([_vp, ctypes.c_int32, ctypes.c_float, ctypes.c_float], ctypes.c_int),
+    "gf_step": ([_vp, ctypes.POINTER(StepParams)], ctypes.c_int),
+    "gf_pressure_result": ([_vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double),
+                            ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
+    "gf_bin_read": ([_vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
+    "gf_enable_timing": ([_vp, ctypes.c_int32], ctypes.c_int),
+    "gf_stage_times": ([_vp, _fp], ctypes.c_int),
+    "gf_active_tiles": ([_vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(_vp)], ctypes.c_int),
+    "gf_vmax": ([_vp, _fp], ctypes.c_int),
+}
+
+_lib = None
+
+
+def header_symbols() -> list[str]:
+    """Names of every function declared in include/gfb200.h."""
+    with open(HEADER) as f:
+        text = f.read()
+    return sorted(set(re.findall(r"^\s*(?:int|int64_t|const char \*)\s*(gf_\w+)\s*\(", text,
+                                 flags=re.M)))
+
+
+def load():
+    """Load libgfb200.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with "
+                               "`python -m gpufluid_b200.build` (nvcc, sm_100a)")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (args, res) in _SIGS.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = lib
+    return _lib
+
+
+def check(status: int, ctx=None, what: str = ""):
+    if status != GF_OK:
+        msg = ""
+        if ctx is not None:
+            raw = load().gf_last_error(ctx)
+            msg = raw.decode() if raw else ""
+        raise GfError(status, f"{what}: {msg}" if what else msg)

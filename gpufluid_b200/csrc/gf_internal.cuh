@@ -1,0 +1,123 @@
+// Internal declarations shared by the gfb200 translation units.
+//
+// Data layout in HBM (all device buffers):
+//  * dense MAC fields exactly as the reference lays them out (C order, k
+//    fastest), so the caller can hand in / read back the same arrays;
+//  * labels as uint8 (0 air, 1 fluid, 2 solid): 1 B per cell instead of the
+//    reference's int32 marker;
+//  * particles in the caller's (n,3) AoS buffers hold the state between
+//    substeps; inside a substep they are read from four float4 streams,
+//    sorted by cell:  rec0 = (x, y, z, pid-as-bits)  rec1 = (vx, vy, vz, C00)
+//    rec2 = (C01, C02, C10, C11)  rec3 = (C12, C20, C21, C22)
+//    (FLIP/PIC use rec0, rec1 only);
+//  * the pressure solve works on a compact array of active 8x8x8 tiles:
+//    element (slot*512 + ((li*8 + lj)*8 + lk)) is cell (8*ti+li, 8*tj+lj,
+//    8*tk+lk) of the slot-th active tile, with a 6-neighbour tile table and a
+//    16-bit stencil code per cell.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/gfb200.h"
+
+namespace gf {
+
+constexpr int TILE = 8;            // tile edge in cells (the reference's BLOCK_SIZE, :950)
+constexpr int TILE_CELLS = 512;    // cells per tile
+constexpr int MAX_PCG_BLOCKS = 4096;
+
+// Stencil code bits (per compact cell).
+constexpr uint16_t CODE_NB_MASK = 0x3F;   // bit b: neighbour b is fluid (-x,+x,-y,+y,-z,+z)
+constexpr int CODE_DIAG_SHIFT = 8;        // bits 8..10: #non-solid in-grid neighbours
+constexpr uint16_t CODE_FLUID = 0x8000;   // the cell itself is fluid
+
+struct PcgState {
+  // scalars of the running solve (device resident)
+  double rz;       // r . z
+  double r0;       // ||r0||^2 (the reference's stop test base)
+  double rr;       // ||r||^2 at the last evaluation
+  double alpha, beta;
+  double b2;       // ||b||^2 (refined solve)
+  double r_true2;  // ||b - A x||^2 in FP64 at the last replacement
+  double r_upd2;   // ||r||^2 at the last residual replacement
+  int iters;
+  int done;
+  int status;      // gf_status
+  int n_replace;   // residual replacements performed (refined solve)
+  unsigned bar_count;
+  unsigned bar_gen;
+  int error;       // set on a barrier timeout
+  int pad;
+};
+
+struct Ctx {
+  // grid
+  int nx = 0, ny = 0, nz = 0;
+  float dx = 0.f, dom[3] = {0, 0, 0};
+  int ntx = 0, nty = 0, ntz = 0, ntiles = 0;
+  int64_t nkeys = 0;  // ntiles * 512
+  int64_t ncell = 0;
+  int device = 0, num_sms = 0;
+  cudaStream_t stream = 0;
+
+  // caller buffers
+  gf_fields f{};
+  gf_particles p{};
+  bool bound = false;
+
+  // binning scratch
+  int64_t cap = 0;
+  int32_t *key = nullptr, *rank = nullptr, *order = nullptr;
+  int32_t *count = nullptr, *start = nullptr, *scan_part = nullptr;
+  int64_t n_scan_blocks = 0;
+  float4 *rec0 = nullptr, *rec1 = nullptr, *rec2 = nullptr, *rec3 = nullptr;
+
+  // pressure workspace (compact active tiles)
+  int32_t *tile_slot = nullptr;  // [ntiles] slot or -1
+  int32_t *tile_list = nullptr;  // [ntiles] tile id of each slot
+  int32_t *tile_nbr = nullptr;   // [ntiles*6] neighbour slot or -1
+  int32_t *n_active = nullptr;   // [1]
+  uint16_t *code = nullptr;      // [nkeys]
+  float *bdiv = nullptr, *xf = nullptr, *r = nullptr, *z = nullptr;
+  float *d0 = nullptr, *d1 = nullptr, *Ad = nullptr;
+  double *x64 = nullptr;
+  double *partials = nullptr;    // [3 * MAX_PCG_BLOCKS]
+  PcgState *state = nullptr;
+  PcgState *state_host = nullptr;  // pinned mirror
+  int last_solver = -1;  // gf_solver of the last gf_pressure
+  int last_iters = 0;    // iteration count of the last Jacobi / GS-RB solve
+
+  // diagnostics
+  bool timing = false;
+  cudaEvent_t ev[8] = {};
+  float stage_ms[7] = {0, 0, 0, 0, 0, 0, 0};
+  int64_t launches = 0;
+  float *vmax_dev = nullptr;
+  std::string err;
+};
+
+// ---- helpers ---------------------------------------------------------------
+int fail(Ctx *c, int status, const std::string &msg);
+int check_cuda(Ctx *c, cudaError_t e, const char *what);
+int check_launch(Ctx *c, const char *what);
+
+__host__ __device__ inline int64_t uidx(int i, int j, int k, int ny, int nz) {
+  return ((int64_t)i * ny + j) * nz + k;
+}
+
+// Stage launchers (defined in the .cu files).
+int launch_bin(Ctx *c, int transfer);
+int launch_p2g(Ctx *c, int transfer);
+int launch_forces_div(Ctx *c, float gravity, float dt, float rho);
+int launch_pressure(Ctx *c, const gf_step_params *prm);
+int launch_project(Ctx *c, float dt, float rho);
+int launch_g2p(Ctx *c, int transfer, float flip_blend, float dt);
+int launch_vmax(Ctx *c);
+
+int pressure_alloc(Ctx *c);
+void pressure_free(Ctx *c);
+
+}  // namespace gf

@@ -1,0 +1,629 @@
+// Pressure projection on a compact array of active 8x8x8 tiles.
+//
+// Set-up (once per solve):
+//   k_tile_flags    tile active iff it holds a fluid cell (k_mark_active_blocks,
+//                   solver3d.py:953-972)
+//   k_tile_compact  ascending slot numbering of active tiles (the reference's
+//                   array_scan + k_compact_active_blocks, :1056-1082)
+//   k_tile_setup    neighbour-tile table, per-cell 16-bit stencil code
+//                   (fluid-neighbour mask + #non-solid neighbours), compact rhs
+// Solvers:
+//   k_jacobi        one sweep of k3_jacobi_pressure (:878-938)
+//   k_gsrb          one colour of k3_gauss_seidel_rb (:1204-1267)
+//   k_pcg<Acc,REF>  the whole Jacobi-preconditioned CG of _pressure_pcg
+//                   (:2917-3043) in ONE persistent cooperative kernel: two
+//                   grid barriers per iteration, dot products reduced
+//                   warp -> block -> fixed-order last-block sum (deterministic),
+//                   convergence decided on the device.  REF=true adds FP64
+//                   residual replacement: x accumulates in FP64 and, whenever
+//                   the FP32 recursive residual has dropped by a fixed factor,
+//                   r is recomputed as b - A x in FP64 (the only FP64 work
+//                   besides the FP64 dot-product accumulation).
+//   k_scatter_p     compact solution -> dense p (non-fluid cells stay 0)
+//
+// Every spin-wait (grid barrier) is bounded; on timeout the kernel records
+// GF_TIMEOUT in the solve state and all blocks return.
+#include "gf_internal.cuh"
+
+namespace gf {
+
+constexpr int PCG_THREADS = 512;
+constexpr long long SPIN_LIMIT = 1LL << 24;  // ~1-2 s with 64 ns sleeps
+
+// ------------------------------------------------------------- set-up
+__global__ void k_tile_flags(const uint8_t *__restrict__ label, int nx, int ny, int nz,
+                             int nty, int ntz, int ntiles, int32_t *__restrict__ flag) {
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (warp >= ntiles) return;
+  int ti = warp / (nty * ntz), tj = (warp / ntz) % nty, tk = warp % ntz;
+  int any = 0;
+  for (int row = lane; row < 64; row += 32) {
+    int gi = ti * 8 + (row >> 3), gj = tj * 8 + (row & 7);
+    if (gi >= nx || gj >= ny) continue;
+    const uint8_t *base = label + ((int64_t)gi * ny + gj) * nz;
+    for (int lk = 0; lk < 8; ++lk) {
+      int gk = tk * 8 + lk;
+      if (gk < nz && base[gk] == 1) any = 1;
+    }
+  }
+  any = __any_sync(0xffffffffu, any);
+  if (lane == 0) flag[warp] = any;
+}
+
+__global__ void k_tile_compact(const int32_t *__restrict__ flag, int ntiles,
+                               int32_t *__restrict__ slot, int32_t *__restrict__ list,
+                               int32_t *__restrict__ n_active) {
+  __shared__ int warp_sums[32];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int off = 0; off < ntiles; off += blockDim.x) {
+    int t = off + threadIdx.x;
+    int f = t < ntiles ? flag[t] : 0;
+    int incl = f;
+    for (int o = 1; o < 32; o <<= 1) {
+      int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= (unsigned)o) incl += v;
+    }
+    if (lane == 31) warp_sums[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+      int s = lane < nw ? warp_sums[lane] : 0, si = s;
+      for (int o = 1; o < 32; o <<= 1) {
+        int v = __shfl_up_sync(0xffffffffu, si, o);
+        if (lane >= (unsigned)o) si += v;
+      }
+      if (lane < nw) warp_sums[lane] = si - s;
+    }
+    __syncthreads();
+    int pre = carry + warp_sums[wid] + incl - f;
+    if (t < ntiles) {
+      slot[t] = f ? pre : -1;
+      if (f) list[pre] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry = pre + f;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *n_active = carry;
+}
+
+struct SetupArgs {
+  const uint8_t *label;
+  const float *div;
+  const int32_t *n_active, *tile_list, *tile_slot;
+  int32_t *tile_nbr;
+  uint16_t *code;
+  float *bdiv, *x, *r, *z, *d0, *d1, *Ad;
+  double *x64;
+  int nx, ny, nz, ntx, nty, ntz;
+};
+
+__global__ void __launch_bounds__(512) k_tile_setup(SetupArgs a) {
+  const int na = *a.n_active;
+  const int l = threadIdx.x, li = l >> 6, lj = (l >> 3) & 7, lk = l & 7;
+  for (int s = blockIdx.x; s < na; s += gridDim.x) {
+    const int t = a.tile_list[s];
+    const int ti = t / (a.nty * a.ntz), tj = (t / a.ntz) % a.nty, tk = t % a.ntz;
+    if (l < 6) {
+      int ni = ti + (l == 0 ? -1 : l == 1 ? 1 : 0), nj = tj + (l == 2 ? -1 : l == 3 ? 1 : 0),
+          nk = tk + (l == 4 ? -1 : l == 5 ? 1 : 0);
+      int ns = -1;
+      if (ni >= 0 && ni < a.ntx && nj >= 0 && nj < a.nty && nk >= 0 && nk < a.ntz)
+        ns = a.tile_slot[(ni * a.nty + nj) * a.ntz + nk];
+      a.tile_nbr[s * 6 + l] = ns;
+    }
+    const int gi = ti * 8 + li, gj = tj * 8 + lj, gk = tk * 8 + lk;
+    const int64_t q = (int64_t)s * TILE_CELLS + l;
+    uint16_t code = 0;
+    float bd = 0.f;
+    if (gi < a.nx && gj < a.ny && gk < a.nz) {
+      const int ny = a.ny, nz = a.nz;
+      const int64_t c = ((int64_t)gi * ny + gj) * nz + gk;
+      if (a.label[c] == 1) {
+        int diag = 0, mask = 0, m;
+        // neighbour order -x, +x, -y, +y, -z, +z as in the reference stencil
+        if (gi > 0) { m = a.label[c - (int64_t)ny * nz]; if (m != 2) { ++diag; if (m == 1) mask |= 1; } }
+        if (gi < a.nx - 1) { m = a.label[c + (int64_t)ny * nz]; if (m != 2) { ++diag; if (m == 1) mask |= 2; } }
+        if (gj > 0) { m = a.label[c - nz]; if (m != 2) { ++diag; if (m == 1) mask |= 4; } }
+        if (gj < ny - 1) { m = a.label[c + nz]; if (m != 2) { ++diag; if (m == 1) mask |= 8; } }
+        if (gk > 0) { m = a.label[c - 1]; if (m != 2) { ++diag; if (m == 1) mask |= 16; } }
+        if (gk < nz - 1) { m = a.label[c + 1]; if (m != 2) { ++diag; if (m == 1) mask |= 32; } }
+        code = (uint16_t)(CODE_FLUID | (diag << CODE_DIAG_SHIFT) | mask);
+        bd = a.div[c];
+      }
+    }
+    a.code[q] = code;
+    a.bdiv[q] = bd;
+    a.x[q] = 0.f;
+    a.r[q] = 0.f;
+    a.z[q] = 0.f;
+    a.d0[q] = 0.f;
+    a.d1[q] = 0.f;
+    a.Ad[q] = 0.f;
+    if (a.x64) a.x64[q] = 0.0;
+  }
+}
+
+// Compact index of neighbour `dir` (0 -x, 1 +x, 2 -y, 3 +y, 4 -z, 5 +z) of q.
+// Only called for fluid neighbours, whose tile is active by construction.
+__device__ __forceinline__ int64_t nb_index(int64_t q, int dir, const int32_t *__restrict__ nbr) {
+  const int s = (int)(q >> 9), l = (int)(q & 511);
+  const int li = l >> 6, lj = (l >> 3) & 7, lk = l & 7;
+  switch (dir) {
+    case 0: return li > 0 ? q - 64 : (int64_t)__ldg(nbr + s * 6 + 0) * 512 + (448 | (l & 63));
+    case 1: return li < 7 ? q + 64 : (int64_t)__ldg(nbr + s * 6 + 1) * 512 + (l & 63);
+    case 2: return lj > 0 ? q - 8 : (int64_t)__ldg(nbr + s * 6 + 2) * 512 + ((l & 0x1C7) | 56);
+    case 3: return lj < 7 ? q + 8 : (int64_t)__ldg(nbr + s * 6 + 3) * 512 + (l & 0x1C7);
+    case 4: return lk > 0 ? q - 1 : (int64_t)__ldg(nbr + s * 6 + 4) * 512 + (l | 7);
+    default: return lk < 7 ? q + 1 : (int64_t)__ldg(nbr + s * 6 + 5) * 512 + (l & ~7);
+  }
+}
+
+// ------------------------------------------------------------- Jacobi / GS
+struct SweepArgs {
+  const int32_t *n_active, *nbr;
+  const uint16_t *code;
+  const float *bdiv;
+};
+
+__global__ void k_jacobi(SweepArgs a, const float *__restrict__ xin, float *__restrict__ xout) {
+  const int64_t total = (int64_t)(*a.n_active) * TILE_CELLS;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const uint16_t code = a.code[q];
+    if (!(code & CODE_FLUID)) continue;  // stays 0
+    float s = 0.0f;
+#pragma unroll
+    for (int d = 0; d < 6; ++d)
+      if (code & (1 << d)) s = s + xin[nb_index(q, d, a.nbr)];
+    const float diag = (float)((code >> CODE_DIAG_SHIFT) & 7);
+    xout[q] = diag < 0.5f ? 0.0f : (s - a.bdiv[q]) / diag;
+  }
+}
+
+__global__ void k_gsrb(SweepArgs a, float *__restrict__ x, int color) {
+  const int64_t total = (int64_t)(*a.n_active) * TILE_CELLS;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int l = (int)(q & 511);
+    if ((((l >> 6) + ((l >> 3) & 7) + (l & 7)) & 1) != color) continue;  // global parity
+    const uint16_t code = a.code[q];
+    if (!(code & CODE_FLUID)) continue;
+    float s = 0.0f;
+#pragma unroll
+    for (int d = 0; d < 6; ++d)
+      if (code & (1 << d)) s = s + x[nb_index(q, d, a.nbr)];
+    const float diag = (float)((code >> CODE_DIAG_SHIFT) & 7);
+    x[q] = diag < 0.5f ? 0.0f : (s - a.bdiv[q]) / diag;
+  }
+}
+
+// ------------------------------------------------------------------ PCG
+struct PcgArgs {
+  const int32_t *n_active, *nbr;
+  const uint16_t *code;
+  const float *bdiv;
+  float *x, *r, *z, *d0, *d1, *Ad;
+  double *x64;
+  double *partials;
+  PcgState *st;
+  int max_iter, check_every;
+  double tol2;     // tol^2
+  double replace2; // residual-replacement factor^2 (refined)
+  float sign;      // b = sign * div
+};
+
+template <typename T>
+__device__ __forceinline__ T block_sum(T v, T *sh) {
+  // deterministic: fixed shuffle tree, then warp 0 sums the per-warp values
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  T t = 0;
+  if (wid == 0) {
+    t = lane < (int)(blockDim.x >> 5) ? sh[lane] : (T)0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+  }
+  __syncthreads();
+  return t;  // valid in thread 0
+}
+
+__device__ __forceinline__ unsigned ld_volatile(const unsigned *p) {
+  return *reinterpret_cast<const volatile unsigned *>(p);
+}
+__device__ __forceinline__ int ld_volatile_i(const int *p) {
+  return *reinterpret_cast<const volatile int *>(p);
+}
+__device__ __forceinline__ double ld_volatile_d(const double *p) {
+  return *reinterpret_cast<const volatile double *>(p);
+}
+
+// Grid-wide reduction of NV values + barrier.  Every block writes its block
+// sums to partials; the last block to arrive sums all partials in a fixed
+// order, runs `fin` (thread 0) on the totals, then releases the others.
+// Returns false when a wait timed out (the caller must return).
+template <typename T, int NV, typename Fin>
+__device__ bool grid_reduce(const PcgArgs &a, T (&v)[NV], Fin fin) {
+  __shared__ T sh[32];
+  __shared__ int s_last, s_ok;
+  T tot[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) tot[k] = block_sum<T>(v[k], sh);
+  const unsigned nb = gridDim.x;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) a.partials[k * MAX_PCG_BLOCKS + blockIdx.x] = (double)tot[k];
+  }
+  __syncthreads();
+  unsigned gen = 0;
+  if (threadIdx.x == 0) {
+    gen = ld_volatile(&a.st->bar_gen);
+    __threadfence();
+    unsigned arrived = atomicAdd(&a.st->bar_count, 1u);
+    s_last = arrived == nb - 1;
+    s_ok = 1;
+  }
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    double all[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      T acc = 0;
+      for (unsigned j = threadIdx.x; j < nb; j += blockDim.x)
+        acc += (T)__ldcg(a.partials + k * MAX_PCG_BLOCKS + j);
+      all[k] = (double)block_sum<T>(acc, sh);
+    }
+    if (threadIdx.x == 0) {
+      fin(all);
+      __threadfence();
+      atomicExch(&a.st->bar_count, 0u);
+      __threadfence();
+      atomicAdd(&a.st->bar_gen, 1u);
+    }
+  } else if (threadIdx.x == 0) {
+    long long spins = 0;
+    while (ld_volatile(&a.st->bar_gen) == gen) {
+      if (++spins > SPIN_LIMIT) {
+        atomicExch(&a.st->error, 1);
+        s_ok = 0;
+        break;
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  if (ld_volatile_i(&a.st->error)) return false;
+  return s_ok;
+}
+
+__device__ bool grid_barrier(const PcgArgs &a) {
+  double v[1] = {0.0};
+  return grid_reduce<double, 1>(a, v, [](double *) {});
+}
+
+template <typename Acc, bool REF>
+__global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
+  const int64_t total = (int64_t)(*a.n_active) * TILE_CELLS;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t q0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  PcgState *st = a.st;
+
+  // ---- init: x = 0, r = b, z = M^-1 r, d = 0 (so the first d = z)
+  {
+    Acc v[2] = {0, 0};
+    for (int64_t q = q0; q < total; q += stride) {
+      const uint16_t code = a.code[q];
+      if (!(code & CODE_FLUID)) continue;
+      const float b = a.sign * a.bdiv[q];
+      const float diag = fmaxf((float)((code >> CODE_DIAG_SHIFT) & 7), 1.0f);
+      const float z = b / diag;
+      a.r[q] = b;
+      a.z[q] = z;
+      v[0] += (Acc)(b * z);
+      v[1] += (Acc)(b * b);
+    }
+    if (!grid_reduce<Acc, 2>(a, v, [&](double *t) {
+          st->rz = t[0];
+          st->r0 = t[1];
+          st->rr = t[1];
+          st->b2 = t[1];
+          st->r_upd2 = t[1];
+          st->r_true2 = t[1];
+          st->beta = 0.0;
+          st->alpha = 0.0;
+          st->iters = 0;
+          st->n_replace = 0;
+          st->status = GF_OK;
+          st->done = t[1] < 1e-30 ? 1 : 0;  // the reference's early exit (:2982-2986)
+        }))
+      return;
+  }
+
+  for (int it = 0; it < a.max_iter; ++it) {
+    if (ld_volatile_i(&st->done)) break;
+    const float beta = (float)ld_volatile_d(&st->beta);
+    const float *__restrict__ dold = (it & 1) ? a.d1 : a.d0;
+    float *__restrict__ dnew = (it & 1) ? a.d0 : a.d1;
+    // ---- phase A: d = z + beta d ; Ad = A d ; p.Ap
+    {
+      Acc v[1] = {0};
+      for (int64_t q = q0; q < total; q += stride) {
+        const uint16_t code = a.code[q];
+        if (!(code & CODE_FLUID)) continue;
+        const float dn = __ldcg(a.z + q) + beta * __ldcg(dold + q);
+        float s = 0.0f;
+#pragma unroll
+        for (int d = 0; d < 6; ++d)
+          if (code & (1 << d)) {
+            const int64_t nq = nb_index(q, d, a.nbr);
+            s = s + (__ldcg(a.z + nq) + beta * __ldcg(dold + nq));
+          }
+        const float diag = (float)((code >> CODE_DIAG_SHIFT) & 7);
+        const float ad = diag * dn - s;
+        dnew[q] = dn;
+        a.Ad[q] = ad;
+        v[0] += (Acc)(dn * ad);
+      }
+      if (!grid_reduce<Acc, 1>(a, v, [&](double *t) {
+            const double pAp = t[0];
+            double al = (Acc)fabs(pAp) < (Acc)1.0e-30 ? 0.0 : (double)((Acc)st->rz / (Acc)pAp);
+            if (!(pAp == pAp)) {  // NaN
+              st->status = GF_NAN;
+              st->done = 1;
+            }
+            st->alpha = al;
+          }))
+        return;
+    }
+    // ---- phase B: x += alpha d ; r -= alpha Ad ; z = M^-1 r ; r.z, r.r
+    {
+      const float alpha = (float)ld_volatile_d(&st->alpha);
+      const float nalpha = -alpha;
+      Acc v[2] = {0, 0};
+      for (int64_t q = q0; q < total; q += stride) {
+        const uint16_t code = a.code[q];
+        if (!(code & CODE_FLUID)) continue;
+        const float dn = __ldcg(dnew + q);
+        a.x[q] = __ldcg(a.x + q) + alpha * dn;
+        const float rn = __ldcg(a.r + q) + nalpha * __ldcg(a.Ad + q);
+        const float diag = fmaxf((float)((code >> CODE_DIAG_SHIFT) & 7), 1.0f);
+        const float z = rn / diag;
+        a.r[q] = rn;
+        a.z[q] = z;
+        v[0] += (Acc)(rn * z);
+        v[1] += (Acc)(rn * rn);
+      }
+      const int it1 = it + 1;
+      if (!grid_reduce<Acc, 2>(a, v, [&](double *t) {
+            const double rz_new = t[0], rr = t[1];
+            st->iters = it1;
+            st->rr = rr;
+            if (!(rr == rr)) {
+              st->status = GF_NAN;
+              st->done = 1;
+              return;
+            }
+            int replace = 0;
+            if (REF) {
+              replace = rr < a.replace2 * st->r_upd2 || rr < a.tol2 * st->b2;
+            } else {
+              const bool check = (it1 % a.check_every) == 0 || it1 == a.max_iter;
+              if (check && rr < a.tol2 * st->r0) st->done = 1;
+            }
+            if (replace) {
+              st->n_replace = -st->n_replace - 1;  // negative: replacement pending
+            } else {
+              const double rz = st->rz;
+              st->beta = (Acc)fabs(rz) < (Acc)1.0e-30 ? 0.0 : (double)((Acc)rz_new / (Acc)rz);
+              st->rz = rz_new;
+            }
+          }))
+        return;
+    }
+    // ---- refined: FP64 residual replacement r = b - A x
+    if (REF && ld_volatile_i(&st->n_replace) < 0) {
+      for (int64_t q = q0; q < total; q += stride) {
+        if (!(a.code[q] & CODE_FLUID)) continue;
+        a.x64[q] = __ldcg(a.x64 + q) + (double)__ldcg(a.x + q);
+        a.x[q] = 0.0f;
+      }
+      if (!grid_barrier(a)) return;
+      double v[3] = {0, 0, 0};
+      for (int64_t q = q0; q < total; q += stride) {
+        const uint16_t code = a.code[q];
+        if (!(code & CODE_FLUID)) continue;
+        double s = 0.0;
+#pragma unroll
+        for (int d = 0; d < 6; ++d)
+          if (code & (1 << d)) s += __ldcg(a.x64 + nb_index(q, d, a.nbr));
+        const double diag = (double)((code >> CODE_DIAG_SHIFT) & 7);
+        const double res = (double)(a.sign * a.bdiv[q]) - (diag * __ldcg(a.x64 + q) - s);
+        const float rf = (float)res;
+        const float z = rf / fmaxf((float)diag, 1.0f);
+        a.r[q] = rf;
+        a.z[q] = z;
+        v[0] += res * res;
+        v[1] += (double)(rf * z);
+        v[2] += (double)(rf * rf);
+      }
+      if (!grid_reduce<double, 3>(a, v, [&](double *t) {
+            st->r_true2 = t[0];
+            st->r_upd2 = t[2];
+            st->rr = t[2];
+            st->n_replace = -st->n_replace;  // back to a positive count (+1)
+            const double rz = st->rz;
+            st->beta = fabs(rz) < 1.0e-30 ? 0.0 : t[1] / rz;
+            st->rz = t[1];
+            if (t[0] <= a.tol2 * st->b2) st->done = 1;
+          }))
+        return;
+    }
+  }
+  if (threadIdx.x == 0 && blockIdx.x == 0 && !ld_volatile_i(&st->done))
+    st->status = GF_NOT_CONVERGED;
+}
+
+struct ScatterArgs {
+  const int32_t *n_active, *tile_list;
+  const uint16_t *code;
+  const float *x;
+  const double *x64;
+  float *p;
+  int ny, nz, nty, ntz;
+};
+
+__global__ void k_scatter_p(ScatterArgs a) {
+  const int64_t total = (int64_t)(*a.n_active) * TILE_CELLS;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    if (!(a.code[q] & CODE_FLUID)) continue;
+    const int s = (int)(q >> 9), l = (int)(q & 511);
+    const int t = a.tile_list[s];
+    const int ti = t / (a.nty * a.ntz), tj = (t / a.ntz) % a.nty, tk = t % a.ntz;
+    const int gi = ti * 8 + (l >> 6), gj = tj * 8 + ((l >> 3) & 7), gk = tk * 8 + (l & 7);
+    float v = a.x[q];
+    if (a.x64) v = (float)(a.x64[q] + (double)v);
+    a.p[((int64_t)gi * a.ny + gj) * a.nz + gk] = v;
+  }
+}
+
+// ------------------------------------------------------------- host side
+int pressure_alloc(Ctx *c) {
+  const int64_t nk = c->nkeys;
+  auto A = [&](void **p, size_t bytes, const char *what) {
+    return check_cuda(c, cudaMalloc(p, bytes), what);
+  };
+  int e;
+  if ((e = A((void **)&c->tile_slot, c->ntiles * 4, "alloc tile_slot"))) return e;
+  if ((e = A((void **)&c->tile_list, c->ntiles * 4, "alloc tile_list"))) return e;
+  if ((e = A((void **)&c->tile_nbr, (size_t)c->ntiles * 6 * 4, "alloc tile_nbr"))) return e;
+  if ((e = A((void **)&c->n_active, 16, "alloc n_active"))) return e;
+  if ((e = A((void **)&c->code, nk * 2, "alloc code"))) return e;
+  float **vecs[7] = {&c->bdiv, &c->xf, &c->r, &c->z, &c->d0, &c->d1, &c->Ad};
+  for (int q = 0; q < 7; ++q)
+    if ((e = A((void **)vecs[q], nk * 4, "alloc pressure vector"))) return e;
+  if ((e = A((void **)&c->x64, nk * 8, "alloc x64"))) return e;
+  if ((e = A((void **)&c->partials, 3 * MAX_PCG_BLOCKS * sizeof(double), "alloc partials")))
+    return e;
+  if ((e = A((void **)&c->state, sizeof(PcgState), "alloc pcg state"))) return e;
+  if ((e = check_cuda(c, cudaMemset(c->state, 0, sizeof(PcgState)), "zero pcg state"))) return e;
+  if ((e = check_cuda(c, cudaMallocHost((void **)&c->state_host, sizeof(PcgState)),
+                      "alloc pinned state")))
+    return e;
+  memset(c->state_host, 0, sizeof(PcgState));
+  return GF_OK;
+}
+
+void pressure_free(Ctx *c) {
+  void *ps[] = {c->tile_slot, c->tile_list, c->tile_nbr, c->n_active, c->code, c->bdiv,
+                c->xf, c->r, c->z, c->d0, c->d1, c->Ad, c->x64, c->partials, c->state};
+  for (void *p : ps)
+    if (p) cudaFree(p);
+  if (c->state_host) cudaFreeHost(c->state_host);
+}
+
+template <typename Acc, bool REF>
+static int coop_grid(Ctx *c) {
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg<Acc, REF>,
+                                                                PCG_THREADS, 0);
+  if (e != cudaSuccess || per_sm < 1) return 0;
+  int g = per_sm * c->num_sms;
+  return g > MAX_PCG_BLOCKS ? MAX_PCG_BLOCKS : g;
+}
+
+template <typename Acc, bool REF>
+static int launch_pcg(Ctx *c, PcgArgs &pa) {
+  int g = coop_grid<Acc, REF>(c);
+  if (g < 1) return fail(c, GF_CUDA_ERROR, "PCG: cooperative occupancy query failed");
+  void *args[] = {&pa};
+  int e = check_cuda(c, cudaLaunchCooperativeKernel((const void *)k_pcg<Acc, REF>, dim3(g),
+                                                    dim3(PCG_THREADS), args, 0, c->stream),
+                     "cooperative PCG launch");
+  c->launches++;
+  return e;
+}
+
+int launch_pressure(Ctx *c, const gf_step_params *prm) {
+  if (!c->bound) return fail(c, GF_INVALID_ARG, "gf_pressure: buffers not bound");
+  const int solver = prm->solver;
+  if (solver < GF_JACOBI || solver > GF_PCG_REFINED)
+    return fail(c, GF_INVALID_ARG, "unknown pressure_solver");
+  if (prm->max_iters < 0) return fail(c, GF_INVALID_ARG, "pressure_iters must be >= 0");
+  cudaStream_t st = c->stream;
+  int e;
+  // ---- active tiles
+  {
+    // the flags live in tile_nbr (>= ntiles entries): k_tile_compact consumes
+    // them before k_tile_setup overwrites that array with the neighbour table
+    int32_t *flag = c->tile_nbr;
+    unsigned g = (unsigned)((c->ntiles * 32 + 255) / 256);
+    k_tile_flags<<<g, 256, 0, st>>>(c->f.label, c->nx, c->ny, c->nz, c->nty, c->ntz,
+                                    c->ntiles, flag);
+    k_tile_compact<<<1, 1024, 0, st>>>(flag, c->ntiles, c->tile_slot, c->tile_list,
+                                       c->n_active);
+    c->launches += 2;
+  }
+  const bool refined = solver == GF_PCG_REFINED;
+  SetupArgs sa{c->f.label, c->f.div, c->n_active, c->tile_list, c->tile_slot, c->tile_nbr,
+               c->code, c->bdiv, c->xf, c->r, c->z, c->d0, c->d1, c->Ad,
+               refined ? c->x64 : nullptr, c->nx, c->ny, c->nz, c->ntx, c->nty, c->ntz};
+  {
+    int g = c->ntiles < c->num_sms * 4 ? c->ntiles : c->num_sms * 4;
+    k_tile_setup<<<g > 0 ? g : 1, 512, 0, st>>>(sa);
+    c->launches++;
+  }
+  const unsigned gs = (unsigned)(c->num_sms * 8);
+  SweepArgs sw{c->n_active, c->tile_nbr, c->code, c->bdiv};
+  const float *result = c->xf;
+  const double *result64 = nullptr;
+  if (solver == GF_JACOBI) {
+    float *a = c->xf, *b = c->z;
+    for (int it = 0; it < prm->max_iters; ++it) {
+      k_jacobi<<<gs, 256, 0, st>>>(sw, a, b);
+      float *t = a; a = b; b = t;
+    }
+    c->launches += prm->max_iters;
+    result = a;
+    c->last_iters = prm->max_iters;
+  } else if (solver == GF_GSRB) {
+    for (int it = 0; it < prm->max_iters; ++it) {
+      k_gsrb<<<gs, 256, 0, st>>>(sw, c->xf, 0);
+      k_gsrb<<<gs, 256, 0, st>>>(sw, c->xf, 1);
+    }
+    c->launches += 2 * prm->max_iters;
+    c->last_iters = prm->max_iters;
+  } else {
+    if ((e = check_cuda(c, cudaMemsetAsync(c->state, 0, sizeof(PcgState), st), "zero state")))
+      return e;
+    PcgArgs pa{c->n_active, c->tile_nbr, c->code, c->bdiv, c->xf, c->r, c->z, c->d0, c->d1,
+               c->Ad, refined ? c->x64 : nullptr, c->partials, c->state,
+               prm->max_iters, prm->check_every > 0 ? prm->check_every : 1,
+               prm->tol * prm->tol, 0.0, prm->rhs_sign >= 0 ? 1.0f : -1.0f};
+    if (refined) {
+      pa.replace2 = 1e-4;  // replace the residual each time it drops by 100x
+      e = launch_pcg<double, true>(c, pa);
+      result64 = c->x64;
+    } else {
+      e = launch_pcg<float, false>(c, pa);
+    }
+    if (e) return e;
+  }
+  if ((e = check_cuda(c, cudaMemsetAsync(c->f.p, 0, c->ncell * 4, st), "zero p"))) return e;
+  ScatterArgs sc{c->n_active, c->tile_list, c->code, result, result64, c->f.p,
+                 c->ny, c->nz, c->nty, c->ntz};
+  k_scatter_p<<<gs, 256, 0, st>>>(sc);
+  c->launches++;
+  c->last_solver = solver;
+  return check_launch(c, "gf_pressure");
+}
+
+}  // namespace gf

@@ -1,0 +1,550 @@
+// Particle <-> grid transfers and the explicit grid stages of one substep.
+//
+//   k_p2g_tile<APIC>  k3_p2g (solver3d.py:72-114) / k3_p2g_apic (:1475-1588):
+//                     one CTA per 8x8x8 cell tile; the tile's sorted particles
+//                     scatter into a shared-memory box covering every face
+//                     they can touch; the box is flushed with plain stores on
+//                     faces no other tile reaches and float atomics on the
+//                     one-cell halo band shared with neighbouring tiles.
+//   k_forces          k3_normalize (:121-142) + k3_add_gravity (:149-156) +
+//                     k3_enforce_solid_bc (:758-799) in one pass over faces.
+//   k_divergence      k3_compute_divergence (:846-871).
+//   k_project         k3_subtract_pressure_grad (:1364-1407) + the second
+//                     k3_enforce_solid_bc of _step_impl (:3635-3642).
+//   k_g2p<MODE>       k3_g2p_and_advect (:1414-1463) / k3_g2p_apic_advect
+//                     (:1591-1732) over sorted particles; results go back to
+//                     the caller's AoS buffers in sorted order (pid follows).
+//
+// The library is compiled with -fmad=false: every product and sum rounds
+// separately, in the reference's operation order, so that each stage is
+// bit-identical to the CPU oracle when its inputs are.  Only the order of the
+// floating-point atomic sums in P2G differs.
+#include "gf_internal.cuh"
+
+namespace gf {
+
+// ---------------------------------------------------------------- P2G
+// Shared-memory boxes, in faces, relative to the tile origin (I0, J0, K0):
+// the normal axis spans [O, O+8] (9 faces), the transverse axes [O-1, O+8]
+// (10 faces).
+constexpr int BOX_N = 9, BOX_T = 10, BOX = BOX_N * BOX_T * BOX_T;  // 900
+
+struct P2GArgs {
+  const int32_t *start;
+  const float4 *rec0, *rec1, *rec2, *rec3;
+  float *u, *v, *w, *uw, *vw, *ww;
+  float dx;
+  int nx, ny, nz, nty, ntz;
+};
+
+// Scatter one face component of one particle into the shared box of `comp`
+// (0 u, 1 v, 2 w).  APIC adds C_row . (x_face - x_p) with world face
+// positions (:1510-1588).
+template <bool APIC>
+__device__ __forceinline__ void scatter_comp(float *s_val, float *s_wt, int comp, float vp,
+                                             float c0, float c1, float c2, float px, float py,
+                                             float pz, float fx, float fy, float fz, int I0,
+                                             int J0, int K0, const P2GArgs &a, float *gval,
+                                             float *gwt) {
+  int snx = a.nx + (comp == 0), sny = a.ny + (comp == 1), snz = a.nz + (comp == 2);
+  int i0 = __float2int_rz(floorf(fx)), j0 = __float2int_rz(floorf(fy)),
+      k0 = __float2int_rz(floorf(fz));
+  float sx = fx - (float)i0, sy = fy - (float)j0, sz = fz - (float)k0;
+  // box origin and extents for this component
+  int bx0 = comp == 0 ? I0 : I0 - 1, by0 = comp == 1 ? J0 : J0 - 1, bz0 = comp == 2 ? K0 : K0 - 1;
+  int ey = comp == 1 ? BOX_N : BOX_T, ez = comp == 2 ? BOX_N : BOX_T;
+  int ex = comp == 0 ? BOX_N : BOX_T;
+#pragma unroll
+  for (int di = 0; di < 2; ++di)
+#pragma unroll
+    for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+      for (int dk = 0; dk < 2; ++dk) {
+        int ii = i0 + di, jj = j0 + dj, kk = k0 + dk;
+        if (ii >= 0 && ii < snx && jj >= 0 && jj < sny && kk >= 0 && kk < snz) {
+          float wxi = di == 0 ? 1.0f - sx : sx;
+          float wyi = dj == 0 ? 1.0f - sy : sy;
+          float wzi = dk == 0 ? 1.0f - sz : sz;
+          float wt = wxi * wyi;
+          wt = wt * wzi;
+          float val = vp;
+          if (APIC) {
+            float ox = comp == 0 ? (float)ii * a.dx - px : ((float)ii + 0.5f) * a.dx - px;
+            float oy = comp == 1 ? (float)jj * a.dx - py : ((float)jj + 0.5f) * a.dx - py;
+            float oz = comp == 2 ? (float)kk * a.dx - pz : ((float)kk + 0.5f) * a.dx - pz;
+            float t0 = c0 * ox, t1 = c1 * oy, t2 = c2 * oz;
+            val = vp + t0;
+            val = val + t1;
+            val = val + t2;
+          }
+          float add = val * wt;
+          int bx = ii - bx0, by = jj - by0, bz = kk - bz0;
+          if (bx >= 0 && bx < ex && by >= 0 && by < ey && bz >= 0 && bz < ez) {
+            int e = (bx * ey + by) * ez + bz;
+            atomicAdd(&s_val[e], add);
+            atomicAdd(&s_wt[e], wt);
+          } else {  // only reachable for positions outside their clamped cell
+            int64_t g = ((int64_t)ii * sny + jj) * snz + kk;
+            atomicAdd(&gval[g], add);
+            atomicAdd(&gwt[g], wt);
+          }
+        }
+      }
+}
+
+template <bool APIC>
+__global__ void __launch_bounds__(256) k_p2g_tile(P2GArgs a) {
+  __shared__ float s_val[3][BOX];
+  __shared__ float s_wt[3][BOX];
+  const int t = blockIdx.x;
+  const int64_t b = a.start[(int64_t)t * TILE_CELLS], e = a.start[(int64_t)(t + 1) * TILE_CELLS];
+  if (b == e) return;
+  for (int q = threadIdx.x; q < 3 * BOX; q += blockDim.x) {
+    (&s_val[0][0])[q] = 0.f;
+    (&s_wt[0][0])[q] = 0.f;
+  }
+  __syncthreads();
+  const int ti = t / (a.nty * a.ntz), tj = (t / a.ntz) % a.nty, tk = t % a.ntz;
+  const int I0 = ti * TILE, J0 = tj * TILE, K0 = tk * TILE;
+  for (int64_t q = b + threadIdx.x; q < e; q += blockDim.x) {
+    float4 r0 = a.rec0[q], r1 = a.rec1[q];
+    float4 r2 = make_float4(0, 0, 0, 0), r3 = r2;
+    if (APIC) {
+      r2 = a.rec2[q];
+      r3 = a.rec3[q];
+    }
+    float gx = __fdiv_rn(r0.x, a.dx), gy = __fdiv_rn(r0.y, a.dx), gz = __fdiv_rn(r0.z, a.dx);
+    float hx = gx - 0.5f, hy = gy - 0.5f, hz = gz - 0.5f;
+    // C rows: (r1.w, r2.x, r2.y) (r2.z, r2.w, r3.x) (r3.y, r3.z, r3.w)
+    scatter_comp<APIC>(s_val[0], s_wt[0], 0, r1.x, r1.w, r2.x, r2.y, r0.x, r0.y, r0.z, gx, hy, hz,
+                       I0, J0, K0, a, a.u, a.uw);
+    scatter_comp<APIC>(s_val[1], s_wt[1], 1, r1.y, r2.z, r2.w, r3.x, r0.x, r0.y, r0.z, hx, gy, hz,
+                       I0, J0, K0, a, a.v, a.vw);
+    scatter_comp<APIC>(s_val[2], s_wt[2], 2, r1.z, r3.y, r3.z, r3.w, r0.x, r0.y, r0.z, hx, hy, gz,
+                       I0, J0, K0, a, a.w, a.ww);
+  }
+  __syncthreads();
+  // flush: faces that only this tile's particles reach are stored, the
+  // shared halo band is accumulated atomically; exact zeros are skipped
+  // (the destination was zeroed before the launch).
+  for (int q = threadIdx.x; q < 3 * BOX; q += blockDim.x) {
+    int comp = q / BOX, e2 = q - comp * BOX;
+    float val = s_val[comp][e2], wt = s_wt[comp][e2];
+    if (val == 0.f && wt == 0.f) continue;
+    int ex = comp == 0 ? BOX_N : BOX_T, ey = comp == 1 ? BOX_N : BOX_T,
+        ez = comp == 2 ? BOX_N : BOX_T;
+    int bx = e2 / (ey * ez), by = (e2 / ez) % ey, bz = e2 % ez;
+    (void)ex;
+    int ii = bx + (comp == 0 ? I0 : I0 - 1), jj = by + (comp == 1 ? J0 : J0 - 1),
+        kk = bz + (comp == 2 ? K0 : K0 - 1);
+    int snx = a.nx + (comp == 0), sny = a.ny + (comp == 1), snz = a.nz + (comp == 2);
+    if (ii < 0 || ii >= snx || jj < 0 || jj >= sny || kk < 0 || kk >= snz) continue;
+    // exclusive: every cell that can reach the face lies in this tile
+    bool ex_x = comp == 0 ? (bx >= 1 && bx <= 7) : (bx >= 2 && bx <= 7);
+    bool ex_y = comp == 1 ? (by >= 1 && by <= 7) : (by >= 2 && by <= 7);
+    bool ex_z = comp == 2 ? (bz >= 1 && bz <= 7) : (bz >= 2 && bz <= 7);
+    int64_t g = ((int64_t)ii * sny + jj) * snz + kk;
+    float *gv = comp == 0 ? a.u : (comp == 1 ? a.v : a.w);
+    float *gw = comp == 0 ? a.uw : (comp == 1 ? a.vw : a.ww);
+    if (ex_x && ex_y && ex_z) {
+      gv[g] = val;
+      gw[g] = wt;
+    } else {
+      atomicAdd(&gv[g], val);
+      atomicAdd(&gw[g], wt);
+    }
+  }
+}
+
+// --------------------------------------------------------------- forces
+struct GridArgs {
+  float *u, *v, *w, *us, *vs, *ws;
+  const float *uw, *vw, *ww;
+  const uint8_t *label;
+  const float *solid_u, *solid_v, *solid_w;
+  float *div;
+  const float *p;
+  int nx, ny, nz;
+};
+
+__global__ void k_forces(GridArgs a, float gd) {
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  int64_t n = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    int k = (int)(q % (nz + 1));
+    int64_t r = q / (nz + 1);
+    int j = (int)(r % (ny + 1)), i = (int)(r / (ny + 1));
+    if (j < ny && k < nz) {  // u face (i,j,k), i <= nx
+      int64_t g = ((int64_t)i * ny + j) * nz + k;
+      float wt = a.uw[g];
+      float val = wt > 1.0e-8f ? a.u[g] / wt : 0.0f;
+      a.us[g] = val;
+      bool left = i == 0 || a.label[((int64_t)(i - 1) * ny + j) * nz + k] == 2;
+      bool right = i == nx || a.label[((int64_t)i * ny + j) * nz + k] == 2;
+      if (left || right) val = a.solid_u ? a.solid_u[g] : 0.0f;
+      a.u[g] = val;
+    }
+    if (i < nx && k < nz) {  // v face (i,j,k), j <= ny
+      int64_t g = ((int64_t)i * (ny + 1) + j) * nz + k;
+      float wt = a.vw[g];
+      float val = wt > 1.0e-8f ? a.v[g] / wt : 0.0f;
+      a.vs[g] = val;
+      val = val + gd;  // gravity on every v face (:149-156)
+      bool bot = j == 0 || a.label[((int64_t)i * ny + (j - 1)) * nz + k] == 2;
+      bool top = j == ny || a.label[((int64_t)i * ny + j) * nz + k] == 2;
+      if (bot || top) val = a.solid_v ? a.solid_v[g] : 0.0f;
+      a.v[g] = val;
+    }
+    if (i < nx && j < ny) {  // w face (i,j,k), k <= nz
+      int64_t g = ((int64_t)i * ny + j) * (nz + 1) + k;
+      float wt = a.ww[g];
+      float val = wt > 1.0e-8f ? a.w[g] / wt : 0.0f;
+      a.ws[g] = val;
+      bool back = k == 0 || a.label[((int64_t)i * ny + j) * nz + (k - 1)] == 2;
+      bool front = k == nz || a.label[((int64_t)i * ny + j) * nz + k] == 2;
+      if (back || front) val = a.solid_w ? a.solid_w[g] : 0.0f;
+      a.w[g] = val;
+    }
+  }
+}
+
+__global__ void k_divergence(GridArgs a, float scale) {
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  int64_t n = (int64_t)nx * ny * nz;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    if (a.label[c] != 1) {
+      a.div[c] = 0.0f;
+      continue;
+    }
+    int k = (int)(c % nz);
+    int64_t r = c / nz;
+    int j = (int)(r % ny), i = (int)(r / ny);
+    float d = a.u[((int64_t)(i + 1) * ny + j) * nz + k] - a.u[c];
+    d = d + a.v[((int64_t)i * (ny + 1) + j + 1) * nz + k];
+    d = d - a.v[((int64_t)i * (ny + 1) + j) * nz + k];
+    d = d + a.w[((int64_t)i * ny + j) * (nz + 1) + k + 1];
+    d = d - a.w[((int64_t)i * ny + j) * (nz + 1) + k];
+    a.div[c] = d * scale;
+  }
+}
+
+__global__ void k_project(GridArgs a, float scale) {
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  int64_t n = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    int k = (int)(q % (nz + 1));
+    int64_t r = q / (nz + 1);
+    int j = (int)(r % (ny + 1)), i = (int)(r / (ny + 1));
+    const int64_t c = ((int64_t)i * ny + j) * nz + k;  // valid when i<nx,j<ny,k<nz
+    if (j < ny && k < nz) {  // u face
+      int64_t g = ((int64_t)i * ny + j) * nz + k;
+      float val = a.u[g];
+      if (i >= 1 && i <= nx - 1) {
+        int ml = a.label[c - (int64_t)ny * nz], mr = a.label[c];
+        if ((ml == 1 || mr == 1) && ml != 2 && mr != 2) {
+          float pl = ml == 1 ? a.p[c - (int64_t)ny * nz] : 0.0f;
+          float pr = mr == 1 ? a.p[c] : 0.0f;
+          float gr = pr - pl;
+          gr = scale * gr;
+          val = val - gr;
+        }
+      }
+      bool left = i == 0 || a.label[c - (int64_t)ny * nz] == 2;
+      bool right = i == nx || a.label[c] == 2;
+      if (left || right) val = a.solid_u ? a.solid_u[g] : 0.0f;
+      a.u[g] = val;
+    }
+    if (i < nx && k < nz) {  // v face
+      int64_t g = ((int64_t)i * (ny + 1) + j) * nz + k;
+      float val = a.v[g];
+      if (j >= 1 && j <= ny - 1) {
+        int mb = a.label[c - nz], mt = a.label[c];
+        if ((mb == 1 || mt == 1) && mb != 2 && mt != 2) {
+          float pb = mb == 1 ? a.p[c - nz] : 0.0f;
+          float pt = mt == 1 ? a.p[c] : 0.0f;
+          float gr = pt - pb;
+          gr = scale * gr;
+          val = val - gr;
+        }
+      }
+      bool bot = j == 0 || a.label[c - nz] == 2;
+      bool top = j == ny || a.label[c] == 2;
+      if (bot || top) val = a.solid_v ? a.solid_v[g] : 0.0f;
+      a.v[g] = val;
+    }
+    if (i < nx && j < ny) {  // w face
+      int64_t g = ((int64_t)i * ny + j) * (nz + 1) + k;
+      float val = a.w[g];
+      if (k >= 1 && k <= nz - 1) {
+        int mba = a.label[c - 1], mfr = a.label[c];
+        if ((mba == 1 || mfr == 1) && mba != 2 && mfr != 2) {
+          float pba = mba == 1 ? a.p[c - 1] : 0.0f;
+          float pfr = mfr == 1 ? a.p[c] : 0.0f;
+          float gr = pfr - pba;
+          gr = scale * gr;
+          val = val - gr;
+        }
+      }
+      bool back = k == 0 || a.label[c - 1] == 2;
+      bool front = k == nz || a.label[c] == 2;
+      if (back || front) val = a.solid_w ? a.solid_w[g] : 0.0f;
+      a.w[g] = val;
+    }
+  }
+}
+
+// ------------------------------------------------------------------- G2P
+__device__ __forceinline__ float clampf(float x, float lo, float hi) {
+  return x < lo ? lo : (x > hi ? hi : x);
+}
+
+// sample3, gridmath.py:29-63
+__device__ __forceinline__ float sample3(const float *__restrict__ f, float fx, float fy,
+                                         float fz, int nxm, int nym, int nzm) {
+  fx = clampf(fx, 0.0f, (float)nxm);
+  fy = clampf(fy, 0.0f, (float)nym);
+  fz = clampf(fz, 0.0f, (float)nzm);
+  int i0 = __float2int_rz(floorf(fx)), j0 = __float2int_rz(floorf(fy)),
+      k0 = __float2int_rz(floorf(fz));
+  if (i0 >= nxm) i0 = nxm - 1;
+  if (j0 >= nym) j0 = nym - 1;
+  if (k0 >= nzm) k0 = nzm - 1;
+  if (i0 < 0) i0 = 0;
+  if (j0 < 0) j0 = 0;
+  if (k0 < 0) k0 = 0;
+  int i1 = i0 + 1, j1 = j0 + 1, k1 = k0 + 1;
+  if (i1 >= nxm) i1 = nxm - 1;
+  if (j1 >= nym) j1 = nym - 1;
+  if (k1 >= nzm) k1 = nzm - 1;
+  float sx = clampf(fx - (float)i0, 0.0f, 1.0f);
+  float sy = clampf(fy - (float)j0, 0.0f, 1.0f);
+  float sz = clampf(fz - (float)k0, 0.0f, 1.0f);
+  const int64_t sI = (int64_t)nym * nzm;
+  const int64_t b00 = i0 * sI + (int64_t)j0 * nzm, b10 = i1 * sI + (int64_t)j0 * nzm,
+                b01 = i0 * sI + (int64_t)j1 * nzm, b11 = i1 * sI + (int64_t)j1 * nzm;
+  float c000 = __ldg(f + b00 + k0), c100 = __ldg(f + b10 + k0);
+  float c010 = __ldg(f + b01 + k0), c110 = __ldg(f + b11 + k0);
+  float c001 = __ldg(f + b00 + k1), c101 = __ldg(f + b10 + k1);
+  float c011 = __ldg(f + b01 + k1), c111 = __ldg(f + b11 + k1);
+  float ox = 1.0f - sx, oy = 1.0f - sy, oz = 1.0f - sz;
+  float c00 = c000 * ox + c100 * sx;
+  float c10 = c010 * ox + c110 * sx;
+  float c01 = c001 * ox + c101 * sx;
+  float c11 = c011 * ox + c111 * sx;
+  float c0 = c00 * oy + c10 * sy;
+  float c1 = c01 * oy + c11 * sy;
+  return c0 * oz + c1 * sz;
+}
+
+// One face component of k3_g2p_apic_advect (:1626-1724): clamped-index
+// gather of velocity and of the C row.
+__device__ __forceinline__ void apic_gather(const float *__restrict__ f, float px, float py,
+                                            float pz, float dx, float fx, float fy, float fz,
+                                            int snx, int sny, int snz, int ax, float inv,
+                                            float &vel, float &c0, float &c1, float &c2) {
+  int i0 = __float2int_rz(floorf(fx)), j0 = __float2int_rz(floorf(fy)),
+      k0 = __float2int_rz(floorf(fz));
+  float sx = fx - (float)i0, sy = fy - (float)j0, sz = fz - (float)k0;
+  float acc = 0.0f;
+  c0 = 0.0f;
+  c1 = 0.0f;
+  c2 = 0.0f;
+#pragma unroll
+  for (int di = 0; di < 2; ++di)
+#pragma unroll
+    for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+      for (int dk = 0; dk < 2; ++dk) {
+        int ii = i0 + di, jj = j0 + dj, kk = k0 + dk;
+        if (ii < 0) ii = 0;
+        if (jj < 0) jj = 0;
+        if (kk < 0) kk = 0;
+        if (ii > snx - 1) ii = snx - 1;
+        if (jj > sny - 1) jj = sny - 1;
+        if (kk > snz - 1) kk = snz - 1;
+        float wxi = di == 0 ? 1.0f - sx : sx;
+        float wyi = dj == 0 ? 1.0f - sy : sy;
+        float wzi = dk == 0 ? 1.0f - sz : sz;
+        float wt = wxi * wyi;
+        wt = wt * wzi;
+        float val = __ldg(f + ((int64_t)ii * sny + jj) * snz + kk);
+        float t = wt * val;
+        acc = acc + t;
+        float ox = ax == 0 ? (float)ii * dx - px : ((float)ii + 0.5f) * dx - px;
+        float oy = ax == 1 ? (float)jj * dx - py : ((float)jj + 0.5f) * dx - py;
+        float oz = ax == 2 ? (float)kk * dx - pz : ((float)kk + 0.5f) * dx - pz;
+        float fu = t * inv;
+        c0 = c0 + fu * ox;
+        c1 = c1 + fu * oy;
+        c2 = c2 + fu * oz;
+      }
+  vel = acc;
+}
+
+struct G2PArgs {
+  const float4 *rec0, *rec1;
+  const float *u, *v, *w, *us, *vs, *ws;
+  float *pos, *vel, *C;
+  int32_t *pid;
+  int64_t n;
+  float dx, dt, flip_blend, dom0, dom1, dom2;
+  int nx, ny, nz;
+};
+
+template <bool APIC>
+__global__ void __launch_bounds__(256) k_g2p(G2PArgs a) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= a.n) return;
+  const float4 r0 = a.rec0[q];
+  const float px = r0.x, py = r0.y, pz = r0.z;
+  const float dx = a.dx;
+  float gx = __fdiv_rn(px, dx), gy = __fdiv_rn(py, dx), gz = __fdiv_rn(pz, dx);
+  float hx = gx - 0.5f, hy = gy - 0.5f, hz = gz - 0.5f;
+  float nu, nv, nw;
+  if (APIC) {
+    float dd = dx * dx;
+    float inv = __fdiv_rn(3.0f, dd);
+    float c[9];
+    apic_gather(a.u, px, py, pz, dx, gx, hy, hz, a.nx + 1, a.ny, a.nz, 0, inv, nu, c[0], c[1], c[2]);
+    apic_gather(a.v, px, py, pz, dx, hx, gy, hz, a.nx, a.ny + 1, a.nz, 1, inv, nv, c[3], c[4], c[5]);
+    apic_gather(a.w, px, py, pz, dx, hx, hy, gz, a.nx, a.ny, a.nz + 1, 2, inv, nw, c[6], c[7], c[8]);
+#pragma unroll
+    for (int m = 0; m < 9; ++m) a.C[9 * q + m] = c[m];
+  } else {
+    const float4 r1 = a.rec1[q];
+    float pic_u = sample3(a.u, gx, hy, hz, a.nx + 1, a.ny, a.nz);
+    float old_u = sample3(a.us, gx, hy, hz, a.nx + 1, a.ny, a.nz);
+    float pic_v = sample3(a.v, hx, gy, hz, a.nx, a.ny + 1, a.nz);
+    float old_v = sample3(a.vs, hx, gy, hz, a.nx, a.ny + 1, a.nz);
+    float pic_w = sample3(a.w, hx, hy, gz, a.nx, a.ny, a.nz + 1);
+    float old_w = sample3(a.ws, hx, hy, gz, a.nx, a.ny, a.nz + 1);
+    float fu = r1.x + (pic_u - old_u), fv = r1.y + (pic_v - old_v), fw = r1.z + (pic_w - old_w);
+    float ob = 1.0f - a.flip_blend;
+    nu = a.flip_blend * fu + ob * pic_u;
+    nv = a.flip_blend * fv + ob * pic_v;
+    nw = a.flip_blend * fw + ob * pic_w;
+  }
+  a.vel[3 * q] = nu;
+  a.vel[3 * q + 1] = nv;
+  a.vel[3 * q + 2] = nw;
+  const float eps = dx * 1.001f;
+  a.pos[3 * q] = clampf(px + nu * a.dt, eps, a.dom0 - eps);
+  a.pos[3 * q + 1] = clampf(py + nv * a.dt, eps, a.dom1 - eps);
+  a.pos[3 * q + 2] = clampf(pz + nw * a.dt, eps, a.dom2 - eps);
+  a.pid[q] = __float_as_int(r0.w);
+}
+
+// ------------------------------------------------------------------- CFL
+__global__ void k_vmax(const float *__restrict__ vel, int64_t n, float *out) {
+  float m = 0.f;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    float x = vel[3 * i], y = vel[3 * i + 1], z = vel[3 * i + 2];
+    float s = x * x + y * y + z * z;
+    m = fmaxf(m, s);
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int *>(out), __float_as_int(m));
+}
+
+// ------------------------------------------------------------- launchers
+static inline unsigned grid_for(int64_t n, int threads, int num_sms) {
+  int64_t g = (n + threads - 1) / threads;
+  int64_t cap = (int64_t)num_sms * 16;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (unsigned)g;
+}
+
+int launch_p2g(Ctx *c, int transfer) {
+  if (!c->bound) return fail(c, GF_INVALID_ARG, "gf_p2g: buffers not bound");
+  if (transfer == GF_APIC && !c->p.C) return fail(c, GF_INVALID_ARG, "gf_p2g: APIC needs C");
+  cudaStream_t st = c->stream;
+  const int64_t nu = (int64_t)(c->nx + 1) * c->ny * c->nz,
+                nv = (int64_t)c->nx * (c->ny + 1) * c->nz,
+                nw = (int64_t)c->nx * c->ny * (c->nz + 1);
+  float *bufs[6] = {c->f.u, c->f.uw, c->f.v, c->f.vw, c->f.w, c->f.ww};
+  int64_t lens[6] = {nu, nu, nv, nv, nw, nw};
+  for (int q = 0; q < 6; ++q) {
+    int e = check_cuda(c, cudaMemsetAsync(bufs[q], 0, lens[q] * 4, st), "memset p2g");
+    if (e) return e;
+  }
+  P2GArgs a{c->start, c->rec0, c->rec1, c->rec2, c->rec3, c->f.u, c->f.v, c->f.w,
+            c->f.uw, c->f.vw, c->f.ww, c->dx, c->nx, c->ny, c->nz, c->nty, c->ntz};
+  if (c->p.n > 0) {
+    if (transfer == GF_APIC)
+      k_p2g_tile<true><<<c->ntiles, 256, 0, st>>>(a);
+    else
+      k_p2g_tile<false><<<c->ntiles, 256, 0, st>>>(a);
+    c->launches++;
+  }
+  return check_launch(c, "gf_p2g");
+}
+
+static GridArgs grid_args(Ctx *c) {
+  GridArgs a;
+  a.u = c->f.u; a.v = c->f.v; a.w = c->f.w;
+  a.us = c->f.us; a.vs = c->f.vs; a.ws = c->f.ws;
+  a.uw = c->f.uw; a.vw = c->f.vw; a.ww = c->f.ww;
+  a.label = c->f.label;
+  a.solid_u = c->f.solid_u; a.solid_v = c->f.solid_v; a.solid_w = c->f.solid_w;
+  a.div = c->f.div; a.p = c->f.p;
+  a.nx = c->nx; a.ny = c->ny; a.nz = c->nz;
+  return a;
+}
+
+int launch_forces_div(Ctx *c, float gravity, float dt, float rho) {
+  if (!c->bound) return fail(c, GF_INVALID_ARG, "gf_forces_div: buffers not bound");
+  GridArgs a = grid_args(c);
+  float gd = gravity * dt;        // g * dt in float32, as k3_add_gravity
+  float scale = rho * c->dx;      // (rho * dx) / dt, as k3_compute_divergence
+  scale = scale / dt;
+  int64_t nf = (int64_t)(c->nx + 1) * (c->ny + 1) * (c->nz + 1);
+  k_forces<<<grid_for(nf, 256, c->num_sms), 256, 0, c->stream>>>(a, gd);
+  k_divergence<<<grid_for(c->ncell, 256, c->num_sms), 256, 0, c->stream>>>(a, scale);
+  c->launches += 2;
+  return check_launch(c, "gf_forces_div");
+}
+
+int launch_project(Ctx *c, float dt, float rho) {
+  if (!c->bound) return fail(c, GF_INVALID_ARG, "gf_project: buffers not bound");
+  GridArgs a = grid_args(c);
+  float scale = rho * c->dx;  // dt / (rho * dx), as k3_subtract_pressure_grad
+  scale = dt / scale;
+  int64_t nf = (int64_t)(c->nx + 1) * (c->ny + 1) * (c->nz + 1);
+  k_project<<<grid_for(nf, 256, c->num_sms), 256, 0, c->stream>>>(a, scale);
+  c->launches++;
+  return check_launch(c, "gf_project");
+}
+
+int launch_g2p(Ctx *c, int transfer, float flip_blend, float dt) {
+  if (!c->bound) return fail(c, GF_INVALID_ARG, "gf_g2p: buffers not bound");
+  if (transfer == GF_APIC && !c->p.C) return fail(c, GF_INVALID_ARG, "gf_g2p: APIC needs C");
+  if (c->p.n == 0) return GF_OK;
+  G2PArgs a{c->rec0, c->rec1, c->f.u, c->f.v, c->f.w, c->f.us, c->f.vs, c->f.ws,
+            c->p.pos, c->p.vel, c->p.C, c->p.pid, c->p.n, c->dx, dt, flip_blend,
+            c->dom[0], c->dom[1], c->dom[2], c->nx, c->ny, c->nz};
+  unsigned g = (unsigned)((c->p.n + 255) / 256);
+  if (transfer == GF_APIC)
+    k_g2p<true><<<g, 256, 0, c->stream>>>(a);
+  else
+    k_g2p<false><<<g, 256, 0, c->stream>>>(a);
+  c->launches++;
+  return check_launch(c, "gf_g2p");
+}
+
+int launch_vmax(Ctx *c) {
+  int e = check_cuda(c, cudaMemsetAsync(c->vmax_dev, 0, 4, c->stream), "memset vmax");
+  if (e) return e;
+  if (c->p.n > 0) {
+    k_vmax<<<grid_for(c->p.n, 256, c->num_sms), 256, 0, c->stream>>>(c->p.vel, c->p.n,
+                                                                     c->vmax_dev);
+    c->launches++;
+  }
+  return check_launch(c, "gf_vmax");
+}
+
+}  // namespace gf

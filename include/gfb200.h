@@ -1,0 +1,152 @@
+/*
+ * gfb200.h -- C ABI of the B200 (sm_100a) FLIP/PIC/APIC substep library.
+ *
+ * Every entry point replaces one stage of the reference's per-substep pipeline
+ * FlipSolver3D._step_impl (src/gpufluid/solvers/solver3d.py:3475-3667); the
+ * citation beside each declaration names the reference kernel(s) it stands in
+ * for.  The Python host (gpufluid_b200.solver.FlipSolver3D) binds these with
+ * ctypes; a C or C++ host can call them directly.
+ *
+ * Conventions
+ *  - Plain pointers and sizes only.  Device buffers passed in gf_fields /
+ *    gf_particles are owned by the caller; the library never frees them.
+ *    The library allocates its own scratch (binning arrays, sorted particle
+ *    records, pressure workspace) inside gf_create / gf_reserve_particles.
+ *  - Layout is the reference's: C order [i][j][k] (k fastest);
+ *    u (nx+1,ny,nz), v (nx,ny+1,nz), w (nx,ny,nz+1), cell arrays (nx,ny,nz);
+ *    labels are uint8 (0 air, 1 fluid, 2 solid); particles are (n,3) float32
+ *    AoS, the APIC matrix (n,3,3) float32 row-major.
+ *  - Every call returns a gf_status; on failure gf_last_error() describes it.
+ *    No C++ exception crosses the ABI.  All work is asynchronous on the bound
+ *    stream except calls documented as synchronising.
+ *  - A context is not thread-safe; use one context per host thread.
+ */
+#ifndef GFB200_H
+#define GFB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum gf_status {
+  GF_OK = 0,
+  GF_INVALID_ARG = 1,   /* bad size, null pointer, unknown mode */
+  GF_CUDA_ERROR = 2,    /* a CUDA runtime call failed */
+  GF_NOT_CONVERGED = 3, /* iterative solve stopped at its iteration cap */
+  GF_NAN = 4,           /* non-finite value met in a reduction */
+  GF_BREAKDOWN = 5,     /* CG denominator vanished */
+  GF_TIMEOUT = 6,       /* a device-side wait exceeded its spin limit */
+  GF_NO_DEVICE = 7      /* no CUDA device / not an sm_100 device */
+} gf_status;
+
+typedef enum gf_transfer { GF_FLIP = 0, GF_PIC = 1, GF_APIC = 2 } gf_transfer;
+
+typedef enum gf_solver {
+  GF_JACOBI = 0, /* k3_jacobi_pressure, solver3d.py:878-938 */
+  GF_GSRB = 1,   /* k3_gauss_seidel_rb, solver3d.py:1204-1267 */
+  GF_PCG = 2,    /* _pressure_pcg, solver3d.py:2917-3043 (FP32) */
+  GF_PCG_REFINED = 3 /* FP32 PCG with FP64 residual replacement (no reference counterpart) */
+} gf_solver;
+
+typedef struct gf_grid_desc {
+  int32_t nx, ny, nz;
+  float dx;     /* cell size; FlipSolver3D.__init__ solver3d.py:2381 */
+  float dom[3]; /* domain extent n*dx rounded to float32 (advection clamp, :1456-1460) */
+} gf_grid_desc;
+
+typedef struct gf_fields {
+  float *u, *v, *w;    /* MAC face velocities */
+  float *uw, *vw, *ww; /* P2G weight sums (scratch of the reference too) */
+  float *us, *vs, *ws; /* saved pre-force velocities for the FLIP delta */
+  float *p;            /* pressure (nx,ny,nz) */
+  float *div;          /* Poisson right-hand side (nx,ny,nz) */
+  uint8_t *label;      /* 0 air, 1 fluid, 2 solid (nx,ny,nz) */
+  const float *solid_u, *solid_v, *solid_w; /* nullable: static solids (velocity 0) */
+} gf_fields;
+
+typedef struct gf_particles {
+  int64_t n;
+  float *pos;   /* (n,3) */
+  float *vel;   /* (n,3) */
+  float *C;     /* (n,3,3); may be NULL unless transfer == GF_APIC */
+  int32_t *pid; /* (n) original id of the particle held in each storage slot */
+} gf_particles;
+
+typedef struct gf_step_params {
+  float dt;
+  float gravity;     /* signed acceleration on y */
+  float rho;
+  float flip_blend;  /* FLIP/PIC blend alpha (GF_FLIP, GF_PIC) */
+  int32_t transfer;  /* gf_transfer */
+  int32_t solver;    /* gf_solver */
+  int32_t max_iters; /* pressure_iters */
+  int32_t check_every; /* PCG convergence test cadence (reference: 10) */
+  double tol;        /* PCG: relative residual target (reference: 1e-4) */
+  int32_t rhs_sign;  /* PCG: -1 solves A p = -div (physical, Jacobi's sign);
+                        +1 reproduces the reference PCG's r0 = +div */
+  int32_t reserved;
+} gf_step_params;
+
+/* ---- context ------------------------------------------------------------ */
+/* Allocates scratch for a grid and up to max_particles particles on the
+ * current CUDA device (FlipSolver3D.__init__, solver3d.py:2358-2500). */
+int gf_create(const gf_grid_desc *grid, int64_t max_particles, void **ctx_out);
+int gf_destroy(void *ctx);
+/* Grows particle scratch to hold n particles (seed_box re-binding, :2826-2910). */
+int gf_reserve_particles(void *ctx, int64_t n);
+/* Binds caller-owned device buffers (rebinding invalidates captured graphs). */
+int gf_bind(void *ctx, const gf_fields *fields, const gf_particles *parts);
+int gf_set_stream(void *ctx, void *cuda_stream);
+const char *gf_last_error(void *ctx);
+/* Number of kernels this context has launched so far. */
+int64_t gf_launch_count(void *ctx);
+
+/* ---- stages ------------------------------------------------------------- */
+/* k3_clear_grid marker reset (solver3d.py:41-65) + the cell/label part of
+ * k3_p2g (:92-101) + canonical binning: per-particle cell key, fluid labels,
+ * per-cell counts, (cell, pid) ordering, sorted particle records. */
+int gf_bin(void *ctx, int32_t transfer);
+/* k3_p2g (:72-114) / k3_p2g_apic (:1475-1588): weighted face sums into
+ * u,v,w and weights into uw,vw,ww (pre-normalisation, as the reference). */
+int gf_p2g(void *ctx, int32_t transfer);
+/* k3_normalize (:121-142) + k3_add_gravity (:149-156) + k3_enforce_solid_bc
+ * (:758-799) + k3_compute_divergence (:846-871), fused. */
+int gf_forces_div(void *ctx, float gravity, float dt, float rho);
+/* Pressure solve into fields.p: Jacobi/GS-RB loops (:3594-3631) or PCG
+ * (_pressure_pcg :2917-3043).  *iters_out (nullable, host) receives the
+ * iteration count; writing it synchronises the stream. */
+int gf_pressure(void *ctx, const gf_step_params *prm, int32_t *iters_out);
+/* k3_subtract_pressure_grad (:1364-1407) + k3_enforce_solid_bc, fused. */
+int gf_project(void *ctx, float dt, float rho);
+/* k3_g2p_and_advect (:1414-1463) / k3_g2p_apic_advect (:1591-1732); writes
+ * pos, vel, C, pid back into the caller's buffers in sorted storage order. */
+int gf_g2p(void *ctx, int32_t transfer, float flip_blend, float dt);
+/* The whole substep in _step_impl order (:3475-3667). */
+int gf_step(void *ctx, const gf_step_params *prm);
+
+/* ---- results and diagnostics ------------------------------------------- */
+/* Last solve's iteration count, final relative residual (||r||/||r0||),
+ * status; synchronises the stream. */
+int gf_pressure_result(void *ctx, int32_t *iters, double *relres, int32_t *status);
+/* Copies the last gf_bin's results to host arrays (any may be NULL):
+ * key[n] per-particle tile-major cell key (8x8x8 tiles) in storage order,
+ * count[ntiles*512] particles per key, order[n] storage slot of each sorted
+ * position.  *nkeys (nullable) receives ntiles*512.  Synchronises. */
+int gf_bin_read(void *ctx, int32_t *key, int32_t *count, int32_t *order, int64_t *nkeys);
+/* Per-stage device times of the last gf_step when timing is on (ms, 7
+ * entries: bin, p2g, forces_div, pressure, project, g2p, total). */
+int gf_enable_timing(void *ctx, int32_t on);
+int gf_stage_times(void *ctx, float *ms7);
+/* Active 8^3 pressure tiles of the last solve (k_mark_active_blocks,
+ * solver3d.py:953-972): count and tile ids (device pointer). */
+int gf_active_tiles(void *ctx, int32_t *n_active, const int32_t **tiles);
+/* Device |v|^2 max for CFL substepping (k3_vmax_sq_reduce :2241-2252);
+ * synchronises. */
+int gf_vmax(void *ctx, float *vmax_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GFB200_H */

@@ -18,3 +18,29 @@ def oracle():
     from oracle import oracle as o
     o.build()
     return o
+
+
+def _cuda_ok():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def pytest_collection_modifyitems(config, items):
+    if _cuda_ok():
+        return
+    skip = pytest.mark.skip(reason="no CUDA device in this environment")
+    for it in items:
+        if "gpu" in it.keywords:
+            it.add_marker(skip)
+
+
+@pytest.fixture(scope="session")
+def gf():
+    """The package with its shared library loaded (fails if it was not built)."""
+    import gpufluid_b200
+    from gpufluid_b200 import _lib
+    _lib.load()
+    return gpufluid_b200
