@@ -1,0 +1,422 @@
+"""Benchmark: FLIP/APIC substeps per second at 128^3 on B200.
+
+Workload (the 128^3 APIC dam-break configuration): 128^3 cells, dx = 1/128,
+solid one-cell walls, fluid block x in [0,0.4], y in [0,0.6], z in [0,1]
+seeded at 8 particles per cell (3,969,024 particles, the reference seeder's
+arithmetic), a solid sphere at (0.7, 0.2, 0.5) radius 0.12, APIC transfer,
+gravity -9.81, dt = 1/480.  A "step" is one full substep (binning, P2G,
+forces/BC/divergence, pressure, projection, G2P + advection) of the evolving
+scene.
+
+  value   substeps/s with the pressure solved by FP32 PCG with FP64 residual
+          replacement to a true relative residual of 1e-8 (inputs resident in
+          HBM; device time over the timed steps, max over ranks).
+  plain   the same substeps with plain FP32 PCG asked for the same 1e-8
+          (recursive residual), with the true residual it actually reached.
+  e2e     the same substep through the C-ABI-backed public API with the
+          particle state in pinned HOST memory: host->device copy of the
+          state, step, device->host copy of the state, every step.
+  roofline  the PCG kernel: algorithmic bytes per launch / its device time,
+          against the measured HBM copy bandwidth.
+  cpu_baseline  the CPU oracle (a C port of the reference kernels) stepping
+          one substep of the same scene on all host threads, with an FP64 CG
+          pressure solve to the same 1e-8 residual.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+Multi-GPU (torchrun): independent replicas, one per rank ("replicas only":
+the single-scene path does not shard); value sums the substeps of all ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("FLIP substeps/s @128³ (refined vs plain FP32 PCG, same residual); fwd+adj/s")
+GRID = 128
+DT = 1.0 / 480.0
+TOL = 1e-8
+MAX_ITERS = 4000
+SPHERE = ((0.7, 0.2, 0.5), 0.12)
+BOX = ((0.0, 0.0, 0.0), (0.4, 0.6, 1.0))
+WORKLOAD = ("APIC dam break + sphere obstacle, 128^3 (dx=1/128), 8 ppc -> 3,969,024 "
+            "particles, dt=1/480, pressure: FP32 PCG + FP64 residual replacement to 1e-8")
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+
+    def start(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+                except ValueError:
+                    continue
+        if not rows:
+            return None
+        mx = max(r[1] for r in rows)
+        load = [r for r in rows if r[0] > 0.5 * mx] or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i, v in enumerate(r[2]) if v == "Active"})
+        return {"sm_mhz": statistics.median(r[0] for r in load), "sm_max_mhz": mx,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------- scene
+def make_solver(gf, device, graphs=True):
+    from gpufluid_b200 import scene
+    s = gf.FlipSolver3D(GRID, GRID, GRID, transfer_mode="apic", flip_blend=0.95,
+                        device=device, pressure_tol=TOL, enable_cuda_graphs=graphs)
+    s.add_solid_from_sdf(scene.sdf_sphere(s.cell_centers_np(), *SPHERE))
+    s.seed_box(*BOX)
+    return s
+
+
+def snapshot(s):
+    return [t.clone() for t in (s._pos, s._vel, s._C, s._pid)]
+
+
+def restore(s, snap):
+    for dst, src in zip((s._pos, s._vel, s._C, s._pid), snap):
+        dst.copy_(src)
+
+
+def true_relres(s) -> float:
+    """||b - A p|| / ||b|| in float64 for the solver's current p (host numpy,
+    measurement only): A = #non-solid neighbours on the diagonal, -1 per fluid
+    neighbour, fluid cells only; b = -div."""
+    lab = s._label.cpu().numpy()
+    p = s._p.cpu().numpy().astype(np.float64)
+    b = -s.div.cpu().numpy().astype(np.float64)
+    fl = lab == 1
+    diag = np.zeros(lab.shape)
+    acc = np.zeros(lab.shape)
+    for ax in range(3):
+        for sh in (-1, 1):
+            nb_lab = np.full(lab.shape, 2, np.uint8)
+            nb_p = np.zeros(lab.shape)
+            src = [slice(None)] * 3
+            dst = [slice(None)] * 3
+            if sh == -1:
+                dst[ax], src[ax] = slice(1, None), slice(None, -1)
+            else:
+                dst[ax], src[ax] = slice(None, -1), slice(1, None)
+            nb_lab[tuple(dst)] = lab[tuple(src)]
+            nb_p[tuple(dst)] = p[tuple(src)]
+            diag += nb_lab != 2
+            acc += np.where(nb_lab == 1, nb_p, 0.0)
+    r = np.where(fl, b - (diag * p - acc), 0.0)
+    bb = np.linalg.norm(np.where(fl, b, 0.0))
+    return float(np.linalg.norm(r) / bb) if bb > 0 else 0.0
+
+
+def pcg_bytes(st) -> float:
+    """Algorithmic bytes of one PCG launch: per fluid cell 14 B of set-up,
+    48 B per iteration (phase A: z, d_old, code in; d_new, Ad out; phase B:
+    d_new, Ad, x, r, code in; x, r, z out), 48 B per FP64 residual
+    replacement (x64, x, code, b in; x64, x, r, z out); 2 B of stencil code
+    per active-tile cell and per phase."""
+    nf, na = st["n_fluid"], st["n_active_tiles"] * 512
+    it, rep = st["iters"], st["replacements"]
+    return float(nf * (14 + 48 * it + 48 * rep) + na * 2 * (1 + 2 * it))
+
+
+def stage_bytes(P, nf, ncell_active, F):
+    """Algorithmic bytes of the other APIC stages at these sizes."""
+    return {"bin_sort": 136 * P + 12 * ncell_active, "p2g": 60 * P + 24 * F,
+            "forces_div": 8 * F + 5 * ncell_active, "project": 8 * F + 5 * ncell_active,
+            "g2p": 12 * P + 4 * F + 64 * P}
+
+
+# ------------------------------------------------------------- timed loops
+def timed_steps(torch, s, steps, solver):
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = s.launch_count()
+    e0.record(stream)
+    for _ in range(steps):
+        s.step(DT, pressure_iters=MAX_ITERS, pressure_solver=solver)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps, s.launch_count() - l0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import gpufluid_b200 as gf
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = f"cuda:{local}"
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device(device))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    s = make_solver(gf, device, graphs=True)
+    P = s.n_particles
+    for _ in range(args.warmup):
+        s.step(DT, pressure_iters=MAX_ITERS, pressure_solver="pcg_refined")
+    torch.cuda.synchronize()
+    snap = snapshot(s)
+
+    # ---- plain FP32 PCG from the same state (same 1e-8 target, recursive residual)
+    s.step(DT, pressure_iters=MAX_ITERS, pressure_solver="pcg")  # capture its graph
+    torch.cuda.synchronize()
+    restore(s, snap)
+    barrier()
+    torch.cuda.synchronize()
+    ms_plain, _ = timed_steps(torch, s, args.steps, "pcg")
+    plain_stats = s.pressure_stats()
+    plain_true = true_relres(s)
+    restore(s, snap)
+
+    # ---- refined (the value)
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ms_ref, launches = timed_steps(torch, s, args.steps, "pcg_refined")
+    clk = clocks.stop()
+    barrier()
+    ms_ref_max = max_over_ranks(ms_ref)
+    ref_stats = s.pressure_stats()
+    ref_true = true_relres(s)
+
+    # ---- per-stage device times and the PCG kernel (live, same workload)
+    restore(s, snap)
+    s._prof.enabled = True
+    s._L.gf_enable_timing(s._ctx, 1)
+    stage, pcg_ms, pcg_b = [], [], []
+    for _ in range(max(3, min(args.steps, 10))):
+        s.step(DT, pressure_iters=MAX_ITERS, pressure_solver="pcg_refined")
+        t = s.stage_times()
+        st = s.pressure_stats()
+        stage.append(t)
+        pcg_ms.append(t[7])
+        pcg_b.append(pcg_bytes(st))
+    s._L.gf_enable_timing(s._ctx, 0)
+    s._prof.enabled = False
+    stage_ms = np.mean(np.array(stage), axis=0)
+    hbm, peak_kind = peaks()
+    achieved = (np.sum(pcg_b) / 1e9) / (np.sum(pcg_ms) / 1e3)
+    nf = st["n_fluid"]
+    F = (GRID + 1) * GRID * GRID * 3
+    sb = stage_bytes(P, nf, st["n_active_tiles"] * 512, F)
+    stage_gbs = {k: round(sb[k] / 1e9 / (stage_ms[i] / 1e3), 1)
+                 for i, k in ((0, "bin_sort"), (1, "p2g"), (2, "forces_div"), (4, "project"),
+                              (5, "g2p"))}
+
+    # ---- e2e through the public API with host buffers
+    restore(s, snap)
+    host = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for t in snap]
+    for h, t in zip(host, snap):
+        h.copy_(t)
+    devs = (s._pos, s._vel, s._C, s._pid)
+    h2d = sum(t.numel() * t.element_size() for t in host)
+    stream = torch.cuda.current_stream()
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        for d, h in zip(devs, host):
+            d.copy_(h, non_blocking=True)
+        s.step(DT, pressure_iters=MAX_ITERS, pressure_solver="pcg_refined")
+        for d, h in zip(devs, host):
+            h.copy_(d, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    barrier()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(steps=1)
+
+    if rank == 0:
+        value = world * 1000.0 / ms_ref_max
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "substeps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_ref_max, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded seed_box lattice of the reference, sphere SDF obstacle)",
+            "config": {"workload": WORKLOAD, "grid": GRID, "particles": P, "transfer": "apic",
+                       "dt": DT, "pressure": "pcg_refined", "tol": TOL,
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2_policy": "inputs larger than L2: particle state "
+                                    f"{P * 64 / 1e6:.0f} MB + MAC grids {F * 4 * 3 / 1e6:.0f} MB "
+                                    "streamed every substep"},
+            "particle_updates_per_s": round(value * P, 1),
+            "plain_fp32": {"substeps_per_s": round(world * 1000.0 / max_over_ranks(ms_plain), 3),
+                           "ms_per_step": round(ms_plain, 4), "iters_last": plain_stats["iters"],
+                           "recursive_relres": plain_stats["relres"],
+                           "true_relres_fp64": plain_true},
+            "refined": {"ms_per_step": round(ms_ref, 4), "iters_last": ref_stats["iters"],
+                        "replacements_last": ref_stats["replacements"],
+                        "true_relres_fp64": ref_true,
+                        "time_vs_plain": round(ms_ref / ms_plain, 3)},
+            "e2e": {"value": round(world * 1000.0 / ms_e2e, 3), "unit": "substeps/s",
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(h2d)},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": "k_pcg<double,true> (persistent cooperative)",
+                         "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                         "frac": round(achieved / hbm, 4), "traffic": None,
+                         "peak_source": peak_kind,
+                         "bytes_per_launch": round(float(np.mean(pcg_b)), 0),
+                         "ms_per_launch": round(float(np.mean(pcg_ms)), 4)},
+            "stages_ms": {k: round(float(stage_ms[i]), 4) for i, k in enumerate(
+                ("bin_sort", "p2g", "forces_div", "pressure", "project", "g2p", "total",
+                 "pcg_kernel"))},
+            "stages_gbs": stage_gbs,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def cpu_baseline(steps=1):
+    """The CPU oracle on the same scene, all host threads, FP64 CG pressure
+    to the same residual; one substep from the seeded state."""
+    from oracle import oracle
+    oracle.build()
+    o = oracle.OracleFlip(GRID, GRID, GRID, transfer_mode="apic", par=True)
+    m = o.marker
+    m[oracle.sphere_sdf(GRID, GRID, GRID, o.dx, *SPHERE) <= 0.0] = 2
+    pos = oracle.seed_box(o.dx, *BOX)
+    o.set_particles(pos, np.zeros_like(pos))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.step(DT, pressure_iters=MAX_ITERS, pressure_solver="pcg64", tol=TOL)
+    dt = time.perf_counter() - t0
+    return {"value": round(steps / dt, 5), "unit": "substeps/s", "cores": oracle.num_threads(),
+            "kind": "port", "sample": f"{steps} substep(s) of the 128^3 APIC scene from the "
+            f"seeded state ({pos.shape[0]} particles), FP64 CG pressure to {TOL}, "
+            f"{dt:.1f} s wall"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle
+    oracle.build()
+    o = oracle.OracleFlip(GRID, GRID, GRID, transfer_mode="apic", par=True)
+    o.marker[oracle.sphere_sdf(GRID, GRID, GRID, o.dx, *SPHERE) <= 0.0] = 2
+    pos = oracle.seed_box(o.dx, *BOX)
+    o.set_particles(pos, np.zeros_like(pos))
+    for _ in range(args.warmup):
+        o.step(DT, pressure_iters=MAX_ITERS, pressure_solver="pcg64", tol=TOL)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.step(DT, pressure_iters=MAX_ITERS, pressure_solver="pcg64", tol=TOL)
+    dt = time.perf_counter() - t0
+    value = args.steps / dt
+    cores = oracle.num_threads()
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 5), "unit": "substeps/s",
+            "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1000 * dt / args.steps, 2),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "grid": GRID,
+                                            "particles": int(pos.shape[0])},
+            "cpu_baseline": {"value": round(value, 5), "unit": "substeps/s", "cores": cores,
+                             "kind": "port",
+                             "sample": "the CPU oracle (C port of the reference kernels, "
+                                       "OpenMP) stepping the full scene; FP64 CG pressure to "
+                                       f"{TOL} (the reference's FP32 PCG cannot reach it)"},
+            "e2e": {"value": round(value, 5), "unit": "substeps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", type=int, default=128,
+                    help="grid side (smaller sides are for profiling captures only)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    global GRID
+    GRID = args.grid
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -57,6 +57,12 @@ class StepParams(ctypes.Structure):
                 ("rhs_sign", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
+class PressureInfo(ctypes.Structure):
+    _fields_ = [("iters", ctypes.c_int32), ("replacements", ctypes.c_int32),
+                ("status", ctypes.c_int32), ("n_active_tiles", ctypes.c_int32),
+                ("n_fluid", ctypes.c_int64), ("relres", ctypes.c_double)]
+
+
 _SIGS = {
     "gf_create": ([ctypes.POINTER(GridDesc), ctypes.c_int64, ctypes.POINTER(_vp)], ctypes.c_int),
     "gf_destroy": ([_vp], ctypes.c_int),
@@ -80,6 +86,7 @@ _SIGS = {
     "gf_stage_times": ([_vp, _fp], ctypes.c_int),
     "gf_active_tiles": ([_vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(_vp)], ctypes.c_int),
     "gf_vmax": ([_vp, _fp], ctypes.c_int),
+    "gf_pressure_stats": ([_vp, ctypes.POINTER(PressureInfo)], ctypes.c_int),
 }
 
 _lib = None

@@ -272,15 +272,38 @@ int gf_enable_timing(void *ctx, int32_t on) {
   return GF_OK;
 }
 
-int gf_stage_times(void *ctx, float *ms7) {
+int gf_stage_times(void *ctx, float *ms8) {
   Ctx *c = as_ctx(ctx);
-  if (!c || !ms7) return GF_INVALID_ARG;
+  if (!c || !ms8) return GF_INVALID_ARG;
   if (!c->timing) return gf::fail(c, GF_INVALID_ARG, "timing is off");
   int e = gf::check_cuda(c, cudaEventSynchronize(c->ev[6]), "sync timing");
   if (e) return e;
-  for (int q = 0; q < 6; ++q) cudaEventElapsedTime(&ms7[q], c->ev[q], c->ev[q + 1]);
-  cudaEventElapsedTime(&ms7[6], c->ev[0], c->ev[6]);
+  for (int q = 0; q < 6; ++q) cudaEventElapsedTime(&ms8[q], c->ev[q], c->ev[q + 1]);
+  cudaEventElapsedTime(&ms8[6], c->ev[0], c->ev[6]);
+  cudaEventElapsedTime(&ms8[7], c->ev[8], c->ev[9]);
   return GF_OK;
+}
+
+int gf_pressure_stats(void *ctx, gf_pressure_info *info) {
+  Ctx *c = as_ctx(ctx);
+  if (!c || !info) return GF_INVALID_ARG;
+  int32_t it = 0, status = 0;
+  double rel = -1.0;
+  int e = gf_pressure_result(ctx, &it, &rel, &status);
+  if (e && e != GF_TIMEOUT) return e;
+  int32_t host[4] = {0, 0, 0, 0};
+  int e2 = gf::check_cuda(c, cudaMemcpy(host, c->n_active, 16, cudaMemcpyDeviceToHost),
+                          "read active/fluid counts");
+  if (e2) return e2;
+  info->iters = it;
+  info->status = status;
+  info->relres = rel;
+  info->n_active_tiles = host[0];
+  int64_t nf;
+  memcpy(&nf, &host[2], 8);
+  info->n_fluid = nf;
+  info->replacements = (c->last_solver == GF_PCG_REFINED) ? c->state_host->n_replace : 0;
+  return e;
 }
 
 int gf_active_tiles(void *ctx, int32_t *n_active, const int32_t **tiles) {

@@ -79,7 +79,7 @@ struct Ctx {
   int32_t *tile_slot = nullptr;  // [ntiles] slot or -1
   int32_t *tile_list = nullptr;  // [ntiles] tile id of each slot
   int32_t *tile_nbr = nullptr;   // [ntiles*6] neighbour slot or -1
-  int32_t *n_active = nullptr;   // [1]
+  int32_t *n_active = nullptr;   // [0] active tiles, [1..2] fluid-cell count (int64)
   uint16_t *code = nullptr;      // [nkeys]
   float *bdiv = nullptr, *xf = nullptr, *r = nullptr, *z = nullptr;
   float *d0 = nullptr, *d1 = nullptr, *Ad = nullptr;
@@ -92,8 +92,7 @@ struct Ctx {
 
   // diagnostics
   bool timing = false;
-  cudaEvent_t ev[8] = {};
-  float stage_ms[7] = {0, 0, 0, 0, 0, 0, 0};
+  cudaEvent_t ev[10] = {};  // 0..6 stage boundaries, 8..9 around the solver kernel
   int64_t launches = 0;
   float *vmax_dev = nullptr;
   std::string err;

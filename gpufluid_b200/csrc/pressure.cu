@@ -98,6 +98,7 @@ struct SetupArgs {
   uint16_t *code;
   float *bdiv, *x, *r, *z, *d0, *d1, *Ad;
   double *x64;
+  int64_t *n_fluid;
   int nx, ny, nz, ntx, nty, ntz;
 };
 
@@ -134,6 +135,11 @@ __global__ void __launch_bounds__(512) k_tile_setup(SetupArgs a) {
         code = (uint16_t)(CODE_FLUID | (diag << CODE_DIAG_SHIFT) | mask);
         bd = a.div[c];
       }
+    }
+    {
+      const int nf = __syncthreads_count(code != 0);
+      if (l == 0 && nf) atomicAdd(reinterpret_cast<unsigned long long *>(a.n_fluid),
+                                 (unsigned long long)nf);
     }
     a.code[q] = code;
     a.bdiv[q] = bd;
@@ -573,9 +579,12 @@ int launch_pressure(Ctx *c, const gf_step_params *prm) {
     c->launches += 2;
   }
   const bool refined = solver == GF_PCG_REFINED;
+  int64_t *n_fluid = reinterpret_cast<int64_t *>(c->n_active + 2);
+  if ((e = check_cuda(c, cudaMemsetAsync(n_fluid, 0, 8, st), "zero fluid count"))) return e;
   SetupArgs sa{c->f.label, c->f.div, c->n_active, c->tile_list, c->tile_slot, c->tile_nbr,
                c->code, c->bdiv, c->xf, c->r, c->z, c->d0, c->d1, c->Ad,
-               refined ? c->x64 : nullptr, c->nx, c->ny, c->nz, c->ntx, c->nty, c->ntz};
+               refined ? c->x64 : nullptr, n_fluid, c->nx, c->ny, c->nz, c->ntx, c->nty,
+               c->ntz};
   {
     int g = c->ntiles < c->num_sms * 4 ? c->ntiles : c->num_sms * 4;
     k_tile_setup<<<g > 0 ? g : 1, 512, 0, st>>>(sa);
@@ -585,6 +594,7 @@ int launch_pressure(Ctx *c, const gf_step_params *prm) {
   SweepArgs sw{c->n_active, c->tile_nbr, c->code, c->bdiv};
   const float *result = c->xf;
   const double *result64 = nullptr;
+  if (c->timing) cudaEventRecord(c->ev[8], st);
   if (solver == GF_JACOBI) {
     float *a = c->xf, *b = c->z;
     for (int it = 0; it < prm->max_iters; ++it) {
@@ -617,6 +627,7 @@ int launch_pressure(Ctx *c, const gf_step_params *prm) {
     }
     if (e) return e;
   }
+  if (c->timing) cudaEventRecord(c->ev[9], st);
   if ((e = check_cuda(c, cudaMemsetAsync(c->f.p, 0, c->ncell * 4, st), "zero p"))) return e;
   ScatterArgs sc{c->n_active, c->tile_list, c->code, result, result64, c->f.p,
                  c->ny, c->nz, c->nty, c->ntz};

@@ -168,6 +168,9 @@ class FlipSolver3D:
         self._cuda_graph_key = None
         self._cuda_graph_hits = 0
         self._cuda_graph_misses = 0
+        self._graph_launches = 0
+        self._captured_launches = 0
+        self._replayed_launches = 0
         self.attr_color = None
         self.attr_temperature = None
         self.inflows: list = []
@@ -366,11 +369,13 @@ class FlipSolver3D:
                    int(pressure_iters))
             if self._cuda_graph is not None and self._cuda_graph_key == key:
                 self._cuda_graph.replay()
+                self._replayed_launches += self._graph_launches
                 self._cuda_graph_hits += 1
                 self._pressure_stale = True
                 return
             self._capture(prm, key)
             self._cuda_graph.replay()
+            self._replayed_launches += self._graph_launches
             self._cuda_graph_misses += 1
             self._pressure_stale = True
             return
@@ -378,7 +383,7 @@ class FlipSolver3D:
         _lib.check(self._L.gf_step(self._ctx, _lib.ctypes.byref(prm)), self._ctx, "gf_step")
         self._pressure_stale = True
         if self._prof.enabled:
-            ms = (_lib.ctypes.c_float * 7)()
+            ms = (_lib.ctypes.c_float * 8)()
             _lib.check(self._L.gf_stage_times(self._ctx, ms), self._ctx, "gf_stage_times")
             self._prof.record(list(ms))
 
@@ -388,10 +393,14 @@ class FlipSolver3D:
         torch.cuda.synchronize(self.device)
         g = torch.cuda.CUDAGraph()
         s = torch.cuda.Stream(self.device)
+        before = int(self._L.gf_launch_count(self._ctx))
         with torch.cuda.graph(g, stream=s):
             self._L.gf_set_stream(self._ctx, s.cuda_stream)
             _lib.check(self._L.gf_step(self._ctx, _lib.ctypes.byref(prm)), self._ctx,
                        "gf_step (capture)")
+        # capturing records launches without running them: count them per replay
+        self._graph_launches = int(self._L.gf_launch_count(self._ctx)) - before
+        self._captured_launches += self._graph_launches
         self._cuda_graph, self._cuda_graph_key = g, key
         self._graph_stream = s
 
@@ -482,8 +491,29 @@ class FlipSolver3D:
         self._set_particles(pos=pos, vel=vel, C=aff)
 
     # --------------------------------------------------------- diagnostics
+    def pressure_stats(self) -> dict:
+        """Iterations, FP64 residual replacements, status, active tiles, fluid
+        cells and final relative residual of the last pressure solve."""
+        info = _lib.PressureInfo()
+        self._set_stream()
+        _lib.check(self._L.gf_pressure_stats(self._ctx, _lib.ctypes.byref(info)), self._ctx,
+                   "gf_pressure_stats")
+        return {"iters": info.iters, "replacements": info.replacements, "status": info.status,
+                "n_active_tiles": info.n_active_tiles, "n_fluid": int(info.n_fluid),
+                "relres": info.relres}
+
+    def stage_times(self) -> list:
+        """Device ms of the last step: bin, p2g, forces_div, pressure,
+        project, g2p, total, solver kernel (needs enable_timing=True)."""
+        ms = (_lib.ctypes.c_float * 8)()
+        _lib.check(self._L.gf_stage_times(self._ctx, ms), self._ctx, "gf_stage_times")
+        return list(ms)
+
     def launch_count(self) -> int:
-        return int(self._L.gf_launch_count(self._ctx))
+        """Kernels of this library executed for this solver (direct launches
+        plus the kernel nodes of every CUDA-graph replay)."""
+        return (int(self._L.gf_launch_count(self._ctx)) - self._captured_launches
+                + self._replayed_launches)
 
 
 def cfl_substep_count(vel_np: np.ndarray, dx: float, target_dt: float, cfl: float = 0.5,

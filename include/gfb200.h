@@ -135,10 +135,22 @@ int gf_pressure_result(void *ctx, int32_t *iters, double *relres, int32_t *statu
  * count[ntiles*512] particles per key, order[n] storage slot of each sorted
  * position.  *nkeys (nullable) receives ntiles*512.  Synchronises. */
 int gf_bin_read(void *ctx, int32_t *key, int32_t *count, int32_t *order, int64_t *nkeys);
-/* Per-stage device times of the last gf_step when timing is on (ms, 7
- * entries: bin, p2g, forces_div, pressure, project, g2p, total). */
+/* Per-stage device times of the last gf_step when timing is on (ms, 8
+ * entries: bin, p2g, forces_div, pressure, project, g2p, total, and the
+ * pressure solver's own kernel(s) without set-up and scatter). */
 int gf_enable_timing(void *ctx, int32_t on);
-int gf_stage_times(void *ctx, float *ms7);
+int gf_stage_times(void *ctx, float *ms8);
+
+typedef struct gf_pressure_info {
+  int32_t iters;        /* iterations of the last solve */
+  int32_t replacements; /* FP64 residual replacements (GF_PCG_REFINED) */
+  int32_t status;       /* gf_status of the solve */
+  int32_t n_active_tiles;
+  int64_t n_fluid;      /* fluid cells in the system */
+  double relres;        /* ||r||/||r0|| (PCG), ||b-Ax||/||b|| in FP64 (refined), -1 otherwise */
+} gf_pressure_info;
+/* Statistics of the last pressure solve; synchronises. */
+int gf_pressure_stats(void *ctx, gf_pressure_info *info);
 /* Active 8^3 pressure tiles of the last solve (k_mark_active_blocks,
  * solver3d.py:953-972): count and tile ids (device pointer). */
 int gf_active_tiles(void *ctx, int32_t *n_active, const int32_t **tiles);

@@ -210,6 +210,13 @@ class OracleFlip:
         elif solver == "gsrb":
             L.og_gsrb(*g, _p(self.p), _p(self.div), _p(self.marker, _i32p), iters, self.par)
             self.last_pressure_iters = iters
+        elif solver == "pcg64":
+            # FP64 Jacobi-PCG to relative residual tol (the CPU counterpart of
+            # the refined solve: same residual target, FP64 throughout)
+            p64, it, _ = pcg64(self.marker, self.div, tol=tol, max_iter=max(iters, 1),
+                               rhs_sign=rhs_sign)
+            self.p[...] = p64.astype(np.float32)
+            self.last_pressure_iters = it
         elif solver == "pcg":
             if self._work is None:
                 self._work = np.zeros(5 * self.nx * self.ny * self.nz, np.float32)
