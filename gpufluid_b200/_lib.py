@@ -54,13 +54,18 @@ class StepParams(ctypes.Structure):
                 ("flip_blend", ctypes.c_float), ("transfer", ctypes.c_int32),
                 ("solver", ctypes.c_int32), ("max_iters", ctypes.c_int32),
                 ("check_every", ctypes.c_int32), ("tol", ctypes.c_double),
-                ("rhs_sign", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("rhs_sign", ctypes.c_int32), ("flags", ctypes.c_int32)]
+
+
+GF_FLAG_GLOBAL_PCG = 1
+GF_FLAG_TRACE = 2
 
 
 class PressureInfo(ctypes.Structure):
     _fields_ = [("iters", ctypes.c_int32), ("replacements", ctypes.c_int32),
                 ("status", ctypes.c_int32), ("n_active_tiles", ctypes.c_int32),
-                ("n_fluid", ctypes.c_int64), ("relres", ctypes.c_double)]
+                ("n_fluid", ctypes.c_int64), ("relres", ctypes.c_double),
+                ("kernel", ctypes.c_int32), ("pad", ctypes.c_int32)]
 
 
 _SIGS = {
@@ -87,6 +92,7 @@ _SIGS = {
     "gf_active_tiles": ([_vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(_vp)], ctypes.c_int),
     "gf_vmax": ([_vp, _fp], ctypes.c_int),
     "gf_pressure_stats": ([_vp, ctypes.POINTER(PressureInfo)], ctypes.c_int),
+    "gf_pcg_trace": ([_vp, _vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
 }
 
 _lib = None

@@ -284,6 +284,25 @@ int gf_stage_times(void *ctx, float *ms8) {
   return GF_OK;
 }
 
+int gf_pcg_trace(void *ctx, int64_t *host, int32_t cap, int32_t *n) {
+  Ctx *c = as_ctx(ctx);
+  if (!c || !n) return GF_INVALID_ARG;
+  int32_t it;
+  double rel;
+  int32_t status;
+  int e = gf_pressure_result(ctx, &it, &rel, &status);
+  if (e) return e;
+  int32_t cnt = c->state_host->trace_n;
+  *n = cnt;
+  if (host && cap > 0) {
+    int32_t m = cnt < cap ? cnt : cap;
+    if (m > 0 && (e = gf::check_cuda(c, cudaMemcpy(host, c->trace, (size_t)m * 8,
+                                                   cudaMemcpyDeviceToHost), "read trace")))
+      return e;
+  }
+  return GF_OK;
+}
+
 int gf_pressure_stats(void *ctx, gf_pressure_info *info) {
   Ctx *c = as_ctx(ctx);
   if (!c || !info) return GF_INVALID_ARG;
@@ -303,6 +322,10 @@ int gf_pressure_stats(void *ctx, gf_pressure_info *info) {
   memcpy(&nf, &host[2], 8);
   info->n_fluid = nf;
   info->replacements = (c->last_solver == GF_PCG_REFINED) ? c->state_host->n_replace : 0;
+  info->kernel = 0;
+  if (c->last_solver == GF_PCG || c->last_solver == GF_PCG_REFINED)
+    info->kernel = c->state_host->smem_solver ? 1 : 2;
+  info->pad = 0;
   return e;
 }
 

@@ -28,6 +28,7 @@ namespace gf {
 constexpr int TILE = 8;            // tile edge in cells (the reference's BLOCK_SIZE, :950)
 constexpr int TILE_CELLS = 512;    // cells per tile
 constexpr int MAX_PCG_BLOCKS = 4096;
+constexpr int TRACE_CAP = 4096;
 
 // Stencil code bits (per compact cell).
 constexpr uint16_t CODE_NB_MASK = 0x3F;   // bit b: neighbour b is fluid (-x,+x,-y,+y,-z,+z)
@@ -50,8 +51,32 @@ struct PcgState {
   unsigned bar_count;
   unsigned bar_gen;
   int error;       // set on a barrier timeout
-  int pad;
+  int fallback;    // 1: the active region exceeded the shared-memory solver
+  unsigned long long bar64;  // monotonic arrival counter (shared-memory solver)
+  int smem_solver; // 1: the last solve ran in the shared-memory solver
+  int trace_n;     // globaltimer stamps recorded (diagnostic trace)
 };
+
+// Shared-memory-resident PCG (pcg_smem.cu).  Returns GF_OK after enqueuing;
+// sets *launched to 1 when it was enqueued (it may still defer at run time to
+// the global-memory solver through PcgState::fallback).
+struct PcgSmemArgs {
+  const int32_t *n_active, *nbr, *tile_cost;
+  const uint16_t *code;
+  const float *bdiv;
+  float *xf;       // result (compact)
+  float *hr0, *hr1, *hw0, *hw1, *hs0, *hs1;  // halo r, w, s by parity (compact index space)
+  double *x64;     // refined: result and FP64 halo (compact)
+  double *partials;  // [2][4][grid]
+  unsigned long long *counter;  // barrier arrival counter (zeroed per solve)
+  PcgState *st;
+  long long *trace;  // nullable: per-phase globaltimer stamps of block 0
+  int trace_cap;
+  int max_iter, check_every;
+  double tol2, replace2;
+  float sign;
+};
+
 
 struct Ctx {
   // grid
@@ -85,6 +110,11 @@ struct Ctx {
   float *d0 = nullptr, *d1 = nullptr, *Ad = nullptr;
   double *x64 = nullptr;
   double *partials = nullptr;    // [3 * MAX_PCG_BLOCKS]
+  unsigned long long *bar_counters = nullptr;  // 8 lines x 16 u64
+  float *halo = nullptr;         // [6 * nkeys] halo publication buffers
+  int32_t *tile_cost = nullptr;  // [ntiles] per-slot PCG work estimate
+  long long *trace = nullptr;    // [TRACE_CAP] PCG phase timestamps
+  bool trace_on = false;
   PcgState *state = nullptr;
   PcgState *state_host = nullptr;  // pinned mirror
   int last_solver = -1;  // gf_solver of the last gf_pressure
@@ -115,6 +145,9 @@ int launch_pressure(Ctx *c, const gf_step_params *prm);
 int launch_project(Ctx *c, float dt, float rho);
 int launch_g2p(Ctx *c, int transfer, float flip_blend, float dt);
 int launch_vmax(Ctx *c);
+
+int launch_pcg_smem(Ctx *c, PcgSmemArgs &a, bool refined);
+bool pcg_smem_fits(Ctx *c, bool refined);
 
 int pressure_alloc(Ctx *c);
 void pressure_free(Ctx *c);

@@ -1,0 +1,676 @@
+// Shared-memory-resident Jacobi-preconditioned CG for the pressure system of
+// _pressure_pcg (src/gpufluid/solvers/solver3d.py:2917-3043): the same
+// operator (diag = #non-solid neighbours, -1 per fluid neighbour), the same
+// preconditioner (z = r / max(diag, 1)) and stop test (||r||^2 < tol^2
+// ||r0||^2, checked every check_every iterations), written in the
+// single-reduction form of Chronopoulos & Gear (1989): with w = A z,
+//   d = z + beta d,  s = w + beta s,  x += alpha d,  r -= alpha s,  z = M r,
+//   w = A z,  gamma = r.z,  delta = w.z,
+//   beta' = gamma'/gamma,  alpha' = gamma' / (delta' - beta' gamma' / alpha),
+// which is algebraically the reference's iteration but needs ONE grid-wide
+// reduction per iteration instead of two.
+//
+// One cooperative block of 1024 threads per SM.  Block b owns the contiguous
+// run of active tile slots [b0, b1) (balanced split of n_active) and keeps its
+// cells' x, r, d, s, stencil codes and a padded 10x10x10 box of z per tile in
+// shared memory for the whole solve (plus the FP64 iterate x64 when
+// refining); w lives in registers.  A tile face whose neighbouring tile
+// belongs to another block is a halo face: its fluid cells publish r, s and w
+// (double-buffered by iteration parity) to global memory, and the neighbour
+// block rebuilds their new z = (r - alpha (w + beta s)) / diag with the
+// owner's float32 operations, so every z value is identical wherever it is
+// computed.  Each iteration: own update -> ring fill of the z boxes (from the
+// neighbouring tile's box or the published halo) -> w = A z as a branch-free
+// fixed-offset stencil -> one grid all-reduce of (r.z, w.z, r.r).
+//
+// The grid all-reduce: thread 0 publishes the block's partial sums, arrives
+// with a release-ordered add on a monotonic counter and polls it with acquire
+// loads (bounded spin); every block then sums all partials in one fixed
+// order, so the scalars -- and every decision taken from them -- are the same
+// in all blocks and bit-reproducible from run to run.
+//
+// Refined mode: x accumulates in float32 between FP64 residual replacements
+// (x64 += x; r = b - A x64 in FP64) taken whenever ||r|| fell 100x since the
+// last one or the float32 recursion claims convergence; the solve ends when
+// the FP64 residual meets the target.
+//
+// If the active region holds more than SmemCfg::MAXT tiles per block the
+// kernel sets PcgState::fallback and returns; the global-memory solver (k_pcg
+// in pressure.cu) launched right after it then performs the solve.
+#include "gf_internal.cuh"
+
+namespace gf {
+
+constexpr int SM_THREADS = 1024;
+constexpr long long SM_SPIN_LIMIT = 1LL << 26;
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Deterministic block sums of NV values, returned to every thread.
+// sh holds >= 33 * NV values of T.
+template <typename T, int NV>
+__device__ __forceinline__ void bsum_all(const T (&v)[NV], T (&out)[NV], T *sh) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  T w[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    w[k] = v[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) w[k] += __shfl_down_sync(0xffffffffu, w[k], o);
+    if (lane == 0) sh[k * 33 + wid] = w[k];
+  }
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      T t = lane < (int)(blockDim.x >> 5) ? sh[k * 33 + lane] : (T)0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+      if (lane == 0) sh[k * 33 + 32] = t;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < NV; ++k) out[k] = sh[k * 33 + 32];
+}
+
+constexpr int SM_MAXG = 160;      // blocks (one per SM)
+
+struct GridSync {
+  double *partials;            // [2][4][G]
+  unsigned long long *counter; // monotonic arrival counter (zeroed per solve)
+  int *err;
+  unsigned long long epoch;
+  long long *trace;            // nullable: SM clock stamps of block 0
+  int trace_n, trace_cap;
+};
+
+__device__ __forceinline__ void trace_mark(GridSync &gs) {
+  if (gs.trace && blockIdx.x == 0 && threadIdx.x == 0 && gs.trace_n < gs.trace_cap)
+    gs.trace[gs.trace_n++] = clock64();
+}
+
+__device__ __forceinline__ void red_release_add(unsigned long long *p, unsigned long long v) {
+  asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Grid-wide sum of NV values; every block obtains the same totals.  Thread 0
+// publishes the block's partial sums and arrives with a release-ordered add
+// on the monotonic counter (after __syncthreads, so the whole block's earlier
+// global writes are ordered before it), then polls it with acquire loads
+// (bounded).  Afterwards every block sums all partials in one fixed order.
+template <typename T, int NV>
+__device__ __forceinline__ bool grid_allreduce(GridSync &gs, const T (&v)[NV], T (&tot)[NV],
+                                               T *sh) {
+  trace_mark(gs);
+  T bs[NV];
+  bsum_all<T, NV>(v, bs, sh);
+  const unsigned G = gridDim.x;
+  const int buf = (int)(gs.epoch & 1ull);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) gs.partials[(buf * 4 + k) * G + blockIdx.x] = (double)bs[k];
+    red_release_add(gs.counter, 1ull);
+    const unsigned long long target = (gs.epoch + 1ull) * G;
+    long long spins = 0;
+    while (ld_acquire_u64(gs.counter) < target) {
+      if (++spins > SM_SPIN_LIMIT) {
+        atomicExch(gs.err, 1);
+        break;
+      }
+    }
+  }
+  gs.epoch++;
+  __syncthreads();
+  if (*reinterpret_cast<volatile int *>(gs.err)) return false;
+  T *s_tot = sh + 33 * NV;
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    double pv[NV][SM_MAXG / 32];
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+#pragma unroll
+      for (int m = 0; m < SM_MAXG / 32; ++m) {
+        const unsigned j = lane + 32 * m;
+        pv[k][m] = j < G ? __ldcg(gs.partials + (buf * 4 + k) * G + j) : 0.0;
+      }
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      T acc = 0;
+#pragma unroll
+      for (int m = 0; m < SM_MAXG / 32; ++m) acc += (T)pv[k][m];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+      if (lane == 0) s_tot[k] = acc;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < NV; ++k) tot[k] = s_tot[k];
+  __syncthreads();
+  trace_mark(gs);
+  return true;
+}
+
+// Where the value of neighbour `dir` of local cell L lives: shared memory
+// (returns true, Lnb) or another block's halo (returns false, qnb).
+__device__ __forceinline__ bool nb_where(int L, int dir, int b0, int b1, const int *s_nbr,
+                                         int &Lnb, int64_t &qnb) {
+  const int tl = L >> 9, l = L & 511;
+  const int li = l >> 6, lj = (l >> 3) & 7, lk = l & 7;
+  int off, lw;
+  bool inside;
+  switch (dir) {
+    case 0: inside = li > 0; off = -64; lw = 448 | (l & 63); break;
+    case 1: inside = li < 7; off = 64; lw = l & 63; break;
+    case 2: inside = lj > 0; off = -8; lw = (l & 0x1C7) | 56; break;
+    case 3: inside = lj < 7; off = 8; lw = l & 0x1C7; break;
+    case 4: inside = lk > 0; off = -1; lw = l | 7; break;
+    default: inside = lk < 7; off = 1; lw = l & ~7; break;
+  }
+  if (inside) {
+    Lnb = L + off;
+    return true;
+  }
+  const int s = s_nbr[tl * 6 + dir];
+  if (s >= b0 && s < b1) {
+    Lnb = (s - b0) * 512 + lw;
+    return true;
+  }
+  qnb = (int64_t)s * 512 + lw;
+  return false;
+}
+
+__device__ __forceinline__ bool is_halo(int L, const uint8_t *s_mask) {
+  const int l = L & 511, m = s_mask[L >> 9];
+  const int li = l >> 6, lj = (l >> 3) & 7, lk = l & 7;
+  return (li == 0 && (m & 1)) || (li == 7 && (m & 2)) || (lj == 0 && (m & 4)) ||
+         (lj == 7 && (m & 8)) || (lk == 0 && (m & 16)) || (lk == 7 && (m & 32));
+}
+
+// Padded-box offsets: a tile's d values live in a 10x10x10 box whose interior
+// (1..8)^3 is the tile and whose one-cell ring holds the neighbours' values.
+__device__ __forceinline__ int pad_of(int l) {
+  return ((l >> 6) + 1) * 100 + (((l >> 3) & 7) + 1) * 10 + ((l & 7) + 1);
+}
+// Ring position (in the box) and neighbour-tile cell index of face position p
+// (0..63) of face `dir`.
+__device__ __forceinline__ void face_map(int dir, int p, int &ring, int &lw) {
+  const int hi = p >> 3, lo = p & 7;
+  switch (dir) {
+    case 0: ring = (hi + 1) * 10 + (lo + 1); lw = 448 + p; break;
+    case 1: ring = 900 + (hi + 1) * 10 + (lo + 1); lw = p; break;
+    case 2: ring = (hi + 1) * 100 + (lo + 1); lw = hi * 64 + 56 + lo; break;
+    case 3: ring = (hi + 1) * 100 + 90 + (lo + 1); lw = hi * 64 + lo; break;
+    case 4: ring = (hi + 1) * 100 + (lo + 1) * 10; lw = hi * 64 + lo * 8 + 7; break;
+    default: ring = (hi + 1) * 100 + (lo + 1) * 10 + 9; lw = hi * 64 + lo * 8; break;
+  }
+}
+
+template <bool REF>
+struct SmemCfg {
+  // per tile: x, r, d, s (2048 B each), padded z box (4000 B), code (1024 B),
+  // remote ring diagonals (384 B), x64 (4096 B, refined)
+  static constexpr size_t TILE_BYTES = 4 * 2048 + 4000 + 1024 + 384 + (REF ? 4096 : 0);
+  static constexpr int MAXT = REF ? 12 : 16;  // tiles per block (<= 227 KB with statics)
+  static constexpr int MAXJ = (MAXT * 512 + SM_THREADS - 1) / SM_THREADS;
+  static constexpr size_t BYTES = (size_t)MAXT * TILE_BYTES;
+};
+
+__device__ __forceinline__ float diagz_of(uint16_t code) {
+  return fmaxf((float)((code >> CODE_DIAG_SHIFT) & 7), 1.0f);
+}
+
+// Block boundaries over the active slots, balanced by the per-slot work
+// estimate (fluid cells + ring) and identical in every block; falls back to
+// an equal split of slots when the balanced split would give some block more
+// than maxt tiles.  Uses `scratch` (>= na ints of shared memory).
+__device__ void partition_slots(const int32_t *__restrict__ cost, int na, int maxt, int *scratch,
+                                int *s_bounds) {
+  const int G = gridDim.x;
+  // inclusive prefix of the costs (chunked block scan)
+  __shared__ int carry, warp_sums[32];
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int off = 0; off < na; off += blockDim.x) {
+    const int t = off + threadIdx.x;
+    const int v = t < na ? cost[t] : 0;
+    int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += u;
+    }
+    if (lane == 31) warp_sums[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+      const int sv = lane < nw ? warp_sums[lane] : 0;
+      int si = sv;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, si, o);
+        if (lane >= o) si += u;
+      }
+      if (lane < nw) warp_sums[lane] = si - sv;
+    }
+    __syncthreads();
+    if (t < na) scratch[t] = carry + warp_sums[wid] + incl;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry += warp_sums[wid] + incl;
+    __syncthreads();
+  }
+  const long long total = na > 0 ? scratch[na - 1] : 0;
+  // bound[g] = first slot whose inclusive prefix exceeds total * g / G
+  for (int g = threadIdx.x; g <= G; g += blockDim.x) {
+    int lo = 0, hi = na;
+    const long long target = total * g / G;
+    if (g == G) {
+      lo = na;
+    } else {
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if ((long long)scratch[mid] <= target) lo = mid + 1; else hi = mid;
+      }
+      if (g == 0) lo = 0;
+    }
+    s_bounds[g] = lo;
+  }
+  __syncthreads();
+  int ok = 1;
+  for (int g = threadIdx.x; g < G; g += blockDim.x)
+    if (s_bounds[g + 1] - s_bounds[g] > maxt || s_bounds[g + 1] < s_bounds[g]) ok = 0;
+  ok = __syncthreads_and(ok);
+  if (!ok)
+    for (int g = threadIdx.x; g <= G; g += blockDim.x) s_bounds[g] = (int)((long long)g * na / G);
+  __syncthreads();
+}
+
+template <typename Acc, bool REF>
+__global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
+  using Cfg = SmemCfg<REF>;
+  constexpr int MAXT = Cfg::MAXT, MAXJ = Cfg::MAXJ;
+  static_assert(MAXJ * 3 <= 32, "diagonal pack");
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_nbr[MAXT * 6];
+  __shared__ uint8_t s_mask[MAXT];
+  __shared__ int s_bounds[SM_MAXG + 1];
+  __shared__ Acc sh[33 * 4];
+  __shared__ double shd[33 * 4];
+
+  PcgState *st = a.st;
+  const int na = *a.n_active;
+  const int G = gridDim.x;
+  if (na > G * MAXT) {  // does not fit: the global-memory solver takes over
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->fallback = 1;
+    return;
+  }
+  GridSync gs{a.partials, a.counter, &st->error, 0ull, a.trace, 0, a.trace_cap};
+  if (G > SM_MAXG) {
+    if (threadIdx.x == 0) atomicExch(&st->error, 1);
+    return;
+  }
+  unsigned char *pb = smem;
+  double *s_x64 = reinterpret_cast<double *>(pb);
+  if (REF) pb += (size_t)MAXT * 4096;
+  float *s_x = reinterpret_cast<float *>(pb);
+  float *s_r = s_x + MAXT * 512;
+  float *s_d = s_r + MAXT * 512;
+  float *s_s = s_d + MAXT * 512;
+  float *s_zb = s_s + MAXT * 512;  // padded z boxes, 1000 per tile
+  uint16_t *s_code = reinterpret_cast<uint16_t *>(s_zb + MAXT * 1000);
+  uint8_t *s_rdiag = reinterpret_cast<uint8_t *>(s_code + MAXT * 512);  // 384 per tile
+
+  // the z boxes are not yet in use: borrow them for the partition prefix
+  partition_slots(a.tile_cost, na, MAXT, reinterpret_cast<int *>(s_zb), s_bounds);
+  const int b0 = s_bounds[blockIdx.x], b1 = s_bounds[blockIdx.x + 1];
+  const int nt = b1 - b0;
+  const int64_t q0 = (int64_t)b0 * 512;
+
+  const int l = threadIdx.x & 511, tl0 = threadIdx.x >> 9;
+  const int pc = pad_of(l);
+
+  for (int i = threadIdx.x; i < nt * 6; i += blockDim.x) s_nbr[i] = a.nbr[(int64_t)b0 * 6 + i];
+  for (int i = threadIdx.x; i < nt * 1000; i += blockDim.x) s_zb[i] = 0.f;
+  __syncthreads();
+  for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+    int m = 0;
+    for (int dir = 0; dir < 6; ++dir) {
+      const int sl = s_nbr[t * 6 + dir];
+      if (sl >= 0 && (sl < b0 || sl >= b1)) m |= 1 << dir;
+    }
+    s_mask[t] = (uint8_t)m;
+  }
+  // diagonal (max(count,1)) of remote ring cells, 0 when not fluid
+  for (int w = threadIdx.x; w < nt * 384; w += SM_THREADS) {
+    const int tl = w / 384, rem = w - tl * 384, dir = rem >> 6, p = rem & 63;
+    int ring, lw;
+    face_map(dir, p, ring, lw);
+    const int sl = s_nbr[tl * 6 + dir];
+    uint8_t dg = 0;
+    if (sl >= 0 && (sl < b0 || sl >= b1)) {
+      const uint16_t cd = a.code[(int64_t)sl * 512 + lw];
+      if (cd & CODE_FLUID) dg = (uint8_t)diagz_of(cd);
+    }
+    s_rdiag[w] = dg;
+  }
+  __syncthreads();
+
+#define HR(par) ((par) ? a.hr1 : a.hr0)
+#define HW(par) ((par) ? a.hw1 : a.hw0)
+#define HS(par) ((par) ? a.hs1 : a.hs0)
+
+  // ---- init: r0 = b, z0 = M r0, w0 = A z0; d_{-1} = s_{-1} = 0.  Per-thread
+  // masks: fluid (bit j), halo (bit j), neighbour count (3 bits per j).
+  unsigned fmask = 0, hmask = 0, dpack = 0;
+#pragma unroll
+  for (int j = 0; j < MAXJ; ++j) {
+    const int tl = tl0 + 2 * j;
+    if (tl >= nt) break;
+    const int L = tl * 512 + l;
+    const uint16_t code = a.code[q0 + L];
+    s_code[L] = code;
+    float b = 0.f;
+    if (code & CODE_FLUID) {
+      fmask |= 1u << j;
+      dpack |= (unsigned)((code >> CODE_DIAG_SHIFT) & 7) << (3 * j);
+      b = a.sign * a.bdiv[q0 + L];
+      s_zb[tl * 1000 + pc] = b / diagz_of(code);
+      if (is_halo(L, s_mask)) {
+        hmask |= 1u << j;
+        HR(0)[q0 + L] = b;
+        HS(0)[q0 + L] = 0.f;
+      }
+    }
+    s_r[L] = b;
+    s_x[L] = 0.f;
+    s_d[L] = 0.f;
+    s_s[L] = 0.f;
+    if (REF) s_x64[L] = 0.0;
+  }
+  __syncthreads();
+  // ring fill of z0: remote z0 = M b (b is read-only input, no barrier needed)
+  for (int w = threadIdx.x; w < nt * 384; w += SM_THREADS) {
+    const int tl = w / 384, rem = w - tl * 384, dir = rem >> 6, p = rem & 63;
+    const int sl = s_nbr[tl * 6 + dir];
+    if (sl < 0) continue;
+    int ring, lw;
+    face_map(dir, p, ring, lw);
+    float v = 0.f;
+    if (sl >= b0 && sl < b1) {
+      v = s_zb[(sl - b0) * 1000 + pad_of(lw)];
+    } else if (s_rdiag[w]) {
+      v = (a.sign * a.bdiv[(int64_t)sl * 512 + lw]) / (float)s_rdiag[w];
+    }
+    s_zb[tl * 1000 + ring] = v;
+  }
+  __syncthreads();
+
+  // w = A z for own fluid cells (non-fluid box entries are exactly 0, so the
+  // branch-free six-neighbour sum equals the reference's fluid-only sum)
+  auto stencil = [&](int j, float &z) -> float {
+    const float *zp = s_zb + (tl0 + 2 * j) * 1000 + pc;
+    float acc = zp[-100];
+    acc = acc + zp[100];
+    acc = acc + zp[-10];
+    acc = acc + zp[10];
+    acc = acc + zp[-1];
+    acc = acc + zp[1];
+    z = *zp;
+    return (float)((dpack >> (3 * j)) & 7) * z - acc;
+  };
+  float wr[MAXJ];
+  Acc v3[3] = {0, 0, 0};
+#pragma unroll
+  for (int j = 0; j < MAXJ; ++j) {
+    wr[j] = 0.f;
+    if (!((fmask >> j) & 1)) continue;
+    const int L = (tl0 + 2 * j) * 512 + l;
+    float z;
+    const float wn = stencil(j, z);
+    const float r = s_r[L];
+    wr[j] = wn;
+    if ((hmask >> j) & 1) HW(0)[q0 + L] = wn;
+    v3[0] += (Acc)(r * z);
+    v3[1] += (Acc)(wn * z);
+    v3[2] += (Acc)(r * r);
+  }
+  Acc t3[3];
+  if (!grid_allreduce<Acc, 3>(gs, v3, t3, sh)) return;
+  Acc gamma = t3[0];
+  const Acc r0 = t3[2];
+  const double b2 = (double)t3[2];
+  double r_upd2 = b2, r_true2 = b2, rr_last = b2;
+  Acc alpha = fabs((double)t3[1]) < 1.0e-30 ? (Acc)0 : gamma / t3[1];
+  Acc beta = 0;
+  int done = (double)r0 < 1e-30 ? 1 : 0, iters = 0, nrep = 0, status = GF_OK;
+
+  for (int it = 0; it < a.max_iter && !done; ++it) {
+    const int par = it & 1, npar = par ^ 1;
+    const float alphaf = (float)alpha, nalpha = -alphaf, betaf = (float)beta;
+    // ---- own: d = z + beta d; s = w + beta s; x += alpha d; r -= alpha s; z = M r
+#pragma unroll
+    for (int j = 0; j < MAXJ; ++j) {
+      if (!((fmask >> j) & 1)) continue;
+      const int tl = tl0 + 2 * j, L = tl * 512 + l;
+      float *zp = s_zb + tl * 1000 + pc;
+      const float dn = *zp + betaf * s_d[L];
+      const float sn = wr[j] + betaf * s_s[L];
+      s_d[L] = dn;
+      s_s[L] = sn;
+      s_x[L] = s_x[L] + alphaf * dn;
+      const float rn = s_r[L] + nalpha * sn;
+      s_r[L] = rn;
+      *zp = rn / fmaxf((float)((dpack >> (3 * j)) & 7), 1.0f);
+      if ((hmask >> j) & 1) {
+        HR(npar)[q0 + L] = rn;
+        HS(npar)[q0 + L] = sn;
+      }
+    }
+    __syncthreads();
+    // ---- ring fill of the new z: another block's cell is rebuilt from its
+    // published r_i, w_i, s_{i-1} with the owner's float32 operations
+    for (int w = threadIdx.x; w < nt * 384; w += SM_THREADS) {
+      const int tl = w / 384, rem = w - tl * 384, dir = rem >> 6, p = rem & 63;
+      const int sl = s_nbr[tl * 6 + dir];
+      if (sl < 0) continue;
+      int ring, lw;
+      face_map(dir, p, ring, lw);
+      if (sl >= b0 && sl < b1) {
+        s_zb[tl * 1000 + ring] = s_zb[(sl - b0) * 1000 + pad_of(lw)];
+      } else if (s_rdiag[w]) {
+        const int64_t qn = (int64_t)sl * 512 + lw;
+        const float sn = __ldcg(HW(par) + qn) + betaf * __ldcg(HS(par) + qn);
+        const float rn = __ldcg(HR(par) + qn) + nalpha * sn;
+        s_zb[tl * 1000 + ring] = rn / (float)s_rdiag[w];
+      }
+    }
+    __syncthreads();
+    // ---- w = A z and the three dot products
+    Acc vv[3] = {0, 0, 0};
+#pragma unroll
+    for (int j = 0; j < MAXJ; ++j) {
+      if (!((fmask >> j) & 1)) continue;
+      const int L = (tl0 + 2 * j) * 512 + l;
+      float z;
+      const float wn = stencil(j, z);
+      const float r = s_r[L];
+      wr[j] = wn;
+      if ((hmask >> j) & 1) HW(npar)[q0 + L] = wn;
+      vv[0] += (Acc)(r * z);
+      vv[1] += (Acc)(wn * z);
+      vv[2] += (Acc)(r * r);
+    }
+    Acc tv[3];
+    if (!grid_allreduce<Acc, 3>(gs, vv, tv, sh)) return;
+    iters = it + 1;
+    double rr = (double)tv[2];
+    rr_last = rr;
+    if (!(rr == rr) || !((double)tv[1] == (double)tv[1])) {
+      status = GF_NAN;
+      done = 1;
+      break;
+    }
+    bool replace = false;
+    if (REF) {
+      replace = rr < a.replace2 * r_upd2 || rr < a.tol2 * b2;
+    } else {
+      const bool check = (iters % a.check_every) == 0 || iters == a.max_iter;
+      if (check && rr < a.tol2 * (double)r0) done = 1;
+    }
+    if (REF && replace) {
+      // ---- FP64 residual replacement: x64 += x, x = 0; r = b - A x64
+#pragma unroll
+      for (int j = 0; j < MAXJ; ++j) {
+        if (!((fmask >> j) & 1)) continue;
+        const int L = (tl0 + 2 * j) * 512 + l;
+        const double x64 = s_x64[L] + (double)s_x[L];
+        s_x64[L] = x64;
+        s_x[L] = 0.f;
+        if ((hmask >> j) & 1) a.x64[q0 + L] = x64;
+      }
+      {
+        double z0[1] = {0.0}, zt[1];
+        if (!grid_allreduce<double, 1>(gs, z0, zt, shd)) return;
+      }
+      double vr[1] = {0.0};
+#pragma unroll
+      for (int j = 0; j < MAXJ; ++j) {
+        if (!((fmask >> j) & 1)) continue;
+        const int tl = tl0 + 2 * j, L = tl * 512 + l;
+        const uint16_t code = s_code[L];
+        double sum = 0.0;
+#pragma unroll
+        for (int dir = 0; dir < 6; ++dir)
+          if (code & (1 << dir)) {
+            int Lnb;
+            int64_t qnb;
+            sum += nb_where(L, dir, b0, b1, s_nbr, Lnb, qnb) ? s_x64[Lnb] : __ldcg(a.x64 + qnb);
+          }
+        const double diag = (double)((code >> CODE_DIAG_SHIFT) & 7);
+        const double res = (double)(a.sign * a.bdiv[q0 + L]) - (diag * s_x64[L] - sum);
+        const float rf = (float)res;
+        s_r[L] = rf;
+        s_zb[tl * 1000 + pc] = rf / diagz_of(code);
+        if ((hmask >> j) & 1) HR(npar)[q0 + L] = rf;
+        vr[0] += res * res;
+      }
+      double tr[1];
+      if (!grid_allreduce<double, 1>(gs, vr, tr, shd)) return;
+      r_true2 = tr[0];
+      // ring fill of z = M r from the replaced residuals, then w = A z
+      for (int w = threadIdx.x; w < nt * 384; w += SM_THREADS) {
+        const int tl = w / 384, rem = w - tl * 384, dir = rem >> 6, p = rem & 63;
+        const int sl = s_nbr[tl * 6 + dir];
+        if (sl < 0) continue;
+        int ring, lw;
+        face_map(dir, p, ring, lw);
+        if (sl >= b0 && sl < b1)
+          s_zb[tl * 1000 + ring] = s_zb[(sl - b0) * 1000 + pad_of(lw)];
+        else if (s_rdiag[w])
+          s_zb[tl * 1000 + ring] = __ldcg(HR(npar) + (int64_t)sl * 512 + lw) / (float)s_rdiag[w];
+      }
+      __syncthreads();
+      Acc vw[3] = {0, 0, 0};
+#pragma unroll
+      for (int j = 0; j < MAXJ; ++j) {
+        if (!((fmask >> j) & 1)) continue;
+        const int L = (tl0 + 2 * j) * 512 + l;
+        float z;
+        const float wn = stencil(j, z);
+        const float r = s_r[L];
+        wr[j] = wn;
+        if ((hmask >> j) & 1) HW(npar)[q0 + L] = wn;
+        vw[0] += (Acc)(r * z);
+        vw[1] += (Acc)(wn * z);
+        vw[2] += (Acc)(r * r);
+      }
+      if (!grid_allreduce<Acc, 3>(gs, vw, tv, sh)) return;
+      ++nrep;
+      r_upd2 = (double)tv[2];
+      rr_last = r_upd2;
+      if (r_true2 <= a.tol2 * b2) done = 1;
+    }
+    // ---- scalars of the next iteration (Chronopoulos-Gear)
+    const Acc gamma_new = tv[0], delta = tv[1];
+    const Acc bnew = fabs((double)gamma) < 1.0e-30 ? (Acc)0 : gamma_new / gamma;
+    const Acc den = delta - (fabs((double)alpha) < 1.0e-30 ? (Acc)0 : bnew * gamma_new / alpha);
+    alpha = fabs((double)den) < 1.0e-30 ? (Acc)0 : gamma_new / den;
+    beta = bnew;
+    gamma = gamma_new;
+  }
+  // ---- results
+#pragma unroll
+  for (int j = 0; j < MAXJ; ++j) {
+    const int tl = tl0 + 2 * j;
+    if (tl >= nt) break;
+    const int L = tl * 512 + l;
+    a.xf[q0 + L] = s_x[L];
+    if (REF) a.x64[q0 + L] = s_x64[L];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->trace_n = gs.trace_n;
+    st->iters = iters;
+    st->r0 = (double)r0;
+    st->rr = rr_last;
+    st->b2 = b2;
+    st->r_true2 = r_true2;
+    st->n_replace = nrep;
+    st->done = done;
+    st->status = done ? status : GF_NOT_CONVERGED;
+    if (status != GF_OK) st->status = status;
+    st->smem_solver = 1;
+  }
+#undef HR
+#undef HW
+#undef HS
+}
+
+template <typename Acc, bool REF>
+static bool fits_t(Ctx *c) {
+  int optin = 0;
+  cudaFuncAttributes fa;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device) !=
+          cudaSuccess ||
+      cudaFuncGetAttributes(&fa, (const void *)k_pcg_smem<Acc, REF>) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return SmemCfg<REF>::BYTES + fa.sharedSizeBytes <= (size_t)optin;
+}
+
+bool pcg_smem_fits(Ctx *c, bool refined) {
+  return refined ? fits_t<double, true>(c) : fits_t<float, false>(c);
+}
+
+template <typename Acc, bool REF>
+static int launch_t(Ctx *c, PcgSmemArgs &a) {
+  const size_t smem = SmemCfg<REF>::BYTES;
+  auto fn = k_pcg_smem<Acc, REF>;
+  int e = check_cuda(c, cudaFuncSetAttribute((const void *)fn,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem),
+                     "PCG shared-memory size");
+  if (e) return e;
+  int per_sm = 0;
+  e = check_cuda(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, SM_THREADS, smem),
+                 "PCG occupancy");
+  if (e) return e;
+  if (per_sm < 1) return fail(c, GF_CUDA_ERROR, "PCG shared-memory kernel does not fit an SM");
+  void *args[] = {&a};
+  e = check_cuda(c, cudaLaunchCooperativeKernel((const void *)fn, dim3(c->num_sms),
+                                                dim3(SM_THREADS), args, smem, c->stream),
+                 "cooperative shared-memory PCG launch");
+  c->launches++;
+  return e;
+}
+
+int launch_pcg_smem(Ctx *c, PcgSmemArgs &a, bool refined) {
+  return refined ? launch_t<double, true>(c, a) : launch_t<float, false>(c, a);
+}
+
+}  // namespace gf

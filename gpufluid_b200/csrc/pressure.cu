@@ -99,6 +99,7 @@ struct SetupArgs {
   float *bdiv, *x, *r, *z, *d0, *d1, *Ad;
   double *x64;
   int64_t *n_fluid;
+  int32_t *tile_cost;  // per slot: fluid cells + 192 (work estimate of the PCG)
   int nx, ny, nz, ntx, nty, ntz;
 };
 
@@ -138,6 +139,7 @@ __global__ void __launch_bounds__(512) k_tile_setup(SetupArgs a) {
     }
     {
       const int nf = __syncthreads_count(code != 0);
+      if (l == 0) a.tile_cost[s] = nf + 192;
       if (l == 0 && nf) atomicAdd(reinterpret_cast<unsigned long long *>(a.n_fluid),
                                  (unsigned long long)nf);
     }
@@ -220,6 +222,7 @@ struct PcgArgs {
   double tol2;     // tol^2
   double replace2; // residual-replacement factor^2 (refined)
   float sign;      // b = sign * div
+  int only_if_fallback;  // run only when the shared-memory solver deferred
 };
 
 template <typename T>
@@ -317,6 +320,7 @@ __device__ bool grid_barrier(const PcgArgs &a) {
 
 template <typename Acc, bool REF>
 __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
+  if (a.only_if_fallback && !ld_volatile_i(&a.st->fallback)) return;
   const int64_t total = (int64_t)(*a.n_active) * TILE_CELLS;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const int64_t q0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -520,6 +524,10 @@ int pressure_alloc(Ctx *c) {
   if ((e = A((void **)&c->partials, 3 * MAX_PCG_BLOCKS * sizeof(double), "alloc partials")))
     return e;
   if ((e = A((void **)&c->state, sizeof(PcgState), "alloc pcg state"))) return e;
+  if ((e = A((void **)&c->bar_counters, 8 * 16 * 8, "alloc barrier counters"))) return e;
+  if ((e = A((void **)&c->trace, TRACE_CAP * 8, "alloc trace"))) return e;
+  if ((e = A((void **)&c->halo, nk * 6 * 4, "alloc halo buffers"))) return e;
+  if ((e = A((void **)&c->tile_cost, (size_t)c->ntiles * 4, "alloc tile cost"))) return e;
   if ((e = check_cuda(c, cudaMemset(c->state, 0, sizeof(PcgState)), "zero pcg state"))) return e;
   if ((e = check_cuda(c, cudaMallocHost((void **)&c->state_host, sizeof(PcgState)),
                       "alloc pinned state")))
@@ -530,7 +538,8 @@ int pressure_alloc(Ctx *c) {
 
 void pressure_free(Ctx *c) {
   void *ps[] = {c->tile_slot, c->tile_list, c->tile_nbr, c->n_active, c->code, c->bdiv,
-                c->xf, c->r, c->z, c->d0, c->d1, c->Ad, c->x64, c->partials, c->state};
+                c->xf, c->r, c->z, c->d0, c->d1, c->Ad, c->x64, c->partials, c->state,
+                c->bar_counters, c->trace, c->halo, c->tile_cost};
   for (void *p : ps)
     if (p) cudaFree(p);
   if (c->state_host) cudaFreeHost(c->state_host);
@@ -583,8 +592,8 @@ int launch_pressure(Ctx *c, const gf_step_params *prm) {
   if ((e = check_cuda(c, cudaMemsetAsync(n_fluid, 0, 8, st), "zero fluid count"))) return e;
   SetupArgs sa{c->f.label, c->f.div, c->n_active, c->tile_list, c->tile_slot, c->tile_nbr,
                c->code, c->bdiv, c->xf, c->r, c->z, c->d0, c->d1, c->Ad,
-               refined ? c->x64 : nullptr, n_fluid, c->nx, c->ny, c->nz, c->ntx, c->nty,
-               c->ntz};
+               refined ? c->x64 : nullptr, n_fluid, c->tile_cost, c->nx, c->ny, c->nz, c->ntx,
+               c->nty, c->ntz};
   {
     int g = c->ntiles < c->num_sms * 4 ? c->ntiles : c->num_sms * 4;
     k_tile_setup<<<g > 0 ? g : 1, 512, 0, st>>>(sa);
@@ -614,12 +623,29 @@ int launch_pressure(Ctx *c, const gf_step_params *prm) {
   } else {
     if ((e = check_cuda(c, cudaMemsetAsync(c->state, 0, sizeof(PcgState), st), "zero state")))
       return e;
+    const int check_every = prm->check_every > 0 ? prm->check_every : 1;
+    const float sign = prm->rhs_sign >= 0 ? 1.0f : -1.0f;
+    const double replace2 = 1e-4;  // replace the residual each time it drops by 100x
+    const bool force_global =
+        (prm->flags & GF_FLAG_GLOBAL_PCG) != 0 || !pcg_smem_fits(c, refined);
+    if (!force_global) {
+      if ((e = check_cuda(c, cudaMemsetAsync(c->bar_counters, 0, 8 * 16 * 8, st),
+                          "zero barrier counters")))
+        return e;
+      float *h = c->halo;
+      const int64_t nk = c->nkeys;
+      PcgSmemArgs sa{c->n_active, c->tile_nbr, c->tile_cost, c->code, c->bdiv, c->xf, h, h + nk, h + 2 * nk,
+                     h + 3 * nk, h + 4 * nk, h + 5 * nk, refined ? c->x64 : nullptr,
+                     c->partials, c->bar_counters, c->state,
+                     (prm->flags & GF_FLAG_TRACE) ? c->trace : nullptr, TRACE_CAP,
+                     prm->max_iters, check_every, prm->tol * prm->tol, replace2, sign};
+      if ((e = launch_pcg_smem(c, sa, refined))) return e;
+    }
     PcgArgs pa{c->n_active, c->tile_nbr, c->code, c->bdiv, c->xf, c->r, c->z, c->d0, c->d1,
                c->Ad, refined ? c->x64 : nullptr, c->partials, c->state,
-               prm->max_iters, prm->check_every > 0 ? prm->check_every : 1,
-               prm->tol * prm->tol, 0.0, prm->rhs_sign >= 0 ? 1.0f : -1.0f};
+               prm->max_iters, check_every, prm->tol * prm->tol, replace2, sign,
+               force_global ? 0 : 1};
     if (refined) {
-      pa.replace2 = 1e-4;  // replace the residual each time it drops by 100x
       e = launch_pcg<double, true>(c, pa);
       result64 = c->x64;
     } else {

@@ -86,8 +86,15 @@ typedef struct gf_step_params {
   double tol;        /* PCG: relative residual target (reference: 1e-4) */
   int32_t rhs_sign;  /* PCG: -1 solves A p = -div (physical, Jacobi's sign);
                         +1 reproduces the reference PCG's r0 = +div */
-  int32_t reserved;
+  int32_t flags;     /* GF_FLAG_* */
 } gf_step_params;
+
+/* flags: run PCG in the global-memory kernel even when the active region fits
+ * the shared-memory solver (both give the same iterates up to reduction order) */
+#define GF_FLAG_GLOBAL_PCG 1
+/* flags: record the SM clock (clock64, cycles) at every phase boundary of the
+ * shared-memory PCG in block 0; read the stamps with gf_pcg_trace */
+#define GF_FLAG_TRACE 2
 
 /* ---- context ------------------------------------------------------------ */
 /* Allocates scratch for a grid and up to max_particles particles on the
@@ -148,7 +155,12 @@ typedef struct gf_pressure_info {
   int32_t n_active_tiles;
   int64_t n_fluid;      /* fluid cells in the system */
   double relres;        /* ||r||/||r0|| (PCG), ||b-Ax||/||b|| in FP64 (refined), -1 otherwise */
+  int32_t kernel;       /* PCG kernel that ran: 1 shared-memory resident, 2 global-memory */
+  int32_t pad;
 } gf_pressure_info;
+/* Copies up to cap timestamps (SM cycles) of the last traced PCG solve into host
+ * memory and returns how many were recorded in *n; synchronises. */
+int gf_pcg_trace(void *ctx, int64_t *host, int32_t cap, int32_t *n);
 /* Statistics of the last pressure solve; synchronises. */
 int gf_pressure_stats(void *ctx, gf_pressure_info *info);
 /* Active 8^3 pressure tiles of the last solve (k_mark_active_blocks,

@@ -153,10 +153,18 @@ def _pressure_case(gf, oracle, grid, seed=5):
     return s, o
 
 
-def _params(gf, solver, iters, tol=1e-4, rhs_sign=-1, check_every=10):
+def _params(gf, solver, iters, tol=1e-4, rhs_sign=-1, check_every=10, flags=0):
     from gpufluid_b200 import _lib
     return _lib.StepParams(1 / 240.0, -9.81, 1.0, 0.95, 0, _lib.SOLVER[solver], iters,
-                           check_every, tol, rhs_sign, 0)
+                           check_every, tol, rhs_sign, flags)
+
+
+def _stats(s):
+    from gpufluid_b200 import _lib
+    info = _lib.PressureInfo()
+    s._set_stream()
+    assert s._L.gf_pressure_stats(s._ctx, ctypes.byref(info)) == 0
+    return info
 
 
 @pytest.mark.parametrize("solver,iters", [("jacobi", 1), ("jacobi", 37), ("gsrb", 1), ("gsrb", 25)])
@@ -258,3 +266,49 @@ def test_g2p_bitexact(gf, oracle, grid, transfer, blend):
     assert_bitexact("vel", s.vel.numpy(), o.vel)
     if transfer == "apic":
         assert_bitexact("C", s.affine_C.numpy(), o.C)
+
+
+@pytest.mark.parametrize("solver,tol", [("pcg", 1e-5), ("pcg_refined", 1e-10)])
+@pytest.mark.parametrize("grid", [(24, 24, 24), (48, 40, 56)])
+def test_pcg_shared_memory_matches_global_kernel(gf, oracle, grid, solver, tol):
+    """The shared-memory-resident solver and the global-memory solver run the
+    same recurrences; only the block partition of the dot products differs."""
+    import torch
+    from gpufluid_b200 import _lib
+    res = {}
+    for flags in (0, _lib.GF_FLAG_GLOBAL_PCG):
+        s, o = _pressure_case(gf, oracle, grid, seed=21)
+        prm = _params(gf, solver, 3000, tol=tol, flags=flags)
+        it = ctypes.c_int32()
+        _call(s, "gf_pressure", ctypes.byref(prm), ctypes.byref(it))
+        torch.cuda.synchronize()
+        info = _stats(s)
+        assert info.kernel == (2 if flags else 1)
+        assert info.status == 0
+        res[flags] = (s._p.cpu().numpy(), info.iters)
+    p_s, it_s = res[0]
+    p_g, it_g = res[_lib.GF_FLAG_GLOBAL_PCG]
+    assert abs(it_s - it_g) <= (10 if solver == "pcg" else 3), (it_s, it_g)
+    assert rel_l2(p_s, p_g) < (1e-4 if solver == "pcg" else 1e-6)
+
+
+def test_pcg_large_region_falls_back_to_global_kernel(gf, oracle):
+    """More active tiles than the shared-memory solver holds (148 SMs x 20
+    tiles): the global-memory kernel takes over and still meets the target."""
+    import torch
+    nx, ny, nz = 192, 64, 192
+    s = gf.FlipSolver3D(nx, ny, nz)
+    lab = s._marker_host.copy()
+    lab[1:-1, 1:48, 1:-1] = 1  # fluid below y = 48, air above
+    rng = np.random.default_rng(5)
+    div = np.where(lab == 1, rng.normal(0, 1, lab.shape), 0).astype(np.float32)
+    s._label.copy_(_t(lab.astype(np.uint8)))
+    s.div.copy_(_t(div))
+    prm = _params(gf, "pcg_refined", 4000, tol=1e-9)
+    it = ctypes.c_int32()
+    _call(s, "gf_pressure", ctypes.byref(prm), ctypes.byref(it))
+    torch.cuda.synchronize()
+    info = _stats(s)
+    assert info.n_active_tiles == 24 * 6 * 24
+    assert info.kernel == 2 and info.status == 0
+    assert info.relres <= 1e-9
