@@ -295,7 +295,9 @@ int gf_pcg_trace(void *ctx, int64_t *host, int32_t cap, int32_t *n) {
   int32_t cnt = c->state_host->trace_n;
   *n = cnt;
   if (host && cap > 0) {
-    int32_t m = cnt < cap ? cnt : cap;
+    // block 0's stamps fill the first half, per-block (busy cycles, tiles)
+    // pairs the second half of the buffer
+    int32_t m = cap < gf::TRACE_CAP ? cap : gf::TRACE_CAP;
     if (m > 0 && (e = gf::check_cuda(c, cudaMemcpy(host, c->trace, (size_t)m * 8,
                                                    cudaMemcpyDeviceToHost), "read trace")))
       return e;

@@ -50,34 +50,6 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
   return v;
 }
 
-// Deterministic block sums of NV values, returned to every thread.
-// sh holds >= 33 * NV values of T.
-template <typename T, int NV>
-__device__ __forceinline__ void bsum_all(const T (&v)[NV], T (&out)[NV], T *sh) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  T w[NV];
-#pragma unroll
-  for (int k = 0; k < NV; ++k) {
-    w[k] = v[k];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) w[k] += __shfl_down_sync(0xffffffffu, w[k], o);
-    if (lane == 0) sh[k * 33 + wid] = w[k];
-  }
-  __syncthreads();
-  if (wid == 0) {
-#pragma unroll
-    for (int k = 0; k < NV; ++k) {
-      T t = lane < (int)(blockDim.x >> 5) ? sh[k * 33 + lane] : (T)0;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
-      if (lane == 0) sh[k * 33 + 32] = t;
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < NV; ++k) out[k] = sh[k * 33 + 32];
-}
-
 constexpr int SM_MAXG = 160;      // blocks (one per SM)
 
 struct GridSync {
@@ -87,6 +59,7 @@ struct GridSync {
   unsigned long long epoch;
   long long *trace;            // nullable: SM clock stamps of block 0
   int trace_n, trace_cap;
+  long long busy, t_last;      // per-block cycles spent outside the all-reduce
 };
 
 __device__ __forceinline__ void trace_mark(GridSync &gs) {
@@ -98,61 +71,84 @@ __device__ __forceinline__ void red_release_add(unsigned long long *p, unsigned 
   asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-// Grid-wide sum of NV values; every block obtains the same totals.  Thread 0
-// publishes the block's partial sums and arrives with a release-ordered add
-// on the monotonic counter (after __syncthreads, so the whole block's earlier
-// global writes are ordered before it), then polls it with acquire loads
-// (bounded).  Afterwards every block sums all partials in one fixed order.
+// Grid-wide sum of NV values; every block obtains the same totals.  Two
+// block-level barriers: (1) every warp's shuffle-reduced values land in shared
+// memory; then warp 0 alone sums the block's warps, lane 0 publishes the
+// block's partials and arrives with a release-ordered add on the monotonic
+// counter (after the barrier, so the whole block's earlier global writes are
+// ordered before it) and polls it with acquire loads (bounded spin), and warp
+// 0 sums all blocks' partials in one fixed order; (2) the totals are
+// broadcast.  Every block therefore derives identical scalars, and the
+// result is bit-reproducible from run to run.  sh holds >= 36 * NV values.
 template <typename T, int NV>
 __device__ __forceinline__ bool grid_allreduce(GridSync &gs, const T (&v)[NV], T (&tot)[NV],
                                                T *sh) {
   trace_mark(gs);
-  T bs[NV];
-  bsum_all<T, NV>(v, bs, sh);
-  const unsigned G = gridDim.x;
+  if (gs.trace && threadIdx.x == 0) gs.busy += clock64() - gs.t_last;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  T *s_tot = sh + 32 * NV;  // NV values, alternated by epoch parity below
   const int buf = (int)(gs.epoch & 1ull);
-  if (threadIdx.x == 0) {
 #pragma unroll
-    for (int k = 0; k < NV; ++k) gs.partials[(buf * 4 + k) * G + blockIdx.x] = (double)bs[k];
-    red_release_add(gs.counter, 1ull);
-    const unsigned long long target = (gs.epoch + 1ull) * G;
-    long long spins = 0;
-    while (ld_acquire_u64(gs.counter) < target) {
-      if (++spins > SM_SPIN_LIMIT) {
-        atomicExch(gs.err, 1);
-        break;
+  for (int k = 0; k < NV; ++k) {
+    T w = v[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) w += __shfl_down_sync(0xffffffffu, w, o);
+    if (lane == 0) sh[k * 32 + wid] = w;
+  }
+  __syncthreads();
+  if (wid == 0) {
+    const unsigned G = gridDim.x;
+    T bsum[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      T t = lane < (int)(blockDim.x >> 5) ? sh[k * 32 + lane] : (T)0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+      bsum[k] = t;
+    }
+    int ok = 1;
+    if (lane == 0) {
+#pragma unroll
+      for (int k = 0; k < NV; ++k) gs.partials[(buf * 4 + k) * G + blockIdx.x] = (double)bsum[k];
+      red_release_add(gs.counter, 1ull);
+      const unsigned long long target = (gs.epoch + 1ull) * G;
+      long long spins = 0;
+      while (ld_acquire_u64(gs.counter) < target) {
+        if (++spins > SM_SPIN_LIMIT) {
+          atomicExch(gs.err, 1);
+          ok = 0;
+          break;
+        }
+      }
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    if (ok) {
+      // fence so that lanes 1..31 read the partials after lane 0's acquire
+      __syncwarp();
+#pragma unroll
+      for (int k = 0; k < NV; ++k) {
+        double pv[SM_MAXG / 32];
+#pragma unroll
+        for (int m = 0; m < SM_MAXG / 32; ++m) {
+          const unsigned j = lane + 32 * m;
+          pv[m] = j < G ? __ldcg(gs.partials + (buf * 4 + k) * G + j) : 0.0;
+        }
+        T acc = 0;
+#pragma unroll
+        for (int m = 0; m < SM_MAXG / 32; ++m) acc += (T)pv[m];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if (lane == 0) s_tot[buf * NV + k] = acc;
       }
     }
   }
   gs.epoch++;
   __syncthreads();
   if (*reinterpret_cast<volatile int *>(gs.err)) return false;
-  T *s_tot = sh + 33 * NV;
-  if (threadIdx.x < 32) {
-    const int lane = threadIdx.x;
-    double pv[NV][SM_MAXG / 32];
 #pragma unroll
-    for (int k = 0; k < NV; ++k)
-#pragma unroll
-      for (int m = 0; m < SM_MAXG / 32; ++m) {
-        const unsigned j = lane + 32 * m;
-        pv[k][m] = j < G ? __ldcg(gs.partials + (buf * 4 + k) * G + j) : 0.0;
-      }
-#pragma unroll
-    for (int k = 0; k < NV; ++k) {
-      T acc = 0;
-#pragma unroll
-      for (int m = 0; m < SM_MAXG / 32; ++m) acc += (T)pv[k][m];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-      if (lane == 0) s_tot[k] = acc;
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < NV; ++k) tot[k] = s_tot[k];
-  __syncthreads();
+  for (int k = 0; k < NV; ++k) tot[k] = s_tot[buf * NV + k];
   trace_mark(gs);
+  if (gs.trace && threadIdx.x == 0) gs.t_last = clock64();
   return true;
 }
 
@@ -211,12 +207,68 @@ __device__ __forceinline__ void face_map(int dir, int p, int &ring, int &lw) {
   }
 }
 
+// Face-wise ring fill: warp w handles faces f = w, w+32, ... of the block's
+// tiles (f = tile * 6 + dir), each lane positions p = lane and lane + 32 of the
+// face, so the face's direction and neighbour kind are uniform in the warp.
+// In-block neighbours are copied box to box (the source cell sits at
+// ring + delta[dir] in the neighbour's box); another block's cell gets
+// remote(face index * 64 + p, global cell index, p); faces without a neighbour
+// tile keep their zeros.
+__constant__ int c_ring_base[6] = {0, 900, 0, 90, 0, 9};
+__constant__ int c_ring_a[6] = {10, 10, 100, 100, 100, 100};
+__constant__ int c_ring_b[6] = {1, 1, 1, 1, 10, 10};
+__constant__ int c_ring_delta[6] = {800, -800, 80, -80, 8, -8};
+
+template <typename Remote>
+__device__ __forceinline__ void ring_fill(float *s_zb, const int *s_nbr, int nt, int b0, int b1,
+                                          Remote remote) {
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int f = wid; f < nt * 6; f += SM_THREADS / 32) {
+    const int sl = s_nbr[f];
+    if (sl < 0) continue;
+    const int tl = f / 6, dir = f - tl * 6;
+    const int base = c_ring_base[dir], ca = c_ring_a[dir], cb = c_ring_b[dir];
+    float *dst = s_zb + tl * 1000;
+    if (sl >= b0 && sl < b1) {
+      const float *src = s_zb + (sl - b0) * 1000 + c_ring_delta[dir];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int p = lane + 32 * h;
+        const int ring = base + ((p >> 3) + 1) * ca + ((p & 7) + 1) * cb;
+        dst[ring] = src[ring];
+      }
+    } else {
+      float v[2];
+      int ring[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int p = lane + 32 * h, hi = p >> 3, lo = p & 7;
+        ring[h] = base + (hi + 1) * ca + (lo + 1) * cb;
+        int lw;
+        switch (dir) {
+          case 0: lw = 448 + p; break;
+          case 1: lw = p; break;
+          case 2: lw = hi * 64 + 56 + lo; break;
+          case 3: lw = hi * 64 + lo; break;
+          case 4: lw = hi * 64 + lo * 8 + 7; break;
+          default: lw = hi * 64 + lo * 8; break;
+        }
+        v[h] = remote(f * 64 + p, (int64_t)sl * 512 + lw);
+      }
+      dst[ring[0]] = v[0];
+      dst[ring[1]] = v[1];
+    }
+  }
+}
+
 template <bool REF>
 struct SmemCfg {
-  // per tile: x, r, d, s (2048 B each), padded z box (4000 B), code (1024 B),
-  // remote ring diagonals (384 B), x64 (4096 B, refined)
-  static constexpr size_t TILE_BYTES = 4 * 2048 + 4000 + 1024 + 384 + (REF ? 4096 : 0);
-  static constexpr int MAXT = REF ? 12 : 16;  // tiles per block (<= 227 KB with statics)
+  // per tile: x, r, d, s, w (2048 B each), padded z box (4000 B), code
+  // (1024 B), remote ring diagonals (384 B), x64 (4096 B, refined).  Shared
+  // memory holds all per-cell state so that no register array spills: with
+  // ~227 KB of the SM's on-chip memory in use, L1 is too small to absorb spills.
+  static constexpr size_t TILE_BYTES = 5 * 2048 + 4000 + 1024 + 384 + (REF ? 4096 : 0);
+  static constexpr int MAXT = REF ? 11 : 14;  // tiles per block (<= 227 KB with statics)
   static constexpr int MAXJ = (MAXT * 512 + SM_THREADS - 1) / SM_THREADS;
   static constexpr size_t BYTES = (size_t)MAXT * TILE_BYTES;
 };
@@ -299,8 +351,8 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   __shared__ int s_nbr[MAXT * 6];
   __shared__ uint8_t s_mask[MAXT];
   __shared__ int s_bounds[SM_MAXG + 1];
-  __shared__ Acc sh[33 * 4];
-  __shared__ double shd[33 * 4];
+  __shared__ Acc sh[36 * 4];
+  __shared__ double shd[36 * 4];
 
   PcgState *st = a.st;
   const int na = *a.n_active;
@@ -309,7 +361,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
     if (blockIdx.x == 0 && threadIdx.x == 0) st->fallback = 1;
     return;
   }
-  GridSync gs{a.partials, a.counter, &st->error, 0ull, a.trace, 0, a.trace_cap};
+  GridSync gs{a.partials, a.counter, &st->error, 0ull, a.trace, 0, a.trace_cap / 2, 0, clock64()};
   if (G > SM_MAXG) {
     if (threadIdx.x == 0) atomicExch(&st->error, 1);
     return;
@@ -321,7 +373,8 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   float *s_r = s_x + MAXT * 512;
   float *s_d = s_r + MAXT * 512;
   float *s_s = s_d + MAXT * 512;
-  float *s_zb = s_s + MAXT * 512;  // padded z boxes, 1000 per tile
+  float *s_w = s_s + MAXT * 512;
+  float *s_zb = s_w + MAXT * 512;  // padded z boxes, 1000 per tile
   uint16_t *s_code = reinterpret_cast<uint16_t *>(s_zb + MAXT * 1000);
   uint8_t *s_rdiag = reinterpret_cast<uint8_t *>(s_code + MAXT * 512);  // 384 per tile
 
@@ -394,20 +447,10 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   }
   __syncthreads();
   // ring fill of z0: remote z0 = M b (b is read-only input, no barrier needed)
-  for (int w = threadIdx.x; w < nt * 384; w += SM_THREADS) {
-    const int tl = w / 384, rem = w - tl * 384, dir = rem >> 6, p = rem & 63;
-    const int sl = s_nbr[tl * 6 + dir];
-    if (sl < 0) continue;
-    int ring, lw;
-    face_map(dir, p, ring, lw);
-    float v = 0.f;
-    if (sl >= b0 && sl < b1) {
-      v = s_zb[(sl - b0) * 1000 + pad_of(lw)];
-    } else if (s_rdiag[w]) {
-      v = (a.sign * a.bdiv[(int64_t)sl * 512 + lw]) / (float)s_rdiag[w];
-    }
-    s_zb[tl * 1000 + ring] = v;
-  }
+  ring_fill(s_zb, s_nbr, nt, b0, b1, [&](int ri, int64_t qn) -> float {
+    const uint8_t dg = s_rdiag[ri];
+    return dg ? (a.sign * a.bdiv[qn]) / (float)dg : 0.f;
+  });
   __syncthreads();
 
   // w = A z for own fluid cells (non-fluid box entries are exactly 0, so the
@@ -423,17 +466,15 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
     z = *zp;
     return (float)((dpack >> (3 * j)) & 7) * z - acc;
   };
-  float wr[MAXJ];
   Acc v3[3] = {0, 0, 0};
 #pragma unroll
   for (int j = 0; j < MAXJ; ++j) {
-    wr[j] = 0.f;
     if (!((fmask >> j) & 1)) continue;
     const int L = (tl0 + 2 * j) * 512 + l;
     float z;
     const float wn = stencil(j, z);
     const float r = s_r[L];
-    wr[j] = wn;
+    s_w[L] = wn;
     if ((hmask >> j) & 1) HW(0)[q0 + L] = wn;
     v3[0] += (Acc)(r * z);
     v3[1] += (Acc)(wn * z);
@@ -459,7 +500,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       const int tl = tl0 + 2 * j, L = tl * 512 + l;
       float *zp = s_zb + tl * 1000 + pc;
       const float dn = *zp + betaf * s_d[L];
-      const float sn = wr[j] + betaf * s_s[L];
+      const float sn = s_w[L] + betaf * s_s[L];
       s_d[L] = dn;
       s_s[L] = sn;
       s_x[L] = s_x[L] + alphaf * dn;
@@ -472,24 +513,18 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       }
     }
     __syncthreads();
+    trace_mark(gs);
     // ---- ring fill of the new z: another block's cell is rebuilt from its
     // published r_i, w_i, s_{i-1} with the owner's float32 operations
-    for (int w = threadIdx.x; w < nt * 384; w += SM_THREADS) {
-      const int tl = w / 384, rem = w - tl * 384, dir = rem >> 6, p = rem & 63;
-      const int sl = s_nbr[tl * 6 + dir];
-      if (sl < 0) continue;
-      int ring, lw;
-      face_map(dir, p, ring, lw);
-      if (sl >= b0 && sl < b1) {
-        s_zb[tl * 1000 + ring] = s_zb[(sl - b0) * 1000 + pad_of(lw)];
-      } else if (s_rdiag[w]) {
-        const int64_t qn = (int64_t)sl * 512 + lw;
-        const float sn = __ldcg(HW(par) + qn) + betaf * __ldcg(HS(par) + qn);
-        const float rn = __ldcg(HR(par) + qn) + nalpha * sn;
-        s_zb[tl * 1000 + ring] = rn / (float)s_rdiag[w];
-      }
-    }
+    ring_fill(s_zb, s_nbr, nt, b0, b1, [&](int ri, int64_t qn) -> float {
+      const uint8_t dg = s_rdiag[ri];
+      if (!dg) return 0.f;
+      const float sn = __ldcg(HW(par) + qn) + betaf * __ldcg(HS(par) + qn);
+      const float rn = __ldcg(HR(par) + qn) + nalpha * sn;
+      return rn / (float)dg;
+    });
     __syncthreads();
+    trace_mark(gs);
     // ---- w = A z and the three dot products
     Acc vv[3] = {0, 0, 0};
 #pragma unroll
@@ -499,7 +534,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       float z;
       const float wn = stencil(j, z);
       const float r = s_r[L];
-      wr[j] = wn;
+      s_w[L] = wn;
       if ((hmask >> j) & 1) HW(npar)[q0 + L] = wn;
       vv[0] += (Acc)(r * z);
       vv[1] += (Acc)(wn * z);
@@ -563,17 +598,10 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       if (!grid_allreduce<double, 1>(gs, vr, tr, shd)) return;
       r_true2 = tr[0];
       // ring fill of z = M r from the replaced residuals, then w = A z
-      for (int w = threadIdx.x; w < nt * 384; w += SM_THREADS) {
-        const int tl = w / 384, rem = w - tl * 384, dir = rem >> 6, p = rem & 63;
-        const int sl = s_nbr[tl * 6 + dir];
-        if (sl < 0) continue;
-        int ring, lw;
-        face_map(dir, p, ring, lw);
-        if (sl >= b0 && sl < b1)
-          s_zb[tl * 1000 + ring] = s_zb[(sl - b0) * 1000 + pad_of(lw)];
-        else if (s_rdiag[w])
-          s_zb[tl * 1000 + ring] = __ldcg(HR(npar) + (int64_t)sl * 512 + lw) / (float)s_rdiag[w];
-      }
+      ring_fill(s_zb, s_nbr, nt, b0, b1, [&](int ri, int64_t qn) -> float {
+        const uint8_t dg = s_rdiag[ri];
+        return dg ? __ldcg(HR(npar) + qn) / (float)dg : 0.f;
+      });
       __syncthreads();
       Acc vw[3] = {0, 0, 0};
 #pragma unroll
@@ -583,7 +611,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
         float z;
         const float wn = stencil(j, z);
         const float r = s_r[L];
-        wr[j] = wn;
+        s_w[L] = wn;
         if ((hmask >> j) & 1) HW(npar)[q0 + L] = wn;
         vw[0] += (Acc)(r * z);
         vw[1] += (Acc)(wn * z);
@@ -611,6 +639,10 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
     const int L = tl * 512 + l;
     a.xf[q0 + L] = s_x[L];
     if (REF) a.x64[q0 + L] = s_x64[L];
+  }
+  if (gs.trace && threadIdx.x == 0) {  // per-block busy cycles and tile counts
+    gs.trace[a.trace_cap / 2 + 2 * blockIdx.x] = gs.busy;
+    gs.trace[a.trace_cap / 2 + 2 * blockIdx.x + 1] = nt;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     st->trace_n = gs.trace_n;

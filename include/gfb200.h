@@ -158,8 +158,10 @@ typedef struct gf_pressure_info {
   int32_t kernel;       /* PCG kernel that ran: 1 shared-memory resident, 2 global-memory */
   int32_t pad;
 } gf_pressure_info;
-/* Copies up to cap timestamps (SM cycles) of the last traced PCG solve into host
- * memory and returns how many were recorded in *n; synchronises. */
+/* Copies the trace buffer of the last traced PCG solve (up to cap int64
+ * entries: block 0's SM-cycle stamps in the first half, *n of them, then per
+ * block a (busy cycles outside the all-reduce, tiles owned) pair) into host
+ * memory; synchronises. */
 int gf_pcg_trace(void *ctx, int64_t *host, int32_t cap, int32_t *n);
 /* Statistics of the last pressure solve; synchronises. */
 int gf_pressure_stats(void *ctx, gf_pressure_info *info);
