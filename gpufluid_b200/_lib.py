@@ -59,6 +59,7 @@ class StepParams(ctypes.Structure):
 
 GF_FLAG_GLOBAL_PCG = 1
 GF_FLAG_TRACE = 2
+GF_NOALLOC_MAX_CELLS = 2097152
 
 
 class PressureInfo(ctypes.Structure):
@@ -93,6 +94,8 @@ _SIGS = {
     "gf_vmax": ([_vp, _fp], ctypes.c_int),
     "gf_pressure_stats": ([_vp, ctypes.POINTER(PressureInfo)], ctypes.c_int),
     "gf_pcg_trace": ([_vp, _vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
+    "gf_jacobi_noalloc": ([ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _vp, _vp, _vp,
+                           ctypes.c_int32, _vp], ctypes.c_int),
 }
 
 _lib = None

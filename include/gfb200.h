@@ -172,6 +172,23 @@ int gf_active_tiles(void *ctx, int32_t *n_active, const int32_t **tiles);
  * synchronises. */
 int gf_vmax(void *ctx, float *vmax_out);
 
+/* ---- allocation-free variant ------------------------------------------- */
+/* No counterpart in the reference.  For callers that may not allocate device
+ * memory (a host that owns every device allocation through its own pool, or
+ * one recording into a CUDA graph): a Jacobi pressure solve with the
+ * arithmetic of gf_pressure(GF_JACOBI) on the dense grid -- label (uint8),
+ * div and p are (nx,ny,nz) device arrays owned by the caller; p receives the
+ * result of `iters` sweeps started from zero.  Its only scratch is a static
+ * device array of GF_NOALLOC_MAX_CELLS floats (8 MiB) that every GPU loading
+ * the library holds until exit; larger grids return GF_INVALID_ARG.  It calls
+ * no cudaMalloc/cudaFree.  Calls share that array: calls overlapping on the
+ * GPU race, calls in order on one stream are safe.  The first call on a
+ * device resolves the array's device address (cudaGetSymbolAddress) and
+ * should come before any stream capture.  Asynchronous on cuda_stream. */
+#define GF_NOALLOC_MAX_CELLS 2097152
+int gf_jacobi_noalloc(int32_t nx, int32_t ny, int32_t nz, const uint8_t *label,
+                      const float *div, float *p, int32_t iters, void *cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif
