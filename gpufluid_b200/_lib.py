@@ -94,6 +94,13 @@ _SIGS = {
     "gf_vmax": ([_vp, _fp], ctypes.c_int),
     "gf_pressure_stats": ([_vp, ctypes.POINTER(PressureInfo)], ctypes.c_int),
     "gf_pcg_trace": ([_vp, _vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
+    "gf_record_bytes": ([_vp, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
+    "gf_step_record": ([_vp, ctypes.POINTER(StepParams), _vp], ctypes.c_int),
+    "gf_step_adjoint": ([_vp, ctypes.POINTER(StepParams), _vp, _vp, _vp, _vp, _vp], ctypes.c_int),
+    "gf_density_splat": ([_vp, _vp, ctypes.c_int64, _vp], ctypes.c_int),
+    "gf_density_splat_adjoint": ([_vp, _vp, ctypes.c_int64, _vp, _vp], ctypes.c_int),
+    "gf_sample_cells": ([_vp, _vp, _vp, ctypes.c_int64, _vp], ctypes.c_int),
+    "gf_sample_cells_adjoint": ([_vp, _vp, ctypes.c_int64, _vp, _vp], ctypes.c_int),
     "gf_jacobi_noalloc": ([ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _vp, _vp, _vp,
                            ctypes.c_int32, _vp], ctypes.c_int),
 }

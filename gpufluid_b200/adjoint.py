@@ -1,0 +1,199 @@
+"""Differentiable rollouts: the adjoint substep behind ``torch.autograd``.
+
+The reference has no differentiation (it is only planned there).  This module
+chains the hand-written adjoint substep of libgfb200 (``gf_step_record`` /
+``gf_step_adjoint``: PIC transfer, cell labels held fixed within a substep)
+into gradients of a loss of the final particle state with respect to an
+initial control, with checkpoints every ``k`` substeps and recomputation in
+between.
+
+The drop-shaping problem (``DropShaping``):
+
+* fluid: a sphere seeded with the jittered lattice in every cell whose centre
+  lies inside it (8 per cell), PIC transfer (flip_blend 0), no reseeding;
+* control: a cell-centred 3-component velocity field U (3, nx, ny, nz); each
+  particle starts with the trilinearly sampled velocity v_p = sum_c N_pc U_c;
+* loss: L = sum_c (rho_c(x_T) - rho*_c)^2 with rho the cell-centred
+  trilinear unit-mass splat (``k_density_scatter``) after T substeps, and
+  rho* the splat of the same sphere translated by ``shift``, blurred by a
+  Gaussian of ``sigma`` cells.
+
+Particles are re-sorted by cell every substep, so storage order changes from
+substep to substep (``pid`` records each slot's particle).  Within a
+recomputed segment the records are mutually consistent; across segment
+boundaries the adjoint is carried by particle id, because float-atomic P2G
+sums make a recomputation differ from the first forward pass at the last bit.
+"""
+from __future__ import annotations
+
+import ctypes
+import time
+
+import numpy as np
+import torch
+
+from . import _lib
+from . import scene as _scene
+from .solver import FlipSolver3D
+
+
+def gaussian_blur(field: np.ndarray, sigma: float) -> np.ndarray:
+    """Separable Gaussian blur (truncated at 4 sigma, zero outside)."""
+    r = int(np.ceil(4.0 * sigma))
+    x = np.arange(-r, r + 1, dtype=np.float64)
+    k = np.exp(-0.5 * (x / sigma) ** 2)
+    k /= k.sum()
+    out = field.astype(np.float64)
+    for ax in range(3):
+        out = np.apply_along_axis(lambda m: np.convolve(m, k, mode="same"), ax, out)
+    return out
+
+
+class DropShaping:
+    """Loss of the final density against a translated, blurred target."""
+
+    def __init__(self, n=64, T=40, dt=1.0 / 240.0, k=10, center=(0.5, 0.35, 0.5), radius=0.15,
+                 shift=(0.15, 0.1, 0.0), sigma=1.5, ppc=8, device="cuda",
+                 pressure_solver="pcg_refined", tol=1e-9, max_iters=4000):
+        self.n, self.T, self.dt, self.k = n, T, dt, k
+        self.device = torch.device(device)
+        self.solver = FlipSolver3D(n, n, n, transfer_mode="pic", flip_blend=0.0,
+                                   pressure_tol=tol, device=device)
+        s = self.solver
+        x0 = _scene.seed_sphere_positions(n, n, n, s.dx, center, radius, ppc)
+        s._set_particles(pos=x0, vel=np.zeros_like(x0))
+        self.P = x0.shape[0]
+        self.x0 = s._pos.clone()
+        self.pressure_solver, self.max_iters = pressure_solver, max_iters
+        self.prm = s._params(dt, max_iters, pressure_solver)
+        shifted = torch.from_numpy(x0 + np.asarray(shift, np.float32)).to(self.device)
+        rho_t = self.splat(shifted).cpu().numpy()
+        self.target = torch.from_numpy(gaussian_blur(rho_t, sigma).astype(np.float32)).to(
+            self.device)
+        nb = ctypes.c_int64()
+        _lib.check(s._L.gf_record_bytes(s._ctx, ctypes.byref(nb)), s._ctx, "gf_record_bytes")
+        self.record_bytes = nb.value
+        self.records = [torch.empty(nb.value, dtype=torch.uint8, device=self.device)
+                        for _ in range(k)]
+        self.labels_log = None
+        self.last_timing = {}
+
+    # ---------------------------------------------------------- primitives
+    def _c(self, name, *args):
+        s = self.solver
+        s._set_stream()
+        _lib.check(getattr(s._L, name)(s._ctx, *args), s._ctx, name)
+
+    def splat(self, pos: torch.Tensor) -> torch.Tensor:
+        rho = torch.empty((self.n,) * 3, dtype=torch.float32, device=self.device)
+        self._c("gf_density_splat", pos.data_ptr(), pos.shape[0], rho.data_ptr())
+        return rho
+
+    def _sample(self, control: torch.Tensor, pos: torch.Tensor) -> torch.Tensor:
+        vel = torch.empty_like(pos)
+        self._c("gf_sample_cells", control.data_ptr(), pos.data_ptr(), pos.shape[0],
+                vel.data_ptr())
+        return vel
+
+    def _load(self, pos, vel, pid):
+        s = self.solver
+        s._pos.copy_(pos)
+        s._vel.copy_(vel)
+        s._pid.copy_(pid)
+
+    # ------------------------------------------------------------- forward
+    def forward(self, control: torch.Tensor, keep_labels: bool = False):
+        """Run T substeps from the control; returns (loss, checkpoints)."""
+        s = self.solver
+        control = control.detach().to(self.device, torch.float32).contiguous()
+        pid0 = torch.arange(self.P, dtype=torch.int32, device=self.device)
+        self._load(self.x0, self._sample(control, self.x0), pid0)
+        ckpts = []
+        labels = [] if keep_labels else None
+        for t in range(self.T):
+            if t % self.k == 0:
+                ckpts.append((s._pos.clone(), s._vel.clone(), s._pid.clone()))
+            self._c("gf_step", ctypes.byref(self.prm))
+            if keep_labels:
+                labels.append(s._label.clone())
+        rho = self.splat(s._pos)
+        loss = float(((rho.double() - self.target.double()) ** 2).sum().item())
+        self.labels_log = labels
+        return loss, ckpts
+
+    # ------------------------------------------------------------ backward
+    def backward(self, control: torch.Tensor, ckpts):
+        """Gradient of the loss with respect to the control (3, n, n, n)."""
+        s = self.solver
+        P, dev = self.P, self.device
+        control = control.detach().to(dev, torch.float32).contiguous()
+        xbar = torch.zeros((P, 3), dtype=torch.float32, device=dev)
+        vbar = torch.zeros_like(xbar)
+        xin = torch.empty_like(xbar)
+        vin = torch.empty_like(xbar)
+        carry_x = carry_v = None  # adjoint by particle id across segments
+        nseg = len(ckpts)
+        for seg in reversed(range(nseg)):
+            t0 = seg * self.k
+            steps = min(self.k, self.T - t0)
+            self._load(*ckpts[seg])
+            for i in range(steps):
+                self._c("gf_step_record", ctypes.byref(self.prm), self.records[i].data_ptr())
+            if seg == nseg - 1:
+                rho = self.splat(s._pos)
+                rho_bar = (2.0 * (rho - self.target)).contiguous()
+                self._c("gf_density_splat_adjoint", s._pos.data_ptr(), P, rho_bar.data_ptr(),
+                        xbar.data_ptr())
+                vbar.zero_()
+            else:  # bring the id-ordered adjoint into this recomputation's slot order
+                idx = s._pid.long()
+                xbar.copy_(carry_x[idx])
+                vbar.copy_(carry_v[idx])
+            for i in reversed(range(steps)):
+                self._c("gf_step_adjoint", ctypes.byref(self.prm), self.records[i].data_ptr(),
+                        xbar.data_ptr(), vbar.data_ptr(), xin.data_ptr(), vin.data_ptr())
+                xbar, xin = xin, xbar
+                vbar, vin = vin, vbar
+            # xbar, vbar are now in the storage order of checkpoint seg
+            idx = ckpts[seg][2].long()
+            carry_x = torch.empty_like(xbar)
+            carry_v = torch.empty_like(vbar)
+            carry_x[idx] = xbar
+            carry_v[idx] = vbar
+        # checkpoint 0 holds the particles in id order: carry is v(0)'s adjoint
+        grad = torch.empty((3,) + (self.n,) * 3, dtype=torch.float32, device=dev)
+        self._c("gf_sample_cells_adjoint", self.x0.data_ptr(), P, carry_v.data_ptr(),
+                grad.data_ptr())
+        return grad
+
+    def loss_and_grad(self, control: torch.Tensor):
+        torch.cuda.synchronize(self.device)
+        t0 = time.perf_counter()
+        loss, ckpts = self.forward(control)
+        torch.cuda.synchronize(self.device)
+        t1 = time.perf_counter()
+        grad = self.backward(control, ckpts)
+        torch.cuda.synchronize(self.device)
+        t2 = time.perf_counter()
+        self.last_timing = {"forward_s": t1 - t0, "backward_s": t2 - t1}
+        return loss, grad
+
+
+class RolloutLoss(torch.autograd.Function):
+    """``loss = RolloutLoss.apply(control, problem)``: the forward pass runs the
+    rollout keeping only the checkpoints; backward recomputes each segment and
+    runs the adjoint substeps."""
+
+    @staticmethod
+    def forward(ctx, control, problem):
+        loss, ckpts = problem.forward(control)
+        ctx.problem = problem
+        ctx.ckpts = ckpts
+        ctx.save_for_backward(control)
+        return torch.tensor(loss, dtype=torch.float64, device=control.device)
+
+    @staticmethod
+    def backward(ctx, gout):
+        (control,) = ctx.saved_tensors
+        grad = ctx.problem.backward(control, ctx.ckpts)
+        return (grad * gout.to(grad.dtype)).to(control.dtype), None

@@ -1,0 +1,575 @@
+// Adjoint of one PIC substep, with the cell labels held fixed.
+//
+// Forward map of a substep (particles in the sorted order of its binning):
+//   P2G      m_f = sum_p W_pf(x_p),  q_f = sum_p W_pf v_p,c(f)        (k3_p2g)
+//   normalize u_f = q_f / m_f  (m_f > 1e-8, else 0)                 (k3_normalize)
+//   forces   v faces += g dt; boundary faces <- 0                  (k3_add_gravity, bc)
+//   project  p = A^-1(-div(u)),  u3 = bc(u - k grad p)              (:846-871, PCG, :1364-1407)
+//   G2P      v'_p = sum_f S_pf(x_p) u3_f                           (k3_g2p_and_advect, blend 0)
+//   advect   x'_p = clamp(x_p + v'_p dt)
+// Adjoint (this file), given xbar', vbar' of the outputs:
+//   k_adj_g2p    vbar'' = vbar' + dt xbar' (unclamped axes), xbar = xbar' (unclamped);
+//                ubar3_f += S_pf vbar''  (scatter), xbar += dS/dx . u3 vbar''
+//   k_adj_grad   pbar_c = sum over c's faces of -/+ k ubar3_f   (pressure-gradient adjoint)
+//   (solve)      A lambda = pbar  -> divbar = -lambda  (same SPD operator, gf_pressure)
+//   k_adj_faces  ubar = bc ? 0 : ubar3 + s (divbar_left - divbar_right);
+//                qbar = ubar / m,  mbar = -ubar u / m
+//   k_adj_p2g    vbar_p += sum_f W_pf qbar_f (gather), xbar_p += dW/dx (v qbar + mbar)
+// Weight derivatives: W = wx wy wz, wx = 1 - sx or sx, sx = x/dx - offset - i0,
+// so dW/dx = (-1 or +1) / dx * wy wz (and likewise for y, z).
+#include "gf_internal.cuh"
+
+namespace gf {
+
+struct AdjArgs {
+  const float4 *rec0, *rec1;  // sorted inputs of the substep: (x,y,z,pid), (vx,vy,vz,-)
+  const int32_t *order;       // storage slot (input order) of each sorted position
+  const float *m[3];          // P2G weight sums per component
+  const float *un[3];         // normalised P2G velocities (pre-force)
+  const float *u3[3];         // final face velocities
+  const uint8_t *label;
+  float *ubar3[3], *qbar[3], *mbar[3];
+  float *div_io;              // pbar in, then -lambda read back as divbar
+  const float *lambda;        // adjoint pressure solution
+  const float *xbar_out, *vbar_out;  // (n,3), sorted order of this substep
+  float *xbar_acc;            // (n,3) scratch
+  float *xbar_in, *vbar_in;   // (n,3), input storage order
+  int64_t n;
+  float dx, dt, rho, dom0, dom1, dom2;
+  int nx, ny, nz;
+};
+
+__device__ __forceinline__ float clampf_(float x, float lo, float hi) {
+  return x < lo ? lo : (x > hi ? hi : x);
+}
+
+// sample3 weights of gridmath.py:29-63 for one component: corner indices,
+// weights and, per axis, d(weight)/dx scale (0 when the coordinate is clamped).
+struct Corners {
+  int64_t idx[8];
+  float w[8];
+  float dw[8][3];
+};
+
+__device__ __forceinline__ void sample_corners(float fx, float fy, float fz, int nxm, int nym,
+                                               int nzm, float inv_dx, Corners &c) {
+  const bool cx = fx < 0.0f || fx > (float)nxm, cy = fy < 0.0f || fy > (float)nym,
+             cz = fz < 0.0f || fz > (float)nzm;
+  fx = clampf_(fx, 0.0f, (float)nxm);
+  fy = clampf_(fy, 0.0f, (float)nym);
+  fz = clampf_(fz, 0.0f, (float)nzm);
+  int i0 = __float2int_rz(floorf(fx)), j0 = __float2int_rz(floorf(fy)),
+      k0 = __float2int_rz(floorf(fz));
+  if (i0 >= nxm) i0 = nxm - 1;
+  if (j0 >= nym) j0 = nym - 1;
+  if (k0 >= nzm) k0 = nzm - 1;
+  if (i0 < 0) i0 = 0;
+  if (j0 < 0) j0 = 0;
+  if (k0 < 0) k0 = 0;
+  int i1 = i0 + 1, j1 = j0 + 1, k1 = k0 + 1;
+  if (i1 >= nxm) i1 = nxm - 1;
+  if (j1 >= nym) j1 = nym - 1;
+  if (k1 >= nzm) k1 = nzm - 1;
+  const float rsx = fx - (float)i0, rsy = fy - (float)j0, rsz = fz - (float)k0;
+  const float sx = clampf_(rsx, 0.0f, 1.0f), sy = clampf_(rsy, 0.0f, 1.0f),
+              sz = clampf_(rsz, 0.0f, 1.0f);
+  const float gx = (cx || rsx < 0.0f || rsx > 1.0f) ? 0.0f : inv_dx;
+  const float gy = (cy || rsy < 0.0f || rsy > 1.0f) ? 0.0f : inv_dx;
+  const float gz = (cz || rsz < 0.0f || rsz > 1.0f) ? 0.0f : inv_dx;
+  const int ii[2] = {i0, i1}, jj[2] = {j0, j1}, kk[2] = {k0, k1};
+  const float wx[2] = {1.0f - sx, sx}, wy[2] = {1.0f - sy, sy}, wz[2] = {1.0f - sz, sz};
+  const float sgn[2] = {-1.0f, 1.0f};
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int q = (a * 2 + b) * 2 + e;
+        c.idx[q] = ((int64_t)ii[a] * nym + jj[b]) * nzm + kk[e];
+        c.w[q] = wx[a] * wy[b] * wz[e];
+        c.dw[q][0] = sgn[a] * gx * wy[b] * wz[e];
+        c.dw[q][1] = sgn[b] * gy * wx[a] * wz[e];
+        c.dw[q][2] = sgn[e] * gz * wx[a] * wy[b];
+      }
+}
+
+// scatter_face weights of gridmath.py:70-95 (P2G): corners dropped when out of
+// the component's grid; idx = -1 for a dropped corner.
+__device__ __forceinline__ void scatter_corners(float fx, float fy, float fz, int snx, int sny,
+                                                int snz, float inv_dx, Corners &c) {
+  const int i0 = __float2int_rz(floorf(fx)), j0 = __float2int_rz(floorf(fy)),
+            k0 = __float2int_rz(floorf(fz));
+  const float sx = fx - (float)i0, sy = fy - (float)j0, sz = fz - (float)k0;
+  const float wx[2] = {1.0f - sx, sx}, wy[2] = {1.0f - sy, sy}, wz[2] = {1.0f - sz, sz};
+  const float sgn[2] = {-1.0f, 1.0f};
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int q = (a * 2 + b) * 2 + e;
+        const int ii = i0 + a, jj = j0 + b, kk = k0 + e;
+        const bool in = ii >= 0 && ii < snx && jj >= 0 && jj < sny && kk >= 0 && kk < snz;
+        c.idx[q] = in ? ((int64_t)ii * sny + jj) * snz + kk : -1;
+        c.w[q] = wx[a] * wy[b] * wz[e];
+        c.dw[q][0] = sgn[a] * inv_dx * wy[b] * wz[e];
+        c.dw[q][1] = sgn[b] * inv_dx * wx[a] * wz[e];
+        c.dw[q][2] = sgn[e] * inv_dx * wx[a] * wy[b];
+      }
+}
+
+__global__ void k_adj_g2p(AdjArgs a) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= a.n) return;
+  const float4 r0 = a.rec0[q];
+  const float p[3] = {r0.x, r0.y, r0.z};
+  const float inv_dx = 1.0f / a.dx;
+  const float g[3] = {__fdiv_rn(p[0], a.dx), __fdiv_rn(p[1], a.dx), __fdiv_rn(p[2], a.dx)};
+  const float h[3] = {g[0] - 0.5f, g[1] - 0.5f, g[2] - 0.5f};
+  const int sz[3][3] = {{a.nx + 1, a.ny, a.nz}, {a.nx, a.ny + 1, a.nz}, {a.nx, a.ny, a.nz + 1}};
+  const float dom[3] = {a.dom0, a.dom1, a.dom2};
+  const float eps = a.dx * 1.001f;
+  Corners cs[3];
+  float vnew[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    sample_corners(c == 0 ? g[0] : h[0], c == 1 ? g[1] : h[1], c == 2 ? g[2] : h[2], sz[c][0],
+                   sz[c][1], sz[c][2], inv_dx, cs[c]);
+    float acc = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) acc += cs[c].w[k] * a.u3[c][cs[c].idx[k]];
+    vnew[c] = acc;
+  }
+  float xb[3], vb[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const float xo = a.xbar_out[3 * q + d], vo = a.vbar_out[3 * q + d];
+    const float xn = p[d] + vnew[d] * a.dt;
+    const bool free = xn >= eps && xn <= dom[d] - eps;
+    xb[d] = free ? xo : 0.0f;
+    vb[d] = vo + (free ? a.dt * xo : 0.0f);
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const float uv = a.u3[c][cs[c].idx[k]];
+      atomicAdd(&a.ubar3[c][cs[c].idx[k]], cs[c].w[k] * vb[c]);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) xb[d] += cs[c].dw[k][d] * uv * vb[c];
+    }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) a.xbar_acc[3 * q + d] = xb[d];
+}
+
+// Gradient step adjoint, per cell: pbar_c = sum_f dU2_f/dp_c * ubar3_f over
+// the faces where k3_subtract_pressure_grad acts (both sides non-solid, one
+// fluid, interior face); p of a non-fluid cell is a constant 0.
+__global__ void k_adj_grad(AdjArgs a, float k) {
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const int64_t n = (int64_t)nx * ny * nz;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    if (a.label[c] != 1) {
+      a.div_io[c] = 0.0f;
+      continue;
+    }
+    const int kk = (int)(c % nz);
+    const int64_t rr = c / nz;
+    const int j = (int)(rr % ny), i = (int)(rr / ny);
+    const int64_t sx = (int64_t)ny * nz;
+    float pb = 0.0f;
+    // u faces i (c on its right: u -= k (p_c - p_left)) and i+1 (c on its left)
+    if (i >= 1) {
+      const int ml = a.label[c - sx];
+      if (ml != 2) pb -= k * a.ubar3[0][((int64_t)i * ny + j) * nz + kk];
+    }
+    if (i + 1 <= nx - 1) {
+      const int mr = a.label[c + sx];
+      if (mr != 2) pb += k * a.ubar3[0][((int64_t)(i + 1) * ny + j) * nz + kk];
+    }
+    if (j >= 1) {
+      const int mb = a.label[c - nz];
+      if (mb != 2) pb -= k * a.ubar3[1][((int64_t)i * (ny + 1) + j) * nz + kk];
+    }
+    if (j + 1 <= ny - 1) {
+      const int mt = a.label[c + nz];
+      if (mt != 2) pb += k * a.ubar3[1][((int64_t)i * (ny + 1) + j + 1) * nz + kk];
+    }
+    if (kk >= 1) {
+      const int mba = a.label[c - 1];
+      if (mba != 2) pb -= k * a.ubar3[2][((int64_t)i * ny + j) * (nz + 1) + kk];
+    }
+    if (kk + 1 <= nz - 1) {
+      const int mfr = a.label[c + 1];
+      if (mfr != 2) pb += k * a.ubar3[2][((int64_t)i * ny + j) * (nz + 1) + kk + 1];
+    }
+    a.div_io[c] = pb;
+  }
+}
+
+// Divergence + boundary + normalisation adjoint, per face.
+__global__ void k_adj_faces(AdjArgs a, float s) {
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const int64_t nf = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nf;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int k = (int)(t % (nz + 1));
+    const int64_t rr = t / (nz + 1);
+    const int j = (int)(rr % (ny + 1)), i = (int)(rr / (ny + 1));
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp) {
+      const int ex = comp == 0, ey = comp == 1, ez = comp == 2;
+      if (i > nx - 1 + ex || j > ny - 1 + ey || k > nz - 1 + ez) continue;
+      const int sny = ny + ey, snz = nz + ez;
+      const int64_t g = ((int64_t)i * sny + j) * snz + k;
+      // cells on the low (L) and high (R) side of the face along comp's axis
+      const int li = i - ex, lj = j - ey, lk = k - ez;
+      const bool hasL = li >= 0 && lj >= 0 && lk >= 0;
+      const bool hasR = i < nx && j < ny && k < nz;
+      const int64_t cL = hasL ? ((int64_t)li * ny + lj) * nz + lk : 0;
+      const int64_t cR = hasR ? ((int64_t)i * ny + j) * nz + k : 0;
+      const int mL = hasL ? a.label[cL] : 2, mR = hasR ? a.label[cR] : 2;
+      const bool bc = !hasL || !hasR || mL == 2 || mR == 2;  // k3_enforce_solid_bc faces
+      float ub = 0.0f;
+      if (!bc) {
+        ub = a.ubar3[comp][g];
+        // div_c = s (sum out - in): this face is L's "out" face, R's "in" face;
+        // divbar = -lambda
+        if (mL == 1) ub += s * (-a.lambda[cL]);
+        if (mR == 1) ub -= s * (-a.lambda[cR]);
+      }
+      const float m = a.m[comp][g];
+      const bool ok = m > 1.0e-8f;
+      a.qbar[comp][g] = ok ? ub / m : 0.0f;
+      a.mbar[comp][g] = ok ? -ub * a.un[comp][g] / m : 0.0f;
+    }
+  }
+}
+
+__global__ void k_adj_p2g(AdjArgs a) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= a.n) return;
+  const float4 r0 = a.rec0[q], r1 = a.rec1[q];
+  const float vel[3] = {r1.x, r1.y, r1.z};
+  const float inv_dx = 1.0f / a.dx;
+  const float g[3] = {__fdiv_rn(r0.x, a.dx), __fdiv_rn(r0.y, a.dx), __fdiv_rn(r0.z, a.dx)};
+  const float h[3] = {g[0] - 0.5f, g[1] - 0.5f, g[2] - 0.5f};
+  const int sz[3][3] = {{a.nx + 1, a.ny, a.nz}, {a.nx, a.ny + 1, a.nz}, {a.nx, a.ny, a.nz + 1}};
+  float xb[3] = {a.xbar_acc[3 * q], a.xbar_acc[3 * q + 1], a.xbar_acc[3 * q + 2]};
+  float vb[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    Corners cs;
+    scatter_corners(c == 0 ? g[0] : h[0], c == 1 ? g[1] : h[1], c == 2 ? g[2] : h[2], sz[c][0],
+                    sz[c][1], sz[c][2], inv_dx, cs);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      if (cs.idx[k] < 0) continue;
+      const float qb = a.qbar[c][cs.idx[k]], mb = a.mbar[c][cs.idx[k]];
+      vb[c] += cs.w[k] * qb;
+      const float coef = vel[c] * qb + mb;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) xb[d] += cs.dw[k][d] * coef;
+    }
+  }
+  const int64_t s = a.order[q];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    a.xbar_in[3 * s + d] = xb[d];
+    a.vbar_in[3 * s + d] = vb[d];
+  }
+}
+
+// ---- density splat (meshing/surface.py:14-43) and control sampling -------
+__global__ void k_splat(const float *__restrict__ pos, int64_t n, float dx, int nx, int ny,
+                        int nz, float *rho) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  Corners cs;
+  scatter_corners(__fdiv_rn(pos[3 * q], dx) - 0.5f, __fdiv_rn(pos[3 * q + 1], dx) - 0.5f,
+                  __fdiv_rn(pos[3 * q + 2], dx) - 0.5f, nx, ny, nz, 1.0f / dx, cs);
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    if (cs.idx[k] >= 0) atomicAdd(&rho[cs.idx[k]], cs.w[k]);
+}
+
+__global__ void k_splat_adj(const float *__restrict__ pos, int64_t n, float dx, int nx, int ny,
+                            int nz, const float *__restrict__ rho_bar, float *pos_bar) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  Corners cs;
+  scatter_corners(__fdiv_rn(pos[3 * q], dx) - 0.5f, __fdiv_rn(pos[3 * q + 1], dx) - 0.5f,
+                  __fdiv_rn(pos[3 * q + 2], dx) - 0.5f, nx, ny, nz, 1.0f / dx, cs);
+  float xb[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    if (cs.idx[k] < 0) continue;
+    const float rb = rho_bar[cs.idx[k]];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) xb[d] += cs.dw[k][d] * rb;
+  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) pos_bar[3 * q + d] = xb[d];
+}
+
+// v_p = sum_c N_pc U_c of a cell-centred 3-component field (3, nx, ny, nz).
+__global__ void k_sample_cells(const float *__restrict__ grid3, const float *__restrict__ pos,
+                               int64_t n, float dx, int nx, int ny, int nz, float *vel) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  Corners cs;
+  scatter_corners(__fdiv_rn(pos[3 * q], dx) - 0.5f, __fdiv_rn(pos[3 * q + 1], dx) - 0.5f,
+                  __fdiv_rn(pos[3 * q + 2], dx) - 0.5f, nx, ny, nz, 1.0f / dx, cs);
+  const int64_t ncell = (int64_t)nx * ny * nz;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    float acc = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if (cs.idx[k] >= 0) acc += cs.w[k] * grid3[d * ncell + cs.idx[k]];
+    vel[3 * q + d] = acc;
+  }
+}
+
+__global__ void k_sample_cells_adj(const float *__restrict__ pos, int64_t n, float dx, int nx,
+                                   int ny, int nz, const float *__restrict__ vel_bar,
+                                   float *grid3_bar) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  Corners cs;
+  scatter_corners(__fdiv_rn(pos[3 * q], dx) - 0.5f, __fdiv_rn(pos[3 * q + 1], dx) - 0.5f,
+                  __fdiv_rn(pos[3 * q + 2], dx) - 0.5f, nx, ny, nz, 1.0f / dx, cs);
+  const int64_t ncell = (int64_t)nx * ny * nz;
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if (cs.idx[k] >= 0) atomicAdd(&grid3_bar[d * ncell + cs.idx[k]], cs.w[k] * vel_bar[3 * q + d]);
+}
+
+// ---- record layout -------------------------------------------------------
+struct RecordLayout {
+  size_t rec0, rec1, order, m[3], un[3], u3[3], label, bytes;
+};
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static RecordLayout layout(const Ctx *c) {
+  RecordLayout L{};
+  const int64_t n = c->p.n;
+  const int64_t fsz[3] = {(int64_t)(c->nx + 1) * c->ny * c->nz, (int64_t)c->nx * (c->ny + 1) * c->nz,
+                          (int64_t)c->nx * c->ny * (c->nz + 1)};
+  size_t o = 0;
+  L.rec0 = o; o = align256(o + n * 16);
+  L.rec1 = o; o = align256(o + n * 16);
+  L.order = o; o = align256(o + n * 4);
+  for (int q = 0; q < 3; ++q) { L.m[q] = o; o = align256(o + fsz[q] * 4); }
+  for (int q = 0; q < 3; ++q) { L.un[q] = o; o = align256(o + fsz[q] * 4); }
+  for (int q = 0; q < 3; ++q) { L.u3[q] = o; o = align256(o + fsz[q] * 4); }
+  L.label = o; o = align256(o + c->ncell);
+  L.bytes = o;
+  return L;
+}
+
+static int adj_reserve(Ctx *c) {
+  const int64_t nf = (int64_t)(c->nx + 1) * (c->ny + 1) * (c->nz + 1);  // >= each component
+  const int64_t need_f = 9 * nf, need_p = 3 * (c->p.n > 0 ? c->p.n : 1);
+  if (c->adj_faces && c->adj_faces_n >= need_f && c->adj_part_n >= need_p) return GF_OK;
+  if (c->adj_faces) cudaFree(c->adj_faces);
+  if (c->adj_part) cudaFree(c->adj_part);
+  c->adj_faces = nullptr;
+  c->adj_part = nullptr;
+  int e = check_cuda(c, cudaMalloc(&c->adj_faces, need_f * 4), "alloc adjoint faces");
+  if (e) return e;
+  if ((e = check_cuda(c, cudaMalloc(&c->adj_part, need_p * 4), "alloc adjoint particles")))
+    return e;
+  c->adj_faces_n = need_f;
+  c->adj_part_n = need_p;
+  return GF_OK;
+}
+
+static bool pic_only(const gf_step_params *prm) {
+  return prm->transfer != GF_APIC && prm->flip_blend == 0.0f;
+}
+
+}  // namespace gf
+
+using gf::Ctx;
+
+extern "C" {
+
+int gf_record_bytes(void *ctx, int64_t *bytes) {
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);
+  if (!c || !bytes) return GF_INVALID_ARG;
+  if (!c->bound) return gf::fail(c, GF_INVALID_ARG, "gf_record_bytes: buffers not bound");
+  *bytes = (int64_t)gf::layout(c).bytes;
+  return GF_OK;
+}
+
+int gf_step_record(void *ctx, const gf_step_params *prm, void *record) {
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);
+  if (!c || !prm || !record) return GF_INVALID_ARG;
+  if (!gf::pic_only(prm))
+    return gf::fail(c, GF_INVALID_ARG, "the adjoint substep supports PIC (flip_blend 0) only");
+  int e = gf_step(ctx, prm);
+  if (e) return e;
+  const gf::RecordLayout L = gf::layout(c);
+  char *r = static_cast<char *>(record);
+  cudaStream_t st = c->stream;
+  const int64_t n = c->p.n;
+  const int64_t fsz[3] = {(int64_t)(c->nx + 1) * c->ny * c->nz,
+                          (int64_t)c->nx * (c->ny + 1) * c->nz,
+                          (int64_t)c->nx * c->ny * (c->nz + 1)};
+  const float *mw[3] = {c->f.uw, c->f.vw, c->f.ww}, *us[3] = {c->f.us, c->f.vs, c->f.ws},
+              *u3[3] = {c->f.u, c->f.v, c->f.w};
+  // 4 particle/label copies + (m, un, u3) per component
+  constexpr int kCopies = 4 + 3 * 3;
+  struct { size_t off; const void *src; size_t bytes; } cp[kCopies] = {
+      {L.rec0, c->rec0, (size_t)n * 16}, {L.rec1, c->rec1, (size_t)n * 16},
+      {L.order, c->order, (size_t)n * 4}, {L.label, c->f.label, (size_t)c->ncell}};
+  int k = 4;
+  for (int q = 0; q < 3; ++q) {
+    cp[k++] = {L.m[q], mw[q], (size_t)fsz[q] * 4};
+    cp[k++] = {L.un[q], us[q], (size_t)fsz[q] * 4};
+    cp[k++] = {L.u3[q], u3[q], (size_t)fsz[q] * 4};
+  }
+  for (auto &x : cp)
+    if (x.bytes && (e = gf::check_cuda(c, cudaMemcpyAsync(r + x.off, x.src, x.bytes,
+                                                          cudaMemcpyDeviceToDevice, st),
+                                       "gf_step_record copy")))
+      return e;
+  return GF_OK;
+}
+
+int gf_step_adjoint(void *ctx, const gf_step_params *prm, const void *record,
+                    const float *xbar_out, const float *vbar_out, float *xbar_in, float *vbar_in) {
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);
+  if (!c || !prm || !record || !xbar_out || !vbar_out || !xbar_in || !vbar_in)
+    return GF_INVALID_ARG;
+  if (!c->bound) return gf::fail(c, GF_INVALID_ARG, "gf_step_adjoint: buffers not bound");
+  if (!gf::pic_only(prm))
+    return gf::fail(c, GF_INVALID_ARG, "the adjoint substep supports PIC (flip_blend 0) only");
+  int e = gf::adj_reserve(c);
+  if (e) return e;
+  const gf::RecordLayout L = gf::layout(c);
+  const char *r = static_cast<const char *>(record);
+  cudaStream_t st = c->stream;
+  const int64_t n = c->p.n;
+  const int64_t nfmax = (int64_t)(c->nx + 1) * (c->ny + 1) * (c->nz + 1);
+  gf::AdjArgs a{};
+  a.rec0 = reinterpret_cast<const float4 *>(r + L.rec0);
+  a.rec1 = reinterpret_cast<const float4 *>(r + L.rec1);
+  a.order = reinterpret_cast<const int32_t *>(r + L.order);
+  a.label = reinterpret_cast<const uint8_t *>(r + L.label);
+  for (int q = 0; q < 3; ++q) {
+    a.m[q] = reinterpret_cast<const float *>(r + L.m[q]);
+    a.un[q] = reinterpret_cast<const float *>(r + L.un[q]);
+    a.u3[q] = reinterpret_cast<const float *>(r + L.u3[q]);
+    a.ubar3[q] = c->adj_faces + q * nfmax;
+    a.qbar[q] = c->adj_faces + (3 + q) * nfmax;
+    a.mbar[q] = c->adj_faces + (6 + q) * nfmax;
+  }
+  a.div_io = c->f.div;
+  a.lambda = c->f.p;
+  a.xbar_out = xbar_out;
+  a.vbar_out = vbar_out;
+  a.xbar_acc = c->adj_part;
+  a.xbar_in = xbar_in;
+  a.vbar_in = vbar_in;
+  a.n = n;
+  a.dx = c->dx;
+  a.dt = prm->dt;
+  a.rho = prm->rho;
+  a.dom0 = c->dom[0];
+  a.dom1 = c->dom[1];
+  a.dom2 = c->dom[2];
+  a.nx = c->nx;
+  a.ny = c->ny;
+  a.nz = c->nz;
+  if ((e = gf::check_cuda(c, cudaMemsetAsync(c->adj_faces, 0, 3 * nfmax * 4, st), "zero ubar")))
+    return e;
+  const unsigned gp = (unsigned)((n + 255) / 256);
+  if (n > 0) {
+    gf::k_adj_g2p<<<gp, 256, 0, st>>>(a);
+    c->launches++;
+  }
+  // pressure-gradient adjoint -> rhs of the adjoint solve, on the recorded labels
+  if ((e = gf::check_cuda(c, cudaMemcpyAsync(c->f.label, a.label, c->ncell,
+                                             cudaMemcpyDeviceToDevice, st),
+                          "restore labels")))
+    return e;
+  float kk = prm->rho * c->dx;  // dt / (rho dx), as k3_subtract_pressure_grad
+  kk = prm->dt / kk;
+  const unsigned gc = (unsigned)((c->ncell + 255) / 256 < (int64_t)c->num_sms * 16
+                                     ? (c->ncell + 255) / 256
+                                     : (int64_t)c->num_sms * 16);
+  gf::k_adj_grad<<<gc, 256, 0, st>>>(a, kk);
+  c->launches++;
+  // A lambda = pbar with the same SPD operator (labels fixed)
+  gf_step_params sp = *prm;
+  sp.rhs_sign = 1;
+  if (sp.solver != GF_PCG && sp.solver != GF_PCG_REFINED) sp.solver = GF_PCG;
+  if ((e = gf::launch_pressure(c, &sp))) return e;
+  float s = prm->rho * c->dx;  // (rho dx) / dt, as k3_compute_divergence
+  s = s / prm->dt;
+  const unsigned gf_ = (unsigned)((nfmax + 255) / 256 < (int64_t)c->num_sms * 16
+                                      ? (nfmax + 255) / 256
+                                      : (int64_t)c->num_sms * 16);
+  gf::k_adj_faces<<<gf_, 256, 0, st>>>(a, s);
+  c->launches++;
+  if (n > 0) {
+    gf::k_adj_p2g<<<gp, 256, 0, st>>>(a);
+    c->launches++;
+  }
+  return gf::check_launch(c, "gf_step_adjoint");
+}
+
+int gf_density_splat(void *ctx, const float *pos, int64_t n, float *rho) {
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);
+  if (!c || (n > 0 && !pos) || !rho) return GF_INVALID_ARG;
+  int e = gf::check_cuda(c, cudaMemsetAsync(rho, 0, c->ncell * 4, c->stream), "zero rho");
+  if (e || n == 0) return e;
+  gf::k_splat<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(pos, n, c->dx, c->nx, c->ny,
+                                                                  c->nz, rho);
+  c->launches++;
+  return gf::check_launch(c, "gf_density_splat");
+}
+
+int gf_density_splat_adjoint(void *ctx, const float *pos, int64_t n, const float *rho_bar,
+                             float *pos_bar) {
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);
+  if (!c || (n > 0 && (!pos || !pos_bar)) || !rho_bar) return GF_INVALID_ARG;
+  if (n == 0) return GF_OK;
+  gf::k_splat_adj<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(pos, n, c->dx, c->nx, c->ny,
+                                                                      c->nz, rho_bar, pos_bar);
+  c->launches++;
+  return gf::check_launch(c, "gf_density_splat_adjoint");
+}
+
+int gf_sample_cells(void *ctx, const float *grid3, const float *pos, int64_t n, float *vel) {
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);
+  if (!c || !grid3 || (n > 0 && (!pos || !vel))) return GF_INVALID_ARG;
+  if (n == 0) return GF_OK;
+  gf::k_sample_cells<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(grid3, pos, n, c->dx,
+                                                                         c->nx, c->ny, c->nz, vel);
+  c->launches++;
+  return gf::check_launch(c, "gf_sample_cells");
+}
+
+int gf_sample_cells_adjoint(void *ctx, const float *pos, int64_t n, const float *vel_bar,
+                            float *grid3_bar) {
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);
+  if (!c || !grid3_bar || (n > 0 && (!pos || !vel_bar))) return GF_INVALID_ARG;
+  int e = gf::check_cuda(c, cudaMemsetAsync(grid3_bar, 0, 3 * c->ncell * 4, c->stream),
+                         "zero grid bar");
+  if (e || n == 0) return e;
+  gf::k_sample_cells_adj<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
+      pos, n, c->dx, c->nx, c->ny, c->nz, vel_bar, grid3_bar);
+  c->launches++;
+  return gf::check_launch(c, "gf_sample_cells_adjoint");
+}
+
+}  // extern "C"

@@ -47,7 +47,7 @@ static int alloc_particles(Ctx *c, int64_t n) {
 static void destroy(Ctx *c) {
   if (!c) return;
   free_particles(c);
-  void *ps[] = {c->count, c->start, c->scan_part, c->vmax_dev};
+  void *ps[] = {c->count, c->start, c->scan_part, c->vmax_dev, c->adj_faces, c->adj_part};
   for (void *p : ps)
     if (p) cudaFree(p);
   pressure_free(c);

@@ -120,6 +120,12 @@ struct Ctx {
   int last_solver = -1;  // gf_solver of the last gf_pressure
   int last_iters = 0;    // iteration count of the last Jacobi / GS-RB solve
 
+  // adjoint workspace (allocated on the first gf_step_adjoint)
+  float *adj_faces = nullptr;  // ubar3, qbar, mbar: 9 face arrays
+  int64_t adj_faces_n = 0;
+  float *adj_part = nullptr;   // per-particle position adjoint scratch
+  int64_t adj_part_n = 0;
+
   // diagnostics
   bool timing = false;
   cudaEvent_t ev[10] = {};  // 0..6 stage boundaries, 8..9 around the solver kernel

@@ -172,6 +172,37 @@ int gf_active_tiles(void *ctx, int32_t *n_active, const int32_t **tiles);
  * synchronises. */
 int gf_vmax(void *ctx, float *vmax_out);
 
+/* ---- adjoint (differentiation through substeps) ------------------------- */
+/* No counterpart in the reference (planned only there).  PIC transfer
+ * (flip_blend 0) with the cell labels held fixed within each substep.
+ * gf_step_record runs gf_step and copies into `record` (a caller-owned device
+ * buffer of gf_record_bytes bytes) what the adjoint needs: the substep's
+ * sorted inputs, their storage slots, the P2G weight sums and normalised
+ * velocities, the final face velocities and the labels.  The outputs of a
+ * recorded substep are in its sorted order; gf_step_adjoint maps the adjoint
+ * of those outputs (xbar_out, vbar_out, (n,3)) to the adjoint of its inputs
+ * in their storage order (xbar_in, vbar_in): G2P/advection adjoint (a scatter
+ * onto the faces), pressure-gradient adjoint, a second solve with the same
+ * SPD Laplacian (prm->solver, rhs sign +1), divergence/boundary/normalisation
+ * adjoint, P2G adjoint (a gather).  It overwrites the context's div, p and
+ * label buffers. */
+int gf_record_bytes(void *ctx, int64_t *bytes);
+int gf_step_record(void *ctx, const gf_step_params *prm, void *record);
+int gf_step_adjoint(void *ctx, const gf_step_params *prm, const void *record,
+                    const float *xbar_out, const float *vbar_out, float *xbar_in,
+                    float *vbar_in);
+/* Cell-centred trilinear density splat of unit-mass particles into rho
+ * (nx,ny,nz) (k_density_scatter, meshing/surface.py:14-43) and its adjoint
+ * with respect to the positions. */
+int gf_density_splat(void *ctx, const float *pos, int64_t n, float *rho);
+int gf_density_splat_adjoint(void *ctx, const float *pos, int64_t n, const float *rho_bar,
+                             float *pos_bar);
+/* Velocities sampled from a cell-centred 3-component field (3,nx,ny,nz) with
+ * the same weights, and the adjoint with respect to the field (a scatter). */
+int gf_sample_cells(void *ctx, const float *grid3, const float *pos, int64_t n, float *vel);
+int gf_sample_cells_adjoint(void *ctx, const float *pos, int64_t n, const float *vel_bar,
+                            float *grid3_bar);
+
 /* ---- allocation-free variant ------------------------------------------- */
 /* No counterpart in the reference.  For callers that may not allocate device
  * memory (a host that owns every device allocation through its own pool, or
