@@ -162,6 +162,57 @@ def true_relres(s) -> float:
     return float(np.linalg.norm(r) / bb) if bb > 0 else 0.0
 
 
+def pressure_error_fp64(torch, s, iters=6000) -> float:
+    """||p - p64|| / ||p64|| for the solver's current float32 p, where p64 solves
+    the same system (A p = -div on the fluid cells) in float64 by Jacobi-
+    preconditioned CG on the device to a relative residual of 1e-13.
+    Measurement only; the system is rebuilt from the labels with dense tensor
+    ops."""
+    dev = s._p.device
+    lab = s._label.to(torch.int32)
+    fl = lab == 1
+    b = torch.where(fl, -s.div.double(), torch.zeros((), dtype=torch.float64, device=dev))
+    pad_lab = torch.nn.functional.pad(lab, (1, 1, 1, 1, 1, 1), value=2)
+    nx, ny, nz = lab.shape
+    views = []
+    for ax in range(3):
+        for sh in (0, 2):
+            sl = [slice(1, 1 + nx), slice(1, 1 + ny), slice(1, 1 + nz)]
+            sl[ax] = slice(sh, sh + lab.shape[ax])
+            views.append(tuple(sl))
+    diag = sum((pad_lab[v] != 2).double() for v in views)
+    nbf = [(pad_lab[v] == 1) for v in views]
+    flf = fl.double()
+    inv_d = torch.where(fl, 1.0 / diag.clamp(min=1.0), torch.zeros_like(diag))
+
+    def A(x):
+        xp = torch.nn.functional.pad(x, (1, 1, 1, 1, 1, 1))
+        acc = sum(torch.where(m, xp[v], torch.zeros_like(x)) for m, v in zip(nbf, views))
+        return (diag * x - acc) * flf
+
+    x = torch.zeros_like(b)
+    r = b.clone()
+    z = r * inv_d
+    pdir = z.clone()
+    rz = float((r * z).sum())
+    bb = float(torch.linalg.vector_norm(b))
+    if bb == 0.0:
+        return 0.0
+    for it in range(iters):
+        q = A(pdir)
+        alpha = rz / float((pdir * q).sum())
+        x += alpha * pdir
+        r -= alpha * q
+        if it % 20 == 0 and float(torch.linalg.vector_norm(r)) < 1e-13 * bb:
+            break
+        z = r * inv_d
+        rz_new = float((r * z).sum())
+        pdir = z + (rz_new / rz) * pdir
+        rz = rz_new
+    p32 = torch.where(fl, s._p.double(), torch.zeros_like(x))
+    return float(torch.linalg.vector_norm(p32 - x) / torch.linalg.vector_norm(x))
+
+
 def pcg_bytes(st) -> float:
     """Algorithmic bytes of one PCG launch: per fluid cell 14 B of set-up,
     48 B per iteration (phase A: z, d_old, code in; d_new, Ad out; phase B:
@@ -191,6 +242,29 @@ def timed_steps(torch, s, steps, solver):
     e1.record(stream)
     torch.cuda.synchronize()
     return e0.elapsed_time(e1) / steps, s.launch_count() - l0
+
+
+def adjoint_leg(torch, device, reps=2):
+    """Forward and forward+adjoint of the drop-shaping rollout (64^3 PIC sphere,
+    40 substeps of 1/240 s, checkpoints every 10 substeps, refined PCG to 1e-9):
+    substeps/s of each and their cost ratio, timed with device synchronisation
+    around whole rollouts."""
+    from gpufluid_b200.adjoint import DropShaping
+    prob = DropShaping(n=64, T=40, k=10, device=device)
+    g = torch.Generator(device="cpu").manual_seed(7)
+    control = (0.3 * torch.randn((3, 64, 64, 64), generator=g)).to(device)
+    prob.loss_and_grad(control)  # warm-up
+    fwd, bwd = [], []
+    for _ in range(reps):
+        prob.loss_and_grad(control)
+        fwd.append(prob.last_timing["forward_s"])
+        bwd.append(prob.last_timing["backward_s"])
+    tf, tb = float(np.median(fwd)), float(np.median(bwd))
+    return {"workload": "drop shaping 64^3 PIC, 40 substeps, checkpoint every 10",
+            "particles": prob.P, "forward_substeps_per_s": round(prob.T / tf, 2),
+            "fwd_adj_substeps_per_s": round(prob.T / (tf + tb), 2),
+            "forward_ms": round(1e3 * tf, 2), "adjoint_ms": round(1e3 * tb, 2),
+            "fwd_adj_over_fwd": round((tf + tb) / tf, 3)}
 
 
 def run_ours(args):
@@ -236,6 +310,7 @@ def run_ours(args):
     ms_plain, _ = timed_steps(torch, s, args.steps, "pcg")
     plain_stats = s.pressure_stats()
     plain_true = true_relres(s)
+    plain_err = pressure_error_fp64(torch, s)
     restore(s, snap)
 
     # ---- refined (the value)
@@ -249,6 +324,7 @@ def run_ours(args):
     ms_ref_max = max_over_ranks(ms_ref)
     ref_stats = s.pressure_stats()
     ref_true = true_relres(s)
+    ref_err = pressure_error_fp64(torch, s)
 
     # ---- per-stage device times and the PCG kernel (live, same workload)
     restore(s, snap)
@@ -297,6 +373,8 @@ def run_ours(args):
     ms_e2e = max_over_ranks(e0.elapsed_time(e1) / args.steps)
     barrier()
 
+    fwd_adj = None if args.no_adjoint else adjoint_leg(torch, device)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(steps=1)
@@ -318,10 +396,12 @@ def run_ours(args):
             "plain_fp32": {"substeps_per_s": round(world * 1000.0 / max_over_ranks(ms_plain), 3),
                            "ms_per_step": round(ms_plain, 4), "iters_last": plain_stats["iters"],
                            "recursive_relres": plain_stats["relres"],
-                           "true_relres_fp64": plain_true},
+                           "true_relres_fp64": plain_true,
+                           "pressure_rel_error_vs_fp64": plain_err},
             "refined": {"ms_per_step": round(ms_ref, 4), "iters_last": ref_stats["iters"],
                         "replacements_last": ref_stats["replacements"],
                         "true_relres_fp64": ref_true,
+                        "pressure_rel_error_vs_fp64": ref_err,
                         "time_vs_plain": round(ms_ref / ms_plain, 3)},
             "e2e": {"value": round(world * 1000.0 / ms_e2e, 3), "unit": "substeps/s",
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(h2d)},
@@ -338,6 +418,7 @@ def run_ours(args):
             "stages_gbs": stage_gbs,
             "clocks": clk,
             "cpu_baseline": cpu,
+            "fwd_adj": fwd_adj,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -405,6 +486,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the forward+adjoint rollout timing")
     ap.add_argument("--grid", type=int, default=128,
                     help="grid side (smaller sides are for profiling captures only)")
     args = ap.parse_args()

@@ -31,6 +31,7 @@ from __future__ import annotations
 
 import logging
 import math
+from collections import OrderedDict
 from pathlib import Path
 from typing import Optional
 
@@ -164,11 +165,11 @@ class FlipSolver3D:
         self._enable_cuda_graphs = bool(enable_cuda_graphs)
         self._enable_sub_dense = bool(enable_sub_dense)
         self._prof = StepProfiler(enabled=enable_timing)
-        self._cuda_graph = None
-        self._cuda_graph_key = None
+        # captured substeps by (transfer, solver, particle count, dt, iters):
+        # a few configurations alternate without recapturing
+        self._cuda_graphs: "OrderedDict[tuple, tuple]" = OrderedDict()
         self._cuda_graph_hits = 0
         self._cuda_graph_misses = 0
-        self._graph_launches = 0
         self._captured_launches = 0
         self._replayed_launches = 0
         self.attr_color = None
@@ -354,9 +355,10 @@ class FlipSolver3D:
                                self.pcg_check_every, float(self.pressure_tol),
                                self.pcg_rhs_sign, 0)
 
+    _MAX_GRAPHS = 4
+
     def _cuda_graph_invalidate(self):
-        self._cuda_graph = None
-        self._cuda_graph_key = None
+        self._cuda_graphs.clear()
 
     def step(self, dt: float, pressure_iters: int = 80, pressure_solver: str = "jacobi",
              pressure_block_sparse: bool = False):
@@ -367,16 +369,18 @@ class FlipSolver3D:
         if self._enable_cuda_graphs and not self._prof.enabled:
             key = (self.transfer_mode, pressure_solver, self.n_particles, float(dt),
                    int(pressure_iters))
-            if self._cuda_graph is not None and self._cuda_graph_key == key:
-                self._cuda_graph.replay()
-                self._replayed_launches += self._graph_launches
+            hit = key in self._cuda_graphs
+            if hit:
+                self._cuda_graphs.move_to_end(key)
+            else:
+                self._capture(prm, key)
+            graph, launches, _ = self._cuda_graphs[key]
+            graph.replay()
+            self._replayed_launches += launches
+            if hit:
                 self._cuda_graph_hits += 1
-                self._pressure_stale = True
-                return
-            self._capture(prm, key)
-            self._cuda_graph.replay()
-            self._replayed_launches += self._graph_launches
-            self._cuda_graph_misses += 1
+            else:
+                self._cuda_graph_misses += 1
             self._pressure_stale = True
             return
         self._set_stream()
@@ -399,10 +403,11 @@ class FlipSolver3D:
             _lib.check(self._L.gf_step(self._ctx, _lib.ctypes.byref(prm)), self._ctx,
                        "gf_step (capture)")
         # capturing records launches without running them: count them per replay
-        self._graph_launches = int(self._L.gf_launch_count(self._ctx)) - before
-        self._captured_launches += self._graph_launches
-        self._cuda_graph, self._cuda_graph_key = g, key
-        self._graph_stream = s
+        launches = int(self._L.gf_launch_count(self._ctx)) - before
+        self._captured_launches += launches
+        self._cuda_graphs[key] = (g, launches, s)
+        while len(self._cuda_graphs) > self._MAX_GRAPHS:
+            self._cuda_graphs.popitem(last=False)
 
     @property
     def last_pressure_iters(self) -> int:
