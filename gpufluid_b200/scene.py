@@ -10,7 +10,9 @@ These run once per scene on the host, as they do in the reference:
   same stream as the reference's per-particle ``rng.random()`` calls.
 * ``seed_sphere_positions`` -- the same lattice restricted to cells whose
   centre lies inside a sphere (a seeder the reference does not have).
-* ``cell_centers``, ``sdf_sphere``, ``sdf_box`` -- primitives/sdf.py:31-56.
+* ``cell_centers``, ``sdf_sphere``, ``sdf_box``, ``sdf_cylinder_y``,
+  ``sdf_plane`` -- the analytic SDFs of primitives/sdf.py:31-80 (the obstacle
+  shapes of the scene TOML; a cell is solid where the SDF is <= 0).
 """
 from __future__ import annotations
 
@@ -37,6 +39,22 @@ def sdf_box(grid_xyz: np.ndarray, center, half_size) -> np.ndarray:
     outside = np.linalg.norm(np.maximum(d, 0.0), axis=-1)
     inside = np.minimum(np.max(d, axis=-1), 0.0)
     return outside + inside
+
+
+def sdf_cylinder_y(grid_xyz: np.ndarray, center, radius: float, half_height: float) -> np.ndarray:
+    """Capped cylinder with its axis along y."""
+    q = grid_xyz - np.asarray(center, dtype=np.float32)
+    d_rad = np.sqrt(q[..., 0] ** 2 + q[..., 2] ** 2) - float(radius)
+    d_ax = np.abs(q[..., 1]) - float(half_height)
+    return (np.sqrt(np.maximum(d_rad, 0.0) ** 2 + np.maximum(d_ax, 0.0) ** 2)
+            + np.minimum(np.maximum(d_rad, d_ax), 0.0))
+
+
+def sdf_plane(grid_xyz: np.ndarray, point, normal) -> np.ndarray:
+    """Half-space, negative on the -normal side of ``point``."""
+    nrm = np.asarray(normal, dtype=np.float32)
+    nrm = nrm / (np.linalg.norm(nrm) + 1e-12)
+    return ((grid_xyz - np.asarray(point, dtype=np.float32)) * nrm).sum(axis=-1)
 
 
 def _lattice(cells: np.ndarray, per_axis: int, dx: float) -> np.ndarray:
