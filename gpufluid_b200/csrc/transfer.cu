@@ -92,49 +92,17 @@ __device__ __forceinline__ void scatter_comp(float *s_val, float *s_wt, int comp
       }
 }
 
-template <bool APIC>
-__global__ void __launch_bounds__(256) k_p2g_tile(P2GArgs a) {
-  __shared__ float s_val[3][BOX];
-  __shared__ float s_wt[3][BOX];
-  const int t = blockIdx.x;
-  const int64_t b = a.start[(int64_t)t * TILE_CELLS], e = a.start[(int64_t)(t + 1) * TILE_CELLS];
-  if (b == e) return;
-  for (int q = threadIdx.x; q < 3 * BOX; q += blockDim.x) {
-    (&s_val[0][0])[q] = 0.f;
-    (&s_wt[0][0])[q] = 0.f;
-  }
-  __syncthreads();
-  const int ti = t / (a.nty * a.ntz), tj = (t / a.ntz) % a.nty, tk = t % a.ntz;
-  const int I0 = ti * TILE, J0 = tj * TILE, K0 = tk * TILE;
-  for (int64_t q = b + threadIdx.x; q < e; q += blockDim.x) {
-    float4 r0 = a.rec0[q], r1 = a.rec1[q];
-    float4 r2 = make_float4(0, 0, 0, 0), r3 = r2;
-    if (APIC) {
-      r2 = a.rec2[q];
-      r3 = a.rec3[q];
-    }
-    float gx = __fdiv_rn(r0.x, a.dx), gy = __fdiv_rn(r0.y, a.dx), gz = __fdiv_rn(r0.z, a.dx);
-    float hx = gx - 0.5f, hy = gy - 0.5f, hz = gz - 0.5f;
-    // C rows: (r1.w, r2.x, r2.y) (r2.z, r2.w, r3.x) (r3.y, r3.z, r3.w)
-    scatter_comp<APIC>(s_val[0], s_wt[0], 0, r1.x, r1.w, r2.x, r2.y, r0.x, r0.y, r0.z, gx, hy, hz,
-                       I0, J0, K0, a, a.u, a.uw);
-    scatter_comp<APIC>(s_val[1], s_wt[1], 1, r1.y, r2.z, r2.w, r3.x, r0.x, r0.y, r0.z, hx, gy, hz,
-                       I0, J0, K0, a, a.v, a.vw);
-    scatter_comp<APIC>(s_val[2], s_wt[2], 2, r1.z, r3.y, r3.z, r3.w, r0.x, r0.y, r0.z, hx, hy, gz,
-                       I0, J0, K0, a, a.w, a.ww);
-  }
-  __syncthreads();
-  // flush: faces that only this tile's particles reach are stored, the
-  // shared halo band is accumulated atomically; exact zeros are skipped
-  // (the destination was zeroed before the launch).
+// Flush a tile's shared box: faces that only this tile's particles reach are
+// stored, the shared halo band is accumulated atomically; exact zeros are
+// skipped (the destination was zeroed before the launch).
+__device__ __forceinline__ void p2g_flush_box(const P2GArgs &a, float (*s_val)[BOX],
+                                              float (*s_wt)[BOX], int I0, int J0, int K0) {
   for (int q = threadIdx.x; q < 3 * BOX; q += blockDim.x) {
     int comp = q / BOX, e2 = q - comp * BOX;
     float val = s_val[comp][e2], wt = s_wt[comp][e2];
     if (val == 0.f && wt == 0.f) continue;
-    int ex = comp == 0 ? BOX_N : BOX_T, ey = comp == 1 ? BOX_N : BOX_T,
-        ez = comp == 2 ? BOX_N : BOX_T;
+    int ey = comp == 1 ? BOX_N : BOX_T, ez = comp == 2 ? BOX_N : BOX_T;
     int bx = e2 / (ey * ez), by = (e2 / ez) % ey, bz = e2 % ez;
-    (void)ex;
     int ii = bx + (comp == 0 ? I0 : I0 - 1), jj = by + (comp == 1 ? J0 : J0 - 1),
         kk = bz + (comp == 2 ? K0 : K0 - 1);
     int snx = a.nx + (comp == 0), sny = a.ny + (comp == 1), snz = a.nz + (comp == 2);
@@ -154,6 +122,50 @@ __global__ void __launch_bounds__(256) k_p2g_tile(P2GArgs a) {
       atomicAdd(&gw[g], wt);
     }
   }
+}
+
+template <bool APIC>
+__global__ void __launch_bounds__(256) k_p2g_tile(P2GArgs a) {
+  __shared__ float s_val[3][BOX];
+  __shared__ float s_wt[3][BOX];
+  const int t = blockIdx.x;
+  const int64_t b = a.start[(int64_t)t * TILE_CELLS], e = a.start[(int64_t)(t + 1) * TILE_CELLS];
+  if (b == e) return;
+  for (int q = threadIdx.x; q < 3 * BOX; q += blockDim.x) {
+    (&s_val[0][0])[q] = 0.f;
+    (&s_wt[0][0])[q] = 0.f;
+  }
+  __syncthreads();
+  const int ti = t / (a.nty * a.ntz), tj = (t / a.ntz) % a.nty, tk = t % a.ntz;
+  const int I0 = ti * TILE, J0 = tj * TILE, K0 = tk * TILE;
+  // Lane l of every warp walks its own contiguous run [l*run, (l+1)*run) of
+  // the tile's cell-sorted particles, so the 32 lanes of one instruction sit
+  // about run/ppc cells apart and their shared atomics rarely share an
+  // address (consecutive lanes would hit the same cell's 8 corners).
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int64_t np_tile = e - b, run = (np_tile + 31) >> 5;
+  for (int64_t s = warp; s < run; s += nwarps) {
+    const int64_t off = (int64_t)lane * run + s;
+    if (off >= np_tile) continue;
+    const int64_t q = b + off;
+    float4 r0 = a.rec0[q], r1 = a.rec1[q];
+    float4 r2 = make_float4(0, 0, 0, 0), r3 = r2;
+    if (APIC) {
+      r2 = a.rec2[q];
+      r3 = a.rec3[q];
+    }
+    float gx = __fdiv_rn(r0.x, a.dx), gy = __fdiv_rn(r0.y, a.dx), gz = __fdiv_rn(r0.z, a.dx);
+    float hx = gx - 0.5f, hy = gy - 0.5f, hz = gz - 0.5f;
+    // C rows: (r1.w, r2.x, r2.y) (r2.z, r2.w, r3.x) (r3.y, r3.z, r3.w)
+    scatter_comp<APIC>(s_val[0], s_wt[0], 0, r1.x, r1.w, r2.x, r2.y, r0.x, r0.y, r0.z, gx, hy, hz,
+                       I0, J0, K0, a, a.u, a.uw);
+    scatter_comp<APIC>(s_val[1], s_wt[1], 1, r1.y, r2.z, r2.w, r3.x, r0.x, r0.y, r0.z, hx, gy, hz,
+                       I0, J0, K0, a, a.v, a.vw);
+    scatter_comp<APIC>(s_val[2], s_wt[2], 2, r1.z, r3.y, r3.z, r3.w, r0.x, r0.y, r0.z, hx, hy, gz,
+                       I0, J0, K0, a, a.w, a.ww);
+  }
+  __syncthreads();
+  p2g_flush_box(a, s_val, s_wt, I0, J0, K0);
 }
 
 // --------------------------------------------------------------- forces
