@@ -69,6 +69,21 @@ class PressureInfo(ctypes.Structure):
                 ("kernel", ctypes.c_int32), ("pad", ctypes.c_int32)]
 
 
+class SceneLayout(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in ("cell0", "fu0", "fv0", "fw0", "tile0", "ntiles",
+                                              "fslot0")]
+
+
+class BatchTotals(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in ("ncell", "nu", "nv", "nw", "ntiles", "nslot")]
+
+
+class TuneInfo(ctypes.Structure):
+    _fields_ = [("g2p_threads", ctypes.c_int32), ("grid_threads", ctypes.c_int32),
+                ("grid_blocks_per_sm", ctypes.c_int32), ("pcg_blocks_per_sm", ctypes.c_int32),
+                ("step_ms_before", ctypes.c_float), ("step_ms_after", ctypes.c_float)]
+
+
 _SIGS = {
     "gf_create": ([ctypes.POINTER(GridDesc), ctypes.c_int64, ctypes.POINTER(_vp)], ctypes.c_int),
     "gf_destroy": ([_vp], ctypes.c_int),
@@ -103,6 +118,18 @@ _SIGS = {
     "gf_sample_cells_adjoint": ([_vp, _vp, ctypes.c_int64, _vp, _vp], ctypes.c_int),
     "gf_jacobi_noalloc": ([ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _vp, _vp, _vp,
                            ctypes.c_int32, _vp], ctypes.c_int),
+    "gf_batch_plan": ([ctypes.POINTER(GridDesc), ctypes.c_int32, ctypes.POINTER(SceneLayout),
+                       ctypes.POINTER(BatchTotals)], ctypes.c_int),
+    "gf_batch_create": ([ctypes.POINTER(GridDesc), ctypes.c_int32, ctypes.c_int64,
+                         ctypes.POINTER(_vp)], ctypes.c_int),
+    "gf_batch_bind": ([_vp, ctypes.POINTER(Fields), ctypes.POINTER(Particles),
+                       ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
+    "gf_batch_pressure_stats": ([_vp, ctypes.POINTER(ctypes.c_int32),
+                                 ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32)],
+                                ctypes.c_int),
+    "gf_autotune": ([_vp, ctypes.POINTER(StepParams), ctypes.POINTER(TuneInfo)], ctypes.c_int),
+    "gf_get_tune": ([_vp, ctypes.POINTER(TuneInfo)], ctypes.c_int),
+    "gf_set_tune": ([_vp, ctypes.POINTER(TuneInfo)], ctypes.c_int),
 }
 
 _lib = None

@@ -404,6 +404,7 @@ extern "C" {
 int gf_record_bytes(void *ctx, int64_t *bytes) {
   Ctx *c = reinterpret_cast<Ctx *>(ctx);
   if (!c || !bytes) return GF_INVALID_ARG;
+  if (c->nseg) return gf::fail(c, GF_INVALID_ARG, "gf_record_bytes: single-scene contexts only");
   if (!c->bound) return gf::fail(c, GF_INVALID_ARG, "gf_record_bytes: buffers not bound");
   *bytes = (int64_t)gf::layout(c).bytes;
   return GF_OK;
@@ -412,6 +413,7 @@ int gf_record_bytes(void *ctx, int64_t *bytes) {
 int gf_step_record(void *ctx, const gf_step_params *prm, void *record) {
   Ctx *c = reinterpret_cast<Ctx *>(ctx);
   if (!c || !prm || !record) return GF_INVALID_ARG;
+  if (c->nseg) return gf::fail(c, GF_INVALID_ARG, "gf_step_record: single-scene contexts only");
   if (!gf::pic_only(prm))
     return gf::fail(c, GF_INVALID_ARG, "the adjoint substep supports PIC (flip_blend 0) only");
   int e = gf_step(ctx, prm);
@@ -449,6 +451,7 @@ int gf_step_adjoint(void *ctx, const gf_step_params *prm, const void *record,
   Ctx *c = reinterpret_cast<Ctx *>(ctx);
   if (!c || !prm || !record || !xbar_out || !vbar_out || !xbar_in || !vbar_in)
     return GF_INVALID_ARG;
+  if (c->nseg) return gf::fail(c, GF_INVALID_ARG, "gf_step_adjoint: single-scene contexts only");
   if (!c->bound) return gf::fail(c, GF_INVALID_ARG, "gf_step_adjoint: buffers not bound");
   if (!gf::pic_only(prm))
     return gf::fail(c, GF_INVALID_ARG, "the adjoint substep supports PIC (flip_blend 0) only");
@@ -530,6 +533,7 @@ int gf_step_adjoint(void *ctx, const gf_step_params *prm, const void *record,
 int gf_density_splat(void *ctx, const float *pos, int64_t n, float *rho) {
   Ctx *c = reinterpret_cast<Ctx *>(ctx);
   if (!c || (n > 0 && !pos) || !rho) return GF_INVALID_ARG;
+  if (c->nseg) return gf::fail(c, GF_INVALID_ARG, "single-scene contexts only");
   int e = gf::check_cuda(c, cudaMemsetAsync(rho, 0, c->ncell * 4, c->stream), "zero rho");
   if (e || n == 0) return e;
   gf::k_splat<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(pos, n, c->dx, c->nx, c->ny,
@@ -542,6 +546,7 @@ int gf_density_splat_adjoint(void *ctx, const float *pos, int64_t n, const float
                              float *pos_bar) {
   Ctx *c = reinterpret_cast<Ctx *>(ctx);
   if (!c || (n > 0 && (!pos || !pos_bar)) || !rho_bar) return GF_INVALID_ARG;
+  if (c->nseg) return gf::fail(c, GF_INVALID_ARG, "single-scene contexts only");
   if (n == 0) return GF_OK;
   gf::k_splat_adj<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(pos, n, c->dx, c->nx, c->ny,
                                                                       c->nz, rho_bar, pos_bar);
@@ -552,6 +557,7 @@ int gf_density_splat_adjoint(void *ctx, const float *pos, int64_t n, const float
 int gf_sample_cells(void *ctx, const float *grid3, const float *pos, int64_t n, float *vel) {
   Ctx *c = reinterpret_cast<Ctx *>(ctx);
   if (!c || !grid3 || (n > 0 && (!pos || !vel))) return GF_INVALID_ARG;
+  if (c->nseg) return gf::fail(c, GF_INVALID_ARG, "single-scene contexts only");
   if (n == 0) return GF_OK;
   gf::k_sample_cells<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(grid3, pos, n, c->dx,
                                                                          c->nx, c->ny, c->nz, vel);
@@ -563,6 +569,7 @@ int gf_sample_cells_adjoint(void *ctx, const float *pos, int64_t n, const float 
                             float *grid3_bar) {
   Ctx *c = reinterpret_cast<Ctx *>(ctx);
   if (!c || !grid3_bar || (n > 0 && (!pos || !vel_bar))) return GF_INVALID_ARG;
+  if (c->nseg) return gf::fail(c, GF_INVALID_ARG, "single-scene contexts only");
   int e = gf::check_cuda(c, cudaMemsetAsync(grid3_bar, 0, 3 * c->ncell * 4, c->stream),
                          "zero grid bar");
   if (e || n == 0) return e;

@@ -57,6 +57,34 @@ __global__ void k_bin_keys(const float *__restrict__ pos, int64_t n, float dx, i
   rank[i] = base + below;
 }
 
+// k_bin_keys over a batch: each particle finds its scene in the particle
+// prefix of the segment table and bins into that scene's cells and tiles.
+__global__ void kb_bin_keys(const float *__restrict__ pos, int64_t n, SegIndex sx,
+                            uint8_t *__restrict__ label, int32_t *__restrict__ key,
+                            int32_t *__restrict__ rank, int32_t *__restrict__ count) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  unsigned amask = __ballot_sync(0xffffffffu, i < n);
+  if (i >= n) return;
+  const SegRow r = sx.row[seg_find(sx.part0, sx.n, i)];
+  float px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
+  int ci = clampi(__float2int_rz(__fdiv_rn(px, r.dx)), 0, r.nx - 1);
+  int cj = clampi(__float2int_rz(__fdiv_rn(py, r.dx)), 0, r.ny - 1);
+  int ck = clampi(__float2int_rz(__fdiv_rn(pz, r.dx)), 0, r.nz - 1);
+  int64_t cell = r.cell0 + ((int64_t)ci * r.ny + cj) * r.nz + ck;
+  if (label[cell] != 2) label[cell] = 1;
+  int64_t t = r.tile0 + ((ci >> 3) * r.nty + (cj >> 3)) * r.ntz + (ck >> 3);
+  int kk = (int)(t * TILE_CELLS + (((ci & 7) * 8 + (cj & 7)) * 8 + (ck & 7)));
+  key[i] = kk;
+  unsigned lane = threadIdx.x & 31u;
+  unsigned peers = __match_any_sync(amask, kk);
+  int leader = __ffs(peers) - 1;
+  int below = __popc(peers & ((1u << lane) - 1u));
+  int base = 0;
+  if ((int)lane == leader) base = atomicAdd(&count[kk], __popc(peers));
+  base = __shfl_sync(amask, base, leader);
+  rank[i] = base + below;
+}
+
 // ---- exclusive scan of int32 counts (3 kernels, 4096 elements per block) ----
 constexpr int SCAN_THREADS = 1024;
 constexpr int SCAN_ITEMS = 4;
@@ -247,7 +275,11 @@ int launch_bin(Ctx *c, int transfer) {
   if ((e = check_cuda(c, cudaMemsetAsync(c->count, 0, c->nkeys * sizeof(int32_t), st),
                       "memset count")))
     return e;
-  if (n > 0) {
+  if (n > 0 && c->nseg > 0) {
+    kb_bin_keys<<<nblk(n, 256), 256, 0, st>>>(c->p.pos, n, seg_index(c), c->f.label, c->key,
+                                              c->rank, c->count);
+    c->launches++;
+  } else if (n > 0) {
     k_bin_keys<<<nblk(n, 256), 256, 0, st>>>(c->p.pos, n, c->dx, c->nx, c->ny, c->nz,
                                              c->nty, c->ntz, c->f.label, c->key, c->rank,
                                              c->count);

@@ -1,6 +1,8 @@
 // C ABI entry points of libgfb200: context lifecycle, binding, stage calls.
+#include <cmath>
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include "gf_internal.cuh"
 
@@ -44,31 +46,30 @@ static int alloc_particles(Ctx *c, int64_t n) {
   return GF_OK;
 }
 
+SegIndex seg_index(const Ctx *c) {
+  const int64_t m = c->nseg + 1;
+  return SegIndex{c->seg, c->seg_off, c->seg_off + m, c->seg_off + 2 * m, c->seg_off + 3 * m,
+                  c->nseg};
+}
+
 static void destroy(Ctx *c) {
   if (!c) return;
   free_particles(c);
-  void *ps[] = {c->count, c->start, c->scan_part, c->vmax_dev, c->adj_faces, c->adj_part};
+  void *ps[] = {c->count, c->start, c->scan_part, c->vmax_dev, c->adj_faces, c->adj_part,
+                c->seg, c->seg_off, c->seg_state, c->seg_slot0};
   for (void *p : ps)
     if (p) cudaFree(p);
+  if (c->seg_state_host) cudaFreeHost(c->seg_state_host);
   pressure_free(c);
   for (auto &e : c->ev)
     if (e) cudaEventDestroy(e);
   delete c;
 }
 
-}  // namespace gf
-
-using gf::Ctx;
-
-static Ctx *as_ctx(void *p) { return reinterpret_cast<Ctx *>(p); }
-
-extern "C" {
-
-int gf_create(const gf_grid_desc *g, int64_t max_particles, void **ctx_out) {
-  if (!g || !ctx_out) return GF_INVALID_ARG;
-  *ctx_out = nullptr;
-  if (g->nx < 1 || g->ny < 1 || g->nz < 1 || !(g->dx > 0.f) || max_particles < 0)
-    return GF_INVALID_ARG;
+// Device check and the allocations every context needs once its totals
+// (ntiles, ncell, nkeys) are set.
+static int new_ctx(Ctx **out) {
+  *out = nullptr;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
     cudaGetLastError();
@@ -83,23 +84,196 @@ int gf_create(const gf_grid_desc *g, int64_t max_particles, void **ctx_out) {
     return GF_NO_DEVICE;
   }
   c->num_sms = prop.multiProcessorCount;
+  *out = c;
+  return GF_OK;
+}
+
+// Layout of a batch: scenes concatenated in table order.
+static int plan_batch(const gf_grid_desc *scenes, int32_t n, gf_scene_layout *rows,
+                      gf_batch_totals *tot) {
+  if (!scenes || n < 1) return GF_INVALID_ARG;
+  int64_t cell = 0, fu = 0, fv = 0, fw = 0, tile = 0, fslot = 0;
+  for (int s = 0; s < n; ++s) {
+    const gf_grid_desc &g = scenes[s];
+    if (g.nx < 1 || g.ny < 1 || g.nz < 1 || !(g.dx > 0.f)) return GF_INVALID_ARG;
+    const int64_t nx = g.nx, ny = g.ny, nz = g.nz;
+    const int64_t nt = ((nx + 7) / 8) * ((ny + 7) / 8) * ((nz + 7) / 8);
+    if (rows) rows[s] = gf_scene_layout{cell, fu, fv, fw, tile, nt, fslot};
+    cell += nx * ny * nz;
+    fu += (nx + 1) * ny * nz;
+    fv += nx * (ny + 1) * nz;
+    fw += nx * ny * (nz + 1);
+    tile += nt;
+    fslot += (nx + 1) * (ny + 1) * (nz + 1);
+  }
+  if ((tile * 512) > INT32_MAX) return GF_INVALID_ARG;  // sort keys are int32
+  if (tot) *tot = gf_batch_totals{cell, fu, fv, fw, tile, fslot};
+  return GF_OK;
+}
+
+
+static int alloc_common(Ctx *c, int64_t max_particles) {
+  c->nkeys = (int64_t)c->ntiles * gf::TILE_CELLS;
+  c->n_scan_blocks = (c->nkeys + 4095) / 4096;
+  int e;
+  if ((e = check_cuda(c, cudaMalloc(&c->count, c->nkeys * 4), "alloc count")) ||
+      (e = check_cuda(c, cudaMalloc(&c->start, (c->nkeys + 1) * 4), "alloc start")) ||
+      (e = check_cuda(c, cudaMalloc(&c->scan_part, (c->n_scan_blocks + 1) * 4), "alloc scan")) ||
+      (e = check_cuda(c, cudaMalloc(&c->vmax_dev, 16), "alloc vmax")) ||
+      (e = pressure_alloc(c)) || (e = alloc_particles(c, max_particles)))
+    return e;
+  for (auto &ev : c->ev) cudaEventCreate(&ev);
+  return GF_OK;
+}
+
+}  // namespace gf
+
+using gf::Ctx;
+
+static Ctx *as_ctx(void *p) { return reinterpret_cast<Ctx *>(p); }
+
+extern "C" {
+
+int gf_batch_plan(const gf_grid_desc *scenes, int32_t n, gf_scene_layout *rows,
+                  gf_batch_totals *tot) {
+  return gf::plan_batch(scenes, n, rows, tot);
+}
+
+
+int gf_batch_create(const gf_grid_desc *scenes, int32_t n, int64_t max_particles,
+                    void **ctx_out) {
+  if (!scenes || !ctx_out || n < 1 || max_particles < 0) return GF_INVALID_ARG;
+  *ctx_out = nullptr;
+  gf_batch_totals tot;
+  std::vector<gf_scene_layout> lay(n);
+  int e = gf::plan_batch(scenes, n, lay.data(), &tot);
+  if (e) return e;
+  Ctx *c = nullptr;
+  if ((e = gf::new_ctx(&c))) return e;
+  c->nseg = n;
+  c->ntiles = (int)tot.ntiles;
+  c->ncell = tot.ncell;
+  c->nu = tot.nu; c->nv = tot.nv; c->nw = tot.nw;
+  c->nfslot = tot.nslot;
+  std::vector<gf::SegRow> rows(n);
+  std::vector<int64_t> off(4 * (n + 1), 0);
+  for (int s = 0; s < n; ++s) {
+    const gf_grid_desc &g = scenes[s];
+    gf::SegRow &r = rows[s];
+    r.nx = g.nx; r.ny = g.ny; r.nz = g.nz;
+    r.ntx = (g.nx + 7) / 8; r.nty = (g.ny + 7) / 8; r.ntz = (g.nz + 7) / 8;
+    r.dx = g.dx; r.dom0 = g.dom[0]; r.dom1 = g.dom[1]; r.dom2 = g.dom[2];
+    r.tile0 = lay[s].tile0; r.cell0 = lay[s].cell0;
+    r.fu0 = lay[s].fu0; r.fv0 = lay[s].fv0; r.fw0 = lay[s].fw0; r.fslot0 = lay[s].fslot0;
+    off[s] = lay[s].tile0;
+    off[(n + 1) + s] = lay[s].cell0;
+    off[2 * (n + 1) + s] = lay[s].fslot0;
+  }
+  off[n] = tot.ntiles;
+  off[(n + 1) + n] = tot.ncell;
+  off[2 * (n + 1) + n] = tot.nslot;
+  // particle prefix: zeros until gf_batch_bind
+  if ((e = gf::check_cuda(c, cudaMalloc(&c->seg, n * sizeof(gf::SegRow)), "alloc segments")) ||
+      (e = gf::check_cuda(c, cudaMalloc(&c->seg_off, off.size() * 8), "alloc segment prefix")) ||
+      (e = gf::check_cuda(c, cudaMalloc(&c->seg_state, n * sizeof(gf::PcgState)),
+                          "alloc scene states")) ||
+      (e = gf::check_cuda(c, cudaMalloc(&c->seg_slot0, (n + 1) * 4), "alloc scene slots")) ||
+      (e = gf::check_cuda(c, cudaMallocHost((void **)&c->seg_state_host,
+                                            n * sizeof(gf::PcgState)),
+                          "alloc pinned scene states")) ||
+      (e = gf::check_cuda(c, cudaMemcpy(c->seg, rows.data(), n * sizeof(gf::SegRow),
+                                        cudaMemcpyHostToDevice),
+                          "upload segments")) ||
+      (e = gf::check_cuda(c, cudaMemcpy(c->seg_off, off.data(), off.size() * 8,
+                                        cudaMemcpyHostToDevice),
+                          "upload segment prefix")) ||
+      (e = gf::check_cuda(c, cudaMemset(c->seg_state, 0, n * sizeof(gf::PcgState)),
+                          "zero scene states")) ||
+      (e = gf::alloc_common(c, max_particles))) {
+    gf::destroy(c);
+    return e;
+  }
+  *ctx_out = c;
+  return GF_OK;
+}
+
+int gf_batch_bind(void *ctx, const gf_fields *f, const gf_particles *p, const int64_t *counts) {
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);
+  if (!c || !f || !p || !counts) return GF_INVALID_ARG;
+  if (c->nseg < 1) return gf::fail(c, GF_INVALID_ARG, "gf_batch_bind: not a batch context");
+  std::vector<int64_t> part0(c->nseg + 1, 0);
+  for (int s = 0; s < c->nseg; ++s) {
+    if (counts[s] < 0) return gf::fail(c, GF_INVALID_ARG, "gf_batch_bind: negative count");
+    part0[s + 1] = part0[s] + counts[s];
+  }
+  if (part0[c->nseg] != p->n)
+    return gf::fail(c, GF_INVALID_ARG, "gf_batch_bind: scene counts do not sum to n");
+  int e = gf::check_cuda(c, cudaMemcpy(c->seg_off + 3 * (c->nseg + 1), part0.data(),
+                                       part0.size() * 8, cudaMemcpyHostToDevice),
+                         "upload particle prefix");
+  if (e) return e;
+  return gf_bind(ctx, f, p);
+}
+
+int gf_batch_pressure_stats(void *ctx, int32_t *iters, double *relres, int32_t *status) {
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);
+  if (!c) return GF_INVALID_ARG;
+  if (c->nseg < 1) return gf::fail(c, GF_INVALID_ARG, "not a batch context");
+  const bool pcg = c->last_solver == GF_PCG || c->last_solver == GF_PCG_REFINED;
+  if (!pcg) {
+    for (int s = 0; s < c->nseg; ++s) {
+      if (iters) iters[s] = c->last_iters;
+      if (relres) relres[s] = -1.0;
+      if (status) status[s] = GF_OK;
+    }
+    return GF_OK;
+  }
+  int e = gf::check_cuda(c, cudaMemcpyAsync(c->seg_state_host, c->seg_state,
+                                            c->nseg * sizeof(gf::PcgState),
+                                            cudaMemcpyDeviceToHost, c->stream),
+                         "read scene states");
+  if (!e) e = gf::check_cuda(c, cudaMemcpyAsync(c->state_host, c->state, sizeof(gf::PcgState),
+                                                cudaMemcpyDeviceToHost, c->stream),
+                             "read barrier state");
+  if (!e) e = gf::check_cuda(c, cudaStreamSynchronize(c->stream), "sync");
+  if (e) return e;
+  for (int s = 0; s < c->nseg; ++s) {
+    const gf::PcgState &S = c->seg_state_host[s];
+    if (iters) iters[s] = S.iters;
+    if (relres) {
+      if (c->last_solver == GF_PCG_REFINED)
+        relres[s] = S.b2 > 0 ? sqrt(S.r_true2 / S.b2) : 0.0;
+      else
+        relres[s] = S.r0 > 0 ? sqrt(S.rr / S.r0) : 0.0;
+    }
+    if (status) status[s] = c->state_host->error ? GF_TIMEOUT : S.status;
+  }
+  if (c->state_host->error) return gf::fail(c, GF_TIMEOUT, "PCG grid barrier timed out");
+  return GF_OK;
+}
+
+
+int gf_create(const gf_grid_desc *g, int64_t max_particles, void **ctx_out) {
+  if (!g || !ctx_out) return GF_INVALID_ARG;
+  *ctx_out = nullptr;
+  if (g->nx < 1 || g->ny < 1 || g->nz < 1 || !(g->dx > 0.f) || max_particles < 0)
+    return GF_INVALID_ARG;
+  Ctx *c = nullptr;
+  int e = gf::new_ctx(&c);
+  if (e) return e;
   c->nx = g->nx; c->ny = g->ny; c->nz = g->nz; c->dx = g->dx;
   for (int q = 0; q < 3; ++q) c->dom[q] = g->dom[q];
   c->ntx = (c->nx + 7) / 8; c->nty = (c->ny + 7) / 8; c->ntz = (c->nz + 7) / 8;
   c->ntiles = c->ntx * c->nty * c->ntz;
-  c->nkeys = (int64_t)c->ntiles * gf::TILE_CELLS;
   c->ncell = (int64_t)c->nx * c->ny * c->nz;
-  c->n_scan_blocks = (c->nkeys + 4095) / 4096;
-  int e;
-  if ((e = gf::check_cuda(c, cudaMalloc(&c->count, c->nkeys * 4), "alloc count")) ||
-      (e = gf::check_cuda(c, cudaMalloc(&c->start, (c->nkeys + 1) * 4), "alloc start")) ||
-      (e = gf::check_cuda(c, cudaMalloc(&c->scan_part, (c->n_scan_blocks + 1) * 4), "alloc scan")) ||
-      (e = gf::check_cuda(c, cudaMalloc(&c->vmax_dev, 16), "alloc vmax")) ||
-      (e = gf::pressure_alloc(c)) || (e = gf::alloc_particles(c, max_particles))) {
+  c->nu = (int64_t)(c->nx + 1) * c->ny * c->nz;
+  c->nv = (int64_t)c->nx * (c->ny + 1) * c->nz;
+  c->nw = (int64_t)c->nx * c->ny * (c->nz + 1);
+  c->nfslot = (int64_t)(c->nx + 1) * (c->ny + 1) * (c->nz + 1);
+  if ((e = gf::alloc_common(c, max_particles))) {
     gf::destroy(c);
     return e;
   }
-  for (auto &ev : c->ev) cudaEventCreate(&ev);
   *ctx_out = c;
   return GF_OK;
 }

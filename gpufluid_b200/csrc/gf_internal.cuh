@@ -78,6 +78,44 @@ struct PcgSmemArgs {
 };
 
 
+// One scene of a batch (a row of the segment table, device resident).  The
+// scenes' arrays are concatenated in table order: cells (labels, p, div),
+// u-, v- and w-shaped faces, 8x8x8 tiles and sort keys, particles.
+struct SegRow {
+  int nx, ny, nz, ntx, nty, ntz;
+  float dx, dom0, dom1, dom2;
+  int64_t tile0;             // first global tile (key = tile * 512 + local cell)
+  int64_t cell0;             // first cell
+  int64_t fu0, fv0, fw0;     // first u, v, w face
+  int64_t fslot0;            // first face slot ((nx+1)(ny+1)(nz+1) per scene)
+};
+
+// Prefix arrays of a batch for the scene lookup of a flat index (n+1 entries
+// each, device resident).
+struct SegIndex {
+  const SegRow *row;
+  const int64_t *tile0, *cell0, *fslot0, *part0;
+  int n;
+};
+
+// Largest s with off[s] <= x (off ascending, off[0] = 0, n scenes).
+__device__ __forceinline__ int seg_find(const int64_t *__restrict__ off, int n, int64_t x) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(off + mid) <= x) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Launch shapes chosen by gf_autotune (defaults until it runs).
+struct Tune {
+  int g2p_threads = 256;
+  int grid_threads = 256;        // forces / divergence / project / sweeps
+  int grid_blocks_per_sm = 16;   // cap of their grid-stride launches
+  int pcg_blocks_per_sm = 0;     // global-memory PCG: 0 = occupancy maximum
+};
+
 struct Ctx {
   // grid
   int nx = 0, ny = 0, nz = 0;
@@ -126,6 +164,17 @@ struct Ctx {
   float *adj_part = nullptr;   // per-particle position adjoint scratch
   int64_t adj_part_n = 0;
 
+  // batch of scenes (nseg > 0): segment table and per-scene solve state
+  int nseg = 0;
+  SegRow *seg = nullptr;                 // [nseg]
+  int64_t *seg_off = nullptr;            // 4 prefix arrays of nseg+1: tile0, cell0, fslot0, part0
+  PcgState *seg_state = nullptr;         // [nseg]
+  PcgState *seg_state_host = nullptr;    // pinned mirror
+  int32_t *seg_slot0 = nullptr;          // [nseg+1] first active slot of each scene
+  int64_t nfslot = 0;                    // face slots of all scenes
+  int64_t nu = 0, nv = 0, nw = 0;        // u, v, w faces of all scenes
+  Tune tune;
+
   // diagnostics
   bool timing = false;
   cudaEvent_t ev[10] = {};  // 0..6 stage boundaries, 8..9 around the solver kernel
@@ -154,6 +203,8 @@ int launch_vmax(Ctx *c);
 
 int launch_pcg_smem(Ctx *c, PcgSmemArgs &a, bool refined);
 bool pcg_smem_fits(Ctx *c, bool refined);
+
+SegIndex seg_index(const Ctx *c);
 
 int pressure_alloc(Ctx *c);
 void pressure_free(Ctx *c);

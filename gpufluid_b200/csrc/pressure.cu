@@ -155,6 +155,111 @@ __global__ void __launch_bounds__(512) k_tile_setup(SetupArgs a) {
   }
 }
 
+// ---- set-up over a batch: tiles are numbered scene after scene, so the
+// compaction keeps every scene's active tiles in one contiguous slot range.
+__global__ void kb_tile_flags(const uint8_t *__restrict__ label, SegIndex sx, int64_t ntiles,
+                              int32_t *__restrict__ flag) {
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= ntiles) return;
+  const SegRow r = sx.row[seg_find(sx.tile0, sx.n, warp)];
+  const int t = (int)(warp - r.tile0);
+  const int ti = t / (r.nty * r.ntz), tj = (t / r.ntz) % r.nty, tk = t % r.ntz;
+  const uint8_t *lab = label + r.cell0;
+  int any = 0;
+  for (int row = lane; row < 64; row += 32) {
+    int gi = ti * 8 + (row >> 3), gj = tj * 8 + (row & 7);
+    if (gi >= r.nx || gj >= r.ny) continue;
+    const uint8_t *base = lab + ((int64_t)gi * r.ny + gj) * r.nz;
+    for (int lk = 0; lk < 8; ++lk) {
+      int gk = tk * 8 + lk;
+      if (gk < r.nz && base[gk] == 1) any = 1;
+    }
+  }
+  any = __any_sync(0xffffffffu, any);
+  if (lane == 0) flag[warp] = any;
+}
+
+// First active slot of every scene (slot0[nseg] = number of active tiles).
+__global__ void kb_slot_ranges(const int32_t *__restrict__ tile_list,
+                               const int32_t *__restrict__ n_active, SegIndex sx,
+                               int32_t *__restrict__ slot0) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s > sx.n) return;
+  const int na = *n_active;
+  if (s == sx.n) {
+    slot0[s] = na;
+    return;
+  }
+  const int64_t t0 = sx.tile0[s];
+  int lo = 0, hi = na;  // first slot whose tile >= t0
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (tile_list[mid] < t0) lo = mid + 1; else hi = mid;
+  }
+  slot0[s] = lo;
+}
+
+struct BatchSetupArgs {
+  SetupArgs a;  // label/div are the concatenated arrays; grid fields unused
+  SegIndex sx;
+};
+
+__global__ void __launch_bounds__(512) kb_tile_setup(BatchSetupArgs ba) {
+  const SetupArgs &a = ba.a;
+  const int na = *a.n_active;
+  const int l = threadIdx.x, li = l >> 6, lj = (l >> 3) & 7, lk = l & 7;
+  for (int s = blockIdx.x; s < na; s += gridDim.x) {
+    const int tg = a.tile_list[s];
+    const SegRow r = ba.sx.row[seg_find(ba.sx.tile0, ba.sx.n, tg)];
+    const int t = (int)(tg - r.tile0);
+    const int ti = t / (r.nty * r.ntz), tj = (t / r.ntz) % r.nty, tk = t % r.ntz;
+    if (l < 6) {
+      int ni = ti + (l == 0 ? -1 : l == 1 ? 1 : 0), nj = tj + (l == 2 ? -1 : l == 3 ? 1 : 0),
+          nk = tk + (l == 4 ? -1 : l == 5 ? 1 : 0);
+      int ns = -1;
+      if (ni >= 0 && ni < r.ntx && nj >= 0 && nj < r.nty && nk >= 0 && nk < r.ntz)
+        ns = a.tile_slot[r.tile0 + (ni * r.nty + nj) * r.ntz + nk];
+      a.tile_nbr[s * 6 + l] = ns;
+    }
+    const int gi = ti * 8 + li, gj = tj * 8 + lj, gk = tk * 8 + lk;
+    const int64_t q = (int64_t)s * TILE_CELLS + l;
+    uint16_t code = 0;
+    float bd = 0.f;
+    if (gi < r.nx && gj < r.ny && gk < r.nz) {
+      const int nx = r.nx, ny = r.ny, nz = r.nz;
+      const uint8_t *lab = a.label + r.cell0;
+      const int64_t c = ((int64_t)gi * ny + gj) * nz + gk;
+      if (lab[c] == 1) {
+        int diag = 0, mask = 0, m;
+        if (gi > 0) { m = lab[c - (int64_t)ny * nz]; if (m != 2) { ++diag; if (m == 1) mask |= 1; } }
+        if (gi < nx - 1) { m = lab[c + (int64_t)ny * nz]; if (m != 2) { ++diag; if (m == 1) mask |= 2; } }
+        if (gj > 0) { m = lab[c - nz]; if (m != 2) { ++diag; if (m == 1) mask |= 4; } }
+        if (gj < ny - 1) { m = lab[c + nz]; if (m != 2) { ++diag; if (m == 1) mask |= 8; } }
+        if (gk > 0) { m = lab[c - 1]; if (m != 2) { ++diag; if (m == 1) mask |= 16; } }
+        if (gk < nz - 1) { m = lab[c + 1]; if (m != 2) { ++diag; if (m == 1) mask |= 32; } }
+        code = (uint16_t)(CODE_FLUID | (diag << CODE_DIAG_SHIFT) | mask);
+        bd = a.div[r.cell0 + c];
+      }
+    }
+    {
+      const int nf = __syncthreads_count(code != 0);
+      if (l == 0) a.tile_cost[s] = nf + 192;
+      if (l == 0 && nf) atomicAdd(reinterpret_cast<unsigned long long *>(a.n_fluid),
+                                 (unsigned long long)nf);
+    }
+    a.code[q] = code;
+    a.bdiv[q] = bd;
+    a.x[q] = 0.f;
+    a.r[q] = 0.f;
+    a.z[q] = 0.f;
+    a.d0[q] = 0.f;
+    a.d1[q] = 0.f;
+    a.Ad[q] = 0.f;
+    if (a.x64) a.x64[q] = 0.0;
+  }
+}
+
 // Compact index of neighbour `dir` (0 -x, 1 +x, 2 -y, 3 +y, 4 -z, 5 +z) of q.
 // Only called for fluid neighbours, whose tile is active by construction.
 __device__ __forceinline__ int64_t nb_index(int64_t q, int dir, const int32_t *__restrict__ nbr) {
@@ -481,6 +586,293 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
     st->status = GF_NOT_CONVERGED;
 }
 
+// ------------------------------------------------------- segmented PCG
+// The Jacobi-PCG of k_pcg for a batch of independent scenes in ONE persistent
+// cooperative kernel: every scene keeps its own scalars (alpha, beta, r.z,
+// residuals, convergence, iteration count) in its PcgState row.  A block
+// works on whole tiles (one thread per cell), so each tile's dot products
+// are block sums written to a per-slot partial; at every reduction point the
+// last block to arrive sums each scene's contiguous slot range in a fixed
+// order (one warp per scene) and updates that scene's scalars.  Tiles of a
+// converged scene are skipped; the solve ends when every scene is done.
+struct SegPcgArgs {
+  const int32_t *n_active, *nbr, *slot0;  // slot0[nseg+1]
+  int nseg;
+  const uint16_t *code;
+  const float *bdiv;
+  float *x, *r, *z, *d0, *d1, *Ad;
+  double *x64;
+  double *partials;  // [3][pstride]
+  int64_t pstride;
+  PcgState *st;      // [nseg]
+  PcgState *g;       // barrier counters; done = scenes finished, n_replace = pending
+  int max_iter, check_every;
+  double tol2, replace2;
+  float sign;
+};
+
+__device__ __forceinline__ int slot_scene(const int32_t *__restrict__ slot0, int n, int sl) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(slot0 + mid) <= sl) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Arrival barrier whose last block runs fin(scene, totals) for every scene
+// that want(scene) selects, on its slot-range sums of the NV partial rows.
+template <typename T, int NV, typename Want, typename Fin>
+__device__ bool seg_reduce(const SegPcgArgs &a, Want want, Fin fin) {
+  __shared__ int s_last, s_ok;
+  __syncthreads();
+  unsigned gen = 0;
+  if (threadIdx.x == 0) {
+    gen = ld_volatile(&a.g->bar_gen);
+    __threadfence();
+    const unsigned arrived = atomicAdd(&a.g->bar_count, 1u);
+    s_last = arrived == gridDim.x - 1;
+    s_ok = 1;
+  }
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int sc = wid; sc < a.nseg; sc += nw) {
+      if (!want(sc)) continue;  // warp-uniform
+      const int b = __ldcg(a.slot0 + sc), e = __ldcg(a.slot0 + sc + 1);
+      double tot[NV];
+#pragma unroll
+      for (int k = 0; k < NV; ++k) {
+        T acc = 0;
+        for (int j = b + lane; j < e; j += 32) acc += (T)__ldcg(a.partials + k * a.pstride + j);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        tot[k] = (double)acc;
+      }
+      if (lane == 0) fin(sc, tot);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicExch(&a.g->bar_count, 0u);
+      __threadfence();
+      atomicAdd(&a.g->bar_gen, 1u);
+    }
+  } else if (threadIdx.x == 0) {
+    long long spins = 0;
+    while (ld_volatile(&a.g->bar_gen) == gen) {
+      if (++spins > SPIN_LIMIT) {
+        atomicExch(&a.g->error, 1);
+        s_ok = 0;
+        break;
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  if (ld_volatile_i(&a.g->error)) return false;
+  return s_ok;
+}
+
+template <typename T, int NV>
+__device__ __forceinline__ void tile_partials(const SegPcgArgs &a, int sl, T (&v)[NV]) {
+  __shared__ T sh[32];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    const T t = block_sum<T>(v[k], sh);
+    if (threadIdx.x == 0) a.partials[k * a.pstride + sl] = (double)t;
+  }
+}
+
+template <typename Acc, bool REF>
+__global__ void __launch_bounds__(TILE_CELLS) k_pcg_seg(SegPcgArgs a) {
+  const int na = *a.n_active;
+  PcgState *st = a.st;
+  const int tid = threadIdx.x;
+  auto all = [](int) { return true; };
+  auto live = [&](int sc) { return !ld_volatile_i(&st[sc].done); };
+
+  // ---- init: r = b, z = M^-1 r; r.z and r.r per scene
+  for (int sl = blockIdx.x; sl < na; sl += gridDim.x) {
+    const int64_t q = (int64_t)sl * TILE_CELLS + tid;
+    const uint16_t code = a.code[q];
+    Acc v[2] = {0, 0};
+    if (code & CODE_FLUID) {
+      const float b = a.sign * a.bdiv[q];
+      const float diag = fmaxf((float)((code >> CODE_DIAG_SHIFT) & 7), 1.0f);
+      const float z = b / diag;
+      a.r[q] = b;
+      a.z[q] = z;
+      v[0] += (Acc)(b * z);
+      v[1] += (Acc)(b * b);
+    }
+    tile_partials<Acc, 2>(a, sl, v);
+  }
+  if (!seg_reduce<Acc, 2>(a, all, [&](int sc, double *t) {
+        PcgState &S = st[sc];
+        S.rz = t[0]; S.r0 = t[1]; S.rr = t[1]; S.b2 = t[1];
+        S.r_upd2 = t[1]; S.r_true2 = t[1];
+        S.beta = 0.0; S.alpha = 0.0; S.iters = 0; S.n_replace = 0; S.status = GF_OK;
+        S.done = t[1] < 1e-30 ? 1 : 0;  // the reference's early exit (:2982-2986)
+        if (S.done) atomicAdd(&a.g->done, 1);
+      }))
+    return;
+
+  for (int it = 0; it < a.max_iter; ++it) {
+    if (ld_volatile_i(&a.g->done) >= a.nseg) break;
+    const float *__restrict__ dold = (it & 1) ? a.d1 : a.d0;
+    float *__restrict__ dnew = (it & 1) ? a.d0 : a.d1;
+    // ---- phase A: d = z + beta d ; Ad = A d ; d.Ad
+    for (int sl = blockIdx.x; sl < na; sl += gridDim.x) {
+      const int sc = slot_scene(a.slot0, a.nseg, sl);
+      if (ld_volatile_i(&st[sc].done)) continue;
+      const float beta = (float)ld_volatile_d(&st[sc].beta);
+      const int64_t q = (int64_t)sl * TILE_CELLS + tid;
+      const uint16_t code = a.code[q];
+      Acc v[1] = {0};
+      if (code & CODE_FLUID) {
+        const float dn = __ldcg(a.z + q) + beta * __ldcg(dold + q);
+        float s = 0.0f;
+#pragma unroll
+        for (int d = 0; d < 6; ++d)
+          if (code & (1 << d)) {
+            const int64_t nq = nb_index(q, d, a.nbr);
+            s = s + (__ldcg(a.z + nq) + beta * __ldcg(dold + nq));
+          }
+        const float diag = (float)((code >> CODE_DIAG_SHIFT) & 7);
+        const float ad = diag * dn - s;
+        dnew[q] = dn;
+        a.Ad[q] = ad;
+        v[0] += (Acc)(dn * ad);
+      }
+      tile_partials<Acc, 1>(a, sl, v);
+    }
+    if (!seg_reduce<Acc, 1>(a, live, [&](int sc, double *t) {
+          PcgState &S = st[sc];
+          const double pAp = t[0];
+          S.alpha = (Acc)fabs(pAp) < (Acc)1.0e-30 ? 0.0 : (double)((Acc)S.rz / (Acc)pAp);
+          if (!(pAp == pAp)) {
+            S.status = GF_NAN;
+            S.done = 1;
+            atomicAdd(&a.g->done, 1);
+          }
+        }))
+      return;
+    // ---- phase B: x += alpha d ; r -= alpha Ad ; z = M^-1 r ; r.z, r.r
+    for (int sl = blockIdx.x; sl < na; sl += gridDim.x) {
+      const int sc = slot_scene(a.slot0, a.nseg, sl);
+      if (ld_volatile_i(&st[sc].done)) continue;
+      const float alpha = (float)ld_volatile_d(&st[sc].alpha);
+      const float nalpha = -alpha;
+      const int64_t q = (int64_t)sl * TILE_CELLS + tid;
+      const uint16_t code = a.code[q];
+      Acc v[2] = {0, 0};
+      if (code & CODE_FLUID) {
+        const float dn = __ldcg(dnew + q);
+        a.x[q] = __ldcg(a.x + q) + alpha * dn;
+        const float rn = __ldcg(a.r + q) + nalpha * __ldcg(a.Ad + q);
+        const float diag = fmaxf((float)((code >> CODE_DIAG_SHIFT) & 7), 1.0f);
+        const float z = rn / diag;
+        a.r[q] = rn;
+        a.z[q] = z;
+        v[0] += (Acc)(rn * z);
+        v[1] += (Acc)(rn * rn);
+      }
+      tile_partials<Acc, 2>(a, sl, v);
+    }
+    const int it1 = it + 1;
+    if (!seg_reduce<Acc, 2>(a, live, [&](int sc, double *t) {
+          PcgState &S = st[sc];
+          const double rz_new = t[0], rr = t[1];
+          S.iters = it1;
+          S.rr = rr;
+          if (!(rr == rr)) {
+            S.status = GF_NAN;
+            S.done = 1;
+            atomicAdd(&a.g->done, 1);
+            return;
+          }
+          int replace = 0;
+          if (REF) {
+            replace = rr < a.replace2 * S.r_upd2 || rr < a.tol2 * S.b2;
+          } else {
+            const bool check = (it1 % a.check_every) == 0 || it1 == a.max_iter;
+            if (check && rr < a.tol2 * S.r0) {
+              S.done = 1;
+              atomicAdd(&a.g->done, 1);
+            }
+          }
+          if (replace) {
+            S.n_replace = -S.n_replace - 1;  // negative: replacement pending
+            atomicAdd(&a.g->n_replace, 1);
+          } else {
+            const double rz = S.rz;
+            S.beta = (Acc)fabs(rz) < (Acc)1.0e-30 ? 0.0 : (double)((Acc)rz_new / (Acc)rz);
+            S.rz = rz_new;
+          }
+        }))
+      return;
+    // ---- refined: FP64 residual replacement r = b - A x for pending scenes
+    if (REF && ld_volatile_i(&a.g->n_replace) > 0) {
+      for (int sl = blockIdx.x; sl < na; sl += gridDim.x) {
+        const int sc = slot_scene(a.slot0, a.nseg, sl);
+        if (ld_volatile_i(&st[sc].n_replace) >= 0) continue;
+        const int64_t q = (int64_t)sl * TILE_CELLS + tid;
+        if (!(a.code[q] & CODE_FLUID)) continue;
+        a.x64[q] = __ldcg(a.x64 + q) + (double)__ldcg(a.x + q);
+        a.x[q] = 0.0f;
+      }
+      if (!seg_reduce<double, 1>(a, [](int) { return false; }, [](int, double *) {})) return;
+      for (int sl = blockIdx.x; sl < na; sl += gridDim.x) {
+        const int sc = slot_scene(a.slot0, a.nseg, sl);
+        if (ld_volatile_i(&st[sc].n_replace) >= 0) continue;
+        const int64_t q = (int64_t)sl * TILE_CELLS + tid;
+        const uint16_t code = a.code[q];
+        double v[3] = {0, 0, 0};
+        if (code & CODE_FLUID) {
+          double s = 0.0;
+#pragma unroll
+          for (int d = 0; d < 6; ++d)
+            if (code & (1 << d)) s += __ldcg(a.x64 + nb_index(q, d, a.nbr));
+          const double diag = (double)((code >> CODE_DIAG_SHIFT) & 7);
+          const double res = (double)(a.sign * a.bdiv[q]) - (diag * __ldcg(a.x64 + q) - s);
+          const float rf = (float)res;
+          const float z = rf / fmaxf((float)diag, 1.0f);
+          a.r[q] = rf;
+          a.z[q] = z;
+          v[0] += res * res;
+          v[1] += (double)(rf * z);
+          v[2] += (double)(rf * rf);
+        }
+        tile_partials<double, 3>(a, sl, v);
+      }
+      if (!seg_reduce<double, 3>(
+              a, [&](int sc) { return ld_volatile_i(&st[sc].n_replace) < 0; },
+              [&](int sc, double *t) {
+                PcgState &S = st[sc];
+                S.r_true2 = t[0];
+                S.r_upd2 = t[2];
+                S.rr = t[2];
+                S.n_replace = -S.n_replace;  // back to a positive count (+1)
+                atomicSub(&a.g->n_replace, 1);
+                const double rz = S.rz;
+                S.beta = fabs(rz) < 1.0e-30 ? 0.0 : t[1] / rz;
+                S.rz = t[1];
+                if (t[0] <= a.tol2 * S.b2) {
+                  S.done = 1;
+                  atomicAdd(&a.g->done, 1);
+                }
+              }))
+        return;
+    }
+  }
+  if (blockIdx.x == 0)
+    for (int sc = tid; sc < a.nseg; sc += blockDim.x)
+      if (!ld_volatile_i(&st[sc].done)) st[sc].status = GF_NOT_CONVERGED;
+}
+
 struct ScatterArgs {
   const int32_t *n_active, *tile_list;
   const uint16_t *code;
@@ -505,6 +897,23 @@ __global__ void k_scatter_p(ScatterArgs a) {
   }
 }
 
+__global__ void kb_scatter_p(ScatterArgs a, SegIndex sx) {
+  const int64_t total = (int64_t)(*a.n_active) * TILE_CELLS;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    if (!(a.code[q] & CODE_FLUID)) continue;
+    const int s = (int)(q >> 9), l = (int)(q & 511);
+    const int tg = a.tile_list[s];
+    const SegRow r = sx.row[seg_find(sx.tile0, sx.n, tg)];
+    const int t = (int)(tg - r.tile0);
+    const int ti = t / (r.nty * r.ntz), tj = (t / r.ntz) % r.nty, tk = t % r.ntz;
+    const int gi = ti * 8 + (l >> 6), gj = tj * 8 + ((l >> 3) & 7), gk = tk * 8 + (l & 7);
+    float v = a.x[q];
+    if (a.x64) v = (float)(a.x64[q] + (double)v);
+    a.p[r.cell0 + ((int64_t)gi * r.ny + gj) * r.nz + gk] = v;
+  }
+}
+
 // ------------------------------------------------------------- host side
 int pressure_alloc(Ctx *c) {
   const int64_t nk = c->nkeys;
@@ -521,8 +930,8 @@ int pressure_alloc(Ctx *c) {
   for (int q = 0; q < 7; ++q)
     if ((e = A((void **)vecs[q], nk * 4, "alloc pressure vector"))) return e;
   if ((e = A((void **)&c->x64, nk * 8, "alloc x64"))) return e;
-  if ((e = A((void **)&c->partials, 3 * MAX_PCG_BLOCKS * sizeof(double), "alloc partials")))
-    return e;
+  const int64_t np = c->ntiles > MAX_PCG_BLOCKS ? c->ntiles : MAX_PCG_BLOCKS;
+  if ((e = A((void **)&c->partials, 3 * np * sizeof(double), "alloc partials"))) return e;
   if ((e = A((void **)&c->state, sizeof(PcgState), "alloc pcg state"))) return e;
   if ((e = A((void **)&c->bar_counters, 8 * 16 * 8, "alloc barrier counters"))) return e;
   if ((e = A((void **)&c->trace, TRACE_CAP * 8, "alloc trace"))) return e;
@@ -551,6 +960,8 @@ static int coop_grid(Ctx *c) {
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg<Acc, REF>,
                                                                 PCG_THREADS, 0);
   if (e != cudaSuccess || per_sm < 1) return 0;
+  if (c->tune.pcg_blocks_per_sm > 0 && c->tune.pcg_blocks_per_sm < per_sm)
+    per_sm = c->tune.pcg_blocks_per_sm;
   int g = per_sm * c->num_sms;
   return g > MAX_PCG_BLOCKS ? MAX_PCG_BLOCKS : g;
 }
@@ -567,12 +978,106 @@ static int launch_pcg(Ctx *c, PcgArgs &pa) {
   return e;
 }
 
+template <typename Acc, bool REF>
+static int launch_pcg_seg(Ctx *c, SegPcgArgs &pa) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_seg<Acc, REF>, TILE_CELLS,
+                                                    0) != cudaSuccess ||
+      per_sm < 1)
+    return fail(c, GF_CUDA_ERROR, "segmented PCG: cooperative occupancy query failed");
+  if (c->tune.pcg_blocks_per_sm > 0 && c->tune.pcg_blocks_per_sm < per_sm)
+    per_sm = c->tune.pcg_blocks_per_sm;
+  void *args[] = {&pa};
+  int e = check_cuda(c, cudaLaunchCooperativeKernel((const void *)k_pcg_seg<Acc, REF>,
+                                                    dim3(per_sm * c->num_sms), dim3(TILE_CELLS),
+                                                    args, 0, c->stream),
+                     "cooperative segmented PCG launch");
+  c->launches++;
+  return e;
+}
+
+// The pressure stage of a batch: set-up over every scene's tiles, then the
+// sweeps (scene-agnostic on the compact layout) or the segmented PCG.
+static int launch_pressure_batch(Ctx *c, const gf_step_params *prm) {
+  cudaStream_t st = c->stream;
+  const int solver = prm->solver;
+  const SegIndex sx = seg_index(c);
+  int e;
+  int32_t *flag = c->tile_nbr;  // consumed by the compaction before the set-up
+  kb_tile_flags<<<(unsigned)((c->ntiles * 32 + 255) / 256), 256, 0, st>>>(c->f.label, sx,
+                                                                          c->ntiles, flag);
+  k_tile_compact<<<1, 1024, 0, st>>>(flag, c->ntiles, c->tile_slot, c->tile_list, c->n_active);
+  kb_slot_ranges<<<(unsigned)((c->nseg + 256) / 256), 256, 0, st>>>(c->tile_list, c->n_active,
+                                                                    sx, c->seg_slot0);
+  c->launches += 3;
+  const bool refined = solver == GF_PCG_REFINED;
+  int64_t *n_fluid = reinterpret_cast<int64_t *>(c->n_active + 2);
+  if ((e = check_cuda(c, cudaMemsetAsync(n_fluid, 0, 8, st), "zero fluid count"))) return e;
+  BatchSetupArgs ba{{c->f.label, c->f.div, c->n_active, c->tile_list, c->tile_slot, c->tile_nbr,
+                     c->code, c->bdiv, c->xf, c->r, c->z, c->d0, c->d1, c->Ad,
+                     refined ? c->x64 : nullptr, n_fluid, c->tile_cost, 0, 0, 0, 0, 0, 0},
+                    sx};
+  {
+    int g = c->ntiles < c->num_sms * 4 ? c->ntiles : c->num_sms * 4;
+    kb_tile_setup<<<g > 0 ? g : 1, 512, 0, st>>>(ba);
+    c->launches++;
+  }
+  const unsigned gs = (unsigned)(c->num_sms * 8);
+  SweepArgs sw{c->n_active, c->tile_nbr, c->code, c->bdiv};
+  const float *result = c->xf;
+  const double *result64 = nullptr;
+  if (c->timing) cudaEventRecord(c->ev[8], st);
+  if (solver == GF_JACOBI) {
+    float *a = c->xf, *b = c->z;
+    for (int it = 0; it < prm->max_iters; ++it) {
+      k_jacobi<<<gs, 256, 0, st>>>(sw, a, b);
+      float *t = a; a = b; b = t;
+    }
+    c->launches += prm->max_iters;
+    result = a;
+    c->last_iters = prm->max_iters;
+  } else if (solver == GF_GSRB) {
+    for (int it = 0; it < prm->max_iters; ++it) {
+      k_gsrb<<<gs, 256, 0, st>>>(sw, c->xf, 0);
+      k_gsrb<<<gs, 256, 0, st>>>(sw, c->xf, 1);
+    }
+    c->launches += 2 * prm->max_iters;
+    c->last_iters = prm->max_iters;
+  } else {
+    if ((e = check_cuda(c, cudaMemsetAsync(c->state, 0, sizeof(PcgState), st), "zero state")) ||
+        (e = check_cuda(c, cudaMemsetAsync(c->seg_state, 0, c->nseg * sizeof(PcgState), st),
+                        "zero scene states")))
+      return e;
+    const int check_every = prm->check_every > 0 ? prm->check_every : 1;
+    const float sign = prm->rhs_sign >= 0 ? 1.0f : -1.0f;
+    SegPcgArgs pa{c->n_active, c->tile_nbr, c->seg_slot0, c->nseg, c->code, c->bdiv, c->xf,
+                  c->r, c->z, c->d0, c->d1, c->Ad, refined ? c->x64 : nullptr, c->partials,
+                  c->ntiles > MAX_PCG_BLOCKS ? c->ntiles : MAX_PCG_BLOCKS, c->seg_state,
+                  c->state, prm->max_iters, check_every, prm->tol * prm->tol, 1e-4, sign};
+    if (refined) {
+      e = launch_pcg_seg<double, true>(c, pa);
+      result64 = c->x64;
+    } else {
+      e = launch_pcg_seg<float, false>(c, pa);
+    }
+    if (e) return e;
+  }
+  if (c->timing) cudaEventRecord(c->ev[9], st);
+  if ((e = check_cuda(c, cudaMemsetAsync(c->f.p, 0, c->ncell * 4, st), "zero p"))) return e;
+  ScatterArgs sc{c->n_active, c->tile_list, c->code, result, result64, c->f.p, 0, 0, 0, 0};
+  kb_scatter_p<<<gs, 256, 0, st>>>(sc, sx);
+  c->launches++;
+  c->last_solver = solver;
+  return check_launch(c, "gf_pressure");
+}
+
 int launch_pressure(Ctx *c, const gf_step_params *prm) {
   if (!c->bound) return fail(c, GF_INVALID_ARG, "gf_pressure: buffers not bound");
   const int solver = prm->solver;
   if (solver < GF_JACOBI || solver > GF_PCG_REFINED)
     return fail(c, GF_INVALID_ARG, "unknown pressure_solver");
   if (prm->max_iters < 0) return fail(c, GF_INVALID_ARG, "pressure_iters must be >= 0");
+  if (c->nseg > 0) return launch_pressure_batch(c, prm);
   cudaStream_t st = c->stream;
   int e;
   // ---- active tiles

@@ -124,12 +124,13 @@ __device__ __forceinline__ void p2g_flush_box(const P2GArgs &a, float (*s_val)[B
   }
 }
 
+// One tile's P2G: t is the tile within its grid (its coordinates), key0 the
+// sort key of its first cell (t * 512 for a single grid).
 template <bool APIC>
-__global__ void __launch_bounds__(256) k_p2g_tile(P2GArgs a) {
+__device__ __forceinline__ void p2g_tile_body(const P2GArgs &a, int t, int64_t key0) {
   __shared__ float s_val[3][BOX];
   __shared__ float s_wt[3][BOX];
-  const int t = blockIdx.x;
-  const int64_t b = a.start[(int64_t)t * TILE_CELLS], e = a.start[(int64_t)(t + 1) * TILE_CELLS];
+  const int64_t b = a.start[key0], e = a.start[key0 + TILE_CELLS];
   if (b == e) return;
   for (int q = threadIdx.x; q < 3 * BOX; q += blockDim.x) {
     (&s_val[0][0])[q] = 0.f;
@@ -168,6 +169,11 @@ __global__ void __launch_bounds__(256) k_p2g_tile(P2GArgs a) {
   p2g_flush_box(a, s_val, s_wt, I0, J0, K0);
 }
 
+template <bool APIC>
+__global__ void __launch_bounds__(256) k_p2g_tile(P2GArgs a) {
+  p2g_tile_body<APIC>(a, blockIdx.x, (int64_t)blockIdx.x * TILE_CELLS);
+}
+
 // --------------------------------------------------------------- forces
 struct GridArgs {
   float *u, *v, *w, *us, *vs, *ws;
@@ -179,11 +185,11 @@ struct GridArgs {
   int nx, ny, nz;
 };
 
-__global__ void k_forces(GridArgs a, float gd) {
+// Face slot q = (i*(ny+1) + j)*(nz+1) + k carries the u, v and w faces (i,j,k)
+// that exist.
+__device__ __forceinline__ void forces_slot(const GridArgs &a, int64_t q, float gd) {
   const int nx = a.nx, ny = a.ny, nz = a.nz;
-  int64_t n = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
-  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
-       q += (int64_t)gridDim.x * blockDim.x) {
+  {
     int k = (int)(q % (nz + 1));
     int64_t r = q / (nz + 1);
     int j = (int)(r % (ny + 1)), i = (int)(r / (ny + 1));
@@ -221,14 +227,19 @@ __global__ void k_forces(GridArgs a, float gd) {
   }
 }
 
-__global__ void k_divergence(GridArgs a, float scale) {
-  const int nx = a.nx, ny = a.ny, nz = a.nz;
-  int64_t n = (int64_t)nx * ny * nz;
-  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
-       c += (int64_t)gridDim.x * blockDim.x) {
+__global__ void k_forces(GridArgs a, float gd) {
+  int64_t n = (int64_t)(a.nx + 1) * (a.ny + 1) * (a.nz + 1);
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
+       q += (int64_t)gridDim.x * blockDim.x)
+    forces_slot(a, q, gd);
+}
+
+__device__ __forceinline__ void divergence_cell(const GridArgs &a, int64_t c, float scale) {
+  const int ny = a.ny, nz = a.nz;
+  {
     if (a.label[c] != 1) {
       a.div[c] = 0.0f;
-      continue;
+      return;
     }
     int k = (int)(c % nz);
     int64_t r = c / nz;
@@ -242,11 +253,16 @@ __global__ void k_divergence(GridArgs a, float scale) {
   }
 }
 
-__global__ void k_project(GridArgs a, float scale) {
+__global__ void k_divergence(GridArgs a, float scale) {
+  int64_t n = (int64_t)a.nx * a.ny * a.nz;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x)
+    divergence_cell(a, c, scale);
+}
+
+__device__ __forceinline__ void project_slot(const GridArgs &a, int64_t q, float scale) {
   const int nx = a.nx, ny = a.ny, nz = a.nz;
-  int64_t n = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
-  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
-       q += (int64_t)gridDim.x * blockDim.x) {
+  {
     int k = (int)(q % (nz + 1));
     int64_t r = q / (nz + 1);
     int j = (int)(r % (ny + 1)), i = (int)(r / (ny + 1));
@@ -306,6 +322,13 @@ __global__ void k_project(GridArgs a, float scale) {
       a.w[g] = val;
     }
   }
+}
+
+__global__ void k_project(GridArgs a, float scale) {
+  int64_t n = (int64_t)(a.nx + 1) * (a.ny + 1) * (a.nz + 1);
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
+       q += (int64_t)gridDim.x * blockDim.x)
+    project_slot(a, q, scale);
 }
 
 // ------------------------------------------------------------------- G2P
@@ -407,9 +430,7 @@ struct G2PArgs {
 };
 
 template <bool APIC>
-__global__ void __launch_bounds__(256) k_g2p(G2PArgs a) {
-  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (q >= a.n) return;
+__device__ __forceinline__ void g2p_particle(const G2PArgs &a, int64_t q) {
   const float4 r0 = a.rec0[q];
   const float px = r0.x, py = r0.y, pz = r0.z;
   const float dx = a.dx;
@@ -449,6 +470,112 @@ __global__ void __launch_bounds__(256) k_g2p(G2PArgs a) {
   a.pid[q] = __float_as_int(r0.w);
 }
 
+template <bool APIC>
+__global__ void __launch_bounds__(512) k_g2p(G2PArgs a) {
+  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= a.n) return;
+  g2p_particle<APIC>(a, q);
+}
+
+// ------------------------------------------------------------- batches
+// The stage kernels over a batch of scenes: every item (tile, face slot,
+// cell, particle) finds its scene in the segment table and runs the
+// single-grid body on that scene's view of the concatenated arrays.
+struct BatchArgs {
+  SegIndex sx;
+  const int32_t *start;
+  const float4 *rec0, *rec1, *rec2, *rec3;
+  float *u, *v, *w, *uw, *vw, *ww, *us, *vs, *ws;
+  const uint8_t *label;
+  float *div;
+  const float *p;
+  float *pos, *vel, *C;
+  int32_t *pid;
+  int64_t n;
+  float dt, flip_blend, rho;
+};
+
+__device__ __forceinline__ GridArgs grid_view(const BatchArgs &b, const SegRow &r) {
+  GridArgs a;
+  a.u = b.u + r.fu0; a.v = b.v + r.fv0; a.w = b.w + r.fw0;
+  a.us = b.us + r.fu0; a.vs = b.vs + r.fv0; a.ws = b.ws + r.fw0;
+  a.uw = b.uw + r.fu0; a.vw = b.vw + r.fv0; a.ww = b.ww + r.fw0;
+  a.label = b.label + r.cell0;
+  a.solid_u = a.solid_v = a.solid_w = nullptr;  // static solids in a batch
+  a.div = b.div + r.cell0;
+  a.p = b.p + r.cell0;
+  a.nx = r.nx; a.ny = r.ny; a.nz = r.nz;
+  return a;
+}
+
+template <bool APIC>
+__global__ void __launch_bounds__(256) kb_p2g_tile(BatchArgs b) {
+  const int64_t t = blockIdx.x;
+  const int s = seg_find(b.sx.tile0, b.sx.n, t);
+  const SegRow r = b.sx.row[s];
+  P2GArgs a{b.start, b.rec0, b.rec1, b.rec2, b.rec3, b.u + r.fu0, b.v + r.fv0, b.w + r.fw0,
+            b.uw + r.fu0, b.vw + r.fv0, b.ww + r.fw0, r.dx, r.nx, r.ny, r.nz, r.nty, r.ntz};
+  p2g_tile_body<APIC>(a, (int)(t - r.tile0), t * TILE_CELLS);
+}
+
+__global__ void kb_forces(BatchArgs b, int64_t nslot, float gravity) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nslot;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int s = seg_find(b.sx.fslot0, b.sx.n, q);
+    const SegRow r = b.sx.row[s];
+    const float gd = gravity * b.dt;
+    forces_slot(grid_view(b, r), q - r.fslot0, gd);
+  }
+}
+
+__global__ void kb_divergence(BatchArgs b, int64_t ncell) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncell;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    const int s = seg_find(b.sx.cell0, b.sx.n, c);
+    const SegRow r = b.sx.row[s];
+    float scale = b.rho * r.dx;  // (rho * dx) / dt per scene
+    scale = scale / b.dt;
+    divergence_cell(grid_view(b, r), c - r.cell0, scale);
+  }
+}
+
+__global__ void kb_project(BatchArgs b, int64_t nslot) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nslot;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int s = seg_find(b.sx.fslot0, b.sx.n, q);
+    const SegRow r = b.sx.row[s];
+    float scale = b.rho * r.dx;  // dt / (rho * dx) per scene
+    scale = b.dt / scale;
+    project_slot(grid_view(b, r), q - r.fslot0, scale);
+  }
+}
+
+template <bool APIC>
+__global__ void __launch_bounds__(512) kb_g2p(BatchArgs b) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= b.n) return;
+  const int s = seg_find(b.sx.part0, b.sx.n, q);
+  const SegRow r = b.sx.row[s];
+  G2PArgs a{b.rec0, b.rec1, b.u + r.fu0, b.v + r.fv0, b.w + r.fw0, b.us + r.fu0,
+            b.vs + r.fv0, b.ws + r.fw0, b.pos, b.vel, b.C, b.pid, b.n, r.dx, b.dt,
+            b.flip_blend, r.dom0, r.dom1, r.dom2, r.nx, r.ny, r.nz};
+  g2p_particle<APIC>(a, q);
+}
+
+static BatchArgs batch_args(Ctx *c) {
+  BatchArgs b{};
+  b.sx = seg_index(c);
+  b.start = c->start;
+  b.rec0 = c->rec0; b.rec1 = c->rec1; b.rec2 = c->rec2; b.rec3 = c->rec3;
+  b.u = c->f.u; b.v = c->f.v; b.w = c->f.w;
+  b.uw = c->f.uw; b.vw = c->f.vw; b.ww = c->f.ww;
+  b.us = c->f.us; b.vs = c->f.vs; b.ws = c->f.ws;
+  b.label = c->f.label; b.div = c->f.div; b.p = c->f.p;
+  b.pos = c->p.pos; b.vel = c->p.vel; b.C = c->p.C; b.pid = c->p.pid;
+  b.n = c->p.n;
+  return b;
+}
+
 // ------------------------------------------------------------------- CFL
 __global__ void k_vmax(const float *__restrict__ vel, int64_t n, float *out) {
   float m = 0.f;
@@ -475,18 +602,22 @@ int launch_p2g(Ctx *c, int transfer) {
   if (!c->bound) return fail(c, GF_INVALID_ARG, "gf_p2g: buffers not bound");
   if (transfer == GF_APIC && !c->p.C) return fail(c, GF_INVALID_ARG, "gf_p2g: APIC needs C");
   cudaStream_t st = c->stream;
-  const int64_t nu = (int64_t)(c->nx + 1) * c->ny * c->nz,
-                nv = (int64_t)c->nx * (c->ny + 1) * c->nz,
-                nw = (int64_t)c->nx * c->ny * (c->nz + 1);
   float *bufs[6] = {c->f.u, c->f.uw, c->f.v, c->f.vw, c->f.w, c->f.ww};
-  int64_t lens[6] = {nu, nu, nv, nv, nw, nw};
+  int64_t lens[6] = {c->nu, c->nu, c->nv, c->nv, c->nw, c->nw};
   for (int q = 0; q < 6; ++q) {
     int e = check_cuda(c, cudaMemsetAsync(bufs[q], 0, lens[q] * 4, st), "memset p2g");
     if (e) return e;
   }
   P2GArgs a{c->start, c->rec0, c->rec1, c->rec2, c->rec3, c->f.u, c->f.v, c->f.w,
             c->f.uw, c->f.vw, c->f.ww, c->dx, c->nx, c->ny, c->nz, c->nty, c->ntz};
-  if (c->p.n > 0) {
+  if (c->p.n > 0 && c->nseg > 0) {
+    BatchArgs b = batch_args(c);
+    if (transfer == GF_APIC)
+      kb_p2g_tile<true><<<c->ntiles, 256, 0, st>>>(b);
+    else
+      kb_p2g_tile<false><<<c->ntiles, 256, 0, st>>>(b);
+    c->launches++;
+  } else if (c->p.n > 0) {
     if (transfer == GF_APIC)
       k_p2g_tile<true><<<c->ntiles, 256, 0, st>>>(a);
     else
@@ -508,26 +639,52 @@ static GridArgs grid_args(Ctx *c) {
   return a;
 }
 
+static inline unsigned grid_tuned(const Ctx *c, int64_t n) {
+  int64_t g = (n + c->tune.grid_threads - 1) / c->tune.grid_threads;
+  int64_t cap = (int64_t)c->num_sms * c->tune.grid_blocks_per_sm;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (unsigned)g;
+}
+
 int launch_forces_div(Ctx *c, float gravity, float dt, float rho) {
   if (!c->bound) return fail(c, GF_INVALID_ARG, "gf_forces_div: buffers not bound");
+  if (c->nseg > 0) {
+    BatchArgs b = batch_args(c);
+    b.dt = dt;
+    b.rho = rho;
+    const int th = c->tune.grid_threads;
+    kb_forces<<<grid_tuned(c, c->nfslot), th, 0, c->stream>>>(b, c->nfslot, gravity);
+    kb_divergence<<<grid_tuned(c, c->ncell), th, 0, c->stream>>>(b, c->ncell);
+    c->launches += 2;
+    return check_launch(c, "gf_forces_div");
+  }
   GridArgs a = grid_args(c);
   float gd = gravity * dt;        // g * dt in float32, as k3_add_gravity
   float scale = rho * c->dx;      // (rho * dx) / dt, as k3_compute_divergence
   scale = scale / dt;
-  int64_t nf = (int64_t)(c->nx + 1) * (c->ny + 1) * (c->nz + 1);
-  k_forces<<<grid_for(nf, 256, c->num_sms), 256, 0, c->stream>>>(a, gd);
-  k_divergence<<<grid_for(c->ncell, 256, c->num_sms), 256, 0, c->stream>>>(a, scale);
+  const int th = c->tune.grid_threads;
+  k_forces<<<grid_tuned(c, c->nfslot), th, 0, c->stream>>>(a, gd);
+  k_divergence<<<grid_tuned(c, c->ncell), th, 0, c->stream>>>(a, scale);
   c->launches += 2;
   return check_launch(c, "gf_forces_div");
 }
 
 int launch_project(Ctx *c, float dt, float rho) {
   if (!c->bound) return fail(c, GF_INVALID_ARG, "gf_project: buffers not bound");
+  const int th = c->tune.grid_threads;
+  if (c->nseg > 0) {
+    BatchArgs b = batch_args(c);
+    b.dt = dt;
+    b.rho = rho;
+    kb_project<<<grid_tuned(c, c->nfslot), th, 0, c->stream>>>(b, c->nfslot);
+    c->launches++;
+    return check_launch(c, "gf_project");
+  }
   GridArgs a = grid_args(c);
   float scale = rho * c->dx;  // dt / (rho * dx), as k3_subtract_pressure_grad
   scale = dt / scale;
-  int64_t nf = (int64_t)(c->nx + 1) * (c->ny + 1) * (c->nz + 1);
-  k_project<<<grid_for(nf, 256, c->num_sms), 256, 0, c->stream>>>(a, scale);
+  k_project<<<grid_tuned(c, c->nfslot), th, 0, c->stream>>>(a, scale);
   c->launches++;
   return check_launch(c, "gf_project");
 }
@@ -536,14 +693,26 @@ int launch_g2p(Ctx *c, int transfer, float flip_blend, float dt) {
   if (!c->bound) return fail(c, GF_INVALID_ARG, "gf_g2p: buffers not bound");
   if (transfer == GF_APIC && !c->p.C) return fail(c, GF_INVALID_ARG, "gf_g2p: APIC needs C");
   if (c->p.n == 0) return GF_OK;
+  const int th = c->tune.g2p_threads;
+  const unsigned g = (unsigned)((c->p.n + th - 1) / th);
+  if (c->nseg > 0) {
+    BatchArgs b = batch_args(c);
+    b.dt = dt;
+    b.flip_blend = flip_blend;
+    if (transfer == GF_APIC)
+      kb_g2p<true><<<g, th, 0, c->stream>>>(b);
+    else
+      kb_g2p<false><<<g, th, 0, c->stream>>>(b);
+    c->launches++;
+    return check_launch(c, "gf_g2p");
+  }
   G2PArgs a{c->rec0, c->rec1, c->f.u, c->f.v, c->f.w, c->f.us, c->f.vs, c->f.ws,
             c->p.pos, c->p.vel, c->p.C, c->p.pid, c->p.n, c->dx, dt, flip_blend,
             c->dom[0], c->dom[1], c->dom[2], c->nx, c->ny, c->nz};
-  unsigned g = (unsigned)((c->p.n + 255) / 256);
   if (transfer == GF_APIC)
-    k_g2p<true><<<g, 256, 0, c->stream>>>(a);
+    k_g2p<true><<<g, th, 0, c->stream>>>(a);
   else
-    k_g2p<false><<<g, 256, 0, c->stream>>>(a);
+    k_g2p<false><<<g, th, 0, c->stream>>>(a);
   c->launches++;
   return check_launch(c, "gf_g2p");
 }

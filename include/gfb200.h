@@ -203,6 +203,55 @@ int gf_sample_cells(void *ctx, const float *grid3, const float *pos, int64_t n, 
 int gf_sample_cells_adjoint(void *ctx, const float *pos, int64_t n, const float *vel_bar,
                             float *grid3_bar);
 
+/* ---- batches of independent scenes -------------------------------------- */
+/* No counterpart in the reference (which steps one FlipSolver3D at a time).
+ * A batch context steps many scenes of uneven grid sizes together: gf_step
+ * (and every stage call) runs ONE launch per stage kernel over all scenes,
+ * each item finding its scene in a segment table; the pressure PCG is one
+ * persistent kernel that keeps per-scene scalars and stops each scene at its
+ * own tolerance.  Scenes are concatenated in table order in every array:
+ * cells (label, p, div), u-, v- and w-shaped faces, particles (the caller
+ * passes each scene's particle count).  gf_batch_plan returns that layout
+ * (per scene, nullable) and the totals without touching a GPU; solid
+ * velocities must be NULL (static solids).  The adjoint and the density /
+ * control-sampling calls take single-scene contexts only. */
+typedef struct gf_scene_layout {
+  int64_t cell0;           /* first cell of the scene in cell arrays */
+  int64_t fu0, fv0, fw0;   /* first u, v, w face in the face arrays */
+  int64_t tile0, ntiles;   /* its 8^3 tiles (sort key = tile*512 + local cell) */
+  int64_t fslot0;          /* first (nx+1)(ny+1)(nz+1) face slot */
+} gf_scene_layout;
+typedef struct gf_batch_totals {
+  int64_t ncell, nu, nv, nw, ntiles, nslot;
+} gf_batch_totals;
+int gf_batch_plan(const gf_grid_desc *scenes, int32_t n, gf_scene_layout *rows,
+                  gf_batch_totals *totals);
+int gf_batch_create(const gf_grid_desc *scenes, int32_t n, int64_t max_particles,
+                    void **ctx_out);
+/* fields: concatenated arrays sized by gf_batch_totals; parts: all scenes'
+ * particles, scene after scene; counts[n]: particles per scene. */
+int gf_batch_bind(void *ctx, const gf_fields *fields, const gf_particles *parts,
+                  const int64_t *counts);
+/* Per-scene iterations, relative residual and status of the last pressure
+ * solve (arrays of n, each nullable); synchronises. */
+int gf_batch_pressure_stats(void *ctx, int32_t *iters, double *relres, int32_t *status);
+
+/* ---- launch-shape autotuner --------------------------------------------- */
+/* No counterpart in the reference.  gf_autotune times real substeps (the
+ * particle state is restored afterwards) and keeps the fastest launch shapes
+ * for G2P, the grid-stride face/cell kernels and the global-memory PCG;
+ * gf_get_tune / gf_set_tune read or impose them.  Synchronises. */
+typedef struct gf_tune_info {
+  int32_t g2p_threads;        /* threads per G2P block (32..512) */
+  int32_t grid_threads;       /* threads per block of forces/divergence/project */
+  int32_t grid_blocks_per_sm; /* cap of their grid-stride launches */
+  int32_t pcg_blocks_per_sm;  /* global-memory PCG residency, 0 = occupancy maximum */
+  float step_ms_before, step_ms_after;  /* gf_autotune: substep time before / after */
+} gf_tune_info;
+int gf_autotune(void *ctx, const gf_step_params *prm, gf_tune_info *out);
+int gf_get_tune(void *ctx, gf_tune_info *out);
+int gf_set_tune(void *ctx, const gf_tune_info *in);
+
 /* ---- allocation-free variant ------------------------------------------- */
 /* No counterpart in the reference.  For callers that may not allocate device
  * memory (a host that owns every device allocation through its own pool, or
