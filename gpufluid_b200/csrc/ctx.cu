@@ -56,7 +56,8 @@ static void destroy(Ctx *c) {
   if (!c) return;
   free_particles(c);
   void *ps[] = {c->count, c->start, c->scan_part, c->vmax_dev, c->adj_faces, c->adj_part,
-                c->seg, c->seg_off, c->seg_state, c->seg_slot0};
+                c->seg, c->seg_off, c->seg_state, c->seg_slot0, c->pcg_blk_job0,
+                c->pcg_jobs};
   for (void *p : ps)
     if (p) cudaFree(p);
   if (c->seg_state_host) cudaFreeHost(c->seg_state_host);
@@ -178,6 +179,10 @@ int gf_batch_create(const gf_grid_desc *scenes, int32_t n, int64_t max_particles
       (e = gf::check_cuda(c, cudaMalloc(&c->seg_state, n * sizeof(gf::PcgState)),
                           "alloc scene states")) ||
       (e = gf::check_cuda(c, cudaMalloc(&c->seg_slot0, (n + 1) * 4), "alloc scene slots")) ||
+      (e = gf::check_cuda(c, cudaMalloc(&c->pcg_blk_job0, (gf::MAX_PCG_BLOCKS + 1) * 4),
+                          "alloc PCG job ranges")) ||
+      (e = gf::check_cuda(c, cudaMalloc(&c->pcg_jobs, gf::pcg_jobs_bytes(n)),
+                          "alloc PCG jobs")) ||
       (e = gf::check_cuda(c, cudaMallocHost((void **)&c->seg_state_host,
                                             n * sizeof(gf::PcgState)),
                           "alloc pinned scene states")) ||

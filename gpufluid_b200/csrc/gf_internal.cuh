@@ -171,6 +171,8 @@ struct Ctx {
   PcgState *seg_state = nullptr;         // [nseg]
   PcgState *seg_state_host = nullptr;    // pinned mirror
   int32_t *seg_slot0 = nullptr;          // [nseg+1] first active slot of each scene
+  int32_t *pcg_blk_job0 = nullptr;       // [MAX_PCG_BLOCKS+1] segmented PCG: jobs per block
+  void *pcg_jobs = nullptr;              // segmented PCG job table (pcg_jobs_bytes)
   int64_t nfslot = 0;                    // face slots of all scenes
   int64_t nu = 0, nv = 0, nw = 0;        // u, v, w faces of all scenes
   Tune tune;
@@ -205,6 +207,7 @@ int launch_pcg_smem(Ctx *c, PcgSmemArgs &a, bool refined);
 bool pcg_smem_fits(Ctx *c, bool refined);
 
 SegIndex seg_index(const Ctx *c);
+size_t pcg_jobs_bytes(int nseg);
 
 int pressure_alloc(Ctx *c);
 void pressure_free(Ctx *c);

@@ -588,13 +588,20 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
 
 // ------------------------------------------------------- segmented PCG
 // The Jacobi-PCG of k_pcg for a batch of independent scenes in ONE persistent
-// cooperative kernel: every scene keeps its own scalars (alpha, beta, r.z,
-// residuals, convergence, iteration count) in its PcgState row.  A block
-// works on whole tiles (one thread per cell), so each tile's dot products
-// are block sums written to a per-slot partial; at every reduction point the
-// last block to arrive sums each scene's contiguous slot range in a fixed
-// order (one warp per scene) and updates that scene's scalars.  Tiles of a
-// converged scene are skipped; the solve ends when every scene is done.
+// cooperative kernel with no grid-wide synchronisation.  A planning kernel
+// (k_pcg_plan) splits the resident blocks among the scenes in proportion to
+// their active tiles: a scene gets `nb` blocks of its own (rank 0..nb-1,
+// tiles slot0[s] + rank + k*nb), and scenes smaller than one block's share
+// are packed several to a block and solved one after the other, each entirely
+// inside that block (block barriers only).  The blocks of a multi-block scene
+// meet at a scene barrier whose last arrival sums the scene's per-block
+// partials in rank order (deterministic) and updates the scene's scalars.
+// Every scene thus iterates at its own pace and stops at its own tolerance;
+// no scene waits for another.
+struct PcgJob {
+  int scene, rank, nb, pbase;  // pbase: first partial of the scene's blocks
+};
+
 struct SegPcgArgs {
   const int32_t *n_active, *nbr, *slot0;  // slot0[nseg+1]
   int nseg;
@@ -602,275 +609,415 @@ struct SegPcgArgs {
   const float *bdiv;
   float *x, *r, *z, *d0, *d1, *Ad;
   double *x64;
-  double *partials;  // [3][pstride]
+  double *partials;  // [3][pstride], indexed by pbase + rank
   int64_t pstride;
-  PcgState *st;      // [nseg]
-  PcgState *g;       // barrier counters; done = scenes finished, n_replace = pending
+  PcgState *st;      // [nseg]: scalars, convergence and the scene barrier
+  PcgState *g;       // error flag of the solve
+  const int32_t *blk_job0;  // [grid+1] first job of each block
+  const PcgJob *jobs;
   int max_iter, check_every;
   double tol2, replace2;
   float sign;
 };
 
-__device__ __forceinline__ int slot_scene(const int32_t *__restrict__ slot0, int n, int sl) {
-  int lo = 0, hi = n - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (__ldg(slot0 + mid) <= sl) lo = mid; else hi = mid - 1;
+// Job table (one thread): `grid` blocks; the target tiles per block grows
+// from total/grid until the multi-block scenes leave at least one block for
+// the packed small ones.
+__global__ void k_pcg_plan(const int32_t *__restrict__ slot0, int nseg, int grid,
+                           PcgState *__restrict__ st, int32_t *__restrict__ blk_job0,
+                           PcgJob *__restrict__ jobs) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int total = slot0[nseg];
+  int target = (total + grid - 1) / grid;
+  if (target < 1) target = 1;
+  for (;;) {
+    int big = 0;
+    for (int s = 0; s < nseg; ++s) {
+      const int n = slot0[s + 1] - slot0[s];
+      if (n > target) big += (n + target - 1) / target;
+    }
+    if (big < grid || target >= total) break;
+    target += target / 16 + 1;
   }
-  return lo;
+  int b = 0, jb = 0, pb = 0;
+  for (int s = 0; s < nseg; ++s) {  // scenes larger than one share: own blocks
+    const int n = slot0[s + 1] - slot0[s];
+    if (n <= target) continue;
+    const int nb = (n + target - 1) / target;
+    for (int r = 0; r < nb; ++r) {
+      blk_job0[b++] = jb;
+      jobs[jb++] = PcgJob{s, r, nb, pb};
+    }
+    pb += nb;
+  }
+  // the block receiving packed small scenes (after its own big scene when
+  // every block holds one)
+  int cur = b < grid ? b : grid - 1;
+  if (b < grid) blk_job0[b] = jb;
+  int load = 0;
+  for (int s = 0; s < nseg; ++s) {
+    const int n = slot0[s + 1] - slot0[s];
+    if (n > target || n == 0) continue;
+    if (load >= target && cur + 1 < grid) {
+      ++cur;
+      blk_job0[cur] = jb;
+      load = 0;
+    }
+    jobs[jb++] = PcgJob{s, 0, 1, pb++};
+    load += n;
+  }
+  for (int q = cur + 1; q <= grid; ++q) blk_job0[q] = jb;
+  for (int s = 0; s < nseg; ++s) {  // scenes without fluid are solved already
+    st[s] = PcgState{};
+    if (slot0[s + 1] == slot0[s]) st[s].done = 1;
+  }
 }
 
-// Arrival barrier whose last block runs fin(scene, totals) for every scene
-// that want(scene) selects, on its slot-range sums of the NV partial rows.
-template <typename T, int NV, typename Want, typename Fin>
-__device__ bool seg_reduce(const SegPcgArgs &a, Want want, Fin fin) {
-  __shared__ int s_last, s_ok;
-  __syncthreads();
-  unsigned gen = 0;
-  if (threadIdx.x == 0) {
-    gen = ld_volatile(&a.g->bar_gen);
-    __threadfence();
-    const unsigned arrived = atomicAdd(&a.g->bar_count, 1u);
-    s_last = arrived == gridDim.x - 1;
-    s_ok = 1;
-  }
-  __syncthreads();
-  if (s_last) {
-    __threadfence();
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int sc = wid; sc < a.nseg; sc += nw) {
-      if (!want(sc)) continue;  // warp-uniform
-      const int b = __ldcg(a.slot0 + sc), e = __ldcg(a.slot0 + sc + 1);
-      double tot[NV];
-#pragma unroll
-      for (int k = 0; k < NV; ++k) {
-        T acc = 0;
-        for (int j = b + lane; j < e; j += 32) acc += (T)__ldcg(a.partials + k * a.pstride + j);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-        tot[k] = (double)acc;
-      }
-      if (lane == 0) fin(sc, tot);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      __threadfence();
-      atomicExch(&a.g->bar_count, 0u);
-      __threadfence();
-      atomicAdd(&a.g->bar_gen, 1u);
-    }
-  } else if (threadIdx.x == 0) {
-    long long spins = 0;
-    while (ld_volatile(&a.g->bar_gen) == gen) {
-      if (++spins > SPIN_LIMIT) {
-        atomicExch(&a.g->error, 1);
-        s_ok = 0;
-        break;
-      }
-      __nanosleep(64);
-    }
-    __threadfence();
-  }
-  __syncthreads();
-  if (ld_volatile_i(&a.g->error)) return false;
-  return s_ok;
-}
+constexpr int SEG_TG = 4;  // tiles per block step: loads of 4 tiles in flight per thread
 
+// Block sums of NV per-thread values added to tot[] (shared, by thread 0),
+// once per phase (all of a block's tiles belong to one scene):
+// per-warp shuffle trees, then warp 0 sums the 16 warp values of each row in
+// a fixed order.
 template <typename T, int NV>
-__device__ __forceinline__ void tile_partials(const SegPcgArgs &a, int sl, T (&v)[NV]) {
-  __shared__ T sh[32];
+__device__ __forceinline__ void block_acc(const T (&v)[NV], double *tot) {
+  __shared__ T sh[NV][16];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
   for (int k = 0; k < NV; ++k) {
-    const T t = block_sum<T>(v[k], sh);
-    if (threadIdx.x == 0) a.partials[k * a.pstride + sl] = (double)t;
+    T x = v[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) sh[k][wid] = x;
   }
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      T x = lane < 16 ? sh[k][lane] : (T)0;
+#pragma unroll
+      for (int o = 8; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+      if (lane == 0) tot[k] += (double)x;
+    }
+  }
+  __syncthreads();
+}
+
+// Scene reduction + barrier: tot[] (shared, this block's sums) becomes the
+// scene's totals and fin(totals) runs once; afterwards every block of the
+// scene sees the updated scene state.  Returns false on a barrier timeout.
+template <int NV, typename Fin>
+__device__ __forceinline__ bool scene_reduce(const SegPcgArgs &a, const PcgJob &j, double *tot, Fin fin) {
+  __shared__ int s_ok;
+  PcgState *S = a.st + j.scene;
+  if (j.nb == 1) {
+    if (threadIdx.x == 0) fin(tot);
+    __syncthreads();
+    return true;
+  }
+  if (threadIdx.x == 0) {
+    s_ok = 1;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) a.partials[k * a.pstride + j.pbase + j.rank] = tot[k];
+    const unsigned gen = ld_volatile(&S->bar_gen);
+    __threadfence();
+    const unsigned arrived = atomicAdd(&S->bar_count, 1u);
+    if (arrived == (unsigned)j.nb - 1) {
+      __threadfence();
+      double all[NV];
+#pragma unroll
+      for (int k = 0; k < NV; ++k) {
+        all[k] = 0.0;
+        for (int r = 0; r < j.nb; ++r) all[k] += __ldcg(a.partials + k * a.pstride + j.pbase + r);
+      }
+      fin(all);
+      __threadfence();
+      atomicExch(&S->bar_count, 0u);
+      __threadfence();
+      atomicAdd(&S->bar_gen, 1u);
+    } else {
+      long long spins = 0;
+      while (ld_volatile(&S->bar_gen) == gen) {
+        if (++spins > SPIN_LIMIT) {
+          atomicExch(&a.g->error, 1);
+          s_ok = 0;
+          break;
+        }
+        __nanosleep(32);
+      }
+      __threadfence();
+    }
+  }
+  __syncthreads();
+  return s_ok && !ld_volatile_i(&a.g->error);
 }
 
 template <typename Acc, bool REF>
-__global__ void __launch_bounds__(TILE_CELLS) k_pcg_seg(SegPcgArgs a) {
-  const int na = *a.n_active;
-  PcgState *st = a.st;
+__device__ __forceinline__ bool pcg_scene(const SegPcgArgs &a, const PcgJob &j) {
+  __shared__ double tot[3];
+  __shared__ float s_scal;   // alpha or beta of the running phase
+  __shared__ int s_flag;     // done / replacement pending
+  PcgState *S = a.st + j.scene;
   const int tid = threadIdx.x;
-  auto all = [](int) { return true; };
-  auto live = [&](int sc) { return !ld_volatile_i(&st[sc].done); };
-
-  // ---- init: r = b, z = M^-1 r; r.z and r.r per scene
-  for (int sl = blockIdx.x; sl < na; sl += gridDim.x) {
-    const int64_t q = (int64_t)sl * TILE_CELLS + tid;
-    const uint16_t code = a.code[q];
-    Acc v[2] = {0, 0};
-    if (code & CODE_FLUID) {
-      const float b = a.sign * a.bdiv[q];
-      const float diag = fmaxf((float)((code >> CODE_DIAG_SHIFT) & 7), 1.0f);
-      const float z = b / diag;
-      a.r[q] = b;
-      a.z[q] = z;
-      v[0] += (Acc)(b * z);
-      v[1] += (Acc)(b * b);
+  const int t_begin = __ldg(a.slot0 + j.scene) + j.rank, t_end = __ldg(a.slot0 + j.scene + 1);
+  const int step = SEG_TG * j.nb;
+  float *__restrict__ X = a.x;
+  float *__restrict__ R = a.r;
+  float *__restrict__ Z = a.z;
+  float *__restrict__ AD = a.Ad;
+  const uint16_t *__restrict__ CODE = a.code;
+  auto clear = [&]() {
+    if (tid < 3) tot[tid] = 0.0;
+    __syncthreads();
+  };
+  // Each phase walks the block's tiles SEG_TG at a time and issues every load
+  // of the group before any store, so the loads of the group's tiles are in
+  // flight together.
+  // ---- init: r = b, z = M^-1 r
+  clear();
+  {
+    Acc v[2] = {0, 0};  // this thread's sums over all the block's tiles
+    for (int base = t_begin; base < t_end; base += step) {
+      uint16_t cd[SEG_TG];
+      float bb[SEG_TG];
+#pragma unroll
+      for (int m = 0; m < SEG_TG; ++m) {
+        const int sl = base + m * j.nb;
+        const int64_t q = (int64_t)sl * TILE_CELLS + tid;
+        cd[m] = sl < t_end ? CODE[q] : (uint16_t)0;
+        bb[m] = (cd[m] & CODE_FLUID) ? a.bdiv[q] : 0.0f;
+      }
+#pragma unroll
+      for (int m = 0; m < SEG_TG; ++m) {
+        if (!(cd[m] & CODE_FLUID)) continue;
+        const int64_t q = (int64_t)(base + m * j.nb) * TILE_CELLS + tid;
+        const float b = a.sign * bb[m];
+        const float diag = fmaxf((float)((cd[m] >> CODE_DIAG_SHIFT) & 7), 1.0f);
+        const float z = b / diag;
+        R[q] = b;
+        Z[q] = z;
+        v[0] += (Acc)(b * z);
+        v[1] += (Acc)(b * b);
+      }
     }
-    tile_partials<Acc, 2>(a, sl, v);
+    block_acc<Acc, 2>(v, tot);
   }
-  if (!seg_reduce<Acc, 2>(a, all, [&](int sc, double *t) {
-        PcgState &S = st[sc];
-        S.rz = t[0]; S.r0 = t[1]; S.rr = t[1]; S.b2 = t[1];
-        S.r_upd2 = t[1]; S.r_true2 = t[1];
-        S.beta = 0.0; S.alpha = 0.0; S.iters = 0; S.n_replace = 0; S.status = GF_OK;
-        S.done = t[1] < 1e-30 ? 1 : 0;  // the reference's early exit (:2982-2986)
-        if (S.done) atomicAdd(&a.g->done, 1);
+  if (!scene_reduce<2>(a, j, tot, [&](double *t) {
+        S->rz = t[0]; S->r0 = t[1]; S->rr = t[1]; S->b2 = t[1];
+        S->r_upd2 = t[1]; S->r_true2 = t[1];
+        S->beta = 0.0; S->alpha = 0.0; S->iters = 0; S->n_replace = 0; S->status = GF_OK;
+        S->done = t[1] < 1e-30 ? 1 : 0;  // the reference's early exit (:2982-2986)
       }))
-    return;
+    return false;
 
   for (int it = 0; it < a.max_iter; ++it) {
-    if (ld_volatile_i(&a.g->done) >= a.nseg) break;
+    if (tid == 0) {
+      s_flag = ld_volatile_i(&S->done);
+      s_scal = (float)ld_volatile_d(&S->beta);
+    }
+    clear();
+    if (s_flag) break;
+    const float beta = s_scal;
     const float *__restrict__ dold = (it & 1) ? a.d1 : a.d0;
     float *__restrict__ dnew = (it & 1) ? a.d0 : a.d1;
     // ---- phase A: d = z + beta d ; Ad = A d ; d.Ad
-    for (int sl = blockIdx.x; sl < na; sl += gridDim.x) {
-      const int sc = slot_scene(a.slot0, a.nseg, sl);
-      if (ld_volatile_i(&st[sc].done)) continue;
-      const float beta = (float)ld_volatile_d(&st[sc].beta);
-      const int64_t q = (int64_t)sl * TILE_CELLS + tid;
-      const uint16_t code = a.code[q];
+    {
       Acc v[1] = {0};
-      if (code & CODE_FLUID) {
-        const float dn = __ldcg(a.z + q) + beta * __ldcg(dold + q);
-        float s = 0.0f;
+      for (int base = t_begin; base < t_end; base += step) {
+        uint16_t cd[SEG_TG];
+        float dn[SEG_TG], sn[SEG_TG];
 #pragma unroll
-        for (int d = 0; d < 6; ++d)
-          if (code & (1 << d)) {
-            const int64_t nq = nb_index(q, d, a.nbr);
-            s = s + (__ldcg(a.z + nq) + beta * __ldcg(dold + nq));
-          }
-        const float diag = (float)((code >> CODE_DIAG_SHIFT) & 7);
-        const float ad = diag * dn - s;
-        dnew[q] = dn;
-        a.Ad[q] = ad;
-        v[0] += (Acc)(dn * ad);
+        for (int m = 0; m < SEG_TG; ++m) {
+          const int sl = base + m * j.nb;
+          const int64_t q = (int64_t)sl * TILE_CELLS + tid;
+          cd[m] = sl < t_end ? CODE[q] : (uint16_t)0;
+        }
+#pragma unroll
+        for (int m = 0; m < SEG_TG; ++m) {
+          dn[m] = 0.0f;
+          sn[m] = 0.0f;
+          if (!(cd[m] & CODE_FLUID)) continue;
+          const int64_t q = (int64_t)(base + m * j.nb) * TILE_CELLS + tid;
+          dn[m] = __ldcg(Z + q) + beta * __ldcg(dold + q);
+          float s = 0.0f;
+#pragma unroll
+          for (int d = 0; d < 6; ++d)
+            if (cd[m] & (1 << d)) {
+              const int64_t nq = nb_index(q, d, a.nbr);
+              s = s + (__ldcg(Z + nq) + beta * __ldcg(dold + nq));
+            }
+          sn[m] = s;
+        }
+#pragma unroll
+        for (int m = 0; m < SEG_TG; ++m) {
+          if (!(cd[m] & CODE_FLUID)) continue;
+          const int64_t q = (int64_t)(base + m * j.nb) * TILE_CELLS + tid;
+          const float diag = (float)((cd[m] >> CODE_DIAG_SHIFT) & 7);
+          const float ad = diag * dn[m] - sn[m];
+          dnew[q] = dn[m];
+          AD[q] = ad;
+          v[0] += (Acc)(dn[m] * ad);
+        }
       }
-      tile_partials<Acc, 1>(a, sl, v);
+      block_acc<Acc, 1>(v, tot);
     }
-    if (!seg_reduce<Acc, 1>(a, live, [&](int sc, double *t) {
-          PcgState &S = st[sc];
+    if (!scene_reduce<1>(a, j, tot, [&](double *t) {
           const double pAp = t[0];
-          S.alpha = (Acc)fabs(pAp) < (Acc)1.0e-30 ? 0.0 : (double)((Acc)S.rz / (Acc)pAp);
+          S->alpha = (Acc)fabs(pAp) < (Acc)1.0e-30 ? 0.0 : (double)((Acc)S->rz / (Acc)pAp);
           if (!(pAp == pAp)) {
-            S.status = GF_NAN;
-            S.done = 1;
-            atomicAdd(&a.g->done, 1);
+            S->status = GF_NAN;
+            S->done = 1;
           }
         }))
-      return;
+      return false;
+    if (tid == 0) {
+      s_flag = ld_volatile_i(&S->done);
+      s_scal = (float)ld_volatile_d(&S->alpha);
+    }
+    clear();
+    if (s_flag) break;
     // ---- phase B: x += alpha d ; r -= alpha Ad ; z = M^-1 r ; r.z, r.r
-    for (int sl = blockIdx.x; sl < na; sl += gridDim.x) {
-      const int sc = slot_scene(a.slot0, a.nseg, sl);
-      if (ld_volatile_i(&st[sc].done)) continue;
-      const float alpha = (float)ld_volatile_d(&st[sc].alpha);
+    {
+      const float alpha = s_scal;
       const float nalpha = -alpha;
-      const int64_t q = (int64_t)sl * TILE_CELLS + tid;
-      const uint16_t code = a.code[q];
       Acc v[2] = {0, 0};
-      if (code & CODE_FLUID) {
-        const float dn = __ldcg(dnew + q);
-        a.x[q] = __ldcg(a.x + q) + alpha * dn;
-        const float rn = __ldcg(a.r + q) + nalpha * __ldcg(a.Ad + q);
-        const float diag = fmaxf((float)((code >> CODE_DIAG_SHIFT) & 7), 1.0f);
-        const float z = rn / diag;
-        a.r[q] = rn;
-        a.z[q] = z;
-        v[0] += (Acc)(rn * z);
-        v[1] += (Acc)(rn * rn);
+      for (int base = t_begin; base < t_end; base += step) {
+        uint16_t cd[SEG_TG];
+        float dd[SEG_TG], xx[SEG_TG], rr[SEG_TG], aa[SEG_TG];
+#pragma unroll
+        for (int m = 0; m < SEG_TG; ++m) {
+          const int sl = base + m * j.nb;
+          const int64_t q = (int64_t)sl * TILE_CELLS + tid;
+          cd[m] = sl < t_end ? CODE[q] : (uint16_t)0;
+        }
+#pragma unroll
+        for (int m = 0; m < SEG_TG; ++m) {
+          dd[m] = xx[m] = rr[m] = aa[m] = 0.0f;
+          if (!(cd[m] & CODE_FLUID)) continue;
+          const int64_t q = (int64_t)(base + m * j.nb) * TILE_CELLS + tid;
+          dd[m] = __ldcg(dnew + q);
+          xx[m] = __ldcg(X + q);
+          rr[m] = __ldcg(R + q);
+          aa[m] = __ldcg(AD + q);
+        }
+#pragma unroll
+        for (int m = 0; m < SEG_TG; ++m) {
+          if (!(cd[m] & CODE_FLUID)) continue;
+          const int64_t q = (int64_t)(base + m * j.nb) * TILE_CELLS + tid;
+          X[q] = xx[m] + alpha * dd[m];
+          const float rn = rr[m] + nalpha * aa[m];
+          const float diag = fmaxf((float)((cd[m] >> CODE_DIAG_SHIFT) & 7), 1.0f);
+          const float z = rn / diag;
+          R[q] = rn;
+          Z[q] = z;
+          v[0] += (Acc)(rn * z);
+          v[1] += (Acc)(rn * rn);
+        }
       }
-      tile_partials<Acc, 2>(a, sl, v);
+      block_acc<Acc, 2>(v, tot);
     }
     const int it1 = it + 1;
-    if (!seg_reduce<Acc, 2>(a, live, [&](int sc, double *t) {
-          PcgState &S = st[sc];
+    if (!scene_reduce<2>(a, j, tot, [&](double *t) {
           const double rz_new = t[0], rr = t[1];
-          S.iters = it1;
-          S.rr = rr;
+          S->iters = it1;
+          S->rr = rr;
           if (!(rr == rr)) {
-            S.status = GF_NAN;
-            S.done = 1;
-            atomicAdd(&a.g->done, 1);
+            S->status = GF_NAN;
+            S->done = 1;
             return;
           }
           int replace = 0;
           if (REF) {
-            replace = rr < a.replace2 * S.r_upd2 || rr < a.tol2 * S.b2;
+            replace = rr < a.replace2 * S->r_upd2 || rr < a.tol2 * S->b2;
           } else {
             const bool check = (it1 % a.check_every) == 0 || it1 == a.max_iter;
-            if (check && rr < a.tol2 * S.r0) {
-              S.done = 1;
-              atomicAdd(&a.g->done, 1);
-            }
+            if (check && rr < a.tol2 * S->r0) S->done = 1;
           }
           if (replace) {
-            S.n_replace = -S.n_replace - 1;  // negative: replacement pending
-            atomicAdd(&a.g->n_replace, 1);
+            S->n_replace = -S->n_replace - 1;  // negative: replacement pending
           } else {
-            const double rz = S.rz;
-            S.beta = (Acc)fabs(rz) < (Acc)1.0e-30 ? 0.0 : (double)((Acc)rz_new / (Acc)rz);
-            S.rz = rz_new;
+            const double rz = S->rz;
+            S->beta = (Acc)fabs(rz) < (Acc)1.0e-30 ? 0.0 : (double)((Acc)rz_new / (Acc)rz);
+            S->rz = rz_new;
           }
         }))
-      return;
-    // ---- refined: FP64 residual replacement r = b - A x for pending scenes
-    if (REF && ld_volatile_i(&a.g->n_replace) > 0) {
-      for (int sl = blockIdx.x; sl < na; sl += gridDim.x) {
-        const int sc = slot_scene(a.slot0, a.nseg, sl);
-        if (ld_volatile_i(&st[sc].n_replace) >= 0) continue;
-        const int64_t q = (int64_t)sl * TILE_CELLS + tid;
-        if (!(a.code[q] & CODE_FLUID)) continue;
-        a.x64[q] = __ldcg(a.x64 + q) + (double)__ldcg(a.x + q);
-        a.x[q] = 0.0f;
-      }
-      if (!seg_reduce<double, 1>(a, [](int) { return false; }, [](int, double *) {})) return;
-      for (int sl = blockIdx.x; sl < na; sl += gridDim.x) {
-        const int sc = slot_scene(a.slot0, a.nseg, sl);
-        if (ld_volatile_i(&st[sc].n_replace) >= 0) continue;
-        const int64_t q = (int64_t)sl * TILE_CELLS + tid;
-        const uint16_t code = a.code[q];
-        double v[3] = {0, 0, 0};
-        if (code & CODE_FLUID) {
-          double s = 0.0;
-#pragma unroll
-          for (int d = 0; d < 6; ++d)
-            if (code & (1 << d)) s += __ldcg(a.x64 + nb_index(q, d, a.nbr));
-          const double diag = (double)((code >> CODE_DIAG_SHIFT) & 7);
-          const double res = (double)(a.sign * a.bdiv[q]) - (diag * __ldcg(a.x64 + q) - s);
-          const float rf = (float)res;
-          const float z = rf / fmaxf((float)diag, 1.0f);
-          a.r[q] = rf;
-          a.z[q] = z;
-          v[0] += res * res;
-          v[1] += (double)(rf * z);
-          v[2] += (double)(rf * rf);
+      return false;
+    // ---- refined: FP64 residual replacement r = b - A x
+    if (REF) {
+      if (tid == 0) s_flag = ld_volatile_i(&S->n_replace) < 0;
+      clear();
+      if (s_flag) {
+        for (int sl = t_begin; sl < t_end; sl += j.nb) {
+          const int64_t q = (int64_t)sl * TILE_CELLS + tid;
+          if (!(CODE[q] & CODE_FLUID)) continue;
+          a.x64[q] = __ldcg(a.x64 + q) + (double)__ldcg(X + q);
+          X[q] = 0.0f;
         }
-        tile_partials<double, 3>(a, sl, v);
+        __syncthreads();
+        if (!scene_reduce<1>(a, j, tot, [](double *) {})) return false;  // x64 complete
+        double v[3] = {0, 0, 0};
+        for (int base = t_begin; base < t_end; base += step) {
+          uint16_t cd[SEG_TG];
+          double res[SEG_TG];
+#pragma unroll
+          for (int m = 0; m < SEG_TG; ++m) {
+            const int sl = base + m * j.nb;
+            const int64_t q = (int64_t)sl * TILE_CELLS + tid;
+            cd[m] = sl < t_end ? CODE[q] : (uint16_t)0;
+          }
+#pragma unroll
+          for (int m = 0; m < SEG_TG; ++m) {
+            res[m] = 0.0;
+            if (!(cd[m] & CODE_FLUID)) continue;
+            const int64_t q = (int64_t)(base + m * j.nb) * TILE_CELLS + tid;
+            double s = 0.0;
+#pragma unroll
+            for (int d = 0; d < 6; ++d)
+              if (cd[m] & (1 << d)) s += __ldcg(a.x64 + nb_index(q, d, a.nbr));
+            const double diag = (double)((cd[m] >> CODE_DIAG_SHIFT) & 7);
+            res[m] = (double)(a.sign * a.bdiv[q]) - (diag * __ldcg(a.x64 + q) - s);
+          }
+#pragma unroll
+          for (int m = 0; m < SEG_TG; ++m) {
+            if (!(cd[m] & CODE_FLUID)) continue;
+            const int64_t q = (int64_t)(base + m * j.nb) * TILE_CELLS + tid;
+            const float rf = (float)res[m];
+            const float diag = fmaxf((float)((cd[m] >> CODE_DIAG_SHIFT) & 7), 1.0f);
+            const float z = rf / diag;
+            R[q] = rf;
+            Z[q] = z;
+            v[0] += res[m] * res[m];
+            v[1] += (double)(rf * z);
+            v[2] += (double)(rf * rf);
+          }
+        }
+        block_acc<double, 3>(v, tot);
+        if (!scene_reduce<3>(a, j, tot, [&](double *t) {
+              S->r_true2 = t[0];
+              S->r_upd2 = t[2];
+              S->rr = t[2];
+              S->n_replace = -S->n_replace;  // back to a positive count (+1)
+              const double rz = S->rz;
+              S->beta = fabs(rz) < 1.0e-30 ? 0.0 : t[1] / rz;
+              S->rz = t[1];
+              if (t[0] <= a.tol2 * S->b2) S->done = 1;
+            }))
+          return false;
       }
-      if (!seg_reduce<double, 3>(
-              a, [&](int sc) { return ld_volatile_i(&st[sc].n_replace) < 0; },
-              [&](int sc, double *t) {
-                PcgState &S = st[sc];
-                S.r_true2 = t[0];
-                S.r_upd2 = t[2];
-                S.rr = t[2];
-                S.n_replace = -S.n_replace;  // back to a positive count (+1)
-                atomicSub(&a.g->n_replace, 1);
-                const double rz = S.rz;
-                S.beta = fabs(rz) < 1.0e-30 ? 0.0 : t[1] / rz;
-                S.rz = t[1];
-                if (t[0] <= a.tol2 * S.b2) {
-                  S.done = 1;
-                  atomicAdd(&a.g->done, 1);
-                }
-              }))
-        return;
     }
   }
-  if (blockIdx.x == 0)
-    for (int sc = tid; sc < a.nseg; sc += blockDim.x)
-      if (!ld_volatile_i(&st[sc].done)) st[sc].status = GF_NOT_CONVERGED;
+  if (tid == 0 && j.rank == 0 && !ld_volatile_i(&S->done)) S->status = GF_NOT_CONVERGED;
+  return true;
+}
+
+template <typename Acc, bool REF>
+__global__ void __launch_bounds__(TILE_CELLS, 2) k_pcg_seg(SegPcgArgs a) {
+  const int j0 = a.blk_job0[blockIdx.x], j1 = a.blk_job0[blockIdx.x + 1];
+  for (int jj = j0; jj < j1; ++jj) {
+    const PcgJob j = a.jobs[jj];
+    if (ld_volatile_i(&a.st[j.scene].done)) continue;  // no fluid
+    if (!pcg_scene<Acc, REF>(a, j)) return;
+  }
 }
 
 struct ScatterArgs {
@@ -930,7 +1077,9 @@ int pressure_alloc(Ctx *c) {
   for (int q = 0; q < 7; ++q)
     if ((e = A((void **)vecs[q], nk * 4, "alloc pressure vector"))) return e;
   if ((e = A((void **)&c->x64, nk * 8, "alloc x64"))) return e;
-  const int64_t np = c->ntiles > MAX_PCG_BLOCKS ? c->ntiles : MAX_PCG_BLOCKS;
+  // per-block partials of the PCGs; a batch's segmented PCG indexes them by
+  // job (at most one per scene plus one per block)
+  const int64_t np = (int64_t)c->ntiles + MAX_PCG_BLOCKS;
   if ((e = A((void **)&c->partials, 3 * np * sizeof(double), "alloc partials"))) return e;
   if ((e = A((void **)&c->state, sizeof(PcgState), "alloc pcg state"))) return e;
   if ((e = A((void **)&c->bar_counters, 8 * 16 * 8, "alloc barrier counters"))) return e;
@@ -987,14 +1136,23 @@ static int launch_pcg_seg(Ctx *c, SegPcgArgs &pa) {
     return fail(c, GF_CUDA_ERROR, "segmented PCG: cooperative occupancy query failed");
   if (c->tune.pcg_blocks_per_sm > 0 && c->tune.pcg_blocks_per_sm < per_sm)
     per_sm = c->tune.pcg_blocks_per_sm;
+  int grid = per_sm * c->num_sms;
+  if (grid > MAX_PCG_BLOCKS) grid = MAX_PCG_BLOCKS;
+  k_pcg_plan<<<1, 32, 0, c->stream>>>(c->seg_slot0, c->nseg, grid, c->seg_state,
+                                      c->pcg_blk_job0, reinterpret_cast<PcgJob *>(c->pcg_jobs));
+  c->launches++;
+  pa.blk_job0 = c->pcg_blk_job0;
+  pa.jobs = reinterpret_cast<const PcgJob *>(c->pcg_jobs);
   void *args[] = {&pa};
-  int e = check_cuda(c, cudaLaunchCooperativeKernel((const void *)k_pcg_seg<Acc, REF>,
-                                                    dim3(per_sm * c->num_sms), dim3(TILE_CELLS),
-                                                    args, 0, c->stream),
+  int e = check_cuda(c, cudaLaunchCooperativeKernel((const void *)k_pcg_seg<Acc, REF>, dim3(grid),
+                                                    dim3(TILE_CELLS), args, 0, c->stream),
                      "cooperative segmented PCG launch");
   c->launches++;
   return e;
 }
+
+// Bytes of the job table of a batch with nseg scenes.
+size_t pcg_jobs_bytes(int nseg) { return (size_t)(nseg + MAX_PCG_BLOCKS) * sizeof(PcgJob); }
 
 // The pressure stage of a batch: set-up over every scene's tiles, then the
 // sweeps (scene-agnostic on the compact layout) or the segmented PCG.
@@ -1044,16 +1202,14 @@ static int launch_pressure_batch(Ctx *c, const gf_step_params *prm) {
     c->launches += 2 * prm->max_iters;
     c->last_iters = prm->max_iters;
   } else {
-    if ((e = check_cuda(c, cudaMemsetAsync(c->state, 0, sizeof(PcgState), st), "zero state")) ||
-        (e = check_cuda(c, cudaMemsetAsync(c->seg_state, 0, c->nseg * sizeof(PcgState), st),
-                        "zero scene states")))
+    if ((e = check_cuda(c, cudaMemsetAsync(c->state, 0, sizeof(PcgState), st), "zero state")))
       return e;
     const int check_every = prm->check_every > 0 ? prm->check_every : 1;
     const float sign = prm->rhs_sign >= 0 ? 1.0f : -1.0f;
     SegPcgArgs pa{c->n_active, c->tile_nbr, c->seg_slot0, c->nseg, c->code, c->bdiv, c->xf,
                   c->r, c->z, c->d0, c->d1, c->Ad, refined ? c->x64 : nullptr, c->partials,
-                  c->ntiles > MAX_PCG_BLOCKS ? c->ntiles : MAX_PCG_BLOCKS, c->seg_state,
-                  c->state, prm->max_iters, check_every, prm->tol * prm->tol, 1e-4, sign};
+                  (int64_t)c->ntiles + MAX_PCG_BLOCKS, c->seg_state, c->state, nullptr,
+                  nullptr, prm->max_iters, check_every, prm->tol * prm->tol, 1e-4, sign};
     if (refined) {
       e = launch_pcg_seg<double, true>(c, pa);
       result64 = c->x64;
