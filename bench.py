@@ -326,6 +326,87 @@ def batched_leg(torch, device, k_steps=10, warm=2, n_scenes=64):
             "autotune": tune}
 
 
+def stage_bytes_flip(P, ncell_active, F):
+    """Algorithmic bytes of the FLIP (non-APIC) stages: sort 64P + 12N,
+    P2G 24P + 24F (the zeroing of the six P2G face arrays counted as for
+    APIC), forces/div 8F + 5N, project 8F + 5N, G2P 48P + 8F."""
+    N = ncell_active
+    return {"bin_sort": 64 * P + 12 * N, "p2g": 24 * P + 24 * F,
+            "forces_div": 8 * F + 5 * N, "project": 8 * F + 5 * N, "g2p": 48 * P + 8 * F}
+
+
+def extra_legs(torch, device, steps=3):
+    """The other single-scene workloads, a few timed substeps each:
+    64^3 FLIP dam break (box [0,.4]x[0,.6]x[0,1]), dt 1/240, Jacobi-PCG to
+    1e-5 with at most 200 iterations; 256^3 double dam break (x in [0,.3] and
+    [.7,1], y in [0,.7]), FLIP 0.97, dt 1/960, refined PCG to 1e-7 (the
+    global-memory solver: the active region exceeds the shared-memory one)
+    and 200 Jacobi sweeps as the plain comparison, with per-stage times and
+    the device memory footprint."""
+    import gpufluid_b200 as gf
+    stream = torch.cuda.current_stream()
+    out = {}
+
+    def timed(s, dt, iters, solver, k):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(k):
+            s.step(dt, pressure_iters=iters, pressure_solver=solver)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k
+
+    s = gf.FlipSolver3D(64, 64, 64, flip_blend=0.95, pressure_tol=1e-5, device=device,
+                        enable_cuda_graphs=True)
+    s.seed_box((0.0, 0.0, 0.0), (0.4, 0.6, 1.0))
+    for _ in range(3):
+        s.step(1 / 240, pressure_iters=200, pressure_solver="pcg")
+    ms = timed(s, 1 / 240, 200, "pcg", 20)
+    out["dam_break_64_flip_pcg1e-5"] = {
+        "particles": s.n_particles, "ms_per_substep": round(ms, 4),
+        "substeps_per_s": round(1000 / ms, 2), "pcg_iters_last": s.last_pressure_iters}
+    del s
+    torch.cuda.empty_cache()
+    free0, _ = torch.cuda.mem_get_info()
+    s = gf.FlipSolver3D(256, 256, 256, flip_blend=0.97, pressure_tol=1e-7, device=device)
+    s.seed_box((0.0, 0.0, 0.0), (0.3, 0.7, 1.0))
+    s.seed_box((0.7, 0.0, 0.0), (1.0, 0.7, 1.0), append=True)
+    dt = 1 / 960
+    s.step(dt, pressure_iters=4000, pressure_solver="pcg_refined")
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    ms_ref = timed(s, dt, 4000, "pcg_refined", steps)
+    st_ref = s.pressure_stats()
+    ms_jac = timed(s, dt, 200, "jacobi", steps)
+    s._prof.enabled = True
+    s._L.gf_enable_timing(s._ctx, 1)
+    s.step(dt, pressure_iters=4000, pressure_solver="pcg_refined")
+    t = s.stage_times()
+    s._L.gf_enable_timing(s._ctx, 0)
+    s._prof.enabled = False
+    P = s.n_particles
+    F = (256 + 1) * 256 * 256 * 3
+    sb = stage_bytes_flip(P, st_ref["n_active_tiles"] * 512, F)
+    gbs = {k: round(sb[k] / 1e9 / (t[i] / 1e3), 1)
+           for i, k in ((0, "bin_sort"), (1, "p2g"), (2, "forces_div"), (4, "project"),
+                        (5, "g2p"))}
+    out["double_dam_break_256"] = {
+        "particles": P, "refined_pcg1e-7_ms_per_substep": round(ms_ref, 3),
+        "refined_substeps_per_s": round(1000 / ms_ref, 3),
+        "refined_iters_last": st_ref["iters"],
+        "pcg_kernel": "global-memory" if st_ref["kernel"] == 2 else "shared-memory",
+        "jacobi200_ms_per_substep": round(ms_jac, 3),
+        "jacobi200_substeps_per_s": round(1000 / ms_jac, 3),
+        "stages_ms": {k: round(float(t[i]), 4) for i, k in enumerate(
+            ("bin_sort", "p2g", "forces_div", "pressure", "project", "g2p", "total"))},
+        "stages_gbs": gbs,
+        "device_footprint_gb": round((free0 - free1) / 1e9, 2)}
+    del s
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -434,6 +515,7 @@ def run_ours(args):
 
     fwd_adj = None if args.no_adjoint else adjoint_leg(torch, device)
     batched = None if args.no_batched else batched_leg(torch, device)
+    extra = None if args.no_extra else extra_legs(torch, device)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -480,6 +562,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "fwd_adj": fwd_adj,
             "batched": batched,
+            "other_configs": extra,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -551,6 +634,8 @@ def main():
                     help="skip the forward+adjoint rollout timing")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched uneven-scenes timing")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the 64^3 and 256^3 single-scene timings")
     ap.add_argument("--grid", type=int, default=128,
                     help="grid side (smaller sides are for profiling captures only)")
     args = ap.parse_args()

@@ -430,6 +430,12 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const int64_t q0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   PcgState *st = a.st;
+  constexpr int KQ = 4;
+  float *__restrict__ X = a.x;
+  float *__restrict__ R = a.r;
+  float *__restrict__ Z = a.z;
+  float *__restrict__ AD = a.Ad;
+  const uint16_t *__restrict__ CODE = a.code;
 
   // ---- init: x = 0, r = b, z = M^-1 r, d = 0 (so the first d = z)
   {
@@ -468,24 +474,43 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
     const float *__restrict__ dold = (it & 1) ? a.d1 : a.d0;
     float *__restrict__ dnew = (it & 1) ? a.d0 : a.d1;
     // ---- phase A: d = z + beta d ; Ad = A d ; p.Ap
+    // (KQ cells per thread per step: every load of the step is issued before
+    // its stores, so the step's loads are in flight together)
     {
       Acc v[1] = {0};
-      for (int64_t q = q0; q < total; q += stride) {
-        const uint16_t code = a.code[q];
-        if (!(code & CODE_FLUID)) continue;
-        const float dn = __ldcg(a.z + q) + beta * __ldcg(dold + q);
-        float s = 0.0f;
+      for (int64_t qb = q0; qb < total; qb += KQ * stride) {
+        uint16_t cd[KQ];
+        float dn[KQ], sn[KQ];
 #pragma unroll
-        for (int d = 0; d < 6; ++d)
-          if (code & (1 << d)) {
-            const int64_t nq = nb_index(q, d, a.nbr);
-            s = s + (__ldcg(a.z + nq) + beta * __ldcg(dold + nq));
-          }
-        const float diag = (float)((code >> CODE_DIAG_SHIFT) & 7);
-        const float ad = diag * dn - s;
-        dnew[q] = dn;
-        a.Ad[q] = ad;
-        v[0] += (Acc)(dn * ad);
+        for (int m = 0; m < KQ; ++m) {
+          const int64_t q = qb + m * stride;
+          cd[m] = q < total ? CODE[q] : (uint16_t)0;
+        }
+#pragma unroll
+        for (int m = 0; m < KQ; ++m) {
+          dn[m] = sn[m] = 0.0f;
+          if (!(cd[m] & CODE_FLUID)) continue;
+          const int64_t q = qb + m * stride;
+          dn[m] = __ldcg(Z + q) + beta * __ldcg(dold + q);
+          float s = 0.0f;
+#pragma unroll
+          for (int d = 0; d < 6; ++d)
+            if (cd[m] & (1 << d)) {
+              const int64_t nq = nb_index(q, d, a.nbr);
+              s = s + (__ldcg(Z + nq) + beta * __ldcg(dold + nq));
+            }
+          sn[m] = s;
+        }
+#pragma unroll
+        for (int m = 0; m < KQ; ++m) {
+          if (!(cd[m] & CODE_FLUID)) continue;
+          const int64_t q = qb + m * stride;
+          const float diag = (float)((cd[m] >> CODE_DIAG_SHIFT) & 7);
+          const float ad = diag * dn[m] - sn[m];
+          dnew[q] = dn[m];
+          AD[q] = ad;
+          v[0] += (Acc)(dn[m] * ad);
+        }
       }
       if (!grid_reduce<Acc, 1>(a, v, [&](double *t) {
             const double pAp = t[0];
@@ -503,18 +528,37 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
       const float alpha = (float)ld_volatile_d(&st->alpha);
       const float nalpha = -alpha;
       Acc v[2] = {0, 0};
-      for (int64_t q = q0; q < total; q += stride) {
-        const uint16_t code = a.code[q];
-        if (!(code & CODE_FLUID)) continue;
-        const float dn = __ldcg(dnew + q);
-        a.x[q] = __ldcg(a.x + q) + alpha * dn;
-        const float rn = __ldcg(a.r + q) + nalpha * __ldcg(a.Ad + q);
-        const float diag = fmaxf((float)((code >> CODE_DIAG_SHIFT) & 7), 1.0f);
-        const float z = rn / diag;
-        a.r[q] = rn;
-        a.z[q] = z;
-        v[0] += (Acc)(rn * z);
-        v[1] += (Acc)(rn * rn);
+      for (int64_t qb = q0; qb < total; qb += KQ * stride) {
+        uint16_t cd[KQ];
+        float dd[KQ], xx[KQ], rr[KQ], aa[KQ];
+#pragma unroll
+        for (int m = 0; m < KQ; ++m) {
+          const int64_t q = qb + m * stride;
+          cd[m] = q < total ? CODE[q] : (uint16_t)0;
+        }
+#pragma unroll
+        for (int m = 0; m < KQ; ++m) {
+          dd[m] = xx[m] = rr[m] = aa[m] = 0.0f;
+          if (!(cd[m] & CODE_FLUID)) continue;
+          const int64_t q = qb + m * stride;
+          dd[m] = __ldcg(dnew + q);
+          xx[m] = __ldcg(X + q);
+          rr[m] = __ldcg(R + q);
+          aa[m] = __ldcg(AD + q);
+        }
+#pragma unroll
+        for (int m = 0; m < KQ; ++m) {
+          if (!(cd[m] & CODE_FLUID)) continue;
+          const int64_t q = qb + m * stride;
+          X[q] = xx[m] + alpha * dd[m];
+          const float rn = rr[m] + nalpha * aa[m];
+          const float diag = fmaxf((float)((cd[m] >> CODE_DIAG_SHIFT) & 7), 1.0f);
+          const float z = rn / diag;
+          R[q] = rn;
+          Z[q] = z;
+          v[0] += (Acc)(rn * z);
+          v[1] += (Acc)(rn * rn);
+        }
       }
       const int it1 = it + 1;
       if (!grid_reduce<Acc, 2>(a, v, [&](double *t) {
