@@ -141,6 +141,7 @@ struct Ctx {
   // pressure workspace (compact active tiles)
   int32_t *tile_slot = nullptr;  // [ntiles] slot or -1
   int32_t *tile_list = nullptr;  // [ntiles] tile id of each slot
+  int32_t *tile_order = nullptr; // [ntiles] Morton order of the tile ids (single grid)
   int32_t *tile_nbr = nullptr;   // [ntiles*6] neighbour slot or -1
   int32_t *n_active = nullptr;   // [0] active tiles, [1..2] fluid-cell count (int64)
   uint16_t *code = nullptr;      // [nkeys]

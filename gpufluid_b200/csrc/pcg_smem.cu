@@ -640,9 +640,22 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
     a.xf[q0 + L] = s_x[L];
     if (REF) a.x64[q0 + L] = s_x64[L];
   }
-  if (gs.trace && threadIdx.x == 0) {  // per-block busy cycles and tile counts
-    gs.trace[a.trace_cap / 2 + 2 * blockIdx.x] = gs.busy;
-    gs.trace[a.trace_cap / 2 + 2 * blockIdx.x + 1] = nt;
+  if (gs.trace) {  // per block: busy cycles, tiles, fluid cells, remote faces
+    __shared__ int s_nf;
+    if (threadIdx.x == 0) s_nf = 0;
+    __syncthreads();
+    atomicAdd(&s_nf, __popc(fmask));
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int remote = 0;
+      for (int f = 0; f < nt * 6; ++f)
+        if (s_nbr[f] >= 0 && !(s_nbr[f] >= b0 && s_nbr[f] < b1)) ++remote;
+      long long *t = gs.trace + a.trace_cap / 2 + 4 * blockIdx.x;
+      t[0] = gs.busy;
+      t[1] = nt;
+      t[2] = s_nf;
+      t[3] = remote;
+    }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     st->trace_n = gs.trace_n;

@@ -3,7 +3,7 @@
 // Set-up (once per solve):
 //   k_tile_flags    tile active iff it holds a fluid cell (k_mark_active_blocks,
 //                   solver3d.py:953-972)
-//   k_tile_compact  ascending slot numbering of active tiles (the reference's
+//   k_tile_compact  slot numbering of active tiles along a Morton curve (the reference's
 //                   array_scan + k_compact_active_blocks, :1056-1082)
 //   k_tile_setup    neighbour-tile table, per-cell 16-bit stencil code
 //                   (fluid-neighbour mask + #non-solid neighbours), compact rhs
@@ -23,6 +23,10 @@
 //
 // Every spin-wait (grid barrier) is bounded; on timeout the kernel records
 // GF_TIMEOUT in the solve state and all blocks return.
+#include <algorithm>
+#include <utility>
+#include <vector>
+
 #include "gf_internal.cuh"
 
 namespace gf {
@@ -51,17 +55,22 @@ __global__ void k_tile_flags(const uint8_t *__restrict__ label, int nx, int ny, 
   if (lane == 0) flag[warp] = any;
 }
 
+// Slots follow `order` (a permutation of the tile ids; identity when NULL):
+// the single-grid solvers number active tiles along a Morton curve, so that
+// contiguous slot runs -- the units the PCG blocks own -- are compact 3-D
+// clusters with few faces on another block's tiles.
 __global__ void k_tile_compact(const int32_t *__restrict__ flag, int ntiles,
-                               int32_t *__restrict__ slot, int32_t *__restrict__ list,
-                               int32_t *__restrict__ n_active) {
+                               const int32_t *__restrict__ order, int32_t *__restrict__ slot,
+                               int32_t *__restrict__ list, int32_t *__restrict__ n_active) {
   __shared__ int warp_sums[32];
   __shared__ int carry;
   if (threadIdx.x == 0) carry = 0;
   __syncthreads();
   const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int off = 0; off < ntiles; off += blockDim.x) {
-    int t = off + threadIdx.x;
-    int f = t < ntiles ? flag[t] : 0;
+    const int i = off + threadIdx.x;
+    const int t = i < ntiles ? (order ? order[i] : i) : ntiles;
+    int f = i < ntiles ? flag[t] : 0;
     int incl = f;
     for (int o = 1; o < 32; o <<= 1) {
       int v = __shfl_up_sync(0xffffffffu, incl, o);
@@ -79,7 +88,7 @@ __global__ void k_tile_compact(const int32_t *__restrict__ flag, int ntiles,
     }
     __syncthreads();
     int pre = carry + warp_sums[wid] + incl - f;
-    if (t < ntiles) {
+    if (i < ntiles) {
       slot[t] = f ? pre : -1;
       if (f) list[pre] = t;
     }
@@ -1114,6 +1123,25 @@ int pressure_alloc(Ctx *c) {
   int e;
   if ((e = A((void **)&c->tile_slot, c->ntiles * 4, "alloc tile_slot"))) return e;
   if ((e = A((void **)&c->tile_list, c->ntiles * 4, "alloc tile_list"))) return e;
+  if (c->nseg == 0) {  // Morton order of the tile grid for the slot numbering
+    std::vector<std::pair<uint64_t, int32_t>> key(c->ntiles);
+    auto spread = [](uint64_t v) {  // bits of v at every third position
+      uint64_t r = 0;
+      for (int b = 0; b < 21; ++b) r |= ((v >> b) & 1ull) << (3 * b);
+      return r;
+    };
+    for (int t = 0; t < c->ntiles; ++t) {
+      const int ti = t / (c->nty * c->ntz), tj = (t / c->ntz) % c->nty, tk = t % c->ntz;
+      key[t] = {(spread(ti) << 2) | (spread(tj) << 1) | spread(tk), t};
+    }
+    std::sort(key.begin(), key.end());
+    std::vector<int32_t> ord(c->ntiles);
+    for (int t = 0; t < c->ntiles; ++t) ord[t] = key[t].second;
+    if ((e = A((void **)&c->tile_order, c->ntiles * 4, "alloc tile_order"))) return e;
+    if ((e = check_cuda(c, cudaMemcpy(c->tile_order, ord.data(), c->ntiles * 4,
+                                      cudaMemcpyHostToDevice), "upload tile_order")))
+      return e;
+  }
   if ((e = A((void **)&c->tile_nbr, (size_t)c->ntiles * 6 * 4, "alloc tile_nbr"))) return e;
   if ((e = A((void **)&c->n_active, 16, "alloc n_active"))) return e;
   if ((e = A((void **)&c->code, nk * 2, "alloc code"))) return e;
@@ -1139,7 +1167,7 @@ int pressure_alloc(Ctx *c) {
 }
 
 void pressure_free(Ctx *c) {
-  void *ps[] = {c->tile_slot, c->tile_list, c->tile_nbr, c->n_active, c->code, c->bdiv,
+  void *ps[] = {c->tile_slot, c->tile_list, c->tile_order, c->tile_nbr, c->n_active, c->code, c->bdiv,
                 c->xf, c->r, c->z, c->d0, c->d1, c->Ad, c->x64, c->partials, c->state,
                 c->bar_counters, c->trace, c->halo, c->tile_cost};
   for (void *p : ps)
@@ -1208,7 +1236,8 @@ static int launch_pressure_batch(Ctx *c, const gf_step_params *prm) {
   int32_t *flag = c->tile_nbr;  // consumed by the compaction before the set-up
   kb_tile_flags<<<(unsigned)((c->ntiles * 32 + 255) / 256), 256, 0, st>>>(c->f.label, sx,
                                                                           c->ntiles, flag);
-  k_tile_compact<<<1, 1024, 0, st>>>(flag, c->ntiles, c->tile_slot, c->tile_list, c->n_active);
+  k_tile_compact<<<1, 1024, 0, st>>>(flag, c->ntiles, nullptr, c->tile_slot, c->tile_list,
+                                     c->n_active);
   kb_slot_ranges<<<(unsigned)((c->nseg + 256) / 256), 256, 0, st>>>(c->tile_list, c->n_active,
                                                                     sx, c->seg_slot0);
   c->launches += 3;
@@ -1288,7 +1317,7 @@ int launch_pressure(Ctx *c, const gf_step_params *prm) {
     unsigned g = (unsigned)((c->ntiles * 32 + 255) / 256);
     k_tile_flags<<<g, 256, 0, st>>>(c->f.label, c->nx, c->ny, c->nz, c->nty, c->ntz,
                                     c->ntiles, flag);
-    k_tile_compact<<<1, 1024, 0, st>>>(flag, c->ntiles, c->tile_slot, c->tile_list,
+    k_tile_compact<<<1, 1024, 0, st>>>(flag, c->ntiles, c->tile_order, c->tile_slot, c->tile_list,
                                        c->n_active);
     c->launches += 2;
   }
