@@ -42,6 +42,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = ("FLIP substeps/s @128³ (refined vs plain FP32 PCG, same residual); fwd+adj/s")
+# DRAM bytes (read + write) of one launch of the shared-memory PCG on this
+# workload, from an ncu capture: 7,125,504 read + 1,236,736 written.  The
+# solve's vectors stay in shared memory; only halos and the FP64 replacement
+# steps touch DRAM, far below the algorithmic bytes of a streaming PCG.
+PCG_DRAM_BYTES = 7125504 + 1236736
 GRID = 128
 DT = 1.0 / 480.0
 TOL = 1e-8
@@ -550,7 +555,10 @@ def run_ours(args):
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": "k_pcg<double,true> (persistent cooperative)",
                          "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-                         "frac": round(achieved / hbm, 4), "traffic": None,
+                         "frac": round(achieved / hbm, 4), "traffic": PCG_DRAM_BYTES,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
+                                           "one launch of this workload "
+                                           "(profiles/p2g_g2p_pcg_128_apic_full.md)",
                          "peak_source": peak_kind,
                          "bytes_per_launch": round(float(np.mean(pcg_b)), 0),
                          "ms_per_launch": round(float(np.mean(pcg_ms)), 4)},
