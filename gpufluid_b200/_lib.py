@@ -112,6 +112,8 @@ _SIGS = {
     "gf_record_bytes": ([_vp, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
     "gf_step_record": ([_vp, ctypes.POINTER(StepParams), _vp], ctypes.c_int),
     "gf_step_adjoint": ([_vp, ctypes.POINTER(StepParams), _vp, _vp, _vp, _vp, _vp], ctypes.c_int),
+    "gf_step_adjoint_apic": ([_vp, ctypes.POINTER(StepParams), _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+                             ctypes.c_int),
     "gf_density_splat": ([_vp, _vp, ctypes.c_int64, _vp], ctypes.c_int),
     "gf_density_splat_adjoint": ([_vp, _vp, ctypes.c_int64, _vp, _vp], ctypes.c_int),
     "gf_sample_cells": ([_vp, _vp, _vp, ctypes.c_int64, _vp], ctypes.c_int),

@@ -10,7 +10,9 @@ between.
 The drop-shaping problem (``DropShaping``):
 
 * fluid: a sphere seeded with the jittered lattice in every cell whose centre
-  lies inside it (8 per cell), PIC transfer (flip_blend 0), no reseeding;
+  lies inside it (8 per cell), PIC (flip_blend 0) or APIC transfer, no
+  reseeding; under APIC the affine matrices start at zero and their adjoint is
+  carried through the substeps beside those of positions and velocities;
 * control: a cell-centred 3-component velocity field U (3, nx, ny, nz); each
   particle starts with the trilinearly sampled velocity v_p = sum_c N_pc U_c;
 * loss: L = sum_c (rho_c(x_T) - rho*_c)^2 with rho the cell-centred
@@ -54,10 +56,13 @@ class DropShaping:
 
     def __init__(self, n=64, T=40, dt=1.0 / 240.0, k=10, center=(0.5, 0.35, 0.5), radius=0.15,
                  shift=(0.15, 0.1, 0.0), sigma=1.5, ppc=8, device="cuda",
-                 pressure_solver="pcg_refined", tol=1e-9, max_iters=4000):
+                 pressure_solver="pcg_refined", tol=1e-9, max_iters=4000, transfer="pic"):
+        if transfer not in ("pic", "apic"):
+            raise ValueError("the adjoint substep supports transfer 'pic' and 'apic'")
         self.n, self.T, self.dt, self.k = n, T, dt, k
+        self.transfer = transfer
         self.device = torch.device(device)
-        self.solver = FlipSolver3D(n, n, n, transfer_mode="pic", flip_blend=0.0,
+        self.solver = FlipSolver3D(n, n, n, transfer_mode=transfer, flip_blend=0.0,
                                    pressure_tol=tol, device=device)
         s = self.solver
         x0 = _scene.seed_sphere_positions(n, n, n, s.dx, center, radius, ppc)
@@ -95,11 +100,15 @@ class DropShaping:
                 vel.data_ptr())
         return vel
 
-    def _load(self, pos, vel, pid):
+    def _load(self, pos, vel, pid, C=None):
         s = self.solver
         s._pos.copy_(pos)
         s._vel.copy_(vel)
         s._pid.copy_(pid)
+        if C is None:
+            s._C.zero_()
+        else:
+            s._C.copy_(C)
 
     # ------------------------------------------------------------- forward
     def forward(self, control: torch.Tensor, keep_labels: bool = False):
@@ -112,7 +121,7 @@ class DropShaping:
         labels = [] if keep_labels else None
         for t in range(self.T):
             if t % self.k == 0:
-                ckpts.append((s._pos.clone(), s._vel.clone(), s._pid.clone()))
+                ckpts.append((s._pos.clone(), s._vel.clone(), s._pid.clone(), s._C.clone()))
             self._c("gf_step", ctypes.byref(self.prm))
             if keep_labels:
                 labels.append(s._label.clone())
@@ -127,11 +136,14 @@ class DropShaping:
         s = self.solver
         P, dev = self.P, self.device
         control = control.detach().to(dev, torch.float32).contiguous()
+        apic = self.transfer == "apic"
         xbar = torch.zeros((P, 3), dtype=torch.float32, device=dev)
         vbar = torch.zeros_like(xbar)
         xin = torch.empty_like(xbar)
         vin = torch.empty_like(xbar)
-        carry_x = carry_v = None  # adjoint by particle id across segments
+        Cbar = torch.zeros((P, 9), dtype=torch.float32, device=dev)
+        Cin = torch.empty_like(Cbar)
+        carry_x = carry_v = carry_C = None  # adjoint by particle id across segments
         nseg = len(ckpts)
         for seg in reversed(range(nseg)):
             t0 = seg * self.k
@@ -145,22 +157,34 @@ class DropShaping:
                 self._c("gf_density_splat_adjoint", s._pos.data_ptr(), P, rho_bar.data_ptr(),
                         xbar.data_ptr())
                 vbar.zero_()
+                Cbar.zero_()
             else:  # bring the id-ordered adjoint into this recomputation's slot order
                 idx = s._pid.long()
                 xbar.copy_(carry_x[idx])
                 vbar.copy_(carry_v[idx])
+                Cbar.copy_(carry_C[idx])
             for i in reversed(range(steps)):
-                self._c("gf_step_adjoint", ctypes.byref(self.prm), self.records[i].data_ptr(),
-                        xbar.data_ptr(), vbar.data_ptr(), xin.data_ptr(), vin.data_ptr())
+                if apic:
+                    self._c("gf_step_adjoint_apic", ctypes.byref(self.prm),
+                            self.records[i].data_ptr(), xbar.data_ptr(), vbar.data_ptr(),
+                            Cbar.data_ptr(), xin.data_ptr(), vin.data_ptr(), Cin.data_ptr())
+                    Cbar, Cin = Cin, Cbar
+                else:
+                    self._c("gf_step_adjoint", ctypes.byref(self.prm),
+                            self.records[i].data_ptr(), xbar.data_ptr(), vbar.data_ptr(),
+                            xin.data_ptr(), vin.data_ptr())
                 xbar, xin = xin, xbar
                 vbar, vin = vin, vbar
-            # xbar, vbar are now in the storage order of checkpoint seg
+            # xbar, vbar (, Cbar) are now in the storage order of checkpoint seg
             idx = ckpts[seg][2].long()
             carry_x = torch.empty_like(xbar)
             carry_v = torch.empty_like(vbar)
+            carry_C = torch.empty_like(Cbar)
             carry_x[idx] = xbar
             carry_v[idx] = vbar
+            carry_C[idx] = Cbar
         # checkpoint 0 holds the particles in id order: carry is v(0)'s adjoint
+        # (C(0) = 0 does not depend on the control)
         grad = torch.empty((3,) + (self.n,) * 3, dtype=torch.float32, device=dev)
         self._c("gf_sample_cells_adjoint", self.x0.data_ptr(), P, carry_v.data_ptr(),
                 grad.data_ptr())

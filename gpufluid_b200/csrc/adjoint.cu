@@ -22,7 +22,10 @@
 namespace gf {
 
 struct AdjArgs {
-  const float4 *rec0, *rec1;  // sorted inputs of the substep: (x,y,z,pid), (vx,vy,vz,-)
+  const float4 *rec0, *rec1;  // sorted inputs of the substep: (x,y,z,pid), (vx,vy,vz,C00)
+  const float4 *rec2, *rec3;  // APIC: (C01,C02,C10,C11), (C12,C20,C21,C22)
+  const float *Cbar_out;      // APIC: (n,9) adjoint of the output C, sorted order
+  float *Cbar_in;             // APIC: (n,9) adjoint of the input C, storage order
   const int32_t *order;       // storage slot (input order) of each sorted position
   const float *m[3];          // P2G weight sums per component
   const float *un[3];         // normalised P2G velocities (pre-force)
@@ -283,6 +286,164 @@ __global__ void k_adj_p2g(AdjArgs a) {
   }
 }
 
+// ---- APIC adjoint --------------------------------------------------------
+// Forward (k3_p2g_apic :1475-1588, k3_g2p_apic_advect :1591-1732), per
+// component c with face offsets o_f = x_f - x_p:
+//   P2G   q_f = sum_p W_pf (v_pc + C_p[c] . o_f),  m_f = sum_p W_pf
+//   G2P   v'_pc = sum_f S_pf u3_f,  C'_p[c][d] = inv sum_f S_pf u3_f o_fd
+//         (S: clamped corner indices, unclamped weights; inv = 3 / dx^2)
+// Adjoint: g_f = vb_c + inv (o_f . Cbar'[c]) carries both outputs back,
+//   ubar3_f += S_pf g_f;  xbar += dS/dx u3_f g_f - inv (sum_f S_pf u3_f) Cbar'[c]
+//   P2G: vbar_c += sum W qbar,  Cbar[c] += sum W qbar o_f,
+//        xbar += dW/dx (val qbar + mbar) - (sum W qbar) C[c].
+
+// Corners of the APIC gather: indices clamped into the grid, weights from
+// s = f - floor(f) unclamped (so d/df is never gated).
+__device__ __forceinline__ void apic_corners(float fx, float fy, float fz, int snx, int sny,
+                                             int snz, int ax, float dx, float inv_dx, float px,
+                                             float py, float pz, Corners &c, float (&o)[8][3]) {
+  const int i0 = __float2int_rz(floorf(fx)), j0 = __float2int_rz(floorf(fy)),
+            k0 = __float2int_rz(floorf(fz));
+  const float sx = fx - (float)i0, sy = fy - (float)j0, sz = fz - (float)k0;
+  const float wx[2] = {1.0f - sx, sx}, wy[2] = {1.0f - sy, sy}, wz[2] = {1.0f - sz, sz};
+  const float sgn[2] = {-1.0f, 1.0f};
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int q = (a * 2 + b) * 2 + e;
+        int ii = i0 + a, jj = j0 + b, kk = k0 + e;
+        ii = ii < 0 ? 0 : (ii > snx - 1 ? snx - 1 : ii);
+        jj = jj < 0 ? 0 : (jj > sny - 1 ? sny - 1 : jj);
+        kk = kk < 0 ? 0 : (kk > snz - 1 ? snz - 1 : kk);
+        c.idx[q] = ((int64_t)ii * sny + jj) * snz + kk;
+        c.w[q] = wx[a] * wy[b] * wz[e];
+        c.dw[q][0] = sgn[a] * inv_dx * wy[b] * wz[e];
+        c.dw[q][1] = sgn[b] * inv_dx * wx[a] * wz[e];
+        c.dw[q][2] = sgn[e] * inv_dx * wx[a] * wy[b];
+        o[q][0] = (ax == 0 ? (float)ii : (float)ii + 0.5f) * dx - px;
+        o[q][1] = (ax == 1 ? (float)jj : (float)jj + 0.5f) * dx - py;
+        o[q][2] = (ax == 2 ? (float)kk : (float)kk + 0.5f) * dx - pz;
+      }
+}
+
+__global__ void k_adj_g2p_apic(AdjArgs a) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= a.n) return;
+  const float4 r0 = a.rec0[q];
+  const float p[3] = {r0.x, r0.y, r0.z};
+  const float dx = a.dx, inv_dx = 1.0f / dx;
+  const float inv = __fdiv_rn(3.0f, dx * dx);
+  const float g[3] = {__fdiv_rn(p[0], dx), __fdiv_rn(p[1], dx), __fdiv_rn(p[2], dx)};
+  const float h[3] = {g[0] - 0.5f, g[1] - 0.5f, g[2] - 0.5f};
+  const int sz[3][3] = {{a.nx + 1, a.ny, a.nz}, {a.nx, a.ny + 1, a.nz}, {a.nx, a.ny, a.nz + 1}};
+  const float dom[3] = {a.dom0, a.dom1, a.dom2};
+  const float eps = dx * 1.001f;
+  // velocity after G2P (for the advection clamp test)
+  float vnew[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    Corners cs;
+    float o[8][3];
+    apic_corners(c == 0 ? g[0] : h[0], c == 1 ? g[1] : h[1], c == 2 ? g[2] : h[2], sz[c][0],
+                 sz[c][1], sz[c][2], c, dx, inv_dx, p[0], p[1], p[2], cs, o);
+    float acc = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) acc += cs.w[k] * a.u3[c][cs.idx[k]];
+    vnew[c] = acc;
+  }
+  float xb[3], vb[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const float xo = a.xbar_out[3 * q + d], vo = a.vbar_out[3 * q + d];
+    const float xn = p[d] + vnew[d] * a.dt;
+    const bool free = xn >= eps && xn <= dom[d] - eps;
+    xb[d] = free ? xo : 0.0f;
+    vb[d] = vo + (free ? a.dt * xo : 0.0f);
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    Corners cs;
+    float o[8][3];
+    apic_corners(c == 0 ? g[0] : h[0], c == 1 ? g[1] : h[1], c == 2 ? g[2] : h[2], sz[c][0],
+                 sz[c][1], sz[c][2], c, dx, inv_dx, p[0], p[1], p[2], cs, o);
+    const float cb[3] = {a.Cbar_out[9 * q + 3 * c], a.Cbar_out[9 * q + 3 * c + 1],
+                         a.Cbar_out[9 * q + 3 * c + 2]};
+    float su = 0.f;  // sum_f S u3
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const float uv = a.u3[c][cs.idx[k]];
+      const float gk = vb[c] + inv * (o[k][0] * cb[0] + o[k][1] * cb[1] + o[k][2] * cb[2]);
+      atomicAdd(&a.ubar3[c][cs.idx[k]], cs.w[k] * gk);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) xb[d] += cs.dw[k][d] * uv * gk;
+      su += cs.w[k] * uv;
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) xb[d] -= inv * su * cb[d];
+  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) a.xbar_acc[3 * q + d] = xb[d];
+}
+
+__global__ void k_adj_p2g_apic(AdjArgs a) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= a.n) return;
+  const float4 r0 = a.rec0[q], r1 = a.rec1[q], r2 = a.rec2[q], r3 = a.rec3[q];
+  const float vel[3] = {r1.x, r1.y, r1.z};
+  const float C[3][3] = {{r1.w, r2.x, r2.y}, {r2.z, r2.w, r3.x}, {r3.y, r3.z, r3.w}};
+  const float p[3] = {r0.x, r0.y, r0.z};
+  const float dx = a.dx, inv_dx = 1.0f / dx;
+  const float g[3] = {__fdiv_rn(p[0], dx), __fdiv_rn(p[1], dx), __fdiv_rn(p[2], dx)};
+  const float h[3] = {g[0] - 0.5f, g[1] - 0.5f, g[2] - 0.5f};
+  const int sz[3][3] = {{a.nx + 1, a.ny, a.nz}, {a.nx, a.ny + 1, a.nz}, {a.nx, a.ny, a.nz + 1}};
+  float xb[3] = {a.xbar_acc[3 * q], a.xbar_acc[3 * q + 1], a.xbar_acc[3 * q + 2]};
+  float vb[3] = {0.f, 0.f, 0.f};
+  float Cb[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    Corners cs;
+    scatter_corners(c == 0 ? g[0] : h[0], c == 1 ? g[1] : h[1], c == 2 ? g[2] : h[2], sz[c][0],
+                    sz[c][1], sz[c][2], inv_dx, cs);
+    const int i0 = __float2int_rz(floorf(c == 0 ? g[0] : h[0])),
+              j0 = __float2int_rz(floorf(c == 1 ? g[1] : h[1])),
+              k0 = __float2int_rz(floorf(c == 2 ? g[2] : h[2]));
+    float wqs = 0.f;  // sum_f W qbar
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      if (cs.idx[k] < 0) continue;
+      const int ii = i0 + (k >> 2), jj = j0 + ((k >> 1) & 1), kk = k0 + (k & 1);
+      const float o[3] = {(c == 0 ? (float)ii : (float)ii + 0.5f) * dx - p[0],
+                          (c == 1 ? (float)jj : (float)jj + 0.5f) * dx - p[1],
+                          (c == 2 ? (float)kk : (float)kk + 0.5f) * dx - p[2]};
+      const float qb = a.qbar[c][cs.idx[k]], mb = a.mbar[c][cs.idx[k]];
+      const float val = vel[c] + C[c][0] * o[0] + C[c][1] * o[1] + C[c][2] * o[2];
+      const float wq = cs.w[k] * qb;
+      vb[c] += wq;
+      wqs += wq;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        Cb[c][d] += wq * o[d];
+        xb[d] += cs.dw[k][d] * (val * qb + mb);
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) xb[d] -= wqs * C[c][d];
+  }
+  const int64_t s = a.order[q];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    a.xbar_in[3 * s + d] = xb[d];
+    a.vbar_in[3 * s + d] = vb[d];
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) a.Cbar_in[9 * s + 3 * c + d] = Cb[c][d];
+}
+
 // ---- density splat (meshing/surface.py:14-43) and control sampling -------
 __global__ void k_splat(const float *__restrict__ pos, int64_t n, float dx, int nx, int ny,
                         int nz, float *rho) {
@@ -352,7 +513,7 @@ __global__ void k_sample_cells_adj(const float *__restrict__ pos, int64_t n, flo
 
 // ---- record layout -------------------------------------------------------
 struct RecordLayout {
-  size_t rec0, rec1, order, m[3], un[3], u3[3], label, bytes;
+  size_t rec0, rec1, rec2, rec3, order, m[3], un[3], u3[3], label, bytes;
 };
 
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -365,6 +526,8 @@ static RecordLayout layout(const Ctx *c) {
   size_t o = 0;
   L.rec0 = o; o = align256(o + n * 16);
   L.rec1 = o; o = align256(o + n * 16);
+  L.rec2 = o; o = align256(o + n * 16);  // APIC: the rest of the input C
+  L.rec3 = o; o = align256(o + n * 16);
   L.order = o; o = align256(o + n * 4);
   for (int q = 0; q < 3; ++q) { L.m[q] = o; o = align256(o + fsz[q] * 4); }
   for (int q = 0; q < 3; ++q) { L.un[q] = o; o = align256(o + fsz[q] * 4); }
@@ -395,6 +558,12 @@ static bool pic_only(const gf_step_params *prm) {
   return prm->transfer != GF_APIC && prm->flip_blend == 0.0f;
 }
 
+// Transfers the recorded substep can be differentiated for: PIC (flip_blend
+// 0) and APIC.
+static bool adjointable(const gf_step_params *prm) {
+  return pic_only(prm) || prm->transfer == GF_APIC;
+}
+
 }  // namespace gf
 
 using gf::Ctx;
@@ -414,8 +583,8 @@ int gf_step_record(void *ctx, const gf_step_params *prm, void *record) {
   Ctx *c = reinterpret_cast<Ctx *>(ctx);
   if (!c || !prm || !record) return GF_INVALID_ARG;
   if (c->nseg) return gf::fail(c, GF_INVALID_ARG, "gf_step_record: single-scene contexts only");
-  if (!gf::pic_only(prm))
-    return gf::fail(c, GF_INVALID_ARG, "the adjoint substep supports PIC (flip_blend 0) only");
+  if (!gf::adjointable(prm))
+    return gf::fail(c, GF_INVALID_ARG, "the adjoint substep supports PIC (flip_blend 0) and APIC");
   int e = gf_step(ctx, prm);
   if (e) return e;
   const gf::RecordLayout L = gf::layout(c);
@@ -427,12 +596,14 @@ int gf_step_record(void *ctx, const gf_step_params *prm, void *record) {
                           (int64_t)c->nx * c->ny * (c->nz + 1)};
   const float *mw[3] = {c->f.uw, c->f.vw, c->f.ww}, *us[3] = {c->f.us, c->f.vs, c->f.ws},
               *u3[3] = {c->f.u, c->f.v, c->f.w};
-  // 4 particle/label copies + (m, un, u3) per component
-  constexpr int kCopies = 4 + 3 * 3;
+  // 6 particle/label copies + (m, un, u3) per component
+  constexpr int kCopies = 6 + 3 * 3;
+  const size_t crec = prm->transfer == GF_APIC ? (size_t)n * 16 : 0;
   struct { size_t off; const void *src; size_t bytes; } cp[kCopies] = {
       {L.rec0, c->rec0, (size_t)n * 16}, {L.rec1, c->rec1, (size_t)n * 16},
+      {L.rec2, c->rec2, crec}, {L.rec3, c->rec3, crec},
       {L.order, c->order, (size_t)n * 4}, {L.label, c->f.label, (size_t)c->ncell}};
-  int k = 4;
+  int k = 6;
   for (int q = 0; q < 3; ++q) {
     cp[k++] = {L.m[q], mw[q], (size_t)fsz[q] * 4};
     cp[k++] = {L.un[q], us[q], (size_t)fsz[q] * 4};
@@ -446,25 +617,28 @@ int gf_step_record(void *ctx, const gf_step_params *prm, void *record) {
   return GF_OK;
 }
 
-int gf_step_adjoint(void *ctx, const gf_step_params *prm, const void *record,
-                    const float *xbar_out, const float *vbar_out, float *xbar_in, float *vbar_in) {
-  Ctx *c = reinterpret_cast<Ctx *>(ctx);
-  if (!c || !prm || !record || !xbar_out || !vbar_out || !xbar_in || !vbar_in)
-    return GF_INVALID_ARG;
-  if (c->nseg) return gf::fail(c, GF_INVALID_ARG, "gf_step_adjoint: single-scene contexts only");
-  if (!c->bound) return gf::fail(c, GF_INVALID_ARG, "gf_step_adjoint: buffers not bound");
-  if (!gf::pic_only(prm))
-    return gf::fail(c, GF_INVALID_ARG, "the adjoint substep supports PIC (flip_blend 0) only");
-  int e = gf::adj_reserve(c);
+}  // extern "C"
+
+namespace gf {
+
+// One substep's adjoint (PIC or APIC kernels around the shared grid part).
+static int step_adjoint(Ctx *c, const gf_step_params *prm, const void *record,
+                        const float *xbar_out, const float *vbar_out, const float *Cbar_out,
+                        float *xbar_in, float *vbar_in, float *Cbar_in, bool apic) {
+  int e = adj_reserve(c);
   if (e) return e;
-  const gf::RecordLayout L = gf::layout(c);
+  const RecordLayout L = layout(c);
   const char *r = static_cast<const char *>(record);
   cudaStream_t st = c->stream;
   const int64_t n = c->p.n;
   const int64_t nfmax = (int64_t)(c->nx + 1) * (c->ny + 1) * (c->nz + 1);
-  gf::AdjArgs a{};
+  AdjArgs a{};
   a.rec0 = reinterpret_cast<const float4 *>(r + L.rec0);
   a.rec1 = reinterpret_cast<const float4 *>(r + L.rec1);
+  a.rec2 = reinterpret_cast<const float4 *>(r + L.rec2);
+  a.rec3 = reinterpret_cast<const float4 *>(r + L.rec3);
+  a.Cbar_out = Cbar_out;
+  a.Cbar_in = Cbar_in;
   a.order = reinterpret_cast<const int32_t *>(r + L.order);
   a.label = reinterpret_cast<const uint8_t *>(r + L.label);
   for (int q = 0; q < 3; ++q) {
@@ -492,42 +666,83 @@ int gf_step_adjoint(void *ctx, const gf_step_params *prm, const void *record,
   a.nx = c->nx;
   a.ny = c->ny;
   a.nz = c->nz;
-  if ((e = gf::check_cuda(c, cudaMemsetAsync(c->adj_faces, 0, 3 * nfmax * 4, st), "zero ubar")))
+  if ((e = check_cuda(c, cudaMemsetAsync(c->adj_faces, 0, 3 * nfmax * 4, st), "zero ubar")))
     return e;
   const unsigned gp = (unsigned)((n + 255) / 256);
   if (n > 0) {
-    gf::k_adj_g2p<<<gp, 256, 0, st>>>(a);
+    if (apic)
+      k_adj_g2p_apic<<<gp, 256, 0, st>>>(a);
+    else
+      k_adj_g2p<<<gp, 256, 0, st>>>(a);
     c->launches++;
   }
   // pressure-gradient adjoint -> rhs of the adjoint solve, on the recorded labels
-  if ((e = gf::check_cuda(c, cudaMemcpyAsync(c->f.label, a.label, c->ncell,
-                                             cudaMemcpyDeviceToDevice, st),
-                          "restore labels")))
+  if ((e = check_cuda(c, cudaMemcpyAsync(c->f.label, a.label, c->ncell,
+                                         cudaMemcpyDeviceToDevice, st),
+                      "restore labels")))
     return e;
   float kk = prm->rho * c->dx;  // dt / (rho dx), as k3_subtract_pressure_grad
   kk = prm->dt / kk;
   const unsigned gc = (unsigned)((c->ncell + 255) / 256 < (int64_t)c->num_sms * 16
                                      ? (c->ncell + 255) / 256
                                      : (int64_t)c->num_sms * 16);
-  gf::k_adj_grad<<<gc, 256, 0, st>>>(a, kk);
+  k_adj_grad<<<gc, 256, 0, st>>>(a, kk);
   c->launches++;
   // A lambda = pbar with the same SPD operator (labels fixed)
   gf_step_params sp = *prm;
   sp.rhs_sign = 1;
   if (sp.solver != GF_PCG && sp.solver != GF_PCG_REFINED) sp.solver = GF_PCG;
-  if ((e = gf::launch_pressure(c, &sp))) return e;
+  if ((e = launch_pressure(c, &sp))) return e;
   float s = prm->rho * c->dx;  // (rho dx) / dt, as k3_compute_divergence
   s = s / prm->dt;
   const unsigned gf_ = (unsigned)((nfmax + 255) / 256 < (int64_t)c->num_sms * 16
                                       ? (nfmax + 255) / 256
                                       : (int64_t)c->num_sms * 16);
-  gf::k_adj_faces<<<gf_, 256, 0, st>>>(a, s);
+  k_adj_faces<<<gf_, 256, 0, st>>>(a, s);
   c->launches++;
   if (n > 0) {
-    gf::k_adj_p2g<<<gp, 256, 0, st>>>(a);
+    if (apic)
+      k_adj_p2g_apic<<<gp, 256, 0, st>>>(a);
+    else
+      k_adj_p2g<<<gp, 256, 0, st>>>(a);
     c->launches++;
   }
-  return gf::check_launch(c, "gf_step_adjoint");
+  return check_launch(c, apic ? "gf_step_adjoint_apic" : "gf_step_adjoint");
+}
+
+}  // namespace gf
+
+extern "C" {
+
+int gf_step_adjoint(void *ctx, const gf_step_params *prm, const void *record,
+                    const float *xbar_out, const float *vbar_out, float *xbar_in, float *vbar_in) {
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);
+  if (!c || !prm || !record || !xbar_out || !vbar_out || !xbar_in || !vbar_in)
+    return GF_INVALID_ARG;
+  if (c->nseg) return gf::fail(c, GF_INVALID_ARG, "gf_step_adjoint: single-scene contexts only");
+  if (!c->bound) return gf::fail(c, GF_INVALID_ARG, "gf_step_adjoint: buffers not bound");
+  if (!gf::pic_only(prm))
+    return gf::fail(c, GF_INVALID_ARG,
+                    "gf_step_adjoint is the PIC (flip_blend 0) adjoint; APIC uses "
+                    "gf_step_adjoint_apic");
+  return gf::step_adjoint(c, prm, record, xbar_out, vbar_out, nullptr, xbar_in, vbar_in, nullptr,
+                          false);
+}
+
+int gf_step_adjoint_apic(void *ctx, const gf_step_params *prm, const void *record,
+                         const float *xbar_out, const float *vbar_out, const float *Cbar_out,
+                         float *xbar_in, float *vbar_in, float *Cbar_in) {
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);
+  if (!c || !prm || !record || !xbar_out || !vbar_out || !Cbar_out || !xbar_in || !vbar_in ||
+      !Cbar_in)
+    return GF_INVALID_ARG;
+  if (c->nseg)
+    return gf::fail(c, GF_INVALID_ARG, "gf_step_adjoint_apic: single-scene contexts only");
+  if (!c->bound) return gf::fail(c, GF_INVALID_ARG, "gf_step_adjoint_apic: buffers not bound");
+  if (prm->transfer != GF_APIC)
+    return gf::fail(c, GF_INVALID_ARG, "gf_step_adjoint_apic needs an APIC substep");
+  return gf::step_adjoint(c, prm, record, xbar_out, vbar_out, Cbar_out, xbar_in, vbar_in, Cbar_in,
+                          true);
 }
 
 int gf_density_splat(void *ctx, const float *pos, int64_t n, float *rho) {

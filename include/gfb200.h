@@ -175,7 +175,7 @@ int gf_vmax(void *ctx, float *vmax_out);
 
 /* ---- adjoint (differentiation through substeps) ------------------------- */
 /* No counterpart in the reference (planned only there).  PIC transfer
- * (flip_blend 0) with the cell labels held fixed within each substep.
+ * (flip_blend 0) or APIC, with the cell labels held fixed within each substep.
  * gf_step_record runs gf_step and copies into `record` (a caller-owned device
  * buffer of gf_record_bytes bytes) what the adjoint needs: the substep's
  * sorted inputs, their storage slots, the P2G weight sums and normalised
@@ -192,6 +192,13 @@ int gf_step_record(void *ctx, const gf_step_params *prm, void *record);
 int gf_step_adjoint(void *ctx, const gf_step_params *prm, const void *record,
                     const float *xbar_out, const float *vbar_out, float *xbar_in,
                     float *vbar_in);
+/* The same for an APIC substep (k3_p2g_apic :1475-1588, k3_g2p_apic_advect
+ * :1591-1732), which also carries the adjoint of the affine matrices:
+ * Cbar_out / Cbar_in are (n,3,3) row-major like C, in the output's sorted
+ * order / the input's storage order. */
+int gf_step_adjoint_apic(void *ctx, const gf_step_params *prm, const void *record,
+                         const float *xbar_out, const float *vbar_out, const float *Cbar_out,
+                         float *xbar_in, float *vbar_in, float *Cbar_in);
 /* Cell-centred trilinear density splat of unit-mass particles into rho
  * (nx,ny,nz) (k_density_scatter, meshing/surface.py:14-43) and its adjoint
  * with respect to the positions. */

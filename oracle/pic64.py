@@ -16,7 +16,10 @@ substep restates the reference kernels in float64 with vectorised NumPy:
 with the cell labels of every substep supplied by the caller (the adjoint
 holds them fixed), plus the control sampling and the density-splat loss, and
 the reverse-mode derivative of all of it in float64 (``substep_adjoint``,
-``grad``), itself checked against central differences.
+``grad``), itself checked against central differences; and the same for the
+APIC transfer (P2G with the affine term C.(x_face - x_p), k3_p2g_apic
+:1475-1588; G2P gathering velocity and C, k3_g2p_apic_advect :1591-1732):
+``substep_apic``, ``substep_apic_adjoint``, ``loss_apic``, ``grad_apic``.
 """
 from __future__ import annotations
 
@@ -92,6 +95,37 @@ def _corner_weights_grad(f, dims, clamp):
                               sg[2] * gate[:, 2] * wx * wy], 1)
                 dw.append(np.where(ok[:, None], d, 0.0))
     return np.stack(idx, 1), np.stack(w, 1), np.stack(dw, 1)
+
+
+def _corners_apic(f, dims, clamp_idx):
+    """Corner flat indices, integer corner coordinates (P,8,3), weights and
+    d(weight)/df (P,8,3) with unclamped weights s = f - floor(f): clamp_idx
+    True clamps each corner index into the grid (apic gather, :1626-1724),
+    False drops corners outside it (scatter_face with positions, :1475-1588)."""
+    dims = np.asarray(dims)
+    i0 = np.floor(f).astype(np.int64)
+    s = f - i0
+    idx, ijk, w, dw = [], [], [], []
+    for a in range(2):
+        for b in range(2):
+            for c in range(2):
+                ii = i0 + np.array([a, b, c])
+                if clamp_idx:
+                    ii = np.minimum(np.maximum(ii, 0), dims - 1)
+                    ok = np.ones(len(f), bool)
+                else:
+                    ok = np.all((ii >= 0) & (ii < dims), axis=1)
+                wx = (1 - s[:, 0]) if a == 0 else s[:, 0]
+                wy = (1 - s[:, 1]) if b == 0 else s[:, 1]
+                wz = (1 - s[:, 2]) if c == 0 else s[:, 2]
+                sg = [(-1.0, 1.0)[a], (-1.0, 1.0)[b], (-1.0, 1.0)[c]]
+                flat = (ii[:, 0] * dims[1] + ii[:, 1]) * dims[2] + ii[:, 2]
+                idx.append(np.where(ok, flat, 0))
+                ijk.append(ii)
+                w.append(np.where(ok, wx * wy * wz, 0.0))
+                d = np.stack([sg[0] * wy * wz, sg[1] * wx * wz, sg[2] * wx * wy], 1)
+                dw.append(np.where(ok[:, None], d, 0.0))
+    return np.stack(idx, 1), np.stack(ijk, 1), np.stack(w, 1), np.stack(dw, 1)
 
 
 class PicFP64:
@@ -312,6 +346,169 @@ class PicFP64:
         for t in reversed(range(len(labels))):
             xt, vt = tape[t]
             xbar, vbar = self.substep_adjoint(xt, vt, labels[t], dt, t, xbar, vbar)
+        idx, w, _ = _corner_weights_grad(x0.astype(np.float64) / self.dx - 0.5, (self.n,) * 3,
+                                         clamp=False)
+        return np.stack([np.bincount(idx.ravel(), weights=(w * vbar[:, c:c + 1]).ravel(),
+                                     minlength=self.n ** 3).reshape((self.n,) * 3)
+                         for c in range(3)])
+
+    # ---- APIC substep (k3_p2g_apic :1475-1588, k3_g2p_apic_advect :1591-1732)
+    _OFFS = [np.array([0.0, 0.5, 0.5]), np.array([0.5, 0.0, 0.5]), np.array([0.5, 0.5, 0.0])]
+
+    def _grid_apic(self, x, v, C, lab, dt, key):
+        """P2G (APIC), forces, BC, divergence, pressure, gradient: the face
+        velocities u3 plus what the adjoint needs."""
+        dx = self.dx
+        gx = x / dx
+        masks = self._bc_masks(lab)
+        pw, un, ms, u = [], [], [], []
+        for c in range(3):
+            idx, ijk, w, dw = _corners_apic(gx - self._OFFS[c], self.dims[c], clamp_idx=False)
+            o = (ijk + self._OFFS[c]) * dx - x[:, None, :]          # x_f - x_p (P,8,3)
+            val = v[:, c:c + 1] + (o * C[:, c, None, :]).sum(-1)   # (P,8)
+            size = int(np.prod(self.dims[c]))
+            m = np.bincount(idx.ravel(), weights=w.ravel(), minlength=size)
+            q = np.bincount(idx.ravel(), weights=(w * val).ravel(), minlength=size)
+            uc = np.where(m > 1e-8, q / np.where(m > 1e-8, m, 1.0), 0.0)
+            pw.append((idx, w, dw, o, val)); un.append(uc); ms.append(m)
+            uu = uc.reshape(self.dims[c]) + (self.g * dt if c == 1 else 0.0)
+            uu[masks[c]] = 0.0
+            u.append(uu)
+        fl = lab == 1
+        s = self.rho * dx / dt
+        div = (u[0][1:] - u[0][:-1]) + (u[1][:, 1:] - u[1][:, :-1]) + (u[2][:, :, 1:] - u[2][:, :, :-1])
+        div = np.where(fl, div * s, 0.0)
+        fl, _, solve = self._system(key, lab)
+        p = np.zeros(lab.shape)
+        if fl.any():
+            p[fl] = solve(-div[fl])
+        k = dt / (self.rho * dx)
+        u3, elig_l = [], []
+        for c in range(3):
+            pl = np.zeros(self.dims[c]); pr = np.zeros(self.dims[c])
+            ml = np.full(self.dims[c], 2, lab.dtype); mr = np.full(self.dims[c], 2, lab.dtype)
+            sl = [slice(None)] * 3; sr = [slice(None)] * 3
+            sl[c] = slice(1, None); sr[c] = slice(None, -1)
+            pl[tuple(sl)] = p; ml[tuple(sl)] = lab
+            pr[tuple(sr)] = p; mr[tuple(sr)] = lab
+            elig = ((ml == 1) | (mr == 1)) & (ml != 2) & (mr != 2) & ~masks[c]
+            pl = np.where(ml == 1, pl, 0.0); pr = np.where(mr == 1, pr, 0.0)
+            uc = np.where(elig, u[c] - k * (pr - pl), u[c])
+            uc[masks[c]] = 0.0
+            u3.append(uc); elig_l.append((elig, ml, mr))
+        return dict(masks=masks, pw=pw, un=un, ms=ms, u3=u3, elig=elig_l, fl=fl, solve=solve,
+                    s=s, k=k)
+
+    def _g2p_apic(self, x, u3):
+        dx = self.dx
+        gx = x / dx
+        inv = 3.0 / (dx * dx)
+        vn = np.zeros_like(x)
+        Cn = np.zeros((len(x), 3, 3))
+        gath = []
+        for c in range(3):
+            idx, ijk, w, dw = _corners_apic(gx - self._OFFS[c], self.dims[c], clamp_idx=True)
+            o = (ijk + self._OFFS[c]) * dx - x[:, None, :]
+            uf = u3[c].ravel()[idx]
+            vn[:, c] = (w * uf).sum(1)
+            Cn[:, c, :] = ((w * uf * inv)[:, :, None] * o).sum(1)
+            gath.append((idx, w, dw, o, uf))
+        return vn, Cn, gath
+
+    def substep_apic(self, x, v, C, lab, dt, key):
+        g = self._grid_apic(x, v, C, lab, dt, key)
+        vn, Cn, _ = self._g2p_apic(x, g["u3"])
+        eps = self.dx * 1.001
+        xn = np.clip(x + vn * dt, eps, self.dom - eps)
+        return xn, vn, Cn
+
+    def substep_apic_adjoint(self, x, v, C, lab, dt, key, xbar, vbar, Cbar):
+        """Reverse-mode derivative of substep_apic: adjoints of (x, v, C)."""
+        dx = self.dx
+        inv = 3.0 / (dx * dx)
+        g = self._grid_apic(x, v, C, lab, dt, key)
+        vn, Cn, gath = self._g2p_apic(x, g["u3"])
+        eps = dx * 1.001
+        xr = x + vn * dt
+        free = (xr >= eps) & (xr <= self.dom - eps)
+        xb = np.where(free, xbar, 0.0)
+        vb = vbar + np.where(free, dt * xbar, 0.0)
+        ub3 = []
+        for c in range(3):
+            idx, w, dw, o, uf = gath[c]
+            # g_c per corner: vb_c + inv * sum_d o_d Cbar[c][d]
+            gc = vb[:, c:c + 1] + inv * (o * Cbar[:, c, None, :]).sum(-1)     # (P,8)
+            size = int(np.prod(self.dims[c]))
+            ub3.append(np.bincount(idx.ravel(), weights=(w * gc).ravel(),
+                                   minlength=size).reshape(self.dims[c]))
+            xb += (dw * (uf * gc)[:, :, None]).sum(1) / dx
+            xb -= (w * uf * inv).sum(1)[:, None] * Cbar[:, c, :]
+        fl, solve, s, k, masks = g["fl"], g["solve"], g["s"], g["k"], g["masks"]
+        pbar = np.zeros(lab.shape)
+        ub = []
+        for c in range(3):
+            elig, ml, mr = g["elig"][c]
+            gg = np.where(elig, ub3[c], 0.0)
+            sl = [slice(None)] * 3; sr = [slice(None)] * 3
+            sl[c] = slice(1, None); sr[c] = slice(None, -1)
+            pbar += np.where(fl, -k * gg[tuple(sr)] * (mr[tuple(sr)] == 1), 0.0)
+            pbar += np.where(fl, k * gg[tuple(sl)] * (ml[tuple(sl)] == 1), 0.0)
+            ub.append(np.where(masks[c], 0.0, ub3[c]))
+        lam = np.zeros(lab.shape)
+        if fl.any():
+            lam[fl] = solve(pbar[fl])
+        divbar = np.where(fl, -lam, 0.0) * s
+        for c in range(3):
+            add = np.zeros(self.dims[c])
+            sl = [slice(None)] * 3; sr = [slice(None)] * 3
+            sl[c] = slice(1, None); sr[c] = slice(None, -1)
+            add[tuple(sl)] += divbar
+            add[tuple(sr)] -= divbar
+            ub[c] = np.where(masks[c], 0.0, ub[c] + add)
+        vb_in = np.zeros_like(v)
+        Cb_in = np.zeros_like(C)
+        for c in range(3):
+            idx, w, dw, o, val = g["pw"][c]
+            ubf = ub[c].ravel()
+            m = g["ms"][c]
+            ok = m > 1e-8
+            qbar = np.where(ok, ubf / np.where(ok, m, 1.0), 0.0)
+            mbar = np.where(ok, -ubf * g["un"][c] / np.where(ok, m, 1.0), 0.0)
+            wq = w * qbar[idx]
+            vb_in[:, c] = wq.sum(1)
+            Cb_in[:, c, :] = (wq[:, :, None] * o).sum(1)
+            xb += (dw * (val * qbar[idx] + mbar[idx])[:, :, None]).sum(1) / dx
+            xb -= wq.sum(1)[:, None] * C[:, c, :]
+        return xb, vb_in, Cb_in
+
+    def loss_apic(self, control, x0, labels, dt, target):
+        x = x0.astype(np.float64)
+        v = self.sample_cells(control.astype(np.float64), x)
+        C = np.zeros((len(x), 3, 3))
+        for t, lab in enumerate(labels):
+            x, v, C = self.substep_apic(x, v, C, lab, dt, key=t)
+        r = self.splat(x) - target
+        return float((r * r).sum())
+
+    def grad_apic(self, control, x0, labels, dt, target):
+        x = x0.astype(np.float64)
+        ctl = control.astype(np.float64)
+        v = self.sample_cells(ctl, x)
+        C = np.zeros((len(x), 3, 3))
+        tape = []
+        for t, lab in enumerate(labels):
+            tape.append((x, v, C))
+            x, v, C = self.substep_apic(x, v, C, lab, dt, key=t)
+        idx, w, dw = _corner_weights_grad(x / self.dx - 0.5, (self.n,) * 3, clamp=False)
+        rho = np.bincount(idx.ravel(), weights=w.ravel(), minlength=self.n ** 3)
+        rbar = 2.0 * (rho - target.ravel())
+        xbar = (dw * rbar[idx][:, :, None]).sum(1) / self.dx
+        vbar = np.zeros_like(xbar)
+        Cbar = np.zeros((len(x), 3, 3))
+        for t in reversed(range(len(labels))):
+            xt, vt, Ct = tape[t]
+            xbar, vbar, Cbar = self.substep_apic_adjoint(xt, vt, Ct, labels[t], dt, t, xbar,
+                                                         vbar, Cbar)
         idx, w, _ = _corner_weights_grad(x0.astype(np.float64) / self.dx - 0.5, (self.n,) * 3,
                                          clamp=False)
         return np.stack([np.bincount(idx.ravel(), weights=(w * vbar[:, c:c + 1]).ravel(),

@@ -21,9 +21,12 @@ def _check(problem, control, n_dirs, eps, tol, seed, tol_l2=1e-4):
     x0 = problem.x0.cpu().numpy()
     target = problem.target.cpu().numpy().astype(np.float64)
     ref = PicFP64(problem.n)
-    L0 = ref.loss(control, x0, labels, problem.dt, target)
+    apic = problem.transfer == "apic"
+    loss_fn = ref.loss_apic if apic else ref.loss
+    grad_fn = ref.grad_apic if apic else ref.grad
+    L0 = loss_fn(control, x0, labels, problem.dt, target)
     assert abs(L0 - loss_gpu) <= 1e-6 * abs(L0), (L0, loss_gpu)
-    g64 = ref.grad(control, x0, labels, problem.dt, target)
+    g64 = grad_fn(control, x0, labels, problem.dt, target)
     rel = np.linalg.norm(grad - g64) / np.linalg.norm(g64)
     assert rel < tol_l2, rel
     rng = np.random.default_rng(seed)
@@ -31,8 +34,8 @@ def _check(problem, control, n_dirs, eps, tol, seed, tol_l2=1e-4):
     for _ in range(n_dirs):
         d = rng.normal(size=control.shape)
         d /= np.linalg.norm(d)
-        lp = ref.loss(control + eps * d, x0, labels, problem.dt, target)
-        lm = ref.loss(control - eps * d, x0, labels, problem.dt, target)
+        lp = loss_fn(control + eps * d, x0, labels, problem.dt, target)
+        lm = loss_fn(control - eps * d, x0, labels, problem.dt, target)
         fd.append((lp - lm) / (2 * eps))
         ad.append(float((grad * d).sum()))
     ad, fd = np.array(ad), np.array(fd)
@@ -72,3 +75,21 @@ def test_rollout_loss_autograd(gf):
     g2 = prob.backward(control.detach(), ck)
     assert control.grad is not None and control.grad.shape == control.shape
     assert torch.allclose(control.grad, g2, rtol=1e-4, atol=1e-7 * float(g2.abs().max()))
+
+
+def test_adjoint_apic_small_uneven_segments(gf):
+    """APIC transfer: 32^3, 7 substeps with checkpoints every 3; the affine
+    matrices' adjoint is carried through the substeps."""
+    from gpufluid_b200.adjoint import DropShaping
+    prob = DropShaping(n=32, T=7, k=3, transfer="apic")
+    control = np.random.default_rng(1).normal(0, 0.1, (3, 32, 32, 32)).astype(np.float32)
+    _check(prob, control, n_dirs=6, eps=1e-3, tol=1e-3, seed=11)
+
+
+def test_adjoint_apic_drop_shaping_64(gf):
+    """The 64^3 drop-shaping problem with APIC transfer: 40 substeps at dt
+    1/240, checkpoints every 10, 16 seeded directions, eps 1e-3."""
+    from gpufluid_b200.adjoint import DropShaping
+    prob = DropShaping(n=64, T=40, k=10, transfer="apic")
+    control = np.random.default_rng(4).normal(0, 0.1, (3, 64, 64, 64)).astype(np.float32)
+    _check(prob, control, n_dirs=16, eps=1e-3, tol=1e-3, seed=7)
