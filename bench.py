@@ -249,13 +249,13 @@ def timed_steps(torch, s, steps, solver):
     return e0.elapsed_time(e1) / steps, s.launch_count() - l0
 
 
-def adjoint_leg(torch, device, reps=2):
+def adjoint_leg(torch, device, reps=2, transfer="pic"):
     """Forward and forward+adjoint of the drop-shaping rollout (64^3 PIC sphere,
     40 substeps of 1/240 s, checkpoints every 10 substeps, refined PCG to 1e-9):
     substeps/s of each and their cost ratio, timed with device synchronisation
     around whole rollouts."""
     from gpufluid_b200.adjoint import DropShaping
-    prob = DropShaping(n=64, T=40, k=10, device=device)
+    prob = DropShaping(n=64, T=40, k=10, device=device, transfer=transfer)
     g = torch.Generator(device="cpu").manual_seed(7)
     control = (0.3 * torch.randn((3, 64, 64, 64), generator=g)).to(device)
     prob.loss_and_grad(control)  # warm-up
@@ -265,14 +265,14 @@ def adjoint_leg(torch, device, reps=2):
         fwd.append(prob.last_timing["forward_s"])
         bwd.append(prob.last_timing["backward_s"])
     tf, tb = float(np.median(fwd)), float(np.median(bwd))
-    return {"workload": "drop shaping 64^3 PIC, 40 substeps, checkpoint every 10",
+    return {"workload": f"drop shaping 64^3 {transfer.upper()}, 40 substeps, checkpoint every 10",
             "particles": prob.P, "forward_substeps_per_s": round(prob.T / tf, 2),
             "fwd_adj_substeps_per_s": round(prob.T / (tf + tb), 2),
             "forward_ms": round(1e3 * tf, 2), "adjoint_ms": round(1e3 * tb, 2),
             "fwd_adj_over_fwd": round((tf + tb) / tf, 3)}
 
 
-def batched_leg(torch, device, k_steps=10, warm=2, n_scenes=64):
+def batched_leg(torch, device, k_steps=10, warm=2, n_scenes=64, ranks=None):
     """64 independent dam breaks of uneven sides {32,48,64,80,96}^3 (seeded
     block extents, 8 ppc), FLIP, dt = 1/240, per-scene refined PCG to 1e-7:
     the whole batch stepped together (one launch per stage, captured graph,
@@ -281,8 +281,15 @@ def batched_leg(torch, device, k_steps=10, warm=2, n_scenes=64):
     substeps from the same state; the value is scene-substeps per second."""
     import gpufluid_b200 as gf
     from gpufluid_b200.batch import BatchedFlip3D, cfg_uneven_scenes
+    from gpufluid_b200.dist import shard_scenes
     scenes = cfg_uneven_scenes(n_scenes, seed=0)
     dt, iters, tol = 1.0 / 240.0, 4000, 1e-7
+    # on N GPUs each rank steps its shard of the scenes (by particle count,
+    # estimated from the seeded block volumes); no exchange while stepping
+    world = ranks.world if ranks else 1
+    est = [int(sc["n"] ** 3 * sc["hi"][0] * sc["hi"][1] * 8) for sc in scenes]
+    mine = shard_scenes(est, world)[ranks.rank if ranks else 0]
+    scenes = [scenes[i] for i in mine]
     stream = torch.cuda.current_stream()
 
     def timed(step):
@@ -318,9 +325,13 @@ def batched_leg(torch, device, k_steps=10, warm=2, n_scenes=64):
         ms_single += timed(lambda: one.step(dt, iters, "pcg_refined"))
         del one
     its = [x["iters"] for x in st]
+    if ranks:  # whole-job figures: max time over ranks, totals over ranks
+        ms_batch, ms_single = ranks.max(ms_batch), ranks.max(ms_single)
+        n_part = int(ranks.sum(n_part))
     return {"workload": f"{n_scenes} dam breaks, sides from {{32,48,64,80,96}}^3, FLIP, 8 ppc, "
                         "dt=1/240, per-scene refined PCG to 1e-7",
             "scenes": n_scenes, "particles": n_part, "timed_substeps": k_steps,
+            "sharding": f"{world} rank(s), scenes split by particle count",
             "batched_scene_substeps_per_s": round(n_scenes * k_steps * 1000.0 / ms_batch, 2),
             "one_at_a_time_scene_substeps_per_s": round(n_scenes * k_steps * 1000.0 / ms_single, 2),
             "speedup": round(ms_single / ms_batch, 3),
@@ -414,30 +425,17 @@ def extra_legs(torch, device, steps=3):
 
 def run_ours(args):
     import torch
-    import torch.distributed as dist
 
     import gpufluid_b200 as gf
+    from gpufluid_b200.dist import Ranks
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     device = f"cuda:{local}"
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device(device))
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks("nccl", device=device)
+    world, rank = ranks.world, ranks.rank
+    barrier = ranks.barrier
+    max_over_ranks = ranks.max
 
     s = make_solver(gf, device, graphs=True)
     P = s.n_particles
@@ -519,8 +517,11 @@ def run_ours(args):
     barrier()
 
     fwd_adj = None if args.no_adjoint else adjoint_leg(torch, device)
-    batched = None if args.no_batched else batched_leg(torch, device)
+    fwd_adj_apic = None if args.no_adjoint else adjoint_leg(torch, device, transfer="apic")
+    batched = None if args.no_batched else batched_leg(torch, device, ranks=ranks)
     extra = None if args.no_extra else extra_legs(torch, device)
+
+    ms_plain_max = max_over_ranks(ms_plain)  # every rank takes part in each collective
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -540,7 +541,7 @@ def run_ours(args):
                                     f"{P * 64 / 1e6:.0f} MB + MAC grids {F * 4 * 3 / 1e6:.0f} MB "
                                     "streamed every substep"},
             "particle_updates_per_s": round(value * P, 1),
-            "plain_fp32": {"substeps_per_s": round(world * 1000.0 / max_over_ranks(ms_plain), 3),
+            "plain_fp32": {"substeps_per_s": round(world * 1000.0 / ms_plain_max, 3),
                            "ms_per_step": round(ms_plain, 4), "iters_last": plain_stats["iters"],
                            "recursive_relres": plain_stats["relres"],
                            "true_relres_fp64": plain_true,
@@ -569,12 +570,12 @@ def run_ours(args):
             "clocks": clk,
             "cpu_baseline": cpu,
             "fwd_adj": fwd_adj,
+            "fwd_adj_apic": fwd_adj_apic,
             "batched": batched,
             "other_configs": extra,
         }
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    ranks.close()
 
 
 def cpu_baseline(steps=1):
