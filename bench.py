@@ -342,6 +342,57 @@ def batched_leg(torch, device, k_steps=10, warm=2, n_scenes=64, ranks=None):
             "autotune": tune}
 
 
+def batched_adjoint_leg(torch, device, n_scenes=64, reps=1, ranks=None):
+    """The drop-shaping loss (sphere, PIC, 40 substeps of 1/240 s, checkpoints
+    every 10, refined PCG to 1e-9) on the 64 scene sides of the batched
+    workload, forward+adjoint of all scenes in one batch context against the
+    same scenes' forward+adjoint one at a time (one single-grid problem per
+    side, each scene with its own control).  Times are whole passes with
+    device synchronisation around them; the value is scene-substeps/s."""
+    from gpufluid_b200.adjoint import BatchedDropShaping, DropShaping
+    from gpufluid_b200.batch import cfg_uneven_scenes
+    from gpufluid_b200.dist import shard_scenes
+    sides_all = [sc["n"] for sc in cfg_uneven_scenes(n_scenes, seed=0)]
+    world = ranks.world if ranks else 1
+    mine = shard_scenes([n ** 3 for n in sides_all], world)[ranks.rank if ranks else 0]
+    sides = [sides_all[i] for i in mine]
+    T = 40
+    prob = BatchedDropShaping(sides, T=T, k=10, device=device)
+    g = torch.Generator(device="cpu").manual_seed(7)
+    control = (0.3 * torch.randn(prob.control_shape, generator=g)).to(device)
+    prob.loss_and_grad(control)  # warm-up
+    tb = []
+    for _ in range(reps):
+        prob.loss_and_grad(control)
+        tb.append(prob.last_timing["forward_s"] + prob.last_timing["backward_s"])
+    t_batch = float(np.median(tb))
+    fwd_s = prob.last_timing["forward_s"]
+    n_part = prob.P
+    del prob
+    singles, t_single = {}, 0.0
+    for i, n in enumerate(sides):
+        if n not in singles:
+            singles[n] = DropShaping(n=n, T=T, k=10, device=device)
+            c = (0.3 * torch.randn((3, n, n, n), generator=g)).to(device)
+            singles[n].loss_and_grad(c)  # warm-up of this side
+        c = (0.3 * torch.randn((3, n, n, n), generator=g)).to(device)
+        singles[n].loss_and_grad(c)
+        t_single += singles[n].last_timing["forward_s"] + singles[n].last_timing["backward_s"]
+    del singles
+    if ranks:
+        t_batch, t_single = ranks.max(t_batch), ranks.max(t_single)
+        n_part = int(ranks.sum(n_part))
+    return {"workload": f"drop shaping on {n_scenes} scenes of sides {{32,48,64,80,96}}^3, PIC, "
+                        "40 substeps, checkpoint every 10, refined PCG to 1e-9",
+            "scenes": n_scenes, "particles": n_part,
+            "sharding": f"{world} rank(s), scenes split by cell count",
+            "batched_fwd_adj_s": round(t_batch, 3), "batched_forward_s": round(fwd_s, 3),
+            "batched_fwd_adj_scene_substeps_per_s": round(n_scenes * T / t_batch, 2),
+            "one_at_a_time_fwd_adj_s": round(t_single, 3),
+            "one_at_a_time_fwd_adj_scene_substeps_per_s": round(n_scenes * T / t_single, 2),
+            "speedup": round(t_single / t_batch, 3)}
+
+
 def stage_bytes_flip(P, ncell_active, F):
     """Algorithmic bytes of the FLIP (non-APIC) stages: sort 64P + 12N,
     P2G 24P + 24F (the zeroing of the six P2G face arrays counted as for
@@ -519,6 +570,8 @@ def run_ours(args):
     fwd_adj = None if args.no_adjoint else adjoint_leg(torch, device)
     fwd_adj_apic = None if args.no_adjoint else adjoint_leg(torch, device, transfer="apic")
     batched = None if args.no_batched else batched_leg(torch, device, ranks=ranks)
+    batched_adj = (None if args.no_batched or args.no_adjoint
+                   else batched_adjoint_leg(torch, device, ranks=ranks))
     extra = None if args.no_extra else extra_legs(torch, device)
 
     ms_plain_max = max_over_ranks(ms_plain)  # every rank takes part in each collective
@@ -572,6 +625,7 @@ def run_ours(args):
             "fwd_adj": fwd_adj,
             "fwd_adj_apic": fwd_adj_apic,
             "batched": batched,
+            "batched_fwd_adj": batched_adj,
             "other_configs": extra,
         }
         print(json.dumps(line), flush=True)

@@ -65,6 +65,8 @@ class DropShaping:
         self.solver = FlipSolver3D(n, n, n, transfer_mode=transfer, flip_blend=0.0,
                                    pressure_tol=tol, device=device)
         s = self.solver
+        self.rho_shape = (n, n, n)        # splat / target buffer
+        self.control_shape = (3, n, n, n)
         x0 = _scene.seed_sphere_positions(n, n, n, s.dx, center, radius, ppc)
         s._set_particles(pos=x0, vel=np.zeros_like(x0))
         self.P = x0.shape[0]
@@ -90,7 +92,7 @@ class DropShaping:
         _lib.check(getattr(s._L, name)(s._ctx, *args), s._ctx, name)
 
     def splat(self, pos: torch.Tensor) -> torch.Tensor:
-        rho = torch.empty((self.n,) * 3, dtype=torch.float32, device=self.device)
+        rho = torch.empty(self.rho_shape, dtype=torch.float32, device=self.device)
         self._c("gf_density_splat", pos.data_ptr(), pos.shape[0], rho.data_ptr())
         return rho
 
@@ -185,7 +187,7 @@ class DropShaping:
             carry_C[idx] = Cbar
         # checkpoint 0 holds the particles in id order: carry is v(0)'s adjoint
         # (C(0) = 0 does not depend on the control)
-        grad = torch.empty((3,) + (self.n,) * 3, dtype=torch.float32, device=dev)
+        grad = torch.empty(self.control_shape, dtype=torch.float32, device=dev)
         self._c("gf_sample_cells_adjoint", self.x0.data_ptr(), P, carry_v.data_ptr(),
                 grad.data_ptr())
         return grad
@@ -201,6 +203,68 @@ class DropShaping:
         t2 = time.perf_counter()
         self.last_timing = {"forward_s": t1 - t0, "backward_s": t2 - t1}
         return loss, grad
+
+
+class BatchedDropShaping(DropShaping):
+    """The drop-shaping problem on many scenes of uneven sizes at once (one
+    batch context: every substep, adjoint substep, splat and sampling is one
+    launch per kernel for all scenes).  Scene s is the single-scene problem at
+    side sides[s] (the same sphere, shift and blur in unit coordinates); the
+    control is each scene's (3, n, n, n) field concatenated (flat), the loss
+    the sum of the scenes' losses."""
+
+    def __init__(self, sides, T=40, dt=1.0 / 240.0, k=10, center=(0.5, 0.35, 0.5), radius=0.15,
+                 shift=(0.15, 0.1, 0.0), sigma=1.5, ppc=8, device="cuda",
+                 pressure_solver="pcg_refined", tol=1e-9, max_iters=4000, transfer="pic"):
+        from .batch import BatchedFlip3D
+        if transfer not in ("pic", "apic"):
+            raise ValueError("the adjoint substep supports transfer 'pic' and 'apic'")
+        self.sides = [int(n) for n in sides]
+        self.n = None
+        self.T, self.dt, self.k = T, dt, k
+        self.transfer = transfer
+        self.device = torch.device(device)
+        self.solver = BatchedFlip3D([(n, n, n) for n in self.sides], transfer_mode=transfer,
+                                    flip_blend=0.0, pressure_tol=tol, device=device)
+        s = self.solver
+        for i, n in enumerate(self.sides):
+            s.set_particles(i, _scene.seed_sphere_positions(n, n, n, 1.0 / n, center, radius, ppc))
+        self.P = s.n_particles
+        self.x0 = s._pos.clone()
+        self.cell0 = [L["cell0"] for L in s.layout]
+        ncell = s.totals["ncell"]
+        self.rho_shape = (ncell,)
+        self.control_shape = (3 * ncell,)
+        self.pressure_solver, self.max_iters = pressure_solver, max_iters
+        self.prm = s._params(dt, max_iters, pressure_solver)
+        shifted = torch.from_numpy(self.x0.cpu().numpy() + np.asarray(shift, np.float32)).to(
+            self.device)
+        rho_t = self.splat(shifted).cpu().numpy()
+        tgt = np.empty(ncell, np.float32)
+        for i, n in enumerate(self.sides):
+            c0 = self.cell0[i]
+            tgt[c0:c0 + n ** 3] = gaussian_blur(rho_t[c0:c0 + n ** 3].reshape(n, n, n),
+                                                sigma).ravel()
+        self.target = torch.from_numpy(tgt).to(self.device)
+        nb = ctypes.c_int64()
+        _lib.check(s._L.gf_record_bytes(s._ctx, ctypes.byref(nb)), s._ctx, "gf_record_bytes")
+        self.record_bytes = nb.value
+        self.records = [torch.empty(nb.value, dtype=torch.uint8, device=self.device)
+                        for _ in range(k)]
+        self.labels_log = None
+        self.last_timing = {}
+
+    def scene_control(self, control: torch.Tensor, s: int) -> torch.Tensor:
+        """View of scene s's (3, n, n, n) block of a flat control (or gradient)."""
+        n = self.sides[s]
+        c0 = 3 * self.cell0[s]
+        return control[c0:c0 + 3 * n ** 3].view(3, n, n, n)
+
+    def scene_losses(self) -> np.ndarray:
+        """Per-scene losses at the current (final) particle state."""
+        rho = self.splat(self.solver._pos)
+        r = ((rho.double() - self.target.double()) ** 2).cpu().numpy()
+        return np.array([r[c0:c0 + n ** 3].sum() for c0, n in zip(self.cell0, self.sides)])
 
 
 class RolloutLoss(torch.autograd.Function):

@@ -123,9 +123,7 @@ __device__ __forceinline__ void scatter_corners(float fx, float fy, float fz, in
       }
 }
 
-__global__ void k_adj_g2p(AdjArgs a) {
-  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (q >= a.n) return;
+__device__ __forceinline__ void adj_g2p_item(const AdjArgs &a, int64_t q) {
   const float4 r0 = a.rec0[q];
   const float p[3] = {r0.x, r0.y, r0.z};
   const float inv_dx = 1.0f / a.dx;
@@ -167,17 +165,20 @@ __global__ void k_adj_g2p(AdjArgs a) {
   for (int d = 0; d < 3; ++d) a.xbar_acc[3 * q + d] = xb[d];
 }
 
+__global__ void k_adj_g2p(AdjArgs a) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q < a.n) adj_g2p_item(a, q);
+}
+
 // Gradient step adjoint, per cell: pbar_c = sum_f dU2_f/dp_c * ubar3_f over
 // the faces where k3_subtract_pressure_grad acts (both sides non-solid, one
 // fluid, interior face); p of a non-fluid cell is a constant 0.
-__global__ void k_adj_grad(AdjArgs a, float k) {
+__device__ __forceinline__ void adj_grad_item(const AdjArgs &a, int64_t c, float k) {
   const int nx = a.nx, ny = a.ny, nz = a.nz;
-  const int64_t n = (int64_t)nx * ny * nz;
-  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
-       c += (int64_t)gridDim.x * blockDim.x) {
+  {
     if (a.label[c] != 1) {
       a.div_io[c] = 0.0f;
-      continue;
+      return;
     }
     const int kk = (int)(c % nz);
     const int64_t rr = c / nz;
@@ -213,12 +214,17 @@ __global__ void k_adj_grad(AdjArgs a, float k) {
   }
 }
 
+__global__ void k_adj_grad(AdjArgs a, float k) {
+  const int64_t n = (int64_t)a.nx * a.ny * a.nz;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x)
+    adj_grad_item(a, c, k);
+}
+
 // Divergence + boundary + normalisation adjoint, per face.
-__global__ void k_adj_faces(AdjArgs a, float s) {
+__device__ __forceinline__ void adj_faces_item(const AdjArgs &a, int64_t t, float s) {
   const int nx = a.nx, ny = a.ny, nz = a.nz;
-  const int64_t nf = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nf;
-       t += (int64_t)gridDim.x * blockDim.x) {
+  {
     const int k = (int)(t % (nz + 1));
     const int64_t rr = t / (nz + 1);
     const int j = (int)(rr % (ny + 1)), i = (int)(rr / (ny + 1));
@@ -252,9 +258,15 @@ __global__ void k_adj_faces(AdjArgs a, float s) {
   }
 }
 
-__global__ void k_adj_p2g(AdjArgs a) {
-  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (q >= a.n) return;
+__global__ void k_adj_faces(AdjArgs a, float s) {
+  const int64_t nf = (int64_t)(a.nx + 1) * (a.ny + 1) * (a.nz + 1);
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nf;
+       t += (int64_t)gridDim.x * blockDim.x)
+    adj_faces_item(a, t, s);
+}
+
+
+__device__ __forceinline__ void adj_p2g_item(const AdjArgs &a, int64_t q) {
   const float4 r0 = a.rec0[q], r1 = a.rec1[q];
   const float vel[3] = {r1.x, r1.y, r1.z};
   const float inv_dx = 1.0f / a.dx;
@@ -284,6 +296,11 @@ __global__ void k_adj_p2g(AdjArgs a) {
     a.xbar_in[3 * s + d] = xb[d];
     a.vbar_in[3 * s + d] = vb[d];
   }
+}
+
+__global__ void k_adj_p2g(AdjArgs a) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q < a.n) adj_p2g_item(a, q);
 }
 
 // ---- APIC adjoint --------------------------------------------------------
@@ -329,9 +346,7 @@ __device__ __forceinline__ void apic_corners(float fx, float fy, float fz, int s
       }
 }
 
-__global__ void k_adj_g2p_apic(AdjArgs a) {
-  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (q >= a.n) return;
+__device__ __forceinline__ void adj_g2p_apic_item(const AdjArgs &a, int64_t q) {
   const float4 r0 = a.rec0[q];
   const float p[3] = {r0.x, r0.y, r0.z};
   const float dx = a.dx, inv_dx = 1.0f / dx;
@@ -388,9 +403,12 @@ __global__ void k_adj_g2p_apic(AdjArgs a) {
   for (int d = 0; d < 3; ++d) a.xbar_acc[3 * q + d] = xb[d];
 }
 
-__global__ void k_adj_p2g_apic(AdjArgs a) {
+__global__ void k_adj_g2p_apic(AdjArgs a) {
   const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (q >= a.n) return;
+  if (q < a.n) adj_g2p_apic_item(a, q);
+}
+
+__device__ __forceinline__ void adj_p2g_apic_item(const AdjArgs &a, int64_t q) {
   const float4 r0 = a.rec0[q], r1 = a.rec1[q], r2 = a.rec2[q], r3 = a.rec3[q];
   const float vel[3] = {r1.x, r1.y, r1.z};
   const float C[3][3] = {{r1.w, r2.x, r2.y}, {r2.z, r2.w, r3.x}, {r3.y, r3.z, r3.w}};
@@ -442,6 +460,65 @@ __global__ void k_adj_p2g_apic(AdjArgs a) {
   for (int c = 0; c < 3; ++c)
 #pragma unroll
     for (int d = 0; d < 3; ++d) a.Cbar_in[9 * s + 3 * c + d] = Cb[c][d];
+}
+
+__global__ void k_adj_p2g_apic(AdjArgs a) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q < a.n) adj_p2g_apic_item(a, q);
+}
+
+// ---- batches: each item finds its scene and runs the single-grid body on
+// the scene's view of the concatenated arrays (particles stay global).
+__device__ __forceinline__ AdjArgs adj_view(const AdjArgs &a, const SegRow &r) {
+  AdjArgs v = a;
+  const int64_t off[3] = {r.fu0, r.fv0, r.fw0};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    v.m[c] = a.m[c] + off[c];
+    v.un[c] = a.un[c] + off[c];
+    v.u3[c] = a.u3[c] + off[c];
+    v.ubar3[c] = a.ubar3[c] + off[c];
+    v.qbar[c] = a.qbar[c] + off[c];
+    v.mbar[c] = a.mbar[c] + off[c];
+  }
+  v.label = a.label + r.cell0;
+  v.div_io = a.div_io + r.cell0;
+  v.lambda = a.lambda + r.cell0;
+  v.dx = r.dx;
+  v.dom0 = r.dom0; v.dom1 = r.dom1; v.dom2 = r.dom2;
+  v.nx = r.nx; v.ny = r.ny; v.nz = r.nz;
+  return v;
+}
+
+template <int KIND>  // 0 g2p, 1 p2g, 2 g2p apic, 3 p2g apic
+__global__ void kb_adj_particles(AdjArgs a, SegIndex sx) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= a.n) return;
+  const AdjArgs v = adj_view(a, sx.row[seg_find(sx.part0, sx.n, q)]);
+  if (KIND == 0) adj_g2p_item(v, q);
+  if (KIND == 1) adj_p2g_item(v, q);
+  if (KIND == 2) adj_g2p_apic_item(v, q);
+  if (KIND == 3) adj_p2g_apic_item(v, q);
+}
+
+__global__ void kb_adj_grad(AdjArgs a, SegIndex sx, int64_t ncell, float rho, float dt) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncell;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    const SegRow r = sx.row[seg_find(sx.cell0, sx.n, c)];
+    float k = rho * r.dx;  // dt / (rho dx) per scene
+    k = dt / k;
+    adj_grad_item(adj_view(a, r), c - r.cell0, k);
+  }
+}
+
+__global__ void kb_adj_faces(AdjArgs a, SegIndex sx, int64_t nslot, float rho, float dt) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nslot;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const SegRow r = sx.row[seg_find(sx.fslot0, sx.n, t)];
+    float s = rho * r.dx;  // (rho dx) / dt per scene
+    s = s / dt;
+    adj_faces_item(adj_view(a, r), t - r.fslot0, s);
+  }
 }
 
 // ---- density splat (meshing/surface.py:14-43) and control sampling -------
@@ -511,6 +588,78 @@ __global__ void k_sample_cells_adj(const float *__restrict__ pos, int64_t n, flo
       if (cs.idx[k] >= 0) atomicAdd(&grid3_bar[d * ncell + cs.idx[k]], cs.w[k] * vel_bar[3 * q + d]);
 }
 
+// Over a batch: particle i belongs to the scene of the particle prefix, the
+// cell arrays are the scenes' arrays concatenated, and a control field holds
+// each scene's (3, nx, ny, nz) block at 3 * cell0.
+__global__ void kb_splat(const float *__restrict__ pos, int64_t n, SegIndex sx, float *rho) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const SegRow r = sx.row[seg_find(sx.part0, sx.n, q)];
+  Corners cs;
+  scatter_corners(__fdiv_rn(pos[3 * q], r.dx) - 0.5f, __fdiv_rn(pos[3 * q + 1], r.dx) - 0.5f,
+                  __fdiv_rn(pos[3 * q + 2], r.dx) - 0.5f, r.nx, r.ny, r.nz, 1.0f / r.dx, cs);
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    if (cs.idx[k] >= 0) atomicAdd(&rho[r.cell0 + cs.idx[k]], cs.w[k]);
+}
+
+__global__ void kb_splat_adj(const float *__restrict__ pos, int64_t n, SegIndex sx,
+                             const float *__restrict__ rho_bar, float *pos_bar) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const SegRow r = sx.row[seg_find(sx.part0, sx.n, q)];
+  Corners cs;
+  scatter_corners(__fdiv_rn(pos[3 * q], r.dx) - 0.5f, __fdiv_rn(pos[3 * q + 1], r.dx) - 0.5f,
+                  __fdiv_rn(pos[3 * q + 2], r.dx) - 0.5f, r.nx, r.ny, r.nz, 1.0f / r.dx, cs);
+  float xb[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    if (cs.idx[k] < 0) continue;
+    const float rb = rho_bar[r.cell0 + cs.idx[k]];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) xb[d] += cs.dw[k][d] * rb;
+  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) pos_bar[3 * q + d] = xb[d];
+}
+
+__global__ void kb_sample_cells(const float *__restrict__ grid3, const float *__restrict__ pos,
+                                int64_t n, SegIndex sx, float *vel) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const SegRow r = sx.row[seg_find(sx.part0, sx.n, q)];
+  Corners cs;
+  scatter_corners(__fdiv_rn(pos[3 * q], r.dx) - 0.5f, __fdiv_rn(pos[3 * q + 1], r.dx) - 0.5f,
+                  __fdiv_rn(pos[3 * q + 2], r.dx) - 0.5f, r.nx, r.ny, r.nz, 1.0f / r.dx, cs);
+  const int64_t nc = (int64_t)r.nx * r.ny * r.nz;
+  const float *g = grid3 + 3 * r.cell0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    float acc = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if (cs.idx[k] >= 0) acc += cs.w[k] * g[d * nc + cs.idx[k]];
+    vel[3 * q + d] = acc;
+  }
+}
+
+__global__ void kb_sample_cells_adj(const float *__restrict__ pos, int64_t n, SegIndex sx,
+                                    const float *__restrict__ vel_bar, float *grid3_bar) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const SegRow r = sx.row[seg_find(sx.part0, sx.n, q)];
+  Corners cs;
+  scatter_corners(__fdiv_rn(pos[3 * q], r.dx) - 0.5f, __fdiv_rn(pos[3 * q + 1], r.dx) - 0.5f,
+                  __fdiv_rn(pos[3 * q + 2], r.dx) - 0.5f, r.nx, r.ny, r.nz, 1.0f / r.dx, cs);
+  const int64_t nc = (int64_t)r.nx * r.ny * r.nz;
+  float *g = grid3_bar + 3 * r.cell0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if (cs.idx[k] >= 0) atomicAdd(&g[d * nc + cs.idx[k]], cs.w[k] * vel_bar[3 * q + d]);
+}
+
 // ---- record layout -------------------------------------------------------
 struct RecordLayout {
   size_t rec0, rec1, rec2, rec3, order, m[3], un[3], u3[3], label, bytes;
@@ -521,8 +670,7 @@ static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 static RecordLayout layout(const Ctx *c) {
   RecordLayout L{};
   const int64_t n = c->p.n;
-  const int64_t fsz[3] = {(int64_t)(c->nx + 1) * c->ny * c->nz, (int64_t)c->nx * (c->ny + 1) * c->nz,
-                          (int64_t)c->nx * c->ny * (c->nz + 1)};
+  const int64_t fsz[3] = {c->nu, c->nv, c->nw};  // all scenes' faces of a batch
   size_t o = 0;
   L.rec0 = o; o = align256(o + n * 16);
   L.rec1 = o; o = align256(o + n * 16);
@@ -538,7 +686,7 @@ static RecordLayout layout(const Ctx *c) {
 }
 
 static int adj_reserve(Ctx *c) {
-  const int64_t nf = (int64_t)(c->nx + 1) * (c->ny + 1) * (c->nz + 1);  // >= each component
+  const int64_t nf = c->nfslot;  // face slots: >= the faces of each component
   const int64_t need_f = 9 * nf, need_p = 3 * (c->p.n > 0 ? c->p.n : 1);
   if (c->adj_faces && c->adj_faces_n >= need_f && c->adj_part_n >= need_p) return GF_OK;
   if (c->adj_faces) cudaFree(c->adj_faces);
@@ -573,7 +721,6 @@ extern "C" {
 int gf_record_bytes(void *ctx, int64_t *bytes) {
   Ctx *c = reinterpret_cast<Ctx *>(ctx);
   if (!c || !bytes) return GF_INVALID_ARG;
-  if (c->nseg) return gf::fail(c, GF_INVALID_ARG, "gf_record_bytes: single-scene contexts only");
   if (!c->bound) return gf::fail(c, GF_INVALID_ARG, "gf_record_bytes: buffers not bound");
   *bytes = (int64_t)gf::layout(c).bytes;
   return GF_OK;
@@ -582,7 +729,6 @@ int gf_record_bytes(void *ctx, int64_t *bytes) {
 int gf_step_record(void *ctx, const gf_step_params *prm, void *record) {
   Ctx *c = reinterpret_cast<Ctx *>(ctx);
   if (!c || !prm || !record) return GF_INVALID_ARG;
-  if (c->nseg) return gf::fail(c, GF_INVALID_ARG, "gf_step_record: single-scene contexts only");
   if (!gf::adjointable(prm))
     return gf::fail(c, GF_INVALID_ARG, "the adjoint substep supports PIC (flip_blend 0) and APIC");
   int e = gf_step(ctx, prm);
@@ -591,9 +737,7 @@ int gf_step_record(void *ctx, const gf_step_params *prm, void *record) {
   char *r = static_cast<char *>(record);
   cudaStream_t st = c->stream;
   const int64_t n = c->p.n;
-  const int64_t fsz[3] = {(int64_t)(c->nx + 1) * c->ny * c->nz,
-                          (int64_t)c->nx * (c->ny + 1) * c->nz,
-                          (int64_t)c->nx * c->ny * (c->nz + 1)};
+  const int64_t fsz[3] = {c->nu, c->nv, c->nw};
   const float *mw[3] = {c->f.uw, c->f.vw, c->f.ww}, *us[3] = {c->f.us, c->f.vs, c->f.ws},
               *u3[3] = {c->f.u, c->f.v, c->f.w};
   // 6 particle/label copies + (m, un, u3) per component
@@ -631,7 +775,7 @@ static int step_adjoint(Ctx *c, const gf_step_params *prm, const void *record,
   const char *r = static_cast<const char *>(record);
   cudaStream_t st = c->stream;
   const int64_t n = c->p.n;
-  const int64_t nfmax = (int64_t)(c->nx + 1) * (c->ny + 1) * (c->nz + 1);
+  const int64_t nfmax = c->nfslot;
   AdjArgs a{};
   a.rec0 = reinterpret_cast<const float4 *>(r + L.rec0);
   a.rec1 = reinterpret_cast<const float4 *>(r + L.rec1);
@@ -669,8 +813,14 @@ static int step_adjoint(Ctx *c, const gf_step_params *prm, const void *record,
   if ((e = check_cuda(c, cudaMemsetAsync(c->adj_faces, 0, 3 * nfmax * 4, st), "zero ubar")))
     return e;
   const unsigned gp = (unsigned)((n + 255) / 256);
+  const bool batch = c->nseg > 0;
+  const SegIndex sx = batch ? seg_index(c) : SegIndex{};
   if (n > 0) {
-    if (apic)
+    if (batch && apic)
+      kb_adj_particles<2><<<gp, 256, 0, st>>>(a, sx);
+    else if (batch)
+      kb_adj_particles<0><<<gp, 256, 0, st>>>(a, sx);
+    else if (apic)
       k_adj_g2p_apic<<<gp, 256, 0, st>>>(a);
     else
       k_adj_g2p<<<gp, 256, 0, st>>>(a);
@@ -686,7 +836,10 @@ static int step_adjoint(Ctx *c, const gf_step_params *prm, const void *record,
   const unsigned gc = (unsigned)((c->ncell + 255) / 256 < (int64_t)c->num_sms * 16
                                      ? (c->ncell + 255) / 256
                                      : (int64_t)c->num_sms * 16);
-  k_adj_grad<<<gc, 256, 0, st>>>(a, kk);
+  if (batch)
+    kb_adj_grad<<<gc, 256, 0, st>>>(a, sx, c->ncell, prm->rho, prm->dt);
+  else
+    k_adj_grad<<<gc, 256, 0, st>>>(a, kk);
   c->launches++;
   // A lambda = pbar with the same SPD operator (labels fixed)
   gf_step_params sp = *prm;
@@ -698,10 +851,17 @@ static int step_adjoint(Ctx *c, const gf_step_params *prm, const void *record,
   const unsigned gf_ = (unsigned)((nfmax + 255) / 256 < (int64_t)c->num_sms * 16
                                       ? (nfmax + 255) / 256
                                       : (int64_t)c->num_sms * 16);
-  k_adj_faces<<<gf_, 256, 0, st>>>(a, s);
+  if (batch)
+    kb_adj_faces<<<gf_, 256, 0, st>>>(a, sx, c->nfslot, prm->rho, prm->dt);
+  else
+    k_adj_faces<<<gf_, 256, 0, st>>>(a, s);
   c->launches++;
   if (n > 0) {
-    if (apic)
+    if (batch && apic)
+      kb_adj_particles<3><<<gp, 256, 0, st>>>(a, sx);
+    else if (batch)
+      kb_adj_particles<1><<<gp, 256, 0, st>>>(a, sx);
+    else if (apic)
       k_adj_p2g_apic<<<gp, 256, 0, st>>>(a);
     else
       k_adj_p2g<<<gp, 256, 0, st>>>(a);
@@ -719,7 +879,6 @@ int gf_step_adjoint(void *ctx, const gf_step_params *prm, const void *record,
   Ctx *c = reinterpret_cast<Ctx *>(ctx);
   if (!c || !prm || !record || !xbar_out || !vbar_out || !xbar_in || !vbar_in)
     return GF_INVALID_ARG;
-  if (c->nseg) return gf::fail(c, GF_INVALID_ARG, "gf_step_adjoint: single-scene contexts only");
   if (!c->bound) return gf::fail(c, GF_INVALID_ARG, "gf_step_adjoint: buffers not bound");
   if (!gf::pic_only(prm))
     return gf::fail(c, GF_INVALID_ARG,
@@ -736,8 +895,6 @@ int gf_step_adjoint_apic(void *ctx, const gf_step_params *prm, const void *recor
   if (!c || !prm || !record || !xbar_out || !vbar_out || !Cbar_out || !xbar_in || !vbar_in ||
       !Cbar_in)
     return GF_INVALID_ARG;
-  if (c->nseg)
-    return gf::fail(c, GF_INVALID_ARG, "gf_step_adjoint_apic: single-scene contexts only");
   if (!c->bound) return gf::fail(c, GF_INVALID_ARG, "gf_step_adjoint_apic: buffers not bound");
   if (prm->transfer != GF_APIC)
     return gf::fail(c, GF_INVALID_ARG, "gf_step_adjoint_apic needs an APIC substep");
@@ -748,11 +905,16 @@ int gf_step_adjoint_apic(void *ctx, const gf_step_params *prm, const void *recor
 int gf_density_splat(void *ctx, const float *pos, int64_t n, float *rho) {
   Ctx *c = reinterpret_cast<Ctx *>(ctx);
   if (!c || (n > 0 && !pos) || !rho) return GF_INVALID_ARG;
-  if (c->nseg) return gf::fail(c, GF_INVALID_ARG, "single-scene contexts only");
   int e = gf::check_cuda(c, cudaMemsetAsync(rho, 0, c->ncell * 4, c->stream), "zero rho");
   if (e || n == 0) return e;
-  gf::k_splat<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(pos, n, c->dx, c->nx, c->ny,
-                                                                  c->nz, rho);
+  if (c->nseg) {
+    if (n != c->p.n) return gf::fail(c, GF_INVALID_ARG, "batch splat: n must be the bound count");
+    gf::kb_splat<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(pos, n, gf::seg_index(c),
+                                                                     rho);
+  } else {
+    gf::k_splat<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(pos, n, c->dx, c->nx, c->ny,
+                                                                    c->nz, rho);
+  }
   c->launches++;
   return gf::check_launch(c, "gf_density_splat");
 }
@@ -761,10 +923,15 @@ int gf_density_splat_adjoint(void *ctx, const float *pos, int64_t n, const float
                              float *pos_bar) {
   Ctx *c = reinterpret_cast<Ctx *>(ctx);
   if (!c || (n > 0 && (!pos || !pos_bar)) || !rho_bar) return GF_INVALID_ARG;
-  if (c->nseg) return gf::fail(c, GF_INVALID_ARG, "single-scene contexts only");
   if (n == 0) return GF_OK;
-  gf::k_splat_adj<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(pos, n, c->dx, c->nx, c->ny,
-                                                                      c->nz, rho_bar, pos_bar);
+  if (c->nseg) {
+    if (n != c->p.n) return gf::fail(c, GF_INVALID_ARG, "batch splat: n must be the bound count");
+    gf::kb_splat_adj<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
+        pos, n, gf::seg_index(c), rho_bar, pos_bar);
+  } else {
+    gf::k_splat_adj<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
+        pos, n, c->dx, c->nx, c->ny, c->nz, rho_bar, pos_bar);
+  }
   c->launches++;
   return gf::check_launch(c, "gf_density_splat_adjoint");
 }
@@ -772,10 +939,15 @@ int gf_density_splat_adjoint(void *ctx, const float *pos, int64_t n, const float
 int gf_sample_cells(void *ctx, const float *grid3, const float *pos, int64_t n, float *vel) {
   Ctx *c = reinterpret_cast<Ctx *>(ctx);
   if (!c || !grid3 || (n > 0 && (!pos || !vel))) return GF_INVALID_ARG;
-  if (c->nseg) return gf::fail(c, GF_INVALID_ARG, "single-scene contexts only");
   if (n == 0) return GF_OK;
-  gf::k_sample_cells<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(grid3, pos, n, c->dx,
-                                                                         c->nx, c->ny, c->nz, vel);
+  if (c->nseg) {
+    if (n != c->p.n) return gf::fail(c, GF_INVALID_ARG, "batch sampling: n must be the bound count");
+    gf::kb_sample_cells<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
+        grid3, pos, n, gf::seg_index(c), vel);
+  } else {
+    gf::k_sample_cells<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
+        grid3, pos, n, c->dx, c->nx, c->ny, c->nz, vel);
+  }
   c->launches++;
   return gf::check_launch(c, "gf_sample_cells");
 }
@@ -784,12 +956,17 @@ int gf_sample_cells_adjoint(void *ctx, const float *pos, int64_t n, const float 
                             float *grid3_bar) {
   Ctx *c = reinterpret_cast<Ctx *>(ctx);
   if (!c || !grid3_bar || (n > 0 && (!pos || !vel_bar))) return GF_INVALID_ARG;
-  if (c->nseg) return gf::fail(c, GF_INVALID_ARG, "single-scene contexts only");
   int e = gf::check_cuda(c, cudaMemsetAsync(grid3_bar, 0, 3 * c->ncell * 4, c->stream),
                          "zero grid bar");
   if (e || n == 0) return e;
-  gf::k_sample_cells_adj<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
-      pos, n, c->dx, c->nx, c->ny, c->nz, vel_bar, grid3_bar);
+  if (c->nseg) {
+    if (n != c->p.n) return gf::fail(c, GF_INVALID_ARG, "batch sampling: n must be the bound count");
+    gf::kb_sample_cells_adj<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
+        pos, n, gf::seg_index(c), vel_bar, grid3_bar);
+  } else {
+    gf::k_sample_cells_adj<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
+        pos, n, c->dx, c->nx, c->ny, c->nz, vel_bar, grid3_bar);
+  }
   c->launches++;
   return gf::check_launch(c, "gf_sample_cells_adjoint");
 }

@@ -201,12 +201,16 @@ int gf_step_adjoint_apic(void *ctx, const gf_step_params *prm, const void *recor
                          float *xbar_in, float *vbar_in, float *Cbar_in);
 /* Cell-centred trilinear density splat of unit-mass particles into rho
  * (nx,ny,nz) (k_density_scatter, meshing/surface.py:14-43) and its adjoint
- * with respect to the positions. */
+ * with respect to the positions.  On a batch context, n is the bound
+ * particle count (scene after scene) and rho the scenes' cell arrays
+ * concatenated. */
 int gf_density_splat(void *ctx, const float *pos, int64_t n, float *rho);
 int gf_density_splat_adjoint(void *ctx, const float *pos, int64_t n, const float *rho_bar,
                              float *pos_bar);
 /* Velocities sampled from a cell-centred 3-component field (3,nx,ny,nz) with
- * the same weights, and the adjoint with respect to the field (a scatter). */
+ * the same weights, and the adjoint with respect to the field (a scatter).
+ * On a batch context the field holds each scene's (3,nx,ny,nz) block at
+ * 3 * cell0 and n is the bound particle count. */
 int gf_sample_cells(void *ctx, const float *grid3, const float *pos, int64_t n, float *vel);
 int gf_sample_cells_adjoint(void *ctx, const float *pos, int64_t n, const float *vel_bar,
                             float *grid3_bar);
@@ -221,8 +225,8 @@ int gf_sample_cells_adjoint(void *ctx, const float *pos, int64_t n, const float 
  * cells (label, p, div), u-, v- and w-shaped faces, particles (the caller
  * passes each scene's particle count).  gf_batch_plan returns that layout
  * (per scene, nullable) and the totals without touching a GPU; solid
- * velocities must be NULL (static solids).  The adjoint and the density /
- * control-sampling calls take single-scene contexts only. */
+ * velocities must be NULL (static solids).  The adjoint, density-splat and
+ * control-sampling calls work on batches too (one launch per kernel). */
 typedef struct gf_scene_layout {
   int64_t cell0;           /* first cell of the scene in cell arrays */
   int64_t fu0, fv0, fw0;   /* first u, v, w face in the face arrays */
