@@ -9,10 +9,14 @@ forces/BC/divergence, pressure, projection, G2P + advection) of the evolving
 scene.
 
   value   substeps/s with the pressure solved by FP32 PCG with FP64 residual
-          replacement to a true relative residual of 1e-8 (inputs resident in
+          replacement to a true relative residual of 1e-8, preconditioned by
+          two sweeps of tile-local symmetric Gauss-Seidel (inputs resident in
           HBM; device time over the timed steps, max over ranks).
-  plain   the same substeps with plain FP32 PCG asked for the same 1e-8
-          (recursive residual), with the true residual it actually reached.
+  refined_jacobi  the same refined solve with the reference's Jacobi
+          preconditioner (the like-for-like comparison with plain).
+  plain   the same substeps with plain FP32 PCG (the reference's Jacobi
+          preconditioner) asked for the same 1e-8 (recursive residual), with
+          the true residual it actually reached.
   e2e     the same substep through the C-ABI-backed public API with the
           particle state in pinned HOST memory: host->device copy of the
           state, step, device->host copy of the state, every step.
@@ -53,8 +57,10 @@ TOL = 1e-8
 MAX_ITERS = 4000
 SPHERE = ((0.7, 0.2, 0.5), 0.12)
 BOX = ((0.0, 0.0, 0.0), (0.4, 0.6, 1.0))
+SGS_SWEEPS = 2  # tile-local symmetric Gauss-Seidel sweeps of the headline solve
 WORKLOAD = ("APIC dam break + sphere obstacle, 128^3 (dx=1/128), 8 ppc -> 3,969,024 "
-            "particles, dt=1/480, pressure: FP32 PCG + FP64 residual replacement to 1e-8")
+            "particles, dt=1/480, pressure: FP32 PCG + FP64 residual replacement to 1e-8, "
+            "tile-local symmetric Gauss-Seidel preconditioner (2 sweeps)")
 
 
 def peaks():
@@ -85,7 +91,7 @@ class ClockSampler:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=self.f, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
@@ -120,10 +126,11 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------- scene
-def make_solver(gf, device, graphs=True):
+def make_solver(gf, device, graphs=True, precond="tile_sgs"):
     from gpufluid_b200 import scene
     s = gf.FlipSolver3D(GRID, GRID, GRID, transfer_mode="apic", flip_blend=0.95,
-                        device=device, pressure_tol=TOL, enable_cuda_graphs=graphs)
+                        device=device, pressure_tol=TOL, enable_cuda_graphs=graphs,
+                        pcg_preconditioner=precond, pcg_sgs_sweeps=SGS_SWEEPS)
     s.add_solid_from_sdf(scene.sdf_sphere(s.cell_centers_np(), *SPHERE))
     s.seed_box(*BOX)
     return s
@@ -218,15 +225,17 @@ def pressure_error_fp64(torch, s, iters=6000) -> float:
     return float(torch.linalg.vector_norm(p32 - x) / torch.linalg.vector_norm(x))
 
 
-def pcg_bytes(st) -> float:
+def pcg_bytes(st, sgs_sweeps=0) -> float:
     """Algorithmic bytes of one PCG launch: per fluid cell 14 B of set-up,
     48 B per iteration (phase A: z, d_old, code in; d_new, Ad out; phase B:
     d_new, Ad, x, r, code in; x, r, z out), 48 B per FP64 residual
     replacement (x64, x, code, b in; x64, x, r, z out); 2 B of stencil code
-    per active-tile cell and per phase."""
+    per active-tile cell and per phase.  A tile-local symmetric Gauss-Seidel
+    preconditioner adds 12 B per fluid cell per sweep (each half-sweep reads
+    r and writes z on its colour and reads z of the other)."""
     nf, na = st["n_fluid"], st["n_active_tiles"] * 512
     it, rep = st["iters"], st["replacements"]
-    return float(nf * (14 + 48 * it + 48 * rep) + na * 2 * (1 + 2 * it))
+    return float(nf * (14 + (48 + 12 * sgs_sweeps) * it + 48 * rep) + na * 2 * (1 + 2 * it))
 
 
 def stage_bytes(P, nf, ncell_active, F):
@@ -495,7 +504,9 @@ def run_ours(args):
     torch.cuda.synchronize()
     snap = snapshot(s)
 
-    # ---- plain FP32 PCG from the same state (same 1e-8 target, recursive residual)
+    # ---- plain FP32 PCG from the same state (same 1e-8 target, recursive
+    # residual), with the reference's Jacobi preconditioner
+    s.pcg_preconditioner = "jacobi"
     s.step(DT, pressure_iters=MAX_ITERS, pressure_solver="pcg")  # capture its graph
     torch.cuda.synchronize()
     restore(s, snap)
@@ -505,6 +516,17 @@ def run_ours(args):
     plain_stats = s.pressure_stats()
     plain_true = true_relres(s)
     plain_err = pressure_error_fp64(torch, s)
+    # ---- the refined solve with the Jacobi preconditioner (like for like)
+    restore(s, snap)
+    s.step(DT, pressure_iters=MAX_ITERS, pressure_solver="pcg_refined")  # capture
+    torch.cuda.synchronize()
+    restore(s, snap)
+    barrier()
+    torch.cuda.synchronize()
+    ms_refj, _ = timed_steps(torch, s, args.steps, "pcg_refined")
+    refj_stats = s.pressure_stats()
+    refj_err = pressure_error_fp64(torch, s)
+    s.pcg_preconditioner = "tile_sgs"
     restore(s, snap)
 
     # ---- refined (the value)
@@ -531,7 +553,7 @@ def run_ours(args):
         st = s.pressure_stats()
         stage.append(t)
         pcg_ms.append(t[7])
-        pcg_b.append(pcg_bytes(st))
+        pcg_b.append(pcg_bytes(st, SGS_SWEEPS))
     s._L.gf_enable_timing(s._ctx, 0)
     s._prof.enabled = False
     stage_ms = np.mean(np.array(stage), axis=0)
@@ -589,6 +611,7 @@ def run_ours(args):
             "data": "synthetic (seeded seed_box lattice of the reference, sphere SDF obstacle)",
             "config": {"workload": WORKLOAD, "grid": GRID, "particles": P, "transfer": "apic",
                        "dt": DT, "pressure": "pcg_refined", "tol": TOL,
+                       "preconditioner": f"tile-local symmetric Gauss-Seidel, {SGS_SWEEPS} sweeps",
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2_policy": "inputs larger than L2: particle state "
                                     f"{P * 64 / 1e6:.0f} MB + MAC grids {F * 4 * 3 / 1e6:.0f} MB "
@@ -604,10 +627,14 @@ def run_ours(args):
                         "true_relres_fp64": ref_true,
                         "pressure_rel_error_vs_fp64": ref_err,
                         "time_vs_plain": round(ms_ref / ms_plain, 3)},
+            "refined_jacobi": {"ms_per_step": round(ms_refj, 4), "iters_last": refj_stats["iters"],
+                               "pressure_rel_error_vs_fp64": refj_err,
+                               "time_vs_plain": round(ms_refj / ms_plain, 3)},
             "e2e": {"value": round(world * 1000.0 / ms_e2e, 3), "unit": "substeps/s",
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(h2d)},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": "k_pcg<double,true> (persistent cooperative)",
+            "roofline": {"bound": "hbm", "kernel": "k_pcg_smem<double,true,true> (persistent cooperative, "
+                                   "shared-memory resident)",
                          "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                          "frac": round(achieved / hbm, 4), "traffic": PCG_DRAM_BYTES,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
@@ -689,7 +716,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

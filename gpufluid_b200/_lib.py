@@ -59,6 +59,7 @@ class StepParams(ctypes.Structure):
 
 GF_FLAG_GLOBAL_PCG = 1
 GF_FLAG_TRACE = 2
+GF_FLAG_SGS_SHIFT = 2  # bits 2-3: tile-local symmetric Gauss-Seidel sweeps
 GF_NOALLOC_MAX_CELLS = 2097152
 
 

@@ -50,6 +50,10 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
   return v;
 }
 
+__device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
 constexpr int SM_MAXG = 160;      // blocks (one per SM)
 
 struct GridSync {
@@ -219,17 +223,20 @@ __constant__ int c_ring_a[6] = {10, 10, 100, 100, 100, 100};
 __constant__ int c_ring_b[6] = {1, 1, 1, 1, 10, 10};
 __constant__ int c_ring_delta[6] = {800, -800, 80, -80, 8, -8};
 
-template <typename Remote>
+// MODE 0 fills every face, 1 only the in-block ones, 2 only another block's.
+template <int MODE = 0, typename Remote>
 __device__ __forceinline__ void ring_fill(float *s_zb, const int *s_nbr, int nt, int b0, int b1,
                                           Remote remote) {
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int f = wid; f < nt * 6; f += SM_THREADS / 32) {
     const int sl = s_nbr[f];
     if (sl < 0) continue;
+    const bool local = sl >= b0 && sl < b1;
+    if ((MODE == 1 && !local) || (MODE == 2 && local)) continue;
     const int tl = f / 6, dir = f - tl * 6;
     const int base = c_ring_base[dir], ca = c_ring_a[dir], cb = c_ring_b[dir];
     float *dst = s_zb + tl * 1000;
-    if (sl >= b0 && sl < b1) {
+    if (local) {
       const float *src = s_zb + (sl - b0) * 1000 + c_ring_delta[dir];
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
@@ -342,13 +349,17 @@ __device__ void partition_slots(const int32_t *__restrict__ cost, int na, int ma
   __syncthreads();
 }
 
-template <typename Acc, bool REF>
+template <typename Acc, bool REF, bool SGS>
 __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   using Cfg = SmemCfg<REF>;
   constexpr int MAXT = Cfg::MAXT, MAXJ = Cfg::MAXJ;
   static_assert(MAXJ * 3 <= 32, "diagonal pack");
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_nbr[MAXT * 6];
+  __shared__ int s_nbl[SM_MAXG];         // SGS: distinct neighbouring blocks
+  __shared__ unsigned s_nbbits[SM_MAXG / 32];
+  __shared__ int s_nnb;
+  __shared__ float s_rtab[16];  // SGS, by (fluid << 3 | count): 0, or 1 / max(count, 1)
   __shared__ uint8_t s_mask[MAXT];
   __shared__ int s_bounds[SM_MAXG + 1];
   __shared__ Acc sh[36 * 4];
@@ -389,6 +400,8 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
 
   for (int i = threadIdx.x; i < nt * 6; i += blockDim.x) s_nbr[i] = a.nbr[(int64_t)b0 * 6 + i];
   for (int i = threadIdx.x; i < nt * 1000; i += blockDim.x) s_zb[i] = 0.f;
+  if (threadIdx.x < 16)
+    s_rtab[threadIdx.x] = threadIdx.x < 8 ? 0.f : 1.0f / fmaxf((float)(threadIdx.x - 8), 1.0f);
   __syncthreads();
   for (int t = threadIdx.x; t < nt; t += blockDim.x) {
     int m = 0;
@@ -411,6 +424,28 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
     }
     s_rdiag[w] = dg;
   }
+  if (SGS) {
+    // the blocks owning a remote face: the last block whose first slot is <= sl
+    if (threadIdx.x < SM_MAXG / 32) s_nbbits[threadIdx.x] = 0u;
+    __syncthreads();
+    for (int f = threadIdx.x; f < nt * 6; f += blockDim.x) {
+      const int sl = s_nbr[f];
+      if (sl < 0 || (sl >= b0 && sl < b1)) continue;
+      int lo = 0, hi = G;
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (s_bounds[mid] <= sl) lo = mid; else hi = mid;
+      }
+      atomicOr(&s_nbbits[lo >> 5], 1u << (lo & 31));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int cnt = 0;
+      for (int g = 0; g < G; ++g)
+        if ((s_nbbits[g >> 5] >> (g & 31)) & 1u) s_nbl[cnt++] = g;
+      s_nnb = cnt;
+    }
+  }
   __syncthreads();
 
 #define HR(par) ((par) ? a.hr1 : a.hr0)
@@ -432,11 +467,14 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       fmask |= 1u << j;
       dpack |= (unsigned)((code >> CODE_DIAG_SHIFT) & 7) << (3 * j);
       b = a.sign * a.bdiv[q0 + L];
-      s_zb[tl * 1000 + pc] = b / diagz_of(code);
+      s_zb[tl * 1000 + pc] =
+          SGS ? b * s_rtab[8 | ((code >> CODE_DIAG_SHIFT) & 7)] : b / diagz_of(code);
       if (is_halo(L, s_mask)) {
         hmask |= 1u << j;
-        HR(0)[q0 + L] = b;
-        HS(0)[q0 + L] = 0.f;
+        if (!SGS) {
+          HR(0)[q0 + L] = b;
+          HS(0)[q0 + L] = 0.f;
+        }
       }
     }
     s_r[L] = b;
@@ -446,12 +484,98 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
     if (REF) s_x64[L] = 0.0;
   }
   __syncthreads();
-  // ring fill of z0: remote z0 = M b (b is read-only input, no barrier needed)
-  ring_fill(s_zb, s_nbr, nt, b0, b1, [&](int ri, int64_t qn) -> float {
-    const uint8_t dg = s_rdiag[ri];
-    return dg ? (a.sign * a.bdiv[qn]) / (float)dg : 0.f;
-  });
-  __syncthreads();
+
+  // ---- tile-local symmetric Gauss-Seidel preconditioner (SGS): z = M r with
+  // M^-1 = sweeps of red-black symmetric Gauss-Seidel on each 8^3 tile from
+  // z = 0, the tile's neighbours held at 0 (the diagonal block of A per tile;
+  // symmetric positive definite, so CG applies).  The first red half-sweep
+  // (z = r/D) is the z = r/D every caller writes for all fluid cells; then
+  // per sweep black, red.  Callers also zero the boxes' rings, and non-fluid
+  // cells hold 0, so a half-sweep is the branch-free six-neighbour sum with a
+  // per-cell factor (0 on non-fluid cells).  It maps thread t to the
+  // (t & 255)-th cell of the colour in tiles (t >> 8) + 4i, so all threads
+  // work.  The result is published on the halo cells and each block releases
+  // its flag; the ring of another block's tile is read after that block's
+  // flag has been acquired.
+  unsigned long long zep = 0;  // z publications, the same sequence in every block
+  float *const HZ = a.hr0;
+  auto half_sweep = [&](int c) {  // z = (r + in-tile fluid neighbours' z) / D, colour c
+    const int k = threadIdx.x & 255;
+    const int li = k >> 5, lj = (k >> 2) & 7;
+    const int lk = 2 * (k & 3) + ((li + lj + c) & 1);
+    const int lc = (li * 8 + lj) * 8 + lk;
+    const int pcc = pad_of(lc);
+    for (int tl = threadIdx.x >> 8; tl < nt; tl += 4) {
+      const int L = tl * 512 + lc;
+      const unsigned code = s_code[L];
+      float *zp = s_zb + tl * 1000 + pcc;
+      float acc = s_r[L];
+      acc = acc + zp[-100];
+      acc = acc + zp[100];
+      acc = acc + zp[-10];
+      acc = acc + zp[10];
+      acc = acc + zp[-1];
+      acc = acc + zp[1];
+      *zp = acc * s_rtab[((code >> 12) & 8) | ((code >> CODE_DIAG_SHIFT) & 7)];
+    }
+  };
+  auto zero_rings = [&]() {  // faces with a neighbouring tile (the others stay 0)
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int f = wid; f < nt * 6; f += SM_THREADS / 32) {
+      if (s_nbr[f] < 0) continue;
+      const int tl = f / 6, dir = f - tl * 6;
+      const int base = c_ring_base[dir], ca = c_ring_a[dir], cb = c_ring_b[dir];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int p = lane + 32 * h;
+        s_zb[tl * 1000 + base + ((p >> 3) + 1) * ca + ((p & 7) + 1) * cb] = 0.f;
+      }
+    }
+  };
+  // Callers have written z = r/D on their fluid cells, zeroed the rings
+  // (zero_rings) and passed a barrier.
+  auto precond_exchange = [&]() {
+    for (int sw = 0; sw < a.sgs_sweeps; ++sw) {
+      half_sweep(1);
+      __syncthreads();
+      half_sweep(0);
+      __syncthreads();
+    }
+    ++zep;
+#pragma unroll
+    for (int j = 0; j < MAXJ; ++j)
+      if ((hmask >> j) & 1) HZ[q0 + (tl0 + 2 * j) * 512 + l] = s_zb[(tl0 + 2 * j) * 1000 + pc];
+    __syncthreads();
+    if (threadIdx.x == 0) st_release_u64(a.flags + blockIdx.x, zep);
+    if (threadIdx.x < 32) {  // acquire the neighbouring blocks' publications
+      long long spins = 0;
+      for (int k = threadIdx.x; k < s_nnb; k += 32) {
+        while (ld_acquire_u64(a.flags + s_nbl[k]) < zep) {
+          if (++spins > SM_SPIN_LIMIT) {
+            atomicExch(&st->error, 1);
+            break;
+          }
+        }
+      }
+    }
+    ring_fill<1>(s_zb, s_nbr, nt, b0, b1, [&](int, int64_t) -> float { return 0.f; });
+    __syncthreads();
+    ring_fill<2>(s_zb, s_nbr, nt, b0, b1, [&](int ri, int64_t qn) -> float {
+      return s_rdiag[ri] ? __ldcg(HZ + qn) : 0.f;
+    });
+    __syncthreads();
+  };
+
+  if (SGS) {
+    precond_exchange();
+  } else {
+    // ring fill of z0: remote z0 = M b (b is read-only input, no barrier needed)
+    ring_fill(s_zb, s_nbr, nt, b0, b1, [&](int ri, int64_t qn) -> float {
+      const uint8_t dg = s_rdiag[ri];
+      return dg ? (a.sign * a.bdiv[qn]) / (float)dg : 0.f;
+    });
+    __syncthreads();
+  }
 
   // w = A z for own fluid cells (non-fluid box entries are exactly 0, so the
   // branch-free six-neighbour sum equals the reference's fluid-only sum)
@@ -475,7 +599,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
     const float wn = stencil(j, z);
     const float r = s_r[L];
     s_w[L] = wn;
-    if ((hmask >> j) & 1) HW(0)[q0 + L] = wn;
+    if (!SGS && ((hmask >> j) & 1)) HW(0)[q0 + L] = wn;
     v3[0] += (Acc)(r * z);
     v3[1] += (Acc)(wn * z);
     v3[2] += (Acc)(r * r);
@@ -506,24 +630,33 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       s_x[L] = s_x[L] + alphaf * dn;
       const float rn = s_r[L] + nalpha * sn;
       s_r[L] = rn;
-      *zp = rn / fmaxf((float)((dpack >> (3 * j)) & 7), 1.0f);
-      if ((hmask >> j) & 1) {
-        HR(npar)[q0 + L] = rn;
-        HS(npar)[q0 + L] = sn;
+      if (SGS) {
+        *zp = rn * s_rtab[8 | ((dpack >> (3 * j)) & 7)];
+      } else {
+        *zp = rn / fmaxf((float)((dpack >> (3 * j)) & 7), 1.0f);
+        if ((hmask >> j) & 1) {
+          HR(npar)[q0 + L] = rn;
+          HS(npar)[q0 + L] = sn;
+        }
       }
     }
+    if (SGS) zero_rings();
     __syncthreads();
     trace_mark(gs);
-    // ---- ring fill of the new z: another block's cell is rebuilt from its
-    // published r_i, w_i, s_{i-1} with the owner's float32 operations
-    ring_fill(s_zb, s_nbr, nt, b0, b1, [&](int ri, int64_t qn) -> float {
-      const uint8_t dg = s_rdiag[ri];
-      if (!dg) return 0.f;
-      const float sn = __ldcg(HW(par) + qn) + betaf * __ldcg(HS(par) + qn);
-      const float rn = __ldcg(HR(par) + qn) + nalpha * sn;
-      return rn / (float)dg;
-    });
-    __syncthreads();
+    if (SGS) {
+      precond_exchange();
+    } else {
+      // ---- ring fill of the new z: another block's cell is rebuilt from its
+      // published r_i, w_i, s_{i-1} with the owner's float32 operations
+      ring_fill(s_zb, s_nbr, nt, b0, b1, [&](int ri, int64_t qn) -> float {
+        const uint8_t dg = s_rdiag[ri];
+        if (!dg) return 0.f;
+        const float sn = __ldcg(HW(par) + qn) + betaf * __ldcg(HS(par) + qn);
+        const float rn = __ldcg(HR(par) + qn) + nalpha * sn;
+        return rn / (float)dg;
+      });
+      __syncthreads();
+    }
     trace_mark(gs);
     // ---- w = A z and the three dot products
     Acc vv[3] = {0, 0, 0};
@@ -535,7 +668,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       const float wn = stencil(j, z);
       const float r = s_r[L];
       s_w[L] = wn;
-      if ((hmask >> j) & 1) HW(npar)[q0 + L] = wn;
+      if (!SGS && ((hmask >> j) & 1)) HW(npar)[q0 + L] = wn;
       vv[0] += (Acc)(r * z);
       vv[1] += (Acc)(wn * z);
       vv[2] += (Acc)(r * r);
@@ -590,19 +723,25 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
         const double res = (double)(a.sign * a.bdiv[q0 + L]) - (diag * s_x64[L] - sum);
         const float rf = (float)res;
         s_r[L] = rf;
-        s_zb[tl * 1000 + pc] = rf / diagz_of(code);
-        if ((hmask >> j) & 1) HR(npar)[q0 + L] = rf;
+        s_zb[tl * 1000 + pc] =
+            SGS ? rf * s_rtab[8 | ((code >> CODE_DIAG_SHIFT) & 7)] : rf / diagz_of(code);
+        if (!SGS && ((hmask >> j) & 1)) HR(npar)[q0 + L] = rf;
         vr[0] += res * res;
       }
+      if (SGS) zero_rings();
       double tr[1];
       if (!grid_allreduce<double, 1>(gs, vr, tr, shd)) return;
       r_true2 = tr[0];
-      // ring fill of z = M r from the replaced residuals, then w = A z
-      ring_fill(s_zb, s_nbr, nt, b0, b1, [&](int ri, int64_t qn) -> float {
-        const uint8_t dg = s_rdiag[ri];
-        return dg ? __ldcg(HR(npar) + qn) / (float)dg : 0.f;
-      });
-      __syncthreads();
+      // z = M r from the replaced residuals (ring included), then w = A z
+      if (SGS) {
+        precond_exchange();
+      } else {
+        ring_fill(s_zb, s_nbr, nt, b0, b1, [&](int ri, int64_t qn) -> float {
+          const uint8_t dg = s_rdiag[ri];
+          return dg ? __ldcg(HR(npar) + qn) / (float)dg : 0.f;
+        });
+        __syncthreads();
+      }
       Acc vw[3] = {0, 0, 0};
 #pragma unroll
       for (int j = 0; j < MAXJ; ++j) {
@@ -612,7 +751,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
         const float wn = stencil(j, z);
         const float r = s_r[L];
         s_w[L] = wn;
-        if ((hmask >> j) & 1) HW(npar)[q0 + L] = wn;
+        if (!SGS && ((hmask >> j) & 1)) HW(npar)[q0 + L] = wn;
         vw[0] += (Acc)(r * z);
         vw[1] += (Acc)(wn * z);
         vw[2] += (Acc)(r * r);
@@ -678,14 +817,17 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
 template <typename Acc, bool REF>
 static bool fits_t(Ctx *c) {
   int optin = 0;
-  cudaFuncAttributes fa;
+  cudaFuncAttributes fa, fb;
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device) !=
           cudaSuccess ||
-      cudaFuncGetAttributes(&fa, (const void *)k_pcg_smem<Acc, REF>) != cudaSuccess) {
+      cudaFuncGetAttributes(&fa, (const void *)k_pcg_smem<Acc, REF, false>) != cudaSuccess ||
+      cudaFuncGetAttributes(&fb, (const void *)k_pcg_smem<Acc, REF, true>) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return SmemCfg<REF>::BYTES + fa.sharedSizeBytes <= (size_t)optin;
+  return SmemCfg<REF>::BYTES + (fa.sharedSizeBytes > fb.sharedSizeBytes ? fa.sharedSizeBytes
+                                                                         : fb.sharedSizeBytes) <=
+         (size_t)optin;
 }
 
 bool pcg_smem_fits(Ctx *c, bool refined) {
@@ -695,7 +837,7 @@ bool pcg_smem_fits(Ctx *c, bool refined) {
 template <typename Acc, bool REF>
 static int launch_t(Ctx *c, PcgSmemArgs &a) {
   const size_t smem = SmemCfg<REF>::BYTES;
-  auto fn = k_pcg_smem<Acc, REF>;
+  auto fn = a.sgs_sweeps > 0 ? k_pcg_smem<Acc, REF, true> : k_pcg_smem<Acc, REF, false>;
   int e = check_cuda(c, cudaFuncSetAttribute((const void *)fn,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem),

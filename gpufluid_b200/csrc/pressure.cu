@@ -32,6 +32,9 @@
 namespace gf {
 
 constexpr int PCG_THREADS = 512;
+// barrier scratch: 8 lines x 16 u64 of counters, then one u64 flag per block
+constexpr int64_t BAR_FLAGS_OFF = 8 * 16;
+constexpr size_t BAR_BYTES = (BAR_FLAGS_OFF + 256) * 8;
 constexpr long long SPIN_LIMIT = 1LL << 24;  // ~1-2 s with 64 ns sleeps
 
 // ------------------------------------------------------------- set-up
@@ -1154,7 +1157,7 @@ int pressure_alloc(Ctx *c) {
   const int64_t np = (int64_t)c->ntiles + MAX_PCG_BLOCKS;
   if ((e = A((void **)&c->partials, 3 * np * sizeof(double), "alloc partials"))) return e;
   if ((e = A((void **)&c->state, sizeof(PcgState), "alloc pcg state"))) return e;
-  if ((e = A((void **)&c->bar_counters, 8 * 16 * 8, "alloc barrier counters"))) return e;
+  if ((e = A((void **)&c->bar_counters, BAR_BYTES, "alloc barrier counters"))) return e;
   if ((e = A((void **)&c->trace, TRACE_CAP * 8, "alloc trace"))) return e;
   if ((e = A((void **)&c->halo, nk * 6 * 4, "alloc halo buffers"))) return e;
   if ((e = A((void **)&c->tile_cost, (size_t)c->ntiles * 4, "alloc tile cost"))) return e;
@@ -1363,7 +1366,7 @@ int launch_pressure(Ctx *c, const gf_step_params *prm) {
     const bool force_global =
         (prm->flags & GF_FLAG_GLOBAL_PCG) != 0 || !pcg_smem_fits(c, refined);
     if (!force_global) {
-      if ((e = check_cuda(c, cudaMemsetAsync(c->bar_counters, 0, 8 * 16 * 8, st),
+      if ((e = check_cuda(c, cudaMemsetAsync(c->bar_counters, 0, BAR_BYTES, st),
                           "zero barrier counters")))
         return e;
       float *h = c->halo;
@@ -1372,7 +1375,9 @@ int launch_pressure(Ctx *c, const gf_step_params *prm) {
                      h + 3 * nk, h + 4 * nk, h + 5 * nk, refined ? c->x64 : nullptr,
                      c->partials, c->bar_counters, c->state,
                      (prm->flags & GF_FLAG_TRACE) ? c->trace : nullptr, TRACE_CAP,
-                     prm->max_iters, check_every, prm->tol * prm->tol, replace2, sign};
+                     prm->max_iters, check_every, prm->tol * prm->tol, replace2, sign,
+                     (prm->flags & GF_FLAG_SGS_MASK) >> GF_FLAG_SGS_SHIFT,
+                     c->bar_counters + BAR_FLAGS_OFF};
       if ((e = launch_pcg_smem(c, sa, refined))) return e;
     }
     PcgArgs pa{c->n_active, c->tile_nbr, c->code, c->bdiv, c->xf, c->r, c->z, c->d0, c->d1,

@@ -95,6 +95,13 @@ typedef struct gf_step_params {
 /* flags: record the SM clock (clock64, cycles) at every phase boundary of the
  * shared-memory PCG in block 0; read the stamps with gf_pcg_trace */
 #define GF_FLAG_TRACE 2
+/* flags bits 2-3: sweeps (1-3) of a tile-local red-black symmetric
+ * Gauss-Seidel preconditioner for GF_PCG / GF_PCG_REFINED in the
+ * shared-memory kernel; 0 keeps the reference's Jacobi preconditioner.  Same
+ * operator and stop test; fewer iterations, one neighbour exchange more per
+ * iteration.  The global-memory kernel always uses Jacobi. */
+#define GF_FLAG_SGS_SHIFT 2
+#define GF_FLAG_SGS_MASK 12
 
 /* ---- context ------------------------------------------------------------ */
 /* Allocates scratch for a grid and up to max_particles particles on the

@@ -312,3 +312,39 @@ def test_pcg_large_region_falls_back_to_global_kernel(gf, oracle):
     assert info.n_active_tiles == 24 * 6 * 24
     assert info.kernel == 2 and info.status == 0
     assert info.relres <= 1e-9
+
+
+@pytest.mark.parametrize("sweeps", [1, 2, 3])
+@pytest.mark.parametrize("grid", [(24, 24, 24), (48, 40, 56), (80, 80, 80)])
+def test_pcg_tile_sgs_preconditioner(gf, oracle, grid, sweeps):
+    """Tile-local symmetric Gauss-Seidel preconditioner (flags bits 2-3): the
+    refined solve reaches the FP64 solution of the same system as the Jacobi-
+    preconditioned one, in fewer iterations.  At 80^3 fluid fills y < 64 (air
+    above, so the system is nonsingular): 800 tiles, several per block, so
+    in-block and remote ring exchanges both run."""
+    import torch
+    from gpufluid_b200 import _lib
+    res = {}
+    for flags in (0, sweeps << _lib.GF_FLAG_SGS_SHIFT):
+        s, o = _pressure_case(gf, oracle, grid, seed=23)
+        if grid == (80, 80, 80):
+            lab = s._marker_host.copy()
+            lab[1:-1, 1:64, 1:-1] = 1
+            rng = np.random.default_rng(3)
+            div = np.where(lab == 1, rng.normal(0, 1, lab.shape), 0).astype(np.float32)
+            s._label.copy_(_t(lab.astype(np.uint8)))
+            s.div.copy_(_t(div))
+            o.marker[...] = lab
+            o.div[...] = div
+        prm = _params(gf, "pcg_refined", 4000, tol=1e-10, flags=flags)
+        it = ctypes.c_int32()
+        _call(s, "gf_pressure", ctypes.byref(prm), ctypes.byref(it))
+        torch.cuda.synchronize()
+        info = _stats(s)
+        assert info.kernel == 1 and info.status == 0, (flags, info.kernel, info.status)
+        assert info.relres <= 1e-10, (flags, info.relres)
+        if not res:  # the same system for both preconditioners
+            p64, _, _ = oracle.pcg64(o.marker, o.div, tol=1e-14)
+        assert rel_l2(s._p.cpu().numpy(), p64) < 1e-6
+        res[flags] = info.iters
+    assert res[sweeps << _lib.GF_FLAG_SGS_SHIFT] < res[0], res
