@@ -76,7 +76,6 @@ struct PcgSmemArgs {
   double tol2, replace2;
   float sign;
   int sgs_sweeps;             // 0: Jacobi (the reference's); 1-3: tile-local symmetric GS
-  unsigned long long *flags;  // SGS: per-block publication epochs (zeroed per solve)
 };
 
 
@@ -151,7 +150,7 @@ struct Ctx {
   float *d0 = nullptr, *d1 = nullptr, *Ad = nullptr;
   double *x64 = nullptr;
   double *partials = nullptr;    // [3 * MAX_PCG_BLOCKS]
-  unsigned long long *bar_counters = nullptr;  // 8 lines x 16 u64, then per-block flags
+  unsigned long long *bar_counters = nullptr;  // 8 lines x 16 u64
   float *halo = nullptr;         // [6 * nkeys] halo publication buffers
   int32_t *tile_cost = nullptr;  // [ntiles] per-slot PCG work estimate
   long long *trace = nullptr;    // [TRACE_CAP] PCG phase timestamps

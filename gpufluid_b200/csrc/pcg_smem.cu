@@ -1,8 +1,9 @@
-// Shared-memory-resident Jacobi-preconditioned CG for the pressure system of
+// Shared-memory-resident preconditioned CG for the pressure system of
 // _pressure_pcg (src/gpufluid/solvers/solver3d.py:2917-3043): the same
 // operator (diag = #non-solid neighbours, -1 per fluid neighbour), the same
-// preconditioner (z = r / max(diag, 1)) and stop test (||r||^2 < tol^2
-// ||r0||^2, checked every check_every iterations), written in the
+// preconditioner by default (Jacobi, z = r / max(diag, 1); optionally
+// tile-local symmetric Gauss-Seidel sweeps) and the same stop test (||r||^2 <
+// tol^2 ||r0||^2, checked every check_every iterations), written in the
 // single-reduction form of Chronopoulos & Gear (1989): with w = A z,
 //   d = z + beta d,  s = w + beta s,  x += alpha d,  r -= alpha s,  z = M r,
 //   w = A z,  gamma = r.z,  delta = w.z,
@@ -12,16 +13,15 @@
 //
 // One cooperative block of 1024 threads per SM.  Block b owns the contiguous
 // run of active tile slots [b0, b1) (balanced split of n_active) and keeps its
-// cells' x, r, d, s, stencil codes and a padded 10x10x10 box of z per tile in
-// shared memory for the whole solve (plus the FP64 iterate x64 when
-// refining); w lives in registers.  A tile face whose neighbouring tile
-// belongs to another block is a halo face: its fluid cells publish r, s and w
-// (double-buffered by iteration parity) to global memory, and the neighbour
-// block rebuilds their new z = (r - alpha (w + beta s)) / diag with the
-// owner's float32 operations, so every z value is identical wherever it is
-// computed.  Each iteration: own update -> ring fill of the z boxes (from the
-// neighbouring tile's box or the published halo) -> w = A z as a branch-free
-// fixed-offset stencil -> one grid all-reduce of (r.z, w.z, r.r).
+// cells' x, r, d, s, w, stencil codes and a padded 10x10x10 box of z per tile
+// in shared memory for the whole solve (plus the FP64 iterate x64 when
+// refining).  A tile face whose neighbouring tile belongs to another block is
+// a halo face: its fluid cells publish z as tagged 64-bit words (the value's
+// bits under a publication count) and the neighbouring block loads them until
+// the count matches.  Each iteration: own update -> z = M r -> halo
+// publication and ring fill of the z boxes (from the neighbouring tile's box
+// or the tagged halo) -> w = A z as a branch-free fixed-offset stencil -> one
+// grid all-reduce of (r.z, w.z, r.r).
 //
 // The grid all-reduce: thread 0 publishes the block's partial sums, arrives
 // with a release-ordered add on a monotonic counter and polls it with acquire
@@ -48,10 +48,6 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
   unsigned long long v;
   asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
-}
-
-__device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned long long v) {
-  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
 constexpr int SM_MAXG = 160;      // blocks (one per SM)
@@ -211,60 +207,84 @@ __device__ __forceinline__ void face_map(int dir, int p, int &ring, int &lw) {
   }
 }
 
-// Face-wise ring fill: warp w handles faces f = w, w+32, ... of the block's
-// tiles (f = tile * 6 + dir), each lane positions p = lane and lane + 32 of the
-// face, so the face's direction and neighbour kind are uniform in the warp.
-// In-block neighbours are copied box to box (the source cell sits at
-// ring + delta[dir] in the neighbour's box); another block's cell gets
-// remote(face index * 64 + p, global cell index, p); faces without a neighbour
-// tile keep their zeros.
+// Ring geometry per face direction: ring position base + (hi+1) a + (lo+1) b
+// of face position p = hi * 8 + lo, and the offset of the source cell in the
+// neighbouring tile's box.
 __constant__ int c_ring_base[6] = {0, 900, 0, 90, 0, 9};
 __constant__ int c_ring_a[6] = {10, 10, 100, 100, 100, 100};
 __constant__ int c_ring_b[6] = {1, 1, 1, 1, 10, 10};
 __constant__ int c_ring_delta[6] = {800, -800, 80, -80, 8, -8};
 
-// MODE 0 fills every face, 1 only the in-block ones, 2 only another block's.
-template <int MODE = 0, typename Remote>
-__device__ __forceinline__ void ring_fill(float *s_zb, const int *s_nbr, int nt, int b0, int b1,
-                                          Remote remote) {
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long *p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Face-wise ring fill from tagged halo words (value bits | publication count
+// << 32): warp w handles faces f = w, w+32, ... of the block's tiles (f = tile
+// * 6 + dir), each lane positions p = lane and lane + 32 of the face, so the
+// face's direction and neighbour kind are uniform in the warp.  In-block
+// faces are copied box to box; another block's face is loaded
+// (both of a lane's words in flight) until both carry the count `ep`.  A
+// wait longer than the spin limit sets *err (the next grid reduction then
+// ends the solve).
+__device__ __forceinline__ void ring_fill_tagged(float *s_zb, const int *s_nbr, int nt, int b0,
+                                                 int b1, const uint8_t *s_rdiag,
+                                                 const unsigned long long *hz,
+                                                 unsigned long long ep, int *err) {
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int f = wid; f < nt * 6; f += SM_THREADS / 32) {
     const int sl = s_nbr[f];
     if (sl < 0) continue;
-    const bool local = sl >= b0 && sl < b1;
-    if ((MODE == 1 && !local) || (MODE == 2 && local)) continue;
     const int tl = f / 6, dir = f - tl * 6;
     const int base = c_ring_base[dir], ca = c_ring_a[dir], cb = c_ring_b[dir];
     float *dst = s_zb + tl * 1000;
-    if (local) {
-      const float *src = s_zb + (sl - b0) * 1000 + c_ring_delta[dir];
+    int ring[2];
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int p = lane + 32 * h;
-        const int ring = base + ((p >> 3) + 1) * ca + ((p & 7) + 1) * cb;
-        dst[ring] = src[ring];
-      }
-    } else {
-      float v[2];
-      int ring[2];
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int p = lane + 32 * h, hi = p >> 3, lo = p & 7;
-        ring[h] = base + (hi + 1) * ca + (lo + 1) * cb;
-        int lw;
-        switch (dir) {
-          case 0: lw = 448 + p; break;
-          case 1: lw = p; break;
-          case 2: lw = hi * 64 + 56 + lo; break;
-          case 3: lw = hi * 64 + lo; break;
-          case 4: lw = hi * 64 + lo * 8 + 7; break;
-          default: lw = hi * 64 + lo * 8; break;
-        }
-        v[h] = remote(f * 64 + p, (int64_t)sl * 512 + lw);
-      }
-      dst[ring[0]] = v[0];
-      dst[ring[1]] = v[1];
+    for (int h = 0; h < 2; ++h) {
+      const int p = lane + 32 * h;
+      ring[h] = base + ((p >> 3) + 1) * ca + ((p & 7) + 1) * cb;
     }
+    if (sl >= b0 && sl < b1) {
+      const float *src = s_zb + (sl - b0) * 1000 + c_ring_delta[dir];
+      dst[ring[0]] = src[ring[0]];
+      dst[ring[1]] = src[ring[1]];
+      continue;
+    }
+    int64_t q[2];
+    bool need[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int p = lane + 32 * h, hi = p >> 3, lo = p & 7;
+      int lw;
+      switch (dir) {
+        case 0: lw = 448 + p; break;
+        case 1: lw = p; break;
+        case 2: lw = hi * 64 + 56 + lo; break;
+        case 3: lw = hi * 64 + lo; break;
+        case 4: lw = hi * 64 + lo * 8 + 7; break;
+        default: lw = hi * 64 + lo * 8; break;
+      }
+      q[h] = (int64_t)sl * 512 + lw;
+      need[h] = s_rdiag[f * 64 + p] != 0;  // non-fluid remote cells read as 0
+    }
+    unsigned long long w0 = need[0] ? ld_relaxed_u64(hz + q[0]) : 0ull;
+    unsigned long long w1 = need[1] ? ld_relaxed_u64(hz + q[1]) : 0ull;
+    long long spins = 0;
+    while ((need[0] && (w0 >> 32) != ep) || (need[1] && (w1 >> 32) != ep)) {
+      if (++spins > SM_SPIN_LIMIT) {
+        atomicExch(err, 1);
+        break;
+      }
+      if (need[0] && (w0 >> 32) != ep) w0 = ld_relaxed_u64(hz + q[0]);
+      if (need[1] && (w1 >> 32) != ep) w1 = ld_relaxed_u64(hz + q[1]);
+    }
+    dst[ring[0]] = need[0] ? __uint_as_float((unsigned)w0) : 0.f;
+    dst[ring[1]] = need[1] ? __uint_as_float((unsigned)w1) : 0.f;
   }
 }
 
@@ -356,10 +376,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   static_assert(MAXJ * 3 <= 32, "diagonal pack");
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_nbr[MAXT * 6];
-  __shared__ int s_nbl[SM_MAXG];         // SGS: distinct neighbouring blocks
-  __shared__ unsigned s_nbbits[SM_MAXG / 32];
-  __shared__ int s_nnb;
-  __shared__ float s_rtab[16];  // SGS, by (fluid << 3 | count): 0, or 1 / max(count, 1)
+  __shared__ float s_rtab[16];  // by (fluid << 3 | count): 0, or 1 / max(count, 1)
   __shared__ uint8_t s_mask[MAXT];
   __shared__ int s_bounds[SM_MAXG + 1];
   __shared__ Acc sh[36 * 4];
@@ -373,6 +390,20 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
     return;
   }
   GridSync gs{a.partials, a.counter, &st->error, 0ull, a.trace, 0, a.trace_cap / 2, 0, clock64()};
+  // Phases of an iteration for the trace (block thread 0's view, cycles):
+  // 0 own update, 1 SGS sweeps, 2 halo publication + neighbour flags +
+  // in-block rings, 3 remote rings, 4 stencil and dot products, 5 grid
+  // all-reduce (with the barrier before it).  s_ph[6] holds the last stamp.
+  __shared__ long long s_ph[7];
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 7; ++k) s_ph[k] = k < 6 ? 0 : clock64();
+  auto phase_mark = [&](int k) {
+    if (a.trace && threadIdx.x == 0) {
+      const long long now = clock64();
+      s_ph[k] += now - s_ph[6];
+      s_ph[6] = now;
+    }
+  };
   if (G > SM_MAXG) {
     if (threadIdx.x == 0) atomicExch(&st->error, 1);
     return;
@@ -424,33 +455,10 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
     }
     s_rdiag[w] = dg;
   }
-  if (SGS) {
-    // the blocks owning a remote face: the last block whose first slot is <= sl
-    if (threadIdx.x < SM_MAXG / 32) s_nbbits[threadIdx.x] = 0u;
-    __syncthreads();
-    for (int f = threadIdx.x; f < nt * 6; f += blockDim.x) {
-      const int sl = s_nbr[f];
-      if (sl < 0 || (sl >= b0 && sl < b1)) continue;
-      int lo = 0, hi = G;
-      while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (s_bounds[mid] <= sl) lo = mid; else hi = mid;
-      }
-      atomicOr(&s_nbbits[lo >> 5], 1u << (lo & 31));
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int cnt = 0;
-      for (int g = 0; g < G; ++g)
-        if ((s_nbbits[g >> 5] >> (g & 31)) & 1u) s_nbl[cnt++] = g;
-      s_nnb = cnt;
-    }
-  }
   __syncthreads();
-
-#define HR(par) ((par) ? a.hr1 : a.hr0)
-#define HW(par) ((par) ? a.hw1 : a.hw0)
-#define HS(par) ((par) ? a.hs1 : a.hs0)
+  // sweeps of the tile SGS preconditioner; 0: Jacobi (the reference's), for
+  // which the instantiation carries no sweep code
+  const int sgs = SGS ? a.sgs_sweeps : 0;
 
   // ---- init: r0 = b, z0 = M r0, w0 = A z0; d_{-1} = s_{-1} = 0.  Per-thread
   // masks: fluid (bit j), halo (bit j), neighbour count (3 bits per j).
@@ -469,13 +477,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       b = a.sign * a.bdiv[q0 + L];
       s_zb[tl * 1000 + pc] =
           SGS ? b * s_rtab[8 | ((code >> CODE_DIAG_SHIFT) & 7)] : b / diagz_of(code);
-      if (is_halo(L, s_mask)) {
-        hmask |= 1u << j;
-        if (!SGS) {
-          HR(0)[q0 + L] = b;
-          HS(0)[q0 + L] = 0.f;
-        }
-      }
+      if (is_halo(L, s_mask)) hmask |= 1u << j;
     }
     s_r[L] = b;
     s_x[L] = 0.f;
@@ -485,7 +487,8 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   }
   __syncthreads();
 
-  // ---- tile-local symmetric Gauss-Seidel preconditioner (SGS): z = M r with
+  // ---- z = M r and its ring.  Jacobi (sgs == 0): z = r/D, written by the
+  // callers.  Tile-local symmetric Gauss-Seidel (sgs sweeps): z = M r with
   // M^-1 = sweeps of red-black symmetric Gauss-Seidel on each 8^3 tile from
   // z = 0, the tile's neighbours held at 0 (the diagonal block of A per tile;
   // symmetric positive definite, so CG applies).  The first red half-sweep
@@ -494,11 +497,14 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   // cells hold 0, so a half-sweep is the branch-free six-neighbour sum with a
   // per-cell factor (0 on non-fluid cells).  It maps thread t to the
   // (t & 255)-th cell of the colour in tiles (t >> 8) + 4i, so all threads
-  // work.  The result is published on the halo cells and each block releases
-  // its flag; the ring of another block's tile is read after that block's
-  // flag has been acquired.
+  // work.  The result is published on the halo cells as 64-bit words, the
+  // float's bits under a 32-bit publication count (relaxed stores: the word
+  // is its own flag, no fence), and the ring of another block's tile is
+  // loaded until the count matches (bounded).  The words are zeroed before
+  // every solve.  A word is overwritten only after the reduction that
+  // follows its reads, so no publication is missed.
   unsigned long long zep = 0;  // z publications, the same sequence in every block
-  float *const HZ = a.hr0;
+  unsigned long long *const HZ = reinterpret_cast<unsigned long long *>(a.hr0);
   auto half_sweep = [&](int c) {  // z = (r + in-tile fluid neighbours' z) / D, colour c
     const int k = threadIdx.x & 255;
     const int li = k >> 5, lj = (k >> 2) & 7;
@@ -533,49 +539,29 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
     }
   };
   // Callers have written z = r/D on their fluid cells, zeroed the rings
-  // (zero_rings) and passed a barrier.
+  // (zero_rings, SGS only) and passed a barrier.
   auto precond_exchange = [&]() {
-    for (int sw = 0; sw < a.sgs_sweeps; ++sw) {
+    for (int sw = 0; sw < sgs; ++sw) {
       half_sweep(1);
       __syncthreads();
       half_sweep(0);
       __syncthreads();
     }
+    phase_mark(1);
     ++zep;
+    const unsigned long long tag = zep << 32;
 #pragma unroll
     for (int j = 0; j < MAXJ; ++j)
-      if ((hmask >> j) & 1) HZ[q0 + (tl0 + 2 * j) * 512 + l] = s_zb[(tl0 + 2 * j) * 1000 + pc];
+      if ((hmask >> j) & 1)
+        st_relaxed_u64(HZ + q0 + (tl0 + 2 * j) * 512 + l,
+                       tag | __float_as_uint(s_zb[(tl0 + 2 * j) * 1000 + pc]));
+    phase_mark(2);
+    ring_fill_tagged(s_zb, s_nbr, nt, b0, b1, s_rdiag, HZ, zep, &st->error);
     __syncthreads();
-    if (threadIdx.x == 0) st_release_u64(a.flags + blockIdx.x, zep);
-    if (threadIdx.x < 32) {  // acquire the neighbouring blocks' publications
-      long long spins = 0;
-      for (int k = threadIdx.x; k < s_nnb; k += 32) {
-        while (ld_acquire_u64(a.flags + s_nbl[k]) < zep) {
-          if (++spins > SM_SPIN_LIMIT) {
-            atomicExch(&st->error, 1);
-            break;
-          }
-        }
-      }
-    }
-    ring_fill<1>(s_zb, s_nbr, nt, b0, b1, [&](int, int64_t) -> float { return 0.f; });
-    __syncthreads();
-    ring_fill<2>(s_zb, s_nbr, nt, b0, b1, [&](int ri, int64_t qn) -> float {
-      return s_rdiag[ri] ? __ldcg(HZ + qn) : 0.f;
-    });
-    __syncthreads();
+    phase_mark(3);
   };
 
-  if (SGS) {
-    precond_exchange();
-  } else {
-    // ring fill of z0: remote z0 = M b (b is read-only input, no barrier needed)
-    ring_fill(s_zb, s_nbr, nt, b0, b1, [&](int ri, int64_t qn) -> float {
-      const uint8_t dg = s_rdiag[ri];
-      return dg ? (a.sign * a.bdiv[qn]) / (float)dg : 0.f;
-    });
-    __syncthreads();
-  }
+  precond_exchange();
 
   // w = A z for own fluid cells (non-fluid box entries are exactly 0, so the
   // branch-free six-neighbour sum equals the reference's fluid-only sum)
@@ -599,7 +585,6 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
     const float wn = stencil(j, z);
     const float r = s_r[L];
     s_w[L] = wn;
-    if (!SGS && ((hmask >> j) & 1)) HW(0)[q0 + L] = wn;
     v3[0] += (Acc)(r * z);
     v3[1] += (Acc)(wn * z);
     v3[2] += (Acc)(r * r);
@@ -615,7 +600,6 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   int done = (double)r0 < 1e-30 ? 1 : 0, iters = 0, nrep = 0, status = GF_OK;
 
   for (int it = 0; it < a.max_iter && !done; ++it) {
-    const int par = it & 1, npar = par ^ 1;
     const float alphaf = (float)alpha, nalpha = -alphaf, betaf = (float)beta;
     // ---- own: d = z + beta d; s = w + beta s; x += alpha d; r -= alpha s; z = M r
 #pragma unroll
@@ -630,33 +614,14 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       s_x[L] = s_x[L] + alphaf * dn;
       const float rn = s_r[L] + nalpha * sn;
       s_r[L] = rn;
-      if (SGS) {
-        *zp = rn * s_rtab[8 | ((dpack >> (3 * j)) & 7)];
-      } else {
-        *zp = rn / fmaxf((float)((dpack >> (3 * j)) & 7), 1.0f);
-        if ((hmask >> j) & 1) {
-          HR(npar)[q0 + L] = rn;
-          HS(npar)[q0 + L] = sn;
-        }
-      }
+      *zp = SGS ? rn * s_rtab[8 | ((dpack >> (3 * j)) & 7)]
+                : rn / fmaxf((float)((dpack >> (3 * j)) & 7), 1.0f);
     }
     if (SGS) zero_rings();
     __syncthreads();
     trace_mark(gs);
-    if (SGS) {
-      precond_exchange();
-    } else {
-      // ---- ring fill of the new z: another block's cell is rebuilt from its
-      // published r_i, w_i, s_{i-1} with the owner's float32 operations
-      ring_fill(s_zb, s_nbr, nt, b0, b1, [&](int ri, int64_t qn) -> float {
-        const uint8_t dg = s_rdiag[ri];
-        if (!dg) return 0.f;
-        const float sn = __ldcg(HW(par) + qn) + betaf * __ldcg(HS(par) + qn);
-        const float rn = __ldcg(HR(par) + qn) + nalpha * sn;
-        return rn / (float)dg;
-      });
-      __syncthreads();
-    }
+    phase_mark(0);
+    precond_exchange();
     trace_mark(gs);
     // ---- w = A z and the three dot products
     Acc vv[3] = {0, 0, 0};
@@ -668,13 +633,14 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       const float wn = stencil(j, z);
       const float r = s_r[L];
       s_w[L] = wn;
-      if (!SGS && ((hmask >> j) & 1)) HW(npar)[q0 + L] = wn;
       vv[0] += (Acc)(r * z);
       vv[1] += (Acc)(wn * z);
       vv[2] += (Acc)(r * r);
     }
+    phase_mark(4);
     Acc tv[3];
     if (!grid_allreduce<Acc, 3>(gs, vv, tv, sh)) return;
+    phase_mark(5);
     iters = it + 1;
     double rr = (double)tv[2];
     rr_last = rr;
@@ -725,7 +691,6 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
         s_r[L] = rf;
         s_zb[tl * 1000 + pc] =
             SGS ? rf * s_rtab[8 | ((code >> CODE_DIAG_SHIFT) & 7)] : rf / diagz_of(code);
-        if (!SGS && ((hmask >> j) & 1)) HR(npar)[q0 + L] = rf;
         vr[0] += res * res;
       }
       if (SGS) zero_rings();
@@ -733,15 +698,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       if (!grid_allreduce<double, 1>(gs, vr, tr, shd)) return;
       r_true2 = tr[0];
       // z = M r from the replaced residuals (ring included), then w = A z
-      if (SGS) {
-        precond_exchange();
-      } else {
-        ring_fill(s_zb, s_nbr, nt, b0, b1, [&](int ri, int64_t qn) -> float {
-          const uint8_t dg = s_rdiag[ri];
-          return dg ? __ldcg(HR(npar) + qn) / (float)dg : 0.f;
-        });
-        __syncthreads();
-      }
+      precond_exchange();
       Acc vw[3] = {0, 0, 0};
 #pragma unroll
       for (int j = 0; j < MAXJ; ++j) {
@@ -751,7 +708,6 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
         const float wn = stencil(j, z);
         const float r = s_r[L];
         s_w[L] = wn;
-        if (!SGS && ((hmask >> j) & 1)) HW(npar)[q0 + L] = wn;
         vw[0] += (Acc)(r * z);
         vw[1] += (Acc)(wn * z);
         vw[2] += (Acc)(r * r);
@@ -789,11 +745,12 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       int remote = 0;
       for (int f = 0; f < nt * 6; ++f)
         if (s_nbr[f] >= 0 && !(s_nbr[f] >= b0 && s_nbr[f] < b1)) ++remote;
-      long long *t = gs.trace + a.trace_cap / 2 + 4 * blockIdx.x;
+      long long *t = gs.trace + a.trace_cap / 2 + 10 * blockIdx.x;
       t[0] = gs.busy;
       t[1] = nt;
       t[2] = s_nf;
       t[3] = remote;
+      for (int k = 0; k < 6; ++k) t[4 + k] = s_ph[k];
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -809,25 +766,19 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
     if (status != GF_OK) st->status = status;
     st->smem_solver = 1;
   }
-#undef HR
-#undef HW
-#undef HS
 }
 
 template <typename Acc, bool REF>
 static bool fits_t(Ctx *c) {
   int optin = 0;
-  cudaFuncAttributes fa, fb;
+  cudaFuncAttributes fa;
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device) !=
           cudaSuccess ||
-      cudaFuncGetAttributes(&fa, (const void *)k_pcg_smem<Acc, REF, false>) != cudaSuccess ||
-      cudaFuncGetAttributes(&fb, (const void *)k_pcg_smem<Acc, REF, true>) != cudaSuccess) {
+      cudaFuncGetAttributes(&fa, (const void *)k_pcg_smem<Acc, REF, true>) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return SmemCfg<REF>::BYTES + (fa.sharedSizeBytes > fb.sharedSizeBytes ? fa.sharedSizeBytes
-                                                                         : fb.sharedSizeBytes) <=
-         (size_t)optin;
+  return SmemCfg<REF>::BYTES + fa.sharedSizeBytes <= (size_t)optin;
 }
 
 bool pcg_smem_fits(Ctx *c, bool refined) {

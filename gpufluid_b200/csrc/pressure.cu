@@ -32,9 +32,7 @@
 namespace gf {
 
 constexpr int PCG_THREADS = 512;
-// barrier scratch: 8 lines x 16 u64 of counters, then one u64 flag per block
-constexpr int64_t BAR_FLAGS_OFF = 8 * 16;
-constexpr size_t BAR_BYTES = (BAR_FLAGS_OFF + 256) * 8;
+constexpr size_t BAR_BYTES = 8 * 16 * 8;  // barrier scratch: 8 lines x 16 u64
 constexpr long long SPIN_LIMIT = 1LL << 24;  // ~1-2 s with 64 ns sleeps
 
 // ------------------------------------------------------------- set-up
@@ -1376,8 +1374,11 @@ int launch_pressure(Ctx *c, const gf_step_params *prm) {
                      c->partials, c->bar_counters, c->state,
                      (prm->flags & GF_FLAG_TRACE) ? c->trace : nullptr, TRACE_CAP,
                      prm->max_iters, check_every, prm->tol * prm->tol, replace2, sign,
-                     (prm->flags & GF_FLAG_SGS_MASK) >> GF_FLAG_SGS_SHIFT,
-                     c->bar_counters + BAR_FLAGS_OFF};
+                     (prm->flags & GF_FLAG_SGS_MASK) >> GF_FLAG_SGS_SHIFT};
+      // the solver publishes tagged 64-bit halo words over the first two halo
+      // arrays; their counts restart at 1 with every solve
+      if ((e = check_cuda(c, cudaMemsetAsync(h, 0, (size_t)nk * 8, st), "zero tagged halo")))
+        return e;
       if ((e = launch_pcg_smem(c, sa, refined))) return e;
     }
     PcgArgs pa{c->n_active, c->tile_nbr, c->code, c->bdiv, c->xf, c->r, c->z, c->d0, c->d1,

@@ -167,9 +167,11 @@ typedef struct gf_pressure_info {
 } gf_pressure_info;
 /* Copies the trace buffer of the last traced PCG solve (up to cap int64
  * entries: block 0's SM-cycle stamps in the first half, *n of them, then per
- * block four values: busy cycles outside the all-reduce, tiles owned, fluid
- * cells owned, faces bordering another block's tile) into host memory;
- * synchronises. */
+ * block ten values: busy cycles outside the all-reduce, tiles owned, fluid
+ * cells owned, faces bordering another block's tile, and the cycles of six
+ * iteration phases as block thread 0 sees them -- own update, SGS sweeps,
+ * halo publication with the neighbour flags and in-block rings, remote rings,
+ * stencil and dot products, grid all-reduce) into host memory; synchronises. */
 int gf_pcg_trace(void *ctx, int64_t *host, int32_t cap, int32_t *n);
 /* Statistics of the last pressure solve; synchronises. */
 int gf_pressure_stats(void *ctx, gf_pressure_info *info);
