@@ -232,14 +232,15 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long
 // (both of a lane's words in flight) until both carry the count `ep`.  A
 // wait longer than the spin limit sets *err (the next grid reduction then
 // ends the solve).
-__device__ __forceinline__ void ring_fill_tagged(float *s_zb, const int *s_nbr, int nt, int b0,
-                                                 int b1, const uint8_t *s_rdiag,
+__device__ __forceinline__ void ring_fill_tagged(float *s_zb, const int *s_nbr,
+                                                 const int *s_forder, int nface, int b0, int b1,
+                                                 const uint8_t *s_rdiag,
                                                  const unsigned long long *hz,
                                                  unsigned long long ep, int *err) {
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int f = wid; f < nt * 6; f += SM_THREADS / 32) {
+  for (int i = wid; i < nface; i += SM_THREADS / 32) {
+    const int f = s_forder[i];
     const int sl = s_nbr[f];
-    if (sl < 0) continue;
     const int tl = f / 6, dir = f - tl * 6;
     const int base = c_ring_base[dir], ca = c_ring_a[dir], cb = c_ring_b[dir];
     float *dst = s_zb + tl * 1000;
@@ -378,6 +379,8 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   __shared__ int s_nbr[MAXT * 6];
   __shared__ float s_rtab[16];  // by (fluid << 3 | count): 0, or 1 / max(count, 1)
   __shared__ uint8_t s_mask[MAXT];
+  __shared__ int s_forder[MAXT * 6];  // faces with a neighbouring tile, another block's first
+  __shared__ int s_nface;
   __shared__ int s_bounds[SM_MAXG + 1];
   __shared__ Acc sh[36 * 4];
   __shared__ double shd[36 * 4];
@@ -441,6 +444,17 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       if (sl >= 0 && (sl < b0 || sl >= b1)) m |= 1 << dir;
     }
     s_mask[t] = (uint8_t)m;
+  }
+  if (threadIdx.x == 0) {  // remote faces lead, so each warp starts with at most one
+    int n = 0;
+    for (int pass = 0; pass < 2; ++pass)
+      for (int f = 0; f < nt * 6; ++f) {
+        const int sl = s_nbr[f];
+        if (sl < 0) continue;
+        const bool remote = sl < b0 || sl >= b1;
+        if (remote == (pass == 0)) s_forder[n++] = f;
+      }
+    s_nface = n;
   }
   // diagonal (max(count,1)) of remote ring cells, 0 when not fluid
   for (int w = threadIdx.x; w < nt * 384; w += SM_THREADS) {
@@ -527,8 +541,8 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   };
   auto zero_rings = [&]() {  // faces with a neighbouring tile (the others stay 0)
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int f = wid; f < nt * 6; f += SM_THREADS / 32) {
-      if (s_nbr[f] < 0) continue;
+    for (int i = wid; i < s_nface; i += SM_THREADS / 32) {
+      const int f = s_forder[i];
       const int tl = f / 6, dir = f - tl * 6;
       const int base = c_ring_base[dir], ca = c_ring_a[dir], cb = c_ring_b[dir];
 #pragma unroll
@@ -556,7 +570,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
         st_relaxed_u64(HZ + q0 + (tl0 + 2 * j) * 512 + l,
                        tag | __float_as_uint(s_zb[(tl0 + 2 * j) * 1000 + pc]));
     phase_mark(2);
-    ring_fill_tagged(s_zb, s_nbr, nt, b0, b1, s_rdiag, HZ, zep, &st->error);
+    ring_fill_tagged(s_zb, s_nbr, s_forder, s_nface, b0, b1, s_rdiag, HZ, zep, &st->error);
     __syncthreads();
     phase_mark(3);
   };
