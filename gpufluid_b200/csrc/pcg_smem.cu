@@ -289,6 +289,104 @@ __device__ __forceinline__ void ring_fill_tagged(float *s_zb, const int *s_nbr,
   }
 }
 
+// One-round-trip grid sum of the three scalars of an iteration.  No halo
+// data rides on it (the halo words carry their own counts), so it needs no
+// fence: warp 0 publishes the block's three sums as float32 payloads under a
+// 32-bit epoch count in three 64-bit words (relaxed stores, double-buffered by
+// epoch parity), and lane t of warps 0-1 reads the words of blocks t, t+64,
+// t+128 -- all in flight -- until every count matches (bounded spin).  Each
+// lane adds its blocks in order, the warps shuffle-reduce, and the two warps'
+// sums are added in warp order, so every block derives the same totals.  The
+// per-block sums travel as float32 (relative rounding 6e-8); the refined
+// solve's accuracy rests on its FP64 residual replacements, not on these.
+constexpr int FAST_WORDS = 4;  // words per block and parity (3 used)
+constexpr int64_t FAST_SLOTS_OFF = 2048;  // in doubles, into the partials buffer
+struct FastSync {
+  unsigned long long *slots;  // [2][SM_MAXG][FAST_WORDS], zeroed per solve
+  unsigned long long epoch;
+  int *err;
+};
+
+template <typename T>
+__device__ __forceinline__ bool fast_allreduce3(FastSync &fs, GridSync &gs, const T (&v)[3],
+                                                T (&tot)[3], T *sh) {
+  trace_mark(gs);
+  if (gs.trace && threadIdx.x == 0) gs.busy += clock64() - gs.t_last;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  T *s_two = sh + 96;  // [2][3] per-warp totals
+  const unsigned G = gridDim.x;
+  const unsigned long long tag = ((fs.epoch + 1ull) & 0xffffffffull) << 32;
+  unsigned long long *slots = fs.slots + (fs.epoch & 1ull) * (SM_MAXG * FAST_WORDS);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    T w = v[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) w += __shfl_down_sync(0xffffffffu, w, o);
+    if (lane == 0) sh[k * 32 + wid] = w;
+  }
+  __syncthreads();
+  if (wid == 0) {
+    T t0 = sh[lane], t1 = sh[32 + lane], t2 = sh[64 + lane];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      t0 += __shfl_down_sync(0xffffffffu, t0, o);
+      t1 += __shfl_down_sync(0xffffffffu, t1, o);
+      t2 += __shfl_down_sync(0xffffffffu, t2, o);
+    }
+    t0 = __shfl_sync(0xffffffffu, t0, 0);
+    t1 = __shfl_sync(0xffffffffu, t1, 0);
+    t2 = __shfl_sync(0xffffffffu, t2, 0);
+    if (lane < 3) {
+      const float f = (float)(lane == 0 ? t0 : (lane == 1 ? t1 : t2));
+      st_relaxed_u64(slots + blockIdx.x * FAST_WORDS + lane, tag | __float_as_uint(f));
+    }
+  }
+  if (wid < 2) {
+    const unsigned idx = threadIdx.x;
+    bool need[3];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) need[m] = idx + 64u * m < G;
+    unsigned long long w[3][3];
+    long long spins = 0;
+    for (;;) {
+      bool all = true;
+#pragma unroll
+      for (int m = 0; m < 3; ++m)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          w[m][k] = need[m] ? ld_relaxed_u64(slots + (idx + 64u * m) * FAST_WORDS + k) : tag;
+          all &= (w[m][k] & 0xffffffff00000000ull) == tag;
+        }
+      if (all) break;
+      if (++spins > SM_SPIN_LIMIT) {
+        atomicExch(fs.err, 1);
+        break;
+      }
+    }
+    T acc[3] = {(T)0, (T)0, (T)0};
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+        if (need[m]) acc[k] += (T)__uint_as_float((unsigned)w[m][k]);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      T t = acc[k];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+      if (lane == 0) s_two[wid * 3 + k] = t;
+    }
+  }
+  fs.epoch++;
+  __syncthreads();
+  if (*reinterpret_cast<volatile int *>(fs.err)) return false;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) tot[k] = s_two[k] + s_two[3 + k];
+  trace_mark(gs);
+  if (gs.trace && threadIdx.x == 0) gs.t_last = clock64();
+  return true;
+}
+
 template <bool REF>
 struct SmemCfg {
   // per tile: x, r, d, s, w (2048 B each), padded z box (4000 B), code
@@ -393,6 +491,8 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
     return;
   }
   GridSync gs{a.partials, a.counter, &st->error, 0ull, a.trace, 0, a.trace_cap / 2, 0, clock64()};
+  FastSync fs{reinterpret_cast<unsigned long long *>(a.partials + FAST_SLOTS_OFF), 0ull,
+              &st->error};
   // Phases of an iteration for the trace (block thread 0's view, cycles):
   // 0 own update, 1 SGS sweeps, 2 halo publication + neighbour flags +
   // in-block rings, 3 remote rings, 4 stencil and dot products, 5 grid
@@ -604,7 +704,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
     v3[2] += (Acc)(r * r);
   }
   Acc t3[3];
-  if (!grid_allreduce<Acc, 3>(gs, v3, t3, sh)) return;
+  if (!fast_allreduce3<Acc>(fs, gs, v3, t3, sh)) return;
   Acc gamma = t3[0];
   const Acc r0 = t3[2];
   const double b2 = (double)t3[2];
@@ -653,7 +753,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
     }
     phase_mark(4);
     Acc tv[3];
-    if (!grid_allreduce<Acc, 3>(gs, vv, tv, sh)) return;
+    if (!fast_allreduce3<Acc>(fs, gs, vv, tv, sh)) return;
     phase_mark(5);
     iters = it + 1;
     double rr = (double)tv[2];
@@ -726,7 +826,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
         vw[1] += (Acc)(wn * z);
         vw[2] += (Acc)(r * r);
       }
-      if (!grid_allreduce<Acc, 3>(gs, vw, tv, sh)) return;
+      if (!fast_allreduce3<Acc>(fs, gs, vw, tv, sh)) return;
       ++nrep;
       r_upd2 = (double)tv[2];
       rr_last = r_upd2;

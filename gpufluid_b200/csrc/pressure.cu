@@ -1367,6 +1367,11 @@ int launch_pressure(Ctx *c, const gf_step_params *prm) {
       if ((e = check_cuda(c, cudaMemsetAsync(c->bar_counters, 0, BAR_BYTES, st),
                           "zero barrier counters")))
         return e;
+      // the one-round-trip reduction words of the shared-memory solver
+      // ([2][160][4] u64 at 2048 doubles into the partials buffer)
+      if ((e = check_cuda(c, cudaMemsetAsync(c->partials + 2048, 0, 2 * 160 * 4 * 8, st),
+                          "zero reduction words")))
+        return e;
       float *h = c->halo;
       const int64_t nk = c->nkeys;
       PcgSmemArgs sa{c->n_active, c->tile_nbr, c->tile_cost, c->code, c->bdiv, c->xf, h, h + nk, h + 2 * nk,
