@@ -47,11 +47,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = ("FLIP substeps/s @128³ (refined vs plain FP32 PCG, same residual); fwd+adj/s")
 # DRAM bytes (read + write) of one launch of the shared-memory PCG with the
-# tile SGS preconditioner on this workload, from an ncu capture: 7,110,912
-# read + 416,768 written.  The solve's vectors stay in shared memory; only
-# the input, result, halos and the FP64 replacement steps touch DRAM, far
-# below the algorithmic bytes of a streaming PCG.
-PCG_DRAM_BYTES = 7110912 + 416768
+# tile SGS preconditioner on this workload, from an ncu capture: 8,792,064
+# read + 690,432 written.  The solve's vectors stay in shared memory; only
+# the input, result, tagged halo words and the FP64 replacement steps touch
+# DRAM, far below the algorithmic bytes of a streaming PCG.
+PCG_DRAM_BYTES = 8792064 + 690432
 GRID = 128
 DT = 1.0 / 480.0
 TOL = 1e-8
@@ -87,7 +87,11 @@ class ClockSampler:
         self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
 
     def start(self):
+        """Start sampling and return once the first sample is written (the tool
+        takes about a second to start), so the samples cover the timed region;
+        samples taken before the return are not counted."""
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        self.skip = 0
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
@@ -96,6 +100,15 @@ class ClockSampler:
                 stdout=self.f, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return
+        t0 = time.time()
+        while time.time() - t0 < 10.0 and self.proc.poll() is None:
+            with open(self.path) as f:
+                n = sum(1 for _ in f)
+            if n > 0:
+                self.skip = n
+                return
+            time.sleep(0.05)
 
     def stop(self):
         if self.proc is None:
@@ -108,7 +121,9 @@ class ClockSampler:
         self.f.close()
         rows = []
         with open(self.path) as f:
-            for line in f:
+            lines = f.readlines()
+            lines = lines[self.skip:] or lines  # samples of the timed region
+            for line in lines:
                 parts = [p.strip() for p in line.split(",")]
                 if len(parts) < 9:
                     continue
