@@ -418,6 +418,45 @@ def batched_adjoint_leg(torch, device, n_scenes=64, reps=1, ranks=None):
             "speedup": round(t_single / t_batch, 3)}
 
 
+def outflow_leg(torch, s, hbm, reps=20):
+    """GPU outflow compaction (gf_outflow_compact) of the bench scene's
+    particles against a slab y <= 0.05 that holds a tenth of them: device
+    time per call (it synchronises for the new count) and algorithmic bytes
+    (positions read twice, velocities once, survivors written: 36 B per
+    particle + 24 B per survivor) against the copy peak."""
+    import ctypes
+    from gpufluid_b200 import _lib
+    pos, vel = s._unsort(s._pos), s._unsort(s._vel)
+    n = pos.shape[0]
+    po, vo = torch.empty_like(pos), torch.empty_like(vel)
+    box = np.ascontiguousarray(np.float32([[0.0, 0.0, 0.0, 1.0, 0.05, 1.0]]))
+    bp = box.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    nout = ctypes.c_int64()
+    s._set_stream()
+
+    def call():
+        _lib.check(s._L.gf_outflow_compact(s._ctx, pos.data_ptr(), vel.data_ptr(), n, bp, 1,
+                                           po.data_ptr(), vo.data_ptr(), ctypes.byref(nout)),
+                   s._ctx, "gf_outflow_compact")
+    for _ in range(3):
+        call()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        call()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    kept = int(nout.value)
+    gbs = (36.0 * n + 24.0 * kept) / 1e9 / (ms / 1e3)
+    return {"workload": "outflow slab y <= 0.05 over the 128^3 scene's particles",
+            "particles": int(n), "kept": kept, "ms_per_call": round(ms, 4),
+            "particles_per_s": round(n / (ms / 1e3), 1), "gbs": round(gbs, 1),
+            "frac": round(gbs / hbm, 4)}
+
+
 def stage_bytes_flip(P, ncell_active, F):
     """Algorithmic bytes of the FLIP (non-APIC) stages: sort 64P + 12N,
     P2G 24P + 24F (the zeroing of the six P2G face arrays counted as for
@@ -606,6 +645,8 @@ def run_ours(args):
     ms_e2e = max_over_ranks(e0.elapsed_time(e1) / args.steps)
     barrier()
 
+    outflow = outflow_leg(torch, s, hbm)
+
     fwd_adj = None if args.no_adjoint else adjoint_leg(torch, device)
     fwd_adj_apic = None if args.no_adjoint else adjoint_leg(torch, device, transfer="apic")
     batched = None if args.no_batched else batched_leg(torch, device, ranks=ranks)
@@ -671,6 +712,7 @@ def run_ours(args):
             "batched": batched,
             "batched_fwd_adj": batched_adj,
             "other_configs": extra,
+            "outflow_compaction": outflow,
         }
         print(json.dumps(line), flush=True)
     ranks.close()

@@ -108,6 +108,8 @@ _SIGS = {
     "gf_stage_times": ([_vp, _fp], ctypes.c_int),
     "gf_active_tiles": ([_vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(_vp)], ctypes.c_int),
     "gf_vmax": ([_vp, _fp], ctypes.c_int),
+    "gf_outflow_compact": ([_vp, _vp, _vp, ctypes.c_int64, _fp, ctypes.c_int32, _vp, _vp,
+                            ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
     "gf_pressure_stats": ([_vp, ctypes.POINTER(PressureInfo)], ctypes.c_int),
     "gf_pcg_trace": ([_vp, _vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
     "gf_record_bytes": ([_vp, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),

@@ -67,8 +67,6 @@ def make_solver(scene, args):
     sim = scene.simulation
     if sim.solver != "flip":
         raise BlockError("C7.1", f"solver {sim.solver!r} is not part of this build (flip only)")
-    if scene.inflow or scene.outflow:
-        raise BlockError("C7.1", "inflow/outflow regions are not part of this build")
     if sim.reseed:
         raise BlockError("C7.1", "reseeding is not part of this build")
     nx, ny, nz = scene.domain.resolution
@@ -89,6 +87,19 @@ def make_solver(scene, args):
     sdf = build_obstacle_sdf(scene, solver.cell_centers_np())
     if sdf is not None:
         solver.add_solid_from_sdf(sdf)
+    # inflows / outflows (commands.py:512-530)
+    from .regions import InflowBox, OutflowBox
+    try:
+        for inf in scene.inflow:
+            solver.add_inflow(InflowBox(lo=inf.lo, hi=inf.hi, velocity=inf.velocity,
+                                        rate_per_sec=inf.rate_per_sec,
+                                        frame_start=inf.frame_start, frame_end=inf.frame_end,
+                                        color=inf.color, temperature=inf.temperature))
+        for out in scene.outflow:
+            solver.add_outflow(OutflowBox(lo=out.lo, hi=out.hi, frame_start=out.frame_start,
+                                          frame_end=out.frame_end))
+    except ValueError as e:
+        raise BlockError("C7.1", str(e)) from None
     return solver
 
 

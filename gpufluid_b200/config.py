@@ -3,7 +3,7 @@
 The sections and keys a FLIP/PIC/APIC scene uses parse exactly as in the
 reference, with the same defaults, into dataclasses of the same names.  The
 keys are [domain], [fluid], [[fluids]], [[obstacle]] (sphere, box,
-cylinder_y, plane), [simulation] and [output].  Problems raise
+cylinder_y, plane), [[inflow]], [[outflow]], [simulation] and [output].  Problems raise
 ``BlockError("C7.1", ...)`` as the reference does (config.py:297-300, :382,
 :390).
 
@@ -13,7 +13,7 @@ reference PCG's), ``pcg_check_every`` (10).
 
 Sections outside this build parse, but a scene that uses them is rejected
 with BlockError("C7.1") when the solver is built: mesh fluids and obstacles,
-inflow/outflow, obstacle motion, and an MPM solver.
+obstacle motion, reseeding, and an MPM solver.
 """
 from __future__ import annotations
 
@@ -144,14 +144,37 @@ class OutputCfg:
 
 
 @dataclass
+class InflowCfg:
+    """config.py:140-158 (``keyframes`` moves MPM emitters only; FLIP ignores it)."""
+    lo: Tuple[float, float, float]
+    hi: Tuple[float, float, float]
+    velocity: Tuple[float, float, float] = (0.0, 0.0, 0.0)
+    rate_per_sec: float = 5000.0
+    frame_start: int = 0
+    frame_end: int = 1_000_000
+    keyframes: List[List[float]] = field(default_factory=list)
+    color: Optional[Tuple[float, float, float]] = None
+    temperature: Optional[float] = None
+
+
+@dataclass
+class OutflowCfg:
+    """config.py:161-166."""
+    lo: Tuple[float, float, float]
+    hi: Tuple[float, float, float]
+    frame_start: int = 0
+    frame_end: int = 1_000_000
+
+
+@dataclass
 class SceneCfg:
     domain: DomainCfg = field(default_factory=DomainCfg)
     fluid: object = field(default_factory=FluidBoxCfg)
     fluids: List[object] = field(default_factory=list)
     obstacle: List[ObstacleCfg] = field(default_factory=list)
     obstacle_motion: List[Optional[dict]] = field(default_factory=list)
-    inflow: List[dict] = field(default_factory=list)
-    outflow: List[dict] = field(default_factory=list)
+    inflow: List[InflowCfg] = field(default_factory=list)
+    outflow: List[OutflowCfg] = field(default_factory=list)
     simulation: SimulationCfg = field(default_factory=SimulationCfg)
     output: OutputCfg = field(default_factory=OutputCfg)
     config_dir: Optional[Path] = None
@@ -172,6 +195,32 @@ def _tuple(seq, n, name):
     if not isinstance(seq, Sequence) or isinstance(seq, str) or len(seq) != n:
         raise BlockError("C7.1", f"{name}: expected list of {n}; got {seq!r}")
     return tuple(seq)
+
+
+def _parse_inflow(d: dict) -> InflowCfg:
+    """config.py:319-333."""
+    try:
+        return InflowCfg(
+            lo=_tuple(d["lo"], 3, "inflow.lo"), hi=_tuple(d["hi"], 3, "inflow.hi"),
+            velocity=_tuple(d.get("velocity", [0, 0, 0]), 3, "inflow.velocity"),
+            rate_per_sec=float(d.get("rate_per_sec", 5000.0)),
+            frame_start=int(d.get("frame_start", 0)),
+            frame_end=int(d.get("frame_end", 1_000_000)),
+            keyframes=[[float(v) for v in row] for row in d.get("keyframes", [])],
+            color=_tuple(d["color"], 3, "inflow.color") if "color" in d else None,
+            temperature=float(d["temperature"]) if "temperature" in d else None)
+    except KeyError as e:
+        raise BlockError("C7.1", f"inflow: missing key {e.args[0]!r}") from None
+
+
+def _parse_outflow(d: dict) -> OutflowCfg:
+    """config.py:336-342."""
+    try:
+        return OutflowCfg(lo=_tuple(d["lo"], 3, "outflow.lo"), hi=_tuple(d["hi"], 3, "outflow.hi"),
+                          frame_start=int(d.get("frame_start", 0)),
+                          frame_end=int(d.get("frame_end", 1_000_000)))
+    except KeyError as e:
+        raise BlockError("C7.1", f"outflow: missing key {e.args[0]!r}") from None
 
 
 def _parse_fluid(fl: dict) -> object:
@@ -257,6 +306,8 @@ def load_scene(path: Union[str, Path]) -> SceneCfg:
             okw[name] = type(default)(v) if not isinstance(default, bool) else bool(v)
     output = OutputCfg(**okw)
     return SceneCfg(domain=domain, fluid=fluid, fluids=fluids, obstacle=obstacles,
-                    obstacle_motion=motions, inflow=list(raw.get("inflow", [])),
-                    outflow=list(raw.get("outflow", [])), simulation=simulation, output=output,
+                    obstacle_motion=motions,
+                    inflow=[_parse_inflow(d) for d in raw.get("inflow", [])],
+                    outflow=[_parse_outflow(d) for d in raw.get("outflow", [])],
+                    simulation=simulation, output=output,
                     config_dir=p.parent.resolve())

@@ -57,7 +57,7 @@ static void destroy(Ctx *c) {
   free_particles(c);
   void *ps[] = {c->count, c->start, c->scan_part, c->vmax_dev, c->adj_faces, c->adj_part,
                 c->seg, c->seg_off, c->seg_state, c->seg_slot0, c->pcg_blk_job0,
-                c->pcg_jobs};
+                c->pcg_jobs, c->region_scratch};
   for (void *p : ps)
     if (p) cudaFree(p);
   if (c->seg_state_host) cudaFreeHost(c->seg_state_host);

@@ -130,6 +130,9 @@ struct Ctx {
   // caller buffers
   gf_fields f{};
   gf_particles p{};
+  // outflow compaction scratch (block counts, offsets, boxes), grown on use
+  int32_t *region_scratch = nullptr;
+  int64_t region_scratch_n = 0;
   bool bound = false;
 
   // binning scratch

@@ -188,6 +188,8 @@ class FlipSolver3D:
         self.attr_temperature = None
         self.inflows: list = []
         self.outflows: list = []
+        # emission generator of the inflows (solver3d.py:2494)
+        self._rng = np.random.default_rng(0)
 
         dev = self.device
         z = lambda *s: torch.zeros(s, dtype=torch.float32, device=dev)  # noqa: E731
@@ -456,11 +458,64 @@ class FlipSolver3D:
             self.step(sub_dt, pressure_iters=pressure_iters, pressure_solver=pressure_solver)
         return n
 
+    def add_inflow(self, region) -> None:
+        """Register an ``InflowBox`` (solver3d.py:2635-2636)."""
+        self.inflows.append(region)
+
+    def add_outflow(self, region) -> None:
+        """Register an ``OutflowBox`` (solver3d.py:2639-2640)."""
+        self.outflows.append(region)
+
     def prepare_frame(self, frame_idx: int, frame_dt: float) -> None:
-        """Per-frame hook (solver3d.py:3909-4072).  Static scenes need no
-        work: animated obstacles and inflow/outflow are outside this build."""
-        if self.inflows or self.outflows:
-            raise NotImplementedError("inflow/outflow regions are outside this build")
+        """Per-frame hook (solver3d.py:3909-4072) for inflow/outflow regions.
+
+        Outflows first: the particles inside any active outflow box are
+        removed on the GPU by stream compaction (``gf_outflow_compact``,
+        survivors in their order).  Then the active inflows emit in
+        registration order from the solver's seeded generator; emitted
+        positions in a solid cell are dropped (solver3d.py:3985-4017) and the
+        rest are appended with their box's velocity.  When the particle count
+        changes, the APIC matrices restart at zero, as the reference drops
+        affine_C.  Animated obstacles are outside this build."""
+        from .regions import apply_inflows, outflow_box_array
+        self._cuda_graph_invalidate()
+        boxes = outflow_box_array(self.outflows, frame_idx)
+        n = self.n_particles
+        if len(boxes) and n:
+            pos = self._unsort(self._pos)
+            vel = self._unsort(self._vel)
+            pos_out, vel_out = torch.empty_like(pos), torch.empty_like(vel)
+            n_out = _lib.ctypes.c_int64()
+            self._set_stream()
+            boxes = np.ascontiguousarray(boxes)
+            _lib.check(self._L.gf_outflow_compact(
+                self._ctx, pos.data_ptr(), vel.data_ptr(), n,
+                boxes.ctypes.data_as(_lib.ctypes.POINTER(_lib.ctypes.c_float)), len(boxes),
+                pos_out.data_ptr(), vel_out.data_ptr(), _lib.ctypes.byref(n_out)),
+                self._ctx, "gf_outflow_compact")
+            m = int(n_out.value)
+            if m != n:
+                self._set_particles(pos=pos_out[:m], vel=vel_out[:m],
+                                    C=torch.zeros((m, 3, 3), dtype=torch.float32,
+                                                  device=self.device))
+        emit_pos, emit_vel = apply_inflows(self.inflows, frame_idx, frame_dt, self._rng)
+        if len(emit_pos):
+            mh = self._marker_host
+            ix = np.clip((emit_pos[:, 0] / self.dx).astype(np.int32), 0, mh.shape[0] - 1)
+            iy = np.clip((emit_pos[:, 1] / self.dx).astype(np.int32), 0, mh.shape[1] - 1)
+            iz = np.clip((emit_pos[:, 2] / self.dx).astype(np.int32), 0, mh.shape[2] - 1)
+            keep = mh[ix, iy, iz] != 2
+            emit_pos, emit_vel = emit_pos[keep], emit_vel[keep]
+        if len(emit_pos):
+            dev = self.device
+            new_p = torch.from_numpy(np.ascontiguousarray(emit_pos)).to(dev)
+            new_v = torch.from_numpy(np.ascontiguousarray(emit_vel)).to(dev)
+            if self.n_particles:
+                new_p = torch.cat([self._unsort(self._pos), new_p])
+                new_v = torch.cat([self._unsort(self._vel), new_v])
+            m = new_p.shape[0]
+            self._set_particles(pos=new_p, vel=new_v,
+                                C=torch.zeros((m, 3, 3), dtype=torch.float32, device=dev))
 
     # ------------------------------------------------------------- results
     def get_particles(self):

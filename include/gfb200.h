@@ -181,6 +181,18 @@ int gf_active_tiles(void *ctx, int32_t *n_active, const int32_t **tiles);
 /* Device |v|^2 max for CFL substepping (k3_vmax_sq_reduce :2241-2252);
  * synchronises. */
 int gf_vmax(void *ctx, float *vmax_out);
+/* Outflow regions (k3_mark_alive_outflows + k3_scatter_alive,
+ * solver3d.py:1943-1985, driven by _apply_outflows_gpu :2659-2730): copies the
+ * n particles (device pos, vel, (n,3) float32) that lie inside none of the
+ * nbox boxes (host array of nbox x {lo.x, lo.y, lo.z, hi.x, hi.y, hi.z};
+ * inside means lo <= p <= hi on all axes) to pos_out / vel_out (device, room
+ * for n, not overlapping the inputs), keeping their order, and writes the new
+ * count to *n_out.  Runs on the bound stream and synchronises for the count;
+ * allocates its scratch in the context on first use.  A box with hi < lo is
+ * GF_INVALID_ARG. */
+int gf_outflow_compact(void *ctx, const float *pos, const float *vel, int64_t n,
+                       const float *boxes, int32_t nbox, float *pos_out, float *vel_out,
+                       int64_t *n_out);
 
 /* ---- adjoint (differentiation through substeps) ------------------------- */
 /* No counterpart in the reference (planned only there).  PIC transfer

@@ -107,11 +107,52 @@ def test_out_of_scope_rejected(tmp_path, extra, what):
     assert what in str(ei.value)
 
 
-def test_inflow_rejected(tmp_path):
+_REGIONS = """
+[[inflow]]
+lo = [0.1, 0.7, 0.1]
+hi = [0.3, 0.8, 0.3]
+velocity = [0.0, -1.0, 0.0]
+rate_per_sec = 2400.0
+
+[[outflow]]
+lo = [0.0, 0.0, 0.0]
+hi = [1.0, 0.12, 1.0]
+frame_start = 1
+"""
+
+
+def test_inflow_outflow_parse(tmp_path):
+    """[[inflow]] / [[outflow]] parse with the reference's keys and defaults
+    (config.py:140-166, :319-342)."""
+    from gpufluid_b200.config import InflowCfg, OutflowCfg
     cfg = _write_minimal(tmp_path)
-    cfg.write_text(cfg.read_text() + '\n[[inflow]]\nlo = [0,0,0]\nhi = [0.1,0.1,0.1]\n')
+    cfg.write_text(cfg.read_text() + _REGIONS)
+    scene = load_scene(cfg)
+    assert scene.inflow == [InflowCfg(lo=(0.1, 0.7, 0.1), hi=(0.3, 0.8, 0.3),
+                                      velocity=(0.0, -1.0, 0.0), rate_per_sec=2400.0)]
+    assert scene.inflow[0].frame_end == 1_000_000 and scene.inflow[0].color is None
+    assert scene.outflow == [OutflowCfg(lo=(0.0, 0.0, 0.0), hi=(1.0, 0.12, 1.0), frame_start=1)]
+    (tmp_path / "b").mkdir()
+    bad = _write_minimal(tmp_path / "b")
+    bad.write_text(bad.read_text() + "\n[[outflow]]\nlo = [0, 0, 0]\n")
     with pytest.raises(BlockError):
-        make_solver(load_scene(cfg), None)
+        load_scene(bad)
+
+
+@pytest.mark.gpu
+def test_simulate_with_inflow_and_outflow(tmp_path):
+    """The inflow adds round(2400/24) = 100 positions a frame (fewer if any
+    land in a solid cell); from frame 1 the outflow slab y <= 0.12 drains."""
+    cfg = _write_minimal(tmp_path, frames=3)
+    cfg.write_text(cfg.read_text() + _REGIONS)
+    assert main(["simulate", str(cfg)]) == 0
+    counts = [len(np.load(tmp_path / "cache" / "particles" / f"frame_{f:04d}.npy"))
+              for f in range(3)]
+    seeded = len(sc.seed_box_positions(1.0 / 16, (0.10, 0.30, 0.10), (0.50, 0.90, 0.50), 8))
+    assert counts[0] == seeded + 100
+    assert counts[1] <= counts[0] + 100 and counts[2] <= counts[1] + 100
+    last = np.load(tmp_path / "cache" / "particles" / "frame_0002.npy")
+    assert np.isfinite(last).all()
 
 
 def test_cli_error_exit_code(tmp_path, capsys):
