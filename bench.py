@@ -457,6 +457,30 @@ def outflow_leg(torch, s, hbm, reps=20):
             "frac": round(gbs / hbm, 4)}
 
 
+def reseed_leg(torch, s, snap, reps=5):
+    """FlipSolver3D.reseed (device binning, rank cull and compaction; host
+    emission list from the per-cell counts) on the bench scene's particle
+    state with the reference's default bounds (4..16 per cell): wall time per
+    call with device synchronisation, from the same state each time."""
+    from gpufluid_b200.reseed import ReseedConfig
+    cfg = ReseedConfig()
+    restore(s, snap)
+    base = [s._unsort(t).clone() for t in (s._pos, s._vel, s._C)]
+    ts, res = [], None
+    for r in range(reps + 1):
+        s._set_particles(pos=base[0], vel=base[1], C=base[2])
+        s.step(DT, pressure_iters=MAX_ITERS, pressure_solver="pcg_refined")  # labels of a substep
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = s.reseed(cfg, np.random.default_rng(123))
+        torch.cuda.synchronize()
+        if r:
+            ts.append(time.perf_counter() - t0)
+    return {"workload": "reseed of the 128^3 scene after one substep, 4..16 per cell",
+            "particles_before": int(snap[0].shape[0]), "emitted": int(res[0]),
+            "culled": int(res[1]), "ms_per_call": round(1e3 * float(np.median(ts)), 3)}
+
+
 def stage_bytes_flip(P, ncell_active, F):
     """Algorithmic bytes of the FLIP (non-APIC) stages: sort 64P + 12N,
     P2G 24P + 24F (the zeroing of the six P2G face arrays counted as for
@@ -646,6 +670,7 @@ def run_ours(args):
     barrier()
 
     outflow = outflow_leg(torch, s, hbm)
+    reseed = reseed_leg(torch, s, snap)
 
     fwd_adj = None if args.no_adjoint else adjoint_leg(torch, device)
     fwd_adj_apic = None if args.no_adjoint else adjoint_leg(torch, device, transfer="apic")
@@ -713,6 +738,7 @@ def run_ours(args):
             "batched_fwd_adj": batched_adj,
             "other_configs": extra,
             "outflow_compaction": outflow,
+            "reseed": reseed,
         }
         print(json.dumps(line), flush=True)
     ranks.close()

@@ -67,8 +67,6 @@ def make_solver(scene, args):
     sim = scene.simulation
     if sim.solver != "flip":
         raise BlockError("C7.1", f"solver {sim.solver!r} is not part of this build (flip only)")
-    if sim.reseed:
-        raise BlockError("C7.1", "reseeding is not part of this build")
     nx, ny, nz = scene.domain.resolution
     try:
         solver = FlipSolver3D(nx=nx, ny=ny, nz=nz, dx=scene.dx, gravity=sim.gravity,
@@ -142,8 +140,19 @@ def cmd_simulate(args) -> int:
     t_sim = 0.0
     truncated = None
     import torch
+    # reseeding every reseed_every_n_frames frames (commands.py:612-660)
+    rng_reseed = np.random.default_rng(123)
+    reseed_cfg = None
+    if sim.reseed:
+        from .reseed import ReseedConfig
+        reseed_cfg = ReseedConfig(min_per_cell=sim.reseed_min_per_cell,
+                                  max_per_cell=sim.reseed_max_per_cell,
+                                  every_n_frames=sim.reseed_every_n_frames)
     for frame in range(start_frame, sim.frames):
         solver.prepare_frame(frame, 1.0 / sim.fps)
+        if (reseed_cfg is not None and frame % reseed_cfg.every_n_frames == 0
+                and solver.n_particles > 0):
+            solver.reseed(reseed_cfg, rng_reseed)
         torch.cuda.synchronize()
         ts = time.time()
         if sim.cfl:

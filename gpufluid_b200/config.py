@@ -13,7 +13,7 @@ reference PCG's), ``pcg_check_every`` (10).
 
 Sections outside this build parse, but a scene that uses them is rejected
 with BlockError("C7.1") when the solver is built: mesh fluids and obstacles,
-obstacle motion, reseeding, and an MPM solver.
+obstacle motion, and an MPM solver.
 """
 from __future__ import annotations
 

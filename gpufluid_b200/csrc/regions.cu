@@ -1,6 +1,14 @@
-// Outflow regions: GPU stream compaction of the particles that leave through
+// Particle-count-changing steps beside the substep, on the GPU:
+//
+// Outflow regions: stream compaction of the particles that leave through
 // outflow boxes (solver3d.py:1943-1985 k3_mark_alive_outflows +
 // k3_scatter_alive, driven by _apply_outflows_gpu :2659-2730).
+//
+// Reseeding (reseed.py:161-396, reseed_particles_gpu): the binning ranks each
+// particle in its cell by id; k_reseed_mark keeps the first max_per_cell of
+// each non-solid cell and k_reseed_counts returns the dense per-cell counts
+// from which the host builds the emission list; the survivors are compacted
+// by the same three launches as the outflows (gf_compact_alive).
 //
 // A particle is removed when it lies inside ANY box (lo <= p <= hi on all
 // three axes, float32 compares); the survivors keep their relative order
@@ -24,11 +32,13 @@ struct RegionArgs {
   float *pos_out, *vel_out;
   const float *box;  // nbox x (lo.xyz, hi.xyz)
   int nbox;
+  const int32_t *alive_in;  // non-null: keep where nonzero (boxes unused)
   int64_t n;
   int32_t *counts;   // [nb] then offsets [nb] then total [1]
 };
 
 __device__ __forceinline__ bool alive_of(const RegionArgs &a, int64_t i) {
+  if (a.alive_in) return a.alive_in[i] != 0;
   const float x = a.pos[3 * i], y = a.pos[3 * i + 1], z = a.pos[3 * i + 2];
   bool alive = true;
   for (int j = 0; j < a.nbox; ++j) {
@@ -103,6 +113,72 @@ __global__ void __launch_bounds__(RG_BLOCK) k_alive_scatter(RegionArgs a, int nb
   }
 }
 
+
+// The three compaction launches and the read-back of the new count.
+static int compact_run(Ctx *c, RegionArgs &a, int nb, int64_t *n_out, const char *what) {
+  cudaStream_t st = c->stream;
+  int e;
+  k_alive_count<<<nb, RG_BLOCK, 0, st>>>(a);
+  k_alive_offsets<<<1, RG_BLOCK, 0, st>>>(a.counts, nb);
+  k_alive_scatter<<<nb, RG_BLOCK, 0, st>>>(a, nb);
+  c->launches += 3;
+  if ((e = check_launch(c, what))) return e;
+  int32_t total = 0;
+  if ((e = check_cuda(c, cudaMemcpyAsync(&total, a.counts + 2 * (int64_t)nb, 4,
+                                         cudaMemcpyDeviceToHost, st),
+                      "read compacted count")))
+    return e;
+  if ((e = check_cuda(c, cudaStreamSynchronize(st), "compacted count sync"))) return e;
+  *n_out = total;
+  return GF_OK;
+}
+
+// Block counts [nb], offsets [nb + 1] and `extra` floats, grown on use.
+static int region_scratch(Ctx *c, int nb, int64_t extra, int32_t **out) {
+  const int64_t need = 2 * (int64_t)nb + 1 + extra;
+  if (c->region_scratch_n < need) {
+    if (c->region_scratch) cudaFree(c->region_scratch);
+    c->region_scratch = nullptr;
+    c->region_scratch_n = 0;
+    int e = check_cuda(c, cudaMalloc(&c->region_scratch, need * 4), "alloc compaction scratch");
+    if (e) return e;
+    c->region_scratch_n = need;
+  }
+  *out = c->region_scratch;
+  return GF_OK;
+}
+
+// Reseed culling (k_count_particles_per_cell + k_mark_keep_by_rank,
+// reseed.py:161-222) on the binned particles: sorted position q holds
+// storage slot order[q] with cell key key[slot]; its rank in the cell is
+// q - start[key], the binning's canonical order being the particles' ids.
+// alive is written by id (original order).
+__global__ void k_reseed_mark(const int32_t *__restrict__ order, const int32_t *__restrict__ key,
+                              const int32_t *__restrict__ start, const int32_t *__restrict__ pid,
+                              const uint8_t *__restrict__ label, int64_t n, int max_per_cell,
+                              int ny, int nz, int nty, int ntz, int32_t *__restrict__ alive) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int slot = order[q];
+  const int k = key[slot];
+  const int rank = (int)(q - start[k]);
+  const int t = k >> 9, l = k & 511;
+  const int ti = t / (nty * ntz), tj = (t / ntz) % nty, tk = t % ntz;
+  const int64_t cell = ((int64_t)(ti * 8 + (l >> 6)) * ny + (tj * 8 + ((l >> 3) & 7))) * nz +
+                       (tk * 8 + (l & 7));
+  alive[pid[slot]] = (label[cell] != 2 && rank < max_per_cell) ? 1 : 0;
+}
+
+// Particles per cell, dense C order, from the binning's per-key counts.
+__global__ void k_reseed_counts(const int32_t *__restrict__ count, int nx, int ny, int nz,
+                                int nty, int ntz, int32_t *__restrict__ dense) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= (int64_t)nx * ny * nz) return;
+  const int k = (int)(c % nz), j = (int)((c / nz) % ny), i = (int)(c / ((int64_t)ny * nz));
+  const int t = ((i >> 3) * nty + (j >> 3)) * ntz + (k >> 3);
+  dense[c] = count[t * 512 + ((i & 7) * 8 + (j & 7)) * 8 + (k & 7)];
+}
+
 }  // namespace gf
 
 using gf::Ctx;
@@ -122,44 +198,62 @@ int gf_outflow_compact(void *ctx, const float *pos, const float *vel, int64_t n,
     for (int d = 0; d < 3; ++d)
       if (boxes[6 * j + 3 + d] < boxes[6 * j + d])
         return gf::fail(c, GF_INVALID_ARG, "gf_outflow_compact: a box has hi < lo");
-  cudaStream_t st = c->stream;
-  int e;
   if (n == 0) {
     *n_out = 0;
     return GF_OK;
   }
   const int nb = (int)((n + gf::RG_BLOCK - 1) / gf::RG_BLOCK);
-  // scratch: counts [nb], offsets [nb + 1], then the boxes (6 floats each)
-  const int64_t need = 2 * (int64_t)nb + 1 + 6 * (int64_t)(nbox > 0 ? nbox : 1);
-  if (c->region_scratch_n < need) {
-    if (c->region_scratch) cudaFree(c->region_scratch);
-    c->region_scratch = nullptr;
-    c->region_scratch_n = 0;
-    if ((e = gf::check_cuda(c, cudaMalloc(&c->region_scratch, need * 4), "alloc outflow scratch")))
-      return e;
-    c->region_scratch_n = need;
-  }
-  int32_t *counts = c->region_scratch;
+  int32_t *counts = nullptr;
+  int e = gf::region_scratch(c, nb, 6 * (int64_t)(nbox > 0 ? nbox : 1), &counts);
+  if (e) return e;
   float *dbox = reinterpret_cast<float *>(counts + 2 * (int64_t)nb + 1);
   if (nbox > 0 &&
       (e = gf::check_cuda(c, cudaMemcpyAsync(dbox, boxes, (size_t)nbox * 6 * 4,
-                                             cudaMemcpyHostToDevice, st),
+                                             cudaMemcpyHostToDevice, c->stream),
                           "copy outflow boxes")))
     return e;
-  gf::RegionArgs a{pos, vel, pos_out, vel_out, dbox, nbox, n, counts};
-  gf::k_alive_count<<<nb, gf::RG_BLOCK, 0, st>>>(a);
-  gf::k_alive_offsets<<<1, gf::RG_BLOCK, 0, st>>>(counts, nb);
-  gf::k_alive_scatter<<<nb, gf::RG_BLOCK, 0, st>>>(a, nb);
-  c->launches += 3;
-  if ((e = gf::check_launch(c, "gf_outflow_compact"))) return e;
-  int32_t total = 0;
-  if ((e = gf::check_cuda(c, cudaMemcpyAsync(&total, counts + 2 * (int64_t)nb, 4,
-                                             cudaMemcpyDeviceToHost, st),
-                          "read outflow count")))
-    return e;
-  if ((e = gf::check_cuda(c, cudaStreamSynchronize(st), "outflow count sync"))) return e;
-  *n_out = total;
-  return GF_OK;
+  gf::RegionArgs a{pos, vel, pos_out, vel_out, dbox, nbox, nullptr, n, counts};
+  return gf::compact_run(c, a, nb, n_out, "gf_outflow_compact");
+}
+
+int gf_compact_alive(void *ctx, const float *pos, const float *vel, int64_t n,
+                     const int32_t *alive, float *pos_out, float *vel_out, int64_t *n_out) {
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);
+  if (!c || !n_out || n < 0 || (n > 0 && (!pos || !vel || !alive || !pos_out || !vel_out)))
+    return GF_INVALID_ARG;
+  if (n > INT32_MAX)
+    return gf::fail(c, GF_INVALID_ARG, "gf_compact_alive: particle count exceeds int32 range");
+  if (n == 0) {
+    *n_out = 0;
+    return GF_OK;
+  }
+  const int nb = (int)((n + gf::RG_BLOCK - 1) / gf::RG_BLOCK);
+  int32_t *counts = nullptr;
+  int e = gf::region_scratch(c, nb, 0, &counts);
+  if (e) return e;
+  gf::RegionArgs a{pos, vel, pos_out, vel_out, nullptr, 0, alive, n, counts};
+  return gf::compact_run(c, a, nb, n_out, "gf_compact_alive");
+}
+
+int gf_reseed_mark(void *ctx, int32_t max_per_cell, int32_t *alive, int32_t *counts) {
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);
+  if (!c || !counts || max_per_cell < 0 || (c->p.n > 0 && !alive)) return GF_INVALID_ARG;
+  if (!c->bound) return gf::fail(c, GF_INVALID_ARG, "gf_reseed_mark: buffers not bound");
+  if (c->nseg > 0) return gf::fail(c, GF_INVALID_ARG, "gf_reseed_mark: single-grid contexts only");
+  int e = gf::launch_bin(c, GF_FLIP);
+  if (e) return e;
+  cudaStream_t st = c->stream;
+  const int64_t n = c->p.n;
+  if (n > 0) {
+    gf::k_reseed_mark<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(
+        c->order, c->key, c->start, c->p.pid, c->f.label, n, max_per_cell, c->ny, c->nz,
+        c->nty, c->ntz, alive);
+    c->launches++;
+  }
+  gf::k_reseed_counts<<<(unsigned)((c->ncell + 255) / 256), 256, 0, st>>>(
+      c->count, c->nx, c->ny, c->nz, c->nty, c->ntz, counts);
+  c->launches++;
+  return gf::check_launch(c, "gf_reseed_mark");
 }
 
 }  // extern "C"

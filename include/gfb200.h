@@ -193,6 +193,19 @@ int gf_vmax(void *ctx, float *vmax_out);
 int gf_outflow_compact(void *ctx, const float *pos, const float *vel, int64_t n,
                        const float *boxes, int32_t nbox, float *pos_out, float *vel_out,
                        int64_t *n_out);
+/* The same compaction with a per-particle keep flag (alive[i] != 0, device
+ * int32[n]) in place of the boxes: k3_scatter_alive / k_scatter_alive_pv
+ * (solver3d.py:1968-1985, reseed.py:226-243). */
+int gf_compact_alive(void *ctx, const float *pos, const float *vel, int64_t n,
+                     const int32_t *alive, float *pos_out, float *vel_out, int64_t *n_out);
+/* Reseed culling on the bound particles (k_count_particles_per_cell +
+ * k_mark_keep_by_rank, reseed.py:161-222): bins them (as gf_bin; labels are
+ * recomputed from the current positions), then writes alive[id] = 1 for the
+ * first max_per_cell particles by id of each non-solid cell and 0 otherwise
+ * (the reference ranks by atomic arrival; ranking by id is one of its
+ * orders), and counts[nx*ny*nz] (device int32, C order) = particles per
+ * cell.  Single-grid contexts; the bound pid must hold ids 0..n-1. */
+int gf_reseed_mark(void *ctx, int32_t max_per_cell, int32_t *alive, int32_t *counts);
 
 /* ---- adjoint (differentiation through substeps) ------------------------- */
 /* No counterpart in the reference (planned only there).  PIC transfer

@@ -252,11 +252,13 @@ def sqrt(x):
 
 
 def atomic_add(arr, *idx_val):
+    """Adds and returns the value before the add (Warp's atomic_add)."""
     *idx, val = idx_val
     base = arr.view(np.ndarray)
     idx = tuple(int(i) for i in idx)
+    old = base[idx].copy()
     base[idx] = base[idx] + val
-    return base[idx]
+    return old
 
 
 def atomic_max(arr, *idx_val):

@@ -97,7 +97,6 @@ def test_bad_vector_length_raises(tmp_path):
 
 @pytest.mark.parametrize("extra, what", [
     ('solver = "mpm"', "flip only"),
-    ("reseed = true", "reseeding"),
     ("viscosity = 0.1", "viscosity"),
 ])
 def test_out_of_scope_rejected(tmp_path, extra, what):
@@ -137,6 +136,17 @@ def test_inflow_outflow_parse(tmp_path):
     bad.write_text(bad.read_text() + "\n[[outflow]]\nlo = [0, 0, 0]\n")
     with pytest.raises(BlockError):
         load_scene(bad)
+
+
+@pytest.mark.gpu
+def test_simulate_with_reseed(tmp_path):
+    """reseed = true: frames 0 and 2 (every 2) reseed; the run completes and
+    the particle counts stay finite."""
+    cfg = _write_minimal(tmp_path, frames=3,
+                         extra_sim="reseed = true\nreseed_every_n_frames = 2")
+    assert main(["simulate", str(cfg)]) == 0
+    last = np.load(tmp_path / "cache" / "particles" / "frame_0002.npy")
+    assert len(last) > 0 and np.isfinite(last).all()
 
 
 @pytest.mark.gpu
