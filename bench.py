@@ -481,6 +481,56 @@ def reseed_leg(torch, s, snap, reps=5):
             "culled": int(res[1]), "ms_per_call": round(1e3 * float(np.median(ts)), 3)}
 
 
+def mesh_leg(torch, s, snap, hbm, reps=5, cpu=True):
+    """MeshExtractor on the bench scene's particles with the scene TOML's
+    [output] defaults (trilinear splat, 2 blur passes, iso 0.6): device time
+    of the density field (zero + splat + 2 blur passes) and of the iso-surface
+    (count, scan, read-back of the totals, emit), wall time of the whole
+    extract including the copy of the mesh to the host, and the oracle's
+    time for the same field and surface on one host thread.  Blur bytes:
+    4 B read + 4 B written per cell per pass (neighbour reads hit cache)."""
+    from gpufluid_b200.mesh import MeshExtractor
+    pos = snap[0]  # the scene's particle positions (storage order)
+    ex = MeshExtractor(GRID, GRID, GRID, s.dx)
+    stream = torch.cuda.current_stream()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    dens_ms, surf_ms, wall = [], [], []
+    v = t = None
+    for r in range(reps + 2):
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        ev[0].record(stream)
+        ex.density(pos, smooth_passes=2)
+        ev[1].record(stream)
+        v, t = ex.surface(0.6)
+        ev[2].record(stream)
+        torch.cuda.synchronize()
+        if r >= 2:
+            wall.append(time.perf_counter() - w0)
+            dens_ms.append(ev[0].elapsed_time(ev[1]))
+            surf_ms.append(ev[1].elapsed_time(ev[2]))
+    nc = GRID ** 3
+    blur_bytes = 2 * 8 * nc
+    out = {"workload": f"{GRID}^3 scene particles -> trilinear density, 2 blur passes, "
+                       "iso 0.6 surface (marching tetrahedra), copied to the host",
+           "particles": int(pos.shape[0]), "verts": 0 if v is None else int(len(v)),
+           "tris": 0 if t is None else int(len(t)),
+           "density_ms": round(float(np.median(dens_ms)), 4),
+           "surface_ms": round(float(np.median(surf_ms)), 4),
+           "extract_wall_ms": round(1e3 * float(np.median(wall)), 3),
+           "blur_bytes": blur_bytes}
+    if cpu:
+        from oracle import mesh as om
+        p_host = pos.cpu().numpy()
+        t0 = time.perf_counter()
+        d = om.density_field(p_host, (GRID, GRID, GRID), s.dx, 2, 0)
+        ov, ot = om.iso_surface(d, 0.6, s.dx)
+        out["cpu_oracle_s"] = round(time.perf_counter() - t0, 3)
+        out["cpu_oracle_cores"] = 1
+        out["cpu_oracle_tris"] = int(len(ot))
+    return out
+
+
 def stage_bytes_flip(P, ncell_active, F):
     """Algorithmic bytes of the FLIP (non-APIC) stages: sort 64P + 12N,
     P2G 24P + 24F (the zeroing of the six P2G face arrays counted as for
@@ -671,6 +721,8 @@ def run_ours(args):
 
     outflow = outflow_leg(torch, s, hbm)
     reseed = reseed_leg(torch, s, snap)
+    mesh = mesh_leg(torch, s, snap, hbm, cpu=(rank == 0 and world == 1
+                                              and not args.no_cpu_baseline))
 
     fwd_adj = None if args.no_adjoint else adjoint_leg(torch, device)
     fwd_adj_apic = None if args.no_adjoint else adjoint_leg(torch, device, transfer="apic")
@@ -739,6 +791,7 @@ def run_ours(args):
             "other_configs": extra,
             "outflow_compaction": outflow,
             "reseed": reseed,
+            "mesh": mesh,
         }
         print(json.dumps(line), flush=True)
     ranks.close()

@@ -85,6 +85,15 @@ class TuneInfo(ctypes.Structure):
                 ("step_ms_before", ctypes.c_float), ("step_ms_after", ctypes.c_float)]
 
 
+GF_MESH_TRILINEAR, GF_MESH_CUBIC = 0, 1
+MESH_METHOD = {"trilinear": GF_MESH_TRILINEAR, "cubic": GF_MESH_CUBIC}
+
+
+class MeshParams(ctypes.Structure):
+    _fields_ = [("method", ctypes.c_int32), ("smooth_passes", ctypes.c_int32),
+                ("wall_margin_cells", ctypes.c_int32), ("cubic_radius_cells", ctypes.c_float)]
+
+
 _SIGS = {
     "gf_create": ([ctypes.POINTER(GridDesc), ctypes.c_int64, ctypes.POINTER(_vp)], ctypes.c_int),
     "gf_destroy": ([_vp], ctypes.c_int),
@@ -138,6 +147,18 @@ _SIGS = {
     "gf_autotune": ([_vp, ctypes.POINTER(StepParams), ctypes.POINTER(TuneInfo)], ctypes.c_int),
     "gf_get_tune": ([_vp, ctypes.POINTER(TuneInfo)], ctypes.c_int),
     "gf_set_tune": ([_vp, ctypes.POINTER(TuneInfo)], ctypes.c_int),
+    "gf_mesher_create": ([ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, _vp,
+                          ctypes.POINTER(_vp)], ctypes.c_int),
+    "gf_mesher_destroy": ([_vp], ctypes.c_int),
+    "gf_mesher_last_error": ([_vp], ctypes.c_char_p),
+    "gf_mesher_set_stream": ([_vp, _vp], ctypes.c_int),
+    "gf_mesher_field": ([_vp], _vp),
+    "gf_mesher_launches": ([_vp], ctypes.c_int64),
+    "gf_mesher_density": ([_vp, _vp, ctypes.c_int64, ctypes.POINTER(MeshParams)], ctypes.c_int),
+    "gf_mesher_extract": ([_vp, _vp, ctypes.c_float, ctypes.POINTER(ctypes.c_int64),
+                           ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
+    "gf_mesher_copy": ([_vp, _vp, _vp], ctypes.c_int),
+    "gf_mesher_copy_field": ([_vp, _vp], ctypes.c_int),
 }
 
 _lib = None
@@ -147,7 +168,7 @@ def header_symbols() -> list[str]:
     """Names of every function declared in include/gfb200.h."""
     with open(HEADER) as f:
         text = f.read()
-    return sorted(set(re.findall(r"^\s*(?:int|int64_t|const char \*)\s*(gf_\w+)\s*\(", text,
+    return sorted(set(re.findall(r"^\s*(?:int|int64_t|float \*|const char \*)\s*(gf_\w+)\s*\(", text,
                                  flags=re.M)))
 
 

@@ -5,15 +5,17 @@ FLIP/PIC/APIC scene:
 - it builds the solver from the TOML, adds the static obstacles' union SDF,
   seeds the fluid or resumes a checkpoint;
 - per frame it runs round(1/(fps*dt)) substeps (or step_cfl when cfl = true),
-  checks has_diverged(), writes particles/frame_NNNN.npy when
-  [output] particles = true, and writes checkpoints every --checkpoint-every
-  frames;
+  checks has_diverged(), writes mesh/frame_NNNN.ply (binary PLY of the GPU
+  iso-surface; an empty placeholder when no surface emerges) when
+  [output] mesh = true, particles/frame_NNNN.npy when [output] particles =
+  true, and writes checkpoints every --checkpoint-every frames;
 - it writes cache.json (CacheManifest keys of src/gpufluid/io/cache.py:28-93)
   and, with --timings, timings.json;
 - it returns 2 on divergence or a configuration error, else 0.
 
-Mesh extraction is not part of this build, so cache.json's mesh_pattern is
-null.
+Mesh options whose reference implementation is third-party code (mesh
+smoothing via scipy, decimation via pyfqmr, the Warp-HashGrid "sdf" method)
+are refused with BlockError("C7.1").
 ``bench`` runs the reference's fixed throughput table (commands.py:953-977)
 with device-synchronised timing.
 """
@@ -62,9 +64,25 @@ def build_obstacle_sdf(scene, grid_xyz):
     return out
 
 
+def check_mesh_options(out):
+    """Refuse the [output] mesh options outside this build (C7.1)."""
+    if not out.mesh:
+        return
+    if out.mesh_method not in ("trilinear", "cubic"):
+        raise BlockError("C7.1", f"output.mesh_method {out.mesh_method!r} is not part of this "
+                                 "build (trilinear, cubic)")
+    if out.mesh_smooth_passes > 0:
+        raise BlockError("C7.1", "output.mesh_smooth_passes > 0 (mesh smoothing) is not part "
+                                 "of this build")
+    if out.decimate_ratio < 1.0:
+        raise BlockError("C7.1", "output.decimate_ratio < 1 (mesh decimation) is not part of "
+                                 "this build")
+
+
 def make_solver(scene, args):
     from .solver import FlipSolver3D
     sim = scene.simulation
+    check_mesh_options(scene.output)
     if sim.solver != "flip":
         raise BlockError("C7.1", f"solver {sim.solver!r} is not part of this build (flip only)")
     nx, ny, nz = scene.domain.resolution
@@ -129,11 +147,17 @@ def cmd_simulate(args) -> int:
     if not cache_dir.is_absolute() and scene.config_dir is not None:
         cache_dir = scene.config_dir / cache_dir
     cache_dir.mkdir(parents=True, exist_ok=True)
+    mesh_dir = cache_dir / "mesh"
+    mesh_dir.mkdir(exist_ok=True)
     parts_dir = cache_dir / "particles"
     if scene.output.particles:
         parts_dir.mkdir(exist_ok=True)
+    extractor = None
     if scene.output.mesh:
-        print("           note: mesh extraction is not part of this build (no mesh/ output)")
+        from .mesh import MeshExtractor, write_ply
+        extractor = MeshExtractor(nx, ny, nz, scene.dx)
+    t_mesh = 0.0
+    verts = None
     steps_per_frame = max(1, int(round(1.0 / (sim.fps * sim.dt))))
     start_frame = int(getattr(args, "start_frame", 0))
     ckpt_every = int(getattr(args, "checkpoint_every", 0))
@@ -170,31 +194,50 @@ def cmd_simulate(args) -> int:
             print(f"[flip] solver diverged at frame {frame} (last dumped: {frame}/{sim.frames}).",
                   file=sys.stderr)
             break
+        if extractor is not None:
+            # commands.py:721-770; the splat reads the solver's particle
+            # storage directly (its order only changes float atomics' order)
+            tm = time.time()
+            out = scene.output
+            verts, faces = extractor.extract(
+                solver._pos[:solver.n_particles], iso_level=out.iso_level,
+                smooth_passes=out.smooth_passes, mesh_smooth_passes=out.mesh_smooth_passes,
+                mesh_smooth_method=out.mesh_smooth_method,
+                wall_margin_cells=out.wall_margin_cells, decimate_ratio=out.decimate_ratio,
+                mesh_method=out.mesh_method, cubic_radius_cells=out.cubic_radius_cells)
+            t_mesh += time.time() - tm
+            if verts is not None:
+                write_ply(mesh_dir / f"frame_{frame:04d}.ply", verts, faces)
+            else:  # an empty placeholder keeps the frame indices aligned
+                write_ply(mesh_dir / f"frame_{frame:04d}.ply", np.zeros((0, 3), np.float32),
+                          np.zeros((0, 3), np.int32))
         if scene.output.particles:
             pos, _ = solver.get_particles()
             np.save(parts_dir / f"frame_{frame:04d}.npy", pos.astype(np.float32))
         if frame % 10 == 0 or frame == sim.frames - 1:
-            print(f"  frame {frame:04d}/{sim.frames}")
+            nv = len(verts) if extractor is not None and verts is not None else 0
+            print(f"  frame {frame:04d}/{sim.frames} V={nv}")
         if ckpt_every > 0 and (frame + 1) % ckpt_every == 0:
             solver.save_checkpoint(cache_dir / f"checkpoint_frame_{frame:04d}.npz")
     manifest = {
         "schema_version": CACHE_SCHEMA_VERSION, "gpufluid_version": f"b200-{__version__}",
         "created_unix": time.time(), "fps": sim.fps,
         "frame_count": (truncated + 1) if truncated is not None else sim.frames,
-        "mesh_pattern": None,
+        "mesh_pattern": "mesh/frame_{:04d}.ply",
         "particles_pattern": "particles/frame_{:04d}.npy" if scene.output.particles else None,
         "domain_size": list(scene.domain_size), "resolution": list(scene.domain.resolution),
-        "dx": scene.dx, "notes": f"sim={t_sim:.1f}s", "solver": "flip",
+        "dx": scene.dx, "notes": f"sim={t_sim:.1f}s mesh={t_mesh:.1f}s", "solver": "flip",
         "truncated_at_frame": int(truncated) if truncated is not None else None,
         "truncation_reason": "flip_divergence" if truncated is not None else None,
     }
     (cache_dir / "cache.json").write_text(json.dumps(manifest, indent=2), encoding="utf-8")
-    print(f"[gpufluid-b200] done. cache: {cache_dir}  sim total: {t_sim:.2f}s")
+    print(f"[gpufluid-b200] done. cache: {cache_dir}  sim total: {t_sim:.2f}s  "
+          f"mesh total: {t_mesh:.2f}s")
     timings = solver._prof.summarize()
     if timings:
         (cache_dir / "timings.json").write_text(json.dumps(
             {"sections_ms": timings, "call_counts": solver._prof.call_counts,
-             "sim_total_s": t_sim, "mesh_total_s": 0.0}, indent=2, sort_keys=True))
+             "sim_total_s": t_sim, "mesh_total_s": t_mesh}, indent=2, sort_keys=True))
     return 0 if truncated is None else 2
 
 

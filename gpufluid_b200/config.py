@@ -138,6 +138,14 @@ class OutputCfg:
     mesh: bool = True
     iso_level: float = 0.6
     smooth_passes: int = 2
+    mesh_smooth_passes: int = 0
+    mesh_smooth_method: str = "taubin"
+    decimate_ratio: float = 1.0
+    wall_margin_cells: int = 0
+    mesh_method: str = "trilinear"
+    cubic_radius_cells: float = 2.0
+    sdf_particle_radius_cells: float = 1.0
+    sdf_search_radius_cells: float = 4.0
     particles: bool = False
     usd: bool = False
     whitewater: bool = False

@@ -1,0 +1,670 @@
+// Particles -> surface mesh, once per frame after the substeps
+// (MeshExtractor.extract, src/gpufluid/meshing/surface.py:353-461).
+//
+// A mesher owns two density fields of the grid's cell count and the
+// extraction scratch, like MeshExtractor's dens / dens_tmp (surface.py:
+// 206-216).  gf_mesher_density builds the field:
+//   k_mesh_zero + k_mesh_splat     trilinear unit-mass splat of each particle
+//                                  (k_density_scatter, surface.py:14-43)
+//   k_mesh_cubic                   or the cubic-falloff splat over a box of
+//                                  cells (k_cubic_scatter, surface.py:53-84)
+//   k_mesh_blur x smooth_passes    3x3x3 boundary-aware box blur
+//                                  (k_box_blur_3d, gridmath.py:103-121); the
+//                                  last pass also zeroes the wall margin
+//   k_mesh_walls                   (k_mc_zero_walls, surface.py:179-193) when
+//                                  there is no blur pass to fold it into
+// The splats add with float atomics in arrival order (as the reference's
+// wp.atomic_add); blur and margin are per-cell and follow the reference's
+// float32 operation order exactly.
+//
+// gf_mesher_extract cuts the iso-surface density >= iso_level out of the field
+// sampled at the cell indices (vertices are index * dx, as the reference's
+// marching cubes returns them).  The reference hands this step to
+// scikit-image's or Warp's marching cubes; this library uses marching
+// tetrahedra on the Kuhn (Freudenthal) split of every cube into the six
+// tetrahedra that share its main diagonal: the split is conforming between
+// neighbouring cubes, has no ambiguous cases and needs no case table.  A
+// vertex sits on each grid edge (offsets x, y, z, the face diagonals and the
+// main diagonal from a node's lower corner) whose end values straddle the
+// level, at the linear crossing from the lower end; axis-edge vertices are the
+// ones marching cubes places.  Triangles face from >= iso to < iso.  Output
+// order is fixed: vertices by (node, edge family), triangles by (cube, tet,
+// triangle), so the mesh is deterministic for a given field.
+//   k_mesh_count  per node: crossing-edge mask, cube corner mask, block sums
+//   k_mesh_scan   block sums -> block offsets and the two totals (int64)
+//   (host reads the totals, grows the output buffers)
+//   k_mesh_vemit  per node: vertex ids and positions
+//   k_mesh_temit  per cube: triangles (vertex ids looked up by edge owner)
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <string>
+
+#include "../../include/gfb200.h"
+
+namespace gfm {
+
+constexpr int MB = 256;        // threads per node block
+constexpr int SCAN_T = 1024;   // threads of the offsets scan
+
+struct Mesher {
+  int nx = 0, ny = 0, nz = 0;
+  float dx = 0.f;
+  int64_t nnode = 0;
+  int nb = 0;  // node blocks
+  cudaStream_t stream = 0;
+  float *dens = nullptr, *tmp = nullptr;
+  uint8_t *vmask = nullptr, *cmask = nullptr;
+  int32_t *vbase = nullptr;
+  int64_t *sums = nullptr;     // [2 nb] block sums (verts, tris), [2 nb] offsets, [2] totals
+  int64_t *tot_host = nullptr; // pinned [2]
+  float *verts = nullptr;
+  int64_t verts_cap = 0;
+  int32_t *tris = nullptr;
+  int64_t tris_cap = 0;
+  int64_t nv = -1, nt = -1;    // counts of the last extraction
+  int64_t launches = 0;
+  std::string err;
+};
+
+static int fail(Mesher *m, int status, const std::string &msg) {
+  if (m) m->err = msg;
+  return status;
+}
+
+static int check(Mesher *m, cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return GF_OK;
+  return fail(m, GF_CUDA_ERROR, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ---- density field ---------------------------------------------------------
+__global__ void k_mesh_zero(float *d, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) d[i] = 0.f;
+}
+
+// k_density_scatter: corner weights (1-s | s) per axis, w = wx * wy * wz.
+__global__ void k_mesh_splat(const float *__restrict__ pos, int64_t n, float dx, int nx, int ny,
+                             int nz, float *dens) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const float fx = __fdiv_rn(pos[3 * q], dx) - 0.5f;
+  const float fy = __fdiv_rn(pos[3 * q + 1], dx) - 0.5f;
+  const float fz = __fdiv_rn(pos[3 * q + 2], dx) - 0.5f;
+  const int i0 = __float2int_rz(floorf(fx)), j0 = __float2int_rz(floorf(fy)),
+            k0 = __float2int_rz(floorf(fz));
+  const float sx = fx - (float)i0, sy = fy - (float)j0, sz = fz - (float)k0;
+  const float wx[2] = {1.0f - sx, sx}, wy[2] = {1.0f - sy, sy}, wz[2] = {1.0f - sz, sz};
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int ii = i0 + a, jj = j0 + b, kk = k0 + e;
+        if (ii >= 0 && ii < nx && jj >= 0 && jj < ny && kk >= 0 && kk < nz)
+          atomicAdd(&dens[((int64_t)ii * ny + jj) * nz + kk], wx[a] * wy[b] * wz[e]);
+      }
+}
+
+// k_cubic_scatter: (1 - r^2)^3 for r^2 = |cell centre - p|^2 / R^2 < 1 over the
+// cells within half_cells of the particle's lower trilinear corner.
+__global__ void k_mesh_cubic(const float *__restrict__ pos, int64_t n, float dx,
+                             float inv_r_world_sq, int half_cells, int nx, int ny, int nz,
+                             float *dens) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const float p0 = pos[3 * q], p1 = pos[3 * q + 1], p2 = pos[3 * q + 2];
+  const int cx = __float2int_rz(floorf(__fdiv_rn(p0, dx) - 0.5f));
+  const int cy = __float2int_rz(floorf(__fdiv_rn(p1, dx) - 0.5f));
+  const int cz = __float2int_rz(floorf(__fdiv_rn(p2, dx) - 0.5f));
+  const int ilo = max(0, cx - half_cells), ihi = min(nx, cx + half_cells + 1);
+  const int jlo = max(0, cy - half_cells), jhi = min(ny, cy + half_cells + 1);
+  const int klo = max(0, cz - half_cells), khi = min(nz, cz + half_cells + 1);
+  for (int i = ilo; i < ihi; ++i) {
+    const float ddx = ((float)i + 0.5f) * dx - p0;
+    for (int j = jlo; j < jhi; ++j) {
+      const float ddy = ((float)j + 0.5f) * dx - p1;
+      for (int k = klo; k < khi; ++k) {
+        const float ddz = ((float)k + 0.5f) * dx - p2;
+        const float r_sq = (ddx * ddx + ddy * ddy + ddz * ddz) * inv_r_world_sq;
+        if (r_sq < 1.0f) {
+          const float om = 1.0f - r_sq;
+          atomicAdd(&dens[((int64_t)i * ny + j) * nz + k], om * om * om);
+        }
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ bool in_margin(int i, int j, int k, int nx, int ny, int nz, int m) {
+  return i < m || i >= nx - m || j < m || j >= ny - m || k < m || k >= nz - m;
+}
+
+// k_box_blur_3d: sum of the in-grid 3x3x3 neighbours (di, dj, dk ascending,
+// float32 adds in that order) divided by their count.  margin > 0 writes 0
+// inside the wall margin instead (k_mc_zero_walls after the last pass).
+__global__ void k_mesh_blur(const float *__restrict__ src, float *__restrict__ dst, int nx,
+                            int ny, int nz, int margin) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= (int64_t)nx * ny * nz) return;
+  const int k = (int)(c % nz), j = (int)((c / nz) % ny), i = (int)(c / ((int64_t)ny * nz));
+  if (margin > 0 && in_margin(i, j, k, nx, ny, nz, margin)) {
+    dst[c] = 0.f;
+    return;
+  }
+  float s = 0.f, cnt = 0.f;
+  for (int di = -1; di <= 1; ++di) {
+    const int ii = i + di;
+    if (ii < 0 || ii >= nx) continue;
+    for (int dj = -1; dj <= 1; ++dj) {
+      const int jj = j + dj;
+      if (jj < 0 || jj >= ny) continue;
+      const float *row = src + ((int64_t)ii * ny + jj) * nz;
+      for (int dk = -1; dk <= 1; ++dk) {
+        const int kk = k + dk;
+        if (kk < 0 || kk >= nz) continue;
+        s = __fadd_rn(s, __ldg(row + kk));
+        cnt += 1.0f;
+      }
+    }
+  }
+  dst[c] = __fdiv_rn(s, cnt);
+}
+
+__global__ void k_mesh_walls(float *d, int nx, int ny, int nz, int margin) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= (int64_t)nx * ny * nz) return;
+  const int k = (int)(c % nz), j = (int)((c / nz) % ny), i = (int)(c / ((int64_t)ny * nz));
+  if (in_margin(i, j, k, nx, ny, nz, margin)) d[c] = 0.f;
+}
+
+// ---- iso-surface -----------------------------------------------------------
+// Corner b of a cube (bit 0: +x, bit 1: +y, bit 2: +z) sits at node
+// n + off(b).  Edge family b (1..7) of a node joins it to n + off(b).
+// Tet t of the Kuhn split visits corners 0, a, a|b', 7 for the axis order
+// (a, b', c) of permutation t; its orientation sign is the permutation's.
+__constant__ uint8_t c_perm[6][2] = {{1, 2}, {1, 4}, {2, 1}, {2, 4}, {4, 1}, {4, 2}};
+__constant__ int8_t c_parity[6] = {1, -1, -1, 1, 1, -1};
+
+__device__ __forceinline__ void tet_corners(int t, int cs[4]) {
+  cs[0] = 0;
+  cs[1] = c_perm[t][0];
+  cs[2] = c_perm[t][0] | c_perm[t][1];
+  cs[3] = 7;
+}
+
+__device__ __forceinline__ int tet_tris(int in4) {
+  const int c = __popc(in4);
+  return (c == 1 || c == 3) ? 1 : (c == 2 ? 2 : 0);
+}
+
+__device__ __forceinline__ int cube_tris(int cm) {
+  int s = 0;
+#pragma unroll
+  for (int t = 0; t < 6; ++t) {
+    int cs[4];
+    tet_corners(t, cs);
+    int in4 = 0;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) in4 |= ((cm >> cs[v]) & 1) << v;
+    s += tet_tris(in4);
+  }
+  return s;
+}
+
+struct NodeIdx {
+  int i, j, k;
+};
+
+__device__ __forceinline__ NodeIdx node_of(int64_t n, int ny, int nz) {
+  return {(int)(n / ((int64_t)ny * nz)), (int)((n / nz) % ny), (int)(n % nz)};
+}
+
+__device__ __forceinline__ int64_t off_of(int b, int ny, int nz) {
+  return (b & 1 ? (int64_t)ny * nz : 0) + (b & 2 ? nz : 0) + (b & 4 ? 1 : 0);
+}
+
+// Block-wide exclusive prefix of v (MB threads); *total gets the block sum.
+__device__ __forceinline__ int block_prefix(int v, int *total) {
+  __shared__ int ws[MB / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int u = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += u;
+  }
+  if (lane == 31) ws[wid] = incl;
+  __syncthreads();
+  int before = 0, all = 0;
+#pragma unroll
+  for (int w = 0; w < MB / 32; ++w) {
+    const int s = ws[w];
+    before += w < wid ? s : 0;
+    all += s;
+  }
+  __syncthreads();
+  *total = all;
+  return before + incl - v;
+}
+
+struct ExtractArgs {
+  const float *dens;
+  float iso;
+  int nx, ny, nz;
+  int64_t nnode;
+  float dx;
+  uint8_t *vmask, *cmask;
+  int32_t *vbase;
+  int64_t *sums;  // block sums v [nb], t [nb]; offsets v [nb], t [nb]; totals [2]
+  int nb;
+  float *verts;
+  int32_t *tris;
+};
+
+__global__ void __launch_bounds__(MB) k_mesh_count(ExtractArgs a) {
+  const int64_t n = blockIdx.x * (int64_t)MB + threadIdx.x;
+  int vm = 0, cm = 0, nt = 0;
+  if (n < a.nnode) {
+    const NodeIdx p = node_of(n, a.ny, a.nz);
+    const bool hx = p.i + 1 < a.nx, hy = p.j + 1 < a.ny, hz = p.k + 1 < a.nz;
+    const float v0 = a.dens[n];
+    const int in0 = v0 >= a.iso;
+    cm = in0;
+#pragma unroll
+    for (int b = 1; b < 8; ++b) {
+      if ((b & 1 && !hx) || (b & 2 && !hy) || (b & 4 && !hz)) continue;
+      const int in = a.dens[n + off_of(b, a.ny, a.nz)] >= a.iso;
+      cm |= in << b;
+      vm |= (in != in0) << b;
+    }
+    if (!(hx && hy && hz)) cm = 0;  // not the lower corner of a cube
+    nt = (hx && hy && hz) ? cube_tris(cm) : 0;
+    a.vmask[n] = (uint8_t)vm;
+    a.cmask[n] = (uint8_t)cm;
+  }
+  __shared__ int red[2][MB / 32];
+  int sv = __popc(vm), st = nt;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    sv += __shfl_down_sync(0xffffffffu, sv, o);
+    st += __shfl_down_sync(0xffffffffu, st, o);
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) {
+    red[0][wid] = sv;
+    red[1][wid] = st;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int64_t tv = 0, tt = 0;
+    for (int w = 0; w < MB / 32; ++w) {
+      tv += red[0][w];
+      tt += red[1][w];
+    }
+    a.sums[blockIdx.x] = tv;
+    a.sums[a.nb + blockIdx.x] = tt;
+  }
+}
+
+// Exclusive offsets of the per-block sums; block 0 scans the vertex sums,
+// block 1 the triangle sums, each in chunks of SCAN_T.
+__global__ void __launch_bounds__(SCAN_T) k_mesh_scan(int64_t *sums, int nb) {
+  __shared__ int64_t ws[SCAN_T / 32];
+  __shared__ int64_t carry;
+  const int64_t *in = sums + (int64_t)blockIdx.x * nb;
+  int64_t *out = sums + 2 * (int64_t)nb + (int64_t)blockIdx.x * nb;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < nb; base += SCAN_T) {
+    const int t = base + threadIdx.x;
+    const int64_t v = t < nb ? in[t] : 0;
+    int64_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int64_t u = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += u;
+    }
+    if (lane == 31) ws[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+      const int64_t s = ws[lane];
+      int64_t si = s;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int64_t u = __shfl_up_sync(0xffffffffu, si, o);
+        if (lane >= o) si += u;
+      }
+      ws[lane] = si - s;
+    }
+    __syncthreads();
+    if (t < nb) out[t] = carry + ws[wid] + incl - v;
+    __syncthreads();
+    if (threadIdx.x == SCAN_T - 1) carry += ws[wid] + incl;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) sums[4 * (int64_t)nb + blockIdx.x] = carry;
+}
+
+__global__ void __launch_bounds__(MB) k_mesh_vemit(ExtractArgs a) {
+  const int64_t n = blockIdx.x * (int64_t)MB + threadIdx.x;
+  const int vm = n < a.nnode ? a.vmask[n] : 0;
+  int total;
+  const int local = block_prefix(__popc(vm), &total);
+  if (n >= a.nnode) return;
+  const int64_t base = a.sums[2 * (int64_t)a.nb + blockIdx.x] + local;
+  a.vbase[n] = (int32_t)base;
+  if (!vm) return;
+  const NodeIdx p = node_of(n, a.ny, a.nz);
+  const float va = a.dens[n];
+  const float fi = (float)p.i, fj = (float)p.j, fk = (float)p.k;
+  int r = 0;
+#pragma unroll
+  for (int b = 1; b < 8; ++b) {
+    if (!(vm >> b & 1)) continue;
+    const float vb = a.dens[n + off_of(b, a.ny, a.nz)];
+    const float t = __fdiv_rn(__fsub_rn(a.iso, va), __fsub_rn(vb, va));
+    float *o = a.verts + 3 * (base + r);
+    o[0] = __fmul_rn(b & 1 ? __fadd_rn(fi, t) : fi, a.dx);
+    o[1] = __fmul_rn(b & 2 ? __fadd_rn(fj, t) : fj, a.dx);
+    o[2] = __fmul_rn(b & 4 ? __fadd_rn(fk, t) : fk, a.dx);
+    ++r;
+  }
+}
+
+// Id of the vertex on the edge from cube corner lo to corner hi (lo's bits
+// a subset of hi's): owned by node n + off(lo), family hi ^ lo.
+__device__ __forceinline__ int32_t edge_vertex(const ExtractArgs &a, int64_t n, int lo, int hi) {
+  const int64_t o = n + off_of(lo, a.ny, a.nz);
+  const int f = hi ^ lo;
+  return a.vbase[o] + __popc(a.vmask[o] & ((1 << f) - 1));
+}
+
+__global__ void __launch_bounds__(MB) k_mesh_temit(ExtractArgs a) {
+  const int64_t n = blockIdx.x * (int64_t)MB + threadIdx.x;
+  const int cm = n < a.nnode ? a.cmask[n] : 0;
+  const int nt = (cm != 0 && cm != 0xff) ? cube_tris(cm) : 0;
+  int total;
+  const int local = block_prefix(nt, &total);
+  if (n >= a.nnode || nt == 0) return;
+  int64_t w = a.sums[3 * (int64_t)a.nb + blockIdx.x] + local;
+  for (int t = 0; t < 6; ++t) {
+    int cs[4];
+    tet_corners(t, cs);
+    int in4 = 0;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) in4 |= ((cm >> cs[v]) & 1) << v;
+    const int cnt = __popc(in4);
+    if (cnt == 0 || cnt == 4) continue;
+    const int s = c_parity[t];
+    int32_t *o = a.tris + 3 * w;
+    if (cnt == 1 || cnt == 3) {
+      // the lone vertex l and the others in ascending order: the triple
+      // faces away from l when (-1)^l * s > 0; away is outward when l is
+      // the inside vertex
+      const int lone_in = cnt == 1;
+      int l = 0;
+      for (int v = 0; v < 4; ++v)
+        if (((in4 >> v) & 1) == lone_in) l = v;
+      int oth[3], m = 0;
+      for (int v = 0; v < 4; ++v)
+        if (v != l) oth[m++] = v;
+      int32_t e[3];
+      for (int q = 0; q < 3; ++q) {
+        const int u = min(l, oth[q]), x = max(l, oth[q]);
+        e[q] = edge_vertex(a, n, cs[u], cs[x]);
+      }
+      const bool away = ((l & 1) ? -s : s) > 0;
+      o[0] = e[0];
+      if (away == (bool)lone_in) {
+        o[1] = e[1];
+        o[2] = e[2];
+      } else {
+        o[1] = e[2];
+        o[2] = e[1];
+      }
+      w += 1;
+    } else {
+      // inside pair (p0 < p1), outside pair (q0 < q1); the cycle
+      // (p0q0, p0q1, p1q1, p1q0) faces outward when the tet reordered as
+      // (p0, p1, q0, q1) is positive
+      int pi[2], qo[2], np = 0, nq = 0;
+      for (int v = 0; v < 4; ++v) {
+        if ((in4 >> v) & 1)
+          pi[np++] = v;
+        else
+          qo[nq++] = v;
+      }
+      const int ord[4] = {pi[0], pi[1], qo[0], qo[1]};
+      int inv = 0;
+      for (int x = 0; x < 4; ++x)
+        for (int y = x + 1; y < 4; ++y) inv += ord[x] > ord[y];
+      const int sp = (inv & 1) ? -s : s;
+      auto E = [&](int u, int x) { return edge_vertex(a, n, cs[min(u, x)], cs[max(u, x)]); };
+      int32_t cyc[4] = {E(pi[0], qo[0]), E(pi[0], qo[1]), E(pi[1], qo[1]), E(pi[1], qo[0])};
+      if (sp < 0) {
+        const int32_t tmp = cyc[1];
+        cyc[1] = cyc[3];
+        cyc[3] = tmp;
+      }
+      o[0] = cyc[0];
+      o[1] = cyc[1];
+      o[2] = cyc[2];
+      o[3] = cyc[0];
+      o[4] = cyc[2];
+      o[5] = cyc[3];
+      w += 2;
+    }
+  }
+}
+
+static int grow(Mesher *m, void **buf, int64_t *cap, int64_t need, int64_t elem,
+                const char *what) {
+  if (*cap >= need) return GF_OK;
+  if (*buf) cudaFree(*buf);
+  *buf = nullptr;
+  *cap = 0;
+  const int64_t n = need + need / 4 + 1024;
+  int e = check(m, cudaMalloc(buf, n * elem), what);
+  if (e) return e;
+  *cap = n;
+  return GF_OK;
+}
+
+static void release(Mesher *m) {
+  void *ps[] = {m->dens, m->tmp, m->vmask, m->cmask, m->vbase, m->sums, m->verts, m->tris};
+  for (void *p : ps)
+    if (p) cudaFree(p);
+  if (m->tot_host) cudaFreeHost(m->tot_host);
+}
+
+}  // namespace gfm
+
+using gfm::Mesher;
+
+extern "C" {
+
+int gf_mesher_create(int32_t nx, int32_t ny, int32_t nz, float dx, void *cuda_stream,
+                     void **mesher_out) {
+  if (!mesher_out || nx < 1 || ny < 1 || nz < 1 || !(dx > 0.f)) return GF_INVALID_ARG;
+  *mesher_out = nullptr;
+  const int64_t nnode = (int64_t)nx * ny * nz;
+  if (nnode > (int64_t)1 << 31) return GF_INVALID_ARG;
+  Mesher *m = new Mesher();
+  m->nx = nx;
+  m->ny = ny;
+  m->nz = nz;
+  m->dx = dx;
+  m->nnode = nnode;
+  m->nb = (int)((nnode + gfm::MB - 1) / gfm::MB);
+  m->stream = reinterpret_cast<cudaStream_t>(cuda_stream);
+  cudaError_t e = cudaSuccess;
+  if (e == cudaSuccess) e = cudaMalloc(&m->dens, nnode * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&m->tmp, nnode * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&m->vmask, nnode);
+  if (e == cudaSuccess) e = cudaMalloc(&m->cmask, nnode);
+  if (e == cudaSuccess) e = cudaMalloc(&m->vbase, nnode * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&m->sums, (4 * (int64_t)m->nb + 2) * 8);
+  if (e == cudaSuccess) e = cudaMallocHost(&m->tot_host, 2 * 8);
+  if (e == cudaSuccess) e = cudaMemsetAsync(m->dens, 0, nnode * 4, m->stream);
+  if (e != cudaSuccess) {
+    gfm::release(m);
+    delete m;
+    return GF_CUDA_ERROR;
+  }
+  *mesher_out = m;
+  return GF_OK;
+}
+
+int gf_mesher_destroy(void *mesher) {
+  Mesher *m = reinterpret_cast<Mesher *>(mesher);
+  if (!m) return GF_INVALID_ARG;
+  cudaStreamSynchronize(m->stream);
+  gfm::release(m);
+  delete m;
+  return GF_OK;
+}
+
+const char *gf_mesher_last_error(void *mesher) {
+  Mesher *m = reinterpret_cast<Mesher *>(mesher);
+  return m ? m->err.c_str() : "null mesher";
+}
+
+int gf_mesher_set_stream(void *mesher, void *cuda_stream) {
+  Mesher *m = reinterpret_cast<Mesher *>(mesher);
+  if (!m) return GF_INVALID_ARG;
+  m->stream = reinterpret_cast<cudaStream_t>(cuda_stream);
+  return GF_OK;
+}
+
+float *gf_mesher_field(void *mesher) {
+  Mesher *m = reinterpret_cast<Mesher *>(mesher);
+  return m ? m->dens : nullptr;
+}
+
+int gf_mesher_copy_field(void *mesher, float *out) {
+  Mesher *m = reinterpret_cast<Mesher *>(mesher);
+  if (!m || !out) return GF_INVALID_ARG;
+  int e = gfm::check(m, cudaMemcpyAsync(out, m->dens, m->nnode * 4, cudaMemcpyDefault, m->stream),
+                     "copy mesh field");
+  if (e) return e;
+  return gfm::check(m, cudaStreamSynchronize(m->stream), "mesh field sync");
+}
+
+int64_t gf_mesher_launches(void *mesher) {
+  Mesher *m = reinterpret_cast<Mesher *>(mesher);
+  return m ? m->launches : -1;
+}
+
+int gf_mesher_density(void *mesher, const float *pos, int64_t n,
+                      const gf_mesh_params *prm) {
+  Mesher *m = reinterpret_cast<Mesher *>(mesher);
+  if (!m || !prm || n < 0 || (n > 0 && !pos)) return GF_INVALID_ARG;
+  if (prm->smooth_passes < 0 || prm->wall_margin_cells < 0)
+    return gfm::fail(m, GF_INVALID_ARG, "gf_mesher_density: negative pass count or margin");
+  if (prm->method != GF_MESH_TRILINEAR && prm->method != GF_MESH_CUBIC)
+    return gfm::fail(m, GF_INVALID_ARG, "gf_mesher_density: unknown mesh method");
+  if (prm->method == GF_MESH_CUBIC && !(prm->cubic_radius_cells > 0.f))
+    return gfm::fail(m, GF_INVALID_ARG, "gf_mesher_density: cubic radius must be > 0");
+  cudaStream_t st = m->stream;
+  const unsigned gc = (unsigned)((m->nnode + 255) / 256);
+  gfm::k_mesh_zero<<<gc, 256, 0, st>>>(m->dens, m->nnode);
+  m->launches++;
+  if (n > 0) {
+    const unsigned gp = (unsigned)((n + 255) / 256);
+    if (prm->method == GF_MESH_TRILINEAR) {
+      gfm::k_mesh_splat<<<gp, 256, 0, st>>>(pos, n, m->dx, m->nx, m->ny, m->nz, m->dens);
+    } else {
+      // surface.py:376-382: radius and falloff scale in double, passed as float
+      const double r_world = (double)prm->cubic_radius_cells * (double)m->dx;
+      const float inv_r_world_sq = (float)(1.0 / (r_world * r_world));
+      const int half_cells = (int)std::ceil((double)prm->cubic_radius_cells) + 1;
+      gfm::k_mesh_cubic<<<gp, 256, 0, st>>>(pos, n, m->dx, inv_r_world_sq, half_cells, m->nx,
+                                            m->ny, m->nz, m->dens);
+    }
+    m->launches++;
+  }
+  for (int p = 0; p < prm->smooth_passes; ++p) {
+    const int margin = p == prm->smooth_passes - 1 ? prm->wall_margin_cells : 0;
+    gfm::k_mesh_blur<<<gc, 256, 0, st>>>(m->dens, m->tmp, m->nx, m->ny, m->nz, margin);
+    float *t = m->dens;
+    m->dens = m->tmp;
+    m->tmp = t;
+    m->launches++;
+  }
+  if (prm->smooth_passes == 0 && prm->wall_margin_cells > 0) {
+    gfm::k_mesh_walls<<<gc, 256, 0, st>>>(m->dens, m->nx, m->ny, m->nz, prm->wall_margin_cells);
+    m->launches++;
+  }
+  m->nv = m->nt = -1;
+  return gfm::check(m, cudaGetLastError(), "gf_mesher_density");
+}
+
+int gf_mesher_extract(void *mesher, const float *field, float iso_level, int64_t *n_verts,
+                      int64_t *n_tris) {
+  Mesher *m = reinterpret_cast<Mesher *>(mesher);
+  if (!m || !n_verts || !n_tris || !std::isfinite(iso_level)) return GF_INVALID_ARG;
+  if (m->nx < 2 || m->ny < 2 || m->nz < 2) {  // no cube: no surface
+    m->nv = m->nt = 0;
+    *n_verts = *n_tris = 0;
+    return GF_OK;
+  }
+  cudaStream_t st = m->stream;
+  gfm::ExtractArgs a{field ? field : m->dens, iso_level, m->nx, m->ny, m->nz, m->nnode, m->dx,
+                     m->vmask, m->cmask, m->vbase, m->sums, m->nb, nullptr, nullptr};
+  gfm::k_mesh_count<<<m->nb, gfm::MB, 0, st>>>(a);
+  gfm::k_mesh_scan<<<2, gfm::SCAN_T, 0, st>>>(m->sums, m->nb);
+  m->launches += 2;
+  int e;
+  if ((e = gfm::check(m, cudaGetLastError(), "gf_mesher_extract count"))) return e;
+  if ((e = gfm::check(m, cudaMemcpyAsync(m->tot_host, m->sums + 4 * (int64_t)m->nb, 16,
+                                         cudaMemcpyDeviceToHost, st),
+                      "read mesh totals")))
+    return e;
+  if ((e = gfm::check(m, cudaStreamSynchronize(st), "mesh totals sync"))) return e;
+  const int64_t nv = m->tot_host[0], nt = m->tot_host[1];
+  if (nv > INT32_MAX)
+    return gfm::fail(m, GF_INVALID_ARG, "gf_mesher_extract: vertex count exceeds int32 range");
+  if ((e = gfm::grow(m, reinterpret_cast<void **>(&m->verts), &m->verts_cap, nv, 12,
+                     "alloc mesh vertices")))
+    return e;
+  if ((e = gfm::grow(m, reinterpret_cast<void **>(&m->tris), &m->tris_cap, nt, 12,
+                     "alloc mesh triangles")))
+    return e;
+  a.verts = m->verts;
+  a.tris = m->tris;
+  if (nv > 0) {
+    gfm::k_mesh_vemit<<<m->nb, gfm::MB, 0, st>>>(a);
+    gfm::k_mesh_temit<<<m->nb, gfm::MB, 0, st>>>(a);
+    m->launches += 2;
+  }
+  m->nv = nv;
+  m->nt = nt;
+  *n_verts = nv;
+  *n_tris = nt;
+  return gfm::check(m, cudaGetLastError(), "gf_mesher_extract emit");
+}
+
+int gf_mesher_copy(void *mesher, float *verts, int32_t *tris) {
+  Mesher *m = reinterpret_cast<Mesher *>(mesher);
+  if (!m) return GF_INVALID_ARG;
+  if (m->nv < 0) return gfm::fail(m, GF_INVALID_ARG, "gf_mesher_copy: no extraction to copy");
+  if ((m->nv > 0 && !verts) || (m->nt > 0 && !tris)) return GF_INVALID_ARG;
+  int e;
+  if (m->nv > 0 &&
+      (e = gfm::check(m, cudaMemcpyAsync(verts, m->verts, m->nv * 12, cudaMemcpyDefault,
+                                         m->stream),
+                      "copy mesh vertices")))
+    return e;
+  if (m->nt > 0 &&
+      (e = gfm::check(m, cudaMemcpyAsync(tris, m->tris, m->nt * 12, cudaMemcpyDefault,
+                                         m->stream),
+                      "copy mesh triangles")))
+    return e;
+  return gfm::check(m, cudaStreamSynchronize(m->stream), "mesh copy sync");
+}
+
+}  // extern "C"

@@ -207,6 +207,50 @@ int gf_compact_alive(void *ctx, const float *pos, const float *vel, int64_t n,
  * cell.  Single-grid contexts; the bound pid must hold ids 0..n-1. */
 int gf_reseed_mark(void *ctx, int32_t max_per_cell, int32_t *alive, int32_t *counts);
 
+/* ---- surface mesh after the substeps ------------------------------------ */
+/* A mesher replaces MeshExtractor (src/gpufluid/meshing/surface.py:199-461):
+ * it owns two cell-centred density fields of nx*ny*nz floats (dens /
+ * dens_tmp, surface.py:206-216) and the extraction scratch, and runs on its
+ * own stream.  It is independent of a solver context: pass it the particle
+ * positions (device (n,3) float32) of any solver. */
+#define GF_MESH_TRILINEAR 0 /* k_density_scatter, surface.py:14-43 */
+#define GF_MESH_CUBIC 1     /* k_cubic_scatter, surface.py:53-84 */
+typedef struct gf_mesh_params {
+  int32_t method;             /* GF_MESH_TRILINEAR | GF_MESH_CUBIC */
+  int32_t smooth_passes;      /* k_box_blur_3d passes (gridmath.py:103-121) */
+  int32_t wall_margin_cells;  /* k_mc_zero_walls margin (surface.py:179-193); 0 = off */
+  float cubic_radius_cells;   /* GF_MESH_CUBIC support radius in cells */
+} gf_mesh_params;
+int gf_mesher_create(int32_t nx, int32_t ny, int32_t nz, float dx, void *cuda_stream,
+                     void **mesher_out);
+int gf_mesher_destroy(void *mesher);
+const char *gf_mesher_last_error(void *mesher);
+int gf_mesher_set_stream(void *mesher, void *cuda_stream);
+/* The density field the last gf_mesher_density left (device, nx*ny*nz,
+ * C order); valid until the next gf_mesher_density. */
+float *gf_mesher_field(void *mesher);
+/* Copy that field (nx*ny*nz floats) to `out` (host or device).  Synchronising. */
+int gf_mesher_copy_field(void *mesher, float *out);
+/* Kernel launches issued by this mesher so far. */
+int64_t gf_mesher_launches(void *mesher);
+/* Zero the field, splat the n particles, blur smooth_passes times, zero the
+ * wall margin (surface.py:388-425, the "trilinear" and "cubic" branches).
+ * Asynchronous. */
+int gf_mesher_density(void *mesher, const float *pos, int64_t n, const gf_mesh_params *prm);
+/* Iso-surface {density >= iso_level} of `field` (device nx*ny*nz floats;
+ * NULL = the mesher's own field) by marching tetrahedra on the Kuhn split of
+ * each cube; stands in for the marching cubes of _mc_extract_gpu /
+ * _mc_extract_cpu (surface.py:286-351), whose vertices are the axis-edge
+ * subset of these.  Vertices are grid index * dx.  Writes the vertex and
+ * triangle counts (0, 0 when no surface crosses the grid: the reference's
+ * "no surface" result) and keeps the mesh in the mesher.  Synchronises once
+ * for the counts. */
+int gf_mesher_extract(void *mesher, const float *field, float iso_level, int64_t *n_verts,
+                      int64_t *n_tris);
+/* Copy the last extraction out: verts (n_verts,3) float32, tris (n_tris,3)
+ * int32, host or device memory.  Synchronising. */
+int gf_mesher_copy(void *mesher, float *verts, int32_t *tris);
+
 /* ---- adjoint (differentiation through substeps) ------------------------- */
 /* No counterpart in the reference (planned only there).  PIC transfer
  * (flip_blend 0) or APIC, with the cell labels held fixed within each substep.

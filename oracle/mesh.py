@@ -1,0 +1,259 @@
+"""CPU oracle for the surface mesh after the substeps -- TEST INFRASTRUCTURE ONLY.
+
+Only ``tests/`` (and the bench's CPU leg) may import this module, as the
+checker; the product (``gpufluid_b200``) never does.
+
+NumPy restatement of the reference's density field
+(src/gpufluid/meshing/surface.py):
+
+* ``splat_trilinear`` -- ``k_density_scatter`` (:14-43): f = p/dx - 0.5,
+  corner weights (1-s | s) per axis, w = (wx*wy)*wz, float32 adds in thread
+  (particle) order, corners (di, dj, dk) ascending;
+* ``splat_cubic``     -- ``k_cubic_scatter`` (:53-84) with the host's
+  radius arithmetic (:376-382);
+* ``box_blur``        -- ``k_box_blur_3d`` (primitives/gridmath.py:103-121):
+  float32 sum of the in-grid 3x3x3 neighbours (di, dj, dk ascending) divided
+  by their count;
+* ``zero_walls``      -- ``k_mc_zero_walls`` (:179-193);
+* ``density_field``   -- the order of ``MeshExtractor.extract`` (:388-425).
+
+Parity pin: ``tests/golden/mesh/density.npz`` holds the reference kernels' own
+outputs run on the sequential Warp stand-in (``tests/golden/make_mesh_golden.py``);
+``tests/test_mesh.py`` checks this restatement against them.
+
+The iso-surface step of the reference is third-party code (scikit-image's
+``marching_cubes`` below 64^3, Warp's ``MarchingCubes`` from 64^3,
+surface.py:286-351); neither is installed, so that step is unpinned.
+``iso_surface`` restates the library's own method -- marching tetrahedra on
+the Kuhn split of each cube -- independently of the CUDA code (orientation
+from integer determinants of the tetrahedra's corners rather than from the
+permutation parity), for bit-exact checks of the GPU extraction on the same
+field; its axis-edge vertices are the crossings marching cubes would place.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+F32 = np.float32
+
+
+def splat_trilinear(pos, shape, dx):
+    nx, ny, nz = shape
+    dens = np.zeros(nx * ny * nz, F32)
+    if len(pos) == 0:
+        return dens.reshape(shape)
+    pos = np.asarray(pos, F32)
+    f = pos / F32(dx) - F32(0.5)
+    i0 = np.floor(f).astype(np.int64)
+    s = f - i0.astype(F32)
+    idx, w = [], []
+    for a in (0, 1):
+        wx = (F32(1.0) - s[:, 0]) if a == 0 else s[:, 0]
+        for b in (0, 1):
+            wy = (F32(1.0) - s[:, 1]) if b == 0 else s[:, 1]
+            for e in (0, 1):
+                wz = (F32(1.0) - s[:, 2]) if e == 0 else s[:, 2]
+                ii, jj, kk = i0[:, 0] + a, i0[:, 1] + b, i0[:, 2] + e
+                ok = (ii >= 0) & (ii < nx) & (jj >= 0) & (jj < ny) & (kk >= 0) & (kk < nz)
+                idx.append(np.where(ok, (ii * ny + jj) * nz + kk, -1))
+                w.append((wx * wy) * wz)
+    idx = np.stack(idx, 1).reshape(-1)  # particle-major, then corner
+    w = np.stack(w, 1).reshape(-1).astype(F32)
+    keep = idx >= 0
+    np.add.at(dens, idx[keep], w[keep])
+    return dens.reshape(shape)
+
+
+def splat_cubic(pos, shape, dx, radius_cells):
+    nx, ny, nz = shape
+    dens = np.zeros(shape, F32)
+    r_world = float(radius_cells) * float(dx)
+    inv = F32(1.0 / (r_world * r_world))
+    half = int(math.ceil(radius_cells)) + 1
+    dx32 = F32(dx)
+    for p in np.asarray(pos, F32):
+        c = np.floor(p / dx32 - F32(0.5)).astype(np.int64)
+        lo = np.maximum(0, c - half)
+        hi = np.minimum([nx, ny, nz], c + half + 1)
+        if (hi <= lo).any():
+            continue
+        ii = np.arange(lo[0], hi[0])
+        jj = np.arange(lo[1], hi[1])
+        kk = np.arange(lo[2], hi[2])
+        ddx = (ii.astype(F32) + F32(0.5)) * dx32 - p[0]
+        ddy = (jj.astype(F32) + F32(0.5)) * dx32 - p[1]
+        ddz = (kk.astype(F32) + F32(0.5)) * dx32 - p[2]
+        d_sq = (ddx[:, None, None] * ddx[:, None, None] + ddy[None, :, None] * ddy[None, :, None]
+                ) + ddz[None, None, :] * ddz[None, None, :]
+        r_sq = d_sq * inv
+        om = F32(1.0) - r_sq
+        val = (om * om) * om
+        blk = dens[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]]
+        blk += np.where(r_sq < F32(1.0), val, F32(0.0))
+    return dens
+
+
+def box_blur(src):
+    src = np.asarray(src, F32)
+    nx, ny, nz = src.shape
+    pad = np.zeros((nx + 2, ny + 2, nz + 2), F32)
+    pad[1:-1, 1:-1, 1:-1] = src
+    one = np.zeros_like(pad)
+    one[1:-1, 1:-1, 1:-1] = 1.0
+    s = np.zeros(src.shape, F32)
+    n = np.zeros(src.shape, F32)
+    for di in (-1, 0, 1):
+        for dj in (-1, 0, 1):
+            for dk in (-1, 0, 1):
+                sl = (slice(1 + di, nx + 1 + di), slice(1 + dj, ny + 1 + dj),
+                      slice(1 + dk, nz + 1 + dk))
+                s = s + pad[sl]  # out-of-grid neighbours add +0.0: exact
+                n = n + one[sl]
+    return (s / n).astype(F32)
+
+
+def zero_walls(d, margin):
+    d = np.array(d, F32, copy=True)
+    if margin > 0:
+        m = int(margin)
+        d[:m], d[-m:] = 0, 0
+        d[:, :m], d[:, -m:] = 0, 0
+        d[:, :, :m], d[:, :, -m:] = 0, 0
+    return d
+
+
+def density_field(pos, shape, dx, smooth_passes=2, wall_margin_cells=0,
+                  mesh_method="trilinear", cubic_radius_cells=2.0):
+    if mesh_method == "trilinear":
+        d = splat_trilinear(pos, shape, dx)
+    elif mesh_method == "cubic":
+        d = splat_cubic(pos, shape, dx, cubic_radius_cells)
+    else:
+        raise ValueError(mesh_method)
+    for _ in range(smooth_passes):
+        d = box_blur(d)
+    return zero_walls(d, wall_margin_cells)
+
+
+# ---- iso-surface: marching tetrahedra on the Kuhn split ------------------
+# Cube corner b = (bit0: +x, bit1: +y, bit2: +z).  The six tetrahedra share
+# corners 0 and 7 and follow the axis orders of the six permutations.
+_AXIS_ORDERS = [(1, 2), (1, 4), (2, 1), (2, 4), (4, 1), (4, 2)]
+
+
+def _corner_xyz(b):
+    return np.array([b & 1, (b >> 1) & 1, (b >> 2) & 1], np.int64)
+
+
+def _det(a, b, c):
+    return int(np.dot(a, np.cross(b, c)))
+
+
+def iso_surface(dens, iso, dx):
+    """(verts (V,3) float32, tris (T,3) int32) of {dens >= iso}; vertices
+    ordered by (node, edge family 1..7), triangles by (cube, tet, triangle)."""
+    d = np.asarray(dens, F32)
+    nx, ny, nz = d.shape
+    if nx < 2 or ny < 2 or nz < 2:  # no cube: no surface
+        return np.zeros((0, 3), F32), np.zeros((0, 3), np.int32)
+    iso32, dx32 = F32(iso), F32(dx)
+    inside = d >= iso32
+    cross = np.zeros((nx, ny, nz, 8), bool)
+    vpos = np.zeros((nx, ny, nz, 8, 3), F32)
+    gi, gj, gk = np.meshgrid(np.arange(nx, dtype=F32), np.arange(ny, dtype=F32),
+                             np.arange(nz, dtype=F32), indexing="ij")
+    for b in range(1, 8):
+        ox, oy, oz = b & 1, (b >> 1) & 1, (b >> 2) & 1
+        lo = (slice(0, nx - ox), slice(0, ny - oy), slice(0, nz - oz))
+        hi = (slice(ox, nx), slice(oy, ny), slice(oz, nz))
+        c = inside[lo] != inside[hi]
+        cross[lo + (b,)] = c
+        with np.errstate(divide="ignore", invalid="ignore"):
+            t = (iso32 - d[lo]) / (d[hi] - d[lo])
+        for axis, (g, o) in enumerate(((gi, ox), (gj, oy), (gk, oz))):
+            base = g[lo]
+            vpos[lo + (b, axis)] = ((base + t) if o else base) * dx32
+    flat = cross.reshape(-1)
+    verts = vpos.reshape(-1, 3)[flat]
+    vid = np.full(flat.shape, -1, np.int64)
+    vid[flat] = np.arange(int(flat.sum()))
+    vid = vid.reshape(nx, ny, nz, 8)
+    if len(verts) == 0:
+        return verts.astype(F32), np.zeros((0, 3), np.int32)
+
+    cx, cy, cz = nx - 1, ny - 1, nz - 1
+    ci, cj, ck = np.meshgrid(np.arange(cx), np.arange(cy), np.arange(cz), indexing="ij")
+    cube_key = (ci * ny + cj) * nz + ck   # node index of the cube's lower corner
+
+    def corner_inside(b):
+        x, y, z = _corner_xyz(b)
+        return inside[x:x + cx, y:y + cy, z:z + cz]
+
+    def edge_vid(lo_b, hi_b, sel):
+        x, y, z = _corner_xyz(lo_b)
+        return vid[x:x + cx, y:y + cy, z:z + cz, hi_b ^ lo_b][sel]
+
+    keys, tris = [], []
+    for t, (a, b2) in enumerate(_AXIS_ORDERS):
+        cs = [0, a, a | b2, 7]
+        xyz = [_corner_xyz(c) for c in cs]
+        ins = [corner_inside(c) for c in cs]
+        code = ins[0] * 1 + ins[1] * 2 + ins[2] * 4 + ins[3] * 8
+        for m in range(1, 15):
+            sel = code == m
+            if not sel.any():
+                continue
+            members = [v for v in range(4) if (m >> v) & 1]
+            if len(members) in (1, 3):
+                lone_in = len(members) == 1
+                l = members[0] if lone_in else [v for v in range(4) if not (m >> v) & 1][0]
+                oth = [v for v in range(4) if v != l]
+                e = [edge_vid(cs[min(l, o)], cs[max(l, o)], sel) for o in oth]
+                det = _det(*(xyz[o] - xyz[l] for o in oth))
+                away = det > 0   # triple (oth ascending) faces away from corner l
+                tri = np.stack([e[0], e[1], e[2]] if away == lone_in else [e[0], e[2], e[1]], 1)
+                keys.append(cube_key[sel] * 12 + t * 2)
+                tris.append(tri)
+            else:
+                p0, p1 = members
+                q0, q1 = [v for v in range(4) if not (m >> v) & 1]
+                E = lambda u, x: edge_vid(cs[min(u, x)], cs[max(u, x)], sel)  # noqa: E731
+                cyc = [E(p0, q0), E(p0, q1), E(p1, q1), E(p1, q0)]
+                if _det(xyz[p1] - xyz[p0], xyz[q0] - xyz[p0], xyz[q1] - xyz[p0]) < 0:
+                    cyc = [cyc[0], cyc[3], cyc[2], cyc[1]]
+                keys.append(cube_key[sel] * 12 + t * 2)
+                tris.append(np.stack([cyc[0], cyc[1], cyc[2]], 1))
+                keys.append(cube_key[sel] * 12 + t * 2 + 1)
+                tris.append(np.stack([cyc[0], cyc[2], cyc[3]], 1))
+    if not keys:
+        return verts.astype(F32), np.zeros((0, 3), np.int32)
+    keys = np.concatenate(keys)
+    tris = np.concatenate(tris)
+    order = np.argsort(keys, kind="stable")
+    return verts.astype(F32), tris[order].astype(np.int32)
+
+
+def mesh_volume(verts, tris):
+    """Signed enclosed volume (divergence theorem), float64."""
+    v = np.asarray(verts, np.float64)
+    a, b, c = v[tris[:, 0]], v[tris[:, 1]], v[tris[:, 2]]
+    return float(np.einsum("ij,ij->i", a, np.cross(b, c)).sum() / 6.0)
+
+
+def mesh_area(verts, tris):
+    v = np.asarray(verts, np.float64)
+    a, b, c = v[tris[:, 0]], v[tris[:, 1]], v[tris[:, 2]]
+    return float(0.5 * np.linalg.norm(np.cross(b - a, c - a), axis=1).sum())
+
+
+def boundary_edges(tris):
+    """Number of undirected edges used by exactly one triangle (0 for a closed
+    surface) and whether every interior edge appears once in each direction."""
+    t = np.asarray(tris, np.int64)
+    e = np.concatenate([t[:, [0, 1]], t[:, [1, 2]], t[:, [2, 0]]])
+    und = np.sort(e, axis=1)
+    _, cnt = np.unique(und, axis=0, return_counts=True)
+    _, dcnt = np.unique(e, axis=0, return_counts=True)
+    return int((cnt == 1).sum()), bool((dcnt == 1).all())

@@ -329,5 +329,6 @@ def install():
     mod.array3d = lambda *a, **k: None
     mod.float32 = float
     mod.int32 = int
+    mod.uint64 = int
     sys.modules["warp"] = mod
     return mod

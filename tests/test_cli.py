@@ -106,6 +106,17 @@ def test_out_of_scope_rejected(tmp_path, extra, what):
     assert what in str(ei.value)
 
 
+@pytest.mark.parametrize("key", ['mesh_method = "sdf"', "mesh_smooth_passes = 2",
+                                 "decimate_ratio = 0.5"])
+def test_mesh_options_outside_build_rejected(tmp_path, key):
+    cfg = _write_minimal(tmp_path)
+    cfg.write_text(cfg.read_text().replace("smooth_passes = 1\n", f"smooth_passes = 1\n{key}\n"))
+    scene = load_scene(cfg)
+    with pytest.raises(BlockError) as ei:
+        make_solver(scene, None)
+    assert ei.value.block_id == "C7.1" and key.split()[0] in str(ei.value)
+
+
 _REGIONS = """
 [[inflow]]
 lo = [0.1, 0.7, 0.1]
@@ -211,8 +222,17 @@ def test_simulate_end_to_end_creates_cache(tmp_path):
         a = np.load(cache / "particles" / f"frame_{f:04d}.npy")
         assert a.dtype == np.float32 and a.ndim == 2 and a.shape[1] == 3
         assert np.isfinite(a).all()
+    # mesh/frame_NNNN.ply per frame (commands.py:721-770)
+    assert m["mesh_pattern"] == "mesh/frame_{:04d}.ply"
+    from gpufluid_b200.mesh import read_ply
+    from oracle import mesh as om
+    for f in range(2):
+        v, tri = read_ply(cache / "mesh" / f"frame_{f:04d}.ply")
+        assert len(v) > 0 and len(tri) > 0 and tri.max() < len(v)
+        assert om.mesh_volume(v, tri) > 0
     t = json.loads((cache / "timings.json").read_text())
     assert set(t["sections_ms"]) >= {"p2g", "pressure", "g2p_advect"}
+    assert t["mesh_total_s"] > 0
     ck = np.load(cache / "checkpoint_frame_0000.npz")
     assert int(ck["nx"]) == 16 and ck["pos"].shape == a.shape
 
