@@ -122,6 +122,9 @@ _SIGS = {
     "gf_compact_alive": ([_vp, _vp, _vp, ctypes.c_int64, _vp, _vp, _vp,
                           ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
     "gf_reseed_mark": ([_vp, ctypes.c_int32, _vp, _vp], ctypes.c_int),
+    "gf_reseed_deficit": ([_vp, _vp, _vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)],
+                          ctypes.c_int),
+    "gf_reseed_emit": ([_vp, _vp, _vp, ctypes.c_int32, _vp, _vp], ctypes.c_int),
     "gf_pressure_stats": ([_vp, ctypes.POINTER(PressureInfo)], ctypes.c_int),
     "gf_pcg_trace": ([_vp, _vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
     "gf_record_bytes": ([_vp, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),

@@ -8,7 +8,13 @@
 // particle in its cell by id; k_reseed_mark keeps the first max_per_cell of
 // each non-solid cell and k_reseed_counts returns the dense per-cell counts
 // from which the host builds the emission list; the survivors are compacted
-// by the same three launches as the outflows (gf_compact_alive).
+// by the same three launches as the outflows (gf_compact_alive).  The
+// emission list is built on the device too: k_deficit_count sums each block
+// of cells' deficits (fluid cells under min_per_cell), k_alive_offsets turns
+// the sums into offsets, and k_deficit_emit places each cell's deficit at its
+// offset in C order of the cells, the order of the reference's np.argwhere /
+// np.repeat; only the jitter (drawn from the host generator, as the reference
+// draws it) crosses the bus.
 //
 // A particle is removed when it lies inside ANY box (lo <= p <= hi on all
 // three axes, float32 compares); the survivors keep their relative order
@@ -179,6 +185,75 @@ __global__ void k_reseed_counts(const int32_t *__restrict__ count, int nx, int n
   dense[c] = count[t * 512 + ((i & 7) * 8 + (j & 7)) * 8 + (k & 7)];
 }
 
+// Deficit of one cell (reseed.py:345-352): fluid = (marked fluid or holding
+// particles) and not solid; deficit = max(min_per_cell - count, 0) there.
+__device__ __forceinline__ int deficit_of(uint8_t lab, int cnt, int mn) {
+  const bool fluid = (lab == 1 || cnt > 0) && lab != 2;
+  return fluid ? max(mn - cnt, 0) : 0;
+}
+
+__global__ void __launch_bounds__(RG_BLOCK) k_deficit_count(const uint8_t *__restrict__ label,
+                                                            const int32_t *__restrict__ counts,
+                                                            int64_t ncell, int mn, int32_t *bsum) {
+  __shared__ int ws[RG_BLOCK / 32];
+  const int64_t c = blockIdx.x * (int64_t)RG_BLOCK + threadIdx.x;
+  int d = c < ncell ? deficit_of(label[c], counts[c], mn) : 0;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) d += __shfl_down_sync(0xffffffffu, d, o);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = d;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < RG_BLOCK / 32; ++w) t += ws[w];
+    bsum[blockIdx.x] = t;
+  }
+}
+
+// Emitted positions (cell + 0.5 + jitter) * dx, float32 adds in that order.
+__global__ void __launch_bounds__(RG_BLOCK) k_deficit_emit(
+    const uint8_t *__restrict__ label, const int32_t *__restrict__ counts, int nx, int ny, int nz,
+    int mn, const int32_t *__restrict__ boff, const float *__restrict__ jit, float dx,
+    float *__restrict__ pos_out) {
+  __shared__ int ws[RG_BLOCK / 32];
+  const int64_t ncell = (int64_t)nx * ny * nz;
+  const int64_t c = blockIdx.x * (int64_t)RG_BLOCK + threadIdx.x;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int d = c < ncell ? deficit_of(label[c], counts[c], mn) : 0;
+  int incl = d;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int u = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += u;
+  }
+  if (lane == 31) ws[wid] = incl;
+  __syncthreads();
+  int before = 0;
+  for (int w = 0; w < wid; ++w) before += ws[w];
+  if (d == 0) return;
+  const int64_t e0 = (int64_t)boff[blockIdx.x] + before + incl - d;
+  const int k = (int)(c % nz), j = (int)((c / nz) % ny), i = (int)(c / ((int64_t)ny * nz));
+  const float ci[3] = {__fadd_rn((float)i, 0.5f), __fadd_rn((float)j, 0.5f),
+                       __fadd_rn((float)k, 0.5f)};
+  for (int r = 0; r < d; ++r) {
+    const int64_t e = e0 + r;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) pos_out[3 * e + a] = __fmul_rn(__fadd_rn(ci[a], jit[3 * e + a]), dx);
+  }
+}
+
+// Deficit sums and offsets (two launches); the total stays at scratch[2 nb].
+static int deficit_offsets(Ctx *c, const uint8_t *label, const int32_t *counts, int mn,
+                           int32_t **scratch, int *nb_out) {
+  const int nb = (int)((c->ncell + RG_BLOCK - 1) / RG_BLOCK);
+  int e = region_scratch(c, nb, 0, scratch);
+  if (e) return e;
+  k_deficit_count<<<nb, RG_BLOCK, 0, c->stream>>>(label, counts, c->ncell, mn, *scratch);
+  k_alive_offsets<<<1, RG_BLOCK, 0, c->stream>>>(*scratch, nb);
+  c->launches += 2;
+  *nb_out = nb;
+  return check_launch(c, "reseed deficit offsets");
+}
+
 }  // namespace gf
 
 using gf::Ctx;
@@ -254,6 +329,39 @@ int gf_reseed_mark(void *ctx, int32_t max_per_cell, int32_t *alive, int32_t *cou
       c->count, c->nx, c->ny, c->nz, c->nty, c->ntz, counts);
   c->launches++;
   return gf::check_launch(c, "gf_reseed_mark");
+}
+
+int gf_reseed_deficit(void *ctx, const uint8_t *label, const int32_t *counts,
+                      int32_t min_per_cell, int64_t *n_emit) {
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);
+  if (!c || !label || !counts || !n_emit || min_per_cell < 0) return GF_INVALID_ARG;
+  int32_t *scr = nullptr;
+  int nb = 0;
+  int e = gf::deficit_offsets(c, label, counts, min_per_cell, &scr, &nb);
+  if (e) return e;
+  int32_t total = 0;
+  if ((e = gf::check_cuda(c, cudaMemcpyAsync(&total, scr + 2 * (int64_t)nb, 4,
+                                             cudaMemcpyDeviceToHost, c->stream),
+                          "read reseed deficit")))
+    return e;
+  if ((e = gf::check_cuda(c, cudaStreamSynchronize(c->stream), "reseed deficit sync"))) return e;
+  *n_emit = total;
+  return GF_OK;
+}
+
+int gf_reseed_emit(void *ctx, const uint8_t *label, const int32_t *counts, int32_t min_per_cell,
+                   const float *jitter, float *pos_out) {
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);
+  if (!c || !label || !counts || !jitter || !pos_out || min_per_cell < 0) return GF_INVALID_ARG;
+  int32_t *scr = nullptr;
+  int nb = 0;
+  int e = gf::deficit_offsets(c, label, counts, min_per_cell, &scr, &nb);
+  if (e) return e;
+  gf::k_deficit_emit<<<nb, gf::RG_BLOCK, 0, c->stream>>>(label, counts, c->nx, c->ny, c->nz,
+                                                         min_per_cell, scr + nb, jitter, c->dx,
+                                                         pos_out);
+  c->launches++;
+  return gf::check_launch(c, "gf_reseed_emit");
 }
 
 }  // extern "C"

@@ -528,14 +528,22 @@ class FlipSolver3D:
         if n == 0:
             return 0, 0
         dev = self.device
-        marker = self._label.cpu().numpy().astype(np.int32)
+        # the binning relabels the cells from the current positions; the
+        # reseed reads, and then restores, the labels the last substep left
+        label = self._label.clone()
         alive = torch.empty(n, dtype=torch.int32, device=dev)
         counts = torch.empty(self.nx * self.ny * self.nz, dtype=torch.int32, device=dev)
         self._set_stream()
         _lib.check(self._L.gf_reseed_mark(self._ctx, int(cfg.max_per_cell), alive.data_ptr(),
                                           counts.data_ptr()), self._ctx, "gf_reseed_mark")
+        ne = _lib.ctypes.c_int64()
+        _lib.check(self._L.gf_reseed_deficit(self._ctx, label.data_ptr(), counts.data_ptr(),
+                                             int(cfg.min_per_cell), _lib.ctypes.byref(ne)),
+                   self._ctx, "gf_reseed_deficit")
+        n_emit = int(ne.value)
         pos, vel = self._unsort(self._pos), self._unsort(self._vel)
-        pos_out, vel_out = torch.empty_like(pos), torch.empty_like(vel)
+        pos_out = torch.empty((n + n_emit, 3), dtype=torch.float32, device=dev)
+        vel_out = torch.empty((n + n_emit, 3), dtype=torch.float32, device=dev)
         n_out = _lib.ctypes.c_int64()
         _lib.check(self._L.gf_compact_alive(self._ctx, pos.data_ptr(), vel.data_ptr(), n,
                                             alive.data_ptr(), pos_out.data_ptr(),
@@ -543,27 +551,20 @@ class FlipSolver3D:
                    self._ctx, "gf_compact_alive")
         m = int(n_out.value)
         n_cull = n - m
-        # the binning relabelled the cells from the current positions; restore
-        # the substep's labels, which the reseed leaves alone
-        self._label.copy_(torch.from_numpy(marker.astype(np.uint8)))
-        c = counts.view(self.nx, self.ny, self.nz).cpu().numpy()
-        solid = marker == 2
-        fluid = ((marker == 1) | (c > 0)) & ~solid
-        deficit = np.clip(cfg.min_per_cell - c, 0, None)
-        deficit[~fluid] = 0
-        n_emit = int(deficit.sum())
+        self._label.copy_(label)
         if n_emit == 0 and n_cull == 0:
             return 0, 0
-        new_p, new_v = pos_out[:m], vel_out[:m]
         if n_emit:
-            cells = np.repeat(np.argwhere(deficit > 0), deficit[deficit > 0], axis=0)
-            cells = cells.astype(np.float32)
+            # the jitter comes from the host generator, as in the reference
             jit = (rng.random((n_emit, 3)) - 0.5).astype(np.float32) * cfg.jitter
-            emit = torch.from_numpy(np.ascontiguousarray((cells + 0.5 + jit) * self.dx)).to(dev)
-            new_p = torch.cat([new_p, emit])
-            new_v = torch.cat([new_v, torch.zeros_like(emit)])
-        k = new_p.shape[0]
-        self._set_particles(pos=new_p, vel=new_v,
+            jit_dev = torch.from_numpy(np.ascontiguousarray(jit, dtype=np.float32)).to(dev)
+            _lib.check(self._L.gf_reseed_emit(self._ctx, label.data_ptr(), counts.data_ptr(),
+                                              int(cfg.min_per_cell), jit_dev.data_ptr(),
+                                              pos_out[m:].data_ptr()),
+                       self._ctx, "gf_reseed_emit")
+            vel_out[m:m + n_emit].zero_()
+        k = m + n_emit
+        self._set_particles(pos=pos_out[:k], vel=vel_out[:k],
                             C=torch.zeros((k, 3, 3), dtype=torch.float32, device=dev))
         return n_emit, n_cull
 

@@ -206,6 +206,19 @@ int gf_compact_alive(void *ctx, const float *pos, const float *vel, int64_t n,
  * orders), and counts[nx*ny*nz] (device int32, C order) = particles per
  * cell.  Single-grid contexts; the bound pid must hold ids 0..n-1. */
 int gf_reseed_mark(void *ctx, int32_t max_per_cell, int32_t *alive, int32_t *counts);
+/* The emission count of reseeding (reseed.py:345-352): the sum over cells of
+ * max(min_per_cell - counts, 0) where the cell is fluid (label 1, or counts >
+ * 0) and not solid (label 2).  label (uint8) and counts (int32) are device
+ * arrays of nx*ny*nz cells in C order: the labels the last substep left and
+ * the counts gf_reseed_mark wrote.  Synchronises for the count. */
+int gf_reseed_deficit(void *ctx, const uint8_t *label, const int32_t *counts,
+                      int32_t min_per_cell, int64_t *n_emit);
+/* The emitted positions (reseed.py:362-367): for each deficit cell in C
+ * order, its deficit copies of (cell + 0.5 + jitter[e]) * dx into
+ * pos_out[e] (device (n_emit,3) float32); jitter is a device (n_emit,3)
+ * float32 array (the reference draws it on the host).  Asynchronous. */
+int gf_reseed_emit(void *ctx, const uint8_t *label, const int32_t *counts, int32_t min_per_cell,
+                   const float *jitter, float *pos_out);
 
 /* ---- surface mesh after the substeps ------------------------------------ */
 /* A mesher replaces MeshExtractor (src/gpufluid/meshing/surface.py:199-461):
