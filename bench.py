@@ -10,8 +10,9 @@ scene.
 
   value   substeps/s with the pressure solved by FP32 PCG with FP64 residual
           replacement to a true relative residual of 1e-8, preconditioned by
-          two sweeps of tile-local symmetric Gauss-Seidel (inputs resident in
-          HBM; device time over the timed steps, max over ranks).
+          two sweeps of tile-local symmetric Gauss-Seidel plus a coarse
+          correction over the solver blocks' regions (inputs resident in HBM;
+          device time over the timed steps, max over ranks).
   refined_jacobi  the same refined solve with the reference's Jacobi
           preconditioner (the like-for-like comparison with plain).
   plain   the same substeps with plain FP32 PCG (the reference's Jacobi
@@ -47,11 +48,12 @@ sys.path.insert(0, ROOT)
 
 METRIC = ("FLIP substeps/s @128³ (refined vs plain FP32 PCG, same residual); fwd+adj/s")
 # DRAM bytes (read + write) of one launch of the shared-memory PCG with the
-# tile SGS preconditioner on this workload, from an ncu capture: 8,792,064
-# read + 690,432 written.  The solve's vectors stay in shared memory; only
-# the input, result, tagged halo words and the FP64 replacement steps touch
-# DRAM, far below the algorithmic bytes of a streaming PCG.
-PCG_DRAM_BYTES = 8792064 + 690432
+# tile SGS preconditioner and the coarse correction on this workload, from an
+# ncu capture: 8,497,152 read + 614,400 written.  The solve's vectors stay in
+# shared memory; only the input, result, tagged halo words and the FP64
+# replacement steps touch DRAM, far below the algorithmic bytes of a
+# streaming PCG.
+PCG_DRAM_BYTES = 8497152 + 614400
 GRID = 128
 DT = 1.0 / 480.0
 TOL = 1e-8
@@ -59,9 +61,11 @@ MAX_ITERS = 4000
 SPHERE = ((0.7, 0.2, 0.5), 0.12)
 BOX = ((0.0, 0.0, 0.0), (0.4, 0.6, 1.0))
 SGS_SWEEPS = 2  # tile-local symmetric Gauss-Seidel sweeps of the headline solve
+COARSE = True   # plus the block-region coarse correction
 WORKLOAD = ("APIC dam break + sphere obstacle, 128^3 (dx=1/128), 8 ppc -> 3,969,024 "
             "particles, dt=1/480, pressure: FP32 PCG + FP64 residual replacement to 1e-8, "
-            "tile-local symmetric Gauss-Seidel preconditioner (2 sweeps)")
+            "tile-local symmetric Gauss-Seidel preconditioner (2 sweeps) + block-region "
+            "coarse correction")
 
 
 def peaks():
@@ -142,11 +146,12 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------- scene
-def make_solver(gf, device, graphs=True, precond="tile_sgs"):
+def make_solver(gf, device, graphs=True, precond="tile_sgs", coarse=COARSE):
     from gpufluid_b200 import scene
     s = gf.FlipSolver3D(GRID, GRID, GRID, transfer_mode="apic", flip_blend=0.95,
                         device=device, pressure_tol=TOL, enable_cuda_graphs=graphs,
-                        pcg_preconditioner=precond, pcg_sgs_sweeps=SGS_SWEEPS)
+                        pcg_preconditioner=precond, pcg_sgs_sweeps=SGS_SWEEPS,
+                        pcg_coarse=coarse)
     s.add_solid_from_sdf(scene.sdf_sphere(s.cell_centers_np(), *SPHERE))
     s.seed_box(*BOX)
     return s
@@ -241,17 +246,20 @@ def pressure_error_fp64(torch, s, iters=6000) -> float:
     return float(torch.linalg.vector_norm(p32 - x) / torch.linalg.vector_norm(x))
 
 
-def pcg_bytes(st, sgs_sweeps=0) -> float:
+def pcg_bytes(st, sgs_sweeps=0, coarse=False) -> float:
     """Algorithmic bytes of one PCG launch: per fluid cell 14 B of set-up,
     48 B per iteration (phase A: z, d_old, code in; d_new, Ad out; phase B:
     d_new, Ad, x, r, code in; x, r, z out), 48 B per FP64 residual
     replacement (x64, x, code, b in; x64, x, r, z out); 2 B of stencil code
     per active-tile cell and per phase.  A tile-local symmetric Gauss-Seidel
     preconditioner adds 12 B per fluid cell per sweep (each half-sweep reads
-    r and writes z on its colour and reads z of the other)."""
+    r and writes z on its colour and reads z of the other); the coarse
+    correction adds 8 B per fluid cell per iteration (z read, z + e written)
+    and 2 B of stencil code per active-tile cell for assembling P^T A P."""
     nf, na = st["n_fluid"], st["n_active_tiles"] * 512
     it, rep = st["iters"], st["replacements"]
-    return float(nf * (14 + (48 + 12 * sgs_sweeps) * it + 48 * rep) + na * 2 * (1 + 2 * it))
+    per_it = 48 + 12 * sgs_sweeps + (8 if coarse else 0)
+    return float(nf * (14 + per_it * it + 48 * rep) + na * 2 * (1 + 2 * it + (1 if coarse else 0)))
 
 
 def stage_bytes(P, nf, ncell_active, F):
@@ -636,6 +644,7 @@ def run_ours(args):
     # ---- plain FP32 PCG from the same state (same 1e-8 target, recursive
     # residual), with the reference's Jacobi preconditioner
     s.pcg_preconditioner = "jacobi"
+    s.pcg_coarse = False
     s.step(DT, pressure_iters=MAX_ITERS, pressure_solver="pcg")  # capture its graph
     torch.cuda.synchronize()
     restore(s, snap)
@@ -657,6 +666,7 @@ def run_ours(args):
     refj_stats = s.pressure_stats()
     refj_err = pressure_error_fp64(torch, s) if check else None
     s.pcg_preconditioner = "tile_sgs"
+    s.pcg_coarse = COARSE
     restore(s, snap)
 
     # ---- refined (the value)
@@ -683,7 +693,7 @@ def run_ours(args):
         st = s.pressure_stats()
         stage.append(t)
         pcg_ms.append(t[7])
-        pcg_b.append(pcg_bytes(st, SGS_SWEEPS))
+        pcg_b.append(pcg_bytes(st, SGS_SWEEPS, COARSE))
     s._L.gf_enable_timing(s._ctx, 0)
     s._prof.enabled = False
     stage_ms = np.mean(np.array(stage), axis=0)
@@ -746,7 +756,8 @@ def run_ours(args):
             "data": "synthetic (seeded seed_box lattice of the reference, sphere SDF obstacle)",
             "config": {"workload": WORKLOAD, "grid": GRID, "particles": P, "transfer": "apic",
                        "dt": DT, "pressure": "pcg_refined", "tol": TOL,
-                       "preconditioner": f"tile-local symmetric Gauss-Seidel, {SGS_SWEEPS} sweeps",
+                       "preconditioner": f"tile-local symmetric Gauss-Seidel, {SGS_SWEEPS} sweeps"
+                                         + (", block-region coarse correction" if COARSE else ""),
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2_policy": "inputs larger than L2: particle state "
                                     f"{P * 64 / 1e6:.0f} MB + MAC grids {F * 4 * 3 / 1e6:.0f} MB "
@@ -768,13 +779,13 @@ def run_ours(args):
             "e2e": {"value": round(world * 1000.0 / ms_e2e, 3), "unit": "substeps/s",
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(h2d)},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": "k_pcg_smem<double,true,true> (persistent cooperative, "
+            "roofline": {"bound": "hbm", "kernel": "k_pcg_smem<double,true,true,true> (persistent cooperative, "
                                    "shared-memory resident)",
                          "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                          "frac": round(achieved / hbm, 4), "traffic": PCG_DRAM_BYTES,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
                                            "one launch of this workload "
-                                           "(profiles/pcg_smem_sgs_128_apic.md)",
+                                           "(profiles/pcg_smem_coarse_128_apic.md)",
                          "peak_source": peak_kind,
                          "bytes_per_launch": round(float(np.mean(pcg_b)), 0),
                          "ms_per_launch": round(float(np.mean(pcg_ms)), 4)},

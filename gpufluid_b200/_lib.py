@@ -60,6 +60,7 @@ class StepParams(ctypes.Structure):
 GF_FLAG_GLOBAL_PCG = 1
 GF_FLAG_TRACE = 2
 GF_FLAG_SGS_SHIFT = 2  # bits 2-3: tile-local symmetric Gauss-Seidel sweeps
+GF_FLAG_COARSE = 16    # block-region coarse correction of the shared-memory PCG
 GF_NOALLOC_MAX_CELLS = 2097152
 
 
@@ -67,7 +68,7 @@ class PressureInfo(ctypes.Structure):
     _fields_ = [("iters", ctypes.c_int32), ("replacements", ctypes.c_int32),
                 ("status", ctypes.c_int32), ("n_active_tiles", ctypes.c_int32),
                 ("n_fluid", ctypes.c_int64), ("relres", ctypes.c_double),
-                ("kernel", ctypes.c_int32), ("pad", ctypes.c_int32)]
+                ("kernel", ctypes.c_int32), ("coarse", ctypes.c_int32)]
 
 
 class SceneLayout(ctypes.Structure):

@@ -28,6 +28,7 @@ namespace gf {
 constexpr int TILE = 8;            // tile edge in cells (the reference's BLOCK_SIZE, :950)
 constexpr int TILE_CELLS = 512;    // cells per tile
 constexpr int MAX_PCG_BLOCKS = 4096;
+constexpr int COARSE_MAXG = 160;  // coarse space: at most one region per block of the smem PCG
 constexpr int TRACE_CAP = 4096;
 
 // Stencil code bits (per compact cell).
@@ -55,6 +56,8 @@ struct PcgState {
   unsigned long long bar64;  // monotonic arrival counter (shared-memory solver)
   int smem_solver; // 1: the last solve ran in the shared-memory solver
   int trace_n;     // globaltimer stamps recorded (diagnostic trace)
+  int coarse_off;  // a block's coarse-column solve failed: coarse correction off
+  int coarse_used; // 1: the last shared-memory solve applied the coarse correction
 };
 
 // Shared-memory-resident PCG (pcg_smem.cu).  Returns GF_OK after enqueuing;
@@ -76,6 +79,8 @@ struct PcgSmemArgs {
   double tol2, replace2;
   float sign;
   int sgs_sweeps;             // 0: Jacobi (the reference's); 1-3: tile-local symmetric GS
+  int coarse;                 // 1: add the block-region coarse correction
+  float *cbuf;                // coarse: [G*G] assembled P^T A P, then [G*G] its inverse
 };
 
 
@@ -155,6 +160,7 @@ struct Ctx {
   double *partials = nullptr;    // [3 * MAX_PCG_BLOCKS]
   unsigned long long *bar_counters = nullptr;  // 8 lines x 16 u64
   float *halo = nullptr;         // [6 * nkeys] halo publication buffers
+  float *coarse_buf = nullptr;   // [2 * COARSE_MAXG^2] coarse operator and inverse
   int32_t *tile_cost = nullptr;  // [ntiles] per-slot PCG work estimate
   long long *trace = nullptr;    // [TRACE_CAP] PCG phase timestamps
   bool trace_on = false;

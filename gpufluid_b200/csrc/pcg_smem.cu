@@ -51,6 +51,7 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
 }
 
 constexpr int SM_MAXG = 160;      // blocks (one per SM)
+static_assert(SM_MAXG == COARSE_MAXG, "coarse buffer sizing");
 
 struct GridSync {
   double *partials;            // [2][4][G]
@@ -301,6 +302,8 @@ __device__ __forceinline__ void ring_fill_tagged(float *s_zb, const int *s_nbr,
 // solve's accuracy rests on its FP64 residual replacements, not on these.
 constexpr int FAST_WORDS = 4;  // words per block and parity (3 used)
 constexpr int64_t FAST_SLOTS_OFF = 2048;  // in doubles, into the partials buffer
+// tagged coarse sums g_I: [2][SM_MAXG] u64 after the reduction words
+constexpr int64_t COARSE_SLOTS_OFF = FAST_SLOTS_OFF + 2 * 160 * FAST_WORDS;
 struct FastSync {
   unsigned long long *slots;  // [2][SM_MAXG][FAST_WORDS], zeroed per solve
   unsigned long long epoch;
@@ -468,7 +471,7 @@ __device__ void partition_slots(const int32_t *__restrict__ cost, int na, int ma
   __syncthreads();
 }
 
-template <typename Acc, bool REF, bool SGS>
+template <typename Acc, bool REF, bool SGS, bool CRS>
 __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   using Cfg = SmemCfg<REF>;
   constexpr int MAXT = Cfg::MAXT, MAXJ = Cfg::MAXJ;
@@ -482,6 +485,12 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   __shared__ int s_bounds[SM_MAXG + 1];
   __shared__ Acc sh[36 * 4];
   __shared__ double shd[36 * 4];
+  // coarse correction: region sums g = P^T r gathered from every block, the
+  // block's row of B, region of each face's neighbouring tile
+  __shared__ float s_g[SM_MAXG], s_brow[SM_MAXG];
+  __shared__ short s_freg[MAXT * 6];
+  __shared__ float s_gw[32];
+  __shared__ float s_eI;
 
   PcgState *st = a.st;
   const int na = *a.n_active;
@@ -532,6 +541,172 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   const int l = threadIdx.x & 511, tl0 = threadIdx.x >> 9;
   const int pc = pad_of(l);
 
+  // ---- coarse space (a.coarse): one constant per block's region of tiles,
+  // P its indicator on fluid cells.  Each block assembles its row of
+  // A_c = P^T A P (diagonal: sum over its cells of diag - #fluid neighbours
+  // in the region; off-diagonal: -#fluid-fluid faces to the other region),
+  // then solves A_c x = e_I for its own column of B = A_c^-1 (one warp,
+  // Jacobi-preconditioned CG in float32 on the compacted rows), which is row
+  // I of the symmetric B.  The preconditioner becomes M^-1 = M_tile^-1 +
+  // P B P^T (additive two-level), symmetric positive definite as long as B
+  // is; any block whose column solve fails switches the correction off for
+  // the whole solve.  Dynamic shared memory is free until the tiles load.
+  bool coarse = CRS && a.cbuf != nullptr;
+  if (coarse) {
+    for (int f = threadIdx.x; f < nt * 6; f += blockDim.x) {
+      const int sl = a.nbr[(int64_t)b0 * 6 + f];
+      int r = -1;
+      if (sl >= 0) {  // the block g with bounds[g] <= sl < bounds[g + 1]
+        int lo = 0, hi = G;
+        while (hi - lo > 1) {
+          const int mid = (lo + hi) >> 1;
+          if (s_bounds[mid] <= sl) lo = mid; else hi = mid;
+        }
+        r = lo;
+      }
+      s_freg[f] = (short)r;
+    }
+    for (int i = threadIdx.x; i < G; i += blockDim.x) s_g[i] = 0.f;
+    __syncthreads();
+    const int I = blockIdx.x;
+    for (int L = threadIdx.x; L < nt * 512; L += blockDim.x) {
+      const uint16_t code = a.code[q0 + L];
+      if (!(code & CODE_FLUID)) continue;
+      const int tl = L >> 9, lc = L & 511;
+      const int li = lc >> 6, lj = (lc >> 3) & 7, lk = lc & 7;
+      int same = 0;
+      for (int dir = 0; dir < 6; ++dir) {
+        if (!(code & (1 << dir))) continue;
+        const bool inside = dir == 0 ? li > 0 : dir == 1 ? li < 7 : dir == 2 ? lj > 0
+                          : dir == 3 ? lj < 7 : dir == 4 ? lk > 0 : lk < 7;
+        const int R = inside ? I : (int)s_freg[tl * 6 + dir];
+        if (R == I || R < 0) ++same; else atomicAdd(&s_g[R], -1.0f);
+      }
+      atomicAdd(&s_g[I], (float)((int)((code >> CODE_DIAG_SHIFT) & 7) - same));
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < G; i += blockDim.x) a.cbuf[(int64_t)I * G + i] = s_g[i];
+    {
+      double z0[1] = {0.0}, zt[1];
+      if (!grid_allreduce<double, 1>(gs, z0, zt, shd)) return;
+    }
+    // compacted rows (stride G) of A_c and the CG vectors in dynamic smem
+    float *cval = reinterpret_cast<float *>(smem);
+    int *ccol = reinterpret_cast<int *>(cval + G * G);
+    float *cx = reinterpret_cast<float *>(ccol + G * G);
+    float *cr = cx + SM_MAXG, *cp = cr + SM_MAXG, *cq = cp + SM_MAXG, *cdi = cq + SM_MAXG;
+    int *s_cnnz = reinterpret_cast<int *>(s_g);  // s_g is free until the solve
+    {
+      const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+      for (int r = wid; r < G; r += 32) {
+        int n = 0;
+        float dg = 0.f;
+        for (int c0 = 0; c0 < G; c0 += 32) {
+          const int c = c0 + lane;
+          const float v = c < G ? __ldcg(a.cbuf + (int64_t)r * G + c) : 0.f;
+          if (c == r) dg = v;
+          const unsigned nzm = __ballot_sync(0xffffffffu, v != 0.f && c != r);
+          if (v != 0.f && c != r) {
+            const int k = n + __popc(nzm & ((1u << lane) - 1u));
+            cval[r * G + k] = v;
+            ccol[r * G + k] = c;
+          }
+          n += __popc(nzm);
+        }
+        if (lane == 0) s_cnnz[r] = n;
+        // the diagonal lives in cdi (1 for an empty region: decoupled)
+        const unsigned have = __ballot_sync(0xffffffffu, dg != 0.f);
+        float dv = 0.f;
+        if (have) dv = __shfl_sync(0xffffffffu, dg, __ffs(have) - 1);
+        if (lane == 0) cdi[r] = dv > 0.f ? dv : 1.0f;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {  // warp 0: CG for column I, Jacobi-preconditioned
+      // warm start from the row this block solved last time (the coarse
+      // operator changes little between solves; zero on the first)
+      const int lane = threadIdx.x;
+      const float *prev = a.cbuf + (int64_t)G * G + (int64_t)I * G;
+      for (int r = lane; r < G; r += 32) {
+        const float x0 = __ldcg(prev + r);
+        cx[r] = isfinite(x0) ? x0 : 0.f;
+      }
+      __syncwarp();
+      float rz = 0.f;
+      for (int r = lane; r < G; r += 32) {
+        float acc = cdi[r] * cx[r];
+        const int n = s_cnnz[r];
+        for (int k = 0; k < n; ++k) acc += cval[r * G + k] * cx[ccol[r * G + k]];
+        const float b = (r == I ? 1.f : 0.f) - acc;
+        cr[r] = b;
+        cp[r] = b / cdi[r];
+        rz += b * cp[r];
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) rz += __shfl_xor_sync(0xffffffffu, rz, o);
+      const float rr0 = 1.f;  // ||e_I||^2
+      bool ok = false;
+      {
+        float rr = 0.f;
+        for (int r = lane; r < G; r += 32) rr += cr[r] * cr[r];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) rr += __shfl_xor_sync(0xffffffffu, rr, o);
+        ok = rr <= 1e-12f * rr0;
+      }
+      __syncwarp();
+      for (int it = 0; it < 4 * SM_MAXG && !ok; ++it) {
+        float pq = 0.f;
+        for (int r = lane; r < G; r += 32) {
+          float acc = cdi[r] * cp[r];
+          const int n = s_cnnz[r];
+          for (int k = 0; k < n; ++k) acc += cval[r * G + k] * cp[ccol[r * G + k]];
+          cq[r] = acc;
+          pq += cp[r] * acc;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) pq += __shfl_xor_sync(0xffffffffu, pq, o);
+        if (!(pq > 0.f)) break;
+        const float al = rz / pq;
+        float rr = 0.f, rz2 = 0.f;
+        for (int r = lane; r < G; r += 32) {
+          cx[r] += al * cp[r];
+          const float rn = cr[r] - al * cq[r];
+          cr[r] = rn;
+          rr += rn * rn;
+          rz2 += rn * rn / cdi[r];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          rr += __shfl_xor_sync(0xffffffffu, rr, o);
+          rz2 += __shfl_xor_sync(0xffffffffu, rz2, o);
+        }
+        if (rr <= 1e-12f * rr0) {
+          ok = true;
+          break;
+        }
+        const float be = rz2 / rz;
+        rz = rz2;
+        __syncwarp();
+        for (int r = lane; r < G; r += 32) cp[r] = cr[r] / cdi[r] + be * cp[r];
+        __syncwarp();
+      }
+      bool finite = true;
+      for (int r = lane; r < G; r += 32) {
+        finite &= isfinite(cx[r]);
+        a.cbuf[(int64_t)G * G + (int64_t)I * G + r] = cx[r];
+        s_brow[r] = cx[r];
+      }
+      finite = __all_sync(0xffffffffu, finite);
+      if (lane == 0 && !(ok && finite)) atomicExch(&st->coarse_off, 1);
+    }
+    __syncthreads();
+    {
+      double z0[1] = {0.0}, zt[1];
+      if (!grid_allreduce<double, 1>(gs, z0, zt, shd)) return;
+    }
+    coarse = *reinterpret_cast<volatile int *>(&st->coarse_off) == 0;
+  }
+
   for (int i = threadIdx.x; i < nt * 6; i += blockDim.x) s_nbr[i] = a.nbr[(int64_t)b0 * 6 + i];
   for (int i = threadIdx.x; i < nt * 1000; i += blockDim.x) s_zb[i] = 0.f;
   if (threadIdx.x < 16)
@@ -577,6 +752,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   // ---- init: r0 = b, z0 = M r0, w0 = A z0; d_{-1} = s_{-1} = 0.  Per-thread
   // masks: fluid (bit j), halo (bit j), neighbour count (3 bits per j).
   unsigned fmask = 0, hmask = 0, dpack = 0;
+  float rsum0 = 0.f;
 #pragma unroll
   for (int j = 0; j < MAXJ; ++j) {
     const int tl = tl0 + 2 * j;
@@ -598,6 +774,12 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
     s_d[L] = 0.f;
     s_s[L] = 0.f;
     if (REF) s_x64[L] = 0.0;
+    if (CRS) rsum0 += b;
+  }
+  if (CRS && coarse) {  // warp partials of g_I = P^T r0
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) rsum0 += __shfl_down_sync(0xffffffffu, rsum0, o);
+    if ((threadIdx.x & 31) == 0) s_gw[threadIdx.x >> 5] = rsum0;
   }
   __syncthreads();
 
@@ -618,6 +800,11 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   // every solve.  A word is overwritten only after the reduction that
   // follows its reads, so no publication is missed.
   unsigned long long zep = 0;  // z publications, the same sequence in every block
+  auto warp_gsum = [&](float v) {  // warp partials of g_I into s_gw (a barrier follows)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) s_gw[threadIdx.x >> 5] = v;
+  };
   unsigned long long *const HZ = reinterpret_cast<unsigned long long *>(a.hr0);
   auto half_sweep = [&](int c) {  // z = (r + in-tile fluid neighbours' z) / D, colour c
     const int k = threadIdx.x & 255;
@@ -654,11 +841,59 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   };
   // Callers have written z = r/D on their fluid cells, zeroed the rings
   // (zero_rings, SGS only) and passed a barrier.
+  // Coarse correction: each block publishes g_I = P^T r (its fluid cells'
+  // residual sum, warp partials in s_gw) as a tagged word before the sweeps
+  // and gathers every block's after them (by then they have arrived), then
+  // adds e_I = B_I . g to its own fluid cells' z, so the halo exchange, the
+  // stencil and the dot products below all see u = z + P e.
+  unsigned long long gep = 0;  // g publications, the same sequence in every block
+  unsigned long long *const GSL =
+      reinterpret_cast<unsigned long long *>(a.partials + COARSE_SLOTS_OFF);
   auto precond_exchange = [&]() {
+    if (CRS && coarse && threadIdx.x == 0) {
+      float g = 0.f;
+#pragma unroll 8
+      for (int w = 0; w < 32; ++w) g += s_gw[w];
+      st_relaxed_u64(GSL + (gep & 1ull) * SM_MAXG + blockIdx.x,
+                     ((gep + 1ull) << 32) | __float_as_uint(g));
+    }
     for (int sw = 0; sw < sgs; ++sw) {
       half_sweep(1);
       __syncthreads();
       half_sweep(0);
+      __syncthreads();
+    }
+    if (CRS && coarse) {
+      const unsigned long long tag = (gep + 1ull) << 32;
+      const unsigned long long *src = GSL + (gep & 1ull) * SM_MAXG;
+      if ((int)threadIdx.x < G) {
+        unsigned long long w = 0;
+        long long spins = 0;
+        for (;;) {
+          w = ld_relaxed_u64(src + threadIdx.x);
+          if ((w & 0xffffffff00000000ull) == tag) break;
+          if (++spins > SM_SPIN_LIMIT) {
+            atomicExch(&st->error, 1);
+            w = 0;
+            break;
+          }
+        }
+        s_g[threadIdx.x] = __uint_as_float((unsigned)w);
+      }
+      ++gep;
+      __syncthreads();
+      if (threadIdx.x < 32) {
+        float acc = 0.f;
+        for (int c = threadIdx.x; c < G; c += 32) acc += s_brow[c] * s_g[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if (threadIdx.x == 0) s_eI = acc;
+      }
+      __syncthreads();
+      const float eI = s_eI;
+#pragma unroll
+      for (int j = 0; j < MAXJ; ++j)
+        if ((fmask >> j) & 1) s_zb[(tl0 + 2 * j) * 1000 + pc] += eI;
       __syncthreads();
     }
     phase_mark(1);
@@ -715,6 +950,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
 
   for (int it = 0; it < a.max_iter && !done; ++it) {
     const float alphaf = (float)alpha, nalpha = -alphaf, betaf = (float)beta;
+    float rsum = 0.f;  // g_I = P^T r (coarse correction)
     // ---- own: d = z + beta d; s = w + beta s; x += alpha d; r -= alpha s; z = M r
 #pragma unroll
     for (int j = 0; j < MAXJ; ++j) {
@@ -728,9 +964,11 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       s_x[L] = s_x[L] + alphaf * dn;
       const float rn = s_r[L] + nalpha * sn;
       s_r[L] = rn;
+      if (CRS) rsum += rn;
       *zp = SGS ? rn * s_rtab[8 | ((dpack >> (3 * j)) & 7)]
                 : rn / fmaxf((float)((dpack >> (3 * j)) & 7), 1.0f);
     }
+    if (CRS && coarse) warp_gsum(rsum);
     if (SGS) zero_rings();
     __syncthreads();
     trace_mark(gs);
@@ -786,6 +1024,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
         if (!grid_allreduce<double, 1>(gs, z0, zt, shd)) return;
       }
       double vr[1] = {0.0};
+      rsum = 0.f;
 #pragma unroll
       for (int j = 0; j < MAXJ; ++j) {
         if (!((fmask >> j) & 1)) continue;
@@ -803,10 +1042,12 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
         const double res = (double)(a.sign * a.bdiv[q0 + L]) - (diag * s_x64[L] - sum);
         const float rf = (float)res;
         s_r[L] = rf;
+        if (CRS) rsum += rf;
         s_zb[tl * 1000 + pc] =
             SGS ? rf * s_rtab[8 | ((code >> CODE_DIAG_SHIFT) & 7)] : rf / diagz_of(code);
         vr[0] += res * res;
       }
+      if (CRS && coarse) warp_gsum(rsum);
       if (SGS) zero_rings();
       double tr[1];
       if (!grid_allreduce<double, 1>(gs, vr, tr, shd)) return;
@@ -879,6 +1120,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
     st->status = done ? status : GF_NOT_CONVERGED;
     if (status != GF_OK) st->status = status;
     st->smem_solver = 1;
+    st->coarse_used = coarse ? 1 : 0;
   }
 }
 
@@ -888,7 +1130,7 @@ static bool fits_t(Ctx *c) {
   cudaFuncAttributes fa;
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device) !=
           cudaSuccess ||
-      cudaFuncGetAttributes(&fa, (const void *)k_pcg_smem<Acc, REF, true>) != cudaSuccess) {
+      cudaFuncGetAttributes(&fa, (const void *)k_pcg_smem<Acc, REF, true, true>) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
@@ -902,7 +1144,10 @@ bool pcg_smem_fits(Ctx *c, bool refined) {
 template <typename Acc, bool REF>
 static int launch_t(Ctx *c, PcgSmemArgs &a) {
   const size_t smem = SmemCfg<REF>::BYTES;
-  auto fn = a.sgs_sweeps > 0 ? k_pcg_smem<Acc, REF, true> : k_pcg_smem<Acc, REF, false>;
+  auto fn = a.sgs_sweeps > 0 ? (a.coarse ? k_pcg_smem<Acc, REF, true, true>
+                                         : k_pcg_smem<Acc, REF, true, false>)
+                             : (a.coarse ? k_pcg_smem<Acc, REF, false, true>
+                                         : k_pcg_smem<Acc, REF, false, false>);
   int e = check_cuda(c, cudaFuncSetAttribute((const void *)fn,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem),

@@ -1158,6 +1158,15 @@ int pressure_alloc(Ctx *c) {
   if ((e = A((void **)&c->bar_counters, BAR_BYTES, "alloc barrier counters"))) return e;
   if ((e = A((void **)&c->trace, TRACE_CAP * 8, "alloc trace"))) return e;
   if ((e = A((void **)&c->halo, nk * 6 * 4, "alloc halo buffers"))) return e;
+  // coarse operator and its inverse (GF_FLAG_COARSE), allocated up front so
+  // that solves can be captured in CUDA graphs
+  if ((e = A((void **)&c->coarse_buf, 2 * (size_t)COARSE_MAXG * COARSE_MAXG * 4,
+             "alloc coarse operator")))
+    return e;
+  // the solves warm-start from the previous inverse rows: zero the first
+  if ((e = check_cuda(c, cudaMemset(c->coarse_buf, 0, 2 * (size_t)COARSE_MAXG * COARSE_MAXG * 4),
+                      "zero coarse operator")))
+    return e;
   if ((e = A((void **)&c->tile_cost, (size_t)c->ntiles * 4, "alloc tile cost"))) return e;
   if ((e = check_cuda(c, cudaMemset(c->state, 0, sizeof(PcgState)), "zero pcg state"))) return e;
   if ((e = check_cuda(c, cudaMallocHost((void **)&c->state_host, sizeof(PcgState)),
@@ -1170,7 +1179,7 @@ int pressure_alloc(Ctx *c) {
 void pressure_free(Ctx *c) {
   void *ps[] = {c->tile_slot, c->tile_list, c->tile_order, c->tile_nbr, c->n_active, c->code, c->bdiv,
                 c->xf, c->r, c->z, c->d0, c->d1, c->Ad, c->x64, c->partials, c->state,
-                c->bar_counters, c->trace, c->halo, c->tile_cost};
+                c->bar_counters, c->trace, c->halo, c->tile_cost, c->coarse_buf};
   for (void *p : ps)
     if (p) cudaFree(p);
   if (c->state_host) cudaFreeHost(c->state_host);
@@ -1368,10 +1377,13 @@ int launch_pressure(Ctx *c, const gf_step_params *prm) {
                           "zero barrier counters")))
         return e;
       // the one-round-trip reduction words of the shared-memory solver
-      // ([2][160][4] u64 at 2048 doubles into the partials buffer)
-      if ((e = check_cuda(c, cudaMemsetAsync(c->partials + 2048, 0, 2 * 160 * 4 * 8, st),
+      // ([2][160][4] u64 at 2048 doubles into the partials buffer), then the
+      // tagged coarse sums ([2][160] u64)
+      if ((e = check_cuda(c, cudaMemsetAsync(c->partials + 2048, 0, (2 * 160 * 4 + 2 * 160) * 8,
+                                             st),
                           "zero reduction words")))
         return e;
+      const bool coarse = (prm->flags & GF_FLAG_COARSE) != 0;
       float *h = c->halo;
       const int64_t nk = c->nkeys;
       PcgSmemArgs sa{c->n_active, c->tile_nbr, c->tile_cost, c->code, c->bdiv, c->xf, h, h + nk, h + 2 * nk,
@@ -1379,7 +1391,8 @@ int launch_pressure(Ctx *c, const gf_step_params *prm) {
                      c->partials, c->bar_counters, c->state,
                      (prm->flags & GF_FLAG_TRACE) ? c->trace : nullptr, TRACE_CAP,
                      prm->max_iters, check_every, prm->tol * prm->tol, replace2, sign,
-                     (prm->flags & GF_FLAG_SGS_MASK) >> GF_FLAG_SGS_SHIFT};
+                     (prm->flags & GF_FLAG_SGS_MASK) >> GF_FLAG_SGS_SHIFT, coarse ? 1 : 0,
+                     c->coarse_buf};
       // the solver publishes tagged 64-bit halo words over the first two halo
       // arrays; their counts restart at 1 with every solve
       if ((e = check_cuda(c, cudaMemsetAsync(h, 0, (size_t)nk * 8, st), "zero tagged halo")))

@@ -23,6 +23,9 @@ default path):
   reference's): red-black symmetric Gauss-Seidel sweeps (``pcg_sgs_sweeps``,
   1-3) on each 8^3 pressure tile with its neighbours held at zero.  Same
   operator and stop test, about half the iterations.
+* ``pcg_coarse=True`` (new): adds a coarse correction to the shared-memory
+  PCG's preconditioner -- one constant per solver block's region of tiles,
+  solved exactly -- for fewer iterations again.
 * Particles are kept sorted by cell inside the solver; ``pos``/``vel``/
   ``affine_C``/``get_particles()`` return them in the caller's original order.
 * Viscosity, surface tension, colour/temperature attributes, sub-dense storage,
@@ -145,7 +148,8 @@ class FlipSolver3D:
                  pcg_rhs_sign: int = -1,
                  pcg_check_every: int = 10,
                  pcg_preconditioner: str = "jacobi",
-                 pcg_sgs_sweeps: int = 2):
+                 pcg_sgs_sweeps: int = 2,
+                 pcg_coarse: bool = False):
         if pcg_preconditioner not in ("jacobi", "tile_sgs"):
             raise ValueError(f"unknown pcg_preconditioner: {pcg_preconditioner!r}")
         if not 1 <= int(pcg_sgs_sweeps) <= 3:
@@ -174,6 +178,7 @@ class FlipSolver3D:
         self.pcg_check_every = int(pcg_check_every)
         self.pcg_preconditioner = pcg_preconditioner
         self.pcg_sgs_sweeps = int(pcg_sgs_sweeps)
+        self.pcg_coarse = bool(pcg_coarse)
         self._enable_cuda_graphs = bool(enable_cuda_graphs)
         self._enable_sub_dense = bool(enable_sub_dense)
         self._prof = StepProfiler(enabled=enable_timing)
@@ -370,9 +375,10 @@ class FlipSolver3D:
                                self.pcg_rhs_sign, self._pcg_flags())
 
     def _pcg_flags(self) -> int:
+        f = _lib.GF_FLAG_COARSE if self.pcg_coarse else 0
         if self.pcg_preconditioner == "tile_sgs":
-            return self.pcg_sgs_sweeps << _lib.GF_FLAG_SGS_SHIFT
-        return 0
+            f |= self.pcg_sgs_sweeps << _lib.GF_FLAG_SGS_SHIFT
+        return f
 
     _MAX_GRAPHS = 4
 

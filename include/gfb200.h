@@ -102,6 +102,12 @@ typedef struct gf_step_params {
  * iteration.  The global-memory kernel always uses Jacobi. */
 #define GF_FLAG_SGS_SHIFT 2
 #define GF_FLAG_SGS_MASK 12
+/* flags: add a coarse correction to the shared-memory PCG's preconditioner
+ * (no counterpart in the reference): one constant per block's region of
+ * tiles, B = (P^T A P)^-1 computed at the start of every solve, M^-1 =
+ * M_tile^-1 + P B P^T.  Same operator, stop test and answer; fewer
+ * iterations.  The global-memory kernel ignores it. */
+#define GF_FLAG_COARSE 16
 
 /* ---- context ------------------------------------------------------------ */
 /* Allocates scratch for a grid and up to max_particles particles on the
@@ -163,7 +169,7 @@ typedef struct gf_pressure_info {
   int64_t n_fluid;      /* fluid cells in the system */
   double relres;        /* ||r||/||r0|| (PCG), ||b-Ax||/||b|| in FP64 (refined), -1 otherwise */
   int32_t kernel;       /* PCG kernel that ran: 1 shared-memory resident, 2 global-memory */
-  int32_t pad;
+  int32_t coarse;       /* 1: the solve applied the GF_FLAG_COARSE correction */
 } gf_pressure_info;
 /* Copies the trace buffer of the last traced PCG solve (up to cap int64
  * entries: block 0's SM-cycle stamps in the first half, *n of them, then per
