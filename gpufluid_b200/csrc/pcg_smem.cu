@@ -490,7 +490,6 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   __shared__ float s_g[SM_MAXG], s_brow[SM_MAXG];
   __shared__ short s_freg[MAXT * 6];
   __shared__ float s_gw[32];
-  __shared__ float s_eI;
 
   PcgState *st = a.st;
   const int na = *a.n_active;
@@ -857,20 +856,26 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       st_relaxed_u64(GSL + (gep & 1ull) * SM_MAXG + blockIdx.x,
                      ((gep + 1ull) << 32) | __float_as_uint(g));
     }
+    // the gather's first load is issued before the last half-sweep, so its
+    // latency hides behind the sweep; it is polled again only if stale
+    const unsigned long long *gsrc = GSL + (gep & 1ull) * SM_MAXG;
+    unsigned long long gpre = 0;
     for (int sw = 0; sw < sgs; ++sw) {
       half_sweep(1);
       __syncthreads();
+      if (CRS && coarse && sw == sgs - 1 && (int)threadIdx.x < G)
+        gpre = ld_relaxed_u64(gsrc + threadIdx.x);
       half_sweep(0);
       __syncthreads();
     }
     if (CRS && coarse) {
       const unsigned long long tag = (gep + 1ull) << 32;
-      const unsigned long long *src = GSL + (gep & 1ull) * SM_MAXG;
       if ((int)threadIdx.x < G) {
-        unsigned long long w = 0;
+        unsigned long long w = sgs > 0 ? gpre : 0ull;
         long long spins = 0;
         for (;;) {
-          w = ld_relaxed_u64(src + threadIdx.x);
+          if ((w & 0xffffffff00000000ull) == tag) break;
+          w = ld_relaxed_u64(gsrc + threadIdx.x);
           if ((w & 0xffffffff00000000ull) == tag) break;
           if (++spins > SM_SPIN_LIMIT) {
             atomicExch(&st->error, 1);
@@ -882,15 +887,10 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       }
       ++gep;
       __syncthreads();
-      if (threadIdx.x < 32) {
-        float acc = 0.f;
-        for (int c = threadIdx.x; c < G; c += 32) acc += s_brow[c] * s_g[c];
+      float eI = 0.f;  // every warp: e_I = B_I . g (the same order in every warp)
+      for (int c = threadIdx.x & 31; c < G; c += 32) eI += s_brow[c] * s_g[c];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-        if (threadIdx.x == 0) s_eI = acc;
-      }
-      __syncthreads();
-      const float eI = s_eI;
+      for (int o = 16; o > 0; o >>= 1) eI += __shfl_xor_sync(0xffffffffu, eI, o);
 #pragma unroll
       for (int j = 0; j < MAXJ; ++j)
         if ((fmask >> j) & 1) s_zb[(tl0 + 2 * j) * 1000 + pc] += eI;
