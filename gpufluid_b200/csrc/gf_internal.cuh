@@ -28,7 +28,13 @@ namespace gf {
 constexpr int TILE = 8;            // tile edge in cells (the reference's BLOCK_SIZE, :950)
 constexpr int TILE_CELLS = 512;    // cells per tile
 constexpr int MAX_PCG_BLOCKS = 4096;
-constexpr int COARSE_MAXG = 160;  // coarse space: at most one region per block of the smem PCG
+constexpr int COARSE_MAXG = 160;  // blocks of the shared-memory PCG, at most
+constexpr int COARSE_K = 4;       // coarse regions per block
+// coarse buffer: rows of B [CMAX][CMAX], then the compact rows of P^T A P
+// (diagonal [CMAX], count [CMAX], values [CMAX][32], columns [CMAX][32])
+constexpr int64_t COARSE_BUF_FLOATS =
+    (int64_t)(COARSE_MAXG * COARSE_K) * (COARSE_MAXG * COARSE_K) + 2 * COARSE_MAXG * COARSE_K +
+    2 * 32 * COARSE_MAXG * COARSE_K;
 constexpr int TRACE_CAP = 4096;
 
 // Stencil code bits (per compact cell).
@@ -79,8 +85,8 @@ struct PcgSmemArgs {
   double tol2, replace2;
   float sign;
   int sgs_sweeps;             // 0: Jacobi (the reference's); 1-3: tile-local symmetric GS
-  int coarse;                 // 1: add the block-region coarse correction
-  float *cbuf;                // coarse: [G*G] assembled P^T A P, then [G*G] its inverse
+  int coarse;                 // coarse regions per block (0: no coarse correction)
+  float *cbuf;                // coarse: rows of B, then the compact rows of P^T A P
 };
 
 
@@ -160,7 +166,7 @@ struct Ctx {
   double *partials = nullptr;    // [3 * MAX_PCG_BLOCKS]
   unsigned long long *bar_counters = nullptr;  // 8 lines x 16 u64
   float *halo = nullptr;         // [6 * nkeys] halo publication buffers
-  float *coarse_buf = nullptr;   // [2 * COARSE_MAXG^2] coarse operator and inverse
+  float *coarse_buf = nullptr;   // [COARSE_BUF_FLOATS] coarse operator and inverse rows
   int32_t *tile_cost = nullptr;  // [ntiles] per-slot PCG work estimate
   long long *trace = nullptr;    // [TRACE_CAP] PCG phase timestamps
   bool trace_on = false;

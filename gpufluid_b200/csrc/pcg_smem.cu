@@ -51,7 +51,10 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
 }
 
 constexpr int SM_MAXG = 160;      // blocks (one per SM)
-static_assert(SM_MAXG == COARSE_MAXG, "coarse buffer sizing");
+constexpr int CK = 4;             // coarse sub-regions per block, at most
+constexpr int CMAX = SM_MAXG * CK;  // coarse regions, at most
+constexpr int CCAP = 32;          // off-diagonal entries per coarse row, at most
+static_assert(SM_MAXG == COARSE_MAXG && CK == COARSE_K, "coarse buffer sizing");
 
 struct GridSync {
   double *partials;            // [2][4][G]
@@ -302,7 +305,7 @@ __device__ __forceinline__ void ring_fill_tagged(float *s_zb, const int *s_nbr,
 // solve's accuracy rests on its FP64 residual replacements, not on these.
 constexpr int FAST_WORDS = 4;  // words per block and parity (3 used)
 constexpr int64_t FAST_SLOTS_OFF = 2048;  // in doubles, into the partials buffer
-// tagged coarse sums g_I: [2][SM_MAXG] u64 after the reduction words
+// tagged coarse sums g_r: [2][CMAX] u64 after the reduction words
 constexpr int64_t COARSE_SLOTS_OFF = FAST_SLOTS_OFF + 2 * 160 * FAST_WORDS;
 struct FastSync {
   unsigned long long *slots;  // [2][SM_MAXG][FAST_WORDS], zeroed per solve
@@ -487,9 +490,9 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   __shared__ double shd[36 * 4];
   // coarse correction: region sums g = P^T r gathered from every block, the
   // block's row of B, region of each face's neighbouring tile
-  __shared__ float s_g[SM_MAXG], s_brow[SM_MAXG];
+  __shared__ float s_ep[CK][32];  // warp partials of e_r = B_r . g
   __shared__ short s_freg[MAXT * 6];
-  __shared__ float s_gw[32];
+  __shared__ float s_gw[CK][32];  // warp partials of the regions' residual sums
 
   PcgState *st = a.st;
   const int na = *a.n_active;
@@ -540,17 +543,27 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   const int l = threadIdx.x & 511, tl0 = threadIdx.x >> 9;
   const int pc = pad_of(l);
 
-  // ---- coarse space (a.coarse): one constant per block's region of tiles,
-  // P its indicator on fluid cells.  Each block assembles its row of
-  // A_c = P^T A P (diagonal: sum over its cells of diag - #fluid neighbours
-  // in the region; off-diagonal: -#fluid-fluid faces to the other region),
-  // then solves A_c x = e_I for its own column of B = A_c^-1 (one warp,
-  // Jacobi-preconditioned CG in float32 on the compacted rows), which is row
-  // I of the symmetric B.  The preconditioner becomes M^-1 = M_tile^-1 +
-  // P B P^T (additive two-level), symmetric positive definite as long as B
-  // is; any block whose column solve fails switches the correction off for
-  // the whole solve.  Dynamic shared memory is free until the tiles load.
-  bool coarse = CRS && a.cbuf != nullptr;
+  // ---- coarse space (a.coarse = K, sub-regions per block): the block's run
+  // of tiles is split into K runs by tile count, and each run's fluid cells
+  // form one region (GR = G K regions); P is their indicator.  Each block
+  // assembles its K rows of A_c = P^T A P (diagonal: sum over the region's
+  // cells of diag - #fluid neighbours in the region; off-diagonal: -#fluid-
+  // fluid faces to each other region), published compactly; then each of its
+  // K warps solves A_c x = e_r for one of its regions r (Jacobi-
+  // preconditioned CG in float32, warm-started from the row solved last
+  // time), which is row r of the symmetric B = A_c^-1.  The preconditioner
+  // becomes M^-1 = M_tile^-1 + P B P^T (additive two-level).  A block whose
+  // solve fails, or whose row has more than CCAP off-diagonal entries,
+  // switches the correction off for the whole solve.  Dynamic shared memory
+  // is free until the tiles load.
+  const int K = (CRS && a.cbuf != nullptr) ? a.coarse : 0;
+  const int GR = G * (K > 0 ? K : 1);
+  bool coarse = K > 0;
+  float *const Bg = a.cbuf;                                   // [GR][GR] rows of B
+  float *const Cdiag = a.cbuf + (int64_t)CMAX * CMAX;         // [GR]
+  int *const Cnnz = reinterpret_cast<int *>(Cdiag + CMAX);    // [GR]
+  float *const Cval = reinterpret_cast<float *>(Cnnz + CMAX); // [GR][CCAP]
+  int *const Ccol = reinterpret_cast<int *>(Cval + CMAX * CCAP);  // [GR][CCAP]
   if (coarse) {
     for (int f = threadIdx.x; f < nt * 6; f += blockDim.x) {
       const int sl = a.nbr[(int64_t)b0 * 6 + f];
@@ -561,11 +574,13 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
           const int mid = (lo + hi) >> 1;
           if (s_bounds[mid] <= sl) lo = mid; else hi = mid;
         }
-        r = lo;
+        const int ntg = s_bounds[lo + 1] - s_bounds[lo];
+        r = lo * K + (sl - s_bounds[lo]) * K / ntg;
       }
       s_freg[f] = (short)r;
     }
-    for (int i = threadIdx.x; i < G; i += blockDim.x) s_g[i] = 0.f;
+    float *rows = reinterpret_cast<float *>(smem);  // [K][GR]
+    for (int i = threadIdx.x; i < K * GR; i += blockDim.x) rows[i] = 0.f;
     __syncthreads();
     const int I = blockIdx.x;
     for (int L = threadIdx.x; L < nt * 512; L += blockDim.x) {
@@ -573,127 +588,134 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       if (!(code & CODE_FLUID)) continue;
       const int tl = L >> 9, lc = L & 511;
       const int li = lc >> 6, lj = (lc >> 3) & 7, lk = lc & 7;
+      const int sub = tl * K / nt, R0 = I * K + sub;
       int same = 0;
       for (int dir = 0; dir < 6; ++dir) {
         if (!(code & (1 << dir))) continue;
         const bool inside = dir == 0 ? li > 0 : dir == 1 ? li < 7 : dir == 2 ? lj > 0
                           : dir == 3 ? lj < 7 : dir == 4 ? lk > 0 : lk < 7;
-        const int R = inside ? I : (int)s_freg[tl * 6 + dir];
-        if (R == I || R < 0) ++same; else atomicAdd(&s_g[R], -1.0f);
+        const int R = inside ? R0 : (int)s_freg[tl * 6 + dir];
+        if (R == R0 || R < 0) ++same; else atomicAdd(&rows[sub * GR + R], -1.0f);
       }
-      atomicAdd(&s_g[I], (float)((int)((code >> CODE_DIAG_SHIFT) & 7) - same));
+      atomicAdd(&rows[sub * GR + R0], (float)((int)((code >> CODE_DIAG_SHIFT) & 7) - same));
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < G; i += blockDim.x) a.cbuf[(int64_t)I * G + i] = s_g[i];
+    {  // warp r publishes row I K + r compactly (diagonal 1 for an empty region)
+      const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+      if (wid < K) {
+        const int gr = I * K + wid;
+        const float *row = rows + wid * GR;
+        int n = 0;
+        for (int c0 = 0; c0 < GR; c0 += 32) {
+          const int c = c0 + lane;
+          const float v = c < GR ? row[c] : 0.f;
+          const bool off = v != 0.f && c != gr;
+          const unsigned m = __ballot_sync(0xffffffffu, off);
+          const int k = n + __popc(m & ((1u << lane) - 1u));
+          if (off && k < CCAP) {
+            Cval[gr * CCAP + k] = v;
+            Ccol[gr * CCAP + k] = c;
+          }
+          n += __popc(m);
+        }
+        if (lane == 0) {
+          const float d = row[gr];
+          Cdiag[gr] = d > 0.f ? d : 1.0f;
+          Cnnz[gr] = n < CCAP ? n : CCAP;
+          if (n > CCAP) atomicExch(&st->coarse_off, 1);
+        }
+      }
+    }
     {
       double z0[1] = {0.0}, zt[1];
       if (!grid_allreduce<double, 1>(gs, z0, zt, shd)) return;
     }
-    // compacted rows (stride G) of A_c and the CG vectors in dynamic smem
-    float *cval = reinterpret_cast<float *>(smem);
-    int *ccol = reinterpret_cast<int *>(cval + G * G);
-    float *cx = reinterpret_cast<float *>(ccol + G * G);
-    float *cr = cx + SM_MAXG, *cp = cr + SM_MAXG, *cq = cp + SM_MAXG, *cdi = cq + SM_MAXG;
-    int *s_cnnz = reinterpret_cast<int *>(s_g);  // s_g is free until the solve
-    {
-      const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-      for (int r = wid; r < G; r += 32) {
-        int n = 0;
-        float dg = 0.f;
-        for (int c0 = 0; c0 < G; c0 += 32) {
-          const int c = c0 + lane;
-          const float v = c < G ? __ldcg(a.cbuf + (int64_t)r * G + c) : 0.f;
-          if (c == r) dg = v;
-          const unsigned nzm = __ballot_sync(0xffffffffu, v != 0.f && c != r);
-          if (v != 0.f && c != r) {
-            const int k = n + __popc(nzm & ((1u << lane) - 1u));
-            cval[r * G + k] = v;
-            ccol[r * G + k] = c;
-          }
-          n += __popc(nzm);
-        }
-        if (lane == 0) s_cnnz[r] = n;
-        // the diagonal lives in cdi (1 for an empty region: decoupled)
-        const unsigned have = __ballot_sync(0xffffffffu, dg != 0.f);
-        float dv = 0.f;
-        if (have) dv = __shfl_sync(0xffffffffu, dg, __ffs(have) - 1);
-        if (lane == 0) cdi[r] = dv > 0.f ? dv : 1.0f;
-      }
+    // all rows of A_c and K sets of CG vectors in dynamic smem
+    float *sdi = reinterpret_cast<float *>(smem);
+    int *snz = reinterpret_cast<int *>(sdi + CMAX);
+    float *sval = reinterpret_cast<float *>(snz + CMAX);
+    short *scol = reinterpret_cast<short *>(sval + CMAX * CCAP);
+    float *vec = reinterpret_cast<float *>(scol + CMAX * CCAP);  // [K][4][CMAX]
+    for (int i = threadIdx.x; i < GR; i += blockDim.x) {
+      sdi[i] = __ldcg(Cdiag + i);
+      snz[i] = __ldcg(Cnnz + i);
+    }
+    for (int i = threadIdx.x; i < GR * CCAP; i += blockDim.x) {
+      sval[i] = __ldcg(Cval + i);
+      scol[i] = (short)__ldcg(Ccol + i);
     }
     __syncthreads();
-    if (threadIdx.x < 32) {  // warp 0: CG for column I, Jacobi-preconditioned
-      // warm start from the row this block solved last time (the coarse
-      // operator changes little between solves; zero on the first)
-      const int lane = threadIdx.x;
-      const float *prev = a.cbuf + (int64_t)G * G + (int64_t)I * G;
-      for (int r = lane; r < G; r += 32) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (wid < K) {  // warp w: CG for column I K + w, Jacobi-preconditioned
+      const int gr = I * K + wid;
+      float *cx = vec + wid * 4 * CMAX, *cr = cx + CMAX, *cp = cr + CMAX, *cq = cp + CMAX;
+      auto matvec = [&](const float *x, int r) {
+        float acc = sdi[r] * x[r];
+        const int n = snz[r];
+        for (int k = 0; k < n; ++k) acc += sval[r * CCAP + k] * x[scol[r * CCAP + k]];
+        return acc;
+      };
+      const float *prev = Bg + (int64_t)gr * GR;
+      for (int r = lane; r < GR; r += 32) {
         const float x0 = __ldcg(prev + r);
         cx[r] = isfinite(x0) ? x0 : 0.f;
       }
       __syncwarp();
-      float rz = 0.f;
-      for (int r = lane; r < G; r += 32) {
-        float acc = cdi[r] * cx[r];
-        const int n = s_cnnz[r];
-        for (int k = 0; k < n; ++k) acc += cval[r * G + k] * cx[ccol[r * G + k]];
-        const float b = (r == I ? 1.f : 0.f) - acc;
+      float rz = 0.f, rr = 0.f;
+      for (int r = lane; r < GR; r += 32) {
+        const float b = (r == gr ? 1.f : 0.f) - matvec(cx, r);
         cr[r] = b;
-        cp[r] = b / cdi[r];
+        cp[r] = b / sdi[r];
         rz += b * cp[r];
+        rr += b * b;
       }
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) rz += __shfl_xor_sync(0xffffffffu, rz, o);
-      const float rr0 = 1.f;  // ||e_I||^2
-      bool ok = false;
-      {
-        float rr = 0.f;
-        for (int r = lane; r < G; r += 32) rr += cr[r] * cr[r];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) rr += __shfl_xor_sync(0xffffffffu, rr, o);
-        ok = rr <= 1e-12f * rr0;
+      for (int o = 16; o > 0; o >>= 1) {
+        rz += __shfl_xor_sync(0xffffffffu, rz, o);
+        rr += __shfl_xor_sync(0xffffffffu, rr, o);
       }
+      bool ok = rr <= 1e-12f;  // ||e_r|| = 1
       __syncwarp();
-      for (int it = 0; it < 4 * SM_MAXG && !ok; ++it) {
+      for (int it = 0; it < 4 * CMAX && !ok; ++it) {
         float pq = 0.f;
-        for (int r = lane; r < G; r += 32) {
-          float acc = cdi[r] * cp[r];
-          const int n = s_cnnz[r];
-          for (int k = 0; k < n; ++k) acc += cval[r * G + k] * cp[ccol[r * G + k]];
-          cq[r] = acc;
-          pq += cp[r] * acc;
+        for (int r = lane; r < GR; r += 32) {
+          const float q = matvec(cp, r);
+          cq[r] = q;
+          pq += cp[r] * q;
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) pq += __shfl_xor_sync(0xffffffffu, pq, o);
         if (!(pq > 0.f)) break;
         const float al = rz / pq;
-        float rr = 0.f, rz2 = 0.f;
-        for (int r = lane; r < G; r += 32) {
+        float rz2 = 0.f;
+        rr = 0.f;
+        for (int r = lane; r < GR; r += 32) {
           cx[r] += al * cp[r];
           const float rn = cr[r] - al * cq[r];
           cr[r] = rn;
           rr += rn * rn;
-          rz2 += rn * rn / cdi[r];
+          rz2 += rn * rn / sdi[r];
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
           rr += __shfl_xor_sync(0xffffffffu, rr, o);
           rz2 += __shfl_xor_sync(0xffffffffu, rz2, o);
         }
-        if (rr <= 1e-12f * rr0) {
+        if (rr <= 1e-12f) {
           ok = true;
           break;
         }
         const float be = rz2 / rz;
         rz = rz2;
         __syncwarp();
-        for (int r = lane; r < G; r += 32) cp[r] = cr[r] / cdi[r] + be * cp[r];
+        for (int r = lane; r < GR; r += 32) cp[r] = cr[r] / sdi[r] + be * cp[r];
         __syncwarp();
       }
       bool finite = true;
-      for (int r = lane; r < G; r += 32) {
+      float *out = Bg + (int64_t)gr * GR;
+      for (int r = lane; r < GR; r += 32) {
         finite &= isfinite(cx[r]);
-        a.cbuf[(int64_t)G * G + (int64_t)I * G + r] = cx[r];
-        s_brow[r] = cx[r];
+        out[r] = cx[r];
       }
       finite = __all_sync(0xffffffffu, finite);
       if (lane == 0 && !(ok && finite)) atomicExch(&st->coarse_off, 1);
@@ -751,7 +773,8 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   // ---- init: r0 = b, z0 = M r0, w0 = A z0; d_{-1} = s_{-1} = 0.  Per-thread
   // masks: fluid (bit j), halo (bit j), neighbour count (3 bits per j).
   unsigned fmask = 0, hmask = 0, dpack = 0;
-  float rsum0 = 0.f;
+  unsigned spack = 0;  // coarse sub-region of the tile of each j (2 bits)
+  float rs[CK] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
   for (int j = 0; j < MAXJ; ++j) {
     const int tl = tl0 + 2 * j;
@@ -773,12 +796,21 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
     s_d[L] = 0.f;
     s_s[L] = 0.f;
     if (REF) s_x64[L] = 0.0;
-    if (CRS) rsum0 += b;
-  }
-  if (CRS && coarse) {  // warp partials of g_I = P^T r0
+    if (CRS && coarse) {
+      const int sub = tl * K / nt;
+      spack |= (unsigned)sub << (2 * j);
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) rsum0 += __shfl_down_sync(0xffffffffu, rsum0, o);
-    if ((threadIdx.x & 31) == 0) s_gw[threadIdx.x >> 5] = rsum0;
+      for (int r = 0; r < CK; ++r) rs[r] += sub == r ? b : 0.f;
+    }
+  }
+  if (CRS && coarse) {  // warp partials of g = P^T r0 for the block's regions
+#pragma unroll
+    for (int r = 0; r < CK; ++r) {
+      float v = rs[r];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if ((threadIdx.x & 31) == 0) s_gw[r][threadIdx.x >> 5] = v;
+    }
   }
   __syncthreads();
 
@@ -799,10 +831,14 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   // every solve.  A word is overwritten only after the reduction that
   // follows its reads, so no publication is missed.
   unsigned long long zep = 0;  // z publications, the same sequence in every block
-  auto warp_gsum = [&](float v) {  // warp partials of g_I into s_gw (a barrier follows)
+  auto warp_gsum = [&](float (&v)[CK]) {  // warp partials into s_gw (a barrier follows)
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0) s_gw[threadIdx.x >> 5] = v;
+    for (int r = 0; r < CK; ++r) {
+      float x = v[r];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+      if ((threadIdx.x & 31) == 0) s_gw[r][threadIdx.x >> 5] = x;
+    }
   };
   unsigned long long *const HZ = reinterpret_cast<unsigned long long *>(a.hr0);
   auto half_sweep = [&](int c) {  // z = (r + in-tile fluid neighbours' z) / D, colour c
@@ -849,33 +885,44 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   unsigned long long *const GSL =
       reinterpret_cast<unsigned long long *>(a.partials + COARSE_SLOTS_OFF);
   auto precond_exchange = [&]() {
-    if (CRS && coarse && threadIdx.x == 0) {
+    if (CRS && coarse && (int)threadIdx.x < K) {  // publish g_r for the block's regions
       float g = 0.f;
 #pragma unroll 8
-      for (int w = 0; w < 32; ++w) g += s_gw[w];
-      st_relaxed_u64(GSL + (gep & 1ull) * SM_MAXG + blockIdx.x,
+      for (int w = 0; w < 32; ++w) g += s_gw[threadIdx.x][w];
+      st_relaxed_u64(GSL + (gep & 1ull) * CMAX + blockIdx.x * K + threadIdx.x,
                      ((gep + 1ull) << 32) | __float_as_uint(g));
     }
-    // the gather's first load is issued before the last half-sweep, so its
-    // latency hides behind the sweep; it is polled again only if stale
-    const unsigned long long *gsrc = GSL + (gep & 1ull) * SM_MAXG;
+    // thread t < GR gathers region t's word and holds B_{I K + r, t}; the
+    // first loads are issued before the last half-sweep, so their latency
+    // hides behind the sweep; a stale word is polled again
+    const unsigned long long *gsrc = GSL + (gep & 1ull) * CMAX;
+    const int t = threadIdx.x;
     unsigned long long gpre = 0;
+    float bpre[CK] = {0.f, 0.f, 0.f, 0.f};
+    auto prefetch = [&]() {
+      if (t < GR) {
+        gpre = ld_relaxed_u64(gsrc + t);
+#pragma unroll
+        for (int r = 0; r < CK; ++r)
+          if (r < K) bpre[r] = __ldcg(a.cbuf + (int64_t)(blockIdx.x * K + r) * GR + t);
+      }
+    };
     for (int sw = 0; sw < sgs; ++sw) {
       half_sweep(1);
       __syncthreads();
-      if (CRS && coarse && sw == sgs - 1 && (int)threadIdx.x < G)
-        gpre = ld_relaxed_u64(gsrc + threadIdx.x);
+      if (CRS && coarse && sw == sgs - 1) prefetch();
       half_sweep(0);
       __syncthreads();
     }
     if (CRS && coarse) {
+      if (sgs == 0) prefetch();
       const unsigned long long tag = (gep + 1ull) << 32;
-      if ((int)threadIdx.x < G) {
-        unsigned long long w = sgs > 0 ? gpre : 0ull;
+      float gt = 0.f;
+      if (t < GR) {
+        unsigned long long w = gpre;
         long long spins = 0;
-        for (;;) {
-          if ((w & 0xffffffff00000000ull) == tag) break;
-          w = ld_relaxed_u64(gsrc + threadIdx.x);
+        while ((w & 0xffffffff00000000ull) != tag) {
+          w = ld_relaxed_u64(gsrc + t);
           if ((w & 0xffffffff00000000ull) == tag) break;
           if (++spins > SM_SPIN_LIMIT) {
             atomicExch(&st->error, 1);
@@ -883,17 +930,34 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
             break;
           }
         }
-        s_g[threadIdx.x] = __uint_as_float((unsigned)w);
+        gt = __uint_as_float((unsigned)w);
       }
       ++gep;
-      __syncthreads();
-      float eI = 0.f;  // every warp: e_I = B_I . g (the same order in every warp)
-      for (int c = threadIdx.x & 31; c < G; c += 32) eI += s_brow[c] * s_g[c];
+      // e_r = sum_t B_{I K + r, t} g_t: warp partials, then a fixed-order sum
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) eI += __shfl_xor_sync(0xffffffffu, eI, o);
+      for (int r = 0; r < CK; ++r) {
+        if (r >= K) break;
+        float v = bpre[r] * gt;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if ((t & 31) == 0) s_ep[r][t >> 5] = v;
+      }
+      __syncthreads();
+      float e[CK] = {0.f, 0.f, 0.f, 0.f};  // every warp sums the 32 partials
+#pragma unroll
+      for (int r = 0; r < CK; ++r) {
+        if (r >= K) break;
+        float x = s_ep[r][t & 31];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        e[r] = x;
+      }
 #pragma unroll
       for (int j = 0; j < MAXJ; ++j)
-        if ((fmask >> j) & 1) s_zb[(tl0 + 2 * j) * 1000 + pc] += eI;
+        if ((fmask >> j) & 1) {
+          const int sub = (spack >> (2 * j)) & 3;
+          s_zb[(tl0 + 2 * j) * 1000 + pc] += sub == 0 ? e[0] : sub == 1 ? e[1] : sub == 2 ? e[2] : e[3];
+        }
       __syncthreads();
     }
     phase_mark(1);
@@ -950,7 +1014,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
 
   for (int it = 0; it < a.max_iter && !done; ++it) {
     const float alphaf = (float)alpha, nalpha = -alphaf, betaf = (float)beta;
-    float rsum = 0.f;  // g_I = P^T r (coarse correction)
+    float rsum[CK] = {0.f, 0.f, 0.f, 0.f};  // g = P^T r of the block's regions
     // ---- own: d = z + beta d; s = w + beta s; x += alpha d; r -= alpha s; z = M r
 #pragma unroll
     for (int j = 0; j < MAXJ; ++j) {
@@ -964,7 +1028,11 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       s_x[L] = s_x[L] + alphaf * dn;
       const float rn = s_r[L] + nalpha * sn;
       s_r[L] = rn;
-      if (CRS) rsum += rn;
+      if (CRS) {
+        const int sub = (spack >> (2 * j)) & 3;
+#pragma unroll
+        for (int r = 0; r < CK; ++r) rsum[r] += sub == r ? rn : 0.f;
+      }
       *zp = SGS ? rn * s_rtab[8 | ((dpack >> (3 * j)) & 7)]
                 : rn / fmaxf((float)((dpack >> (3 * j)) & 7), 1.0f);
     }
@@ -1024,7 +1092,8 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
         if (!grid_allreduce<double, 1>(gs, z0, zt, shd)) return;
       }
       double vr[1] = {0.0};
-      rsum = 0.f;
+#pragma unroll
+      for (int r = 0; r < CK; ++r) rsum[r] = 0.f;
 #pragma unroll
       for (int j = 0; j < MAXJ; ++j) {
         if (!((fmask >> j) & 1)) continue;
@@ -1042,7 +1111,11 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
         const double res = (double)(a.sign * a.bdiv[q0 + L]) - (diag * s_x64[L] - sum);
         const float rf = (float)res;
         s_r[L] = rf;
-        if (CRS) rsum += rf;
+        if (CRS) {
+          const int sub = (spack >> (2 * j)) & 3;
+#pragma unroll
+          for (int r = 0; r < CK; ++r) rsum[r] += sub == r ? rf : 0.f;
+        }
         s_zb[tl * 1000 + pc] =
             SGS ? rf * s_rtab[8 | ((code >> CODE_DIAG_SHIFT) & 7)] : rf / diagz_of(code);
         vr[0] += res * res;

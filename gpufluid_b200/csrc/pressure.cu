@@ -1160,11 +1160,10 @@ int pressure_alloc(Ctx *c) {
   if ((e = A((void **)&c->halo, nk * 6 * 4, "alloc halo buffers"))) return e;
   // coarse operator and its inverse (GF_FLAG_COARSE), allocated up front so
   // that solves can be captured in CUDA graphs
-  if ((e = A((void **)&c->coarse_buf, 2 * (size_t)COARSE_MAXG * COARSE_MAXG * 4,
-             "alloc coarse operator")))
+  if ((e = A((void **)&c->coarse_buf, (size_t)COARSE_BUF_FLOATS * 4, "alloc coarse operator")))
     return e;
   // the solves warm-start from the previous inverse rows: zero the first
-  if ((e = check_cuda(c, cudaMemset(c->coarse_buf, 0, 2 * (size_t)COARSE_MAXG * COARSE_MAXG * 4),
+  if ((e = check_cuda(c, cudaMemset(c->coarse_buf, 0, (size_t)COARSE_BUF_FLOATS * 4),
                       "zero coarse operator")))
     return e;
   if ((e = A((void **)&c->tile_cost, (size_t)c->ntiles * 4, "alloc tile cost"))) return e;
@@ -1378,9 +1377,9 @@ int launch_pressure(Ctx *c, const gf_step_params *prm) {
         return e;
       // the one-round-trip reduction words of the shared-memory solver
       // ([2][160][4] u64 at 2048 doubles into the partials buffer), then the
-      // tagged coarse sums ([2][160] u64)
-      if ((e = check_cuda(c, cudaMemsetAsync(c->partials + 2048, 0, (2 * 160 * 4 + 2 * 160) * 8,
-                                             st),
+      // tagged coarse sums ([2][640] u64)
+      if ((e = check_cuda(c, cudaMemsetAsync(c->partials + 2048, 0,
+                                             (2 * 160 * 4 + 2 * COARSE_MAXG * COARSE_K) * 8, st),
                           "zero reduction words")))
         return e;
       const bool coarse = (prm->flags & GF_FLAG_COARSE) != 0;
@@ -1391,8 +1390,8 @@ int launch_pressure(Ctx *c, const gf_step_params *prm) {
                      c->partials, c->bar_counters, c->state,
                      (prm->flags & GF_FLAG_TRACE) ? c->trace : nullptr, TRACE_CAP,
                      prm->max_iters, check_every, prm->tol * prm->tol, replace2, sign,
-                     (prm->flags & GF_FLAG_SGS_MASK) >> GF_FLAG_SGS_SHIFT, coarse ? 1 : 0,
-                     c->coarse_buf};
+                     (prm->flags & GF_FLAG_SGS_MASK) >> GF_FLAG_SGS_SHIFT,
+                     coarse ? COARSE_K : 0, c->coarse_buf};
       // the solver publishes tagged 64-bit halo words over the first two halo
       // arrays; their counts restart at 1 with every solve
       if ((e = check_cuda(c, cudaMemsetAsync(h, 0, (size_t)nk * 8, st), "zero tagged halo")))
