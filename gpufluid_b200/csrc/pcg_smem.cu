@@ -54,6 +54,7 @@ constexpr int SM_MAXG = 160;      // blocks (one per SM)
 constexpr int CK = 4;             // coarse sub-regions per block, at most
 constexpr int CMAX = SM_MAXG * CK;  // coarse regions, at most
 constexpr int CCAP = 32;          // off-diagonal entries per coarse row, at most
+constexpr float kCoarseTol2 = 1e-6f;  // squared residual target of the coarse row solves
 static_assert(SM_MAXG == COARSE_MAXG && CK == COARSE_K, "coarse buffer sizing");
 
 struct GridSync {
@@ -646,79 +647,96 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
     }
     __syncthreads();
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (wid < K) {  // warp w: CG for column I K + w, Jacobi-preconditioned
-      const int gr = I * K + wid;
-      float *cx = vec + wid * 4 * CMAX, *cr = cx + CMAX, *cp = cr + CMAX, *cq = cp + CMAX;
+    {  // the K systems A_c x = e_{I K + q}, 32 / K warps each, in lockstep:
+       // Jacobi-preconditioned CG, warm-started from last solve's rows
+      const int per = 32 / K;                  // warps per system
+      const int q = wid / per;                 // system of this warp
+      const int nth = per * 32, lt = threadIdx.x - q * nth;
+      const int gr = I * K + q;
+      float *cx = vec + q * 4 * CMAX, *cr = cx + CMAX, *cp = cr + CMAX, *cq = cp + CMAX;
+      float *red = reinterpret_cast<float *>(vec + CK * 4 * CMAX);  // [32 warps][2] partials
       auto matvec = [&](const float *x, int r) {
         float acc = sdi[r] * x[r];
         const int n = snz[r];
         for (int k = 0; k < n; ++k) acc += sval[r * CCAP + k] * x[scol[r * CCAP + k]];
         return acc;
       };
+      // sum of v over the system's threads (all threads call it: a barrier)
+      auto sys_sum = [&](float v0, float v1, float *o0, float *o1) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          v0 += __shfl_xor_sync(0xffffffffu, v0, o);
+          v1 += __shfl_xor_sync(0xffffffffu, v1, o);
+        }
+        if (lane == 0) {
+          red[wid * 2 + 0] = v0;
+          red[wid * 2 + 1] = v1;
+        }
+        __syncthreads();
+        float s0 = 0.f, s1 = 0.f;
+        for (int w = q * per; w < (q + 1) * per; ++w) {
+          s0 += red[w * 2 + 0];
+          s1 += red[w * 2 + 1];
+        }
+        __syncthreads();
+        *o0 = s0;
+        *o1 = s1;
+      };
       const float *prev = Bg + (int64_t)gr * GR;
-      for (int r = lane; r < GR; r += 32) {
+      for (int r = lt; r < GR; r += nth) {
         const float x0 = __ldcg(prev + r);
         cx[r] = isfinite(x0) ? x0 : 0.f;
       }
-      __syncwarp();
+      __syncthreads();
       float rz = 0.f, rr = 0.f;
-      for (int r = lane; r < GR; r += 32) {
-        const float b = (r == gr ? 1.f : 0.f) - matvec(cx, r);
-        cr[r] = b;
-        cp[r] = b / sdi[r];
-        rz += b * cp[r];
-        rr += b * b;
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        rz += __shfl_xor_sync(0xffffffffu, rz, o);
-        rr += __shfl_xor_sync(0xffffffffu, rr, o);
-      }
-      bool ok = rr <= 1e-12f;  // ||e_r|| = 1
-      __syncwarp();
-      for (int it = 0; it < 4 * CMAX && !ok; ++it) {
-        float pq = 0.f;
-        for (int r = lane; r < GR; r += 32) {
-          const float q = matvec(cp, r);
-          cq[r] = q;
-          pq += cp[r] * q;
+      {
+        float a0 = 0.f, a1 = 0.f;
+        for (int r = lt; r < GR; r += nth) {
+          const float b = (r == gr ? 1.f : 0.f) - matvec(cx, r);
+          cr[r] = b;
+          cp[r] = b / sdi[r];
+          a0 += b * cp[r];
+          a1 += b * b;
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) pq += __shfl_xor_sync(0xffffffffu, pq, o);
-        if (!(pq > 0.f)) break;
-        const float al = rz / pq;
-        float rz2 = 0.f;
-        rr = 0.f;
-        for (int r = lane; r < GR; r += 32) {
+        sys_sum(a0, a1, &rz, &rr);
+      }
+      bool ok = rr <= kCoarseTol2;  // relative to ||e_r|| = 1
+      bool dead = false;
+      for (int it = 0; it < 4 * CMAX; ++it) {
+        if (__syncthreads_and(ok || dead)) break;  // every system converged
+        float pq = 0.f, dummy = 0.f;
+        for (int r = lt; r < GR; r += nth) {
+          const float v = matvec(cp, r);
+          cq[r] = v;
+          pq += cp[r] * v;
+        }
+        sys_sum(pq, 0.f, &pq, &dummy);
+        const bool run = !(ok || dead);
+        if (run && !(pq > 0.f)) dead = true;
+        const float al = (run && !dead) ? rz / pq : 0.f;
+        float a0 = 0.f, a1 = 0.f;
+        for (int r = lt; r < GR; r += nth) {
           cx[r] += al * cp[r];
           const float rn = cr[r] - al * cq[r];
           cr[r] = rn;
-          rr += rn * rn;
-          rz2 += rn * rn / sdi[r];
+          a0 += rn * rn;
+          a1 += rn * rn / sdi[r];
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          rr += __shfl_xor_sync(0xffffffffu, rr, o);
-          rz2 += __shfl_xor_sync(0xffffffffu, rz2, o);
-        }
-        if (rr <= 1e-12f) {
-          ok = true;
-          break;
-        }
-        const float be = rz2 / rz;
-        rz = rz2;
-        __syncwarp();
-        for (int r = lane; r < GR; r += 32) cp[r] = cr[r] / sdi[r] + be * cp[r];
-        __syncwarp();
+        float rz2;
+        sys_sum(a0, a1, &rr, &rz2);
+        if (run && !dead && rr <= kCoarseTol2) ok = true;
+        const float be = (run && !dead && !ok) ? rz2 / rz : 0.f;
+        if (run && !dead) rz = rz2;
+        for (int r = lt; r < GR; r += nth) cp[r] = cr[r] / sdi[r] + be * cp[r];
       }
       bool finite = true;
       float *out = Bg + (int64_t)gr * GR;
-      for (int r = lane; r < GR; r += 32) {
+      for (int r = lt; r < GR; r += nth) {
         finite &= isfinite(cx[r]);
         out[r] = cx[r];
       }
-      finite = __all_sync(0xffffffffu, finite);
-      if (lane == 0 && !(ok && finite)) atomicExch(&st->coarse_off, 1);
+      if (lt == 0 && (!ok || dead)) atomicExch(&st->coarse_off, 1);
+      if (!finite) atomicExch(&st->coarse_off, 1);
     }
     __syncthreads();
     {
