@@ -24,8 +24,8 @@ default path):
   1-3) on each 8^3 pressure tile with its neighbours held at zero.  Same
   operator and stop test, about half the iterations.
 * ``pcg_coarse=True`` (new): adds a coarse correction to the shared-memory
-  PCG's preconditioner -- one constant per solver block's region of tiles,
-  solved exactly -- for fewer iterations again.
+  PCG's preconditioner -- one constant per region, four regions of tiles per
+  solver block -- for fewer iterations again.
 * Particles are kept sorted by cell inside the solver; ``pos``/``vel``/
   ``affine_C``/``get_particles()`` return them in the caller's original order.
 * Viscosity, surface tension, colour/temperature attributes, sub-dense storage,

@@ -103,10 +103,10 @@ typedef struct gf_step_params {
 #define GF_FLAG_SGS_SHIFT 2
 #define GF_FLAG_SGS_MASK 12
 /* flags: add a coarse correction to the shared-memory PCG's preconditioner
- * (no counterpart in the reference): one constant per block's region of
- * tiles, B = (P^T A P)^-1 computed at the start of every solve, M^-1 =
- * M_tile^-1 + P B P^T.  Same operator, stop test and answer; fewer
- * iterations.  The global-memory kernel ignores it. */
+ * (no counterpart in the reference): one constant per region (four regions
+ * of tiles per solver block), B ~ (P^T A P)^-1 solved at the start of every
+ * solve, M^-1 = M_tile^-1 + P B P^T.  Same operator, stop test and answer;
+ * fewer iterations.  The global-memory kernel ignores it. */
 #define GF_FLAG_COARSE 16
 
 /* ---- context ------------------------------------------------------------ */
