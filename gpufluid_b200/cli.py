@@ -97,7 +97,9 @@ def make_solver(scene, args):
                               enable_cuda_graphs=bool(getattr(args, "enable_cuda_graphs", False)),
                               enable_sub_dense=bool(getattr(args, "enable_sub_dense", False)),
                               pressure_tol=sim.pressure_tol, pcg_rhs_sign=sim.pcg_rhs_sign,
-                              pcg_check_every=sim.pcg_check_every)
+                              pcg_check_every=sim.pcg_check_every,
+                              pcg_preconditioner=sim.pcg_preconditioner,
+                              pcg_sgs_sweeps=sim.pcg_sgs_sweeps, pcg_coarse=sim.pcg_coarse)
     except (NotImplementedError, ValueError) as e:
         raise BlockError("C7.1", str(e)) from None
     sdf = build_obstacle_sdf(scene, solver.cell_centers_np())

@@ -9,7 +9,9 @@ cylinder_y, plane), [[inflow]], [[outflow]], [simulation] and [output].  Problem
 
 Added optional [simulation] keys (reference defaults when absent):
 ``pressure_tol`` (1e-4), ``pcg_rhs_sign`` (-1: physical sign; +1: the
-reference PCG's), ``pcg_check_every`` (10).
+reference PCG's), ``pcg_check_every`` (10), ``pcg_preconditioner``
+("jacobi", the reference's, or "tile_sgs"), ``pcg_sgs_sweeps`` (2) and
+``pcg_coarse`` (false).
 
 Sections outside this build parse, but a scene that uses them is rejected
 with BlockError("C7.1") when the solver is built: mesh fluids and obstacles,
@@ -130,6 +132,9 @@ class SimulationCfg:
     pressure_tol: float = 1e-4
     pcg_rhs_sign: int = -1
     pcg_check_every: int = 10
+    pcg_preconditioner: str = "jacobi"
+    pcg_sgs_sweeps: int = 2
+    pcg_coarse: bool = False
 
 
 @dataclass

@@ -634,7 +634,7 @@ class FlipSolver3D:
                    "gf_pressure_stats")
         return {"iters": info.iters, "replacements": info.replacements, "status": info.status,
                 "n_active_tiles": info.n_active_tiles, "n_fluid": int(info.n_fluid),
-                "relres": info.relres, "kernel": info.kernel}
+                "relres": info.relres, "kernel": info.kernel, "coarse": info.coarse}
 
     def stage_times(self) -> list:
         """Device ms of the last step: bin, p2g, forces_div, pressure,

@@ -64,6 +64,16 @@ def test_parse_minimal(tmp_path):
     assert scene.output.particles is True
 
 
+def test_preconditioner_keys_parse(tmp_path):
+    """Optional [simulation] keys of this build: the PCG preconditioner."""
+    cfg = _write_minimal(tmp_path, extra_sim='pcg_preconditioner = "tile_sgs"\n'
+                                             'pcg_sgs_sweeps = 3\npcg_coarse = true')
+    sim = load_scene(cfg).simulation
+    assert (sim.pcg_preconditioner, sim.pcg_sgs_sweeps, sim.pcg_coarse) == ("tile_sgs", 3, True)
+    sim = load_scene(_write_minimal(tmp_path)).simulation
+    assert (sim.pcg_preconditioner, sim.pcg_sgs_sweeps, sim.pcg_coarse) == ("jacobi", 2, False)
+
+
 def test_defaults_match_reference():
     # defaults of SimulationCfg in src/gpufluid/cli/config.py
     s = SimulationCfg()
