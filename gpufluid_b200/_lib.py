@@ -88,6 +88,8 @@ class TuneInfo(ctypes.Structure):
 
 GF_MESH_TRILINEAR, GF_MESH_CUBIC = 0, 1
 MESH_METHOD = {"trilinear": GF_MESH_TRILINEAR, "cubic": GF_MESH_CUBIC}
+GF_MESH_SMOOTH_LAPLACIAN, GF_MESH_SMOOTH_TAUBIN = 0, 1
+MESH_SMOOTH = {"laplacian": GF_MESH_SMOOTH_LAPLACIAN, "taubin": GF_MESH_SMOOTH_TAUBIN}
 
 
 class MeshParams(ctypes.Structure):
@@ -163,6 +165,8 @@ _SIGS = {
                            ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
     "gf_mesher_copy": ([_vp, _vp, _vp], ctypes.c_int),
     "gf_mesher_copy_field": ([_vp, _vp], ctypes.c_int),
+    "gf_mesher_smooth": ([_vp, _vp, ctypes.c_int64, _vp, ctypes.c_int64, ctypes.c_int32,
+                          ctypes.c_int32, ctypes.c_double, ctypes.c_double], ctypes.c_int),
 }
 
 _lib = None

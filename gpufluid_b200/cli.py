@@ -13,9 +13,8 @@ FLIP/PIC/APIC scene:
   and, with --timings, timings.json;
 - it returns 2 on divergence or a configuration error, else 0.
 
-Mesh options whose reference implementation is third-party code (mesh
-smoothing via scipy, decimation via pyfqmr, the Warp-HashGrid "sdf" method)
-are refused with BlockError("C7.1").
+Mesh options whose reference implementation is third-party code (decimation
+via pyfqmr, the Warp-HashGrid "sdf" method) are refused with BlockError("C7.1").
 ``bench`` runs the reference's fixed throughput table (commands.py:953-977)
 with device-synchronised timing.
 """
@@ -71,9 +70,9 @@ def check_mesh_options(out):
     if out.mesh_method not in ("trilinear", "cubic"):
         raise BlockError("C7.1", f"output.mesh_method {out.mesh_method!r} is not part of this "
                                  "build (trilinear, cubic)")
-    if out.mesh_smooth_passes > 0:
-        raise BlockError("C7.1", "output.mesh_smooth_passes > 0 (mesh smoothing) is not part "
-                                 "of this build")
+    if out.mesh_smooth_passes > 0 and out.mesh_smooth_method not in ("taubin", "laplacian"):
+        raise BlockError("C7.1", f"output.mesh_smooth_method {out.mesh_smooth_method!r}: "
+                                 "expected 'taubin' or 'laplacian'")
     if out.decimate_ratio < 1.0:
         raise BlockError("C7.1", "output.decimate_ratio < 1 (mesh decimation) is not part of "
                                  "this build")

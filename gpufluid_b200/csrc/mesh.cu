@@ -37,6 +37,7 @@
 //   k_mesh_temit  per cube: triangles (vertex ids looked up by edge owner)
 #include <cuda_runtime.h>
 
+#include <cub/cub.cuh>
 #include <cmath>
 #include <cstdint>
 #include <string>
@@ -65,6 +66,9 @@ struct Mesher {
   int64_t tris_cap = 0;
   int64_t nv = -1, nt = -1;    // counts of the last extraction
   int64_t launches = 0;
+  // mesh smoothing scratch, grown on use
+  void *sm_buf = nullptr;
+  size_t sm_cap = 0;
   std::string err;
 };
 
@@ -474,8 +478,153 @@ static int grow(Mesher *m, void **buf, int64_t *cap, int64_t need, int64_t elem,
   return GF_OK;
 }
 
+// ---- mesh smoothing (smoothing.py:22-72) ------------------------------------
+// The uniform Laplacian L = D^-1 A - I of the triangles' 1-rings, A the
+// 0/1 adjacency of distinct neighbours, D = diag(#neighbours) (1 for an
+// isolated vertex).  The reference builds it with scipy in float64 from a
+// float32 1/deg; a row of its CSR holds the diagonal first and then the
+// neighbours in ascending order, and L @ v accumulates in that order from 0,
+// a multiply and an add per entry.  Each pass replaces v by v + c (L v) in
+// float64 (c = lam; Taubin adds a second step with c = mu); the result is
+// rounded to float32 once at the end.  The adjacency: the 6 directed edges
+// of every triangle as (row << 32 | col) keys, radix-sorted, deduplicated and
+// counted per row into CSR offsets.
+__global__ void k_edge_keys(const int32_t *__restrict__ tris, int64_t nt,
+                            unsigned long long *keys) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= nt) return;
+  const unsigned long long a = (unsigned)tris[3 * t], b = (unsigned)tris[3 * t + 1],
+                           c = (unsigned)tris[3 * t + 2];
+  unsigned long long *k = keys + 6 * t;
+  k[0] = a << 32 | b;
+  k[1] = b << 32 | a;
+  k[2] = b << 32 | c;
+  k[3] = c << 32 | b;
+  k[4] = c << 32 | a;
+  k[5] = a << 32 | c;
+}
+
+__global__ void k_row_counts(const unsigned long long *__restrict__ ukeys,
+                             const int64_t *__restrict__ nu, int32_t *counts) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= *nu) return;
+  atomicAdd(&counts[(int64_t)(ukeys[i] >> 32)], 1);
+}
+
+__global__ void k_to_double(const float *__restrict__ v, int64_t n, double *d) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) d[i] = (double)v[i];
+}
+
+__global__ void k_to_float(const double *__restrict__ d, int64_t n, float *v) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) v[i] = (float)d[i];
+}
+
+// v_out = v_in + c (L v_in), one vertex per thread, the reference's order
+__global__ void k_smooth_step(const double *__restrict__ vin, double *__restrict__ vout,
+                              const int32_t *__restrict__ row, const unsigned long long *__restrict__ ukeys,
+                              int64_t nv, double c) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  const int b = row[i], e = row[i + 1];
+  const int deg = e - b;
+  const double dinv = (double)__fdiv_rn(1.0f, (float)(deg > 0 ? deg : 1));
+  double acc[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) acc[k] = __dadd_rn(0.0, __dmul_rn(-1.0, vin[3 * i + k]));
+  for (int q = b; q < e; ++q) {
+    const int64_t j = (int64_t)(ukeys[q] & 0xffffffffull);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) acc[k] = __dadd_rn(acc[k], __dmul_rn(dinv, vin[3 * j + k]));
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) vout[3 * i + k] = __dadd_rn(vin[3 * i + k], __dmul_rn(c, acc[k]));
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static int smooth(Mesher *m, float *verts, int64_t nv, const int32_t *tris, int64_t nt,
+                  int method, int passes, double lam, double mu) {
+  cudaStream_t st = m->stream;
+  const int64_t ne = 6 * nt;
+  // scratch: keys, sorted keys, unique keys, unique count, row offsets, two
+  // double vertex buffers, CUB temporaries
+  size_t tmp_sort = 0, tmp_uniq = 0, tmp_scan = 0;
+  cub::DeviceRadixSort::SortKeys(nullptr, tmp_sort, (unsigned long long *)nullptr,
+                                 (unsigned long long *)nullptr, (int64_t)ne, 0, 64, st);
+  cub::DeviceSelect::Unique(nullptr, tmp_uniq, (unsigned long long *)nullptr,
+                            (unsigned long long *)nullptr, (int64_t *)nullptr, (int64_t)ne, st);
+  cub::DeviceScan::ExclusiveSum(nullptr, tmp_scan, (int32_t *)nullptr, (int32_t *)nullptr,
+                                (int64_t)(nv + 1), st);
+  size_t tmp = tmp_sort > tmp_uniq ? tmp_sort : tmp_uniq;
+  tmp = tmp > tmp_scan ? tmp : tmp_scan;
+  const size_t o_k0 = 0, o_k1 = align256(o_k0 + ne * 8), o_nu = align256(o_k1 + ne * 8),
+               o_cnt = align256(o_nu + 8), o_row = align256(o_cnt + (nv + 1) * 4),
+               o_v0 = align256(o_row + (nv + 1) * 4),
+               o_v1 = align256(o_v0 + nv * 24), o_tmp = align256(o_v1 + nv * 24),
+               total = o_tmp + tmp;
+  if (m->sm_cap < total) {
+    if (m->sm_buf) cudaFree(m->sm_buf);
+    m->sm_buf = nullptr;
+    m->sm_cap = 0;
+    int e = check(m, cudaMalloc(&m->sm_buf, total), "alloc smoothing scratch");
+    if (e) return e;
+    m->sm_cap = total;
+  }
+  char *base = reinterpret_cast<char *>(m->sm_buf);
+  auto *k0 = reinterpret_cast<unsigned long long *>(base + o_k0);
+  auto *k1 = reinterpret_cast<unsigned long long *>(base + o_k1);
+  auto *nu = reinterpret_cast<int64_t *>(base + o_nu);
+  auto *cnt = reinterpret_cast<int32_t *>(base + o_cnt);
+  auto *row = reinterpret_cast<int32_t *>(base + o_row);
+  auto *v0 = reinterpret_cast<double *>(base + o_v0);
+  auto *v1 = reinterpret_cast<double *>(base + o_v1);
+  void *cub_tmp = base + o_tmp;
+  int e;
+  const unsigned g_t = (unsigned)((nt + 255) / 256), g_e = (unsigned)((ne + 255) / 256),
+                 g_v = (unsigned)((nv + 255) / 256), g_c = (unsigned)((3 * nv + 255) / 256);
+  if (ne == 0) return fail(m, GF_INVALID_ARG, "gf_mesher_smooth: no triangles");
+  k_edge_keys<<<g_t, 256, 0, st>>>(tris, nt, k0);
+  size_t t1 = tmp;
+  if ((e = check(m, cub::DeviceRadixSort::SortKeys(cub_tmp, t1, k0, k1, (int64_t)ne, 0, 64, st),
+                 "sort edge keys")))
+    return e;
+  t1 = tmp;
+  if ((e = check(m, cub::DeviceSelect::Unique(cub_tmp, t1, k1, k0, nu, (int64_t)ne, st),
+                 "unique edge keys")))
+    return e;
+  if ((e = check(m, cudaMemsetAsync(cnt, 0, (nv + 1) * 4, st), "zero row counts"))) return e;
+  k_row_counts<<<g_e, 256, 0, st>>>(k0, nu, cnt);
+  t1 = tmp;
+  if ((e = check(m, cub::DeviceScan::ExclusiveSum(cub_tmp, t1, cnt, row, (int64_t)(nv + 1), st),
+                 "row offsets")))
+    return e;
+  k_to_double<<<g_c, 256, 0, st>>>(verts, 3 * nv, v0);
+  m->launches += 4;
+  double *a = v0, *b = v1;
+  for (int p = 0; p < passes; ++p) {
+    k_smooth_step<<<g_v, 256, 0, st>>>(a, b, row, k0, nv, lam);
+    double *t = a;
+    a = b;
+    b = t;
+    m->launches++;
+    if (method == GF_MESH_SMOOTH_TAUBIN) {
+      k_smooth_step<<<g_v, 256, 0, st>>>(a, b, row, k0, nv, mu);
+      t = a;
+      a = b;
+      b = t;
+      m->launches++;
+    }
+  }
+  k_to_float<<<g_c, 256, 0, st>>>(a, 3 * nv, verts);
+  m->launches++;
+  return check(m, cudaGetLastError(), "mesh smoothing");
+}
+
 static void release(Mesher *m) {
-  void *ps[] = {m->dens, m->tmp, m->vmask, m->cmask, m->vbase, m->sums, m->verts, m->tris};
+  void *ps[] = {m->dens, m->tmp, m->vmask, m->cmask, m->vbase, m->sums, m->verts, m->tris,
+                m->sm_buf};
   for (void *p : ps)
     if (p) cudaFree(p);
   if (m->tot_host) cudaFreeHost(m->tot_host);
@@ -665,6 +814,27 @@ int gf_mesher_copy(void *mesher, float *verts, int32_t *tris) {
                       "copy mesh triangles")))
     return e;
   return gfm::check(m, cudaStreamSynchronize(m->stream), "mesh copy sync");
+}
+
+int gf_mesher_smooth(void *mesher, float *verts, int64_t n_verts, const int32_t *tris,
+                     int64_t n_tris, int32_t method, int32_t passes, double lam, double mu) {
+  Mesher *m = reinterpret_cast<Mesher *>(mesher);
+  if (!m || passes < 0 || n_verts < 0 || n_tris < 0) return GF_INVALID_ARG;
+  if (method != GF_MESH_SMOOTH_LAPLACIAN && method != GF_MESH_SMOOTH_TAUBIN)
+    return gfm::fail(m, GF_INVALID_ARG, "gf_mesher_smooth: unknown smoothing method");
+  if (!verts) {  // the last extraction
+    if (m->nv < 0) return gfm::fail(m, GF_INVALID_ARG, "gf_mesher_smooth: no extraction");
+    verts = m->verts;
+    n_verts = m->nv;
+    tris = m->tris;
+    n_tris = m->nt;
+  } else if (n_tris > 0 && !tris) {
+    return GF_INVALID_ARG;
+  }
+  if (n_verts > INT32_MAX || 6 * n_tris > INT32_MAX)
+    return gfm::fail(m, GF_INVALID_ARG, "gf_mesher_smooth: mesh exceeds int32 indexing");
+  if (passes == 0 || n_verts == 0) return GF_OK;
+  return gfm::smooth(m, verts, n_verts, tris, n_tris, method, passes, lam, mu);
 }
 
 }  // extern "C"

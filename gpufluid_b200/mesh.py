@@ -12,9 +12,11 @@ are grid index * dx as there, and the axis-edge vertices are the ones
 marching cubes places, but each cube yields up to 12 triangles instead of up
 to 5.  Triangles face from density >= iso_level towards lower density.
 
-Options the reference delegates to absent third-party code are refused with
-ValueError: ``decimate_ratio < 1`` (pyfqmr), ``mesh_method="sdf"`` (Warp's
-HashGrid), ``mesh_smooth_passes > 0`` (a scipy sparse Laplacian).
+Mesh smoothing (``mesh_smooth_passes``, ``smooth_laplacian``, ``smooth_taubin``;
+src/gpufluid/meshing/smoothing.py) runs on the device in float64 with the
+reference's order of operations.  Options the reference delegates to absent
+third-party code are refused with ValueError: ``decimate_ratio < 1`` (pyfqmr)
+and ``mesh_method="sdf"`` (Warp's HashGrid).
 """
 from __future__ import annotations
 
@@ -101,11 +103,15 @@ class MeshExtractor:
                                               p.shape[0], ctypes.byref(prm)),
                     "gf_mesher_density")
 
-    def surface(self, iso_level: float, field: Optional[torch.Tensor] = None
+    def surface(self, iso_level: float, field: Optional[torch.Tensor] = None,
+                smooth_passes: int = 0, smooth_method: str = "taubin"
                 ) -> Tuple[Optional[np.ndarray], Optional[np.ndarray]]:
         """Iso-surface of the mesher's field (or of ``field``, a device
-        (nx, ny, nz) float32 tensor): (verts (N,3) float32, faces (M,3) int32)
-        on the host, or (None, None) when no surface crosses the grid."""
+        (nx, ny, nz) float32 tensor), smoothed on the device when
+        ``smooth_passes`` > 0: (verts (N,3) float32, faces (M,3) int32) on the
+        host, or (None, None) when no surface crosses the grid."""
+        if smooth_passes > 0 and smooth_method not in _lib.MESH_SMOOTH:
+            raise ValueError(f"unknown mesh_smooth_method: {smooth_method}")
         if field is not None:
             field = field.to(device=self.device, dtype=torch.float32).contiguous()
             if field.numel() != self.nx * self.ny * self.nz:
@@ -118,6 +124,12 @@ class MeshExtractor:
         self.n_verts, self.n_tris = int(nv.value), int(nt.value)
         if self.n_verts == 0:
             return None, None
+        if smooth_passes > 0:
+            lam, mu = (0.5, -0.53) if smooth_method == "taubin" else (0.5, 0.0)
+            self._check(self._L.gf_mesher_smooth(self._h, None, 0, None, 0,
+                                                 _lib.MESH_SMOOTH[smooth_method],
+                                                 int(smooth_passes), lam, mu),
+                        "gf_mesher_smooth")
         verts = np.empty((self.n_verts, 3), np.float32)
         faces = np.empty((self.n_tris, 3), np.int32)
         self._check(self._L.gf_mesher_copy(self._h, verts.ctypes.data, faces.ctypes.data),
@@ -132,15 +144,52 @@ class MeshExtractor:
                 ) -> Tuple[Optional[np.ndarray], Optional[np.ndarray]]:
         """Density splat + box blur + wall margin + iso-surface
         (surface.py:353-461).  (None, None) for no particles or no surface."""
-        if mesh_smooth_passes > 0:
-            raise ValueError("mesh_smooth_passes > 0 (Laplacian / Taubin mesh smoothing) "
-                             "is not part of this build")
         if decimate_ratio < 1.0:
             raise ValueError("decimate_ratio < 1 (quadric decimation) is not part of this build")
         if pos is None or _as_device_pos(pos, self.device).shape[0] == 0:
             return None, None
         self.density(pos, smooth_passes, wall_margin_cells, mesh_method, cubic_radius_cells)
-        return self.surface(iso_level)
+        return self.surface(iso_level, smooth_passes=mesh_smooth_passes,
+                            smooth_method=mesh_smooth_method)
+
+
+def _smooth(verts, faces, method: str, passes: int, lam: float, mu: float) -> np.ndarray:
+    if verts is None or len(verts) == 0 or passes <= 0:
+        return verts
+    faces = np.asarray(faces)
+    if faces.ndim != 2 or faces.shape[1] != 3 or len(faces) == 0:
+        raise ValueError("faces must be a non-empty (M,3) array")
+    if faces.min() < 0 or faces.max() >= len(verts):
+        raise ValueError("faces index a vertex outside verts")
+    L = _lib.load()
+    h = ctypes.c_void_p()
+    dev = torch.device("cuda")
+    _lib.check(L.gf_mesher_create(1, 1, 1, ctypes.c_float(1.0),
+                                  torch.cuda.current_stream(dev).cuda_stream, ctypes.byref(h)),
+               None, "gf_mesher_create")
+    try:
+        v = torch.from_numpy(np.ascontiguousarray(verts, dtype=np.float32)).to(dev)
+        f = torch.from_numpy(np.ascontiguousarray(faces, dtype=np.int32)).to(dev)
+        st = L.gf_mesher_smooth(h, v.data_ptr(), v.shape[0], f.data_ptr(), f.shape[0],
+                                _lib.MESH_SMOOTH[method], int(passes), float(lam), float(mu))
+        if st != _lib.GF_OK:
+            raw = L.gf_mesher_last_error(h)
+            raise _lib.GfError(st, f"gf_mesher_smooth: {raw.decode() if raw else ''}")
+        return v.cpu().numpy()
+    finally:
+        L.gf_mesher_destroy(h)
+
+
+def smooth_laplacian(verts: np.ndarray, faces: np.ndarray, passes: int = 1,
+                     lam: float = 0.5) -> np.ndarray:
+    """smoothing.py:40-52 on the device: smoothed float32 vertex positions."""
+    return _smooth(verts, faces, "laplacian", passes, lam, 0.0)
+
+
+def smooth_taubin(verts: np.ndarray, faces: np.ndarray, passes: int = 2, lam: float = 0.5,
+                  mu: float = -0.53) -> np.ndarray:
+    """smoothing.py:55-72 on the device: smoothed float32 vertex positions."""
+    return _smooth(verts, faces, "taubin", passes, lam, mu)
 
 
 def particles_to_mesh(pos, nx, ny, nz, dx, iso_level=0.5, smooth_passes=2, **_ignored):

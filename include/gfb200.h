@@ -269,6 +269,16 @@ int gf_mesher_extract(void *mesher, const float *field, float iso_level, int64_t
 /* Copy the last extraction out: verts (n_verts,3) float32, tris (n_tris,3)
  * int32, host or device memory.  Synchronising. */
 int gf_mesher_copy(void *mesher, float *verts, int32_t *tris);
+/* Uniform-Laplacian mesh smoothing (smoothing.py:22-72): `passes` steps of
+ * v += lam L v (GF_MESH_SMOOTH_LAPLACIAN) or pairs v += lam L v; v += mu L v
+ * (GF_MESH_SMOOTH_TAUBIN), L = D^-1 A - I of the triangles' 1-rings, in
+ * float64 and in the reference's order of operations, then rounded to float32
+ * in place.  verts/tris: device arrays, or verts = NULL for the mesher's last
+ * extraction (before gf_mesher_copy).  Asynchronous. */
+#define GF_MESH_SMOOTH_LAPLACIAN 0
+#define GF_MESH_SMOOTH_TAUBIN 1
+int gf_mesher_smooth(void *mesher, float *verts, int64_t n_verts, const int32_t *tris,
+                     int64_t n_tris, int32_t method, int32_t passes, double lam, double mu);
 
 /* ---- adjoint (differentiation through substeps) ------------------------- */
 /* No counterpart in the reference (planned only there).  PIC transfer

@@ -15,11 +15,15 @@ NumPy restatement of the reference's density field
   float32 sum of the in-grid 3x3x3 neighbours (di, dj, dk ascending) divided
   by their count;
 * ``zero_walls``      -- ``k_mc_zero_walls`` (:179-193);
-* ``density_field``   -- the order of ``MeshExtractor.extract`` (:388-425).
+* ``density_field``   -- the order of ``MeshExtractor.extract`` (:388-425);
+* ``smooth``          -- ``smooth_laplacian`` / ``smooth_taubin``
+  (meshing/smoothing.py:22-72).
 
 Parity pin: ``tests/golden/mesh/density.npz`` holds the reference kernels' own
-outputs run on the sequential Warp stand-in (``tests/golden/make_mesh_golden.py``);
-``tests/test_mesh.py`` checks this restatement against them.
+outputs run on the sequential Warp stand-in, and ``tests/golden/mesh/smoothing.npz``
+the reference's smoothing functions' outputs (NumPy + SciPy, run directly)
+(``tests/golden/make_mesh_golden.py``); ``tests/test_mesh.py`` checks this
+restatement against them.
 
 The iso-surface step of the reference is third-party code (scikit-image's
 ``marching_cubes`` below 64^3, Warp's ``MarchingCubes`` from 64^3,
@@ -233,6 +237,40 @@ def iso_surface(dens, iso, dx):
     tris = np.concatenate(tris)
     order = np.argsort(keys, kind="stable")
     return verts.astype(F32), tris[order].astype(np.int32)
+
+
+def smooth(verts, faces, method="taubin", passes=2, lam=0.5, mu=-0.53):
+    """``smooth_laplacian`` / ``smooth_taubin`` (src/gpufluid/meshing/
+    smoothing.py:22-72): L = D^-1 A - I of the distinct 1-ring neighbours
+    (D = #neighbours, 1 when none; 1/D rounded to float32 as the reference's
+    scipy matrices hold it), applied in float64 with each row's diagonal first
+    and then its neighbours in ascending order, a multiply and an add per
+    entry; v += lam L v per pass (Taubin adds v += mu L v); float32 at the end."""
+    v = np.asarray(verts, np.float32).astype(np.float64)
+    if len(v) == 0 or passes <= 0:
+        return np.asarray(verts, np.float32)
+    f = np.asarray(faces, np.int64)
+    e = np.concatenate([f[:, [0, 1]], f[:, [1, 0]], f[:, [1, 2]], f[:, [2, 1]],
+                        f[:, [2, 0]], f[:, [0, 2]]])
+    e = np.unique(e, axis=0)  # sorted by (row, col)
+    n = len(v)
+    deg = np.bincount(e[:, 0], minlength=n)
+    start = np.concatenate([[0], np.cumsum(deg)])
+    dinv = (np.float32(1.0) / np.maximum(deg, 1).astype(np.float32)).astype(np.float64)
+    maxd = int(deg.max()) if len(e) else 0
+    nbr = np.zeros((n, max(maxd, 1)), np.int64)
+    mask = np.zeros((n, max(maxd, 1)), bool)
+    for k in range(maxd):
+        has = deg > k
+        nbr[has, k] = e[start[:-1][has] + k, 1]
+        mask[has, k] = True
+    steps = [lam] * passes if method == "laplacian" else [c for _ in range(passes) for c in (lam, mu)]
+    for c in steps:
+        acc = 0.0 + (-1.0 * v)
+        for k in range(maxd):
+            acc = np.where(mask[:, k:k + 1], acc + dinv[:, None] * v[nbr[:, k]], acc)
+        v = v + c * acc
+    return v.astype(np.float32)
 
 
 def mesh_volume(verts, tris):

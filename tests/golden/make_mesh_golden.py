@@ -15,7 +15,10 @@ two reference modules unmodified.  The iso-surface step after them is a
 third-party routine there (scikit-image's or Warp's marching cubes, neither
 installed here) and is not recorded.
 
-Writes ``tests/golden/mesh/density.npz``.
+It also runs the reference's mesh smoothing (``meshing/smoothing.py``, NumPy +
+SciPy, imported as it is) on two marching-tetrahedra surfaces.
+
+Writes ``tests/golden/mesh/density.npz`` and ``tests/golden/mesh/smoothing.npz``.
 """
 from __future__ import annotations
 
@@ -89,6 +92,24 @@ def main():
     d = os.path.join(HERE, "mesh")
     os.makedirs(d, exist_ok=True)
     np.savez_compressed(os.path.join(d, "density.npz"), **out)
+
+    # mesh smoothing: the reference's functions (NumPy + SciPy) on the
+    # marching-tetrahedra surfaces of two fields, one closed and one open
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from oracle import mesh as om
+    from gpufluid.meshing.smoothing import smooth_laplacian, smooth_taubin
+    import scipy
+    sm = {"scipy_version": np.array(scipy.__version__)}
+    n = 20
+    i, j, k = np.meshgrid(*[np.arange(n)] * 3, indexing="ij")
+    fields = [(6.3 - np.sqrt((i - 9.4) ** 2 + (j - 10.1) ** 2 + (k - 8.7) ** 2)).astype(np.float32),
+              (np.sin(i / 3.0) + np.cos(j / 4.0) - k / 10.0).astype(np.float32)]
+    for c, f in enumerate(fields):
+        v, t = om.iso_surface(f, 0.0, 1.0 / n)
+        sm[f"verts_{c}"], sm[f"faces_{c}"] = v, t
+        sm[f"taubin_{c}"] = smooth_taubin(v, t, passes=2)
+        sm[f"laplacian_{c}"] = smooth_laplacian(v, t, passes=3, lam=0.4)
+    np.savez_compressed(os.path.join(d, "smoothing.npz"), **sm)
     print({k: (v.shape, float(v.max())) for k, v in out.items() if k.startswith("density")})
 
 

@@ -116,7 +116,8 @@ def test_out_of_scope_rejected(tmp_path, extra, what):
     assert what in str(ei.value)
 
 
-@pytest.mark.parametrize("key", ['mesh_method = "sdf"', "mesh_smooth_passes = 2",
+@pytest.mark.parametrize("key", ['mesh_method = "sdf"',
+                                 'mesh_smooth_method = "cotan"\nmesh_smooth_passes = 2',
                                  "decimate_ratio = 0.5"])
 def test_mesh_options_outside_build_rejected(tmp_path, key):
     cfg = _write_minimal(tmp_path)

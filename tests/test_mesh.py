@@ -129,7 +129,9 @@ def test_mesh_options_outside_build_are_refused():
     check_mesh_options(OutputCfg())
     check_mesh_options(OutputCfg(mesh_method="cubic"))
     check_mesh_options(OutputCfg(mesh=False, mesh_method="sdf"))
-    for kw in (dict(mesh_method="sdf"), dict(mesh_smooth_passes=2), dict(decimate_ratio=0.5)):
+    check_mesh_options(OutputCfg(mesh_smooth_passes=2))
+    for kw in (dict(mesh_method="sdf"), dict(mesh_smooth_passes=2, mesh_smooth_method="cotan"),
+               dict(decimate_ratio=0.5)):
         with pytest.raises(BlockError) as e:
             check_mesh_options(OutputCfg(**kw))
         assert e.value.block_id == "C7.1"
@@ -256,7 +258,14 @@ def test_extract_on_solver_particles(gf):
     with pytest.raises(ValueError):
         ex.extract(pos, mesh_method="sdf")
     with pytest.raises(ValueError):
-        ex.extract(pos, mesh_smooth_passes=1)
+        ex.extract(pos, mesh_smooth_passes=1, mesh_smooth_method="cotan")
+    # Taubin smoothing on the device after extraction equals the oracle's
+    # smoothing of the unsmoothed surface
+    vs, ts = ex.extract(s.pos, iso_level=0.6, smooth_passes=2, wall_margin_cells=1,
+                        mesh_smooth_passes=2)
+    d2 = ex.dens.cpu().numpy()
+    ov, ot = om.iso_surface(d2, 0.6, s.dx)
+    assert np.array_equal(ts, ot) and np.array_equal(vs, om.smooth(ov, ot, "taubin", 2))
     with pytest.raises(ValueError):
         ex.extract(pos, decimate_ratio=0.5)
     vc, tc = ex.extract(s.pos, iso_level=3.0, mesh_method="cubic", cubic_radius_cells=2.0)
@@ -266,6 +275,34 @@ def test_extract_on_solver_particles(gf):
     ov, ot = om.iso_surface(dc, 3.0, s.dx)
     assert np.array_equal(vc, ov) and np.array_equal(tc, ot)
     assert ex.launches > 0
+
+
+def test_oracle_smoothing_matches_reference():
+    g = dict(np.load(os.path.join(os.path.dirname(GOLD), "smoothing.npz")))
+    for c in (0, 1):
+        v, t = g[f"verts_{c}"], g[f"faces_{c}"]
+        assert np.array_equal(om.smooth(v, t, "taubin", 2), g[f"taubin_{c}"])
+        assert np.array_equal(om.smooth(v, t, "laplacian", 3, 0.4), g[f"laplacian_{c}"])
+
+
+@pytest.mark.gpu
+def test_smoothing_matches_reference(gf):
+    """smoothing.py's functions, bit for bit: the device runs the float64
+    Laplacian in the reference's order of operations."""
+    from gpufluid_b200.mesh import smooth_laplacian, smooth_taubin
+    g = dict(np.load(os.path.join(os.path.dirname(GOLD), "smoothing.npz")))
+    for c in (0, 1):
+        v, t = g[f"verts_{c}"], g[f"faces_{c}"]
+        assert np.array_equal(smooth_taubin(v, t, passes=2), g[f"taubin_{c}"])
+        assert np.array_equal(smooth_laplacian(v, t, passes=3, lam=0.4), g[f"laplacian_{c}"])
+    # isolated vertices and a larger mesh
+    v = np.concatenate([g["verts_0"], np.float32([[9.0, 9.0, 9.0]])])
+    assert np.array_equal(smooth_laplacian(v, g["faces_0"], passes=2),
+                          om.smooth(v, g["faces_0"], "laplacian", 2))
+    f = _sphere(96, (47.3, 45.9, 48.2), 30.5)
+    ov, ot = om.iso_surface(f, 0.0, 1.0 / 96)
+    assert np.array_equal(smooth_taubin(ov, ot, passes=3), om.smooth(ov, ot, "taubin", 3))
+    assert smooth_taubin(np.zeros((0, 3), np.float32), np.zeros((0, 3), np.int32)).shape == (0, 3)
 
 
 @pytest.mark.gpu
