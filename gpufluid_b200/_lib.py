@@ -86,15 +86,17 @@ class TuneInfo(ctypes.Structure):
                 ("step_ms_before", ctypes.c_float), ("step_ms_after", ctypes.c_float)]
 
 
-GF_MESH_TRILINEAR, GF_MESH_CUBIC = 0, 1
-MESH_METHOD = {"trilinear": GF_MESH_TRILINEAR, "cubic": GF_MESH_CUBIC}
+GF_MESH_TRILINEAR, GF_MESH_CUBIC, GF_MESH_SDF = 0, 1, 2
+MESH_METHOD = {"trilinear": GF_MESH_TRILINEAR, "cubic": GF_MESH_CUBIC, "sdf": GF_MESH_SDF}
 GF_MESH_SMOOTH_LAPLACIAN, GF_MESH_SMOOTH_TAUBIN = 0, 1
 MESH_SMOOTH = {"laplacian": GF_MESH_SMOOTH_LAPLACIAN, "taubin": GF_MESH_SMOOTH_TAUBIN}
 
 
 class MeshParams(ctypes.Structure):
     _fields_ = [("method", ctypes.c_int32), ("smooth_passes", ctypes.c_int32),
-                ("wall_margin_cells", ctypes.c_int32), ("cubic_radius_cells", ctypes.c_float)]
+                ("wall_margin_cells", ctypes.c_int32), ("cubic_radius_cells", ctypes.c_float),
+                ("sdf_particle_radius_cells", ctypes.c_float),
+                ("sdf_search_radius_cells", ctypes.c_float)]
 
 
 _SIGS = {
@@ -165,6 +167,7 @@ _SIGS = {
                            ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
     "gf_mesher_copy": ([_vp, _vp, _vp], ctypes.c_int),
     "gf_mesher_copy_field": ([_vp, _vp], ctypes.c_int),
+    "gf_mesher_set_inside_below": ([_vp, ctypes.c_int32], ctypes.c_int),
     "gf_mesher_smooth": ([_vp, _vp, ctypes.c_int64, _vp, ctypes.c_int64, ctypes.c_int32,
                           ctypes.c_int32, ctypes.c_double, ctypes.c_double], ctypes.c_int),
 }

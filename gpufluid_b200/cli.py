@@ -13,8 +13,8 @@ FLIP/PIC/APIC scene:
   and, with --timings, timings.json;
 - it returns 2 on divergence or a configuration error, else 0.
 
-Mesh options whose reference implementation is third-party code (decimation
-via pyfqmr, the Warp-HashGrid "sdf" method) are refused with BlockError("C7.1").
+Mesh decimation (pyfqmr in the reference: third-party code) is refused with
+BlockError("C7.1").
 ``bench`` runs the reference's fixed throughput table (commands.py:953-977)
 with device-synchronised timing.
 """
@@ -67,9 +67,9 @@ def check_mesh_options(out):
     """Refuse the [output] mesh options outside this build (C7.1)."""
     if not out.mesh:
         return
-    if out.mesh_method not in ("trilinear", "cubic"):
-        raise BlockError("C7.1", f"output.mesh_method {out.mesh_method!r} is not part of this "
-                                 "build (trilinear, cubic)")
+    if out.mesh_method not in ("trilinear", "cubic", "sdf"):
+        raise BlockError("C7.1", f"output.mesh_method {out.mesh_method!r}: expected "
+                                 "'trilinear', 'cubic' or 'sdf'")
     if out.mesh_smooth_passes > 0 and out.mesh_smooth_method not in ("taubin", "laplacian"):
         raise BlockError("C7.1", f"output.mesh_smooth_method {out.mesh_smooth_method!r}: "
                                  "expected 'taubin' or 'laplacian'")
@@ -205,7 +205,9 @@ def cmd_simulate(args) -> int:
                 smooth_passes=out.smooth_passes, mesh_smooth_passes=out.mesh_smooth_passes,
                 mesh_smooth_method=out.mesh_smooth_method,
                 wall_margin_cells=out.wall_margin_cells, decimate_ratio=out.decimate_ratio,
-                mesh_method=out.mesh_method, cubic_radius_cells=out.cubic_radius_cells)
+                mesh_method=out.mesh_method, cubic_radius_cells=out.cubic_radius_cells,
+                sdf_particle_radius_cells=out.sdf_particle_radius_cells,
+                sdf_search_radius_cells=out.sdf_search_radius_cells)
             t_mesh += time.time() - tm
             if verts is not None:
                 write_ply(mesh_dir / f"frame_{frame:04d}.ply", verts, faces)

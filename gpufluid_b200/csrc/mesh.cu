@@ -13,6 +13,8 @@
 //                                  last pass also zeroes the wall margin
 //   k_mesh_walls                   (k_mc_zero_walls, surface.py:179-193) when
 //                                  there is no blur pass to fold it into
+//   k_sdf_init/_scatter/_finish    or the signed distance to the nearest
+//                                  particle (k_sdf_field, surface.py:100-122)
 // The splats add with float atomics in arrival order (as the reference's
 // wp.atomic_add); blur and margin are per-cell and follow the reference's
 // float32 operation order exactly.
@@ -65,6 +67,7 @@ struct Mesher {
   int32_t *tris = nullptr;
   int64_t tris_cap = 0;
   int64_t nv = -1, nt = -1;    // counts of the last extraction
+  int below = 0;               // 1: the surface encloses field <= iso (signed distances)
   int64_t launches = 0;
   // mesh smoothing scratch, grown on use
   void *sm_buf = nullptr;
@@ -184,6 +187,51 @@ __global__ void k_mesh_walls(float *d, int nx, int ny, int nz, int margin) {
   if (in_margin(i, j, k, nx, ny, nz, margin)) d[c] = 0.f;
 }
 
+// k_sdf_field (surface.py:100-122): phi = sqrt(min(R^2, nearest d^2)) - r over
+// the cell centres; the reference asks a hash grid for every cell's
+// candidates, here every particle lowers the squared distance of the cells
+// around it (an atomic minimum on the float's bits, which order like the
+// non-negative floats).  d = centre - p, d^2 = (dx dx + dy dy) + dz dz.
+__global__ void k_sdf_init(unsigned *bits, int64_t n, float r2) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) bits[i] = __float_as_uint(r2);
+}
+
+__global__ void k_sdf_scatter(const float *__restrict__ pos, int64_t n, float dx, float R,
+                              float r2, int nx, int ny, int nz, unsigned *bits) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const float p[3] = {pos[3 * q], pos[3 * q + 1], pos[3 * q + 2]};
+  const int dims[3] = {nx, ny, nz};
+  int lo[3], hi[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {  // cells whose centre may lie within R, one cell of margin
+    lo[a] = max(0, __float2int_rd(__fdiv_rn(p[a] - R, dx) - 0.5f) - 1);
+    hi[a] = min(dims[a] - 1, __float2int_rd(__fdiv_rn(p[a] + R, dx) - 0.5f) + 1);
+  }
+  for (int i = lo[0]; i <= hi[0]; ++i) {
+    const float ddx = ((float)i + 0.5f) * dx - p[0];
+    for (int j = lo[1]; j <= hi[1]; ++j) {
+      const float ddy = ((float)j + 0.5f) * dx - p[1];
+      const float sxy = ddx * ddx + ddy * ddy;
+      if (!(sxy < r2)) continue;
+      for (int k = lo[2]; k <= hi[2]; ++k) {
+        const float ddz = ((float)k + 0.5f) * dx - p[2];
+        const float d2 = sxy + ddz * ddz;
+        if (!(d2 < r2)) continue;
+        unsigned *b = bits + ((int64_t)i * ny + j) * nz + k;
+        const unsigned v = __float_as_uint(d2);
+        if (v < *b) atomicMin(b, v);
+      }
+    }
+  }
+}
+
+__global__ void k_sdf_finish(float *phi, int64_t n, float r) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) phi[i] = __fsqrt_rn(phi[i]) - r;  // phi holds the minimum's bits
+}
+
 // ---- iso-surface -----------------------------------------------------------
 // Corner b of a cube (bit 0: +x, bit 1: +y, bit 2: +z) sits at node
 // n + off(b).  Edge family b (1..7) of a node joins it to n + off(b).
@@ -257,6 +305,7 @@ __device__ __forceinline__ int block_prefix(int v, int *total) {
 struct ExtractArgs {
   const float *dens;
   float iso;
+  int below;  // inside = value <= iso instead of >= iso
   int nx, ny, nz;
   int64_t nnode;
   float dx;
@@ -275,12 +324,13 @@ __global__ void __launch_bounds__(MB) k_mesh_count(ExtractArgs a) {
     const NodeIdx p = node_of(n, a.ny, a.nz);
     const bool hx = p.i + 1 < a.nx, hy = p.j + 1 < a.ny, hz = p.k + 1 < a.nz;
     const float v0 = a.dens[n];
-    const int in0 = v0 >= a.iso;
+    const int in0 = a.below ? v0 <= a.iso : v0 >= a.iso;
     cm = in0;
 #pragma unroll
     for (int b = 1; b < 8; ++b) {
       if ((b & 1 && !hx) || (b & 2 && !hy) || (b & 4 && !hz)) continue;
-      const int in = a.dens[n + off_of(b, a.ny, a.nz)] >= a.iso;
+      const float vb = a.dens[n + off_of(b, a.ny, a.nz)];
+      const int in = a.below ? vb <= a.iso : vb >= a.iso;
       cm |= in << b;
       vm |= (in != in0) << b;
     }
@@ -714,12 +764,41 @@ int gf_mesher_density(void *mesher, const float *pos, int64_t n,
   if (!m || !prm || n < 0 || (n > 0 && !pos)) return GF_INVALID_ARG;
   if (prm->smooth_passes < 0 || prm->wall_margin_cells < 0)
     return gfm::fail(m, GF_INVALID_ARG, "gf_mesher_density: negative pass count or margin");
-  if (prm->method != GF_MESH_TRILINEAR && prm->method != GF_MESH_CUBIC)
+  if (prm->method != GF_MESH_TRILINEAR && prm->method != GF_MESH_CUBIC &&
+      prm->method != GF_MESH_SDF)
     return gfm::fail(m, GF_INVALID_ARG, "gf_mesher_density: unknown mesh method");
   if (prm->method == GF_MESH_CUBIC && !(prm->cubic_radius_cells > 0.f))
     return gfm::fail(m, GF_INVALID_ARG, "gf_mesher_density: cubic radius must be > 0");
+  if (prm->method == GF_MESH_SDF &&
+      !(prm->sdf_search_radius_cells > 0.f && prm->sdf_particle_radius_cells >= 0.f))
+    return gfm::fail(m, GF_INVALID_ARG, "gf_mesher_density: bad sdf radii");
   cudaStream_t st = m->stream;
   const unsigned gc = (unsigned)((m->nnode + 255) / 256);
+  if (prm->method == GF_MESH_SDF) {
+    // surface.py:405-420: radii in cells times dx (double), passed as float;
+    // no wall margin (a zeroed wall would be a false surface)
+    const float R = (float)((double)prm->sdf_search_radius_cells * (double)m->dx);
+    const float r = (float)((double)prm->sdf_particle_radius_cells * (double)m->dx);
+    const float r2 = R * R;
+    unsigned *bits = reinterpret_cast<unsigned *>(m->dens);
+    gfm::k_sdf_init<<<gc, 256, 0, st>>>(bits, m->nnode, r2);
+    if (n > 0)
+      gfm::k_sdf_scatter<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(
+          pos, n, m->dx, R, r2, m->nx, m->ny, m->nz, bits);
+    gfm::k_sdf_finish<<<gc, 256, 0, st>>>(m->dens, m->nnode, r);
+    m->launches += n > 0 ? 3 : 2;
+    for (int p = 0; p < prm->smooth_passes; ++p) {
+      gfm::k_mesh_blur<<<gc, 256, 0, st>>>(m->dens, m->tmp, m->nx, m->ny, m->nz, 0);
+      float *t = m->dens;
+      m->dens = m->tmp;
+      m->tmp = t;
+      m->launches++;
+    }
+    m->below = 1;
+    m->nv = m->nt = -1;
+    return gfm::check(m, cudaGetLastError(), "gf_mesher_density");
+  }
+  m->below = 0;
   gfm::k_mesh_zero<<<gc, 256, 0, st>>>(m->dens, m->nnode);
   m->launches++;
   if (n > 0) {
@@ -762,7 +841,8 @@ int gf_mesher_extract(void *mesher, const float *field, float iso_level, int64_t
     return GF_OK;
   }
   cudaStream_t st = m->stream;
-  gfm::ExtractArgs a{field ? field : m->dens, iso_level, m->nx, m->ny, m->nz, m->nnode, m->dx,
+  gfm::ExtractArgs a{field ? field : m->dens, iso_level, m->below, m->nx, m->ny, m->nz, m->nnode,
+                     m->dx,
                      m->vmask, m->cmask, m->vbase, m->sums, m->nb, nullptr, nullptr};
   gfm::k_mesh_count<<<m->nb, gfm::MB, 0, st>>>(a);
   gfm::k_mesh_scan<<<2, gfm::SCAN_T, 0, st>>>(m->sums, m->nb);
@@ -795,6 +875,13 @@ int gf_mesher_extract(void *mesher, const float *field, float iso_level, int64_t
   *n_verts = nv;
   *n_tris = nt;
   return gfm::check(m, cudaGetLastError(), "gf_mesher_extract emit");
+}
+
+int gf_mesher_set_inside_below(void *mesher, int32_t below) {
+  Mesher *m = reinterpret_cast<Mesher *>(mesher);
+  if (!m) return GF_INVALID_ARG;
+  m->below = below ? 1 : 0;
+  return GF_OK;
 }
 
 int gf_mesher_copy(void *mesher, float *verts, int32_t *tris) {

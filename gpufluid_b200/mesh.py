@@ -14,9 +14,9 @@ to 5.  Triangles face from density >= iso_level towards lower density.
 
 Mesh smoothing (``mesh_smooth_passes``, ``smooth_laplacian``, ``smooth_taubin``;
 src/gpufluid/meshing/smoothing.py) runs on the device in float64 with the
-reference's order of operations.  Options the reference delegates to absent
-third-party code are refused with ValueError: ``decimate_ratio < 1`` (pyfqmr)
-and ``mesh_method="sdf"`` (Warp's HashGrid).
+reference's order of operations, and the "sdf" method's nearest-particle
+distance (the reference's hash-grid query) as an atomic minimum per cell.
+``decimate_ratio < 1`` (pyfqmr, third-party) is refused with ValueError.
 """
 from __future__ import annotations
 
@@ -30,7 +30,7 @@ import torch
 from . import _lib
 from .config import BlockError
 
-MESH_METHODS = ("trilinear", "cubic")
+MESH_METHODS = ("trilinear", "cubic", "sdf")
 
 
 def _as_device_pos(pos, device) -> torch.Tensor:
@@ -90,26 +90,36 @@ class MeshExtractor:
         return out.view(self.nx, self.ny, self.nz)
 
     def density(self, pos, smooth_passes: int = 2, wall_margin_cells: int = 0,
-                mesh_method: str = "trilinear", cubic_radius_cells: float = 2.0) -> None:
-        """Build the density field (surface.py:388-425) on the device."""
+                mesh_method: str = "trilinear", cubic_radius_cells: float = 2.0,
+                sdf_particle_radius_cells: float = 1.0,
+                sdf_search_radius_cells: float = 4.0) -> None:
+        """Build the density field (surface.py:388-425) on the device; for
+        ``mesh_method="sdf"`` the blurred signed distance to the particles,
+        whose surface is its zero level (inside below it)."""
         if mesh_method not in MESH_METHODS:
-            raise ValueError(f"unknown mesh_method: {mesh_method!r}; expected one of "
-                             f"{MESH_METHODS} (the 'sdf' method is not part of this build)")
+            raise ValueError(f"unknown mesh_method: {mesh_method!r}; expected 'trilinear', "
+                             "'cubic', or 'sdf'")
         p = _as_device_pos(pos, self.device)
         prm = _lib.MeshParams(_lib.MESH_METHOD[mesh_method], int(smooth_passes),
-                              int(wall_margin_cells), float(cubic_radius_cells))
+                              int(wall_margin_cells), float(cubic_radius_cells),
+                              float(sdf_particle_radius_cells), float(sdf_search_radius_cells))
         self._stream()
         self._check(self._L.gf_mesher_density(self._h, p.data_ptr() if p.numel() else None,
                                               p.shape[0], ctypes.byref(prm)),
                     "gf_mesher_density")
 
     def surface(self, iso_level: float, field: Optional[torch.Tensor] = None,
-                smooth_passes: int = 0, smooth_method: str = "taubin"
+                smooth_passes: int = 0, smooth_method: str = "taubin",
+                inside_below: Optional[bool] = None
                 ) -> Tuple[Optional[np.ndarray], Optional[np.ndarray]]:
         """Iso-surface of the mesher's field (or of ``field``, a device
         (nx, ny, nz) float32 tensor), smoothed on the device when
         ``smooth_passes`` > 0: (verts (N,3) float32, faces (M,3) int32) on the
-        host, or (None, None) when no surface crosses the grid."""
+        host, or (None, None) when no surface crosses the grid.  The inside is
+        the field >= iso_level, or <= iso_level after an "sdf" field or with
+        ``inside_below=True``."""
+        if inside_below is not None:
+            self._L.gf_mesher_set_inside_below(self._h, 1 if inside_below else 0)
         if smooth_passes > 0 and smooth_method not in _lib.MESH_SMOOTH:
             raise ValueError(f"unknown mesh_smooth_method: {smooth_method}")
         if field is not None:
@@ -148,8 +158,11 @@ class MeshExtractor:
             raise ValueError("decimate_ratio < 1 (quadric decimation) is not part of this build")
         if pos is None or _as_device_pos(pos, self.device).shape[0] == 0:
             return None, None
-        self.density(pos, smooth_passes, wall_margin_cells, mesh_method, cubic_radius_cells)
-        return self.surface(iso_level, smooth_passes=mesh_smooth_passes,
+        self.density(pos, smooth_passes, wall_margin_cells, mesh_method, cubic_radius_cells,
+                     sdf_particle_radius_cells, sdf_search_radius_cells)
+        # the sdf method's surface is the zero level (surface.py:428-430)
+        level = 0.0 if mesh_method == "sdf" else iso_level
+        return self.surface(level, smooth_passes=mesh_smooth_passes,
                             smooth_method=mesh_smooth_method)
 
 

@@ -234,11 +234,15 @@ int gf_reseed_emit(void *ctx, const uint8_t *label, const int32_t *counts, int32
  * positions (device (n,3) float32) of any solver. */
 #define GF_MESH_TRILINEAR 0 /* k_density_scatter, surface.py:14-43 */
 #define GF_MESH_CUBIC 1     /* k_cubic_scatter, surface.py:53-84 */
+#define GF_MESH_SDF 2       /* k_sdf_field, surface.py:100-122 (surface at phi <= 0) */
 typedef struct gf_mesh_params {
-  int32_t method;             /* GF_MESH_TRILINEAR | GF_MESH_CUBIC */
+  int32_t method;             /* GF_MESH_TRILINEAR | GF_MESH_CUBIC | GF_MESH_SDF */
   int32_t smooth_passes;      /* k_box_blur_3d passes (gridmath.py:103-121) */
-  int32_t wall_margin_cells;  /* k_mc_zero_walls margin (surface.py:179-193); 0 = off */
+  int32_t wall_margin_cells;  /* k_mc_zero_walls margin (surface.py:179-193); 0 = off;
+                                 ignored by GF_MESH_SDF, as in the reference */
   float cubic_radius_cells;   /* GF_MESH_CUBIC support radius in cells */
+  float sdf_particle_radius_cells; /* GF_MESH_SDF particle radius in cells */
+  float sdf_search_radius_cells;   /* GF_MESH_SDF search radius in cells */
 } gf_mesh_params;
 int gf_mesher_create(int32_t nx, int32_t ny, int32_t nz, float dx, void *cuda_stream,
                      void **mesher_out);
@@ -266,6 +270,10 @@ int gf_mesher_density(void *mesher, const float *pos, int64_t n, const gf_mesh_p
  * for the counts. */
 int gf_mesher_extract(void *mesher, const float *field, float iso_level, int64_t *n_verts,
                       int64_t *n_tris);
+/* Which side of the level is inside for the next gf_mesher_extract: 0 (the
+ * default after a GF_MESH_TRILINEAR / GF_MESH_CUBIC field) encloses
+ * values >= iso, 1 (set by a GF_MESH_SDF field) values <= iso. */
+int gf_mesher_set_inside_below(void *mesher, int32_t below);
 /* Copy the last extraction out: verts (n_verts,3) float32, tris (n_tris,3)
  * int32, host or device memory.  Synchronising. */
 int gf_mesher_copy(void *mesher, float *verts, int32_t *tris);

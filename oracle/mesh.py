@@ -15,6 +15,7 @@ NumPy restatement of the reference's density field
   float32 sum of the in-grid 3x3x3 neighbours (di, dj, dk ascending) divided
   by their count;
 * ``zero_walls``      -- ``k_mc_zero_walls`` (:179-193);
+* ``sdf_field``       -- ``k_sdf_field`` (:100-122) with the host radii;
 * ``density_field``   -- the order of ``MeshExtractor.extract`` (:388-425);
 * ``smooth``          -- ``smooth_laplacian`` / ``smooth_taubin``
   (meshing/smoothing.py:22-72).
@@ -128,12 +129,45 @@ def zero_walls(d, margin):
     return d
 
 
+def sdf_field(pos, shape, dx, particle_radius_cells=1.0, search_radius_cells=4.0):
+    """``k_sdf_field`` (:100-122) with the host's radii (:405-420): phi =
+    sqrt(min(R^2, d^2 to the nearest particle)) - r at the cell centres, d =
+    centre - p, d^2 = (dx dx + dy dy) + dz dz in float32."""
+    nx, ny, nz = shape
+    R = F32(float(search_radius_cells) * float(dx))
+    r = F32(float(particle_radius_cells) * float(dx))
+    r2 = R * R
+    best = np.full(shape, r2, F32)
+    dx32 = F32(dx)
+    rc = int(math.ceil(float(R) / float(dx))) + 2
+    for p in np.asarray(pos, F32):
+        c = np.floor(p / dx32).astype(np.int64)
+        lo = np.maximum(0, c - rc)
+        hi = np.minimum([nx, ny, nz], c + rc + 1)
+        if (hi <= lo).any():
+            continue
+        ddx = (np.arange(lo[0], hi[0]).astype(F32) + F32(0.5)) * dx32 - p[0]
+        ddy = (np.arange(lo[1], hi[1]).astype(F32) + F32(0.5)) * dx32 - p[1]
+        ddz = (np.arange(lo[2], hi[2]).astype(F32) + F32(0.5)) * dx32 - p[2]
+        d2 = (ddx[:, None, None] * ddx[:, None, None] + ddy[None, :, None] * ddy[None, :, None]
+              ) + ddz[None, None, :] * ddz[None, None, :]
+        blk = best[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]]
+        np.minimum(blk, d2, out=blk)
+    return (np.sqrt(best) - r).astype(F32)
+
+
 def density_field(pos, shape, dx, smooth_passes=2, wall_margin_cells=0,
-                  mesh_method="trilinear", cubic_radius_cells=2.0):
+                  mesh_method="trilinear", cubic_radius_cells=2.0,
+                  sdf_particle_radius_cells=1.0, sdf_search_radius_cells=4.0):
     if mesh_method == "trilinear":
         d = splat_trilinear(pos, shape, dx)
     elif mesh_method == "cubic":
         d = splat_cubic(pos, shape, dx, cubic_radius_cells)
+    elif mesh_method == "sdf":
+        d = sdf_field(pos, shape, dx, sdf_particle_radius_cells, sdf_search_radius_cells)
+        for _ in range(smooth_passes):
+            d = box_blur(d)
+        return d  # no wall margin for signed distances (surface.py:422-425)
     else:
         raise ValueError(mesh_method)
     for _ in range(smooth_passes):
@@ -155,15 +189,16 @@ def _det(a, b, c):
     return int(np.dot(a, np.cross(b, c)))
 
 
-def iso_surface(dens, iso, dx):
-    """(verts (V,3) float32, tris (T,3) int32) of {dens >= iso}; vertices
-    ordered by (node, edge family 1..7), triangles by (cube, tet, triangle)."""
+def iso_surface(dens, iso, dx, below=False):
+    """(verts (V,3) float32, tris (T,3) int32) of {dens >= iso} ({dens <= iso}
+    with ``below``); vertices ordered by (node, edge family 1..7), triangles by
+    (cube, tet, triangle)."""
     d = np.asarray(dens, F32)
     nx, ny, nz = d.shape
     if nx < 2 or ny < 2 or nz < 2:  # no cube: no surface
         return np.zeros((0, 3), F32), np.zeros((0, 3), np.int32)
     iso32, dx32 = F32(iso), F32(dx)
-    inside = d >= iso32
+    inside = d <= iso32 if below else d >= iso32
     cross = np.zeros((nx, ny, nz, 8), bool)
     vpos = np.zeros((nx, ny, nz, 8, 3), F32)
     gi, gj, gk = np.meshgrid(np.arange(nx, dtype=F32), np.arange(ny, dtype=F32),

@@ -1,9 +1,10 @@
 """Generate golden vectors for the mesh density field from the reference's
 own kernels (src/gpufluid/meshing/surface.py:14-43 k_density_scatter, :53-84
-k_cubic_scatter, src/gpufluid/primitives/gridmath.py:103-121 k_box_blur_3d,
-surface.py:179-193 k_mc_zero_walls), run in the order of
-``MeshExtractor.extract`` (:353-425) for mesh_method "trilinear" and
-"cubic".
+k_cubic_scatter, :100-122 k_sdf_field, src/gpufluid/primitives/gridmath.py:
+103-121 k_box_blur_3d, surface.py:179-193 k_mc_zero_walls), run in the order of
+``MeshExtractor.extract`` (:353-425) for mesh_method "trilinear", "cubic" and
+"sdf" (the stand-in's hash-grid query returns every point, a superset of the
+points within the radius, which is all Warp's query promises).
 
 Test-fixture generator (run by hand, in a container that holds the reference
 checkout; nothing at test or bench time reads the reference):
@@ -35,6 +36,8 @@ DX = 1.0 / 16.0
 # (mesh_method, smooth_passes, wall_margin_cells, cubic_radius_cells)
 CASES = [("trilinear", 2, 0, 0.0), ("trilinear", 1, 2, 0.0), ("trilinear", 0, 0, 0.0),
          ("cubic", 1, 0, 2.0), ("cubic", 0, 1, 1.5)]
+# (smooth_passes, sdf_particle_radius_cells, sdf_search_radius_cells)
+SDF_CASES = [(0, 1.0, 4.0), (2, 1.5, 3.0)]
 
 
 def particles():
@@ -64,7 +67,8 @@ def main():
     sys.modules.setdefault("skimage", skimage)
     sys.modules.setdefault("skimage.measure", skimage.measure)
     from gpufluid.primitives.gridmath import k_box_blur_3d
-    from gpufluid.meshing.surface import k_cubic_scatter, k_density_scatter, k_mc_zero_walls
+    from gpufluid.meshing.surface import (k_cubic_scatter, k_density_scatter, k_mc_zero_walls,
+                                          k_sdf_field)
 
     pos = particles()
     out = {"pos": pos, "dx": DX}
@@ -89,6 +93,27 @@ def main():
             wp.launch(k_mc_zero_walls, dim=(NX, NY, NZ), inputs=[a, int(margin)])
         out[f"density_{c}"] = np.asarray(a.numpy(), np.float32)
         out[f"case_{c}"] = np.array([method == "cubic", passes, margin, radius], np.float64)
+    # mesh_method "sdf" (surface.py:405-420): phi = sqrt(min(R^2, nearest d^2)) - r
+    # on a subset of the particles, then the blur (no wall margin for sdf)
+    sub = pos[::4]
+    out["sdf_pos"] = sub
+    for c, (passes, r_cells, s_cells) in enumerate(SDF_CASES):
+        search_r_world = float(s_cells) * DX
+        particle_r_world = float(r_cells) * DX
+        phi = wp.zeros((NX, NY, NZ), dtype=float)
+        tmp = wp.zeros((NX, NY, NZ), dtype=float)
+        phi.fill_(search_r_world)
+        grid = wp.HashGrid(64, 64, 64)
+        pw = wp.array(sub, dtype=wp.vec3)
+        grid.build(pw, search_r_world)
+        wp.launch(k_sdf_field, dim=(NX, NY, NZ),
+                  inputs=[grid.id, pw, phi, DX, NX, NY, NZ, search_r_world, particle_r_world])
+        a, b = phi, tmp
+        for _ in range(passes):
+            wp.launch(k_box_blur_3d, dim=(NX, NY, NZ), inputs=[a, b])
+            a, b = b, a
+        out[f"sdf_{c}"] = np.asarray(a.numpy(), np.float32)
+        out[f"sdf_case_{c}"] = np.array([passes, r_cells, s_cells], np.float64)
     d = os.path.join(HERE, "mesh")
     os.makedirs(d, exist_ok=True)
     np.savez_compressed(os.path.join(d, "density.npz"), **out)

@@ -251,6 +251,31 @@ def sqrt(x):
     return np.sqrt(_F32(x))
 
 
+def dot(a, b):
+    return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]
+
+
+_GRIDS = {}
+
+
+class HashGrid:
+    """Point grid for neighbour queries (only what a query returns matters)."""
+
+    def __init__(self, dim_x=1, dim_y=1, dim_z=1, device=None):
+        self.id = len(_GRIDS) + 1
+        self.points = np.zeros((0, 3), _F32)
+        _GRIDS[self.id] = self
+
+    def build(self, points, radius):
+        self.points = np.asarray(points, dtype=_F32).reshape(-1, 3)
+
+
+def hash_grid_query(grid_id, point, radius):
+    """Every point of the grid: a superset of the points within ``radius``,
+    which is all a Warp hash-grid query promises (callers test distances)."""
+    return range(len(_GRIDS[int(grid_id)].points))
+
+
 def atomic_add(arr, *idx_val):
     """Adds and returns the value before the add (Warp's atomic_add)."""
     *idx, val = idx_val

@@ -116,7 +116,7 @@ def test_out_of_scope_rejected(tmp_path, extra, what):
     assert what in str(ei.value)
 
 
-@pytest.mark.parametrize("key", ['mesh_method = "sdf"',
+@pytest.mark.parametrize("key", ['mesh_method = "marching"',
                                  'mesh_smooth_method = "cotan"\nmesh_smooth_passes = 2',
                                  "decimate_ratio = 0.5"])
 def test_mesh_options_outside_build_rejected(tmp_path, key):

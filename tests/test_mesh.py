@@ -49,11 +49,21 @@ def _sphere(n, centre, radius, shape=None):
 
 
 # ------------------------------------------------------------------- CPU
+def _sdf_cases(g):
+    for c in range(2):
+        passes, r_cells, s_cells = g[f"sdf_case_{c}"]
+        yield c, int(passes), float(r_cells), float(s_cells)
+
+
 def test_oracle_density_matches_reference():
     g = _gold()
     for c, method, passes, margin, radius in _cases(g):
         d = om.density_field(g["pos"], SHAPE, float(g["dx"]), passes, margin, method, radius)
         assert np.array_equal(d, g[f"density_{c}"]), (c, method)
+    for c, passes, r_cells, s_cells in _sdf_cases(g):
+        d = om.density_field(g["sdf_pos"], SHAPE, float(g["dx"]), passes, 0, "sdf",
+                             sdf_particle_radius_cells=r_cells, sdf_search_radius_cells=s_cells)
+        assert np.array_equal(d, g[f"sdf_{c}"]), c
 
 
 def test_oracle_iso_surface_closed_sphere():
@@ -128,9 +138,11 @@ def test_mesh_options_outside_build_are_refused():
     from gpufluid_b200.config import OutputCfg
     check_mesh_options(OutputCfg())
     check_mesh_options(OutputCfg(mesh_method="cubic"))
-    check_mesh_options(OutputCfg(mesh=False, mesh_method="sdf"))
+    check_mesh_options(OutputCfg(mesh=False, mesh_method="marching"))
     check_mesh_options(OutputCfg(mesh_smooth_passes=2))
-    for kw in (dict(mesh_method="sdf"), dict(mesh_smooth_passes=2, mesh_smooth_method="cotan"),
+    check_mesh_options(OutputCfg(mesh_method="sdf"))
+    for kw in (dict(mesh_method="marching"),
+               dict(mesh_smooth_passes=2, mesh_smooth_method="cotan"),
                dict(decimate_ratio=0.5)):
         with pytest.raises(BlockError) as e:
             check_mesh_options(OutputCfg(**kw))
@@ -154,6 +166,21 @@ def test_density_matches_reference(gf):
         # float32 atomics add in arrival order: a few ulp of the largest value
         np.testing.assert_allclose(d, ref, rtol=0, atol=4e-6 * float(ref.max()), err_msg=str(c))
         assert np.array_equal(d == 0, ref == 0)
+
+
+@pytest.mark.gpu
+def test_sdf_density_matches_reference(gf):
+    """k_sdf_field on the stand-in, bit for bit: a minimum does not depend on
+    the order in which particles are met."""
+    g = _gold()
+    ex = _extractor(SHAPE, float(g["dx"]))
+    for c, passes, r_cells, s_cells in _sdf_cases(g):
+        ex.density(g["sdf_pos"], passes, 0, "sdf", sdf_particle_radius_cells=r_cells,
+                   sdf_search_radius_cells=s_cells)
+        assert np.array_equal(ex.dens.cpu().numpy(), g[f"sdf_{c}"]), c
+    ex.density(np.zeros((0, 3), np.float32), 0, 0, "sdf")  # no particles: R - r everywhere
+    d = ex.dens.cpu().numpy()
+    assert np.all(d == d.flat[0]) and d.flat[0] > 0
 
 
 @pytest.mark.gpu
@@ -256,7 +283,16 @@ def test_extract_on_solver_particles(gf):
     far = np.full((10, 3), 0.5, np.float32)  # density 10 at most: below iso 20
     assert ex.extract(far, iso_level=20.0) == (None, None)
     with pytest.raises(ValueError):
-        ex.extract(pos, mesh_method="sdf")
+        ex.extract(pos, mesh_method="marching")
+    # the "sdf" method: signed distance to the nearest particle (no atomics
+    # of float sums: bit-exact), surface at its zero level, inside below it
+    vd, td = ex.extract(s.pos, mesh_method="sdf", smooth_passes=1)
+    dd = ex.dens.cpu().numpy()
+    refd = om.density_field(pos, (48, 48, 48), s.dx, 1, 0, "sdf")
+    assert np.array_equal(dd, refd)
+    ov, ot = om.iso_surface(dd, 0.0, s.dx, below=True)
+    assert np.array_equal(vd, ov) and np.array_equal(td, ot)
+    assert om.mesh_volume(vd, td) > 0  # faces outward from the fluid
     with pytest.raises(ValueError):
         ex.extract(pos, mesh_smooth_passes=1, mesh_smooth_method="cotan")
     # Taubin smoothing on the device after extraction equals the oracle's
