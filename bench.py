@@ -555,6 +555,20 @@ def mesh_leg(torch, s, snap, hbm, reps=5, cpu=True):
             wall.append(time.perf_counter() - w0)
             dens_ms.append(ev[0].elapsed_time(ev[1]))
             surf_ms.append(ev[1].elapsed_time(ev[2]))
+    # the other field method and the smoothing: device time of one call each
+    def dev_ms(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+    sdf_ms = dev_ms(lambda: ex.density(pos, smooth_passes=2, mesh_method="sdf"))
+    ex.density(pos, smooth_passes=2)
+    smooth_ms = dev_ms(lambda: ex.surface(0.6, smooth_passes=2, smooth_method="taubin"))
     nc = GRID ** 3
     blur_bytes = 2 * 8 * nc
     out = {"workload": f"{GRID}^3 scene particles -> trilinear density, 2 blur passes, "
@@ -564,7 +578,9 @@ def mesh_leg(torch, s, snap, hbm, reps=5, cpu=True):
            "density_ms": round(float(np.median(dens_ms)), 4),
            "surface_ms": round(float(np.median(surf_ms)), 4),
            "extract_wall_ms": round(1e3 * float(np.median(wall)), 3),
-           "blur_bytes": blur_bytes}
+           "blur_bytes": blur_bytes,
+           "sdf_density_ms": round(sdf_ms, 3),
+           "surface_taubin2_with_copy_ms": round(smooth_ms, 3)}
     if cpu:
         from oracle import mesh as om
         p_host = pos.cpu().numpy()
