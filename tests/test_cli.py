@@ -172,6 +172,23 @@ def test_simulate_with_reseed(tmp_path):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("mesh_keys", ['mesh_method = "sdf"\n',
+                                       'mesh_smooth_passes = 2\nmesh_smooth_method = "laplacian"\n'])
+def test_simulate_with_coarse_pcg_and_mesh_options(tmp_path, mesh_keys):
+    """The preconditioner keys and the mesh options through the command line:
+    refined PCG with tile SGS and the coarse correction; an sdf surface or a
+    smoothed one per frame."""
+    cfg = _write_minimal(tmp_path, frames=2,
+                         extra_sim='pressure_solver = "pcg_refined"\n'
+                                   'pcg_preconditioner = "tile_sgs"\npcg_coarse = true')
+    cfg.write_text(cfg.read_text().replace("smooth_passes = 1\n", "smooth_passes = 1\n" + mesh_keys))
+    assert main(["simulate", str(cfg)]) == 0
+    from gpufluid_b200.mesh import read_ply
+    v, t = read_ply(tmp_path / "cache" / "mesh" / "frame_0001.ply")
+    assert len(v) > 0 and len(t) > 0 and np.isfinite(v).all()
+
+
+@pytest.mark.gpu
 def test_simulate_with_inflow_and_outflow(tmp_path):
     """The inflow adds round(2400/24) = 100 positions a frame (fewer if any
     land in a solid cell); from frame 1 the outflow slab y <= 0.12 drains."""
