@@ -61,6 +61,7 @@ GF_FLAG_GLOBAL_PCG = 1
 GF_FLAG_TRACE = 2
 GF_FLAG_SGS_SHIFT = 2  # bits 2-3: tile-local symmetric Gauss-Seidel sweeps
 GF_FLAG_COARSE = 16    # block-region coarse correction of the shared-memory PCG
+GF_FLAG_TEST_STALL = 64  # test only: the first grid reduction of the PCG runs out its wait
 GF_NOALLOC_MAX_CELLS = 2097152
 
 
@@ -69,6 +70,11 @@ class PressureInfo(ctypes.Structure):
                 ("status", ctypes.c_int32), ("n_active_tiles", ctypes.c_int32),
                 ("n_fluid", ctypes.c_int64), ("relres", ctypes.c_double),
                 ("kernel", ctypes.c_int32), ("coarse", ctypes.c_int32)]
+
+
+class Health(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in ("worst_status", "solves", "not_converged",
+                                              "failed", "last_status")]
 
 
 class SceneLayout(ctypes.Structure):
@@ -131,6 +137,7 @@ _SIGS = {
                           ctypes.c_int),
     "gf_reseed_emit": ([_vp, _vp, _vp, ctypes.c_int32, _vp, _vp], ctypes.c_int),
     "gf_pressure_stats": ([_vp, ctypes.POINTER(PressureInfo)], ctypes.c_int),
+    "gf_health_read": ([_vp, ctypes.c_int32, ctypes.POINTER(Health)], ctypes.c_int),
     "gf_pcg_trace": ([_vp, _vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
     "gf_record_bytes": ([_vp, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
     "gf_step_record": ([_vp, ctypes.POINTER(StepParams), _vp], ctypes.c_int),

@@ -5,7 +5,8 @@ FLIP/PIC/APIC scene:
 - it builds the solver from the TOML, adds the static obstacles' union SDF,
   seeds the fluid or resumes a checkpoint;
 - per frame it runs round(1/(fps*dt)) substeps (or step_cfl when cfl = true),
-  checks has_diverged(), writes mesh/frame_NNNN.ply (binary PLY of the GPU
+  checks has_diverged() and the frame's pressure-solve health (a failed solve
+  truncates the bake like a divergence), writes mesh/frame_NNNN.ply (binary PLY of the GPU
   iso-surface; an empty placeholder when no surface emerges) when
   [output] mesh = true, particles/frame_NNNN.npy when [output] particles =
   true, and writes checkpoints every --checkpoint-every frames;
@@ -140,7 +141,11 @@ def cmd_simulate(args) -> int:
     print(f"           resolution {nx}x{ny}x{nz}   dx={scene.dx:.5f}   domain={scene.domain_size}")
     solver = make_solver(scene, args)
     if getattr(args, "resume", None):
-        solver.load_checkpoint(args.resume)
+        try:
+            solver.load_checkpoint(args.resume)
+        except RuntimeError as e:
+            print(f"error: resume: {e}", file=sys.stderr)
+            return 2
     else:
         _seed(solver, scene)
     print(f"           particles: {solver.n_particles}")
@@ -163,7 +168,9 @@ def cmd_simulate(args) -> int:
     start_frame = int(getattr(args, "start_frame", 0))
     ckpt_every = int(getattr(args, "checkpoint_every", 0))
     t_sim = 0.0
-    truncated = None
+    truncated, reason = None, None
+    n_capped = 0  # pressure solves that stopped at their iteration cap
+    solver.pressure_health(reset=True)
     import torch
     # reseeding every reseed_every_n_frames frames (commands.py:612-660)
     rng_reseed = np.random.default_rng(123)
@@ -191,10 +198,20 @@ def cmd_simulate(args) -> int:
         torch.cuda.synchronize()
         t_sim += time.time() - ts
         if solver.has_diverged():
-            truncated = frame
+            truncated, reason = frame, "flip_divergence"
             print(f"[flip] solver diverged at frame {frame} (last dumped: {frame}/{sim.frames}).",
                   file=sys.stderr)
             break
+        # the frame's pressure solves, read once: a failed solve (CG
+        # breakdown, a non-finite value, a device wait that ran out) ends the
+        # bake like a divergence; solves stopped at their cap are counted
+        health = solver.pressure_health(reset=True)
+        if health["failed"]:
+            truncated, reason = frame, "pressure_solve_failed"
+            print(f"[flip] pressure solve failed ({health['worst_status']}) at frame {frame} "
+                  f"(last dumped: {frame}/{sim.frames}).", file=sys.stderr)
+            break
+        n_capped += health["not_converged"]
         if extractor is not None:
             # commands.py:721-770; the splat reads the solver's particle
             # storage directly (its order only changes float atomics' order)
@@ -229,9 +246,12 @@ def cmd_simulate(args) -> int:
         "mesh_pattern": "mesh/frame_{:04d}.ply",
         "particles_pattern": "particles/frame_{:04d}.npy" if scene.output.particles else None,
         "domain_size": list(scene.domain_size), "resolution": list(scene.domain.resolution),
-        "dx": scene.dx, "notes": f"sim={t_sim:.1f}s mesh={t_mesh:.1f}s", "solver": "flip",
+        "dx": scene.dx,
+        "notes": f"sim={t_sim:.1f}s mesh={t_mesh:.1f}s" + (
+            f" pressure_at_cap={n_capped}" if n_capped else ""),
+        "solver": "flip",
         "truncated_at_frame": int(truncated) if truncated is not None else None,
-        "truncation_reason": "flip_divergence" if truncated is not None else None,
+        "truncation_reason": reason,
     }
     (cache_dir / "cache.json").write_text(json.dumps(manifest, indent=2), encoding="utf-8")
     print(f"[gpufluid-b200] done. cache: {cache_dir}  sim total: {t_sim:.2f}s  "
@@ -240,7 +260,8 @@ def cmd_simulate(args) -> int:
     if timings:
         (cache_dir / "timings.json").write_text(json.dumps(
             {"sections_ms": timings, "call_counts": solver._prof.call_counts,
-             "sim_total_s": t_sim, "mesh_total_s": t_mesh}, indent=2, sort_keys=True))
+             "sim_total_s": t_sim, "mesh_total_s": t_mesh,
+             "pressure_solves_at_cap": n_capped}, indent=2, sort_keys=True))
     return 0 if truncated is None else 2
 
 

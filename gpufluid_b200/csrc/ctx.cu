@@ -510,6 +510,29 @@ int gf_pressure_stats(void *ctx, gf_pressure_info *info) {
   return e;
 }
 
+int gf_health_read(void *ctx, int32_t reset, gf_health *out) {
+  Ctx *c = as_ctx(ctx);
+  if (!c || !out) return GF_INVALID_ARG;
+  int32_t h[8];
+  int e = gf::check_cuda(c, cudaMemcpyAsync(h, c->health, sizeof(h), cudaMemcpyDeviceToHost,
+                                            c->stream),
+                         "read solve health");
+  if (e) return e;
+  if (reset && (e = gf::check_cuda(c, cudaMemsetAsync(c->health, 0, sizeof(h), c->stream),
+                                   "reset solve health")))
+    return e;
+  if ((e = gf::check_cuda(c, cudaStreamSynchronize(c->stream), "sync"))) return e;
+  static const int32_t by_severity[5] = {GF_OK, GF_NOT_CONVERGED, GF_BREAKDOWN, GF_NAN,
+                                         GF_TIMEOUT};
+  auto status_of = [&](int32_t sev) { return by_severity[sev < 0 ? 0 : (sev > 4 ? 4 : sev)]; };
+  out->worst_status = status_of(h[0]);
+  out->solves = h[1];
+  out->not_converged = h[2];
+  out->failed = h[3];
+  out->last_status = status_of(h[4]);
+  return GF_OK;
+}
+
 int gf_active_tiles(void *ctx, int32_t *n_active, const int32_t **tiles) {
   Ctx *c = as_ctx(ctx);
   if (!c) return GF_INVALID_ARG;

@@ -87,6 +87,8 @@ struct PcgSmemArgs {
   int sgs_sweeps;             // 0: Jacobi (the reference's); 1-3: tile-local symmetric GS
   int coarse;                 // coarse regions per block (0: no coarse correction)
   float *cbuf;                // coarse: rows of B, then the compact rows of P^T A P
+  int test_stall;             // GF_FLAG_TEST_STALL: the first all-reduce waits for a count
+                              // no block publishes, with a short spin limit
 };
 
 
@@ -172,6 +174,10 @@ struct Ctx {
   bool trace_on = false;
   PcgState *state = nullptr;
   PcgState *state_host = nullptr;  // pinned mirror
+  // solve health since the last gf_health_read reset (device int32[8]):
+  // [0] worst severity, [1] solves, [2] not converged, [3] failed, [4]
+  // severity of the last call; folded in by the pressure scatter kernel
+  int32_t *health = nullptr;
   int last_solver = -1;  // gf_solver of the last gf_pressure
   int last_iters = 0;    // iteration count of the last Jacobi / GS-RB solve
 

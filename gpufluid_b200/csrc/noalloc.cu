@@ -3,10 +3,9 @@
 // Some callers cannot allocate GPU memory at the moment they need a pressure
 // solve: a host application that owns every device allocation through its
 // own pool (a DCC plugin host, a game engine) and forbids libraries from
-// calling cudaMalloc, or a host that records its whole frame into a CUDA
-// graph, where allocating is not allowed.  They still own the inputs and the
-// output; this entry point keeps its only scratch -- the second Jacobi
-// buffer -- in a file-scope static device array, so it never calls
+// calling cudaMalloc or cudaFree behind its back.  They still own the inputs
+// and the output; this entry point keeps its only scratch -- the second
+// Jacobi buffer -- in a file-scope static device array, so it never calls
 // cudaMalloc, cudaFree or any allocating library routine.
 //
 // The array holds GF_NOALLOC_MAX_CELLS floats (8 MiB).  Every GPU that loads
@@ -19,7 +18,10 @@
 // The first call on a device looks up the array's device address with
 // cudaGetSymbolAddress while that device is current (host code may not use
 // the array's name as a device pointer); make that first call before any
-// stream capture begins.
+// stream capture begins -- a first call on a capturing stream is refused.
+// The label, div and p buffers and the stream must belong to the current
+// device.  Errors left pending by earlier, unrelated work on the thread are
+// cleared on entry, so the returned status describes this call only.
 #include <mutex>
 
 #include "gf_internal.cuh"
@@ -57,8 +59,9 @@ __global__ void k_jacobi_dense(const uint8_t *__restrict__ label, const float *_
   }
 }
 
-// Device address of g_jacobi_scratch per device, looked up once per device.
-static float *scratch_for_current_device(int *status) {
+// Device address of g_jacobi_scratch per device, looked up once per device
+// (refused while `st` is capturing: the lookup must not enter a capture).
+static float *scratch_for_current_device(cudaStream_t st, int *status) {
   constexpr int MAX_DEVICES = 64;
   static std::mutex mu;
   static float *addr[MAX_DEVICES] = {};
@@ -70,6 +73,12 @@ static float *scratch_for_current_device(int *status) {
   }
   std::lock_guard<std::mutex> lock(mu);
   if (!addr[dev]) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) {
+      cudaGetLastError();
+      *status = GF_INVALID_ARG;
+      return nullptr;
+    }
     void *p = nullptr;
     if (cudaGetSymbolAddress(&p, g_jacobi_scratch) != cudaSuccess || !p) {
       cudaGetLastError();
@@ -89,10 +98,11 @@ extern "C" int gf_jacobi_noalloc(int32_t nx, int32_t ny, int32_t nz, const uint8
   if (nx < 1 || ny < 1 || nz < 1 || iters < 0 || !label || !div || !p) return GF_INVALID_ARG;
   const int64_t n = (int64_t)nx * ny * nz;
   if (n > GF_NOALLOC_MAX_CELLS) return GF_INVALID_ARG;  // beyond the static scratch
-  int status = GF_OK;
-  float *scratch = gf::scratch_for_current_device(&status);
-  if (!scratch) return status;
+  cudaGetLastError();  // errors pending from earlier work are not this call's
   cudaStream_t st = reinterpret_cast<cudaStream_t>(cuda_stream);
+  int status = GF_OK;
+  float *scratch = gf::scratch_for_current_device(st, &status);
+  if (!scratch) return status;
   // the reference starts both Jacobi buffers at zero (solver3d.py:3595)
   if (cudaMemsetAsync(p, 0, n * sizeof(float), st) != cudaSuccess ||
       cudaMemsetAsync(scratch, 0, n * sizeof(float), st) != cudaSuccess) {

@@ -312,6 +312,8 @@ struct FastSync {
   unsigned long long *slots;  // [2][SM_MAXG][FAST_WORDS], zeroed per solve
   unsigned long long epoch;
   int *err;
+  long long spin_limit;       // polls before a wait gives up
+  int stall;                  // test only: the first reduction waits for a count nobody publishes
 };
 
 template <typename T>
@@ -323,6 +325,10 @@ __device__ __forceinline__ bool fast_allreduce3(FastSync &fs, GridSync &gs, cons
   T *s_two = sh + 96;  // [2][3] per-warp totals
   const unsigned G = gridDim.x;
   const unsigned long long tag = ((fs.epoch + 1ull) & 0xffffffffull) << 32;
+  // the count the readers wait for; under the test stall the first reduction
+  // waits for the next epoch's count, which no block publishes before every
+  // block has left this one, so every wait runs out
+  const unsigned long long want = (fs.stall && fs.epoch == 0ull) ? tag + (1ull << 32) : tag;
   unsigned long long *slots = fs.slots + (fs.epoch & 1ull) * (SM_MAXG * FAST_WORDS);
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
@@ -361,11 +367,11 @@ __device__ __forceinline__ bool fast_allreduce3(FastSync &fs, GridSync &gs, cons
       for (int m = 0; m < 3; ++m)
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-          w[m][k] = need[m] ? ld_relaxed_u64(slots + (idx + 64u * m) * FAST_WORDS + k) : tag;
-          all &= (w[m][k] & 0xffffffff00000000ull) == tag;
+          w[m][k] = need[m] ? ld_relaxed_u64(slots + (idx + 64u * m) * FAST_WORDS + k) : want;
+          all &= (w[m][k] & 0xffffffff00000000ull) == want;
         }
       if (all) break;
-      if (++spins > SM_SPIN_LIMIT) {
+      if (++spins > fs.spin_limit) {
         atomicExch(fs.err, 1);
         break;
       }
@@ -504,7 +510,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   }
   GridSync gs{a.partials, a.counter, &st->error, 0ull, a.trace, 0, a.trace_cap / 2, 0, clock64()};
   FastSync fs{reinterpret_cast<unsigned long long *>(a.partials + FAST_SLOTS_OFF), 0ull,
-              &st->error};
+              &st->error, a.test_stall ? 4096ll : SM_SPIN_LIMIT, a.test_stall};
   // Phases of an iteration for the trace (block thread 0's view, cycles):
   // 0 own update, 1 SGS sweeps, 2 halo publication + neighbour flags +
   // in-block rings, 3 remote rings, 4 stencil and dot products, 5 grid

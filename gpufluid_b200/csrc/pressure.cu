@@ -1081,9 +1081,58 @@ struct ScatterArgs {
   const double *x64;
   float *p;
   int ny, nz, nty, ntz;
+  // solve health: the statuses of the solve just finished (nst scenes,
+  // nullptr for the fixed-sweep Jacobi / GS-RB), the solve's barrier-timeout
+  // flag, and the context's health words
+  const PcgState *st;
+  const PcgState *st_err;
+  int nst;
+  int32_t *health;
 };
 
+// Severity of a solve status: OK < NOT_CONVERGED < BREAKDOWN < NAN < TIMEOUT.
+__host__ __device__ inline int status_severity(int s) {
+  switch (s) {
+    case GF_OK: return 0;
+    case GF_NOT_CONVERGED: return 1;
+    case GF_BREAKDOWN: return 2;
+    case GF_NAN: return 3;
+    case GF_TIMEOUT: return 4;
+    default: return 2;
+  }
+}
+
+// Block 0 folds the finished solve into the context's health words: one
+// solve per scene, the worst severity since the last reset and of this call,
+// and the counts of solves that stopped at their cap or failed.  Runs before
+// the scatter loop, uniformly in block 0 (it holds a block barrier).
+__device__ void fold_health(const ScatterArgs &a) {
+  if (blockIdx.x != 0 || a.health == nullptr) return;
+  __shared__ int s_worst;
+  if (threadIdx.x == 0) s_worst = 0;
+  __syncthreads();
+  const bool timeout = a.st_err != nullptr && ld_volatile_i(&a.st_err->error) != 0;
+  int nc = 0, nfail = 0, worst = 0;
+  for (int s = threadIdx.x; s < a.nst; s += blockDim.x) {
+    const int status = a.st == nullptr ? GF_OK : (timeout ? GF_TIMEOUT : a.st[s].status);
+    const int sev = status_severity(status);
+    worst = sev > worst ? sev : worst;
+    nc += status == GF_NOT_CONVERGED;
+    nfail += sev >= 2;
+  }
+  if (worst) atomicMax(&s_worst, worst);
+  if (nc) atomicAdd(&a.health[2], nc);
+  if (nfail) atomicAdd(&a.health[3], nfail);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    atomicMax(&a.health[0], s_worst);
+    atomicAdd(&a.health[1], a.nst);
+    a.health[4] = s_worst;
+  }
+}
+
 __global__ void k_scatter_p(ScatterArgs a) {
+  fold_health(a);
   const int64_t total = (int64_t)(*a.n_active) * TILE_CELLS;
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total;
        q += (int64_t)gridDim.x * blockDim.x) {
@@ -1099,6 +1148,7 @@ __global__ void k_scatter_p(ScatterArgs a) {
 }
 
 __global__ void kb_scatter_p(ScatterArgs a, SegIndex sx) {
+  fold_health(a);
   const int64_t total = (int64_t)(*a.n_active) * TILE_CELLS;
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total;
        q += (int64_t)gridDim.x * blockDim.x) {
@@ -1167,6 +1217,8 @@ int pressure_alloc(Ctx *c) {
                       "zero coarse operator")))
     return e;
   if ((e = A((void **)&c->tile_cost, (size_t)c->ntiles * 4, "alloc tile cost"))) return e;
+  if ((e = A((void **)&c->health, 8 * 4, "alloc solve health"))) return e;
+  if ((e = check_cuda(c, cudaMemset(c->health, 0, 8 * 4), "zero solve health"))) return e;
   if ((e = check_cuda(c, cudaMemset(c->state, 0, sizeof(PcgState)), "zero pcg state"))) return e;
   if ((e = check_cuda(c, cudaMallocHost((void **)&c->state_host, sizeof(PcgState)),
                       "alloc pinned state")))
@@ -1178,7 +1230,8 @@ int pressure_alloc(Ctx *c) {
 void pressure_free(Ctx *c) {
   void *ps[] = {c->tile_slot, c->tile_list, c->tile_order, c->tile_nbr, c->n_active, c->code, c->bdiv,
                 c->xf, c->r, c->z, c->d0, c->d1, c->Ad, c->x64, c->partials, c->state,
-                c->bar_counters, c->trace, c->halo, c->tile_cost, c->coarse_buf};
+                c->bar_counters, c->trace, c->halo, c->tile_cost, c->coarse_buf,
+                c->health};
   for (void *p : ps)
     if (p) cudaFree(p);
   if (c->state_host) cudaFreeHost(c->state_host);
@@ -1302,7 +1355,9 @@ static int launch_pressure_batch(Ctx *c, const gf_step_params *prm) {
   }
   if (c->timing) cudaEventRecord(c->ev[9], st);
   if ((e = check_cuda(c, cudaMemsetAsync(c->f.p, 0, c->ncell * 4, st), "zero p"))) return e;
-  ScatterArgs sc{c->n_active, c->tile_list, c->code, result, result64, c->f.p, 0, 0, 0, 0};
+  const bool pcg = solver == GF_PCG || solver == GF_PCG_REFINED;
+  ScatterArgs sc{c->n_active, c->tile_list, c->code, result, result64, c->f.p, 0, 0, 0, 0,
+                 pcg ? c->seg_state : nullptr, pcg ? c->state : nullptr, c->nseg, c->health};
   kb_scatter_p<<<gs, 256, 0, st>>>(sc, sx);
   c->launches++;
   c->last_solver = solver;
@@ -1391,7 +1446,8 @@ int launch_pressure(Ctx *c, const gf_step_params *prm) {
                      (prm->flags & GF_FLAG_TRACE) ? c->trace : nullptr, TRACE_CAP,
                      prm->max_iters, check_every, prm->tol * prm->tol, replace2, sign,
                      (prm->flags & GF_FLAG_SGS_MASK) >> GF_FLAG_SGS_SHIFT,
-                     coarse ? COARSE_K : 0, c->coarse_buf};
+                     coarse ? COARSE_K : 0, c->coarse_buf,
+                     (prm->flags & GF_FLAG_TEST_STALL) ? 1 : 0};
       // the solver publishes tagged 64-bit halo words over the first two halo
       // arrays; their counts restart at 1 with every solve
       if ((e = check_cuda(c, cudaMemsetAsync(h, 0, (size_t)nk * 8, st), "zero tagged halo")))
@@ -1412,8 +1468,10 @@ int launch_pressure(Ctx *c, const gf_step_params *prm) {
   }
   if (c->timing) cudaEventRecord(c->ev[9], st);
   if ((e = check_cuda(c, cudaMemsetAsync(c->f.p, 0, c->ncell * 4, st), "zero p"))) return e;
+  const bool pcg = solver == GF_PCG || solver == GF_PCG_REFINED;
   ScatterArgs sc{c->n_active, c->tile_list, c->code, result, result64, c->f.p,
-                 c->ny, c->nz, c->nty, c->ntz};
+                 c->ny, c->nz, c->nty, c->ntz, pcg ? c->state : nullptr,
+                 pcg ? c->state : nullptr, 1, c->health};
   k_scatter_p<<<gs, 256, 0, st>>>(sc);
   c->launches++;
   c->last_solver = solver;

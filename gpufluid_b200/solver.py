@@ -61,6 +61,20 @@ class FlipDivergenceError(RuntimeError):
         self.requested_frames = int(requested_frames)
 
 
+class PressureSolveError(RuntimeError):
+    """A pressure solve failed: its CG broke down, met a non-finite value, or a
+    device-side wait ran out (GF_BREAKDOWN, GF_NAN, GF_TIMEOUT).  The
+    reference has no such check (its PCG stops silently, solver3d.py:
+    2917-3043); a solve that stopped at its iteration cap is reported by
+    ``pressure_health`` but is not an error, as in the reference."""
+
+    def __init__(self, frame: int, health: dict) -> None:
+        super().__init__(f"pressure solve failed ({health['worst_status']}) in "
+                         f"{health['failed']} of {health['solves']} solves up to frame {frame}")
+        self.frame = int(frame)
+        self.health = dict(health)
+
+
 class DeviceArray:
     """Read-only view of a device tensor with the ``.numpy()`` accessor the
     reference's Warp arrays offer."""
@@ -392,8 +406,8 @@ class FlipSolver3D:
         prm = self._params(dt, pressure_iters, pressure_solver)
         self._last_params = prm
         if self._enable_cuda_graphs and not self._prof.enabled:
-            key = (self.transfer_mode, pressure_solver, self.n_particles, float(dt),
-                   int(pressure_iters), int(prm.flags))
+            # every parameter is baked into the captured launches
+            key = (self.n_particles,) + tuple(getattr(prm, f) for f, _ in prm._fields_)
             hit = key in self._cuda_graphs
             if hit:
                 self._cuda_graphs.move_to_end(key)
@@ -598,31 +612,18 @@ class FlipSolver3D:
             transfer_mode=str(self.transfer_mode), surface_tension=self.surface_tension)
 
     def load_checkpoint(self, path) -> None:
-        """solver3d.py:4159-4222: topology and dx must match."""
-        data = np.load(str(path), allow_pickle=False)
-        nx, ny, nz = int(data["nx"]), int(data["ny"]), int(data["nz"])
-        if (nx, ny, nz) != (self.nx, self.ny, self.nz):
-            raise RuntimeError(f"checkpoint grid {(nx, ny, nz)} != solver {(self.nx, self.ny, self.nz)}")
-        ckpt_dx = float(data["dx"])
-        if abs(ckpt_dx - self.dx) > 1e-9:
-            raise RuntimeError(f"checkpoint dx={ckpt_dx} != solver dx={self.dx} "
-                               f"(same grid resolution but different domain size)")
-        for key, live in (("gravity", self.gravity), ("rho", self.rho),
-                          ("viscosity", self.viscosity), ("flip_blend", self.flip_blend),
-                          ("surface_tension", self.surface_tension)):
-            if key in data.files and abs(float(data[key]) - float(live)) > 1e-9:
-                logging.getLogger("gpufluid.checkpoint").warning(
-                    "resume: %s drift saved=%s live=%s -- running with LIVE value",
-                    key, float(data[key]), live)
-        if "attr_color" in data.files and len(data["attr_color"]):
-            raise NotImplementedError("colour attributes are outside this build")
+        """solver3d.py:4159-4222: topology and dx must match; physics knobs
+        that differ from the saved ones log a warning and the live values
+        win.  A file that is not a readable checkpoint raises RuntimeError
+        before any state changes (``read_checkpoint``)."""
+        data = read_checkpoint(path, (self.nx, self.ny, self.nz), self.dx,
+                               {"gravity": self.gravity, "rho": self.rho,
+                                "viscosity": self.viscosity, "flip_blend": self.flip_blend,
+                                "surface_tension": self.surface_tension})
         marker = data["marker"].astype(np.int32)
         self._marker_host = marker.copy()
         self._label.copy_(torch.from_numpy(marker.astype(np.uint8)))
-        pos, vel, aff = data["pos"], data["vel"], data["affine_C"]
-        if len(aff) != len(pos):
-            aff = np.zeros((len(pos), 3, 3), np.float32)
-        self._set_particles(pos=pos, vel=vel, C=aff)
+        self._set_particles(pos=data["pos"], vel=data["vel"], C=data["affine_C"])
 
     # --------------------------------------------------------- diagnostics
     def pressure_stats(self) -> dict:
@@ -636,6 +637,31 @@ class FlipSolver3D:
                 "n_active_tiles": info.n_active_tiles, "n_fluid": int(info.n_fluid),
                 "relres": info.relres, "kernel": info.kernel, "coarse": info.coarse}
 
+    def pressure_health(self, reset: bool = True) -> dict:
+        """Status of the pressure solves since the last reset, kept on the
+        device by every substep (direct or replayed from a CUDA graph), so one
+        read per frame covers all its substeps: the worst status
+        (``"OK" < "NOT_CONVERGED" < "BREAKDOWN" < "NAN" < "TIMEOUT"``), the
+        number of solves, those that stopped at their iteration cap and those
+        that failed, and the worst status of the last solve.  Synchronises."""
+        h = _lib.Health()
+        self._set_stream()
+        _lib.check(self._L.gf_health_read(self._ctx, 1 if reset else 0, _lib.ctypes.byref(h)),
+                   self._ctx, "gf_health_read")
+        names = _lib.STATUS_NAMES
+        return {"worst_status": names[h.worst_status], "solves": int(h.solves),
+                "not_converged": int(h.not_converged), "failed": int(h.failed),
+                "last_status": names[h.last_status]}
+
+    def check_pressure(self, frame: int = -1) -> dict:
+        """Per-frame failure check beside ``has_diverged``: reads and resets
+        ``pressure_health`` and raises ``PressureSolveError`` if any solve
+        since the last check failed; returns the health otherwise."""
+        h = self.pressure_health(reset=True)
+        if h["failed"]:
+            raise PressureSolveError(frame, h)
+        return h
+
     def stage_times(self) -> list:
         """Device ms of the last step: bin, p2g, forces_div, pressure,
         project, g2p, total, solver kernel (needs enable_timing=True)."""
@@ -648,6 +674,52 @@ class FlipSolver3D:
         plus the kernel nodes of every CUDA-graph replay)."""
         return (int(self._L.gf_launch_count(self._ctx)) - self._captured_launches
                 + self._replayed_launches)
+
+
+_CKPT_KEYS = ("pos", "vel", "affine_C", "marker", "nx", "ny", "nz", "dx")
+
+
+def read_checkpoint(path, grid, dx, live=None) -> dict:
+    """Read and validate a checkpoint written by ``save_checkpoint`` here or
+    by the reference's (solver3d.py:4127-4157; the same keys), with the
+    reference loader's checks (solver3d.py:4159-4191): the grid must match
+    ``grid`` and dx must match within 1e-9 (RuntimeError), and a physics knob
+    in ``live`` that differs from the saved value logs a warning.  Beyond the
+    reference, a truncated or damaged archive, missing keys and inconsistent
+    array shapes raise RuntimeError too.  Returns pos, vel, affine_C (zeros
+    when its length differs from pos, as the reference drops it) and marker."""
+    try:
+        with np.load(str(path), allow_pickle=False) as npz:
+            data = {k: npz[k] for k in npz.files}
+    except (OSError, ValueError, EOFError, KeyError) as e:
+        raise RuntimeError(f"checkpoint {path}: not a readable .npz ({e})") from None
+    except Exception as e:  # zipfile / zlib errors of a damaged archive
+        raise RuntimeError(f"checkpoint {path}: damaged archive ({e})") from None
+    missing = [k for k in _CKPT_KEYS if k not in data]
+    if missing:
+        raise RuntimeError(f"checkpoint {path}: keys missing {missing}")
+    nx, ny, nz = int(data["nx"]), int(data["ny"]), int(data["nz"])
+    if (nx, ny, nz) != tuple(grid):
+        raise RuntimeError(f"checkpoint grid {(nx, ny, nz)} != solver {tuple(grid)}")
+    ckpt_dx = float(data["dx"])
+    if abs(ckpt_dx - dx) > 1e-9:
+        raise RuntimeError(f"checkpoint dx={ckpt_dx} != solver dx={dx} "
+                           f"(same grid resolution but different domain size)")
+    for key, val in (live or {}).items():
+        if key in data and abs(float(data[key]) - float(val)) > 1e-9:
+            logging.getLogger("gpufluid.checkpoint").warning(
+                "resume: %s drift saved=%s live=%s -- running with LIVE value",
+                key, float(data[key]), val)
+    if "attr_color" in data and len(data["attr_color"]):
+        raise NotImplementedError("colour attributes are outside this build")
+    pos, vel, aff = data["pos"], data["vel"], data["affine_C"]
+    if (data["marker"].shape != tuple(grid) or pos.ndim != 2 or pos.shape[1:] != (3,)
+            or vel.shape != pos.shape):
+        raise RuntimeError(f"checkpoint {path}: inconsistent array shapes "
+                           f"(marker {data['marker'].shape}, pos {pos.shape}, vel {vel.shape})")
+    if len(aff) != len(pos):
+        aff = np.zeros((len(pos), 3, 3), np.float32)
+    return {"pos": pos, "vel": vel, "affine_C": aff, "marker": data["marker"]}
 
 
 def cfl_substep_count(vel_np: np.ndarray, dx: float, target_dt: float, cfl: float = 0.5,

@@ -108,6 +108,13 @@ typedef struct gf_step_params {
  * solve, M^-1 = M_tile^-1 + P B P^T.  Same operator, stop test and answer;
  * fewer iterations.  The global-memory kernel ignores it. */
 #define GF_FLAG_COARSE 16
+/* flags, test only: the shared-memory PCG's first grid reduction waits for a
+ * publication count that no block writes, with a spin limit of 4096 polls
+ * instead of the normal one, so every block's wait runs out, the kernel
+ * returns and the solve reports GF_TIMEOUT (gf_pressure_result,
+ * gf_health_read).  It exercises the bounded-wait exit path without a fault;
+ * the context stays usable.  No effect on the global-memory kernel. */
+#define GF_FLAG_TEST_STALL 64
 
 /* ---- context ------------------------------------------------------------ */
 /* Allocates scratch for a grid and up to max_particles particles on the
@@ -181,6 +188,22 @@ typedef struct gf_pressure_info {
 int gf_pcg_trace(void *ctx, int64_t *host, int32_t cap, int32_t *n);
 /* Statistics of the last pressure solve; synchronises. */
 int gf_pressure_stats(void *ctx, gf_pressure_info *info);
+/* Health of the pressure solves since the last reset, folded in on the device
+ * by every gf_pressure / gf_step (and every replay of a captured gf_step), so
+ * a host can check once per frame instead of synchronising per substep.  The
+ * reference's PCG stops silently at its cap (_pressure_pcg, solver3d.py:
+ * 2917-3043); its only failure check is the per-frame NaN probe of
+ * has_diverged (:2642-2656).  On a batch every scene counts as one solve.
+ * reset != 0 zeroes the record after reading it.  Synchronises. */
+typedef struct gf_health {
+  int32_t worst_status;  /* most severe gf_status since the reset: GF_OK < GF_NOT_CONVERGED <
+                            GF_BREAKDOWN < GF_NAN < GF_TIMEOUT */
+  int32_t solves;        /* pressure solves since the reset */
+  int32_t not_converged; /* solves that stopped at their iteration cap */
+  int32_t failed;        /* solves that ended in GF_BREAKDOWN, GF_NAN or GF_TIMEOUT */
+  int32_t last_status;   /* most severe status of the last solve call */
+} gf_health;
+int gf_health_read(void *ctx, int32_t reset, gf_health *out);
 /* Active 8^3 pressure tiles of the last solve (k_mark_active_blocks,
  * solver3d.py:953-972): count and tile ids (device pointer). */
 int gf_active_tiles(void *ctx, int32_t *n_active, const int32_t **tiles);
@@ -381,8 +404,9 @@ int gf_set_tune(void *ctx, const gf_tune_info *in);
 
 /* ---- allocation-free variant ------------------------------------------- */
 /* No counterpart in the reference.  For callers that may not allocate device
- * memory (a host that owns every device allocation through its own pool, or
- * one recording into a CUDA graph): a Jacobi pressure solve with the
+ * memory (a host that owns every device allocation through its own pool and
+ * forbids libraries from calling cudaMalloc / cudaFree): a Jacobi pressure
+ * solve with the
  * arithmetic of gf_pressure(GF_JACOBI) on the dense grid -- label (uint8),
  * div and p are (nx,ny,nz) device arrays owned by the caller; p receives the
  * result of `iters` sweeps started from zero.  Its only scratch is a static
@@ -391,7 +415,10 @@ int gf_set_tune(void *ctx, const gf_tune_info *in);
  * no cudaMalloc/cudaFree.  Calls share that array: calls overlapping on the
  * GPU race, calls in order on one stream are safe.  The first call on a
  * device resolves the array's device address (cudaGetSymbolAddress) and
- * should come before any stream capture.  Asynchronous on cuda_stream. */
+ * should come before any stream capture (on a capturing stream it returns
+ * GF_INVALID_ARG).  label, div, p and the stream belong to the current device.
+ * Errors pending from earlier work are cleared on entry, so the status is
+ * this call's own.  Asynchronous on cuda_stream. */
 #define GF_NOALLOC_MAX_CELLS 2097152
 int gf_jacobi_noalloc(int32_t nx, int32_t ny, int32_t nz, const uint8_t *label,
                       const float *div, float *p, int32_t iters, void *cuda_stream);

@@ -3,7 +3,7 @@
 Test-fixture generator (run by hand, in a container that holds the reference
 checkout; nothing at test or bench time reads the reference):
 
-    python tests/golden/make_golden.py [--reference /root/reference] [--only NAME]
+    python tests/golden/make_golden.py --reference <path of the GPUFLUID checkout> [--only NAME]
 
 It installs the sequential Warp stand-in (``warp_shim.py``), imports
 ``gpufluid.solvers.solver3d`` from the reference checkout unmodified, builds
@@ -159,7 +159,9 @@ def run_scene(name, cfg, ref_src):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("GPUFLUID_REFERENCE"),
+                    required="GPUFLUID_REFERENCE" not in os.environ,
+                    help="GPUFLUID source checkout (or set GPUFLUID_REFERENCE)")
     ap.add_argument("--only", default=None)
     a = ap.parse_args()
     ref_src = os.path.join(a.reference, "src")

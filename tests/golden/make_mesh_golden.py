@@ -9,7 +9,7 @@ points within the radius, which is all Warp's query promises).
 Test-fixture generator (run by hand, in a container that holds the reference
 checkout; nothing at test or bench time reads the reference):
 
-    python tests/golden/make_mesh_golden.py [--reference /root/reference]
+    python tests/golden/make_mesh_golden.py --reference <path of the GPUFLUID checkout>
 
 It installs the sequential Warp stand-in (``warp_shim.py``) and imports the
 two reference modules unmodified.  The iso-surface step after them is a
@@ -49,7 +49,9 @@ def particles():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("GPUFLUID_REFERENCE"),
+                    required="GPUFLUID_REFERENCE" not in os.environ,
+                    help="GPUFLUID source checkout (or set GPUFLUID_REFERENCE)")
     args = ap.parse_args()
     sys.path.insert(0, HERE)
     import warp_shim

@@ -4,7 +4,7 @@ own ``gpufluid.domain.regions`` (src/gpufluid/domain/regions.py).
 Test-fixture generator (run by hand, in a container that holds the reference
 checkout; nothing at test or bench time reads the reference):
 
-    python tests/golden/make_regions_golden.py [--reference /root/reference]
+    python tests/golden/make_regions_golden.py --reference <path of the GPUFLUID checkout>
 
 It imports the reference module unmodified (pure NumPy, no Warp needed) and
 records:
@@ -54,7 +54,9 @@ def outflow_inputs():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("GPUFLUID_REFERENCE"),
+                    required="GPUFLUID_REFERENCE" not in os.environ,
+                    help="GPUFLUID source checkout (or set GPUFLUID_REFERENCE)")
     args = ap.parse_args()
     sys.path.insert(0, os.path.join(args.reference, "src"))
     from gpufluid.domain.regions import InflowBox, OutflowBox, apply_inflows, apply_outflows

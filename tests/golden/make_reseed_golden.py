@@ -4,7 +4,7 @@
 Test-fixture generator (run by hand, in a container that holds the reference
 checkout; nothing at test or bench time reads the reference):
 
-    python tests/golden/make_reseed_golden.py [--reference /root/reference]
+    python tests/golden/make_reseed_golden.py --reference <path of the GPUFLUID checkout>
 
 It installs the sequential Warp stand-in (``warp_shim.py``) plus a
 ``warp.utils.array_scan`` restated from Warp's documentation (an inclusive or
@@ -57,7 +57,9 @@ def scene():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("GPUFLUID_REFERENCE"),
+                    required="GPUFLUID_REFERENCE" not in os.environ,
+                    help="GPUFLUID source checkout (or set GPUFLUID_REFERENCE)")
     args = ap.parse_args()
     sys.path.insert(0, HERE)
     import warp_shim

@@ -1,10 +1,11 @@
 """The allocation-free Jacobi entry point, gf_jacobi_noalloc.
 
 It serves callers that may not allocate device memory (a host that owns all
-device allocations through its own pool, or one recording a CUDA graph): its
-scratch is a static device array, so it must give exactly what the regular
-context-based gf_pressure(GF_JACOBI) gives on the same inputs -- also on a
-second call in a row, which reuses the array the first call left behind.
+device allocations through its own pool and forbids libraries from calling
+cudaMalloc / cudaFree): its scratch is a static device array, so it must give
+exactly what the regular context-based gf_pressure(GF_JACOBI) gives on the
+same inputs -- also on a second call in a row, which reuses the array the
+first call left behind.
 This file is collected last so a failure here cannot hide any other test.
 """
 import ctypes
