@@ -598,14 +598,14 @@ def e2e_pipelined(torch, gf, device, snap, steps, barrier, max_over_ranks, depth
     return ms, depth
 
 
-def mesh_leg(torch, s, snap, hbm, reps=5, cpu=True):
+def mesh_leg(torch, s, snap, hbm, reps=5):
     """MeshExtractor on the bench scene's particles with the scene TOML's
     [output] defaults (trilinear splat, 2 blur passes, iso 0.6): device time
     of the density field (zero + splat + 2 blur passes) and of the iso-surface
     (count, scan, read-back of the totals, emit), wall time of the whole
-    extract including the copy of the mesh to the host, and the oracle's
-    time for the same field and surface on one host thread.  Blur bytes:
-    4 B read + 4 B written per cell per pass (neighbour reads hit cache)."""
+    extract including the copy of the mesh to the host, and the marching-
+    tetrahedra surface of the same field for comparison.  Blur bytes: 4 B read
+    + 4 B written per cell per pass (neighbour reads hit cache)."""
     from gpufluid_b200.mesh import MeshExtractor
     pos = snap[0]  # the scene's particle positions (storage order)
     ex = MeshExtractor(GRID, GRID, GRID, s.dx)
@@ -640,28 +640,24 @@ def mesh_leg(torch, s, snap, hbm, reps=5, cpu=True):
     sdf_ms = dev_ms(lambda: ex.density(pos, smooth_passes=2, mesh_method="sdf"))
     ex.density(pos, smooth_passes=2)
     smooth_ms = dev_ms(lambda: ex.surface(0.6, smooth_passes=2, smooth_method="taubin"))
+    ex.surface_method = "marching_tetrahedra"
+    mt_ms = dev_ms(lambda: ex.surface(0.6))
+    mt_tris = ex.n_tris
+    ex.surface_method = "marching_cubes"
     nc = GRID ** 3
     blur_bytes = 2 * 8 * nc
-    out = {"workload": f"{GRID}^3 scene particles -> trilinear density, 2 blur passes, "
-                       "iso 0.6 surface (marching tetrahedra), copied to the host",
-           "particles": int(pos.shape[0]), "verts": 0 if v is None else int(len(v)),
-           "tris": 0 if t is None else int(len(t)),
-           "density_ms": round(float(np.median(dens_ms)), 4),
-           "surface_ms": round(float(np.median(surf_ms)), 4),
-           "extract_wall_ms": round(1e3 * float(np.median(wall)), 3),
-           "blur_bytes": blur_bytes,
-           "sdf_density_ms": round(sdf_ms, 3),
-           "surface_taubin2_with_copy_ms": round(smooth_ms, 3)}
-    if cpu:
-        from oracle import mesh as om
-        p_host = pos.cpu().numpy()
-        t0 = time.perf_counter()
-        d = om.density_field(p_host, (GRID, GRID, GRID), s.dx, 2, 0)
-        ov, ot = om.iso_surface(d, 0.6, s.dx)
-        out["cpu_oracle_s"] = round(time.perf_counter() - t0, 3)
-        out["cpu_oracle_cores"] = 1
-        out["cpu_oracle_tris"] = int(len(ot))
-    return out
+    return {"workload": f"{GRID}^3 scene particles -> trilinear density, 2 blur passes, "
+                        "iso 0.6 surface (marching cubes), copied to the host",
+            "particles": int(pos.shape[0]), "verts": 0 if v is None else int(len(v)),
+            "tris": 0 if t is None else int(len(t)),
+            "density_ms": round(float(np.median(dens_ms)), 4),
+            "surface_ms": round(float(np.median(surf_ms)), 4),
+            "extract_wall_ms": round(1e3 * float(np.median(wall)), 3),
+            "blur_bytes": blur_bytes,
+            "sdf_density_ms": round(sdf_ms, 3),
+            "surface_taubin2_with_copy_ms": round(smooth_ms, 3),
+            "marching_tetrahedra_surface_with_copy_ms": round(mt_ms, 3),
+            "marching_tetrahedra_tris": int(mt_tris)}
 
 
 def stage_bytes_flip(P, ncell_active, F):
@@ -679,8 +675,9 @@ def extra_legs(torch, device, steps=3):
     1e-5 with at most 200 iterations; 256^3 double dam break (x in [0,.3] and
     [.7,1], y in [0,.7]), FLIP 0.97, dt 1/960, refined PCG to 1e-7 (the
     global-memory solver: the active region exceeds the shared-memory one)
-    and 200 Jacobi sweeps as the plain comparison, with per-stage times and
-    the device memory footprint."""
+    with the tile SGS preconditioner and, from the same state, with the
+    reference's Jacobi one, and 200 Jacobi sweeps as the plain comparison,
+    with per-stage times and the device memory footprint."""
     import gpufluid_b200 as gf
     stream = torch.cuda.current_stream()
     out = {}
@@ -707,15 +704,24 @@ def extra_legs(torch, device, steps=3):
     del s
     torch.cuda.empty_cache()
     free0, _ = torch.cuda.mem_get_info()
-    s = gf.FlipSolver3D(256, 256, 256, flip_blend=0.97, pressure_tol=1e-7, device=device)
+    s = gf.FlipSolver3D(256, 256, 256, flip_blend=0.97, pressure_tol=1e-7, device=device,
+                        pcg_preconditioner="tile_sgs", pcg_sgs_sweeps=2)
     s.seed_box((0.0, 0.0, 0.0), (0.3, 0.7, 1.0))
     s.seed_box((0.7, 0.0, 0.0), (1.0, 0.7, 1.0), append=True)
     dt = 1 / 960
     s.step(dt, pressure_iters=4000, pressure_solver="pcg_refined")
     torch.cuda.synchronize()
     free1, _ = torch.cuda.mem_get_info()
+    snap = snapshot(s)
     ms_ref = timed(s, dt, 4000, "pcg_refined", steps)
     st_ref = s.pressure_stats()
+    # the same substeps with the reference's Jacobi preconditioner
+    restore(s, snap)
+    s.pcg_preconditioner = "jacobi"
+    ms_ref_jac = timed(s, dt, 4000, "pcg_refined", steps)
+    st_ref_jac = s.pressure_stats()
+    s.pcg_preconditioner = "tile_sgs"
+    restore(s, snap)
     ms_jac = timed(s, dt, 200, "jacobi", steps)
     s._prof.enabled = True
     s._L.gf_enable_timing(s._ctx, 1)
@@ -733,6 +739,9 @@ def extra_legs(torch, device, steps=3):
         "particles": P, "refined_pcg1e-7_ms_per_substep": round(ms_ref, 3),
         "refined_substeps_per_s": round(1000 / ms_ref, 3),
         "refined_iters_last": st_ref["iters"],
+        "refined_preconditioner": "tile-local symmetric Gauss-Seidel, 2 sweeps",
+        "refined_jacobi_precond_ms_per_substep": round(ms_ref_jac, 3),
+        "refined_jacobi_precond_iters_last": st_ref_jac["iters"],
         "pcg_kernel": "global-memory" if st_ref["kernel"] == 2 else "shared-memory",
         "jacobi200_ms_per_substep": round(ms_jac, 3),
         "jacobi200_substeps_per_s": round(1000 / ms_jac, 3),
@@ -863,8 +872,7 @@ def run_ours(args):
 
     outflow = outflow_leg(torch, s, hbm)
     reseed = reseed_leg(torch, s, snap)
-    mesh = mesh_leg(torch, s, snap, hbm, cpu=(rank == 0 and world == 1
-                                              and not args.no_cpu_baseline))
+    mesh = mesh_leg(torch, s, snap, hbm)
 
     fwd_adj = None if args.no_adjoint else adjoint_leg(torch, device)
     fwd_adj_apic = None if args.no_adjoint else adjoint_leg(torch, device, transfer="apic")
@@ -878,6 +886,7 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(steps=1)
+        cpu["mesh"] = cpu_mesh_baseline(snap[0].cpu().numpy(), s.dx)
 
     if rank == 0:
         value = world * 1000.0 / ms_ref_max
@@ -973,6 +982,17 @@ def cpu_baseline(steps=1):
             "kind": "port", "sample": f"{steps} substep(s) of the 128^3 APIC scene from the "
             f"seeded state ({pos.shape[0]} particles), FP64 CG pressure to {TOL}, "
             f"{dt:.1f} s wall"}
+
+
+def cpu_mesh_baseline(pos, dx):
+    """The oracle's density field and marching-cubes surface of the same
+    particles on one host thread (the mesh leg's CPU comparison)."""
+    from oracle import mesh as om
+    t0 = time.perf_counter()
+    d = om.density_field(pos, (GRID, GRID, GRID), dx, 2, 0)
+    _, ot = om.iso_surface_mc(d, 0.6, dx)
+    return {"seconds": round(time.perf_counter() - t0, 3), "cores": 1, "tris": int(len(ot)),
+            "sample": f"{GRID}^3 field of {len(pos)} particles, 2 blur passes, iso 0.6"}
 
 
 def run_reference(args):

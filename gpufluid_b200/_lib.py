@@ -74,7 +74,7 @@ class PressureInfo(ctypes.Structure):
 
 class Health(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int32) for n in ("worst_status", "solves", "not_converged",
-                                              "failed", "last_status")]
+                                              "failed", "last_status", "wait_timeouts")]
 
 
 class SceneLayout(ctypes.Structure):
@@ -94,6 +94,9 @@ class TuneInfo(ctypes.Structure):
 
 GF_MESH_TRILINEAR, GF_MESH_CUBIC, GF_MESH_SDF = 0, 1, 2
 MESH_METHOD = {"trilinear": GF_MESH_TRILINEAR, "cubic": GF_MESH_CUBIC, "sdf": GF_MESH_SDF}
+GF_SURFACE_MARCHING_CUBES, GF_SURFACE_MARCHING_TETRAHEDRA = 0, 1
+SURFACE = {"marching_cubes": GF_SURFACE_MARCHING_CUBES,
+           "marching_tetrahedra": GF_SURFACE_MARCHING_TETRAHEDRA}
 GF_MESH_SMOOTH_LAPLACIAN, GF_MESH_SMOOTH_TAUBIN = 0, 1
 MESH_SMOOTH = {"laplacian": GF_MESH_SMOOTH_LAPLACIAN, "taubin": GF_MESH_SMOOTH_TAUBIN}
 
@@ -175,6 +178,8 @@ _SIGS = {
     "gf_mesher_copy": ([_vp, _vp, _vp], ctypes.c_int),
     "gf_mesher_copy_field": ([_vp, _vp], ctypes.c_int),
     "gf_mesher_set_inside_below": ([_vp, ctypes.c_int32], ctypes.c_int),
+    "gf_mesher_set_surface": ([_vp, ctypes.c_int32], ctypes.c_int),
+    "gf_marching_cubes_table": ([_vp, _vp, _vp], ctypes.c_int),
     "gf_mesher_smooth": ([_vp, _vp, ctypes.c_int64, _vp, ctypes.c_int64, ctypes.c_int32,
                           ctypes.c_int32, ctypes.c_double, ctypes.c_double], ctypes.c_int),
 }

@@ -310,7 +310,7 @@ int gf_bind(void *ctx, const gf_fields *f, const gf_particles *p) {
   c->f = *f;
   c->p = *p;
   c->bound = true;
-  return GF_OK;
+  return gf::encode_face_maps(c);
 }
 
 int gf_set_stream(void *ctx, void *stream) {
@@ -530,6 +530,7 @@ int gf_health_read(void *ctx, int32_t reset, gf_health *out) {
   out->not_converged = h[2];
   out->failed = h[3];
   out->last_status = status_of(h[4]);
+  out->wait_timeouts = h[5];
   return GF_OK;
 }
 

@@ -16,6 +16,7 @@
 //    16-bit stencil code per cell.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap (encoded through the runtime's driver entry point)
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -122,6 +123,16 @@ __device__ __forceinline__ int seg_find(const int64_t *__restrict__ off, int n, 
   return lo;
 }
 
+// TMA descriptors of the six face arrays G2P stages per tile (u, v, w, us,
+// vs, ws), encoded when the caller's buffers are bound.  Bit a of `mask` is
+// set when array a's layout allows a tiled tensor map (16-byte aligned base
+// and row / plane strides); G2P loads the other arrays' boxes with plain
+// loads.
+struct FaceMaps {
+  CUtensorMap m[6];
+  int mask;
+};
+
 // Launch shapes chosen by gf_autotune (defaults until it runs).
 struct Tune {
   int g2p_threads = 256;
@@ -143,6 +154,7 @@ struct Ctx {
   // caller buffers
   gf_fields f{};
   gf_particles p{};
+  FaceMaps face_maps{};  // tensor maps of the bound face arrays (single grid)
   // outflow compaction scratch (block counts, offsets, boxes), grown on use
   int32_t *region_scratch = nullptr;
   int64_t region_scratch_n = 0;
@@ -176,7 +188,8 @@ struct Ctx {
   PcgState *state_host = nullptr;  // pinned mirror
   // solve health since the last gf_health_read reset (device int32[8]):
   // [0] worst severity, [1] solves, [2] not converged, [3] failed, [4]
-  // severity of the last call; folded in by the pressure scatter kernel
+  // severity of the last call (folded in by the pressure scatter kernel),
+  // [5] stage-kernel waits that ran out (the G2P tile loads)
   int32_t *health = nullptr;
   int last_solver = -1;  // gf_solver of the last gf_pressure
   int last_iters = 0;    // iteration count of the last Jacobi / GS-RB solve
@@ -225,6 +238,7 @@ int launch_pressure(Ctx *c, const gf_step_params *prm);
 int launch_project(Ctx *c, float dt, float rho);
 int launch_g2p(Ctx *c, int transfer, float flip_blend, float dt);
 int launch_vmax(Ctx *c);
+int encode_face_maps(Ctx *c);
 
 int launch_pcg_smem(Ctx *c, PcgSmemArgs &a, bool refined);
 bool pcg_smem_fits(Ctx *c, bool refined);

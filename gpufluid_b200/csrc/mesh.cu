@@ -22,16 +22,30 @@
 // gf_mesher_extract cuts the iso-surface density >= iso_level out of the field
 // sampled at the cell indices (vertices are index * dx, as the reference's
 // marching cubes returns them).  The reference hands this step to
-// scikit-image's or Warp's marching cubes; this library uses marching
-// tetrahedra on the Kuhn (Freudenthal) split of every cube into the six
-// tetrahedra that share its main diagonal: the split is conforming between
-// neighbouring cubes, has no ambiguous cases and needs no case table.  A
-// vertex sits on each grid edge (offsets x, y, z, the face diagonals and the
-// main diagonal from a node's lower corner) whose end values straddle the
-// level, at the linear crossing from the lower end; axis-edge vertices are the
-// ones marching cubes places.  Triangles face from >= iso to < iso.  Output
-// order is fixed: vertices by (node, edge family), triangles by (cube, tet,
-// triangle), so the mesh is deterministic for a given field.
+// scikit-image's or Warp's marching cubes (surface.py:286-351).  This library
+// writes its own, two ways (gf_mesher_set_surface):
+//  * marching cubes (the default; Lorensen & Cline 1987).  A vertex sits on
+//    each axis edge whose end values straddle the level, at the linear
+//    crossing from the lower end.  The triangles of a cube come from a case
+//    table this file generates (build_mc_table): on each cube face the
+//    crossing edges pair into segments -- on an ambiguous face (two diagonal
+//    corners inside, two outside) the pairs cut off the inside corners, so the
+//    inside corners are never joined across a face.  That rule depends on the
+//    face alone, so two cubes sharing a face cut it the same way and the
+//    surface is closed wherever it does not meet the grid boundary.  The
+//    segments chain into loops around the cube; each is oriented with the
+//    inside on its right as seen from outside the cube, which makes every
+//    triangle face from >= iso to < iso, listed from its lowest edge, and
+//    fanned from its first vertex whose diagonals all leave the cube's faces
+//    (a diagonal inside a face would meet the neighbouring cube's).  At most
+//    5 triangles per cube.
+//  * marching tetrahedra on the Kuhn (Freudenthal) split of every cube into
+//    the six tetrahedra that share its main diagonal: conforming between
+//    cubes, no ambiguous cases, no table.  Vertices also sit on the face
+//    diagonals and the main diagonal (offsets from a node's lower corner); its
+//    axis-edge vertices are the marching-cubes ones.
+// Output order is fixed: vertices by (node, edge family), triangles by (cube,
+// table entry or tet), so the mesh is deterministic for a given field.
 //   k_mesh_count  per node: crossing-edge mask, cube corner mask, block sums
 //   k_mesh_scan   block sums -> block offsets and the two totals (int64)
 //   (host reads the totals, grows the output buffers)
@@ -42,6 +56,7 @@
 #include <cub/cub.cuh>
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 #include <string>
 
 #include "../../include/gfb200.h"
@@ -68,6 +83,7 @@ struct Mesher {
   int64_t tris_cap = 0;
   int64_t nv = -1, nt = -1;    // counts of the last extraction
   int below = 0;               // 1: the surface encloses field <= iso (signed distances)
+  int surface = GF_SURFACE_MARCHING_CUBES;
   int64_t launches = 0;
   // mesh smoothing scratch, grown on use
   void *sm_buf = nullptr;
@@ -266,6 +282,118 @@ __device__ __forceinline__ int cube_tris(int cm) {
   return s;
 }
 
+// ---- marching-cubes case table ----------------------------------------------
+// Edge e of a cube runs along axis bit a = 1, 2, 4 for e / 4 = 0, 1, 2, from
+// corner lo, the (e % 4)-th corner (ascending) without bit a, to lo | a.
+// Case cm (bit c: corner c is inside) has c_mc_ntri[cm] triangles, edges
+// c_mc_tri[cm][3 t + 0..2].
+struct McTable {
+  uint8_t edge[12][2];
+  uint8_t ntri[256];
+  uint8_t tri[256][15];
+};
+__constant__ McTable c_mc;
+
+static McTable build_mc_table() {
+  McTable t{};
+  int ne = 0;
+  for (int a = 1; a <= 4; a <<= 1)
+    for (int lo = 0; lo < 8; ++lo)
+      if (!(lo & a)) {
+        t.edge[ne][0] = (uint8_t)lo;
+        t.edge[ne][1] = (uint8_t)(lo | a);
+        ++ne;
+      }
+  // doubled coordinates: corner c at 2 * bits, an edge's midpoint at the sum
+  auto cc = [](int c, int k) { return 2 * ((c >> k) & 1); };
+  for (int cm = 0; cm < 256; ++cm) {
+    auto in = [&](int c) { return (cm >> c) & 1; };
+    int next[12];
+    bool cross[12];
+    for (int e = 0; e < 12; ++e) {
+      next[e] = -1;
+      cross[e] = in(t.edge[e][0]) != in(t.edge[e][1]);
+    }
+    for (int k = 0; k < 3; ++k)
+      for (int side = 0; side < 2; ++side) {
+        const int a = 1 << k, sv = side ? a : 0;
+        int fe[4], nf = 0;  // crossing edges of the face
+        for (int e = 0; e < 12; ++e)
+          if ((t.edge[e][0] & a) == sv && (t.edge[e][1] & a) == sv && cross[e]) fe[nf++] = e;
+        int pairs[2][2], np = 0;
+        if (nf == 2) {
+          pairs[0][0] = fe[0];
+          pairs[0][1] = fe[1];
+          np = 1;
+        } else if (nf == 4) {  // ambiguous face: cut off each inside corner
+          for (int c = 0; c < 8; ++c) {
+            if ((c & a) != sv || !in(c)) continue;
+            int m = 0;
+            for (int q = 0; q < 4; ++q)
+              if (t.edge[fe[q]][0] == c || t.edge[fe[q]][1] == c) pairs[np][m++] = fe[q];
+            ++np;
+          }
+        }
+        for (int q = 0; q < np; ++q) {
+          const int e1 = pairs[q][0], e2 = pairs[q][1];
+          int m1[3], m2[3], n[3] = {0, 0, 0}, w[3];
+          const int cin = in(t.edge[e1][0]) ? t.edge[e1][0] : t.edge[e1][1];
+          for (int d = 0; d < 3; ++d) {
+            m1[d] = cc(t.edge[e1][0], d) + cc(t.edge[e1][1], d);
+            m2[d] = cc(t.edge[e2][0], d) + cc(t.edge[e2][1], d);
+            w[d] = 2 * cc(cin, d) - m1[d];
+          }
+          n[k] = side ? 1 : -1;  // the face's outward normal
+          const int dv[3] = {m2[0] - m1[0], m2[1] - m1[1], m2[2] - m1[2]};
+          const int lx = n[1] * dv[2] - n[2] * dv[1], ly = n[2] * dv[0] - n[0] * dv[2],
+                    lz = n[0] * dv[1] - n[1] * dv[0];
+          const bool left = lx * w[0] + ly * w[1] + lz * w[2] > 0;
+          if (left)  // keep the inside on the right
+            next[e2] = e1;
+          else
+            next[e1] = e2;
+        }
+      }
+    // faces holding edge e: bit 2 k + side for the two faces off its axis
+    auto fmask = [&](int e) {
+      const int lo = t.edge[e][0], ax = t.edge[e][1] ^ lo;
+      int m = 0;
+      for (int k = 0; k < 3; ++k)
+        if ((1 << k) != ax) m |= 1 << (2 * k + ((lo >> k) & 1));
+      return m;
+    };
+    bool seen[12] = {};
+    int nt = 0;
+    for (int e0 = 0; e0 < 12; ++e0) {
+      if (!cross[e0] || seen[e0]) continue;
+      int loop[12], nl = 0;
+      for (int e = e0; e >= 0 && !seen[e]; e = next[e]) {
+        seen[e] = true;
+        loop[nl++] = e;
+      }
+      // fan from the first vertex whose diagonals all leave the cube's faces:
+      // a diagonal inside a face would meet the neighbouring cube's
+      int s0 = 0;
+      for (int k = 0; k < nl; ++k) {
+        bool ok = true;
+        for (int q = 2; q + 1 < nl; ++q) ok = ok && !(fmask(loop[k]) & fmask(loop[(k + q) % nl]));
+        if (ok) {
+          s0 = k;
+          break;
+        }
+      }
+      for (int q = 1; q + 1 < nl; ++q) {
+        t.tri[cm][3 * nt] = (uint8_t)loop[s0];
+        t.tri[cm][3 * nt + 1] = (uint8_t)loop[(s0 + q) % nl];
+        t.tri[cm][3 * nt + 2] = (uint8_t)loop[(s0 + q + 1) % nl];
+        ++nt;
+      }
+    }
+    t.ntri[cm] = (uint8_t)nt;
+  }
+  return t;
+}
+
 struct NodeIdx {
   int i, j, k;
 };
@@ -306,6 +434,7 @@ struct ExtractArgs {
   const float *dens;
   float iso;
   int below;  // inside = value <= iso instead of >= iso
+  int mc;     // 1: marching cubes (axis-edge vertices, table triangles)
   int nx, ny, nz;
   int64_t nnode;
   float dx;
@@ -332,10 +461,10 @@ __global__ void __launch_bounds__(MB) k_mesh_count(ExtractArgs a) {
       const float vb = a.dens[n + off_of(b, a.ny, a.nz)];
       const int in = a.below ? vb <= a.iso : vb >= a.iso;
       cm |= in << b;
-      vm |= (in != in0) << b;
+      if (!a.mc || b == 1 || b == 2 || b == 4) vm |= (in != in0) << b;
     }
     if (!(hx && hy && hz)) cm = 0;  // not the lower corner of a cube
-    nt = (hx && hy && hz) ? cube_tris(cm) : 0;
+    nt = (hx && hy && hz) ? (a.mc ? c_mc.ntri[cm] : cube_tris(cm)) : 0;
     a.vmask[n] = (uint8_t)vm;
     a.cmask[n] = (uint8_t)cm;
   }
@@ -440,11 +569,19 @@ __device__ __forceinline__ int32_t edge_vertex(const ExtractArgs &a, int64_t n, 
 __global__ void __launch_bounds__(MB) k_mesh_temit(ExtractArgs a) {
   const int64_t n = blockIdx.x * (int64_t)MB + threadIdx.x;
   const int cm = n < a.nnode ? a.cmask[n] : 0;
-  const int nt = (cm != 0 && cm != 0xff) ? cube_tris(cm) : 0;
+  const int nt = (cm != 0 && cm != 0xff) ? (a.mc ? c_mc.ntri[cm] : cube_tris(cm)) : 0;
   int total;
   const int local = block_prefix(nt, &total);
   if (n >= a.nnode || nt == 0) return;
   int64_t w = a.sums[3 * (int64_t)a.nb + blockIdx.x] + local;
+  if (a.mc) {
+    int32_t *o = a.tris + 3 * w;
+    for (int q = 0; q < 3 * nt; ++q) {
+      const int e = c_mc.tri[cm][q];
+      o[q] = edge_vertex(a, n, c_mc.edge[e][0], c_mc.edge[e][1]);
+    }
+    return;
+  }
   for (int t = 0; t < 6; ++t) {
     int cs[4];
     tet_corners(t, cs);
@@ -709,6 +846,11 @@ int gf_mesher_create(int32_t nx, int32_t ny, int32_t nz, float dx, void *cuda_st
   if (e == cudaSuccess) e = cudaMalloc(&m->sums, (4 * (int64_t)m->nb + 2) * 8);
   if (e == cudaSuccess) e = cudaMallocHost(&m->tot_host, 2 * 8);
   if (e == cudaSuccess) e = cudaMemsetAsync(m->dens, 0, nnode * 4, m->stream);
+  if (e == cudaSuccess) {  // the case table, once per device (constant memory)
+    static const gfm::McTable table = gfm::build_mc_table();
+    e = cudaMemcpyToSymbolAsync(gfm::c_mc, &table, sizeof(table), 0, cudaMemcpyHostToDevice,
+                                m->stream);
+  }
   if (e != cudaSuccess) {
     gfm::release(m);
     delete m;
@@ -841,8 +983,9 @@ int gf_mesher_extract(void *mesher, const float *field, float iso_level, int64_t
     return GF_OK;
   }
   cudaStream_t st = m->stream;
-  gfm::ExtractArgs a{field ? field : m->dens, iso_level, m->below, m->nx, m->ny, m->nz, m->nnode,
-                     m->dx,
+  gfm::ExtractArgs a{field ? field : m->dens, iso_level, m->below,
+                     m->surface == GF_SURFACE_MARCHING_CUBES ? 1 : 0, m->nx, m->ny, m->nz,
+                     m->nnode, m->dx,
                      m->vmask, m->cmask, m->vbase, m->sums, m->nb, nullptr, nullptr};
   gfm::k_mesh_count<<<m->nb, gfm::MB, 0, st>>>(a);
   gfm::k_mesh_scan<<<2, gfm::SCAN_T, 0, st>>>(m->sums, m->nb);
@@ -875,6 +1018,24 @@ int gf_mesher_extract(void *mesher, const float *field, float iso_level, int64_t
   *n_verts = nv;
   *n_tris = nt;
   return gfm::check(m, cudaGetLastError(), "gf_mesher_extract emit");
+}
+
+int gf_marching_cubes_table(uint8_t *edges, uint8_t *ntri, uint8_t *tri) {
+  if (!edges || !ntri || !tri) return GF_INVALID_ARG;
+  static const gfm::McTable table = gfm::build_mc_table();
+  memcpy(edges, table.edge, sizeof(table.edge));
+  memcpy(ntri, table.ntri, sizeof(table.ntri));
+  memcpy(tri, table.tri, sizeof(table.tri));
+  return GF_OK;
+}
+
+int gf_mesher_set_surface(void *mesher, int32_t method) {
+  Mesher *m = reinterpret_cast<Mesher *>(mesher);
+  if (!m) return GF_INVALID_ARG;
+  if (method != GF_SURFACE_MARCHING_CUBES && method != GF_SURFACE_MARCHING_TETRAHEDRA)
+    return gfm::fail(m, GF_INVALID_ARG, "gf_mesher_set_surface: unknown method");
+  m->surface = method;
+  return GF_OK;
 }
 
 int gf_mesher_set_inside_below(void *mesher, int32_t below) {

@@ -10,8 +10,10 @@
 // Solvers:
 //   k_jacobi        one sweep of k3_jacobi_pressure (:878-938)
 //   k_gsrb          one colour of k3_gauss_seidel_rb (:1204-1267)
-//   k_pcg<Acc,REF>  the whole Jacobi-preconditioned CG of _pressure_pcg
-//                   (:2917-3043) in ONE persistent cooperative kernel: two
+//   k_pcg<Acc,REF,SGS>  the whole preconditioned CG of _pressure_pcg
+//                   (:2917-3043; the reference's Jacobi preconditioner, or with
+//                   SGS the tile-local symmetric Gauss-Seidel one of the
+//                   shared-memory solver) in ONE persistent cooperative kernel: two
 //                   grid barriers per iteration, dot products reduced
 //                   warp -> block -> fixed-order last-block sum (deterministic),
 //                   convergence decided on the device.  REF=true adds FP64
@@ -338,7 +340,59 @@ struct PcgArgs {
   double replace2; // residual-replacement factor^2 (refined)
   float sign;      // b = sign * div
   int only_if_fallback;  // run only when the shared-memory solver deferred
+  int sgs;         // tile-local symmetric Gauss-Seidel sweeps (SGS instantiation)
 };
+
+// ---- tile-local symmetric Gauss-Seidel preconditioner of the global-memory
+// PCG: z = M^-1 r with M^-1 = `sgs` red-black symmetric Gauss-Seidel sweeps
+// on each 8^3 tile from z = r / D, the tile's neighbours held at zero (the
+// diagonal block of A per tile: symmetric positive definite, so CG applies).
+// The same preconditioner as the shared-memory solver's.  A block takes
+// SGS_TB tiles per round: each thread owns local cell `tid` of every tile of
+// the round for the update, then the half-sweeps run in shared memory on
+// 10^3 padded boxes whose one-cell ring stays zero.
+constexpr int SGS_TB = 4;
+struct SgsSmem {
+  float zb[SGS_TB * 1000];
+  float r[SGS_TB * 512];
+  uint16_t code[SGS_TB * 512];
+};
+
+__device__ __forceinline__ int tile_pad(int l) {
+  return ((l >> 6) + 1) * 100 + (((l >> 3) & 7) + 1) * 10 + ((l & 7) + 1);
+}
+__device__ __forceinline__ float sgs_factor(unsigned code) {  // 1 / max(D, 1) on fluid, else 0
+  return (code & CODE_FLUID) ? 1.0f / fmaxf((float)((code >> CODE_DIAG_SHIFT) & 7), 1.0f) : 0.0f;
+}
+// z = (r + the in-tile fluid neighbours' z) / D on colour c of the round's
+// tiles (thread t: the (t & 255)-th cell of the colour in tiles t >> 8, +2).
+__device__ __forceinline__ void sgs_half(SgsSmem &S, int c) {
+  const int k = threadIdx.x & 255;
+  const int li = k >> 5, lj = (k >> 2) & 7, lk = 2 * (k & 3) + ((li + lj + c) & 1);
+  const int lc = (li * 8 + lj) * 8 + lk, pc = tile_pad(lc);
+  for (int m = threadIdx.x >> 8; m < SGS_TB; m += PCG_THREADS / 256) {
+    float *zp = S.zb + m * 1000 + pc;
+    float acc = S.r[m * 512 + lc];
+    acc = acc + zp[-100];
+    acc = acc + zp[100];
+    acc = acc + zp[-10];
+    acc = acc + zp[10];
+    acc = acc + zp[-1];
+    acc = acc + zp[1];
+    *zp = acc * sgs_factor(S.code[m * 512 + lc]);
+  }
+}
+// After the round's r and code are in S (and z = r / D in the boxes): the
+// sweeps; the caller then reads z of its cells from S.zb.
+__device__ __forceinline__ void sgs_sweeps(SgsSmem &S, int sweeps) {
+  __syncthreads();
+  for (int sw = 0; sw < sweeps; ++sw) {
+    sgs_half(S, 1);
+    __syncthreads();
+    sgs_half(S, 0);
+    __syncthreads();
+  }
+}
 
 template <typename T>
 __device__ __forceinline__ T block_sum(T v, T *sh) {
@@ -433,9 +487,15 @@ __device__ bool grid_barrier(const PcgArgs &a) {
   return grid_reduce<double, 1>(a, v, [](double *) {});
 }
 
-template <typename Acc, bool REF>
+template <typename Acc, bool REF, bool SGS>
 __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
   if (a.only_if_fallback && !ld_volatile_i(&a.st->fallback)) return;
+  __shared__ alignas(16) unsigned char sgs_raw[SGS ? sizeof(SgsSmem) : 16];
+  SgsSmem &S = *reinterpret_cast<SgsSmem *>(sgs_raw);  // boxes of the SGS instantiation
+  const int na = *a.n_active;
+  if (SGS) {  // the boxes' rings stay zero for the whole solve
+    for (int q = threadIdx.x; q < SGS_TB * 1000; q += blockDim.x) S.zb[q] = 0.f;
+  }
   const int64_t total = (int64_t)(*a.n_active) * TILE_CELLS;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const int64_t q0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -450,16 +510,44 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
   // ---- init: x = 0, r = b, z = M^-1 r, d = 0 (so the first d = z)
   {
     Acc v[2] = {0, 0};
-    for (int64_t q = q0; q < total; q += stride) {
-      const uint16_t code = a.code[q];
-      if (!(code & CODE_FLUID)) continue;
-      const float b = a.sign * a.bdiv[q];
-      const float diag = fmaxf((float)((code >> CODE_DIAG_SHIFT) & 7), 1.0f);
-      const float z = b / diag;
-      a.r[q] = b;
-      a.z[q] = z;
-      v[0] += (Acc)(b * z);
-      v[1] += (Acc)(b * b);
+    if (SGS) {
+      const int tid = threadIdx.x;
+      for (int base = blockIdx.x * SGS_TB; base < na; base += gridDim.x * SGS_TB) {
+        float bb[SGS_TB];
+#pragma unroll
+        for (int m = 0; m < SGS_TB; ++m) {
+          const int64_t q = (int64_t)(base + m) * 512 + tid;
+          const uint16_t code = base + m < na ? CODE[q] : (uint16_t)0;
+          bb[m] = (code & CODE_FLUID) ? a.sign * a.bdiv[q] : 0.0f;
+          if (code & CODE_FLUID) a.r[q] = bb[m];
+          S.r[m * 512 + tid] = bb[m];
+          S.code[m * 512 + tid] = code;
+          S.zb[m * 1000 + tile_pad(tid)] = bb[m] * sgs_factor(code);
+        }
+        sgs_sweeps(S, a.sgs);
+#pragma unroll
+        for (int m = 0; m < SGS_TB; ++m) {
+          if (!(S.code[m * 512 + tid] & CODE_FLUID)) continue;
+          const int64_t q = (int64_t)(base + m) * 512 + tid;
+          const float z = S.zb[m * 1000 + tile_pad(tid)];
+          a.z[q] = z;
+          v[0] += (Acc)(bb[m] * z);
+          v[1] += (Acc)(bb[m] * bb[m]);
+        }
+        __syncthreads();
+      }
+    } else {
+      for (int64_t q = q0; q < total; q += stride) {
+        const uint16_t code = a.code[q];
+        if (!(code & CODE_FLUID)) continue;
+        const float b = a.sign * a.bdiv[q];
+        const float diag = fmaxf((float)((code >> CODE_DIAG_SHIFT) & 7), 1.0f);
+        const float z = b / diag;
+        a.r[q] = b;
+        a.z[q] = z;
+        v[0] += (Acc)(b * z);
+        v[1] += (Acc)(b * b);
+      }
     }
     if (!grid_reduce<Acc, 2>(a, v, [&](double *t) {
           st->rz = t[0];
@@ -538,6 +626,49 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
       const float alpha = (float)ld_volatile_d(&st->alpha);
       const float nalpha = -alpha;
       Acc v[2] = {0, 0};
+      if (SGS) {
+        const int tid = threadIdx.x;
+        for (int base = blockIdx.x * SGS_TB; base < na; base += gridDim.x * SGS_TB) {
+          uint16_t cd[SGS_TB];
+          float dd[SGS_TB], xx[SGS_TB], rr[SGS_TB], aa[SGS_TB];
+#pragma unroll
+          for (int m = 0; m < SGS_TB; ++m) {
+            const int64_t q = (int64_t)(base + m) * 512 + tid;
+            cd[m] = base + m < na ? CODE[q] : (uint16_t)0;
+            dd[m] = xx[m] = rr[m] = aa[m] = 0.0f;
+            if (!(cd[m] & CODE_FLUID)) continue;
+            dd[m] = __ldcg(dnew + q);
+            xx[m] = __ldcg(X + q);
+            rr[m] = __ldcg(R + q);
+            aa[m] = __ldcg(AD + q);
+          }
+#pragma unroll
+          for (int m = 0; m < SGS_TB; ++m) {
+            const int64_t q = (int64_t)(base + m) * 512 + tid;
+            float rn = 0.0f;
+            if (cd[m] & CODE_FLUID) {
+              X[q] = xx[m] + alpha * dd[m];
+              rn = rr[m] + nalpha * aa[m];
+              R[q] = rn;
+            }
+            rr[m] = rn;
+            S.r[m * 512 + tid] = rn;
+            S.code[m * 512 + tid] = cd[m];
+            S.zb[m * 1000 + tile_pad(tid)] = rn * sgs_factor(cd[m]);
+          }
+          sgs_sweeps(S, a.sgs);
+#pragma unroll
+          for (int m = 0; m < SGS_TB; ++m) {
+            if (!(cd[m] & CODE_FLUID)) continue;
+            const int64_t q = (int64_t)(base + m) * 512 + tid;
+            const float z = S.zb[m * 1000 + tile_pad(tid)];
+            Z[q] = z;
+            v[0] += (Acc)(rr[m] * z);
+            v[1] += (Acc)(rr[m] * rr[m]);
+          }
+          __syncthreads();
+        }
+      } else
       for (int64_t qb = q0; qb < total; qb += KQ * stride) {
         uint16_t cd[KQ];
         float dd[KQ], xx[KQ], rr[KQ], aa[KQ];
@@ -606,22 +737,58 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
       }
       if (!grid_barrier(a)) return;
       double v[3] = {0, 0, 0};
-      for (int64_t q = q0; q < total; q += stride) {
-        const uint16_t code = a.code[q];
-        if (!(code & CODE_FLUID)) continue;
+      auto residual = [&](int64_t q, uint16_t code) {  // b - A x64 in FP64
         double s = 0.0;
 #pragma unroll
         for (int d = 0; d < 6; ++d)
           if (code & (1 << d)) s += __ldcg(a.x64 + nb_index(q, d, a.nbr));
         const double diag = (double)((code >> CODE_DIAG_SHIFT) & 7);
-        const double res = (double)(a.sign * a.bdiv[q]) - (diag * __ldcg(a.x64 + q) - s);
-        const float rf = (float)res;
-        const float z = rf / fmaxf((float)diag, 1.0f);
-        a.r[q] = rf;
-        a.z[q] = z;
-        v[0] += res * res;
-        v[1] += (double)(rf * z);
-        v[2] += (double)(rf * rf);
+        return (double)(a.sign * a.bdiv[q]) - (diag * __ldcg(a.x64 + q) - s);
+      };
+      if (SGS) {
+        const int tid = threadIdx.x;
+        for (int base = blockIdx.x * SGS_TB; base < na; base += gridDim.x * SGS_TB) {
+          float rf[SGS_TB];
+#pragma unroll
+          for (int m = 0; m < SGS_TB; ++m) {
+            const int64_t q = (int64_t)(base + m) * 512 + tid;
+            const uint16_t code = base + m < na ? CODE[q] : (uint16_t)0;
+            rf[m] = 0.0f;
+            if (code & CODE_FLUID) {
+              const double res = residual(q, code);
+              rf[m] = (float)res;
+              a.r[q] = rf[m];
+              v[0] += res * res;
+            }
+            S.r[m * 512 + tid] = rf[m];
+            S.code[m * 512 + tid] = code;
+            S.zb[m * 1000 + tile_pad(tid)] = rf[m] * sgs_factor(code);
+          }
+          sgs_sweeps(S, a.sgs);
+#pragma unroll
+          for (int m = 0; m < SGS_TB; ++m) {
+            if (!(S.code[m * 512 + tid] & CODE_FLUID)) continue;
+            const int64_t q = (int64_t)(base + m) * 512 + tid;
+            const float z = S.zb[m * 1000 + tile_pad(tid)];
+            a.z[q] = z;
+            v[1] += (double)(rf[m] * z);
+            v[2] += (double)(rf[m] * rf[m]);
+          }
+          __syncthreads();
+        }
+      } else {
+        for (int64_t q = q0; q < total; q += stride) {
+          const uint16_t code = a.code[q];
+          if (!(code & CODE_FLUID)) continue;
+          const double res = residual(q, code);
+          const float rf = (float)res;
+          const float z = rf / fmaxf((float)((code >> CODE_DIAG_SHIFT) & 7), 1.0f);
+          a.r[q] = rf;
+          a.z[q] = z;
+          v[0] += res * res;
+          v[1] += (double)(rf * z);
+          v[2] += (double)(rf * rf);
+        }
       }
       if (!grid_reduce<double, 3>(a, v, [&](double *t) {
             st->r_true2 = t[0];
@@ -1237,10 +1404,10 @@ void pressure_free(Ctx *c) {
   if (c->state_host) cudaFreeHost(c->state_host);
 }
 
-template <typename Acc, bool REF>
+template <typename Acc, bool REF, bool SGS>
 static int coop_grid(Ctx *c) {
   int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg<Acc, REF>,
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg<Acc, REF, SGS>,
                                                                 PCG_THREADS, 0);
   if (e != cudaSuccess || per_sm < 1) return 0;
   if (c->tune.pcg_blocks_per_sm > 0 && c->tune.pcg_blocks_per_sm < per_sm)
@@ -1249,16 +1416,21 @@ static int coop_grid(Ctx *c) {
   return g > MAX_PCG_BLOCKS ? MAX_PCG_BLOCKS : g;
 }
 
-template <typename Acc, bool REF>
-static int launch_pcg(Ctx *c, PcgArgs &pa) {
-  int g = coop_grid<Acc, REF>(c);
+template <typename Acc, bool REF, bool SGS>
+static int launch_pcg_t(Ctx *c, PcgArgs &pa) {
+  int g = coop_grid<Acc, REF, SGS>(c);
   if (g < 1) return fail(c, GF_CUDA_ERROR, "PCG: cooperative occupancy query failed");
   void *args[] = {&pa};
-  int e = check_cuda(c, cudaLaunchCooperativeKernel((const void *)k_pcg<Acc, REF>, dim3(g),
+  int e = check_cuda(c, cudaLaunchCooperativeKernel((const void *)k_pcg<Acc, REF, SGS>, dim3(g),
                                                     dim3(PCG_THREADS), args, 0, c->stream),
                      "cooperative PCG launch");
   c->launches++;
   return e;
+}
+
+template <typename Acc, bool REF>
+static int launch_pcg(Ctx *c, PcgArgs &pa) {
+  return pa.sgs > 0 ? launch_pcg_t<Acc, REF, true>(c, pa) : launch_pcg_t<Acc, REF, false>(c, pa);
 }
 
 template <typename Acc, bool REF>
@@ -1457,7 +1629,7 @@ int launch_pressure(Ctx *c, const gf_step_params *prm) {
     PcgArgs pa{c->n_active, c->tile_nbr, c->code, c->bdiv, c->xf, c->r, c->z, c->d0, c->d1,
                c->Ad, refined ? c->x64 : nullptr, c->partials, c->state,
                prm->max_iters, check_every, prm->tol * prm->tol, replace2, sign,
-               force_global ? 0 : 1};
+               force_global ? 0 : 1, (prm->flags & GF_FLAG_SGS_MASK) >> GF_FLAG_SGS_SHIFT};
     if (refined) {
       e = launch_pcg<double, true>(c, pa);
       result64 = c->x64;

@@ -28,6 +28,12 @@ namespace gf {
 // the normal axis spans [O, O+8] (9 faces), the transverse axes [O-1, O+8]
 // (10 faces).
 constexpr int BOX_N = 9, BOX_T = 10, BOX = BOX_N * BOX_T * BOX_T;  // 900
+// Type of the shared-memory face sums of a tile (the sums are rounded to
+// float32 once, at the flush).
+#ifndef GF_P2G_ACC
+#define GF_P2G_ACC float
+#endif
+using P2G_ACC = GF_P2G_ACC;
 
 struct P2GArgs {
   const int32_t *start;
@@ -40,8 +46,8 @@ struct P2GArgs {
 // Scatter one face component of one particle into the shared box of `comp`
 // (0 u, 1 v, 2 w).  APIC adds C_row . (x_face - x_p) with world face
 // positions (:1510-1588).
-template <bool APIC>
-__device__ __forceinline__ void scatter_comp(float *s_val, float *s_wt, int comp, float vp,
+template <bool APIC, typename T>
+__device__ __forceinline__ void scatter_comp(T *s_val, T *s_wt, int comp, float vp,
                                              float c0, float c1, float c2, float px, float py,
                                              float pz, float fx, float fy, float fz, int I0,
                                              int J0, int K0, const P2GArgs &a, float *gval,
@@ -81,8 +87,8 @@ __device__ __forceinline__ void scatter_comp(float *s_val, float *s_wt, int comp
           int bx = ii - bx0, by = jj - by0, bz = kk - bz0;
           if (bx >= 0 && bx < ex && by >= 0 && by < ey && bz >= 0 && bz < ez) {
             int e = (bx * ey + by) * ez + bz;
-            atomicAdd(&s_val[e], add);
-            atomicAdd(&s_wt[e], wt);
+            atomicAdd(&s_val[e], (T)add);
+            atomicAdd(&s_wt[e], (T)wt);
           } else {  // only reachable for positions outside their clamped cell
             int64_t g = ((int64_t)ii * sny + jj) * snz + kk;
             atomicAdd(&gval[g], add);
@@ -92,14 +98,73 @@ __device__ __forceinline__ void scatter_comp(float *s_val, float *s_wt, int comp
       }
 }
 
+// The common case of scatter_comp: the particle's 2x2x2 stencil lies inside
+// the grid and inside the tile's box, so no corner needs a bounds check.  The
+// per-axis factors are formed once -- weights (1-s, s), and for APIC the
+// affine terms vp + c0 ox, c1 oy, c2 oz at both corners of each axis (ox one
+// dx apart) -- and each corner costs two products, two adds and the two
+// shared-memory adds.  The sums are tolerance-checked (their order is the
+// atomics' anyway), so the factors use fused multiply-adds.  Returns false,
+// touching nothing, when the stencil does not fit (scatter_comp then runs).
+template <bool APIC, typename T>
+__device__ __forceinline__ bool scatter_comp_fast(T *s_val, T *s_wt, int comp, float vp,
+                                                  float c0, float c1, float c2, float px,
+                                                  float py, float pz, float fx, float fy,
+                                                  float fz, int I0, int J0, int K0,
+                                                  const P2GArgs &a) {
+  const int snx = a.nx + (comp == 0), sny = a.ny + (comp == 1), snz = a.nz + (comp == 2);
+  const int i0 = __float2int_rz(floorf(fx)), j0 = __float2int_rz(floorf(fy)),
+            k0 = __float2int_rz(floorf(fz));
+  const int ey = comp == 1 ? BOX_N : BOX_T, ez = comp == 2 ? BOX_N : BOX_T;
+  const int ex = comp == 0 ? BOX_N : BOX_T;
+  const int bx = i0 - (comp == 0 ? I0 : I0 - 1), by = j0 - (comp == 1 ? J0 : J0 - 1),
+            bz = k0 - (comp == 2 ? K0 : K0 - 1);
+  if (!(i0 >= 0 && i0 + 1 < snx && j0 >= 0 && j0 + 1 < sny && k0 >= 0 && k0 + 1 < snz &&
+        bx >= 0 && bx + 1 < ex && by >= 0 && by + 1 < ey && bz >= 0 && bz + 1 < ez))
+    return false;
+  const float sx = fx - (float)i0, sy = fy - (float)j0, sz = fz - (float)k0;
+  const float wx[2] = {1.0f - sx, sx}, wy[2] = {1.0f - sy, sy}, wz[2] = {1.0f - sz, sz};
+  float A[2] = {vp, vp}, B[2] = {0.f, 0.f}, C[2] = {0.f, 0.f};
+  if (APIC) {
+    const float dx = a.dx;
+    const float ox = ((float)i0 + (comp == 0 ? 0.0f : 0.5f)) * dx - px;
+    const float oy = ((float)j0 + (comp == 1 ? 0.0f : 0.5f)) * dx - py;
+    const float oz = ((float)k0 + (comp == 2 ? 0.0f : 0.5f)) * dx - pz;
+    A[0] = __fmaf_rn(c0, ox, vp);
+    A[1] = __fmaf_rn(c0, dx, A[0]);
+    B[0] = c1 * oy;
+    B[1] = __fmaf_rn(c1, dx, B[0]);
+    C[0] = c2 * oz;
+    C[1] = __fmaf_rn(c2, dx, C[0]);
+  }
+  const int base = (bx * ey + by) * ez + bz;
+#pragma unroll
+  for (int di = 0; di < 2; ++di)
+#pragma unroll
+    for (int dj = 0; dj < 2; ++dj) {
+      const float wxy = wx[di] * wy[dj];
+      const float ab = A[di] + B[dj];
+#pragma unroll
+      for (int dk = 0; dk < 2; ++dk) {
+        const float wt = wxy * wz[dk];
+        const float val = ab + C[dk];
+        const int e = base + (di * ey + dj) * ez + dk;
+        atomicAdd(&s_val[e], (T)(val * wt));
+        atomicAdd(&s_wt[e], (T)wt);
+      }
+    }
+  return true;
+}
+
 // Flush a tile's shared box: faces that only this tile's particles reach are
 // stored, the shared halo band is accumulated atomically; exact zeros are
 // skipped (the destination was zeroed before the launch).
-__device__ __forceinline__ void p2g_flush_box(const P2GArgs &a, float (*s_val)[BOX],
-                                              float (*s_wt)[BOX], int I0, int J0, int K0) {
+template <typename T>
+__device__ __forceinline__ void p2g_flush_box(const P2GArgs &a, T (*s_val)[BOX],
+                                              T (*s_wt)[BOX], int I0, int J0, int K0) {
   for (int q = threadIdx.x; q < 3 * BOX; q += blockDim.x) {
     int comp = q / BOX, e2 = q - comp * BOX;
-    float val = s_val[comp][e2], wt = s_wt[comp][e2];
+    float val = (float)s_val[comp][e2], wt = (float)s_wt[comp][e2];
     if (val == 0.f && wt == 0.f) continue;
     int ey = comp == 1 ? BOX_N : BOX_T, ez = comp == 2 ? BOX_N : BOX_T;
     int bx = e2 / (ey * ez), by = (e2 / ez) % ey, bz = e2 % ez;
@@ -126,15 +191,15 @@ __device__ __forceinline__ void p2g_flush_box(const P2GArgs &a, float (*s_val)[B
 
 // One tile's P2G: t is the tile within its grid (its coordinates), key0 the
 // sort key of its first cell (t * 512 for a single grid).
-template <bool APIC>
+template <bool APIC, typename T = P2G_ACC>
 __device__ __forceinline__ void p2g_tile_body(const P2GArgs &a, int t, int64_t key0) {
-  __shared__ float s_val[3][BOX];
-  __shared__ float s_wt[3][BOX];
+  __shared__ T s_val[3][BOX];
+  __shared__ T s_wt[3][BOX];
   const int64_t b = a.start[key0], e = a.start[key0 + TILE_CELLS];
   if (b == e) return;
   for (int q = threadIdx.x; q < 3 * BOX; q += blockDim.x) {
-    (&s_val[0][0])[q] = 0.f;
-    (&s_wt[0][0])[q] = 0.f;
+    (&s_val[0][0])[q] = (T)0;
+    (&s_wt[0][0])[q] = (T)0;
   }
   __syncthreads();
   const int ti = t / (a.nty * a.ntz), tj = (t / a.ntz) % a.nty, tk = t % a.ntz;
@@ -158,15 +223,21 @@ __device__ __forceinline__ void p2g_tile_body(const P2GArgs &a, int t, int64_t k
     float gx = __fdiv_rn(r0.x, a.dx), gy = __fdiv_rn(r0.y, a.dx), gz = __fdiv_rn(r0.z, a.dx);
     float hx = gx - 0.5f, hy = gy - 0.5f, hz = gz - 0.5f;
     // C rows: (r1.w, r2.x, r2.y) (r2.z, r2.w, r3.x) (r3.y, r3.z, r3.w)
-    scatter_comp<APIC>(s_val[0], s_wt[0], 0, r1.x, r1.w, r2.x, r2.y, r0.x, r0.y, r0.z, gx, hy, hz,
-                       I0, J0, K0, a, a.u, a.uw);
-    scatter_comp<APIC>(s_val[1], s_wt[1], 1, r1.y, r2.z, r2.w, r3.x, r0.x, r0.y, r0.z, hx, gy, hz,
-                       I0, J0, K0, a, a.v, a.vw);
-    scatter_comp<APIC>(s_val[2], s_wt[2], 2, r1.z, r3.y, r3.z, r3.w, r0.x, r0.y, r0.z, hx, hy, gz,
-                       I0, J0, K0, a, a.w, a.ww);
+    if (!scatter_comp_fast<APIC, T>(s_val[0], s_wt[0], 0, r1.x, r1.w, r2.x, r2.y, r0.x, r0.y,
+                                    r0.z, gx, hy, hz, I0, J0, K0, a))
+      scatter_comp<APIC, T>(s_val[0], s_wt[0], 0, r1.x, r1.w, r2.x, r2.y, r0.x, r0.y, r0.z, gx,
+                            hy, hz, I0, J0, K0, a, a.u, a.uw);
+    if (!scatter_comp_fast<APIC, T>(s_val[1], s_wt[1], 1, r1.y, r2.z, r2.w, r3.x, r0.x, r0.y,
+                                    r0.z, hx, gy, hz, I0, J0, K0, a))
+      scatter_comp<APIC, T>(s_val[1], s_wt[1], 1, r1.y, r2.z, r2.w, r3.x, r0.x, r0.y, r0.z, hx,
+                            gy, hz, I0, J0, K0, a, a.v, a.vw);
+    if (!scatter_comp_fast<APIC, T>(s_val[2], s_wt[2], 2, r1.z, r3.y, r3.z, r3.w, r0.x, r0.y,
+                                    r0.z, hx, hy, gz, I0, J0, K0, a))
+      scatter_comp<APIC, T>(s_val[2], s_wt[2], 2, r1.z, r3.y, r3.z, r3.w, r0.x, r0.y, r0.z, hx,
+                            hy, gz, I0, J0, K0, a, a.w, a.ww);
   }
   __syncthreads();
-  p2g_flush_box(a, s_val, s_wt, I0, J0, K0);
+  p2g_flush_box<T>(a, s_val, s_wt, I0, J0, K0);
 }
 
 template <bool APIC>
@@ -336,34 +407,53 @@ __device__ __forceinline__ float clampf(float x, float lo, float hi) {
   return x < lo ? lo : (x > hi ? hi : x);
 }
 
-// sample3, gridmath.py:29-63
-__device__ __forceinline__ float sample3(const float *__restrict__ f, float fx, float fy,
-                                         float fz, int nxm, int nym, int nzm) {
+// Face-array accessors of the G2P gathers: the array in global memory, or a
+// staged box of it in shared memory (origin oi, oj, ok; nj x nk per i-plane).
+struct GlobalAt {
+  const float *__restrict__ f;
+  int64_t si, sj;
+  __device__ __forceinline__ float operator()(int i, int j, int k) const {
+    return __ldg(f + (int64_t)i * si + (int64_t)j * sj + k);
+  }
+};
+struct BoxAt {
+  const float *s;
+  int oi, oj, ok, nj, nk;
+  __device__ __forceinline__ float operator()(int i, int j, int k) const {
+    return s[((i - oi) * nj + (j - oj)) * nk + (k - ok)];
+  }
+};
+
+// sample3, gridmath.py:29-63 (clamped coordinates, clamped indices).
+__device__ __forceinline__ void sample3_index(float &fx, float &fy, float &fz, int nxm, int nym,
+                                              int nzm, int &i0, int &j0, int &k0, int &i1,
+                                              int &j1, int &k1) {
   fx = clampf(fx, 0.0f, (float)nxm);
   fy = clampf(fy, 0.0f, (float)nym);
   fz = clampf(fz, 0.0f, (float)nzm);
-  int i0 = __float2int_rz(floorf(fx)), j0 = __float2int_rz(floorf(fy)),
-      k0 = __float2int_rz(floorf(fz));
+  i0 = __float2int_rz(floorf(fx)), j0 = __float2int_rz(floorf(fy)), k0 = __float2int_rz(floorf(fz));
   if (i0 >= nxm) i0 = nxm - 1;
   if (j0 >= nym) j0 = nym - 1;
   if (k0 >= nzm) k0 = nzm - 1;
   if (i0 < 0) i0 = 0;
   if (j0 < 0) j0 = 0;
   if (k0 < 0) k0 = 0;
-  int i1 = i0 + 1, j1 = j0 + 1, k1 = k0 + 1;
+  i1 = i0 + 1, j1 = j0 + 1, k1 = k0 + 1;
   if (i1 >= nxm) i1 = nxm - 1;
   if (j1 >= nym) j1 = nym - 1;
   if (k1 >= nzm) k1 = nzm - 1;
+}
+
+template <class F>
+__device__ __forceinline__ float sample3_at(const F &at, float fx, float fy, float fz, int i0,
+                                            int j0, int k0, int i1, int j1, int k1) {
   float sx = clampf(fx - (float)i0, 0.0f, 1.0f);
   float sy = clampf(fy - (float)j0, 0.0f, 1.0f);
   float sz = clampf(fz - (float)k0, 0.0f, 1.0f);
-  const int64_t sI = (int64_t)nym * nzm;
-  const int64_t b00 = i0 * sI + (int64_t)j0 * nzm, b10 = i1 * sI + (int64_t)j0 * nzm,
-                b01 = i0 * sI + (int64_t)j1 * nzm, b11 = i1 * sI + (int64_t)j1 * nzm;
-  float c000 = __ldg(f + b00 + k0), c100 = __ldg(f + b10 + k0);
-  float c010 = __ldg(f + b01 + k0), c110 = __ldg(f + b11 + k0);
-  float c001 = __ldg(f + b00 + k1), c101 = __ldg(f + b10 + k1);
-  float c011 = __ldg(f + b01 + k1), c111 = __ldg(f + b11 + k1);
+  float c000 = at(i0, j0, k0), c100 = at(i1, j0, k0);
+  float c010 = at(i0, j1, k0), c110 = at(i1, j1, k0);
+  float c001 = at(i0, j0, k1), c101 = at(i1, j0, k1);
+  float c011 = at(i0, j1, k1), c111 = at(i1, j1, k1);
   float ox = 1.0f - sx, oy = 1.0f - sy, oz = 1.0f - sz;
   float c00 = c000 * ox + c100 * sx;
   float c10 = c010 * ox + c110 * sx;
@@ -374,12 +464,20 @@ __device__ __forceinline__ float sample3(const float *__restrict__ f, float fx, 
   return c0 * oz + c1 * sz;
 }
 
+__device__ __forceinline__ float sample3(const float *__restrict__ f, float fx, float fy,
+                                         float fz, int nxm, int nym, int nzm) {
+  int i0, j0, k0, i1, j1, k1;
+  sample3_index(fx, fy, fz, nxm, nym, nzm, i0, j0, k0, i1, j1, k1);
+  return sample3_at(GlobalAt{f, (int64_t)nym * nzm, nzm}, fx, fy, fz, i0, j0, k0, i1, j1, k1);
+}
+
 // One face component of k3_g2p_apic_advect (:1626-1724): clamped-index
 // gather of velocity and of the C row.
-__device__ __forceinline__ void apic_gather(const float *__restrict__ f, float px, float py,
-                                            float pz, float dx, float fx, float fy, float fz,
-                                            int snx, int sny, int snz, int ax, float inv,
-                                            float &vel, float &c0, float &c1, float &c2) {
+template <class F>
+__device__ __forceinline__ void apic_gather_at(const F &at, float px, float py, float pz,
+                                               float dx, float fx, float fy, float fz, int snx,
+                                               int sny, int snz, int ax, float inv, float &vel,
+                                               float &c0, float &c1, float &c2) {
   int i0 = __float2int_rz(floorf(fx)), j0 = __float2int_rz(floorf(fy)),
       k0 = __float2int_rz(floorf(fz));
   float sx = fx - (float)i0, sy = fy - (float)j0, sz = fz - (float)k0;
@@ -405,7 +503,7 @@ __device__ __forceinline__ void apic_gather(const float *__restrict__ f, float p
         float wzi = dk == 0 ? 1.0f - sz : sz;
         float wt = wxi * wyi;
         wt = wt * wzi;
-        float val = __ldg(f + ((int64_t)ii * sny + jj) * snz + kk);
+        float val = at(ii, jj, kk);
         float t = wt * val;
         acc = acc + t;
         float ox = ax == 0 ? (float)ii * dx - px : ((float)ii + 0.5f) * dx - px;
@@ -417,6 +515,14 @@ __device__ __forceinline__ void apic_gather(const float *__restrict__ f, float p
         c2 = c2 + fu * oz;
       }
   vel = acc;
+}
+
+__device__ __forceinline__ void apic_gather(const float *__restrict__ f, float px, float py,
+                                            float pz, float dx, float fx, float fy, float fz,
+                                            int snx, int sny, int snz, int ax, float inv,
+                                            float &vel, float &c0, float &c1, float &c2) {
+  apic_gather_at(GlobalAt{f, (int64_t)sny * snz, snz}, px, py, pz, dx, fx, fy, fz, snx, sny, snz,
+                 ax, inv, vel, c0, c1, c2);
 }
 
 struct G2PArgs {
@@ -475,6 +581,320 @@ __global__ void __launch_bounds__(512) k_g2p(G2PArgs a) {
   int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (q >= a.n) return;
   g2p_particle<APIC>(a, q);
+}
+
+// ------------------------------------------------------- G2P, tile-staged
+// k_g2p_tile: one CTA per 8x8x8 tile of the cell-sorted particles.  The faces
+// the tile's particles can gather -- per component a box of 9 faces on its
+// normal axis and 10 on the transverse axes around the tile -- are staged in
+// shared memory first: by TMA (cp.async.bulk.tensor, completion on an
+// mbarrier) for every face array whose layout admits a tensor map, by plain
+// loads for the others.  The gathers then read shared memory, and the
+// outputs (positions, velocities, C, ids; AoS) go through a shared staging
+// buffer so that each warp writes whole cache lines with 16-byte stores.
+// The arithmetic is that of k_g2p, operation for operation.
+//
+// Box of component c (0 u, 1 v, 2 w) at tile origin (I0, J0, K0), in face
+// indices: i from oi = I0 - (c != 0) over gbox_ni(c) planes, j from
+// oj = J0 - (c != 1) over gbox_nj(c) rows, k from ok over gbox_nk(c): u and v
+// need k in [K0-1, K0+8] and load [K0-4, K0+12), w needs [K0, K0+8] and loads
+// [K0, K0+12) -- the start and width of the innermost axis are multiples of
+// 16 bytes, as a tiled TMA copy requires.  Boxes start on 128-byte
+// boundaries; a set of three boxes (u, v, w) takes GBOX_SET floats.
+__host__ __device__ constexpr int gbox_ni(int c) { return c == 0 ? 9 : 10; }
+__host__ __device__ constexpr int gbox_nj(int c) { return c == 1 ? 9 : 10; }
+__host__ __device__ constexpr int gbox_nk(int c) { return c == 2 ? 12 : 16; }
+__host__ __device__ constexpr int gbox_vol(int c) { return gbox_ni(c) * gbox_nj(c) * gbox_nk(c); }
+__host__ __device__ constexpr int gbox_off(int c) { return c == 0 ? 0 : (c == 1 ? 1440 : 2880); }
+constexpr int GBOX_SET = 4096;
+static_assert(gbox_vol(0) == 1440 && gbox_vol(1) == 1440 && gbox_vol(2) == 1200, "boxes");
+static_assert(gbox_off(2) + gbox_vol(2) <= GBOX_SET, "box set");
+constexpr int G2P_TILE_THREADS = 256;
+constexpr long long G2P_WAIT_LIMIT = 1LL << 22;  // try_wait polls before giving up
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Tiled 3-D TMA load of one box into this CTA's shared memory (no multicast).
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int c0, int c1,
+                                            int c2, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// Copy n floats from shared memory to global memory: scalar stores up to the
+// first 16-byte boundary of dst, then 16-byte stores, then the scalar tail.
+__device__ __forceinline__ void store_run(float *dst, const float *src, int n) {
+  int head = (int)(((16u - (uint32_t)(reinterpret_cast<uintptr_t>(dst) & 15u)) & 15u) >> 2);
+  if (head > n) head = n;
+  const int tid = threadIdx.x;
+  if (tid < head) dst[tid] = src[tid];
+  const int nv = (n - head) >> 2;
+  float4 *d4 = reinterpret_cast<float4 *>(dst + head);
+  const float *s4 = src + head;
+  for (int v = tid; v < nv; v += G2P_TILE_THREADS)
+    d4[v] = make_float4(s4[4 * v], s4[4 * v + 1], s4[4 * v + 2], s4[4 * v + 3]);
+  for (int q = head + 4 * nv + tid; q < n; q += G2P_TILE_THREADS) dst[q] = src[q];
+}
+
+struct G2PTileArgs {
+  G2PArgs g;
+  const int32_t *start;
+  int nty, ntz;
+  int32_t *wait_err;  // incremented when the box loads do not complete in time
+};
+
+// True when the clamped gather indices [lo, hi] of every axis lie inside the
+// component's box (always, for a particle inside its binned cell; a particle
+// outside the grid or with a non-finite position takes the global path).
+__device__ __forceinline__ bool in_box(const BoxAt &b, int ni, int i0, int i1, int j0, int j1,
+                                       int k0, int k1) {
+  return i0 >= b.oi && i1 < b.oi + ni && j0 >= b.oj && j1 < b.oj + b.nj && k0 >= b.ok &&
+         k1 < b.ok + b.nk;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(G2P_TILE_THREADS)
+    k_g2p_tile(const G2PTileArgs ta, const __grid_constant__ FaceMaps fm) {
+  constexpr bool APIC = MODE == GF_APIC;
+  constexpr int NARR = APIC ? 3 : 6;  // u, v, w (+ us, vs, ws for the FLIP delta)
+  constexpr int OUTF = APIC ? 4096 : 1792;  // staging: pos 768, vel 768, [C 2304], pid 256
+  __shared__ alignas(128) float s_box[(NARR / 3) * GBOX_SET];
+  __shared__ alignas(16) float s_out[OUTF];
+  __shared__ alignas(8) uint64_t s_bar;
+  __shared__ int s_ok;
+  const G2PArgs &a = ta.g;
+  const int t = blockIdx.x, tid = threadIdx.x;
+  const int64_t b = ta.start[(int64_t)t * TILE_CELLS], e = ta.start[(int64_t)t * TILE_CELLS + TILE_CELLS];
+  if (b == e) return;
+  const int ti = t / (ta.nty * ta.ntz), tj = (t / ta.ntz) % ta.nty, tk = t % ta.ntz;
+  const int I0 = ti * TILE, J0 = tj * TILE, K0 = tk * TILE;
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+
+  // ---- stage the boxes
+  uint32_t tx = 0;
+#pragma unroll
+  for (int q = 0; q < NARR; ++q)
+    if ((fm.mask >> q) & 1) tx += (uint32_t)gbox_vol(q % 3) * 4u;
+  if (tid == 0) {
+    s_ok = 1;
+    if (tx) {
+      mbar_init(&s_bar, 1);
+      mbar_init_fence();
+    }
+  }
+  __syncthreads();
+  if (tid == 0 && tx) {
+    mbar_expect_tx(&s_bar, tx);
+#pragma unroll
+    for (int q = 0; q < NARR; ++q) {
+      if (!((fm.mask >> q) & 1)) continue;
+      const int c = q % 3;
+      tma_load_3d(s_box + (q / 3) * GBOX_SET + gbox_off(c), &fm.m[q], c == 2 ? K0 : K0 - 4,
+                  J0 - (c != 1), I0 - (c != 0), &s_bar);
+    }
+  }
+  {
+    const float *src[6] = {a.u, a.v, a.w, a.us, a.vs, a.ws};
+#pragma unroll
+    for (int q = 0; q < NARR; ++q) {
+      if ((fm.mask >> q) & 1) continue;
+      const int c = q % 3;
+      const int snx = nx + (c == 0), sny = ny + (c == 1), snz = nz + (c == 2);
+      const int ni = gbox_ni(c), nj = gbox_nj(c), nk = gbox_nk(c);
+      const int oi = I0 - (c != 0), oj = J0 - (c != 1), ok = c == 2 ? K0 : K0 - 4;
+      float *dst = s_box + (q / 3) * GBOX_SET + gbox_off(c);
+      for (int v = tid; v < ni * nj * nk; v += G2P_TILE_THREADS) {
+        const int bk = v % nk, r = v / nk, bj = r % nj, bi = r / nj;
+        const int gi = oi + bi, gj = oj + bj, gk = ok + bk;
+        float val = 0.f;
+        if (gi >= 0 && gi < snx && gj >= 0 && gj < sny && gk >= 0 && gk < snz)
+          val = __ldg(src[q] + ((int64_t)gi * sny + gj) * snz + gk);
+        dst[v] = val;
+      }
+    }
+  }
+  if (tx) {  // every thread observes the completed phase (bounded wait)
+    long long spins = 0;
+    while (!mbar_try_wait(&s_bar, 0)) {
+      if (++spins > G2P_WAIT_LIMIT) {
+        s_ok = 0;
+        break;
+      }
+    }
+  }
+  __syncthreads();
+  if (!s_ok) {  // record it, give the copies in flight a second bounded wait, leave
+    if (tid == 0) {
+      atomicAdd(ta.wait_err, 1);
+      for (long long k = 0; k < G2P_WAIT_LIMIT && !mbar_try_wait(&s_bar, 0); ++k) {
+      }
+    }
+    __syncthreads();
+    return;
+  }
+
+  BoxAt bx[6];
+#pragma unroll
+  for (int q = 0; q < NARR; ++q) {
+    const int c = q % 3;
+    bx[q] = BoxAt{s_box + (q / 3) * GBOX_SET + gbox_off(c), I0 - (c != 0), J0 - (c != 1),
+                  c == 2 ? K0 : K0 - 4, gbox_nj(c), gbox_nk(c)};
+  }
+  const float dx = a.dx;
+  int *s_pid = reinterpret_cast<int *>(s_out + (APIC ? 3840 : 1536));
+  for (int64_t base = b; base < e; base += G2P_TILE_THREADS) {
+    const int m = (int)(e - base < G2P_TILE_THREADS ? e - base : G2P_TILE_THREADS);
+    if (tid < m) {
+      const int64_t q = base + tid;
+      const float4 r0 = a.rec0[q];
+      const float px = r0.x, py = r0.y, pz = r0.z;
+      float gx = __fdiv_rn(px, dx), gy = __fdiv_rn(py, dx), gz = __fdiv_rn(pz, dx);
+      float hx = gx - 0.5f, hy = gy - 0.5f, hz = gz - 0.5f;
+      float nu, nv, nw;
+      if (APIC) {
+        float dd = dx * dx;
+        float inv = __fdiv_rn(3.0f, dd);
+        float c[9];
+        const float fxs[3] = {gx, hx, hx}, fys[3] = {hy, gy, hy}, fzs[3] = {hz, hz, gz};
+        float vel3[3];
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+          const int snx = nx + (cc == 0), sny = ny + (cc == 1), snz = nz + (cc == 2);
+          const int i0 = __float2int_rz(floorf(fxs[cc])), j0 = __float2int_rz(floorf(fys[cc])),
+                    k0 = __float2int_rz(floorf(fzs[cc]));
+          auto cl = [](int v, int n) { return v < 0 ? 0 : (v > n - 1 ? n - 1 : v); };
+          if (in_box(bx[cc], gbox_ni(cc), cl(i0, snx), cl(i0 + 1, snx), cl(j0, sny),
+                     cl(j0 + 1, sny), cl(k0, snz), cl(k0 + 1, snz)))
+            apic_gather_at(bx[cc], px, py, pz, dx, fxs[cc], fys[cc], fzs[cc], snx, sny, snz, cc,
+                           inv, vel3[cc], c[3 * cc], c[3 * cc + 1], c[3 * cc + 2]);
+          else
+            apic_gather_at(GlobalAt{cc == 0 ? a.u : (cc == 1 ? a.v : a.w),
+                                    (int64_t)sny * snz, snz},
+                           px, py, pz, dx, fxs[cc], fys[cc], fzs[cc], snx, sny, snz, cc, inv,
+                           vel3[cc], c[3 * cc], c[3 * cc + 1], c[3 * cc + 2]);
+        }
+        nu = vel3[0];
+        nv = vel3[1];
+        nw = vel3[2];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) s_out[1536 + 9 * tid + k] = c[k];
+      } else {
+        const float4 r1 = a.rec1[q];
+        float pic[3], old[3];
+        const float fxs[3] = {gx, hx, hx}, fys[3] = {hy, gy, hy}, fzs[3] = {hz, hz, gz};
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+          const int snx = nx + (cc == 0), sny = ny + (cc == 1), snz = nz + (cc == 2);
+          float fx = fxs[cc], fy = fys[cc], fz = fzs[cc];
+          int i0, j0, k0, i1, j1, k1;
+          sample3_index(fx, fy, fz, snx, sny, snz, i0, j0, k0, i1, j1, k1);
+          if (in_box(bx[cc], gbox_ni(cc), i0, i1, j0, j1, k0, k1)) {
+            pic[cc] = sample3_at(bx[cc], fx, fy, fz, i0, j0, k0, i1, j1, k1);
+            old[cc] = sample3_at(bx[cc + 3], fx, fy, fz, i0, j0, k0, i1, j1, k1);
+          } else {
+            const float *fp = cc == 0 ? a.u : (cc == 1 ? a.v : a.w);
+            const float *fs = cc == 0 ? a.us : (cc == 1 ? a.vs : a.ws);
+            pic[cc] = sample3_at(GlobalAt{fp, (int64_t)sny * snz, snz}, fx, fy, fz, i0, j0, k0,
+                                 i1, j1, k1);
+            old[cc] = sample3_at(GlobalAt{fs, (int64_t)sny * snz, snz}, fx, fy, fz, i0, j0, k0,
+                                 i1, j1, k1);
+          }
+        }
+        float fu = r1.x + (pic[0] - old[0]), fv = r1.y + (pic[1] - old[1]),
+              fw = r1.z + (pic[2] - old[2]);
+        float ob = 1.0f - a.flip_blend;
+        nu = a.flip_blend * fu + ob * pic[0];
+        nv = a.flip_blend * fv + ob * pic[1];
+        nw = a.flip_blend * fw + ob * pic[2];
+      }
+      s_out[768 + 3 * tid] = nu;
+      s_out[768 + 3 * tid + 1] = nv;
+      s_out[768 + 3 * tid + 2] = nw;
+      const float eps = dx * 1.001f;
+      s_out[3 * tid] = clampf(px + nu * a.dt, eps, a.dom0 - eps);
+      s_out[3 * tid + 1] = clampf(py + nv * a.dt, eps, a.dom1 - eps);
+      s_out[3 * tid + 2] = clampf(pz + nw * a.dt, eps, a.dom2 - eps);
+      s_pid[tid] = __float_as_int(r0.w);
+    }
+    __syncthreads();
+    store_run(a.pos + 3 * base, s_out, 3 * m);
+    store_run(a.vel + 3 * base, s_out + 768, 3 * m);
+    if (APIC) store_run(a.C + 9 * base, s_out + 1536, 9 * m);
+    store_run(reinterpret_cast<float *>(a.pid + base), reinterpret_cast<const float *>(s_pid), m);
+    __syncthreads();
+  }
+}
+
+// Tensor maps of the bound face arrays for k_g2p_tile (single-grid contexts).
+// cuTensorMapEncodeTiled is reached through the runtime's driver entry point,
+// so the library does not link the driver library directly.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+    }
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+
+int encode_face_maps(Ctx *c) {
+  c->face_maps.mask = 0;
+  if (c->nseg > 0) return GF_OK;  // batches use the per-particle G2P
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return GF_OK;  // plain loads for every box
+  const float *arr[6] = {c->f.u, c->f.v, c->f.w, c->f.us, c->f.vs, c->f.ws};
+  for (int q = 0; q < 6; ++q) {
+    const int comp = q % 3;
+    const uint64_t snx = c->nx + (comp == 0), sny = c->ny + (comp == 1), snz = c->nz + (comp == 2);
+    const cuuint64_t dims[3] = {snz, sny, snx};
+    const cuuint64_t strides[2] = {snz * 4, sny * snz * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)gbox_nk(comp), (cuuint32_t)gbox_nj(comp),
+                               (cuuint32_t)gbox_ni(comp)};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    if (reinterpret_cast<uintptr_t>(arr[q]) % 16 || strides[0] % 16 || strides[1] % 16) continue;
+    if (fn(&c->face_maps.m[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(arr[q]),
+           dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS)
+      c->face_maps.mask |= 1 << q;
+  }
+  return GF_OK;
 }
 
 // ------------------------------------------------------------- batches
@@ -709,10 +1129,11 @@ int launch_g2p(Ctx *c, int transfer, float flip_blend, float dt) {
   G2PArgs a{c->rec0, c->rec1, c->f.u, c->f.v, c->f.w, c->f.us, c->f.vs, c->f.ws,
             c->p.pos, c->p.vel, c->p.C, c->p.pid, c->p.n, c->dx, dt, flip_blend,
             c->dom[0], c->dom[1], c->dom[2], c->nx, c->ny, c->nz};
+  G2PTileArgs ta{a, c->start, c->nty, c->ntz, c->health + 5};
   if (transfer == GF_APIC)
-    k_g2p<true><<<g, th, 0, c->stream>>>(a);
+    k_g2p_tile<GF_APIC><<<c->ntiles, G2P_TILE_THREADS, 0, c->stream>>>(ta, c->face_maps);
   else
-    k_g2p<false><<<g, th, 0, c->stream>>>(a);
+    k_g2p_tile<GF_FLIP><<<c->ntiles, G2P_TILE_THREADS, 0, c->stream>>>(ta, c->face_maps);
   c->launches++;
   return check_launch(c, "gf_g2p");
 }

@@ -6,11 +6,14 @@ Drop-in for the reference's ``MeshExtractor`` / ``particles_to_mesh``
 margin) and the iso-surface run in ``libgfb200.so`` (``gf_mesher_*``); the
 host reads back the finished mesh only.
 
-The iso-surface is cut by marching tetrahedra on the Kuhn split of each cube,
-where the reference calls scikit-image's or Warp's marching cubes: vertices
-are grid index * dx as there, and the axis-edge vertices are the ones
-marching cubes places, but each cube yields up to 12 triangles instead of up
-to 5.  Triangles face from density >= iso_level towards lower density.
+The iso-surface is cut by marching cubes, where the reference calls
+scikit-image's or Warp's marching cubes: vertices on the axis edges at grid
+index * dx as there, at most 5 triangles per cube from a case table in which
+an ambiguous face keeps its inside corners apart (so neighbouring cubes agree
+and the surface is closed).  ``surface_method="marching_tetrahedra"`` cuts it
+on the six-tetrahedron Kuhn split of each cube instead (no ambiguous cases;
+extra vertices on face and body diagonals, up to 12 triangles per cube).
+Triangles face from density >= iso_level towards lower density.
 
 Mesh smoothing (``mesh_smooth_passes``, ``smooth_laplacian``, ``smooth_taubin``;
 src/gpufluid/meshing/smoothing.py) runs on the device in float64 with the
@@ -49,7 +52,7 @@ class MeshExtractor:
     the current torch stream of ``device``."""
 
     def __init__(self, nx: int, ny: int, nz: int, dx: float, device=None,
-                 use_gpu_mc: Optional[bool] = None):
+                 use_gpu_mc: Optional[bool] = None, surface_method: str = "marching_cubes"):
         self.nx, self.ny, self.nz, self.dx = int(nx), int(ny), int(nz), float(dx)
         self.device = torch.device(device if device is not None else "cuda")
         self.use_gpu_mc = True  # the iso-surface always runs on the device
@@ -61,6 +64,20 @@ class MeshExtractor:
             None, "gf_mesher_create")
         self._h = h
         self.n_verts = self.n_tris = 0
+        self.surface_method = surface_method
+
+    @property
+    def surface_method(self) -> str:
+        return self._surface_method
+
+    @surface_method.setter
+    def surface_method(self, method: str) -> None:
+        if method not in _lib.SURFACE:
+            raise ValueError(f"unknown surface_method: {method!r}; expected "
+                             "'marching_cubes' or 'marching_tetrahedra'")
+        self._check(self._L.gf_mesher_set_surface(self._h, _lib.SURFACE[method]),
+                    "gf_mesher_set_surface")
+        self._surface_method = method
 
     def __del__(self):
         h = getattr(self, "_h", None)

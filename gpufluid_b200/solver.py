@@ -649,9 +649,14 @@ class FlipSolver3D:
         _lib.check(self._L.gf_health_read(self._ctx, 1 if reset else 0, _lib.ctypes.byref(h)),
                    self._ctx, "gf_health_read")
         names = _lib.STATUS_NAMES
-        return {"worst_status": names[h.worst_status], "solves": int(h.solves),
-                "not_converged": int(h.not_converged), "failed": int(h.failed),
-                "last_status": names[h.last_status]}
+        out = {"worst_status": names[h.worst_status], "solves": int(h.solves),
+               "not_converged": int(h.not_converged), "failed": int(h.failed),
+               "last_status": names[h.last_status]}
+        if h.wait_timeouts:  # a stage kernel's bounded wait ran out: its results are void
+            out["wait_timeouts"] = int(h.wait_timeouts)
+            out["worst_status"] = "TIMEOUT"
+            out["failed"] += int(h.wait_timeouts)
+        return out
 
     def check_pressure(self, frame: int = -1) -> dict:
         """Per-frame failure check beside ``has_diverged``: reads and resets

@@ -99,7 +99,8 @@ typedef struct gf_step_params {
  * Gauss-Seidel preconditioner for GF_PCG / GF_PCG_REFINED in the
  * shared-memory kernel; 0 keeps the reference's Jacobi preconditioner.  Same
  * operator and stop test; fewer iterations, one neighbour exchange more per
- * iteration.  The global-memory kernel always uses Jacobi. */
+ * iteration.  The global-memory kernel (active regions too large for the
+ * shared-memory solver) applies the same tile preconditioner. */
 #define GF_FLAG_SGS_SHIFT 2
 #define GF_FLAG_SGS_MASK 12
 /* flags: add a coarse correction to the shared-memory PCG's preconditioner
@@ -202,6 +203,8 @@ typedef struct gf_health {
   int32_t not_converged; /* solves that stopped at their iteration cap */
   int32_t failed;        /* solves that ended in GF_BREAKDOWN, GF_NAN or GF_TIMEOUT */
   int32_t last_status;   /* most severe status of the last solve call */
+  int32_t wait_timeouts; /* stage-kernel waits that ran out since the reset (the G2P
+                            tile loads); the stage's results are then incomplete */
 } gf_health;
 int gf_health_read(void *ctx, int32_t reset, gf_health *out);
 /* Active 8^3 pressure tiles of the last solve (k_mark_active_blocks,
@@ -284,15 +287,29 @@ int64_t gf_mesher_launches(void *mesher);
  * Asynchronous. */
 int gf_mesher_density(void *mesher, const float *pos, int64_t n, const gf_mesh_params *prm);
 /* Iso-surface {density >= iso_level} of `field` (device nx*ny*nz floats;
- * NULL = the mesher's own field) by marching tetrahedra on the Kuhn split of
- * each cube; stands in for the marching cubes of _mc_extract_gpu /
- * _mc_extract_cpu (surface.py:286-351), whose vertices are the axis-edge
- * subset of these.  Vertices are grid index * dx.  Writes the vertex and
- * triangle counts (0, 0 when no surface crosses the grid: the reference's
- * "no surface" result) and keeps the mesh in the mesher.  Synchronises once
- * for the counts. */
+ * NULL = the mesher's own field); replaces the marching cubes of
+ * _mc_extract_gpu / _mc_extract_cpu (surface.py:286-351).  By default
+ * marching cubes: vertices on the axis edges at the linear crossing, the
+ * triangles of each cube from a case table in which ambiguous faces keep
+ * their inside corners apart (so neighbouring cubes agree and the surface is
+ * closed), at most 5 per cube, facing from >= iso to < iso.  Vertices are
+ * grid index * dx.  Writes the vertex and triangle counts (0, 0 when no
+ * surface crosses the grid: the reference's "no surface" result) and keeps
+ * the mesh in the mesher.  Synchronises once for the counts. */
 int gf_mesher_extract(void *mesher, const float *field, float iso_level, int64_t *n_verts,
                       int64_t *n_tris);
+/* Surface method of gf_mesher_extract: GF_SURFACE_MARCHING_CUBES (default) or
+ * GF_SURFACE_MARCHING_TETRAHEDRA (the six-tetrahedron Kuhn split of each
+ * cube: no ambiguous cases, vertices also on face and body diagonals, up to
+ * 12 triangles per cube; its axis-edge vertices are the marching-cubes ones). */
+#define GF_SURFACE_MARCHING_CUBES 0
+#define GF_SURFACE_MARCHING_TETRAHEDRA 1
+int gf_mesher_set_surface(void *mesher, int32_t method);
+/* The marching-cubes case table gf_mesher_extract uses (host memory, no
+ * device needed): edges[12][2] corner pairs (corner bit 0 +x, bit 1 +y, bit 2
+ * +z), ntri[256] triangles per case (bit c of the case: corner c inside),
+ * tri[256][15] edge indices, three per triangle. */
+int gf_marching_cubes_table(uint8_t *edges, uint8_t *ntri, uint8_t *tri);
 /* Which side of the level is inside for the next gf_mesher_extract: 0 (the
  * default after a GF_MESH_TRILINEAR / GF_MESH_CUBIC field) encloses
  * values >= iso, 1 (set by a GF_MESH_SDF field) values <= iso. */

@@ -28,12 +28,22 @@ restatement against them.
 
 The iso-surface step of the reference is third-party code (scikit-image's
 ``marching_cubes`` below 64^3, Warp's ``MarchingCubes`` from 64^3,
-surface.py:286-351); neither is installed, so that step is unpinned.
-``iso_surface`` restates the library's own method -- marching tetrahedra on
-the Kuhn split of each cube -- independently of the CUDA code (orientation
-from integer determinants of the tetrahedra's corners rather than from the
-permutation parity), for bit-exact checks of the GPU extraction on the same
-field; its axis-edge vertices are the crossings marching cubes would place.
+surface.py:286-351); neither is installed, so that step is unpinned.  The
+library's own methods are restated here independently of the CUDA code, for
+bit-exact checks of the GPU extraction on the same field:
+
+* ``iso_surface_mc`` -- marching cubes (Lorensen & Cline 1987): vertices on
+  the axis edges at the linear crossing; each cube's triangles traced per
+  case on the fly -- face segments (an ambiguous face cuts off its inside
+  corners), loops oriented with the inside on their right as seen from outside
+  the cube (decided here with floating-point midpoint geometry, where the CUDA
+  table generator uses doubled integer coordinates), each loop listed from its
+  lowest edge and fanned from its first vertex whose diagonals all leave the
+  cube's faces;
+* ``iso_surface`` -- marching tetrahedra on the Kuhn split of each cube
+  (orientation from integer determinants of the tetrahedra's corners rather
+  than from the permutation parity); its axis-edge vertices are the
+  marching-cubes ones.
 """
 from __future__ import annotations
 
@@ -266,6 +276,124 @@ def iso_surface(dens, iso, dx, below=False):
                 tris.append(np.stack([cyc[0], cyc[1], cyc[2]], 1))
                 keys.append(cube_key[sel] * 12 + t * 2 + 1)
                 tris.append(np.stack([cyc[0], cyc[2], cyc[3]], 1))
+    if not keys:
+        return verts.astype(F32), np.zeros((0, 3), np.int32)
+    keys = np.concatenate(keys)
+    tris = np.concatenate(tris)
+    order = np.argsort(keys, kind="stable")
+    return verts.astype(F32), tris[order].astype(np.int32)
+
+
+# ---- marching cubes ----------------------------------------------------------
+# Corner c of a cube: bit 0 +x, bit 1 +y, bit 2 +z.  Edge e: along x for
+# e < 4, y for e < 8, z otherwise, from the (e % 4)-th corner (ascending)
+# without that bit.
+MC_EDGES = [(lo, lo | a) for a in (1, 2, 4) for lo in range(8) if not lo & a]
+
+
+def _corner_pos(c):
+    return np.array([c & 1, (c >> 1) & 1, (c >> 2) & 1], np.float64)
+
+
+def mc_case(cm):
+    """Triangles (edge-index triples) of case cm (bit c: corner c inside)."""
+    inside = [(cm >> c) & 1 for c in range(8)]
+    cross = [e for e, (lo, hi) in enumerate(MC_EDGES) if inside[lo] != inside[hi]]
+    succ = {}
+    for axis in range(3):
+        a = 1 << axis
+        for side in (0, a):
+            on_face = [e for e in cross if (MC_EDGES[e][0] & a) == side and (MC_EDGES[e][1] & a) == side]
+            if len(on_face) == 2:
+                pairs = [on_face]
+            elif len(on_face) == 4:  # ambiguous: each inside corner is cut off alone
+                pairs = [[e for e in on_face if c in MC_EDGES[e]]
+                         for c in range(8) if (c & a) == side and inside[c]]
+            else:
+                pairs = []
+            normal = np.zeros(3)
+            normal[axis] = 1.0 if side else -1.0
+            for e1, e2 in pairs:
+                m1 = _corner_pos(MC_EDGES[e1][0]) * 0.5 + _corner_pos(MC_EDGES[e1][1]) * 0.5
+                m2 = _corner_pos(MC_EDGES[e2][0]) * 0.5 + _corner_pos(MC_EDGES[e2][1]) * 0.5
+                c_in = MC_EDGES[e1][0] if inside[MC_EDGES[e1][0]] else MC_EDGES[e1][1]
+                on_left = np.dot(np.cross(normal, m2 - m1), _corner_pos(c_in) - m1) > 0
+                a_, b_ = (e2, e1) if on_left else (e1, e2)  # inside stays on the right
+                assert a_ not in succ
+                succ[a_] = b_
+    assert sorted(succ) == cross
+    def faces(e):  # the two cube faces holding edge e, as (axis bit, side)
+        lo, hi = MC_EDGES[e]
+        return {(b, lo & b) for b in (1, 2, 4) if b != hi ^ lo}
+
+    tris, done = [], set()
+    for e0 in cross:  # ascending: each loop starts at its lowest edge
+        if e0 in done:
+            continue
+        loop, e = [], e0
+        while e not in done:
+            done.add(e)
+            loop.append(e)
+            e = succ[e]
+        n = len(loop)
+        # fan from the first vertex whose diagonals all leave the cube's faces
+        # (a diagonal inside a face would meet the neighbouring cube's)
+        s = next(k for k in range(n)
+                 if all(not faces(loop[k]) & faces(loop[(k + i) % n]) for i in range(2, n - 1)))
+        tris += [(loop[s], loop[(s + i) % n], loop[(s + i + 1) % n]) for i in range(1, n - 1)]
+    return tris
+
+
+def iso_surface_mc(dens, iso, dx, below=False):
+    """Marching cubes of {dens >= iso} ({dens <= iso} with ``below``):
+    (verts (V,3) float32, tris (T,3) int32); vertices ordered by (node, axis
+    x y z), triangles by (cube, case triangle)."""
+    d = np.asarray(dens, F32)
+    nx, ny, nz = d.shape
+    if nx < 2 or ny < 2 or nz < 2:
+        return np.zeros((0, 3), F32), np.zeros((0, 3), np.int32)
+    iso32, dx32 = F32(iso), F32(dx)
+    inside = d <= iso32 if below else d >= iso32
+    cross = np.zeros((nx, ny, nz, 3), bool)
+    vpos = np.zeros((nx, ny, nz, 3, 3), F32)
+    gi, gj, gk = np.meshgrid(np.arange(nx, dtype=F32), np.arange(ny, dtype=F32),
+                             np.arange(nz, dtype=F32), indexing="ij")
+    for axis in range(3):
+        o = [0, 0, 0]
+        o[axis] = 1
+        lo = (slice(0, nx - o[0]), slice(0, ny - o[1]), slice(0, nz - o[2]))
+        hi = (slice(o[0], nx), slice(o[1], ny), slice(o[2], nz))
+        cross[lo + (axis,)] = inside[lo] != inside[hi]
+        with np.errstate(divide="ignore", invalid="ignore"):
+            t = (iso32 - d[lo]) / (d[hi] - d[lo])
+        for k, g in enumerate((gi, gj, gk)):
+            vpos[lo + (axis, k)] = ((g[lo] + t) if k == axis else g[lo]) * dx32
+    flat = cross.reshape(-1)
+    verts = vpos.reshape(-1, 3)[flat]
+    vid = np.full(flat.shape, -1, np.int64)
+    vid[flat] = np.arange(int(flat.sum()))
+    vid = vid.reshape(nx, ny, nz, 3)
+    if len(verts) == 0:
+        return verts.astype(F32), np.zeros((0, 3), np.int32)
+    cx, cy, cz = nx - 1, ny - 1, nz - 1
+    case = np.zeros((cx, cy, cz), np.int64)
+    for c in range(8):
+        x, y, z = c & 1, (c >> 1) & 1, (c >> 2) & 1
+        case |= inside[x:x + cx, y:y + cy, z:z + cz].astype(np.int64) << c
+    ci, cj, ck = np.meshgrid(np.arange(cx), np.arange(cy), np.arange(cz), indexing="ij")
+    cube_key = (ci * ny + cj) * nz + ck
+
+    def edge_vid(e, sel):
+        lo, hi = MC_EDGES[e]
+        x, y, z = lo & 1, (lo >> 1) & 1, (lo >> 2) & 1
+        return vid[x:x + cx, y:y + cy, z:z + cz, {1: 0, 2: 1, 4: 2}[hi ^ lo]][sel]
+
+    keys, tris = [], []
+    for cm in np.unique(case):
+        sel = case == cm
+        for q, (e0, e1, e2) in enumerate(mc_case(int(cm))):
+            keys.append(cube_key[sel] * 8 + q)
+            tris.append(np.stack([edge_vid(e0, sel), edge_vid(e1, sel), edge_vid(e2, sel)], 1))
     if not keys:
         return verts.astype(F32), np.zeros((0, 3), np.int32)
     keys = np.concatenate(keys)

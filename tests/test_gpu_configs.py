@@ -22,8 +22,9 @@ seeded inputs.
   within 1e-6 of an FP64 solve of the oracle's system.
 * 256^3 double dam break (56,088,576 particles): the first substep's
   pressure system through the global-memory PCG (the active region exceeds
-  the shared-memory solver), refined to 1e-7, against an FP64 CG solve of
-  the same system; 20 Jacobi sweeps bit-exact against the oracle.
+  the shared-memory solver), refined to 1e-7 with the reference's Jacobi
+  preconditioner and with the tile SGS one, against an FP64 CG solve of the
+  same system; 20 Jacobi sweeps bit-exact against the oracle.
 
 ``GF_PARITY_OUT`` (an environment variable naming a directory) makes the
 64^3 runs write their per-substep drift tables there as JSON.
@@ -287,18 +288,24 @@ def test_cfg3_256_global_pcg_against_fp64(gf, oracle):
         _call(s, name, *args)
     torch.cuda.synchronize()
     lab_dev, div_dev = s._label.clone(), s.div.clone()
-    prm = s._params(dt, 8000, "pcg_refined")
-    _call(s, "gf_pressure", ctypes.byref(prm), None)
-    st = s.pressure_stats()
-    assert st["kernel"] == 2, st  # the global-memory solver
-    assert st["status"] == 0 and st["relres"] <= 1e-7, st
-    assert st["n_fluid"] > 6_000_000
     x64, rel = _fp64_cg(torch, lab_dev, -div_dev.double())
     assert rel < 1e-12, rel
     fl = lab_dev == 1
-    p = torch.where(fl, s._p.double(), torch.zeros_like(x64))
-    err = float(torch.linalg.vector_norm(p - x64) / torch.linalg.vector_norm(x64))
-    assert err < 1e-5, err
+    iters = {}
+    for precond in ("jacobi", "tile_sgs"):
+        s.pcg_preconditioner = precond
+        prm = s._params(dt, 8000, "pcg_refined")
+        _call(s, "gf_pressure", ctypes.byref(prm), None)
+        st = s.pressure_stats()
+        assert st["kernel"] == 2, st  # the global-memory solver
+        assert st["status"] == 0 and st["relres"] <= 1e-7, (precond, st)
+        assert st["n_fluid"] > 6_000_000
+        p = torch.where(fl, s._p.double(), torch.zeros_like(x64))
+        err = float(torch.linalg.vector_norm(p - x64) / torch.linalg.vector_norm(x64))
+        assert err < 1e-5, (precond, err)
+        iters[precond] = st["iters"]
+    assert iters["tile_sgs"] < iters["jacobi"], iters
+    s.pcg_preconditioner = "jacobi"
     # 20 Jacobi sweeps: bit-exact against the oracle on the same system
     prm = s._params(dt, 20, "jacobi")
     s.div.copy_(div_dev)

@@ -82,6 +82,57 @@ def test_oracle_iso_surface_closed_sphere():
     assert np.abs(r - 10.0).max() < 0.1
 
 
+def test_marching_cubes_table_matches_oracle():
+    """The library's generated case table (gf_marching_cubes_table, host code,
+    no device) equals the oracle's per-case loop tracing; at most 5 triangles
+    per case, none for the empty and the full cube, and a case and its
+    complement cross the same edges."""
+    import ctypes
+    from gpufluid_b200 import _lib
+    L = _lib.load()
+    edges, ntri, tri = np.zeros(24, np.uint8), np.zeros(256, np.uint8), np.zeros(3840, np.uint8)
+    assert L.gf_marching_cubes_table(edges.ctypes.data, ntri.ctypes.data, tri.ctypes.data) == 0
+    assert [tuple(int(x) for x in e) for e in edges.reshape(12, 2)] == om.MC_EDGES
+    tri = tri.reshape(256, 15)
+    for cm in range(256):
+        want = om.mc_case(cm)
+        assert ntri[cm] == len(want), cm
+        assert [tuple(int(x) for x in tri[cm][3 * q:3 * q + 3]) for q in range(len(want))] == want
+        used = {e for t in want for e in t}
+        assert used == {e for t in om.mc_case(255 - cm) for e in t}
+    assert ntri.max() == 5 and ntri[0] == 0 and ntri[255] == 0
+    assert L.gf_marching_cubes_table(None, ntri.ctypes.data, tri.ctypes.data) == _lib.GF_INVALID_ARG
+
+
+def test_oracle_marching_cubes_closed_sphere_and_orientation():
+    n, dx = 40, 1.0 / 40
+    f = _sphere(n, (19.3, 20.1, 18.7), 10.0)
+    v, t = om.iso_surface_mc(f, 0.0, dx)
+    nb, once = om.boundary_edges(t)
+    assert nb == 0 and once
+    edges = np.unique(np.sort(np.concatenate([t[:, [0, 1]], t[:, [1, 2]], t[:, [2, 0]]]), 1),
+                      axis=0)
+    assert len(v) - len(edges) + len(t) == 2
+    exact = 4.0 / 3.0 * np.pi * (10 * dx) ** 3
+    assert 0.98 * exact < om.mesh_volume(v, t) < exact
+    r = np.linalg.norm(v / dx - np.float32([19.3, 20.1, 18.7]), axis=1)
+    assert np.abs(r - 10.0).max() < 0.1
+    # the tetrahedra's surface of the same field: the same axis-edge vertices
+    vt, tt = om.iso_surface(f, 0.0, dx)
+    assert len(vt) > len(v) and len(tt) > len(t)
+    assert {tuple(x) for x in v} <= {tuple(x) for x in vt}
+    # noise: every ambiguous face occurs; the surface is still closed away
+    # from the grid walls and consistently oriented
+    g = np.random.default_rng(3).normal(size=(20, 18, 22)).astype(np.float32)
+    g[[0, -1]] = -1.0
+    g[:, [0, -1]] = -1.0
+    g[:, :, [0, -1]] = -1.0
+    v, t = om.iso_surface_mc(g, 0.0, 1.0)
+    nb, once = om.boundary_edges(t)
+    assert nb == 0 and once
+    assert om.mesh_volume(v, t) > 0
+
+
 def test_oracle_iso_surface_open_and_inverted():
     """A slab touching the grid walls is open; the complement field gives the
     same vertices with every triangle reversed."""
@@ -199,8 +250,9 @@ def test_density_bit_exact_on_dyadic_splat(gf, passes, margin):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("method", ["marching_cubes", "marching_tetrahedra"])
 @pytest.mark.parametrize("case", ["sphere", "noise", "ties", "ragged", "wall", "tiny", "flat"])
-def test_iso_surface_bit_exact(gf, case):
+def test_iso_surface_bit_exact(gf, case, method):
     import torch
     rng = np.random.default_rng(5)
     dx, iso = 0.05, 0.0
@@ -219,13 +271,21 @@ def test_iso_surface_bit_exact(gf, case):
     else:  # one cell thick: no cube, no surface
         f = rng.normal(size=(1, 9, 9)).astype(np.float32)
     ex = _extractor(f.shape, dx)
+    ex.surface_method = method
     v, t = ex.surface(iso, field=torch.from_numpy(f).cuda())
-    ov, ot = om.iso_surface(f, iso, dx)
+    ov, ot = (om.iso_surface_mc if method == "marching_cubes" else om.iso_surface)(f, iso, dx)
     if len(ot) == 0:
         assert v is None and t is None
         return
     assert np.array_equal(v, ov) and np.array_equal(t, ot)
     assert ex.n_verts == len(ov) and ex.n_tris == len(ot)
+    if method == "marching_cubes":
+        # the vertices are the axis-edge subset of the tetrahedra's, bit for bit
+        ex.surface_method = "marching_tetrahedra"
+        vt, _ = ex.surface(iso, field=torch.from_numpy(f).cuda())
+        key = lambda a: a.view(np.uint32).view([("x", "u4"), ("y", "u4"), ("z", "u4")]).ravel()  # noqa: E731
+        assert np.isin(key(v), key(vt)).all()
+        assert len(t) <= 5 * np.prod(np.array(f.shape) - 1)
 
 
 @pytest.mark.gpu
@@ -240,6 +300,7 @@ def test_iso_surface_properties_at_256(gf):
     f = torch.maximum(sph, 20.5 - J)  # plus a floor slab y < 20.5
     ex = _extractor((n, n, n), dx)
     v, t = ex.surface(0.0, field=f.contiguous())
+    assert ex.surface_method == "marching_cubes"
     assert v is not None and t.min() >= 0 and t.max() < len(v)
     nb, once = om.boundary_edges(t)
     assert once  # consistent orientation across all cubes
@@ -252,6 +313,15 @@ def test_iso_surface_properties_at_256(gf):
     sel = v[:, 1] > 30 * dx  # the sphere's vertices
     r = np.linalg.norm(v[sel] / dx - np.float32([127.3, 140.6, 120.2]), axis=1)
     assert np.abs(r - 60.0).max() < 0.05
+    # the sphere alone: closed, Euler characteristic 2, enclosed volume
+    v, t = ex.surface(0.0, field=sph.contiguous())
+    nb, once = om.boundary_edges(t)
+    assert nb == 0 and once
+    edges = np.unique(np.sort(np.concatenate([t[:, [0, 1]], t[:, [1, 2]], t[:, [2, 0]]]), 1),
+                      axis=0)
+    assert len(v) - len(edges) + len(t) == 2
+    exact = 4.0 / 3.0 * np.pi * (60.0 * dx) ** 3
+    assert 0.995 * exact < om.mesh_volume(v, t) < exact
 
 
 @pytest.mark.gpu
@@ -270,7 +340,7 @@ def test_extract_on_solver_particles(gf):
     d = ex.dens.cpu().numpy()
     ref = om.density_field(pos, (48, 48, 48), s.dx, 2, 1)
     np.testing.assert_allclose(d, ref, rtol=0, atol=4e-6 * float(ref.max()))
-    ov, ot = om.iso_surface(d, 0.6, s.dx)
+    ov, ot = om.iso_surface_mc(d, 0.6, s.dx)
     assert np.array_equal(v, ov) and np.array_equal(t, ot)
     assert om.boundary_edges(t)[0] == 0  # the wall margin closes the surface
     assert om.mesh_volume(v, t) > 0
@@ -290,7 +360,7 @@ def test_extract_on_solver_particles(gf):
     dd = ex.dens.cpu().numpy()
     refd = om.density_field(pos, (48, 48, 48), s.dx, 1, 0, "sdf")
     assert np.array_equal(dd, refd)
-    ov, ot = om.iso_surface(dd, 0.0, s.dx, below=True)
+    ov, ot = om.iso_surface_mc(dd, 0.0, s.dx, below=True)
     assert np.array_equal(vd, ov) and np.array_equal(td, ot)
     assert om.mesh_volume(vd, td) > 0  # faces outward from the fluid
     with pytest.raises(ValueError):
@@ -300,7 +370,7 @@ def test_extract_on_solver_particles(gf):
     vs, ts = ex.extract(s.pos, iso_level=0.6, smooth_passes=2, wall_margin_cells=1,
                         mesh_smooth_passes=2)
     d2 = ex.dens.cpu().numpy()
-    ov, ot = om.iso_surface(d2, 0.6, s.dx)
+    ov, ot = om.iso_surface_mc(d2, 0.6, s.dx)
     assert np.array_equal(ts, ot) and np.array_equal(vs, om.smooth(ov, ot, "taubin", 2))
     with pytest.raises(ValueError):
         ex.extract(pos, decimate_ratio=0.5)
@@ -308,7 +378,7 @@ def test_extract_on_solver_particles(gf):
     dc = ex.dens.cpu().numpy()
     refc = om.density_field(pos, (48, 48, 48), s.dx, 2, 0, "cubic", 2.0)
     np.testing.assert_allclose(dc, refc, rtol=0, atol=4e-6 * float(refc.max()))
-    ov, ot = om.iso_surface(dc, 3.0, s.dx)
+    ov, ot = om.iso_surface_mc(dc, 3.0, s.dx)
     assert np.array_equal(vc, ov) and np.array_equal(tc, ot)
     assert ex.launches > 0
 
