@@ -598,18 +598,14 @@ class FlipSolver3D:
         return bool(torch.isnan(self._pos).any().item())
 
     def save_checkpoint(self, path) -> None:
-        """Same .npz keys as solver3d.py:4127-4157."""
-        Path(path).parent.mkdir(parents=True, exist_ok=True)
+        """Same .npz keys as solver3d.py:4127-4157 (``write_checkpoint``)."""
         n = self.n_particles
-        pos = self.pos.numpy() if n else np.zeros((0, 3), np.float32)
-        vel = self.vel.numpy() if n else np.zeros((0, 3), np.float32)
-        aff = self.affine_C.numpy() if n else np.zeros((0, 3, 3), np.float32)
-        np.savez_compressed(
-            str(path), pos=pos, vel=vel, affine_C=aff, marker=self.marker.numpy(),
-            attr_color=np.zeros((0, 3), np.float32), attr_temperature=np.zeros((0,), np.float32),
-            nx=self.nx, ny=self.ny, nz=self.nz, dx=self.dx, gravity=self.gravity,
-            flip_blend=self.flip_blend, rho=self.rho, viscosity=self.viscosity,
-            transfer_mode=str(self.transfer_mode), surface_tension=self.surface_tension)
+        write_checkpoint(
+            path, self.pos.numpy() if n else None, self.vel.numpy() if n else None,
+            self.affine_C.numpy() if n else None, self.marker.numpy(),
+            dict(nx=self.nx, ny=self.ny, nz=self.nz, dx=self.dx, gravity=self.gravity,
+                 flip_blend=self.flip_blend, rho=self.rho, viscosity=self.viscosity,
+                 transfer_mode=str(self.transfer_mode), surface_tension=self.surface_tension))
 
     def load_checkpoint(self, path) -> None:
         """solver3d.py:4159-4222: topology and dx must match; physics knobs
@@ -682,6 +678,22 @@ class FlipSolver3D:
 
 
 _CKPT_KEYS = ("pos", "vel", "affine_C", "marker", "nx", "ny", "nz", "dx")
+
+
+def write_checkpoint(path, pos, vel, affine_C, marker, meta: dict) -> None:
+    """Write a checkpoint with the keys, dtypes and compression of the
+    reference's save_checkpoint (solver3d.py:4127-4157): pos, vel (n,3),
+    affine_C (n,3,3) float32 (empty arrays for no particles), marker int32,
+    empty colour and temperature arrays (this build carries no particle
+    attributes), and the grid and physics scalars in ``meta`` (nx, ny, nz, dx,
+    gravity, flip_blend, rho, viscosity, transfer_mode, surface_tension)."""
+    Path(path).parent.mkdir(parents=True, exist_ok=True)
+    f32 = lambda a, shape: (np.zeros(shape, np.float32) if a is None  # noqa: E731
+                            else np.ascontiguousarray(a, np.float32))
+    np.savez_compressed(
+        str(path), pos=f32(pos, (0, 3)), vel=f32(vel, (0, 3)), affine_C=f32(affine_C, (0, 3, 3)),
+        marker=np.asarray(marker, np.int32), attr_color=np.zeros((0, 3), np.float32),
+        attr_temperature=np.zeros((0,), np.float32), **meta)
 
 
 def read_checkpoint(path, grid, dx, live=None) -> dict:
