@@ -11,7 +11,12 @@ import os
 import re
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libgfb200.so")
+# GFB200_LIB=libgfb200_checked.so selects the bounds-checked build
+LIB_VARIANTS = ("libgfb200.so", "libgfb200_checked.so")
+_variant = os.environ.get("GFB200_LIB", LIB_VARIANTS[0])
+if _variant not in LIB_VARIANTS:
+    raise RuntimeError(f"GFB200_LIB={_variant!r}: expected one of {LIB_VARIANTS}")
+LIB_PATH = os.path.join(HERE, _variant)
 HEADER = os.path.join(os.path.dirname(HERE), "include", "gfb200.h")
 
 GF_OK, GF_INVALID_ARG, GF_CUDA_ERROR, GF_NOT_CONVERGED = 0, 1, 2, 3
@@ -124,6 +129,9 @@ _SIGS = {
     "gf_project": ([_vp, ctypes.c_float, ctypes.c_float], ctypes.c_int),
     "gf_g2p": ([_vp, ctypes.c_int32, ctypes.c_float, ctypes.c_float], ctypes.c_int),
     "gf_step": ([_vp, ctypes.POINTER(StepParams)], ctypes.c_int),
+    "gf_graph_capture": ([_vp, ctypes.POINTER(StepParams), ctypes.POINTER(_vp)], ctypes.c_int),
+    "gf_graph_replay": ([_vp, _vp], ctypes.c_int),
+    "gf_graph_destroy": ([_vp], ctypes.c_int),
     "gf_pressure_result": ([_vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double),
                             ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
     "gf_bin_read": ([_vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
@@ -141,6 +149,9 @@ _SIGS = {
     "gf_reseed_emit": ([_vp, _vp, _vp, ctypes.c_int32, _vp, _vp], ctypes.c_int),
     "gf_pressure_stats": ([_vp, ctypes.POINTER(PressureInfo)], ctypes.c_int),
     "gf_health_read": ([_vp, ctypes.c_int32, ctypes.POINTER(Health)], ctypes.c_int),
+    "gf_bounds_status": ([ctypes.c_int32, ctypes.POINTER(ctypes.c_int64),
+                          ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)],
+                         ctypes.c_int),
     "gf_pcg_trace": ([_vp, _vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
     "gf_record_bytes": ([_vp, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
     "gf_step_record": ([_vp, ctypes.POINTER(StepParams), _vp], ctypes.c_int),

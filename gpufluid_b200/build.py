@@ -1,6 +1,6 @@
 """Build libgfb200.so in-tree with nvcc for sm_100a.
 
-    python -m gpufluid_b200.build [--verbose]
+    python -m gpufluid_b200.build [--verbose] [--bounds-check]
 
 Every translation unit is compiled to an object (in parallel) and the objects
 are linked into one shared library.  The library is written for B200 only:
@@ -28,6 +28,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgfb200.so")
 OBJ = os.path.join(HERE, "_build")
+# the bounds-checked variant: every instrumented index is checked (GF_IN)
+LIB_CHECKED = os.path.join(HERE, "libgfb200_checked.so")
+OBJ_CHECKED = os.path.join(HERE, "_build_checked")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -46,10 +49,10 @@ def unit_flags(src: str) -> list:
     return [*COMMON, f"-fmad={fma}"]
 
 
-def needs_build() -> bool:
-    if not os.path.exists(LIB):
+def needs_build(lib: str = LIB) -> bool:
+    if not os.path.exists(lib):
         return True
-    t = os.path.getmtime(LIB)
+    t = os.path.getmtime(lib)
     deps = sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + [
         os.path.join(HERE, "..", "include", "gfb200.h"), os.path.abspath(__file__)]
     return any(os.path.getmtime(p) > t for p in deps)
@@ -62,33 +65,38 @@ def _env():
     return env
 
 
-def _compile(src: str, verbose: bool):
-    obj = os.path.join(OBJ, os.path.basename(src)[:-3] + ".o")
-    cmd = [NVCC, *unit_flags(src), *(["-Xptxas", "-v"] if verbose else []), "-c", "-o", obj, src]
+def _compile(src: str, verbose: bool, objdir: str, extra: list):
+    obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
+    cmd = [NVCC, *unit_flags(src), *extra, *(["-Xptxas", "-v"] if verbose else []), "-c", "-o",
+           obj, src]
     r = subprocess.run(cmd, capture_output=True, text=True, env=_env())
     return obj, r
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and not needs_build():
-        return LIB
-    os.makedirs(OBJ, exist_ok=True)
+def build(force: bool = False, verbose: bool = False, checked: bool = False) -> str:
+    """Build libgfb200.so, or with ``checked`` the bounds-checked
+    libgfb200_checked.so (-DGF_BOUNDS_CHECK)."""
+    lib, objdir = (LIB_CHECKED, OBJ_CHECKED) if checked else (LIB, OBJ)
+    extra = ["-DGF_BOUNDS_CHECK"] if checked else []
+    if not force and not needs_build(lib):
+        return lib
+    os.makedirs(objdir, exist_ok=True)
     srcs = sources()
     with ThreadPoolExecutor(max_workers=min(len(srcs), os.cpu_count() or 4)) as ex:
-        results = list(ex.map(lambda s: _compile(s, verbose), srcs))
+        results = list(ex.map(lambda s: _compile(s, verbose, objdir, extra), srcs))
     errs = [r.stdout + r.stderr for _, r in results if r.returncode != 0]
     if errs:
         raise RuntimeError("nvcc failed:\n" + "\n".join(errs))
     if verbose:
         for _, r in results:
             sys.stdout.write(r.stdout + r.stderr)
-    cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *(o for o, _ in results)]
+    cmd = [NVCC, *ARCH, "-shared", "-o", lib, *(o for o, _ in results)]
     r = subprocess.run(cmd, capture_output=True, text=True, env=_env())
     if r.returncode != 0:
         raise RuntimeError("nvcc link failed:\n" + r.stdout + r.stderr)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":
-    build(force=True, verbose="--verbose" in sys.argv)
-    print(LIB)
+    print(build(force=True, verbose="--verbose" in sys.argv,
+                checked="--bounds-check" in sys.argv))

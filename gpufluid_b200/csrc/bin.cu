@@ -33,7 +33,7 @@ __device__ __forceinline__ int clampi(int v, int lo, int hi) {
 __global__ void k_bin_keys(const float *__restrict__ pos, int64_t n, float dx, int nx,
                            int ny, int nz, int nty, int ntz, uint8_t *__restrict__ label,
                            int32_t *__restrict__ key, int32_t *__restrict__ rank,
-                           int32_t *__restrict__ count) {
+                           int32_t *__restrict__ count, int64_t nkeys) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   unsigned amask = __ballot_sync(0xffffffffu, i < n);
   if (i >= n) return;
@@ -43,7 +43,8 @@ __global__ void k_bin_keys(const float *__restrict__ pos, int64_t n, float dx, i
   int cj = clampi(__float2int_rz(__fdiv_rn(py, dx)), 0, ny - 1);
   int ck = clampi(__float2int_rz(__fdiv_rn(pz, dx)), 0, nz - 1);
   int64_t cell = ((int64_t)ci * ny + cj) * nz + ck;
-  if (label[cell] != 2) label[cell] = 1;  // benign race: every writer stores 1
+  if (GF_IN(cell, (int64_t)nx * ny * nz) && label[cell] != 2)
+    label[cell] = 1;  // benign race: every writer stores 1
   int t = ((ci >> 3) * nty + (cj >> 3)) * ntz + (ck >> 3);
   int kk = t * TILE_CELLS + (((ci & 7) * 8 + (cj & 7)) * 8 + (ck & 7));
   key[i] = kk;
@@ -52,7 +53,7 @@ __global__ void k_bin_keys(const float *__restrict__ pos, int64_t n, float dx, i
   int leader = __ffs(peers) - 1;
   int below = __popc(peers & ((1u << lane) - 1u));
   int base = 0;
-  if ((int)lane == leader) base = atomicAdd(&count[kk], __popc(peers));
+  if ((int)lane == leader && GF_IN(kk, nkeys)) base = atomicAdd(&count[kk], __popc(peers));
   base = __shfl_sync(amask, base, leader);
   rank[i] = base + below;
 }
@@ -61,7 +62,8 @@ __global__ void k_bin_keys(const float *__restrict__ pos, int64_t n, float dx, i
 // prefix of the segment table and bins into that scene's cells and tiles.
 __global__ void kb_bin_keys(const float *__restrict__ pos, int64_t n, SegIndex sx,
                             uint8_t *__restrict__ label, int32_t *__restrict__ key,
-                            int32_t *__restrict__ rank, int32_t *__restrict__ count) {
+                            int32_t *__restrict__ rank, int32_t *__restrict__ count,
+                            int64_t ncell, int64_t nkeys) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   unsigned amask = __ballot_sync(0xffffffffu, i < n);
   if (i >= n) return;
@@ -71,7 +73,7 @@ __global__ void kb_bin_keys(const float *__restrict__ pos, int64_t n, SegIndex s
   int cj = clampi(__float2int_rz(__fdiv_rn(py, r.dx)), 0, r.ny - 1);
   int ck = clampi(__float2int_rz(__fdiv_rn(pz, r.dx)), 0, r.nz - 1);
   int64_t cell = r.cell0 + ((int64_t)ci * r.ny + cj) * r.nz + ck;
-  if (label[cell] != 2) label[cell] = 1;
+  if (GF_IN(cell, ncell) && label[cell] != 2) label[cell] = 1;
   int64_t t = r.tile0 + ((ci >> 3) * r.nty + (cj >> 3)) * r.ntz + (ck >> 3);
   int kk = (int)(t * TILE_CELLS + (((ci & 7) * 8 + (cj & 7)) * 8 + (ck & 7)));
   key[i] = kk;
@@ -80,7 +82,7 @@ __global__ void kb_bin_keys(const float *__restrict__ pos, int64_t n, SegIndex s
   int leader = __ffs(peers) - 1;
   int below = __popc(peers & ((1u << lane) - 1u));
   int base = 0;
-  if ((int)lane == leader) base = atomicAdd(&count[kk], __popc(peers));
+  if ((int)lane == leader && GF_IN(kk, nkeys)) base = atomicAdd(&count[kk], __popc(peers));
   base = __shfl_sync(amask, base, leader);
   rank[i] = base + below;
 }
@@ -191,19 +193,22 @@ __global__ void k_place(const int32_t *__restrict__ key, const int32_t *__restri
                         const int32_t *__restrict__ start, int64_t n,
                         int32_t *__restrict__ order) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i < n) order[start[key[i]] + rank[i]] = (int32_t)i;
+  if (i >= n) return;
+  const int64_t slot = (int64_t)start[key[i]] + rank[i];
+  if (GF_IN(slot, n)) order[slot] = (int32_t)i;
 }
 
 // Sort each multi-particle cell segment of `order` by original particle id.
 constexpr int CANON_LOCAL = 48;
 __global__ void k_canon(const int32_t *__restrict__ count, const int32_t *__restrict__ start,
                         int64_t nkeys, const int32_t *__restrict__ pid,
-                        int32_t *__restrict__ order) {
+                        int32_t *__restrict__ order, int64_t n) {
   int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (q >= nkeys) return;
   int cnt = count[q];
   if (cnt < 2) return;
   int s = start[q];
+  if (!GF_IN(s, n) || !GF_IN((int64_t)s + cnt - 1, n)) return;
   if (cnt <= CANON_LOCAL) {
     int ids[CANON_LOCAL], idx[CANON_LOCAL];
     for (int a = 0; a < cnt; ++a) {
@@ -239,6 +244,7 @@ __global__ void k_permute(const int32_t *__restrict__ order, int64_t n,
   int64_t d = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (d >= n) return;
   int64_t s = order[d];
+  if (!GF_IN(s, n)) return;
   float4 a, b;
   a.x = pos[3 * s];
   a.y = pos[3 * s + 1];
@@ -277,12 +283,12 @@ int launch_bin(Ctx *c, int transfer) {
     return e;
   if (n > 0 && c->nseg > 0) {
     kb_bin_keys<<<nblk(n, 256), 256, 0, st>>>(c->p.pos, n, seg_index(c), c->f.label, c->key,
-                                              c->rank, c->count);
+                                              c->rank, c->count, c->ncell, c->nkeys);
     c->launches++;
   } else if (n > 0) {
     k_bin_keys<<<nblk(n, 256), 256, 0, st>>>(c->p.pos, n, c->dx, c->nx, c->ny, c->nz,
                                              c->nty, c->ntz, c->f.label, c->key, c->rank,
-                                             c->count);
+                                             c->count, c->nkeys);
     c->launches++;
   }
   k_scan_block_sums<<<(unsigned)c->n_scan_blocks, SCAN_THREADS, 0, st>>>(c->count, c->nkeys,
@@ -295,7 +301,7 @@ int launch_bin(Ctx *c, int transfer) {
   if (n > 0) {
     k_place<<<nblk(n, 256), 256, 0, st>>>(c->key, c->rank, c->start, n, c->order);
     k_canon<<<nblk(c->nkeys, 256), 256, 0, st>>>(c->count, c->start, c->nkeys, c->p.pid,
-                                                 c->order);
+                                                 c->order, n);
     const float *Cp = transfer == GF_APIC ? c->p.C : nullptr;
     k_permute<<<nblk(n, 256), 256, 0, st>>>(c->order, n, c->p.pos, c->p.vel, Cp, c->p.pid,
                                             c->rec0, c->rec1, c->rec2, c->rec3);
@@ -303,5 +309,7 @@ int launch_bin(Ctx *c, int transfer) {
   }
   return check_launch(c, "gf_bin");
 }
+
+GF_BOUNDS_READER(bin)
 
 }  // namespace gf

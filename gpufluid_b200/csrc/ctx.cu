@@ -401,6 +401,83 @@ int gf_step(void *ctx, const gf_step_params *prm) {
   return GF_OK;
 }
 
+// A captured substep: the instantiated graph and the kernels it launches.
+struct GfGraph {
+  cudaGraphExec_t exec = nullptr;
+  int64_t launches = 0;
+};
+
+int gf_graph_capture(void *ctx, const gf_step_params *prm, void **graph_out) {
+  Ctx *c = as_ctx(ctx);
+  if (!c || !prm || !graph_out) return GF_INVALID_ARG;
+  *graph_out = nullptr;
+  cudaStream_t st = c->stream;
+  bool own = false;
+  if (!st) {  // the legacy default stream cannot be captured: use a private one
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      return gf::fail(c, GF_CUDA_ERROR, "gf_graph_capture: stream creation failed");
+    }
+    own = true;
+  }
+  // everything the substep reads must be ready before the capture's first node
+  int e = gf::check_cuda(c, cudaStreamSynchronize(c->stream), "gf_graph_capture sync");
+  if (e) {
+    if (own) cudaStreamDestroy(st);
+    return e;
+  }
+  const bool timing = c->timing;
+  const cudaStream_t saved = c->stream;
+  c->timing = false;
+  c->stream = st;
+  const int64_t before = c->launches;
+  e = gf::check_cuda(c, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal),
+                     "gf_graph_capture begin");
+  int step_e = e ? e : gf_step(ctx, prm);
+  cudaGraph_t graph = nullptr;
+  if (!e) {
+    const cudaError_t ee = cudaStreamEndCapture(st, &graph);
+    if (!step_e && ee != cudaSuccess) step_e = gf::check_cuda(c, ee, "gf_graph_capture end");
+  }
+  c->timing = timing;
+  c->stream = saved;
+  const int64_t captured = c->launches - before;
+  c->launches = before;  // capturing ran nothing
+  GfGraph *g = nullptr;
+  if (!step_e && graph) {
+    g = new GfGraph();
+    g->launches = captured;
+    step_e = gf::check_cuda(c, cudaGraphInstantiate(&g->exec, graph, 0),
+                            "gf_graph_capture instantiate");
+  }
+  if (graph) cudaGraphDestroy(graph);
+  if (own) cudaStreamDestroy(st);
+  if (step_e) {
+    cudaGetLastError();
+    delete g;
+    return step_e;
+  }
+  *graph_out = g;
+  return GF_OK;
+}
+
+int gf_graph_replay(void *ctx, void *graph) {
+  Ctx *c = as_ctx(ctx);
+  GfGraph *g = reinterpret_cast<GfGraph *>(graph);
+  if (!c || !g || !g->exec) return GF_INVALID_ARG;
+  int e = gf::check_cuda(c, cudaGraphLaunch(g->exec, c->stream), "gf_graph_replay");
+  if (!e) c->launches += g->launches;
+  return e;
+}
+
+int gf_graph_destroy(void *graph) {
+  GfGraph *g = reinterpret_cast<GfGraph *>(graph);
+  if (!g) return GF_INVALID_ARG;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  delete g;
+  return GF_OK;
+}
+
 int gf_pressure_result(void *ctx, int32_t *iters, double *relres, int32_t *status) {
   Ctx *c = as_ctx(ctx);
   if (!c) return GF_INVALID_ARG;
@@ -508,6 +585,30 @@ int gf_pressure_stats(void *ctx, gf_pressure_info *info) {
     info->kernel = c->state_host->smem_solver ? 1 : 2;
   info->coarse = (info->kernel == 1 && c->state_host->coarse_used) ? 1 : 0;
   return e;
+}
+
+int gf_bounds_status(int32_t reset, int64_t *violations, int32_t *first_line,
+                     int32_t *checked) {
+  if (!violations || !first_line || !checked) return GF_INVALID_ARG;
+#ifdef GF_BOUNDS_CHECK
+  *checked = 1;
+#else
+  *checked = 0;
+#endif
+  *violations = 0;
+  *first_line = 0;
+  int (*readers[])(unsigned long long *, int *, int) = {gf::bounds_read_bin,
+                                                        gf::bounds_read_transfer,
+                                                        gf::bounds_read_pressure};
+  for (auto rd : readers) {
+    unsigned long long h = 0;
+    int line = 0;
+    const int e = rd(&h, &line, reset);
+    if (e) return e;
+    if (h && !*violations) *first_line = line;
+    *violations += (int64_t)h;
+  }
+  return GF_OK;
 }
 
 int gf_health_read(void *ctx, int32_t reset, gf_health *out) {

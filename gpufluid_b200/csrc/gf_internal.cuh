@@ -221,6 +221,47 @@ struct Ctx {
   std::string err;
 };
 
+// ---- bounds-checked build ---------------------------------------------------
+// Built with -DGF_BOUNDS_CHECK (libgfb200_checked.so), GF_IN(i, n) checks
+// 0 <= i < n for an index about to address global memory; a violation is
+// counted in the translation unit's device counter (with the source line of
+// the first one) and the access is skipped.  In the regular library GF_IN is
+// `true` and compiles away.  Each instrumented file ends with
+// GF_BOUNDS_READER(name), the host reader gf_bounds_status collects.
+#ifdef GF_BOUNDS_CHECK
+static __device__ unsigned long long g_bounds_hits;
+static __device__ int g_bounds_line;
+__device__ __forceinline__ bool gf_in(int64_t i, int64_t n, int line) {
+  if (i >= 0 && i < n) return true;
+  if (atomicAdd(&g_bounds_hits, 1ull) == 0ull) g_bounds_line = line;
+  return false;
+}
+#define GF_IN(i, n) ::gf::gf_in((int64_t)(i), (int64_t)(n), __LINE__)
+#define GF_BOUNDS_READER(name)                                                          \
+  int bounds_read_##name(unsigned long long *hits, int *line, int reset) {             \
+    if (cudaMemcpyFromSymbol(hits, g_bounds_hits, sizeof(*hits)) != cudaSuccess ||     \
+        cudaMemcpyFromSymbol(line, g_bounds_line, sizeof(*line)) != cudaSuccess)        \
+      return GF_CUDA_ERROR;                                                              \
+    if (reset) {                                                                         \
+      const unsigned long long z = 0;                                                    \
+      if (cudaMemcpyToSymbol(g_bounds_hits, &z, sizeof(z)) != cudaSuccess)               \
+        return GF_CUDA_ERROR;                                                            \
+    }                                                                                    \
+    return GF_OK;                                                                        \
+  }
+#else
+#define GF_IN(i, n) true
+#define GF_BOUNDS_READER(name)                                                          \
+  int bounds_read_##name(unsigned long long *hits, int *line, int) {                   \
+    *hits = 0;                                                                           \
+    *line = 0;                                                                           \
+    return GF_OK;                                                                        \
+  }
+#endif
+int bounds_read_transfer(unsigned long long *hits, int *line, int reset);
+int bounds_read_bin(unsigned long long *hits, int *line, int reset);
+int bounds_read_pressure(unsigned long long *hits, int *line, int reset);
+
 // ---- helpers ---------------------------------------------------------------
 int fail(Ctx *c, int status, const std::string &msg);
 int check_cuda(Ctx *c, cudaError_t e, const char *what);

@@ -303,7 +303,10 @@ __global__ void k_jacobi(SweepArgs a, const float *__restrict__ xin, float *__re
     float s = 0.0f;
 #pragma unroll
     for (int d = 0; d < 6; ++d)
-      if (code & (1 << d)) s = s + xin[nb_index(q, d, a.nbr)];
+      if (code & (1 << d)) {
+        const int64_t nq = nb_index(q, d, a.nbr);
+        if (GF_IN(nq, total)) s = s + xin[nq];
+      }
     const float diag = (float)((code >> CODE_DIAG_SHIFT) & 7);
     xout[q] = diag < 0.5f ? 0.0f : (s - a.bdiv[q]) / diag;
   }
@@ -320,7 +323,10 @@ __global__ void k_gsrb(SweepArgs a, float *__restrict__ x, int color) {
     float s = 0.0f;
 #pragma unroll
     for (int d = 0; d < 6; ++d)
-      if (code & (1 << d)) s = s + x[nb_index(q, d, a.nbr)];
+      if (code & (1 << d)) {
+        const int64_t nq = nb_index(q, d, a.nbr);
+        if (GF_IN(nq, total)) s = s + x[nq];
+      }
     const float diag = (float)((code >> CODE_DIAG_SHIFT) & 7);
     x[q] = diag < 0.5f ? 0.0f : (s - a.bdiv[q]) / diag;
   }
@@ -595,7 +601,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
           for (int d = 0; d < 6; ++d)
             if (cd[m] & (1 << d)) {
               const int64_t nq = nb_index(q, d, a.nbr);
-              s = s + (__ldcg(Z + nq) + beta * __ldcg(dold + nq));
+              if (GF_IN(nq, total)) s = s + (__ldcg(Z + nq) + beta * __ldcg(dold + nq));
             }
           sn[m] = s;
         }
@@ -741,7 +747,10 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
         double s = 0.0;
 #pragma unroll
         for (int d = 0; d < 6; ++d)
-          if (code & (1 << d)) s += __ldcg(a.x64 + nb_index(q, d, a.nbr));
+          if (code & (1 << d)) {
+            const int64_t nq = nb_index(q, d, a.nbr);
+            if (GF_IN(nq, total)) s += __ldcg(a.x64 + nq);
+          }
         const double diag = (double)((code >> CODE_DIAG_SHIFT) & 7);
         return (double)(a.sign * a.bdiv[q]) - (diag * __ldcg(a.x64 + q) - s);
       };
@@ -980,6 +989,8 @@ __device__ __forceinline__ bool pcg_scene(const SegPcgArgs &a, const PcgJob &j) 
   __shared__ int s_flag;     // done / replacement pending
   PcgState *S = a.st + j.scene;
   const int tid = threadIdx.x;
+  const int64_t total = (int64_t)(*a.n_active) * TILE_CELLS;  // compact cells (bounds checks)
+  (void)total;
   const int t_begin = __ldg(a.slot0 + j.scene) + j.rank, t_end = __ldg(a.slot0 + j.scene + 1);
   const int step = SEG_TG * j.nb;
   float *__restrict__ X = a.x;
@@ -1065,7 +1076,7 @@ __device__ __forceinline__ bool pcg_scene(const SegPcgArgs &a, const PcgJob &j) 
           for (int d = 0; d < 6; ++d)
             if (cd[m] & (1 << d)) {
               const int64_t nq = nb_index(q, d, a.nbr);
-              s = s + (__ldcg(Z + nq) + beta * __ldcg(dold + nq));
+              if (GF_IN(nq, total)) s = s + (__ldcg(Z + nq) + beta * __ldcg(dold + nq));
             }
           sn[m] = s;
         }
@@ -1255,6 +1266,7 @@ struct ScatterArgs {
   const PcgState *st_err;
   int nst;
   int32_t *health;
+  int64_t ncell;  // cells of p (all scenes of a batch)
 };
 
 // Severity of a solve status: OK < NOT_CONVERGED < BREAKDOWN < NAN < TIMEOUT.
@@ -1310,7 +1322,8 @@ __global__ void k_scatter_p(ScatterArgs a) {
     const int gi = ti * 8 + (l >> 6), gj = tj * 8 + ((l >> 3) & 7), gk = tk * 8 + (l & 7);
     float v = a.x[q];
     if (a.x64) v = (float)(a.x64[q] + (double)v);
-    a.p[((int64_t)gi * a.ny + gj) * a.nz + gk] = v;
+    const int64_t g = ((int64_t)gi * a.ny + gj) * a.nz + gk;
+    if (GF_IN(g, a.ncell)) a.p[g] = v;
   }
 }
 
@@ -1328,7 +1341,8 @@ __global__ void kb_scatter_p(ScatterArgs a, SegIndex sx) {
     const int gi = ti * 8 + (l >> 6), gj = tj * 8 + ((l >> 3) & 7), gk = tk * 8 + (l & 7);
     float v = a.x[q];
     if (a.x64) v = (float)(a.x64[q] + (double)v);
-    a.p[r.cell0 + ((int64_t)gi * r.ny + gj) * r.nz + gk] = v;
+    const int64_t g = r.cell0 + ((int64_t)gi * r.ny + gj) * r.nz + gk;
+    if (GF_IN(g, a.ncell)) a.p[g] = v;
   }
 }
 
@@ -1529,7 +1543,8 @@ static int launch_pressure_batch(Ctx *c, const gf_step_params *prm) {
   if ((e = check_cuda(c, cudaMemsetAsync(c->f.p, 0, c->ncell * 4, st), "zero p"))) return e;
   const bool pcg = solver == GF_PCG || solver == GF_PCG_REFINED;
   ScatterArgs sc{c->n_active, c->tile_list, c->code, result, result64, c->f.p, 0, 0, 0, 0,
-                 pcg ? c->seg_state : nullptr, pcg ? c->state : nullptr, c->nseg, c->health};
+                 pcg ? c->seg_state : nullptr, pcg ? c->state : nullptr, c->nseg, c->health,
+                 c->ncell};
   kb_scatter_p<<<gs, 256, 0, st>>>(sc, sx);
   c->launches++;
   c->last_solver = solver;
@@ -1643,11 +1658,13 @@ int launch_pressure(Ctx *c, const gf_step_params *prm) {
   const bool pcg = solver == GF_PCG || solver == GF_PCG_REFINED;
   ScatterArgs sc{c->n_active, c->tile_list, c->code, result, result64, c->f.p,
                  c->ny, c->nz, c->nty, c->ntz, pcg ? c->state : nullptr,
-                 pcg ? c->state : nullptr, 1, c->health};
+                 pcg ? c->state : nullptr, 1, c->health, c->ncell};
   k_scatter_p<<<gs, 256, 0, st>>>(sc);
   c->launches++;
   c->last_solver = solver;
   return check_launch(c, "gf_pressure");
 }
+
+GF_BOUNDS_READER(pressure)
 
 }  // namespace gf

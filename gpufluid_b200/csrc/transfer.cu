@@ -91,8 +91,10 @@ __device__ __forceinline__ void scatter_comp(T *s_val, T *s_wt, int comp, float 
             atomicAdd(&s_wt[e], (T)wt);
           } else {  // only reachable for positions outside their clamped cell
             int64_t g = ((int64_t)ii * sny + jj) * snz + kk;
-            atomicAdd(&gval[g], add);
-            atomicAdd(&gwt[g], wt);
+            if (GF_IN(g, (int64_t)snx * sny * snz)) {
+              atomicAdd(&gval[g], add);
+              atomicAdd(&gwt[g], wt);
+            }
           }
         }
       }
@@ -149,6 +151,7 @@ __device__ __forceinline__ bool scatter_comp_fast(T *s_val, T *s_wt, int comp, f
         const float wt = wxy * wz[dk];
         const float val = ab + C[dk];
         const int e = base + (di * ey + dj) * ez + dk;
+        if (!GF_IN(e, BOX)) continue;
         atomicAdd(&s_val[e], (T)(val * wt));
         atomicAdd(&s_wt[e], (T)wt);
       }
@@ -179,6 +182,7 @@ __device__ __forceinline__ void p2g_flush_box(const P2GArgs &a, T (*s_val)[BOX],
     int64_t g = ((int64_t)ii * sny + jj) * snz + kk;
     float *gv = comp == 0 ? a.u : (comp == 1 ? a.v : a.w);
     float *gw = comp == 0 ? a.uw : (comp == 1 ? a.vw : a.ww);
+    if (!GF_IN(g, (int64_t)snx * sny * snz)) continue;
     if (ex_x && ex_y && ex_z) {
       gv[g] = val;
       gw[g] = wt;
@@ -412,15 +416,18 @@ __device__ __forceinline__ float clampf(float x, float lo, float hi) {
 struct GlobalAt {
   const float *__restrict__ f;
   int64_t si, sj;
+  int64_t n;  // elements of the array (checked in the bounds-checked build)
   __device__ __forceinline__ float operator()(int i, int j, int k) const {
-    return __ldg(f + (int64_t)i * si + (int64_t)j * sj + k);
+    const int64_t q = (int64_t)i * si + (int64_t)j * sj + k;
+    return GF_IN(q, n) ? __ldg(f + q) : 0.0f;
   }
 };
 struct BoxAt {
   const float *s;
-  int oi, oj, ok, nj, nk;
+  int oi, oj, ok, nj, nk, vol;
   __device__ __forceinline__ float operator()(int i, int j, int k) const {
-    return s[((i - oi) * nj + (j - oj)) * nk + (k - ok)];
+    const int q = ((i - oi) * nj + (j - oj)) * nk + (k - ok);
+    return GF_IN(q, vol) ? s[q] : 0.0f;
   }
 };
 
@@ -468,7 +475,8 @@ __device__ __forceinline__ float sample3(const float *__restrict__ f, float fx, 
                                          float fz, int nxm, int nym, int nzm) {
   int i0, j0, k0, i1, j1, k1;
   sample3_index(fx, fy, fz, nxm, nym, nzm, i0, j0, k0, i1, j1, k1);
-  return sample3_at(GlobalAt{f, (int64_t)nym * nzm, nzm}, fx, fy, fz, i0, j0, k0, i1, j1, k1);
+  return sample3_at(GlobalAt{f, (int64_t)nym * nzm, nzm, (int64_t)nxm * nym * nzm}, fx, fy, fz,
+                    i0, j0, k0, i1, j1, k1);
 }
 
 // One face component of k3_g2p_apic_advect (:1626-1724): clamped-index
@@ -521,8 +529,8 @@ __device__ __forceinline__ void apic_gather(const float *__restrict__ f, float p
                                             float pz, float dx, float fx, float fy, float fz,
                                             int snx, int sny, int snz, int ax, float inv,
                                             float &vel, float &c0, float &c1, float &c2) {
-  apic_gather_at(GlobalAt{f, (int64_t)sny * snz, snz}, px, py, pz, dx, fx, fy, fz, snx, sny, snz,
-                 ax, inv, vel, c0, c1, c2);
+  apic_gather_at(GlobalAt{f, (int64_t)sny * snz, snz, (int64_t)snx * sny * snz}, px, py, pz, dx,
+                 fx, fy, fz, snx, sny, snz, ax, inv, vel, c0, c1, c2);
 }
 
 struct G2PArgs {
@@ -733,7 +741,8 @@ __global__ void __launch_bounds__(G2P_TILE_THREADS)
         const int bk = v % nk, r = v / nk, bj = r % nj, bi = r / nj;
         const int gi = oi + bi, gj = oj + bj, gk = ok + bk;
         float val = 0.f;
-        if (gi >= 0 && gi < snx && gj >= 0 && gj < sny && gk >= 0 && gk < snz)
+        if (gi >= 0 && gi < snx && gj >= 0 && gj < sny && gk >= 0 && gk < snz &&
+            GF_IN(((int64_t)gi * sny + gj) * snz + gk, (int64_t)snx * sny * snz))
           val = __ldg(src[q] + ((int64_t)gi * sny + gj) * snz + gk);
         dst[v] = val;
       }
@@ -764,7 +773,7 @@ __global__ void __launch_bounds__(G2P_TILE_THREADS)
   for (int q = 0; q < NARR; ++q) {
     const int c = q % 3;
     bx[q] = BoxAt{s_box + (q / 3) * GBOX_SET + gbox_off(c), I0 - (c != 0), J0 - (c != 1),
-                  c == 2 ? K0 : K0 - 4, gbox_nj(c), gbox_nk(c)};
+                  c == 2 ? K0 : K0 - 4, gbox_nj(c), gbox_nk(c), gbox_vol(c)};
   }
   const float dx = a.dx;
   int *s_pid = reinterpret_cast<int *>(s_out + (APIC ? 3840 : 1536));
@@ -795,7 +804,7 @@ __global__ void __launch_bounds__(G2P_TILE_THREADS)
                            inv, vel3[cc], c[3 * cc], c[3 * cc + 1], c[3 * cc + 2]);
           else
             apic_gather_at(GlobalAt{cc == 0 ? a.u : (cc == 1 ? a.v : a.w),
-                                    (int64_t)sny * snz, snz},
+                                    (int64_t)sny * snz, snz, (int64_t)snx * sny * snz},
                            px, py, pz, dx, fxs[cc], fys[cc], fzs[cc], snx, sny, snz, cc, inv,
                            vel3[cc], c[3 * cc], c[3 * cc + 1], c[3 * cc + 2]);
         }
@@ -820,10 +829,11 @@ __global__ void __launch_bounds__(G2P_TILE_THREADS)
           } else {
             const float *fp = cc == 0 ? a.u : (cc == 1 ? a.v : a.w);
             const float *fs = cc == 0 ? a.us : (cc == 1 ? a.vs : a.ws);
-            pic[cc] = sample3_at(GlobalAt{fp, (int64_t)sny * snz, snz}, fx, fy, fz, i0, j0, k0,
-                                 i1, j1, k1);
-            old[cc] = sample3_at(GlobalAt{fs, (int64_t)sny * snz, snz}, fx, fy, fz, i0, j0, k0,
-                                 i1, j1, k1);
+            const int64_t nf = (int64_t)snx * sny * snz;
+            pic[cc] = sample3_at(GlobalAt{fp, (int64_t)sny * snz, snz, nf}, fx, fy, fz, i0, j0,
+                                 k0, i1, j1, k1);
+            old[cc] = sample3_at(GlobalAt{fs, (int64_t)sny * snz, snz, nf}, fx, fy, fz, i0, j0,
+                                 k0, i1, j1, k1);
           }
         }
         float fu = r1.x + (pic[0] - old[0]), fv = r1.y + (pic[1] - old[1]),
@@ -1148,5 +1158,7 @@ int launch_vmax(Ctx *c) {
   }
   return check_launch(c, "gf_vmax");
 }
+
+GF_BOUNDS_READER(transfer)
 
 }  // namespace gf

@@ -153,6 +153,18 @@ int gf_project(void *ctx, float dt, float rho);
 int gf_g2p(void *ctx, int32_t transfer, float flip_blend, float dt);
 /* The whole substep in _step_impl order (:3475-3667). */
 int gf_step(void *ctx, const gf_step_params *prm);
+/* The substep captured once as a CUDA graph and replayed: the reference's
+ * graph cache (_cuda_graph_*, solver3d.py:3361-3418).  gf_graph_capture
+ * synchronises the bound stream, records gf_step(prm) on it (on a private
+ * stream when none is bound) without running it, and returns an instantiated
+ * graph in *graph_out; every parameter and the bound buffers are baked in,
+ * so rebinding or new parameters need a new capture.  gf_graph_replay
+ * launches it on the bound stream (asynchronous); gf_graph_destroy frees it.
+ * gf_step allocates nothing and never synchronises, which is what makes it
+ * capturable; the stage-timing events are left out of a capture. */
+int gf_graph_capture(void *ctx, const gf_step_params *prm, void **graph_out);
+int gf_graph_replay(void *ctx, void *graph);
+int gf_graph_destroy(void *graph);
 
 /* ---- results and diagnostics ------------------------------------------- */
 /* Last solve's iteration count, final relative residual (||r||/||r0||),
@@ -207,6 +219,16 @@ typedef struct gf_health {
                             tile loads); the stage's results are then incomplete */
 } gf_health;
 int gf_health_read(void *ctx, int32_t reset, gf_health *out);
+/* The bounds-checked build (libgfb200_checked.so, compiled with
+ * -DGF_BOUNDS_CHECK; no counterpart in the reference, whose kernels index
+ * unchecked, solver3d.py:100-101) checks the grid, tile, sort-slot and
+ * neighbour indices its binning, transfer and pressure kernels compute before
+ * they address global or shared memory, skips any access out of range and
+ * counts it.  This reads the count since the last reset (all contexts of the
+ * process) and the source line of the first violation; *checked = 1 in that
+ * build, 0 in the regular one (where the count is always 0).  Synchronises. */
+int gf_bounds_status(int32_t reset, int64_t *violations, int32_t *first_line,
+                     int32_t *checked);
 /* Active 8^3 pressure tiles of the last solve (k_mark_active_blocks,
  * solver3d.py:953-972): count and tile ids (device pointer). */
 int gf_active_tiles(void *ctx, int32_t *n_active, const int32_t **tiles);

@@ -148,6 +148,43 @@ def test_graph_replay_matches_direct(gf, solver):
     assert rel_l2(out[1][1], out[0][1]) < 1e-6
 
 
+@pytest.mark.parametrize("solver", ["jacobi", "pcg_refined"])
+def test_c_abi_graph_capture_matches_direct(gf, solver):
+    """gf_graph_capture / gf_graph_replay (the reference's graph cache,
+    solver3d.py:3361-3418, as C entry points): five replays give the state of
+    five direct gf_step calls, and the launch count advances per replay."""
+    import ctypes
+    import torch
+    from gpufluid_b200 import _lib
+    out = []
+    for use_graph in (False, True):
+        s = dam_break(gf.FlipSolver3D, (24, 24, 24), box=((0.1, 0.1, 0.1), (0.5, 0.7, 0.5)))
+        s.vel = np.random.default_rng(3).normal(0, 0.5, (s.n_particles, 3)).astype(np.float32)
+        prm = s._params(0.005, 60, solver)
+        s._set_stream()
+        if use_graph:
+            g = ctypes.c_void_p()
+            _lib.check(s._L.gf_graph_capture(s._ctx, ctypes.byref(prm), ctypes.byref(g)),
+                       s._ctx, "gf_graph_capture")
+            n0 = int(s._L.gf_launch_count(s._ctx))
+            for _ in range(5):
+                _lib.check(s._L.gf_graph_replay(s._ctx, g), s._ctx, "gf_graph_replay")
+            torch.cuda.synchronize()
+            per = (int(s._L.gf_launch_count(s._ctx)) - n0) // 5
+            assert per > 5
+            assert s._L.gf_graph_destroy(g) == 0
+        else:
+            for _ in range(5):
+                _lib.check(s._L.gf_step(s._ctx, ctypes.byref(prm)), s._ctx, "gf_step")
+        s._pressure_stale = True
+        out.append((np.concatenate([s.u.numpy().ravel(), s.v.numpy().ravel(),
+                                    s.w.numpy().ravel()]), s.get_particles()[0],
+                    s.pressure_health()["solves"]))
+    assert rel_l2(out[1][0], out[0][0]) < 1e-4
+    assert rel_l2(out[1][1], out[0][1]) < 1e-6
+    assert out[0][2] == out[1][2] == 5  # the solve health is folded in on replay too
+
+
 def test_checkpoint_resume_matches_continuous(gf, tmp_path):
     """test_f3_5_checkpoint.py:11-41."""
     a = dam_break(gf.FlipSolver3D, (16, 16, 16), transfer="apic")
