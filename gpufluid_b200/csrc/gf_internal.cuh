@@ -90,6 +90,13 @@ struct PcgSmemArgs {
   float *cbuf;                // coarse: rows of B, then the compact rows of P^T A P
   int test_stall;             // GF_FLAG_TEST_STALL: the first all-reduce waits for a count
                               // no block publishes, with a short spin limit
+  // GF_FLAG_WARM_START (refined solve): start from the dense pressure p0 (the
+  // previous substep's) instead of 0; tile_list and the grid shape map a
+  // compact cell to its dense index
+  int warm;
+  const float *p0;
+  const int32_t *tile_list;
+  int ny, nz, nty, ntz;
 };
 
 

@@ -799,6 +799,12 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   unsigned fmask = 0, hmask = 0, dpack = 0;
   unsigned spack = 0;  // coarse sub-region of the tile of each j (2 bits)
   float rs[CK] = {0.f, 0.f, 0.f, 0.f};
+  // warm start (refined only): x64 = the dense p0 at the cell, r = b - A x64
+  // in FP64 with the neighbours' p0 read from the dense array (complete and
+  // read-only during the solve, so no halo exchange); the stop test stays
+  // relative to ||b||, so the accuracy target is the cold start's
+  const bool warm = REF && a.warm && a.p0 != nullptr;
+  double wb2 = 0.0, wr2 = 0.0;  // this thread's sums of b^2 and r0^2
 #pragma unroll
   for (int j = 0; j < MAXJ; ++j) {
     const int tl = tl0 + 2 * j;
@@ -807,10 +813,28 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
     const uint16_t code = a.code[q0 + L];
     s_code[L] = code;
     float b = 0.f;
+    double x0 = 0.0;
     if (code & CODE_FLUID) {
       fmask |= 1u << j;
       dpack |= (unsigned)((code >> CODE_DIAG_SHIFT) & 7) << (3 * j);
       b = a.sign * a.bdiv[q0 + L];
+      if (warm) {
+        const int t = a.tile_list[b0 + tl];
+        const int ti = t / (a.nty * a.ntz), tj = (t / a.ntz) % a.nty, tk = t % a.ntz;
+        const int64_t sI = (int64_t)a.ny * a.nz;
+        const int64_t g = (int64_t)(ti * 8 + (l >> 6)) * sI + (tj * 8 + ((l >> 3) & 7)) * a.nz +
+                          (tk * 8 + (l & 7));
+        x0 = (double)a.p0[g];
+        const int64_t off[6] = {-sI, sI, -(int64_t)a.nz, (int64_t)a.nz, -1, 1};
+        double sum = 0.0;
+#pragma unroll
+        for (int dir = 0; dir < 6; ++dir)
+          if (code & (1 << dir)) sum += (double)a.p0[g + off[dir]];
+        const double res = (double)b - ((double)((code >> CODE_DIAG_SHIFT) & 7) * x0 - sum);
+        wb2 += (double)b * (double)b;
+        wr2 += res * res;
+        b = (float)res;  // from here on, the initial residual
+      }
       s_zb[tl * 1000 + pc] =
           SGS ? b * s_rtab[8 | ((code >> CODE_DIAG_SHIFT) & 7)] : b / diagz_of(code);
       if (is_halo(L, s_mask)) hmask |= 1u << j;
@@ -819,7 +843,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
     s_x[L] = 0.f;
     s_d[L] = 0.f;
     s_s[L] = 0.f;
-    if (REF) s_x64[L] = 0.0;
+    if (REF) s_x64[L] = x0;
     if (CRS && coarse) {
       const int sub = tl * K / nt;
       spack |= (unsigned)sub << (2 * j);
@@ -1028,13 +1052,19 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   }
   Acc t3[3];
   if (!fast_allreduce3<Acc>(fs, gs, v3, t3, sh)) return;
+  double wtot[2] = {0.0, 0.0};
+  if (warm) {  // ||b||^2 and the FP64 ||b - A x0||^2 of the warm start
+    const double wv[2] = {wb2, wr2};
+    if (!grid_allreduce<double, 2>(gs, wv, wtot, shd)) return;
+  }
   Acc gamma = t3[0];
   const Acc r0 = t3[2];
-  const double b2 = (double)t3[2];
-  double r_upd2 = b2, r_true2 = b2, rr_last = b2;
+  const double b2 = warm ? wtot[0] : (double)t3[2];
+  double r_upd2 = (double)t3[2], r_true2 = warm ? wtot[1] : b2, rr_last = (double)t3[2];
   Acc alpha = fabs((double)t3[1]) < 1.0e-30 ? (Acc)0 : gamma / t3[1];
   Acc beta = 0;
-  int done = (double)r0 < 1e-30 ? 1 : 0, iters = 0, nrep = 0, status = GF_OK;
+  int done = warm ? (b2 < 1e-30 || r_true2 <= a.tol2 * b2 ? 1 : 0) : ((double)r0 < 1e-30 ? 1 : 0);
+  int iters = 0, nrep = 0, status = GF_OK;
 
   for (int it = 0; it < a.max_iter && !done; ++it) {
     const float alphaf = (float)alpha, nalpha = -alphaf, betaf = (float)beta;

@@ -1634,7 +1634,9 @@ int launch_pressure(Ctx *c, const gf_step_params *prm) {
                      prm->max_iters, check_every, prm->tol * prm->tol, replace2, sign,
                      (prm->flags & GF_FLAG_SGS_MASK) >> GF_FLAG_SGS_SHIFT,
                      coarse ? COARSE_K : 0, c->coarse_buf,
-                     (prm->flags & GF_FLAG_TEST_STALL) ? 1 : 0};
+                     (prm->flags & GF_FLAG_TEST_STALL) ? 1 : 0,
+                     (refined && (prm->flags & GF_FLAG_WARM_START)) ? 1 : 0, c->f.p,
+                     c->tile_list, c->ny, c->nz, c->nty, c->ntz};
       // the solver publishes tagged 64-bit halo words over the first two halo
       // arrays; their counts restart at 1 with every solve
       if ((e = check_cuda(c, cudaMemsetAsync(h, 0, (size_t)nk * 8, st), "zero tagged halo")))

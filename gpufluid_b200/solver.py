@@ -26,6 +26,9 @@ default path):
 * ``pcg_coarse=True`` (new): adds a coarse correction to the shared-memory
   PCG's preconditioner -- one constant per region, four regions of tiles per
   solver block -- for fewer iterations again.
+* ``pcg_warm_start=True`` (new): the refined shared-memory PCG starts from
+  the previous substep's pressure instead of zero (the reference's solves
+  start from zero); the stop test stays relative to ||b||.
 * Particles are kept sorted by cell inside the solver; ``pos``/``vel``/
   ``affine_C``/``get_particles()`` return them in the caller's original order.
 * Viscosity, surface tension, colour/temperature attributes, sub-dense storage,
@@ -163,7 +166,8 @@ class FlipSolver3D:
                  pcg_check_every: int = 10,
                  pcg_preconditioner: str = "jacobi",
                  pcg_sgs_sweeps: int = 2,
-                 pcg_coarse: bool = False):
+                 pcg_coarse: bool = False,
+                 pcg_warm_start: bool = False):
         if pcg_preconditioner not in ("jacobi", "tile_sgs"):
             raise ValueError(f"unknown pcg_preconditioner: {pcg_preconditioner!r}")
         if not 1 <= int(pcg_sgs_sweeps) <= 3:
@@ -193,6 +197,7 @@ class FlipSolver3D:
         self.pcg_preconditioner = pcg_preconditioner
         self.pcg_sgs_sweeps = int(pcg_sgs_sweeps)
         self.pcg_coarse = bool(pcg_coarse)
+        self.pcg_warm_start = bool(pcg_warm_start)
         self._enable_cuda_graphs = bool(enable_cuda_graphs)
         self._enable_sub_dense = bool(enable_sub_dense)
         self._prof = StepProfiler(enabled=enable_timing)
@@ -390,6 +395,8 @@ class FlipSolver3D:
 
     def _pcg_flags(self) -> int:
         f = _lib.GF_FLAG_COARSE if self.pcg_coarse else 0
+        if self.pcg_warm_start:
+            f |= _lib.GF_FLAG_WARM_START
         if self.pcg_preconditioner == "tile_sgs":
             f |= self.pcg_sgs_sweeps << _lib.GF_FLAG_SGS_SHIFT
         return f

@@ -116,6 +116,13 @@ typedef struct gf_step_params {
  * gf_health_read).  It exercises the bounded-wait exit path without a fault;
  * the context stays usable.  No effect on the global-memory kernel. */
 #define GF_FLAG_TEST_STALL 64
+/* flags: the refined shared-memory PCG starts from the pressure in fields.p
+ * (the previous substep's solution) instead of from zero; the initial
+ * residual b - A p is formed in FP64 and the stop test stays ||b - A x|| <=
+ * tol ||b||, so the answer's accuracy is the cold start's.  No counterpart in
+ * the reference (its solves start from zero every substep); other solvers
+ * ignore it. */
+#define GF_FLAG_WARM_START 128
 
 /* ---- context ------------------------------------------------------------ */
 /* Allocates scratch for a grid and up to max_particles particles on the

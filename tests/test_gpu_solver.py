@@ -230,3 +230,27 @@ def test_unknown_solver_raises(gf):
     s = dam_break(gf.FlipSolver3D, (8, 8, 8))
     with pytest.raises(ValueError, match="unknown pressure_solver"):
         s.step(0.005, pressure_solver="multigrid")
+
+
+def test_refined_pcg_warm_start(gf, oracle):
+    """pcg_warm_start: the refined solve starts from the previous substep's
+    pressure.  Same FP64-residual target (relative to ||b||), the answer
+    within 1e-6 of an FP64 solve of each substep's system, fewer iterations
+    than the cold start once the flow is under way."""
+    from gpufluid_b200 import scene
+    it = {}
+    for warm in (False, True):
+        s = gf.FlipSolver3D(64, 64, 64, transfer_mode="apic", pressure_tol=1e-8,
+                            pcg_preconditioner="tile_sgs", pcg_coarse=True, pcg_warm_start=warm)
+        s.add_solid_from_sdf(scene.sdf_sphere(s.cell_centers_np(), (0.7, 0.2, 0.5), 0.12))
+        s.seed_box((0.0, 0.0, 0.0), (0.4, 0.6, 1.0))
+        n = []
+        for k in range(12):
+            s.step(1 / 480, pressure_iters=4000, pressure_solver="pcg_refined")
+            st = s.pressure_stats()
+            assert st["status"] == 0 and st["kernel"] == 1 and st["relres"] <= 1e-8, (warm, st)
+            n.append(st["iters"])
+        p64, _, _ = oracle.pcg64(s.marker.numpy(), s.div.cpu().numpy(), tol=1e-14)
+        assert rel_l2(s.p.numpy(), p64) < 1e-6
+        it[warm] = n
+    assert sum(it[True][4:]) < sum(it[False][4:]), it
