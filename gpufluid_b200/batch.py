@@ -47,7 +47,8 @@ class BatchedFlip3D:
                  flip_blend: float = 0.95, rho: float = 1.0, transfer_mode: str = "flip",
                  device: Optional[str] = None, pressure_tol: float = 1e-4,
                  pcg_rhs_sign: int = -1, pcg_check_every: int = 10,
-                 enable_cuda_graphs: bool = True):
+                 enable_cuda_graphs: bool = True, pcg_preconditioner: str = "jacobi",
+                 pcg_sgs_sweeps: int = 2):
         if transfer_mode not in _lib.TRANSFER:
             raise ValueError(f"unknown transfer_mode: {transfer_mode!r}")
         if not torch.cuda.is_available():
@@ -60,6 +61,14 @@ class BatchedFlip3D:
         self.pressure_tol = float(pressure_tol)
         self.pcg_rhs_sign = -1 if pcg_rhs_sign < 0 else 1
         self.pcg_check_every = int(pcg_check_every)
+        if pcg_preconditioner not in ("jacobi", "tile_sgs"):
+            raise ValueError(f"unknown pcg_preconditioner: {pcg_preconditioner!r}")
+        if not 1 <= int(pcg_sgs_sweeps) <= 3:
+            raise ValueError("pcg_sgs_sweeps must be 1, 2 or 3")
+        # "tile_sgs": tile-local symmetric Gauss-Seidel sweeps precondition
+        # every scene's PCG (the reference's Jacobi by default)
+        self.pcg_preconditioner = pcg_preconditioner
+        self.pcg_sgs_sweeps = int(pcg_sgs_sweeps)
         self._enable_cuda_graphs = bool(enable_cuda_graphs)
         self.grids = []
         descs = (_lib.GridDesc * len(grids))()
@@ -171,7 +180,9 @@ class BatchedFlip3D:
         return _lib.StepParams(float(dt), float(self.gravity), float(self.rho),
                                float(self.flip_blend), _lib.TRANSFER[self.transfer_mode],
                                _lib.SOLVER[pressure_solver], int(pressure_iters),
-                               self.pcg_check_every, self.pressure_tol, self.pcg_rhs_sign, 0)
+                               self.pcg_check_every, self.pressure_tol, self.pcg_rhs_sign,
+                               (self.pcg_sgs_sweeps << _lib.GF_FLAG_SGS_SHIFT)
+                               if self.pcg_preconditioner == "tile_sgs" else 0)
 
     def _set_stream(self):
         self._L.gf_set_stream(self._ctx, torch.cuda.current_stream(self.device).cuda_stream)
@@ -183,7 +194,7 @@ class BatchedFlip3D:
             self._set_stream()
             _lib.check(self._L.gf_step(self._ctx, ctypes.byref(prm)), self._ctx, "gf_step")
             return
-        key = (pressure_solver, self.n_particles, float(dt), int(pressure_iters))
+        key = (self.n_particles,) + tuple(getattr(prm, f) for f, _ in prm._fields_)
         if key in self._graphs:
             self._graphs.move_to_end(key)
         else:

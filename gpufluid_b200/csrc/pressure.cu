@@ -848,6 +848,7 @@ struct SegPcgArgs {
   int max_iter, check_every;
   double tol2, replace2;
   float sign;
+  int sgs;           // tile-local symmetric Gauss-Seidel sweeps (0: Jacobi)
 };
 
 // Job table (one thread): `grid` blocks; the target tiles per block grows
@@ -904,6 +905,8 @@ __global__ void k_pcg_plan(const int32_t *__restrict__ slot0, int nseg, int grid
 }
 
 constexpr int SEG_TG = 4;  // tiles per block step: loads of 4 tiles in flight per thread
+static_assert(SEG_TG == SGS_TB && TILE_CELLS == PCG_THREADS,
+              "the segmented PCG's tile groups are the preconditioner's rounds");
 
 // Block sums of NV per-thread values added to tot[] (shared, by thread 0),
 // once per phase (all of a block's tiles belong to one scene):
@@ -982,9 +985,16 @@ __device__ __forceinline__ bool scene_reduce(const SegPcgArgs &a, const PcgJob &
   return s_ok && !ld_volatile_i(&a.g->error);
 }
 
-template <typename Acc, bool REF>
+template <typename Acc, bool REF, bool SGS>
 __device__ __forceinline__ bool pcg_scene(const SegPcgArgs &a, const PcgJob &j) {
   __shared__ double tot[3];
+  // boxes of the tile preconditioner (SGS instantiation), rings zero throughout
+  __shared__ alignas(16) unsigned char sg_raw[SGS ? sizeof(SgsSmem) : 16];
+  SgsSmem &SG = *reinterpret_cast<SgsSmem *>(sg_raw);
+  if (SGS) {
+    for (int q = threadIdx.x; q < SGS_TB * 1000; q += blockDim.x) SG.zb[q] = 0.f;
+    __syncthreads();
+  }
   __shared__ float s_scal;   // alpha or beta of the running phase
   __shared__ int s_flag;     // done / replacement pending
   PcgState *S = a.st + j.scene;
@@ -1018,6 +1028,30 @@ __device__ __forceinline__ bool pcg_scene(const SegPcgArgs &a, const PcgJob &j) 
         const int64_t q = (int64_t)sl * TILE_CELLS + tid;
         cd[m] = sl < t_end ? CODE[q] : (uint16_t)0;
         bb[m] = (cd[m] & CODE_FLUID) ? a.bdiv[q] : 0.0f;
+      }
+      if (SGS) {  // z = M^-1 r by tile-local symmetric Gauss-Seidel sweeps
+#pragma unroll
+        for (int m = 0; m < SEG_TG; ++m) {
+          const int64_t q = (int64_t)(base + m * j.nb) * TILE_CELLS + tid;
+          const float b = (cd[m] & CODE_FLUID) ? a.sign * bb[m] : 0.0f;
+          if (cd[m] & CODE_FLUID) R[q] = b;
+          bb[m] = b;
+          SG.r[m * 512 + tid] = b;
+          SG.code[m * 512 + tid] = cd[m];
+          SG.zb[m * 1000 + tile_pad(tid)] = b * sgs_factor(cd[m]);
+        }
+        sgs_sweeps(SG, a.sgs);
+#pragma unroll
+        for (int m = 0; m < SEG_TG; ++m) {
+          if (!(cd[m] & CODE_FLUID)) continue;
+          const int64_t q = (int64_t)(base + m * j.nb) * TILE_CELLS + tid;
+          const float z = SG.zb[m * 1000 + tile_pad(tid)];
+          Z[q] = z;
+          v[0] += (Acc)(bb[m] * z);
+          v[1] += (Acc)(bb[m] * bb[m]);
+        }
+        __syncthreads();
+        continue;
       }
 #pragma unroll
       for (int m = 0; m < SEG_TG; ++m) {
@@ -1132,6 +1166,34 @@ __device__ __forceinline__ bool pcg_scene(const SegPcgArgs &a, const PcgJob &j) 
           rr[m] = __ldcg(R + q);
           aa[m] = __ldcg(AD + q);
         }
+        if (SGS) {
+#pragma unroll
+          for (int m = 0; m < SEG_TG; ++m) {
+            const int64_t q = (int64_t)(base + m * j.nb) * TILE_CELLS + tid;
+            float rn = 0.0f;
+            if (cd[m] & CODE_FLUID) {
+              X[q] = xx[m] + alpha * dd[m];
+              rn = rr[m] + nalpha * aa[m];
+              R[q] = rn;
+            }
+            rr[m] = rn;
+            SG.r[m * 512 + tid] = rn;
+            SG.code[m * 512 + tid] = cd[m];
+            SG.zb[m * 1000 + tile_pad(tid)] = rn * sgs_factor(cd[m]);
+          }
+          sgs_sweeps(SG, a.sgs);
+#pragma unroll
+          for (int m = 0; m < SEG_TG; ++m) {
+            if (!(cd[m] & CODE_FLUID)) continue;
+            const int64_t q = (int64_t)(base + m * j.nb) * TILE_CELLS + tid;
+            const float z = SG.zb[m * 1000 + tile_pad(tid)];
+            Z[q] = z;
+            v[0] += (Acc)(rr[m] * z);
+            v[1] += (Acc)(rr[m] * rr[m]);
+          }
+          __syncthreads();
+          continue;
+        }
 #pragma unroll
         for (int m = 0; m < SEG_TG; ++m) {
           if (!(cd[m] & CODE_FLUID)) continue;
@@ -1205,9 +1267,39 @@ __device__ __forceinline__ bool pcg_scene(const SegPcgArgs &a, const PcgJob &j) 
             double s = 0.0;
 #pragma unroll
             for (int d = 0; d < 6; ++d)
-              if (cd[m] & (1 << d)) s += __ldcg(a.x64 + nb_index(q, d, a.nbr));
+              if (cd[m] & (1 << d)) {
+                const int64_t nq = nb_index(q, d, a.nbr);
+                if (GF_IN(nq, total)) s += __ldcg(a.x64 + nq);
+              }
             const double diag = (double)((cd[m] >> CODE_DIAG_SHIFT) & 7);
             res[m] = (double)(a.sign * a.bdiv[q]) - (diag * __ldcg(a.x64 + q) - s);
+          }
+          if (SGS) {
+            float rf[SEG_TG];
+#pragma unroll
+            for (int m = 0; m < SEG_TG; ++m) {
+              const int64_t q = (int64_t)(base + m * j.nb) * TILE_CELLS + tid;
+              rf[m] = (cd[m] & CODE_FLUID) ? (float)res[m] : 0.0f;
+              if (cd[m] & CODE_FLUID) {
+                R[q] = rf[m];
+                v[0] += res[m] * res[m];
+              }
+              SG.r[m * 512 + tid] = rf[m];
+              SG.code[m * 512 + tid] = cd[m];
+              SG.zb[m * 1000 + tile_pad(tid)] = rf[m] * sgs_factor(cd[m]);
+            }
+            sgs_sweeps(SG, a.sgs);
+#pragma unroll
+            for (int m = 0; m < SEG_TG; ++m) {
+              if (!(cd[m] & CODE_FLUID)) continue;
+              const int64_t q = (int64_t)(base + m * j.nb) * TILE_CELLS + tid;
+              const float z = SG.zb[m * 1000 + tile_pad(tid)];
+              Z[q] = z;
+              v[1] += (double)(rf[m] * z);
+              v[2] += (double)(rf[m] * rf[m]);
+            }
+            __syncthreads();
+            continue;
           }
 #pragma unroll
           for (int m = 0; m < SEG_TG; ++m) {
@@ -1242,13 +1334,13 @@ __device__ __forceinline__ bool pcg_scene(const SegPcgArgs &a, const PcgJob &j) 
   return true;
 }
 
-template <typename Acc, bool REF>
+template <typename Acc, bool REF, bool SGS>
 __global__ void __launch_bounds__(TILE_CELLS, 2) k_pcg_seg(SegPcgArgs a) {
   const int j0 = a.blk_job0[blockIdx.x], j1 = a.blk_job0[blockIdx.x + 1];
   for (int jj = j0; jj < j1; ++jj) {
     const PcgJob j = a.jobs[jj];
     if (ld_volatile_i(&a.st[j.scene].done)) continue;  // no fluid
-    if (!pcg_scene<Acc, REF>(a, j)) return;
+    if (!pcg_scene<Acc, REF, SGS>(a, j)) return;
   }
 }
 
@@ -1447,11 +1539,11 @@ static int launch_pcg(Ctx *c, PcgArgs &pa) {
   return pa.sgs > 0 ? launch_pcg_t<Acc, REF, true>(c, pa) : launch_pcg_t<Acc, REF, false>(c, pa);
 }
 
-template <typename Acc, bool REF>
-static int launch_pcg_seg(Ctx *c, SegPcgArgs &pa) {
+template <typename Acc, bool REF, bool SGS>
+static int launch_pcg_seg_t(Ctx *c, SegPcgArgs &pa) {
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_seg<Acc, REF>, TILE_CELLS,
-                                                    0) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_seg<Acc, REF, SGS>,
+                                                    TILE_CELLS, 0) != cudaSuccess ||
       per_sm < 1)
     return fail(c, GF_CUDA_ERROR, "segmented PCG: cooperative occupancy query failed");
   if (c->tune.pcg_blocks_per_sm > 0 && c->tune.pcg_blocks_per_sm < per_sm)
@@ -1464,11 +1556,18 @@ static int launch_pcg_seg(Ctx *c, SegPcgArgs &pa) {
   pa.blk_job0 = c->pcg_blk_job0;
   pa.jobs = reinterpret_cast<const PcgJob *>(c->pcg_jobs);
   void *args[] = {&pa};
-  int e = check_cuda(c, cudaLaunchCooperativeKernel((const void *)k_pcg_seg<Acc, REF>, dim3(grid),
-                                                    dim3(TILE_CELLS), args, 0, c->stream),
+  int e = check_cuda(c, cudaLaunchCooperativeKernel((const void *)k_pcg_seg<Acc, REF, SGS>,
+                                                    dim3(grid), dim3(TILE_CELLS), args, 0,
+                                                    c->stream),
                      "cooperative segmented PCG launch");
   c->launches++;
   return e;
+}
+
+template <typename Acc, bool REF>
+static int launch_pcg_seg(Ctx *c, SegPcgArgs &pa) {
+  return pa.sgs > 0 ? launch_pcg_seg_t<Acc, REF, true>(c, pa)
+                    : launch_pcg_seg_t<Acc, REF, false>(c, pa);
 }
 
 // Bytes of the job table of a batch with nseg scenes.
@@ -1530,7 +1629,8 @@ static int launch_pressure_batch(Ctx *c, const gf_step_params *prm) {
     SegPcgArgs pa{c->n_active, c->tile_nbr, c->seg_slot0, c->nseg, c->code, c->bdiv, c->xf,
                   c->r, c->z, c->d0, c->d1, c->Ad, refined ? c->x64 : nullptr, c->partials,
                   (int64_t)c->ntiles + MAX_PCG_BLOCKS, c->seg_state, c->state, nullptr,
-                  nullptr, prm->max_iters, check_every, prm->tol * prm->tol, 1e-4, sign};
+                  nullptr, prm->max_iters, check_every, prm->tol * prm->tol, 1e-4, sign,
+                  (prm->flags & GF_FLAG_SGS_MASK) >> GF_FLAG_SGS_SHIFT};
     if (refined) {
       e = launch_pcg_seg<double, true>(c, pa);
       result64 = c->x64;
