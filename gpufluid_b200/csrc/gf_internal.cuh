@@ -142,6 +142,8 @@ struct FaceMaps {
 
 // Launch shapes chosen by gf_autotune (defaults until it runs).
 struct Tune {
+  int p2g_tiles_k = 1;           // P2G and G2P blocks: 8 x 8 x 8 (1) or 8 x 8 x 16 cells (2)
+  int g2p_tiles_k = 1;
   int g2p_threads = 256;
   int grid_threads = 256;        // forces / divergence / project / sweeps
   int grid_blocks_per_sm = 16;   // cap of their grid-stride launches
@@ -161,7 +163,8 @@ struct Ctx {
   // caller buffers
   gf_fields f{};
   gf_particles p{};
-  FaceMaps face_maps{};  // tensor maps of the bound face arrays (single grid)
+  FaceMaps face_maps{};   // tensor maps of the bound face arrays (single grid): 8^3 blocks
+  FaceMaps face_maps2{};  // the same for 8 x 8 x 16 blocks (Tune::g2p_tiles_k = 2)
   // outflow compaction scratch (block counts, offsets, boxes), grown on use
   int32_t *region_scratch = nullptr;
   int64_t region_scratch_n = 0;

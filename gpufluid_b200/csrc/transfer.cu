@@ -24,10 +24,18 @@
 namespace gf {
 
 // ---------------------------------------------------------------- P2G
-// Shared-memory boxes, in faces, relative to the tile origin (I0, J0, K0):
-// the normal axis spans [O, O+8] (9 faces), the transverse axes [O-1, O+8]
-// (10 faces).
-constexpr int BOX_N = 9, BOX_T = 10, BOX = BOX_N * BOX_T * BOX_T;  // 900
+// A CTA scatters a block of KT tiles along k (8 x 8 x 8 KT cells; KT = 1 or
+// 2, chosen by the autotuner) into shared-memory boxes, in faces, relative to
+// the block origin (I0, J0, K0): on the i and j axes the normal axis spans
+// [O, O+8] (9 faces) and the transverse ones [O-1, O+8] (10 faces); on the k
+// axis [K0, K0+8KT] for w and [K0-1, K0+8KT] for u and v.  Each component's
+// box takes P2G_BOXK(KT) entries (the largest of the three).
+constexpr int BOX_N = 9, BOX_T = 10;
+__host__ __device__ constexpr int p2g_ez(int comp, int KT) {
+  return comp == 2 ? 8 * KT + 1 : 8 * KT + 2;
+}
+__host__ __device__ constexpr int P2G_BOXK(int KT) { return BOX_T * BOX_T * (8 * KT + 1); }
+static_assert(P2G_BOXK(1) == 900 && BOX_N * BOX_T * 10 <= P2G_BOXK(1), "P2G box");
 // Type of the shared-memory face sums of a tile (the sums are rounded to
 // float32 once, at the flush).
 #ifndef GF_P2G_ACC
@@ -46,7 +54,7 @@ struct P2GArgs {
 // Scatter one face component of one particle into the shared box of `comp`
 // (0 u, 1 v, 2 w).  APIC adds C_row . (x_face - x_p) with world face
 // positions (:1510-1588).
-template <bool APIC, typename T>
+template <bool APIC, int KT, typename T>
 __device__ __forceinline__ void scatter_comp(T *s_val, T *s_wt, int comp, float vp,
                                              float c0, float c1, float c2, float px, float py,
                                              float pz, float fx, float fy, float fz, int I0,
@@ -58,7 +66,7 @@ __device__ __forceinline__ void scatter_comp(T *s_val, T *s_wt, int comp, float 
   float sx = fx - (float)i0, sy = fy - (float)j0, sz = fz - (float)k0;
   // box origin and extents for this component
   int bx0 = comp == 0 ? I0 : I0 - 1, by0 = comp == 1 ? J0 : J0 - 1, bz0 = comp == 2 ? K0 : K0 - 1;
-  int ey = comp == 1 ? BOX_N : BOX_T, ez = comp == 2 ? BOX_N : BOX_T;
+  int ey = comp == 1 ? BOX_N : BOX_T, ez = p2g_ez(comp, KT);
   int ex = comp == 0 ? BOX_N : BOX_T;
 #pragma unroll
   for (int di = 0; di < 2; ++di)
@@ -108,7 +116,7 @@ __device__ __forceinline__ void scatter_comp(T *s_val, T *s_wt, int comp, float 
 // shared-memory adds.  The sums are tolerance-checked (their order is the
 // atomics' anyway), so the factors use fused multiply-adds.  Returns false,
 // touching nothing, when the stencil does not fit (scatter_comp then runs).
-template <bool APIC, typename T>
+template <bool APIC, int KT, typename T>
 __device__ __forceinline__ bool scatter_comp_fast(T *s_val, T *s_wt, int comp, float vp,
                                                   float c0, float c1, float c2, float px,
                                                   float py, float pz, float fx, float fy,
@@ -117,7 +125,7 @@ __device__ __forceinline__ bool scatter_comp_fast(T *s_val, T *s_wt, int comp, f
   const int snx = a.nx + (comp == 0), sny = a.ny + (comp == 1), snz = a.nz + (comp == 2);
   const int i0 = __float2int_rz(floorf(fx)), j0 = __float2int_rz(floorf(fy)),
             k0 = __float2int_rz(floorf(fz));
-  const int ey = comp == 1 ? BOX_N : BOX_T, ez = comp == 2 ? BOX_N : BOX_T;
+  const int ey = comp == 1 ? BOX_N : BOX_T, ez = p2g_ez(comp, KT);
   const int ex = comp == 0 ? BOX_N : BOX_T;
   const int bx = i0 - (comp == 0 ? I0 : I0 - 1), by = j0 - (comp == 1 ? J0 : J0 - 1),
             bz = k0 - (comp == 2 ? K0 : K0 - 1);
@@ -151,7 +159,7 @@ __device__ __forceinline__ bool scatter_comp_fast(T *s_val, T *s_wt, int comp, f
         const float wt = wxy * wz[dk];
         const float val = ab + C[dk];
         const int e = base + (di * ey + dj) * ez + dk;
-        if (!GF_IN(e, BOX)) continue;
+        if (!GF_IN(e, P2G_BOXK(KT))) continue;
         atomicAdd(&s_val[e], (T)(val * wt));
         atomicAdd(&s_wt[e], (T)wt);
       }
@@ -162,14 +170,16 @@ __device__ __forceinline__ bool scatter_comp_fast(T *s_val, T *s_wt, int comp, f
 // Flush a tile's shared box: faces that only this tile's particles reach are
 // stored, the shared halo band is accumulated atomically; exact zeros are
 // skipped (the destination was zeroed before the launch).
-template <typename T>
-__device__ __forceinline__ void p2g_flush_box(const P2GArgs &a, T (*s_val)[BOX],
-                                              T (*s_wt)[BOX], int I0, int J0, int K0) {
-  for (int q = threadIdx.x; q < 3 * BOX; q += blockDim.x) {
-    int comp = q / BOX, e2 = q - comp * BOX;
-    float val = (float)s_val[comp][e2], wt = (float)s_wt[comp][e2];
+template <int KT, typename T>
+__device__ __forceinline__ void p2g_flush_box(const P2GArgs &a, const T *s_val, const T *s_wt,
+                                              int I0, int J0, int K0) {
+  constexpr int BK = P2G_BOXK(KT);
+  for (int q = threadIdx.x; q < 3 * BK; q += blockDim.x) {
+    int comp = q / BK, e2 = q - comp * BK;
+    int ey = comp == 1 ? BOX_N : BOX_T, ez = p2g_ez(comp, KT);
+    if (e2 >= (comp == 0 ? BOX_N : BOX_T) * ey * ez) continue;  // beyond this component's box
+    float val = (float)s_val[q], wt = (float)s_wt[q];
     if (val == 0.f && wt == 0.f) continue;
-    int ey = comp == 1 ? BOX_N : BOX_T, ez = comp == 2 ? BOX_N : BOX_T;
     int bx = e2 / (ey * ez), by = (e2 / ez) % ey, bz = e2 % ez;
     int ii = bx + (comp == 0 ? I0 : I0 - 1), jj = by + (comp == 1 ? J0 : J0 - 1),
         kk = bz + (comp == 2 ? K0 : K0 - 1);
@@ -178,7 +188,7 @@ __device__ __forceinline__ void p2g_flush_box(const P2GArgs &a, T (*s_val)[BOX],
     // exclusive: every cell that can reach the face lies in this tile
     bool ex_x = comp == 0 ? (bx >= 1 && bx <= 7) : (bx >= 2 && bx <= 7);
     bool ex_y = comp == 1 ? (by >= 1 && by <= 7) : (by >= 2 && by <= 7);
-    bool ex_z = comp == 2 ? (bz >= 1 && bz <= 7) : (bz >= 2 && bz <= 7);
+    bool ex_z = comp == 2 ? (bz >= 1 && bz <= 8 * KT - 1) : (bz >= 2 && bz <= 8 * KT - 1);
     int64_t g = ((int64_t)ii * sny + jj) * snz + kk;
     float *gv = comp == 0 ? a.u : (comp == 1 ? a.v : a.w);
     float *gw = comp == 0 ? a.uw : (comp == 1 ? a.vw : a.ww);
@@ -193,17 +203,22 @@ __device__ __forceinline__ void p2g_flush_box(const P2GArgs &a, T (*s_val)[BOX],
   }
 }
 
-// One tile's P2G: t is the tile within its grid (its coordinates), key0 the
-// sort key of its first cell (t * 512 for a single grid).
-template <bool APIC, typename T = P2G_ACC>
-__device__ __forceinline__ void p2g_tile_body(const P2GArgs &a, int t, int64_t key0) {
-  __shared__ T s_val[3][BOX];
-  __shared__ T s_wt[3][BOX];
-  const int64_t b = a.start[key0], e = a.start[key0 + TILE_CELLS];
+// One block's P2G: t is its first tile within the grid (the block's
+// coordinates), key0 the sort key of that tile's first cell (t * 512 for a
+// single grid), ntk (<= KT) the tiles it holds along k, which are consecutive
+// in the sorted order.  The boxes live in dynamic shared memory
+// (p2g_smem_bytes).
+template <bool APIC, int KT, typename T = P2G_ACC>
+__device__ __forceinline__ void p2g_tile_body(const P2GArgs &a, int t, int64_t key0, int ntk) {
+  extern __shared__ __align__(16) unsigned char p2g_smem[];
+  constexpr int BK = P2G_BOXK(KT);
+  T *s_val = reinterpret_cast<T *>(p2g_smem);
+  T *s_wt = s_val + 3 * BK;
+  const int64_t b = a.start[key0], e = a.start[key0 + (int64_t)ntk * TILE_CELLS];
   if (b == e) return;
-  for (int q = threadIdx.x; q < 3 * BOX; q += blockDim.x) {
-    (&s_val[0][0])[q] = (T)0;
-    (&s_wt[0][0])[q] = (T)0;
+  for (int q = threadIdx.x; q < 3 * BK; q += blockDim.x) {
+    s_val[q] = (T)0;
+    s_wt[q] = (T)0;
   }
   __syncthreads();
   const int ti = t / (a.nty * a.ntz), tj = (t / a.ntz) % a.nty, tk = t % a.ntz;
@@ -227,26 +242,38 @@ __device__ __forceinline__ void p2g_tile_body(const P2GArgs &a, int t, int64_t k
     float gx = __fdiv_rn(r0.x, a.dx), gy = __fdiv_rn(r0.y, a.dx), gz = __fdiv_rn(r0.z, a.dx);
     float hx = gx - 0.5f, hy = gy - 0.5f, hz = gz - 0.5f;
     // C rows: (r1.w, r2.x, r2.y) (r2.z, r2.w, r3.x) (r3.y, r3.z, r3.w)
-    if (!scatter_comp_fast<APIC, T>(s_val[0], s_wt[0], 0, r1.x, r1.w, r2.x, r2.y, r0.x, r0.y,
-                                    r0.z, gx, hy, hz, I0, J0, K0, a))
-      scatter_comp<APIC, T>(s_val[0], s_wt[0], 0, r1.x, r1.w, r2.x, r2.y, r0.x, r0.y, r0.z, gx,
-                            hy, hz, I0, J0, K0, a, a.u, a.uw);
-    if (!scatter_comp_fast<APIC, T>(s_val[1], s_wt[1], 1, r1.y, r2.z, r2.w, r3.x, r0.x, r0.y,
-                                    r0.z, hx, gy, hz, I0, J0, K0, a))
-      scatter_comp<APIC, T>(s_val[1], s_wt[1], 1, r1.y, r2.z, r2.w, r3.x, r0.x, r0.y, r0.z, hx,
-                            gy, hz, I0, J0, K0, a, a.v, a.vw);
-    if (!scatter_comp_fast<APIC, T>(s_val[2], s_wt[2], 2, r1.z, r3.y, r3.z, r3.w, r0.x, r0.y,
-                                    r0.z, hx, hy, gz, I0, J0, K0, a))
-      scatter_comp<APIC, T>(s_val[2], s_wt[2], 2, r1.z, r3.y, r3.z, r3.w, r0.x, r0.y, r0.z, hx,
-                            hy, gz, I0, J0, K0, a, a.w, a.ww);
+    T *v0 = s_val, *w0 = s_wt, *v1 = s_val + BK, *w1 = s_wt + BK, *v2 = s_val + 2 * BK,
+      *w2 = s_wt + 2 * BK;
+    if (!scatter_comp_fast<APIC, KT, T>(v0, w0, 0, r1.x, r1.w, r2.x, r2.y, r0.x, r0.y, r0.z, gx,
+                                        hy, hz, I0, J0, K0, a))
+      scatter_comp<APIC, KT, T>(v0, w0, 0, r1.x, r1.w, r2.x, r2.y, r0.x, r0.y, r0.z, gx, hy, hz,
+                                I0, J0, K0, a, a.u, a.uw);
+    if (!scatter_comp_fast<APIC, KT, T>(v1, w1, 1, r1.y, r2.z, r2.w, r3.x, r0.x, r0.y, r0.z, hx,
+                                        gy, hz, I0, J0, K0, a))
+      scatter_comp<APIC, KT, T>(v1, w1, 1, r1.y, r2.z, r2.w, r3.x, r0.x, r0.y, r0.z, hx, gy, hz,
+                                I0, J0, K0, a, a.v, a.vw);
+    if (!scatter_comp_fast<APIC, KT, T>(v2, w2, 2, r1.z, r3.y, r3.z, r3.w, r0.x, r0.y, r0.z, hx,
+                                        hy, gz, I0, J0, K0, a))
+      scatter_comp<APIC, KT, T>(v2, w2, 2, r1.z, r3.y, r3.z, r3.w, r0.x, r0.y, r0.z, hx, hy, gz,
+                                I0, J0, K0, a, a.w, a.ww);
   }
   __syncthreads();
-  p2g_flush_box<T>(a, s_val, s_wt, I0, J0, K0);
+  p2g_flush_box<KT, T>(a, s_val, s_wt, I0, J0, K0);
 }
 
-template <bool APIC>
+__host__ __device__ constexpr size_t p2g_smem_bytes(int KT) {
+  return 2 * 3 * (size_t)P2G_BOXK(KT) * sizeof(P2G_ACC);
+}
+
+// One CTA per block of KT tiles along k: block b holds tiles (ti, tj, KT*kb
+// .. KT*kb + KT - 1) with kb = b % ceil(ntz / KT), clipped to the grid.
+template <bool APIC, int KT>
 __global__ void __launch_bounds__(256) k_p2g_tile(P2GArgs a) {
-  p2g_tile_body<APIC>(a, blockIdx.x, (int64_t)blockIdx.x * TILE_CELLS);
+  const int ntkb = (a.ntz + KT - 1) / KT;
+  const int kb = blockIdx.x % ntkb, r = blockIdx.x / ntkb;
+  const int t = r * a.ntz + KT * kb;  // r = ti * nty + tj
+  const int ntk = a.ntz - KT * kb < KT ? a.ntz - KT * kb : KT;
+  p2g_tile_body<APIC, KT>(a, t, (int64_t)t * TILE_CELLS, ntk);
 }
 
 // --------------------------------------------------------------- forces
@@ -609,14 +636,29 @@ __global__ void __launch_bounds__(512) k_g2p(G2PArgs a) {
 // [K0, K0+12) -- the start and width of the innermost axis are multiples of
 // 16 bytes, as a tiled TMA copy requires.  Boxes start on 128-byte
 // boundaries; a set of three boxes (u, v, w) takes GBOX_SET floats.
+// With KT tiles per block along k (the autotuner's tile shape) the k ranges
+// grow by 8 (KT - 1): u and v load [K0-4, K0+8KT+4), w [K0, K0+8KT+4).
 __host__ __device__ constexpr int gbox_ni(int c) { return c == 0 ? 9 : 10; }
 __host__ __device__ constexpr int gbox_nj(int c) { return c == 1 ? 9 : 10; }
-__host__ __device__ constexpr int gbox_nk(int c) { return c == 2 ? 12 : 16; }
-__host__ __device__ constexpr int gbox_vol(int c) { return gbox_ni(c) * gbox_nj(c) * gbox_nk(c); }
-__host__ __device__ constexpr int gbox_off(int c) { return c == 0 ? 0 : (c == 1 ? 1440 : 2880); }
+__host__ __device__ constexpr int gbox_nk(int c, int KT = 1) {
+  return c == 2 ? 8 * KT + 4 : 8 * KT + 8;
+}
+__host__ __device__ constexpr int gbox_vol(int c, int KT = 1) {
+  return gbox_ni(c) * gbox_nj(c) * gbox_nk(c, KT);
+}
+__host__ __device__ constexpr int align32(int v) { return (v + 31) & ~31; }  // 128 bytes
+__host__ __device__ constexpr int gbox_off(int c, int KT = 1) {
+  return c == 0 ? 0
+                : (c == 1 ? align32(gbox_vol(0, KT))
+                          : align32(gbox_vol(0, KT)) + align32(gbox_vol(1, KT)));
+}
+__host__ __device__ constexpr int gbox_set(int KT) {
+  return align32(gbox_off(2, KT) + gbox_vol(2, KT));
+}
 constexpr int GBOX_SET = 4096;
 static_assert(gbox_vol(0) == 1440 && gbox_vol(1) == 1440 && gbox_vol(2) == 1200, "boxes");
-static_assert(gbox_off(2) + gbox_vol(2) <= GBOX_SET, "box set");
+static_assert(gbox_off(2) == 2880 && gbox_set(1) == GBOX_SET, "box set");
+static_assert(gbox_set(2) == 6368, "box set of 8 x 8 x 16 blocks");
 constexpr int G2P_TILE_THREADS = 256;
 constexpr long long G2P_WAIT_LIMIT = 1LL << 22;  // try_wait polls before giving up
 
@@ -677,6 +719,10 @@ struct G2PTileArgs {
   int32_t *wait_err;  // incremented when the box loads do not complete in time
 };
 
+__host__ __device__ constexpr size_t g2p_smem_bytes(int mode, int KT) {
+  return (size_t)(mode == GF_APIC ? 1 : 2) * gbox_set(KT) * sizeof(float);
+}
+
 // True when the clamped gather indices [lo, hi] of every axis lie inside the
 // component's box (always, for a particle inside its binned cell; a particle
 // outside the grid or with a non-finite position takes the global path).
@@ -686,29 +732,37 @@ __device__ __forceinline__ bool in_box(const BoxAt &b, int ni, int i0, int i1, i
          k1 < b.ok + b.nk;
 }
 
-template <int MODE>
+template <int MODE, int KT>
 __global__ void __launch_bounds__(G2P_TILE_THREADS)
     k_g2p_tile(const G2PTileArgs ta, const __grid_constant__ FaceMaps fm) {
   constexpr bool APIC = MODE == GF_APIC;
   constexpr int NARR = APIC ? 3 : 6;  // u, v, w (+ us, vs, ws for the FLIP delta)
   constexpr int OUTF = APIC ? 4096 : 1792;  // staging: pos 768, vel 768, [C 2304], pid 256
-  __shared__ alignas(128) float s_box[(NARR / 3) * GBOX_SET];
+  constexpr int SET = gbox_set(KT);
+  extern __shared__ __align__(128) unsigned char g2p_smem[];
+  float *s_box = reinterpret_cast<float *>(g2p_smem);  // (NARR / 3) sets of boxes
   __shared__ alignas(16) float s_out[OUTF];
   __shared__ alignas(8) uint64_t s_bar;
   __shared__ int s_ok;
   const G2PArgs &a = ta.g;
-  const int t = blockIdx.x, tid = threadIdx.x;
-  const int64_t b = ta.start[(int64_t)t * TILE_CELLS], e = ta.start[(int64_t)t * TILE_CELLS + TILE_CELLS];
+  const int tid = threadIdx.x;
+  // block -> its KT tiles along k (clipped at the grid's last tile)
+  const int ntkb = (ta.ntz + KT - 1) / KT;
+  const int kb = blockIdx.x % ntkb, rij = blockIdx.x / ntkb;
+  const int t = rij * ta.ntz + KT * kb;
+  const int ntk = ta.ntz - KT * kb < KT ? ta.ntz - KT * kb : KT;
+  const int64_t b = ta.start[(int64_t)t * TILE_CELLS],
+                e = ta.start[(int64_t)(t + ntk) * TILE_CELLS];
   if (b == e) return;
-  const int ti = t / (ta.nty * ta.ntz), tj = (t / ta.ntz) % ta.nty, tk = t % ta.ntz;
-  const int I0 = ti * TILE, J0 = tj * TILE, K0 = tk * TILE;
+  const int ti = rij / ta.nty, tj = rij % ta.nty;
+  const int I0 = ti * TILE, J0 = tj * TILE, K0 = KT * kb * TILE;
   const int nx = a.nx, ny = a.ny, nz = a.nz;
 
   // ---- stage the boxes
   uint32_t tx = 0;
 #pragma unroll
   for (int q = 0; q < NARR; ++q)
-    if ((fm.mask >> q) & 1) tx += (uint32_t)gbox_vol(q % 3) * 4u;
+    if ((fm.mask >> q) & 1) tx += (uint32_t)gbox_vol(q % 3, KT) * 4u;
   if (tid == 0) {
     s_ok = 1;
     if (tx) {
@@ -723,7 +777,7 @@ __global__ void __launch_bounds__(G2P_TILE_THREADS)
     for (int q = 0; q < NARR; ++q) {
       if (!((fm.mask >> q) & 1)) continue;
       const int c = q % 3;
-      tma_load_3d(s_box + (q / 3) * GBOX_SET + gbox_off(c), &fm.m[q], c == 2 ? K0 : K0 - 4,
+      tma_load_3d(s_box + (q / 3) * SET + gbox_off(c, KT), &fm.m[q], c == 2 ? K0 : K0 - 4,
                   J0 - (c != 1), I0 - (c != 0), &s_bar);
     }
   }
@@ -734,9 +788,9 @@ __global__ void __launch_bounds__(G2P_TILE_THREADS)
       if ((fm.mask >> q) & 1) continue;
       const int c = q % 3;
       const int snx = nx + (c == 0), sny = ny + (c == 1), snz = nz + (c == 2);
-      const int ni = gbox_ni(c), nj = gbox_nj(c), nk = gbox_nk(c);
+      const int ni = gbox_ni(c), nj = gbox_nj(c), nk = gbox_nk(c, KT);
       const int oi = I0 - (c != 0), oj = J0 - (c != 1), ok = c == 2 ? K0 : K0 - 4;
-      float *dst = s_box + (q / 3) * GBOX_SET + gbox_off(c);
+      float *dst = s_box + (q / 3) * SET + gbox_off(c, KT);
       for (int v = tid; v < ni * nj * nk; v += G2P_TILE_THREADS) {
         const int bk = v % nk, r = v / nk, bj = r % nj, bi = r / nj;
         const int gi = oi + bi, gj = oj + bj, gk = ok + bk;
@@ -772,8 +826,8 @@ __global__ void __launch_bounds__(G2P_TILE_THREADS)
 #pragma unroll
   for (int q = 0; q < NARR; ++q) {
     const int c = q % 3;
-    bx[q] = BoxAt{s_box + (q / 3) * GBOX_SET + gbox_off(c), I0 - (c != 0), J0 - (c != 1),
-                  c == 2 ? K0 : K0 - 4, gbox_nj(c), gbox_nk(c), gbox_vol(c)};
+    bx[q] = BoxAt{s_box + (q / 3) * SET + gbox_off(c, KT), I0 - (c != 0), J0 - (c != 1),
+                  c == 2 ? K0 : K0 - 4, gbox_nj(c), gbox_nk(c, KT), gbox_vol(c, KT)};
   }
   const float dx = a.dx;
   int *s_pid = reinterpret_cast<int *>(s_out + (APIC ? 3840 : 1536));
@@ -885,24 +939,30 @@ static EncodeTiledFn encode_fn() {
 }
 
 int encode_face_maps(Ctx *c) {
-  c->face_maps.mask = 0;
+  FaceMaps *sets[2] = {&c->face_maps, &c->face_maps2};
+  for (FaceMaps *fm : sets) fm->mask = 0;
   if (c->nseg > 0) return GF_OK;  // batches use the per-particle G2P
   EncodeTiledFn fn = encode_fn();
   if (!fn) return GF_OK;  // plain loads for every box
   const float *arr[6] = {c->f.u, c->f.v, c->f.w, c->f.us, c->f.vs, c->f.ws};
-  for (int q = 0; q < 6; ++q) {
-    const int comp = q % 3;
-    const uint64_t snx = c->nx + (comp == 0), sny = c->ny + (comp == 1), snz = c->nz + (comp == 2);
-    const cuuint64_t dims[3] = {snz, sny, snx};
-    const cuuint64_t strides[2] = {snz * 4, sny * snz * 4};
-    const cuuint32_t box[3] = {(cuuint32_t)gbox_nk(comp), (cuuint32_t)gbox_nj(comp),
-                               (cuuint32_t)gbox_ni(comp)};
-    const cuuint32_t estr[3] = {1, 1, 1};
-    if (reinterpret_cast<uintptr_t>(arr[q]) % 16 || strides[0] % 16 || strides[1] % 16) continue;
-    if (fn(&c->face_maps.m[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(arr[q]),
-           dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS)
-      c->face_maps.mask |= 1 << q;
+  for (int kt = 1; kt <= 2; ++kt) {
+    FaceMaps *fm = sets[kt - 1];
+    for (int q = 0; q < 6; ++q) {
+      const int comp = q % 3;
+      const uint64_t snx = c->nx + (comp == 0), sny = c->ny + (comp == 1),
+                     snz = c->nz + (comp == 2);
+      const cuuint64_t dims[3] = {snz, sny, snx};
+      const cuuint64_t strides[2] = {snz * 4, sny * snz * 4};
+      const cuuint32_t box[3] = {(cuuint32_t)gbox_nk(comp, kt), (cuuint32_t)gbox_nj(comp),
+                                 (cuuint32_t)gbox_ni(comp)};
+      const cuuint32_t estr[3] = {1, 1, 1};
+      if (reinterpret_cast<uintptr_t>(arr[q]) % 16 || strides[0] % 16 || strides[1] % 16)
+        continue;
+      if (fn(&fm->m[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(arr[q]), dims,
+             strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS)
+        fm->mask |= 1 << q;
+    }
   }
   return GF_OK;
 }
@@ -945,7 +1005,7 @@ __global__ void __launch_bounds__(256) kb_p2g_tile(BatchArgs b) {
   const SegRow r = b.sx.row[s];
   P2GArgs a{b.start, b.rec0, b.rec1, b.rec2, b.rec3, b.u + r.fu0, b.v + r.fv0, b.w + r.fw0,
             b.uw + r.fu0, b.vw + r.fv0, b.ww + r.fw0, r.dx, r.nx, r.ny, r.nz, r.nty, r.ntz};
-  p2g_tile_body<APIC>(a, (int)(t - r.tile0), t * TILE_CELLS);
+  p2g_tile_body<APIC, 1>(a, (int)(t - r.tile0), t * TILE_CELLS, 1);
 }
 
 __global__ void kb_forces(BatchArgs b, int64_t nslot, float gravity) {
@@ -1042,16 +1102,26 @@ int launch_p2g(Ctx *c, int transfer) {
             c->f.uw, c->f.vw, c->f.ww, c->dx, c->nx, c->ny, c->nz, c->nty, c->ntz};
   if (c->p.n > 0 && c->nseg > 0) {
     BatchArgs b = batch_args(c);
+    const size_t sm = p2g_smem_bytes(1);
     if (transfer == GF_APIC)
-      kb_p2g_tile<true><<<c->ntiles, 256, 0, st>>>(b);
+      kb_p2g_tile<true><<<c->ntiles, 256, sm, st>>>(b);
     else
-      kb_p2g_tile<false><<<c->ntiles, 256, 0, st>>>(b);
+      kb_p2g_tile<false><<<c->ntiles, 256, sm, st>>>(b);
     c->launches++;
   } else if (c->p.n > 0) {
+    const int kt = c->tune.p2g_tiles_k == 2 ? 2 : 1;
+    const unsigned g = (unsigned)(c->ntx * c->nty * ((c->ntz + kt - 1) / kt));
+    const size_t sm = p2g_smem_bytes(kt);
+    auto launch = [&](auto kern) {
+      if (sm > 48 * 1024)
+        cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sm);
+      kern<<<g, 256, sm, st>>>(a);
+    };
     if (transfer == GF_APIC)
-      k_p2g_tile<true><<<c->ntiles, 256, 0, st>>>(a);
+      kt == 2 ? launch(k_p2g_tile<true, 2>) : launch(k_p2g_tile<true, 1>);
     else
-      k_p2g_tile<false><<<c->ntiles, 256, 0, st>>>(a);
+      kt == 2 ? launch(k_p2g_tile<false, 2>) : launch(k_p2g_tile<false, 1>);
     c->launches++;
   }
   return check_launch(c, "gf_p2g");
@@ -1140,10 +1210,19 @@ int launch_g2p(Ctx *c, int transfer, float flip_blend, float dt) {
             c->p.pos, c->p.vel, c->p.C, c->p.pid, c->p.n, c->dx, dt, flip_blend,
             c->dom[0], c->dom[1], c->dom[2], c->nx, c->ny, c->nz};
   G2PTileArgs ta{a, c->start, c->nty, c->ntz, c->health + 5};
+  const int kt = c->tune.g2p_tiles_k == 2 ? 2 : 1;
+  const unsigned gb = (unsigned)(c->ntx * c->nty * ((c->ntz + kt - 1) / kt));
+  const FaceMaps &fm = kt == 2 ? c->face_maps2 : c->face_maps;
+  auto launch = [&](auto kern, int mode) {
+    const size_t sm = g2p_smem_bytes(mode, kt);  // beside the static staging buffers
+    cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sm);
+    kern<<<gb, G2P_TILE_THREADS, sm, c->stream>>>(ta, fm);
+  };
   if (transfer == GF_APIC)
-    k_g2p_tile<GF_APIC><<<c->ntiles, G2P_TILE_THREADS, 0, c->stream>>>(ta, c->face_maps);
+    kt == 2 ? launch(k_g2p_tile<GF_APIC, 2>, GF_APIC) : launch(k_g2p_tile<GF_APIC, 1>, GF_APIC);
   else
-    k_g2p_tile<GF_FLIP><<<c->ntiles, G2P_TILE_THREADS, 0, c->stream>>>(ta, c->face_maps);
+    kt == 2 ? launch(k_g2p_tile<GF_FLIP, 2>, GF_FLIP) : launch(k_g2p_tile<GF_FLIP, 1>, GF_FLIP);
   c->launches++;
   return check_launch(c, "gf_g2p");
 }

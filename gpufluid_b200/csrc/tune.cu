@@ -3,7 +3,11 @@
 // gf_autotune times real substeps of the bound scene (or batch) with the
 // stage events of gf_step and picks, one knob after the other (coordinate
 // descent), the fastest of a few candidates:
-//   g2p_threads                 threads per block of G2P            (G2P stage)
+//   p2g_tiles_k, g2p_tiles_k    tile shape of P2G and of the tile-staged G2P
+//                               (single grid): blocks of 8 x 8 x 8 cells (1)
+//                               or 8 x 8 x 16 (2)              (P2G, G2P stage)
+//   g2p_threads                 threads per block of the batches' per-particle
+//                               G2P                                 (G2P stage)
 //   grid_threads, blocks_per_sm launch shape of the grid-stride face/cell
 //                               kernels (forces, divergence, project)
 //   pcg_blocks_per_sm           resident blocks per SM of the global-memory
@@ -72,8 +76,8 @@ static void snap_free(Snapshot &s) {
 }
 
 // Stage times of one substep from the snapshot: [0] whole step, [1] G2P,
-// [2] forces + divergence + project, [3] pressure solver kernel(s).
-static int trial(Ctx *c, const Snapshot &s, const gf_step_params *prm, float out[4]) {
+// [2] forces + divergence + project, [3] pressure solver kernel(s), [4] P2G.
+static int trial(Ctx *c, const Snapshot &s, const gf_step_params *prm, float out[5]) {
   int e = snap_restore(c, s);
   if (e) return e;
   if ((e = gf_step(c, prm))) return e;
@@ -88,6 +92,7 @@ static int trial(Ctx *c, const Snapshot &s, const gf_step_params *prm, float out
   out[3] = 0.f;
   if (prm->solver == GF_PCG || prm->solver == GF_PCG_REFINED)
     cudaEventElapsedTime(&out[3], c->ev[8], c->ev[9]);
+  cudaEventElapsedTime(&out[4], c->ev[1], c->ev[2]);
   return GF_OK;
 }
 
@@ -96,7 +101,7 @@ static int measure(Ctx *c, const Snapshot &s, const gf_step_params *prm, int whi
                    float *best) {
   *best = 3.4e38f;
   for (int r = 0; r < reps; ++r) {
-    float t[4];
+    float t[5];
     int e = trial(c, s, prm, t);
     if (e) return e;
     if (t[which] < *best) *best = t[which];
@@ -105,6 +110,8 @@ static int measure(Ctx *c, const Snapshot &s, const gf_step_params *prm, int whi
 }
 
 static void to_info(const Tune &t, gf_tune_info *o) {
+  o->p2g_tiles_k = t.p2g_tiles_k;
+  o->g2p_tiles_k = t.g2p_tiles_k;
   o->g2p_threads = t.g2p_threads;
   o->grid_threads = t.grid_threads;
   o->grid_blocks_per_sm = t.grid_blocks_per_sm;
@@ -126,8 +133,23 @@ int gf_autotune(void *ctx, const gf_step_params *prm, gf_tune_info *out) {
   float before = 0.f, after = 0.f;
   const int reps = 2;
   if (!e) e = gf::measure(c, snap, prm, 0, reps, &before);
-  // G2P block size
-  if (!e) {
+  // tile shapes of P2G and G2P (single grid), fastest stage time of each
+  if (!e && c->nseg == 0) {
+    for (int knob = 0; knob < 2 && !e; ++knob) {
+      int &v = knob == 0 ? c->tune.p2g_tiles_k : c->tune.g2p_tiles_k;
+      int best_v = v;
+      float best = 3.4e38f;
+      for (int kt = 1; kt <= 2; ++kt) {
+        v = kt;
+        float t;
+        if ((e = gf::measure(c, snap, prm, knob == 0 ? 4 : 1, reps, &t))) break;
+        if (t < best) { best = t; best_v = kt; }
+      }
+      v = best_v;
+    }
+  }
+  // G2P block size of the batches' per-particle kernel
+  if (!e && c->nseg > 0) {
     const int cand[] = {128, 256, 512};
     int best_v = c->tune.g2p_threads;
     float best = 3.4e38f;
@@ -201,8 +223,11 @@ int gf_set_tune(void *ctx, const gf_tune_info *in) {
   auto ok_threads = [](int t, int hi) { return t >= 32 && t <= hi && t % 32 == 0; };
   if (!ok_threads(in->g2p_threads, 512) || !ok_threads(in->grid_threads, 1024) ||
       in->grid_blocks_per_sm < 1 || in->grid_blocks_per_sm > 64 || in->pcg_blocks_per_sm < 0 ||
-      in->pcg_blocks_per_sm > 8)
+      in->pcg_blocks_per_sm > 8 || in->p2g_tiles_k < 1 || in->p2g_tiles_k > 2 ||
+      in->g2p_tiles_k < 1 || in->g2p_tiles_k > 2)
     return gf::fail(c, GF_INVALID_ARG, "gf_set_tune: launch shape out of range");
+  c->tune.p2g_tiles_k = in->p2g_tiles_k;
+  c->tune.g2p_tiles_k = in->g2p_tiles_k;
   c->tune.g2p_threads = in->g2p_threads;
   c->tune.grid_threads = in->grid_threads;
   c->tune.grid_blocks_per_sm = in->grid_blocks_per_sm;

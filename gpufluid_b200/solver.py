@@ -677,6 +677,31 @@ class FlipSolver3D:
         _lib.check(self._L.gf_stage_times(self._ctx, ms), self._ctx, "gf_stage_times")
         return list(ms)
 
+    def autotune(self, dt: float, pressure_iters: int = 80,
+                 pressure_solver: str = "jacobi") -> dict:
+        """Time substeps from the current state (restored afterwards) and keep
+        the fastest tile shapes of P2G and G2P (8^3 or 8 x 8 x 16 cells per
+        block) and launch shapes of the grid kernels; returns the choice and
+        the substep time before and after (``gf_autotune``)."""
+        prm = self._params(dt, pressure_iters, pressure_solver)
+        info = _lib.TuneInfo()
+        self._set_stream()
+        _lib.check(self._L.gf_autotune(self._ctx, _lib.ctypes.byref(prm),
+                                       _lib.ctypes.byref(info)), self._ctx, "gf_autotune")
+        self._cuda_graph_invalidate()  # shapes changed: recapture
+        return {k: getattr(info, k) for k, _ in _lib.TuneInfo._fields_}
+
+    def set_tune(self, **shape) -> None:
+        """Impose tile and launch shapes (keys of ``gf_tune_info``)."""
+        info = _lib.TuneInfo()
+        _lib.check(self._L.gf_get_tune(self._ctx, _lib.ctypes.byref(info)), self._ctx,
+                   "gf_get_tune")
+        for k, v in shape.items():
+            setattr(info, k, v)
+        _lib.check(self._L.gf_set_tune(self._ctx, _lib.ctypes.byref(info)), self._ctx,
+                   "gf_set_tune")
+        self._cuda_graph_invalidate()
+
     def launch_count(self) -> int:
         """Kernels of this library executed for this solver (direct launches
         plus the kernel nodes of every CUDA-graph replay)."""

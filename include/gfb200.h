@@ -434,15 +434,19 @@ int gf_batch_pressure_stats(void *ctx, int32_t *iters, double *relres, int32_t *
 
 /* ---- launch-shape autotuner --------------------------------------------- */
 /* No counterpart in the reference.  gf_autotune times real substeps (the
- * particle state is restored afterwards) and keeps the fastest launch shapes
- * for G2P, the grid-stride face/cell kernels and the global-memory PCG;
- * gf_get_tune / gf_set_tune read or impose them.  Synchronises. */
+ * particle state is restored afterwards) and keeps the fastest tile and launch
+ * shapes: the cell blocks of P2G and of the tile-staged G2P (single grid),
+ * the batches' G2P block size, the grid-stride face/cell kernels and the
+ * global-memory PCG's residency; gf_get_tune / gf_set_tune read or impose
+ * them.  Synchronises. */
 typedef struct gf_tune_info {
-  int32_t g2p_threads;        /* threads per G2P block (32..512) */
+  int32_t g2p_threads;        /* threads per block of the batches' G2P (32..512) */
   int32_t grid_threads;       /* threads per block of forces/divergence/project */
   int32_t grid_blocks_per_sm; /* cap of their grid-stride launches */
   int32_t pcg_blocks_per_sm;  /* global-memory PCG residency, 0 = occupancy maximum */
   float step_ms_before, step_ms_after;  /* gf_autotune: substep time before / after */
+  int32_t p2g_tiles_k;        /* P2G blocks: 8^3 cells (1) or 8 x 8 x 16 (2) */
+  int32_t g2p_tiles_k;        /* tile-staged G2P blocks: 8^3 cells (1) or 8 x 8 x 16 (2) */
 } gf_tune_info;
 int gf_autotune(void *ctx, const gf_step_params *prm, gf_tune_info *out);
 int gf_get_tune(void *ctx, gf_tune_info *out);

@@ -254,3 +254,24 @@ def test_refined_pcg_warm_start(gf, oracle):
         assert rel_l2(s.p.numpy(), p64) < 1e-6
         it[warm] = n
     assert sum(it[True][4:]) < sum(it[False][4:]), it
+
+
+def test_autotune_tile_shapes_and_state_restored(gf):
+    """gf_autotune on a single scene: picks P2G and G2P tile shapes (8^3 or
+    8 x 8 x 16 blocks), leaves the particle state where it was, and the
+    tuned substep reaches the state an untuned one does."""
+    out = []
+    for tune in (False, True):
+        s = dam_break(gf.FlipSolver3D, (48, 40, 64), transfer="apic")
+        s.vel = np.random.default_rng(5).normal(0, 0.5, (s.n_particles, 3)).astype(np.float32)
+        before = s.get_particles()
+        if tune:
+            info = s.autotune(1 / 240, 60, "jacobi")
+            assert info["p2g_tiles_k"] in (1, 2) and info["g2p_tiles_k"] in (1, 2), info
+            assert info["step_ms_before"] > 0 and info["step_ms_after"] > 0
+            after = s.get_particles()
+            assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
+        for _ in range(3):
+            s.step(1 / 240, pressure_iters=60, pressure_solver="jacobi")
+        out.append(s.get_particles()[0])
+    assert rel_l2(out[1], out[0]) < 1e-5

@@ -84,12 +84,17 @@ def test_bin_labels_keys_order_bitexact(gf, oracle, grid):
     assert_bitexact("sort order", order_g, order_o.astype(np.int32))
 
 
+@pytest.mark.parametrize("tiles_k", [1, 2])
 @pytest.mark.parametrize("transfer", ["flip", "apic"])
-@pytest.mark.parametrize("grid", GRIDS[:2])
-def test_p2g_matches_oracle(gf, oracle, grid, transfer):
+@pytest.mark.parametrize("grid", GRIDS[:2] + [(17, 12, 40)])
+def test_p2g_matches_oracle(gf, oracle, grid, transfer, tiles_k):
+    """P2G with blocks of 8^3 or 8 x 8 x 16 cells per CTA (the autotuner's
+    tile shapes; 40 cells along k give an odd tile count, so the last block
+    holds one tile)."""
     import torch
     nx, ny, nz = grid
     s = _mk(gf, grid, transfer=transfer)
+    s.set_tune(p2g_tiles_k=tiles_k)
     pos, vel, C = random_particles(nx, ny, nz, s.dx, 30000, seed=7)
     s._set_particles(pos=pos, vel=vel, C=C)
     _call(s, "gf_bin", 2 if transfer == "apic" else 0)
@@ -236,12 +241,17 @@ def test_project_bitexact(gf, oracle, grid):
         assert_bitexact(k, getattr(s, "_" + k).cpu().numpy(), getattr(o, k))
 
 
+@pytest.mark.parametrize("tiles_k", [1, 2])
 @pytest.mark.parametrize("transfer,blend", [("flip", 0.95), ("pic", 0.0), ("apic", 0.95)])
-@pytest.mark.parametrize("grid", GRIDS)
-def test_g2p_bitexact(gf, oracle, grid, transfer, blend):
+@pytest.mark.parametrize("grid", GRIDS + [(24, 16, 40), (32, 32, 32)])
+def test_g2p_bitexact(gf, oracle, grid, transfer, blend, tiles_k):
+    """G2P (the tile-staged kernel: TMA boxes where the strides allow, e.g.
+    u and v at 24x16x40 and all six arrays but w, ws at 32^3, plain loads
+    otherwise) with blocks of 8^3 or 8 x 8 x 16 cells."""
     import torch
     nx, ny, nz = grid
     s = _mk(gf, grid, transfer=transfer)
+    s.set_tune(g2p_tiles_k=tiles_k)
     s.flip_blend = blend
     rng = np.random.default_rng(nx * 31 + ny)
     o = _oracle(oracle, s)
