@@ -96,7 +96,8 @@ class TuneInfo(ctypes.Structure):
     _fields_ = [("g2p_threads", ctypes.c_int32), ("grid_threads", ctypes.c_int32),
                 ("grid_blocks_per_sm", ctypes.c_int32), ("pcg_blocks_per_sm", ctypes.c_int32),
                 ("step_ms_before", ctypes.c_float), ("step_ms_after", ctypes.c_float),
-                ("p2g_tiles_k", ctypes.c_int32), ("g2p_tiles_k", ctypes.c_int32)]
+                ("p2g_tiles_k", ctypes.c_int32), ("g2p_tiles_k", ctypes.c_int32),
+                ("p2g_map", ctypes.c_int32)]
 
 
 GF_MESH_TRILINEAR, GF_MESH_CUBIC, GF_MESH_SDF = 0, 1, 2

@@ -208,7 +208,7 @@ __device__ __forceinline__ void p2g_flush_box(const P2GArgs &a, const T *s_val, 
 // single grid), ntk (<= KT) the tiles it holds along k, which are consecutive
 // in the sorted order.  The boxes live in dynamic shared memory
 // (p2g_smem_bytes).
-template <bool APIC, int KT, typename T = P2G_ACC>
+template <bool APIC, int KT, int MAP = 0, typename T = P2G_ACC>
 __device__ __forceinline__ void p2g_tile_body(const P2GArgs &a, int t, int64_t key0, int ntk) {
   extern __shared__ __align__(16) unsigned char p2g_smem[];
   constexpr int BK = P2G_BOXK(KT);
@@ -223,16 +223,50 @@ __device__ __forceinline__ void p2g_tile_body(const P2GArgs &a, int t, int64_t k
   __syncthreads();
   const int ti = t / (a.nty * a.ntz), tj = (t / a.ntz) % a.nty, tk = t % a.ntz;
   const int I0 = ti * TILE, J0 = tj * TILE, K0 = tk * TILE;
-  // Lane l of every warp walks its own contiguous run [l*run, (l+1)*run) of
-  // the tile's cell-sorted particles, so the 32 lanes of one instruction sit
-  // about run/ppc cells apart and their shared atomics rarely share an
-  // address (consecutive lanes would hit the same cell's 8 corners).
+  // Lane-to-particle mapping (the autotuner's p2g_map):
+  //  0: lane l of every warp walks its own contiguous run [l*run, (l+1)*run)
+  //     of the block's cell-sorted particles, so the 32 lanes of one
+  //     instruction sit about run/ppc cells apart and their shared atomics
+  //     rarely share an address (consecutive lanes would hit one cell's 8
+  //     corners), and every lane has the same work;
+  //  1: a warp takes 32 cells at a time -- 4 rows of 8 along k, consecutive
+  //     in the sort key -- and lane l the k-th particle of cell l in round k,
+  //     so one instruction's atomics land on nearly consecutive box entries
+  //     (few bank conflicts); lanes of emptier cells idle.
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int64_t np_tile = e - b, run = (np_tile + 31) >> 5;
-  for (int64_t s = warp; s < run; s += nwarps) {
-    const int64_t off = (int64_t)lane * run + s;
-    if (off >= np_tile) continue;
-    const int64_t q = b + off;
+  const int ngroups = MAP == 1 ? ntk * (TILE_CELLS / 32) : 0;
+  int g = warp, kround = 0, cnt = 0;
+  int64_t first = 0;
+  if (MAP == 1 && g < ngroups) {
+    const int64_t key = key0 + g * 32 + lane;
+    first = a.start[key];
+    cnt = (int)(a.start[key + 1] - first);
+  }
+  for (int64_t s = warp;; s += nwarps) {
+    int64_t q;
+    if (MAP == 0) {
+      if (s >= run) break;
+      const int64_t off = (int64_t)lane * run + s;
+      if (off >= np_tile) continue;
+      q = b + off;
+    } else {
+      // next (cell group, round) with work for this warp
+      while (g < ngroups && kround >= __reduce_max_sync(0xffffffffu, (unsigned)cnt)) {
+        g += nwarps;
+        kround = 0;
+        cnt = 0;
+        if (g < ngroups) {
+          const int64_t key = key0 + g * 32 + lane;
+          first = a.start[key];
+          cnt = (int)(a.start[key + 1] - first);
+        }
+      }
+      if (g >= ngroups) break;
+      const int kk = kround++;
+      if (kk >= cnt) continue;
+      q = first + kk;
+    }
     float4 r0 = a.rec0[q], r1 = a.rec1[q];
     float4 r2 = make_float4(0, 0, 0, 0), r3 = r2;
     if (APIC) {
@@ -267,13 +301,13 @@ __host__ __device__ constexpr size_t p2g_smem_bytes(int KT) {
 
 // One CTA per block of KT tiles along k: block b holds tiles (ti, tj, KT*kb
 // .. KT*kb + KT - 1) with kb = b % ceil(ntz / KT), clipped to the grid.
-template <bool APIC, int KT>
+template <bool APIC, int KT, int MAP>
 __global__ void __launch_bounds__(256) k_p2g_tile(P2GArgs a) {
   const int ntkb = (a.ntz + KT - 1) / KT;
   const int kb = blockIdx.x % ntkb, r = blockIdx.x / ntkb;
   const int t = r * a.ntz + KT * kb;  // r = ti * nty + tj
   const int ntk = a.ntz - KT * kb < KT ? a.ntz - KT * kb : KT;
-  p2g_tile_body<APIC, KT>(a, t, (int64_t)t * TILE_CELLS, ntk);
+  p2g_tile_body<APIC, KT, MAP>(a, t, (int64_t)t * TILE_CELLS, ntk);
 }
 
 // --------------------------------------------------------------- forces
@@ -1118,10 +1152,14 @@ int launch_p2g(Ctx *c, int transfer) {
                              (int)sm);
       kern<<<g, 256, sm, st>>>(a);
     };
-    if (transfer == GF_APIC)
-      kt == 2 ? launch(k_p2g_tile<true, 2>) : launch(k_p2g_tile<true, 1>);
-    else
-      kt == 2 ? launch(k_p2g_tile<false, 2>) : launch(k_p2g_tile<false, 1>);
+    const int map = c->tune.p2g_map == 1 ? 1 : 0;
+    if (transfer == GF_APIC) {
+      if (map) kt == 2 ? launch(k_p2g_tile<true, 2, 1>) : launch(k_p2g_tile<true, 1, 1>);
+      else     kt == 2 ? launch(k_p2g_tile<true, 2, 0>) : launch(k_p2g_tile<true, 1, 0>);
+    } else {
+      if (map) kt == 2 ? launch(k_p2g_tile<false, 2, 1>) : launch(k_p2g_tile<false, 1, 1>);
+      else     kt == 2 ? launch(k_p2g_tile<false, 2, 0>) : launch(k_p2g_tile<false, 1, 0>);
+    }
     c->launches++;
   }
   return check_launch(c, "gf_p2g");

@@ -6,6 +6,8 @@
 //   p2g_tiles_k, g2p_tiles_k    tile shape of P2G and of the tile-staged G2P
 //                               (single grid): blocks of 8 x 8 x 8 cells (1)
 //                               or 8 x 8 x 16 (2)              (P2G, G2P stage)
+//   p2g_map                     P2G lanes: runs of particles (0) or one cell
+//                               each (1)                            (P2G stage)
 //   g2p_threads                 threads per block of the batches' per-particle
 //                               G2P                                 (G2P stage)
 //   grid_threads, blocks_per_sm launch shape of the grid-stride face/cell
@@ -111,6 +113,7 @@ static int measure(Ctx *c, const Snapshot &s, const gf_step_params *prm, int whi
 
 static void to_info(const Tune &t, gf_tune_info *o) {
   o->p2g_tiles_k = t.p2g_tiles_k;
+  o->p2g_map = t.p2g_map;
   o->g2p_tiles_k = t.g2p_tiles_k;
   o->g2p_threads = t.g2p_threads;
   o->grid_threads = t.grid_threads;
@@ -135,15 +138,16 @@ int gf_autotune(void *ctx, const gf_step_params *prm, gf_tune_info *out) {
   if (!e) e = gf::measure(c, snap, prm, 0, reps, &before);
   // tile shapes of P2G and G2P (single grid), fastest stage time of each
   if (!e && c->nseg == 0) {
-    for (int knob = 0; knob < 2 && !e; ++knob) {
-      int &v = knob == 0 ? c->tune.p2g_tiles_k : c->tune.g2p_tiles_k;
+    for (int knob = 0; knob < 3 && !e; ++knob) {
+      int &v = knob == 0 ? c->tune.p2g_tiles_k : (knob == 1 ? c->tune.p2g_map : c->tune.g2p_tiles_k);
+      const int lo = knob == 1 ? 0 : 1;
       int best_v = v;
       float best = 3.4e38f;
-      for (int kt = 1; kt <= 2; ++kt) {
-        v = kt;
+      for (int x = lo; x <= lo + 1; ++x) {
+        v = x;
         float t;
-        if ((e = gf::measure(c, snap, prm, knob == 0 ? 4 : 1, reps, &t))) break;
-        if (t < best) { best = t; best_v = kt; }
+        if ((e = gf::measure(c, snap, prm, knob == 2 ? 1 : 4, reps, &t))) break;
+        if (t < best) { best = t; best_v = x; }
       }
       v = best_v;
     }
@@ -224,9 +228,10 @@ int gf_set_tune(void *ctx, const gf_tune_info *in) {
   if (!ok_threads(in->g2p_threads, 512) || !ok_threads(in->grid_threads, 1024) ||
       in->grid_blocks_per_sm < 1 || in->grid_blocks_per_sm > 64 || in->pcg_blocks_per_sm < 0 ||
       in->pcg_blocks_per_sm > 8 || in->p2g_tiles_k < 1 || in->p2g_tiles_k > 2 ||
-      in->g2p_tiles_k < 1 || in->g2p_tiles_k > 2)
+      in->g2p_tiles_k < 1 || in->g2p_tiles_k > 2 || in->p2g_map < 0 || in->p2g_map > 1)
     return gf::fail(c, GF_INVALID_ARG, "gf_set_tune: launch shape out of range");
   c->tune.p2g_tiles_k = in->p2g_tiles_k;
+  c->tune.p2g_map = in->p2g_map;
   c->tune.g2p_tiles_k = in->g2p_tiles_k;
   c->tune.g2p_threads = in->g2p_threads;
   c->tune.grid_threads = in->grid_threads;

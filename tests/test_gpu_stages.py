@@ -84,17 +84,17 @@ def test_bin_labels_keys_order_bitexact(gf, oracle, grid):
     assert_bitexact("sort order", order_g, order_o.astype(np.int32))
 
 
-@pytest.mark.parametrize("tiles_k", [1, 2])
+@pytest.mark.parametrize("tiles_k,lanes", [(1, 0), (2, 0), (1, 1), (2, 1)])
 @pytest.mark.parametrize("transfer", ["flip", "apic"])
 @pytest.mark.parametrize("grid", GRIDS[:2] + [(17, 12, 40)])
-def test_p2g_matches_oracle(gf, oracle, grid, transfer, tiles_k):
-    """P2G with blocks of 8^3 or 8 x 8 x 16 cells per CTA (the autotuner's
-    tile shapes; 40 cells along k give an odd tile count, so the last block
-    holds one tile)."""
+def test_p2g_matches_oracle(gf, oracle, grid, transfer, tiles_k, lanes):
+    """P2G with blocks of 8^3 or 8 x 8 x 16 cells per CTA and either lane
+    mapping (the autotuner's choices; 40 cells along k give an odd tile count,
+    so the last block holds one tile)."""
     import torch
     nx, ny, nz = grid
     s = _mk(gf, grid, transfer=transfer)
-    s.set_tune(p2g_tiles_k=tiles_k)
+    s.set_tune(p2g_tiles_k=tiles_k, p2g_map=lanes)
     pos, vel, C = random_particles(nx, ny, nz, s.dx, 30000, seed=7)
     s._set_particles(pos=pos, vel=vel, C=C)
     _call(s, "gf_bin", 2 if transfer == "apic" else 0)
