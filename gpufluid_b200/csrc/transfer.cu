@@ -323,12 +323,29 @@ struct GridArgs {
 
 // Face slot q = (i*(ny+1) + j)*(nz+1) + k carries the u, v and w faces (i,j,k)
 // that exist.
-__device__ __forceinline__ void forces_slot(const GridArgs &a, int64_t q, float gd) {
+// (i, j, k) of face slot q; 32-bit division when the slot count allows it
+// (a 64-bit division is several times the instructions).
+__device__ __forceinline__ void slot_ijk(int64_t q, int ny1, int nz1, bool small, int &i, int &j,
+                                         int &k) {
+  if (small) {
+    const uint32_t u = (uint32_t)q, r = u / (uint32_t)nz1;
+    k = (int)(u - r * (uint32_t)nz1);
+    j = (int)(r % (uint32_t)ny1);
+    i = (int)(r / (uint32_t)ny1);
+  } else {
+    k = (int)(q % nz1);
+    const int64_t r = q / nz1;
+    j = (int)(r % ny1);
+    i = (int)(r / ny1);
+  }
+}
+
+__device__ __forceinline__ void forces_slot(const GridArgs &a, int64_t q, float gd,
+                                            bool small = false) {
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   {
-    int k = (int)(q % (nz + 1));
-    int64_t r = q / (nz + 1);
-    int j = (int)(r % (ny + 1)), i = (int)(r / (ny + 1));
+    int i, j, k;
+    slot_ijk(q, ny + 1, nz + 1, small, i, j, k);
     if (j < ny && k < nz) {  // u face (i,j,k), i <= nx
       int64_t g = ((int64_t)i * ny + j) * nz + k;
       float wt = a.uw[g];
@@ -365,21 +382,22 @@ __device__ __forceinline__ void forces_slot(const GridArgs &a, int64_t q, float 
 
 __global__ void k_forces(GridArgs a, float gd) {
   int64_t n = (int64_t)(a.nx + 1) * (a.ny + 1) * (a.nz + 1);
+  const bool small = n < ((int64_t)1 << 32);
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
        q += (int64_t)gridDim.x * blockDim.x)
-    forces_slot(a, q, gd);
+    forces_slot(a, q, gd, small);
 }
 
-__device__ __forceinline__ void divergence_cell(const GridArgs &a, int64_t c, float scale) {
+__device__ __forceinline__ void divergence_cell(const GridArgs &a, int64_t c, float scale,
+                                                bool small = false) {
   const int ny = a.ny, nz = a.nz;
   {
     if (a.label[c] != 1) {
       a.div[c] = 0.0f;
       return;
     }
-    int k = (int)(c % nz);
-    int64_t r = c / nz;
-    int j = (int)(r % ny), i = (int)(r / ny);
+    int i, j, k;
+    slot_ijk(c, ny, nz, small, i, j, k);
     float d = a.u[((int64_t)(i + 1) * ny + j) * nz + k] - a.u[c];
     d = d + a.v[((int64_t)i * (ny + 1) + j + 1) * nz + k];
     d = d - a.v[((int64_t)i * (ny + 1) + j) * nz + k];
@@ -391,17 +409,18 @@ __device__ __forceinline__ void divergence_cell(const GridArgs &a, int64_t c, fl
 
 __global__ void k_divergence(GridArgs a, float scale) {
   int64_t n = (int64_t)a.nx * a.ny * a.nz;
+  const bool small = n < ((int64_t)1 << 32);
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
        c += (int64_t)gridDim.x * blockDim.x)
-    divergence_cell(a, c, scale);
+    divergence_cell(a, c, scale, small);
 }
 
-__device__ __forceinline__ void project_slot(const GridArgs &a, int64_t q, float scale) {
+__device__ __forceinline__ void project_slot(const GridArgs &a, int64_t q, float scale,
+                                             bool small = false) {
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   {
-    int k = (int)(q % (nz + 1));
-    int64_t r = q / (nz + 1);
-    int j = (int)(r % (ny + 1)), i = (int)(r / (ny + 1));
+    int i, j, k;
+    slot_ijk(q, ny + 1, nz + 1, small, i, j, k);
     const int64_t c = ((int64_t)i * ny + j) * nz + k;  // valid when i<nx,j<ny,k<nz
     if (j < ny && k < nz) {  // u face
       int64_t g = ((int64_t)i * ny + j) * nz + k;
@@ -462,9 +481,10 @@ __device__ __forceinline__ void project_slot(const GridArgs &a, int64_t q, float
 
 __global__ void k_project(GridArgs a, float scale) {
   int64_t n = (int64_t)(a.nx + 1) * (a.ny + 1) * (a.nz + 1);
+  const bool small = n < ((int64_t)1 << 32);
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
        q += (int64_t)gridDim.x * blockDim.x)
-    project_slot(a, q, scale);
+    project_slot(a, q, scale, small);
 }
 
 // ------------------------------------------------------------------- G2P
