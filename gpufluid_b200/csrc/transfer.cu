@@ -673,7 +673,8 @@ __global__ void __launch_bounds__(512) k_g2p(G2PArgs a) {
 }
 
 // ------------------------------------------------------- G2P, tile-staged
-// k_g2p_tile: one CTA per 8x8x8 tile of the cell-sorted particles.  The faces
+// k_g2p_tile: CTAs per 8x8x8 tile (or 8x8x16 block) of the cell-sorted
+// particles, up to G2P_SPLIT_N particles each.  The faces
 // the tile's particles can gather -- per component a box of 9 faces on its
 // normal axis and 10 on the transverse axes around the tile -- are staged in
 // shared memory first: by TMA (cp.async.bulk.tensor, completion on an
@@ -714,6 +715,8 @@ static_assert(gbox_vol(0) == 1440 && gbox_vol(1) == 1440 && gbox_vol(2) == 1200,
 static_assert(gbox_off(2) == 2880 && gbox_set(1) == GBOX_SET, "box set");
 static_assert(gbox_set(2) == 6368, "box set of 8 x 8 x 16 blocks");
 constexpr int G2P_TILE_THREADS = 256;
+constexpr int G2P_SPLIT_N = 1024;  // particles per CTA (4 rounds of 256)
+constexpr int G2P_SPLITS = 4;      // CTAs per 8^3 tile: 4096 particles at 8 per cell
 constexpr long long G2P_WAIT_LIMIT = 1LL << 22;  // try_wait polls before giving up
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
@@ -800,14 +803,21 @@ __global__ void __launch_bounds__(G2P_TILE_THREADS)
   __shared__ int s_ok;
   const G2PArgs &a = ta.g;
   const int tid = threadIdx.x;
-  // block -> its KT tiles along k (clipped at the grid's last tile)
+  // CTA -> (block of KT tiles along k, clipped at the grid's last tile; part
+  // of the block's particles): G2P_SPLIT_N particles per CTA, the last part
+  // taking whatever a crowded block holds beyond, so the work is spread over
+  // many more CTAs than blocks
+  constexpr int S = G2P_SPLITS * KT;
+  const int sidx = blockIdx.x % S, blk = blockIdx.x / S;
   const int ntkb = (ta.ntz + KT - 1) / KT;
-  const int kb = blockIdx.x % ntkb, rij = blockIdx.x / ntkb;
+  const int kb = blk % ntkb, rij = blk / ntkb;
   const int t = rij * ta.ntz + KT * kb;
   const int ntk = ta.ntz - KT * kb < KT ? ta.ntz - KT * kb : KT;
-  const int64_t b = ta.start[(int64_t)t * TILE_CELLS],
-                e = ta.start[(int64_t)(t + ntk) * TILE_CELLS];
-  if (b == e) return;
+  const int64_t b0 = ta.start[(int64_t)t * TILE_CELLS],
+                e0 = ta.start[(int64_t)(t + ntk) * TILE_CELLS];
+  const int64_t b = b0 + (int64_t)sidx * G2P_SPLIT_N;
+  const int64_t e = sidx == S - 1 ? e0 : (b + G2P_SPLIT_N < e0 ? b + G2P_SPLIT_N : e0);
+  if (b >= e) return;
   const int ti = rij / ta.nty, tj = rij % ta.nty;
   const int I0 = ti * TILE, J0 = tj * TILE, K0 = KT * kb * TILE;
   const int nx = a.nx, ny = a.ny, nz = a.nz;
@@ -1267,9 +1277,18 @@ int launch_g2p(Ctx *c, int transfer, float flip_blend, float dt) {
   G2PArgs a{c->rec0, c->rec1, c->f.u, c->f.v, c->f.w, c->f.us, c->f.vs, c->f.ws,
             c->p.pos, c->p.vel, c->p.C, c->p.pid, c->p.n, c->dx, dt, flip_blend,
             c->dom[0], c->dom[1], c->dom[2], c->nx, c->ny, c->nz};
+  if (c->tune.g2p_tiles_k == 0) {  // no staging: one thread per particle, L1/L2 gathers
+    if (transfer == GF_APIC)
+      k_g2p<true><<<g, th, 0, c->stream>>>(a);
+    else
+      k_g2p<false><<<g, th, 0, c->stream>>>(a);
+    c->launches++;
+    return check_launch(c, "gf_g2p");
+  }
   G2PTileArgs ta{a, c->start, c->nty, c->ntz, c->health + 5};
   const int kt = c->tune.g2p_tiles_k == 2 ? 2 : 1;
-  const unsigned gb = (unsigned)(c->ntx * c->nty * ((c->ntz + kt - 1) / kt));
+  const unsigned gb =
+      (unsigned)(c->ntx * c->nty * ((c->ntz + kt - 1) / kt) * G2P_SPLITS * kt);
   const FaceMaps &fm = kt == 2 ? c->face_maps2 : c->face_maps;
   auto launch = [&](auto kern, int mode) {
     const size_t sm = g2p_smem_bytes(mode, kt);  // beside the static staging buffers

@@ -5,7 +5,8 @@
 // descent), the fastest of a few candidates:
 //   p2g_tiles_k, g2p_tiles_k    tile shape of P2G and of the tile-staged G2P
 //                               (single grid): blocks of 8 x 8 x 8 cells (1)
-//                               or 8 x 8 x 16 (2)              (P2G, G2P stage)
+//                               or 8 x 8 x 16 (2); for G2P also 0, the
+//                               unstaged per-particle kernel   (P2G, G2P stage)
 //   p2g_map                     P2G lanes: runs of particles (0) or one cell
 //                               each (1)                            (P2G stage)
 //   g2p_threads                 threads per block of the batches' per-particle
@@ -140,10 +141,11 @@ int gf_autotune(void *ctx, const gf_step_params *prm, gf_tune_info *out) {
   if (!e && c->nseg == 0) {
     for (int knob = 0; knob < 3 && !e; ++knob) {
       int &v = knob == 0 ? c->tune.p2g_tiles_k : (knob == 1 ? c->tune.p2g_map : c->tune.g2p_tiles_k);
-      const int lo = knob == 1 ? 0 : 1;
+      // P2G blocks 1..2 tiles, lane maps 0..1, G2P 0 (unstaged) ..2 tiles
+      const int lo = knob == 0 ? 1 : 0, hi = knob == 1 ? 1 : 2;
       int best_v = v;
       float best = 3.4e38f;
-      for (int x = lo; x <= lo + 1; ++x) {
+      for (int x = lo; x <= hi; ++x) {
         v = x;
         float t;
         if ((e = gf::measure(c, snap, prm, knob == 2 ? 1 : 4, reps, &t))) break;
@@ -228,7 +230,7 @@ int gf_set_tune(void *ctx, const gf_tune_info *in) {
   if (!ok_threads(in->g2p_threads, 512) || !ok_threads(in->grid_threads, 1024) ||
       in->grid_blocks_per_sm < 1 || in->grid_blocks_per_sm > 64 || in->pcg_blocks_per_sm < 0 ||
       in->pcg_blocks_per_sm > 8 || in->p2g_tiles_k < 1 || in->p2g_tiles_k > 2 ||
-      in->g2p_tiles_k < 1 || in->g2p_tiles_k > 2 || in->p2g_map < 0 || in->p2g_map > 1)
+      in->g2p_tiles_k < 0 || in->g2p_tiles_k > 2 || in->p2g_map < 0 || in->p2g_map > 1)
     return gf::fail(c, GF_INVALID_ARG, "gf_set_tune: launch shape out of range");
   c->tune.p2g_tiles_k = in->p2g_tiles_k;
   c->tune.p2g_map = in->p2g_map;

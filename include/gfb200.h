@@ -446,7 +446,8 @@ typedef struct gf_tune_info {
   int32_t pcg_blocks_per_sm;  /* global-memory PCG residency, 0 = occupancy maximum */
   float step_ms_before, step_ms_after;  /* gf_autotune: substep time before / after */
   int32_t p2g_tiles_k;        /* P2G blocks: 8^3 cells (1) or 8 x 8 x 16 (2) */
-  int32_t g2p_tiles_k;        /* tile-staged G2P blocks: 8^3 cells (1) or 8 x 8 x 16 (2) */
+  int32_t g2p_tiles_k;        /* tile-staged G2P blocks: 8^3 cells (1) or 8 x 8 x 16 (2);
+                                 0: one thread per particle, no staged boxes */
   int32_t p2g_map;            /* P2G lanes: runs of a block's particles (0), one cell each (1) */
 } gf_tune_info;
 int gf_autotune(void *ctx, const gf_step_params *prm, gf_tune_info *out);

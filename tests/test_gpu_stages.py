@@ -241,13 +241,14 @@ def test_project_bitexact(gf, oracle, grid):
         assert_bitexact(k, getattr(s, "_" + k).cpu().numpy(), getattr(o, k))
 
 
-@pytest.mark.parametrize("tiles_k", [1, 2])
+@pytest.mark.parametrize("tiles_k", [0, 1, 2])
 @pytest.mark.parametrize("transfer,blend", [("flip", 0.95), ("pic", 0.0), ("apic", 0.95)])
 @pytest.mark.parametrize("grid", GRIDS + [(24, 16, 40), (32, 32, 32)])
 def test_g2p_bitexact(gf, oracle, grid, transfer, blend, tiles_k):
     """G2P (the tile-staged kernel: TMA boxes where the strides allow, e.g.
     u and v at 24x16x40 and all six arrays but w, ws at 32^3, plain loads
-    otherwise) with blocks of 8^3 or 8 x 8 x 16 cells."""
+    otherwise) with blocks of 8^3 or 8 x 8 x 16 cells, and the unstaged
+    per-particle kernel (tile shape 0)."""
     import torch
     nx, ny, nz = grid
     s = _mk(gf, grid, transfer=transfer)

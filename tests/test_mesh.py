@@ -420,5 +420,5 @@ def test_particles_to_mesh(gf):
     d = om.density_field(pos, (32, 32, 32), 1.0 / 32, 2, 0)
     assert v is not None and om.mesh_volume(v, t) > 0
     # the blob's extent agrees with the oracle's field to within a cell
-    ov, _ = om.iso_surface(d, 0.5, 1.0 / 32)
+    ov, _ = om.iso_surface_mc(d, 0.5, 1.0 / 32)
     assert abs(len(v) - len(ov)) <= 0.01 * len(ov)
