@@ -678,8 +678,9 @@ def extra_legs(torch, device, steps=3):
     1e-5 with at most 200 iterations; 256^3 double dam break (x in [0,.3] and
     [.7,1], y in [0,.7]), FLIP 0.97, dt 1/960, refined PCG to 1e-7 (the
     global-memory solver: the active region exceeds the shared-memory one)
-    with the tile SGS preconditioner and, from the same state, with the
-    reference's Jacobi one, and 200 Jacobi sweeps as the plain comparison,
+    with the tile SGS preconditioner, then warm-started from the previous
+    substep's pressure, and, from the same state, with the reference's Jacobi
+    preconditioner, and 200 Jacobi sweeps as the plain comparison,
     with per-stage times and the device memory footprint."""
     import gpufluid_b200 as gf
     stream = torch.cuda.current_stream()
@@ -718,6 +719,15 @@ def extra_legs(torch, device, steps=3):
     snap = snapshot(s)
     ms_ref = timed(s, dt, 4000, "pcg_refined", steps)
     st_ref = s.pressure_stats()
+    # the same substeps with each solve started from the previous pressure
+    # (one untimed substep first, so the first timed solve starts from its
+    # predecessor's answer)
+    restore(s, snap)
+    s.pcg_warm_start = True
+    s.step(dt, pressure_iters=4000, pressure_solver="pcg_refined")
+    ms_warm = timed(s, dt, 4000, "pcg_refined", steps)
+    st_warm = s.pressure_stats()
+    s.pcg_warm_start = False
     # the same substeps with the reference's Jacobi preconditioner
     restore(s, snap)
     s.pcg_preconditioner = "jacobi"
@@ -743,6 +753,10 @@ def extra_legs(torch, device, steps=3):
         "refined_substeps_per_s": round(1000 / ms_ref, 3),
         "refined_iters_last": st_ref["iters"],
         "refined_preconditioner": "tile-local symmetric Gauss-Seidel, 2 sweeps",
+        "refined_warm_start_ms_per_substep": round(ms_warm, 3),
+        "refined_warm_start_substeps_per_s": round(1000 / ms_warm, 3),
+        "refined_warm_start_iters_last": st_warm["iters"],
+        "refined_warm_start_relres_last": st_warm["relres"],
         "refined_jacobi_precond_ms_per_substep": round(ms_ref_jac, 3),
         "refined_jacobi_precond_iters_last": st_ref_jac["iters"],
         "pcg_kernel": "global-memory" if st_ref["kernel"] == 2 else "shared-memory",

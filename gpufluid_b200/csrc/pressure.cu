@@ -347,6 +347,12 @@ struct PcgArgs {
   float sign;      // b = sign * div
   int only_if_fallback;  // run only when the shared-memory solver deferred
   int sgs;         // tile-local symmetric Gauss-Seidel sweeps (SGS instantiation)
+  // warm start (refined only): x64 starts at the dense pressure p0 of the
+  // previous solve; the tile list and grid sizes map a slot to its cell of p0
+  int warm;
+  const float *p0;
+  const int32_t *tile_list;
+  int ny, nz, nty, ntz;
 };
 
 // ---- tile-local symmetric Gauss-Seidel preconditioner of the global-memory
@@ -513,7 +519,31 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
   float *__restrict__ AD = a.Ad;
   const uint16_t *__restrict__ CODE = a.code;
 
-  // ---- init: x = 0, r = b, z = M^-1 r, d = 0 (so the first d = z)
+  // ---- init: x = 0, r = b, z = M^-1 r, d = 0 (so the first d = z).  With
+  // the warm start (refined only) x64 = p0 at each fluid cell and r = b - A p0
+  // in FP64 from the dense p0 (complete and read-only during the solve); the
+  // stop test stays relative to ||b||, so the accuracy target is unchanged.
+  const bool warm = REF && a.warm && a.p0 != nullptr;
+  double wb2 = 0.0, wr2 = 0.0;  // this thread's sums of b^2 and (b - A p0)^2
+  auto warm_residual = [&](int64_t q, uint16_t code, float b) -> float {
+    const int t = a.tile_list[q >> 9];
+    const int l = (int)(q & 511);
+    const int ti = t / (a.nty * a.ntz), tj = (t / a.ntz) % a.nty, tk = t % a.ntz;
+    const int64_t sI = (int64_t)a.ny * a.nz;
+    const int64_t g = (int64_t)(ti * 8 + (l >> 6)) * sI + (tj * 8 + ((l >> 3) & 7)) * a.nz +
+                      (tk * 8 + (l & 7));
+    const double x0 = (double)a.p0[g];
+    const int64_t off[6] = {-sI, sI, -(int64_t)a.nz, (int64_t)a.nz, -1, 1};
+    double sum = 0.0;
+#pragma unroll
+    for (int dir = 0; dir < 6; ++dir)
+      if (code & (1 << dir)) sum += (double)a.p0[g + off[dir]];
+    const double res = (double)b - ((double)((code >> CODE_DIAG_SHIFT) & 7) * x0 - sum);
+    a.x64[q] = x0;
+    wb2 += (double)b * (double)b;
+    wr2 += res * res;
+    return (float)res;
+  };
   {
     Acc v[2] = {0, 0};
     if (SGS) {
@@ -525,6 +555,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
           const int64_t q = (int64_t)(base + m) * 512 + tid;
           const uint16_t code = base + m < na ? CODE[q] : (uint16_t)0;
           bb[m] = (code & CODE_FLUID) ? a.sign * a.bdiv[q] : 0.0f;
+          if (warm && (code & CODE_FLUID)) bb[m] = warm_residual(q, code, bb[m]);
           if (code & CODE_FLUID) a.r[q] = bb[m];
           S.r[m * 512 + tid] = bb[m];
           S.code[m * 512 + tid] = code;
@@ -546,7 +577,8 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
       for (int64_t q = q0; q < total; q += stride) {
         const uint16_t code = a.code[q];
         if (!(code & CODE_FLUID)) continue;
-        const float b = a.sign * a.bdiv[q];
+        float b = a.sign * a.bdiv[q];
+        if (warm) b = warm_residual(q, code, b);
         const float diag = fmaxf((float)((code >> CODE_DIAG_SHIFT) & 7), 1.0f);
         const float z = b / diag;
         a.r[q] = b;
@@ -555,19 +587,32 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
         v[1] += (Acc)(b * b);
       }
     }
+    if (warm) {
+      double w[2] = {wb2, wr2};
+      if (!grid_reduce<double, 2>(a, w, [&](double *t) {
+            st->b2 = t[0];
+            st->r_true2 = t[1];
+          }))
+        return;
+    }
     if (!grid_reduce<Acc, 2>(a, v, [&](double *t) {
           st->rz = t[0];
           st->r0 = t[1];
           st->rr = t[1];
-          st->b2 = t[1];
           st->r_upd2 = t[1];
-          st->r_true2 = t[1];
           st->beta = 0.0;
           st->alpha = 0.0;
           st->iters = 0;
           st->n_replace = 0;
           st->status = GF_OK;
-          st->done = t[1] < 1e-30 ? 1 : 0;  // the reference's early exit (:2982-2986)
+          if (warm) {
+            const double b2 = ld_volatile_d(&st->b2), rt2 = ld_volatile_d(&st->r_true2);
+            st->done = b2 < 1e-30 || rt2 <= a.tol2 * b2 ? 1 : 0;
+          } else {
+            st->b2 = t[1];
+            st->r_true2 = t[1];
+            st->done = t[1] < 1e-30 ? 1 : 0;  // the reference's early exit (:2982-2986)
+          }
         }))
       return;
   }
@@ -1746,7 +1791,9 @@ int launch_pressure(Ctx *c, const gf_step_params *prm) {
     PcgArgs pa{c->n_active, c->tile_nbr, c->code, c->bdiv, c->xf, c->r, c->z, c->d0, c->d1,
                c->Ad, refined ? c->x64 : nullptr, c->partials, c->state,
                prm->max_iters, check_every, prm->tol * prm->tol, replace2, sign,
-               force_global ? 0 : 1, (prm->flags & GF_FLAG_SGS_MASK) >> GF_FLAG_SGS_SHIFT};
+               force_global ? 0 : 1, (prm->flags & GF_FLAG_SGS_MASK) >> GF_FLAG_SGS_SHIFT,
+               (refined && (prm->flags & GF_FLAG_WARM_START)) ? 1 : 0, c->f.p, c->tile_list,
+               c->ny, c->nz, c->nty, c->ntz};
     if (refined) {
       e = launch_pcg<double, true>(c, pa);
       result64 = c->x64;

@@ -203,6 +203,120 @@ __device__ __forceinline__ void p2g_flush_box(const P2GArgs &a, const T *s_val, 
   }
 }
 
+// Per-cell register accumulation (p2g_map 2), one face component COMP: lane
+// l owns cell (ci, cj, ck) and sums the contributions of all its particles
+// to the union of their stencils -- 2 faces along the component's normal
+// axis (i0 = the cell index), 3 along each transverse one (i0 = cell - 1 or
+// cell) -- in 18 register pairs, then adds the non-empty sums to the box: at
+// most 36 shared atomics per cell and component where scattering particle by
+// particle costs 16 per particle.  At each step of the flush the lanes add to
+// distinct faces (distinct cells, one common offset).  Each corner weight is
+// wx * wy * wz with zero factors off the particle's own 2 x 2 x 2 corners,
+// so the per-face sums are those of the particle-by-particle scatter in
+// another order.  A particle whose stencil does not start in its cell's
+// pattern (a position outside the grid, binned into a boundary cell) goes
+// through scatter_comp.
+template <bool APIC, int KT, int COMP, typename T>
+__device__ __forceinline__ void p2g_cell_comp(const P2GArgs &a, T *s_val, T *s_wt, int64_t first,
+                                              int cnt, int maxcnt, int ci, int cj, int ck,
+                                              int I0, int J0, int K0) {
+  constexpr int EX = COMP == 0 ? 2 : 3, EY = COMP == 1 ? 2 : 3, EZ = COMP == 2 ? 2 : 3;
+  constexpr float HX = COMP == 0 ? 0.0f : 0.5f, HY = COMP == 1 ? 0.0f : 0.5f,
+                  HZ = COMP == 2 ? 0.0f : 0.5f;
+  const int xo = ci - (COMP != 0), yo = cj - (COMP != 1), zo = ck - (COMP != 2);
+  const float dx = a.dx;
+  float av[EX * EY * EZ], aw[EX * EY * EZ];
+#pragma unroll
+  for (int m = 0; m < EX * EY * EZ; ++m) av[m] = aw[m] = 0.0f;
+  for (int kp = 0; kp < maxcnt; ++kp) {
+    if (kp >= cnt) continue;
+    const int64_t q = first + kp;
+    const float4 r0 = a.rec0[q];
+    float vp, c0 = 0.f, c1 = 0.f, c2 = 0.f;
+    // C rows: (r1.w, r2.x, r2.y) (r2.z, r2.w, r3.x) (r3.y, r3.z, r3.w)
+    if (COMP == 0) {
+      const float4 r1 = a.rec1[q];
+      vp = r1.x;
+      if (APIC) {
+        const float4 r2 = a.rec2[q];
+        c0 = r1.w; c1 = r2.x; c2 = r2.y;
+      }
+    } else if (COMP == 1) {
+      vp = a.rec1[q].y;
+      if (APIC) {
+        const float4 r2 = a.rec2[q], r3 = a.rec3[q];
+        c0 = r2.z; c1 = r2.w; c2 = r3.x;
+      }
+    } else {
+      vp = a.rec1[q].z;
+      if (APIC) {
+        const float4 r3 = a.rec3[q];
+        c0 = r3.y; c1 = r3.z; c2 = r3.w;
+      }
+    }
+    const float fx = __fdiv_rn(r0.x, dx) - HX, fy = __fdiv_rn(r0.y, dx) - HY,
+                fz = __fdiv_rn(r0.z, dx) - HZ;
+    const int i0 = __float2int_rz(floorf(fx)), j0 = __float2int_rz(floorf(fy)),
+              k0 = __float2int_rz(floorf(fz));
+    const int rx = i0 - xo, ry = j0 - yo, rz = k0 - zo;
+    if (rx < 0 || rx + 2 > EX || ry < 0 || ry + 2 > EY || rz < 0 || rz + 2 > EZ) {
+      float *gv = COMP == 0 ? a.u : (COMP == 1 ? a.v : a.w);
+      float *gw = COMP == 0 ? a.uw : (COMP == 1 ? a.vw : a.ww);
+      scatter_comp<APIC, KT, T>(s_val, s_wt, COMP, vp, c0, c1, c2, r0.x, r0.y, r0.z, fx, fy, fz,
+                                I0, J0, K0, a, gv, gw);
+      continue;
+    }
+    const float sx = fx - (float)i0, sy = fy - (float)j0, sz = fz - (float)k0;
+    float wx[EX], wy[EY], wz[EZ], A[EX], B[EY], C[EZ];
+#pragma unroll
+    for (int m = 0; m < EX; ++m) {
+      wx[m] = m == rx ? 1.0f - sx : (m == rx + 1 ? sx : 0.0f);
+      A[m] = APIC ? __fmaf_rn(c0, ((float)(xo + m) + HX) * dx - r0.x, vp) : vp;
+    }
+#pragma unroll
+    for (int m = 0; m < EY; ++m) {
+      wy[m] = m == ry ? 1.0f - sy : (m == ry + 1 ? sy : 0.0f);
+      B[m] = APIC ? c1 * (((float)(yo + m) + HY) * dx - r0.y) : 0.0f;
+    }
+#pragma unroll
+    for (int m = 0; m < EZ; ++m) {
+      wz[m] = m == rz ? 1.0f - sz : (m == rz + 1 ? sz : 0.0f);
+      C[m] = APIC ? c2 * (((float)(zo + m) + HZ) * dx - r0.z) : 0.0f;
+    }
+#pragma unroll
+    for (int x = 0; x < EX; ++x)
+#pragma unroll
+      for (int y = 0; y < EY; ++y) {
+        const float wxy = wx[x] * wy[y];
+        const float ab = A[x] + B[y];
+#pragma unroll
+        for (int z = 0; z < EZ; ++z) {
+          const int m = (x * EY + y) * EZ + z;
+          const float wt = wxy * wz[z];
+          av[m] = __fmaf_rn(ab + C[z], wt, av[m]);
+          aw[m] += wt;
+        }
+      }
+  }
+  // box offsets: the register origin (xo, yo, zo) sits at box entry
+  // (ci - I0, cj - J0, ck - K0) of this component's box
+  const int ey = COMP == 1 ? BOX_N : BOX_T, ez = p2g_ez(COMP, KT);
+  const int e0 = ((ci - I0) * ey + (cj - J0)) * ez + (ck - K0);
+#pragma unroll
+  for (int x = 0; x < EX; ++x)
+#pragma unroll
+    for (int y = 0; y < EY; ++y)
+#pragma unroll
+      for (int z = 0; z < EZ; ++z) {
+        const int m = (x * EY + y) * EZ + z;
+        if (aw[m] == 0.0f) continue;
+        const int e = e0 + (x * ey + y) * ez + z;
+        if (!GF_IN(e, P2G_BOXK(KT))) continue;
+        atomicAdd(&s_val[e], (T)av[m]);
+        atomicAdd(&s_wt[e], (T)aw[m]);
+      }
+}
+
 // One block's P2G: t is its first tile within the grid (the block's
 // coordinates), key0 the sort key of that tile's first cell (t * 512 for a
 // single grid), ntk (<= KT) the tiles it holds along k, which are consecutive
@@ -232,7 +346,30 @@ __device__ __forceinline__ void p2g_tile_body(const P2GArgs &a, int t, int64_t k
   //  1: a warp takes 32 cells at a time -- 4 rows of 8 along k, consecutive
   //     in the sort key -- and lane l the k-th particle of cell l in round k,
   //     so one instruction's atomics land on nearly consecutive box entries
-  //     (few bank conflicts); lanes of emptier cells idle.
+  //     (few bank conflicts); lanes of emptier cells idle;
+  //  2: the cells of 1, each lane summing its cell's particles in registers
+  //     first, one component at a time (p2g_cell_comp).
+  if (MAP == 2) {
+    const int lane2 = threadIdx.x & 31;
+    for (int g2 = threadIdx.x >> 5; g2 < ntk * (TILE_CELLS / 32); g2 += blockDim.x >> 5) {
+      const int cl = g2 * 32 + lane2;
+      const int64_t key = key0 + cl;
+      const int64_t first = a.start[key];
+      const int cnt = (int)(a.start[key + 1] - first);
+      const int maxcnt = (int)__reduce_max_sync(0xffffffffu, (unsigned)cnt);
+      if (maxcnt == 0) continue;
+      const int l = cl & (TILE_CELLS - 1);
+      const int ci = I0 + (l >> 6), cj = J0 + ((l >> 3) & 7), ck = K0 + (cl >> 9) * TILE + (l & 7);
+      p2g_cell_comp<APIC, KT, 0, T>(a, s_val, s_wt, first, cnt, maxcnt, ci, cj, ck, I0, J0, K0);
+      p2g_cell_comp<APIC, KT, 1, T>(a, s_val + BK, s_wt + BK, first, cnt, maxcnt, ci, cj, ck, I0,
+                                    J0, K0);
+      p2g_cell_comp<APIC, KT, 2, T>(a, s_val + 2 * BK, s_wt + 2 * BK, first, cnt, maxcnt, ci, cj,
+                                    ck, I0, J0, K0);
+    }
+    __syncthreads();
+    p2g_flush_box<KT, T>(a, s_val, s_wt, I0, J0, K0);
+    return;
+  }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int64_t np_tile = e - b, run = (np_tile + 31) >> 5;
   const int ngroups = MAP == 1 ? ntk * (TILE_CELLS / 32) : 0;
@@ -301,8 +438,11 @@ __host__ __device__ constexpr size_t p2g_smem_bytes(int KT) {
 
 // One CTA per block of KT tiles along k: block b holds tiles (ti, tj, KT*kb
 // .. KT*kb + KT - 1) with kb = b % ceil(ntz / KT), clipped to the grid.
+#ifndef GF_P2G_MINB
+#define GF_P2G_MINB 2  // resident CTAs per SM the register-summing map is compiled for
+#endif
 template <bool APIC, int KT, int MAP>
-__global__ void __launch_bounds__(256) k_p2g_tile(P2GArgs a) {
+__global__ void __launch_bounds__(256, MAP == 2 ? GF_P2G_MINB : 1) k_p2g_tile(P2GArgs a) {
   const int ntkb = (a.ntz + KT - 1) / KT;
   const int kb = blockIdx.x % ntkb, r = blockIdx.x / ntkb;
   const int t = r * a.ntz + KT * kb;  // r = ti * nty + tj
@@ -1182,12 +1322,14 @@ int launch_p2g(Ctx *c, int transfer) {
                              (int)sm);
       kern<<<g, 256, sm, st>>>(a);
     };
-    const int map = c->tune.p2g_map == 1 ? 1 : 0;
+    const int map = c->tune.p2g_map >= 1 && c->tune.p2g_map <= 2 ? c->tune.p2g_map : 0;
     if (transfer == GF_APIC) {
-      if (map) kt == 2 ? launch(k_p2g_tile<true, 2, 1>) : launch(k_p2g_tile<true, 1, 1>);
+      if (map == 2) kt == 2 ? launch(k_p2g_tile<true, 2, 2>) : launch(k_p2g_tile<true, 1, 2>);
+      else if (map) kt == 2 ? launch(k_p2g_tile<true, 2, 1>) : launch(k_p2g_tile<true, 1, 1>);
       else     kt == 2 ? launch(k_p2g_tile<true, 2, 0>) : launch(k_p2g_tile<true, 1, 0>);
     } else {
-      if (map) kt == 2 ? launch(k_p2g_tile<false, 2, 1>) : launch(k_p2g_tile<false, 1, 1>);
+      if (map == 2) kt == 2 ? launch(k_p2g_tile<false, 2, 2>) : launch(k_p2g_tile<false, 1, 2>);
+      else if (map) kt == 2 ? launch(k_p2g_tile<false, 2, 1>) : launch(k_p2g_tile<false, 1, 1>);
       else     kt == 2 ? launch(k_p2g_tile<false, 2, 0>) : launch(k_p2g_tile<false, 1, 0>);
     }
     c->launches++;

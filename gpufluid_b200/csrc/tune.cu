@@ -141,8 +141,8 @@ int gf_autotune(void *ctx, const gf_step_params *prm, gf_tune_info *out) {
   if (!e && c->nseg == 0) {
     for (int knob = 0; knob < 3 && !e; ++knob) {
       int &v = knob == 0 ? c->tune.p2g_tiles_k : (knob == 1 ? c->tune.p2g_map : c->tune.g2p_tiles_k);
-      // P2G blocks 1..2 tiles, lane maps 0..1, G2P 0 (unstaged) ..2 tiles
-      const int lo = knob == 0 ? 1 : 0, hi = knob == 1 ? 1 : 2;
+      // P2G blocks 1..2 tiles, lane maps 0..2, G2P 0 (unstaged) ..2 tiles
+      const int lo = knob == 0 ? 1 : 0, hi = 2;
       int best_v = v;
       float best = 3.4e38f;
       for (int x = lo; x <= hi; ++x) {
@@ -230,7 +230,7 @@ int gf_set_tune(void *ctx, const gf_tune_info *in) {
   if (!ok_threads(in->g2p_threads, 512) || !ok_threads(in->grid_threads, 1024) ||
       in->grid_blocks_per_sm < 1 || in->grid_blocks_per_sm > 64 || in->pcg_blocks_per_sm < 0 ||
       in->pcg_blocks_per_sm > 8 || in->p2g_tiles_k < 1 || in->p2g_tiles_k > 2 ||
-      in->g2p_tiles_k < 0 || in->g2p_tiles_k > 2 || in->p2g_map < 0 || in->p2g_map > 1)
+      in->g2p_tiles_k < 0 || in->g2p_tiles_k > 2 || in->p2g_map < 0 || in->p2g_map > 2)
     return gf::fail(c, GF_INVALID_ARG, "gf_set_tune: launch shape out of range");
   c->tune.p2g_tiles_k = in->p2g_tiles_k;
   c->tune.p2g_map = in->p2g_map;

@@ -26,7 +26,7 @@ default path):
 * ``pcg_coarse=True`` (new): adds a coarse correction to the shared-memory
   PCG's preconditioner -- one constant per region, four regions of tiles per
   solver block -- for fewer iterations again.
-* ``pcg_warm_start=True`` (new): the refined shared-memory PCG starts from
+* ``pcg_warm_start=True`` (new): the refined PCG (either kernel) starts from
   the previous substep's pressure instead of zero (the reference's solves
   start from zero); the stop test stays relative to ||b||.
 * Particles are kept sorted by cell inside the solver; ``pos``/``vel``/

@@ -116,12 +116,12 @@ typedef struct gf_step_params {
  * gf_health_read).  It exercises the bounded-wait exit path without a fault;
  * the context stays usable.  No effect on the global-memory kernel. */
 #define GF_FLAG_TEST_STALL 64
-/* flags: the refined shared-memory PCG starts from the pressure in fields.p
- * (the previous substep's solution) instead of from zero; the initial
- * residual b - A p is formed in FP64 and the stop test stays ||b - A x|| <=
- * tol ||b||, so the answer's accuracy is the cold start's.  No counterpart in
- * the reference (its solves start from zero every substep); other solvers
- * ignore it. */
+/* flags: the refined PCG (shared-memory or global-memory kernel) starts from
+ * the pressure in fields.p (the previous substep's solution) instead of from
+ * zero; the initial residual b - A p is formed in FP64 and the stop test
+ * stays ||b - A x|| <= tol ||b||, so the answer's accuracy is the cold
+ * start's.  No counterpart in the reference (its solves start from zero every
+ * substep); other solvers ignore it. */
 #define GF_FLAG_WARM_START 128
 
 /* ---- context ------------------------------------------------------------ */
@@ -448,7 +448,8 @@ typedef struct gf_tune_info {
   int32_t p2g_tiles_k;        /* P2G blocks: 8^3 cells (1) or 8 x 8 x 16 (2) */
   int32_t g2p_tiles_k;        /* tile-staged G2P blocks: 8^3 cells (1) or 8 x 8 x 16 (2);
                                  0: one thread per particle, no staged boxes */
-  int32_t p2g_map;            /* P2G lanes: runs of a block's particles (0), one cell each (1) */
+  int32_t p2g_map;            /* P2G lanes: runs of a block's particles (0), one cell each (1),
+                                 one cell each summed in registers first (2) */
 } gf_tune_info;
 int gf_autotune(void *ctx, const gf_step_params *prm, gf_tune_info *out);
 int gf_get_tune(void *ctx, gf_tune_info *out);

@@ -169,7 +169,7 @@ def test_pcg_at_its_cap_is_reported_not_raised(gf, graphs):
                                    "failed": 0, "last_status": "OK"}
 
 
-def _stall_case(gf, oracle, n=32):
+def _stall_case(gf, n=32):
     import torch
     s = gf.FlipSolver3D(n, n, n)
     lab = s._marker_host.copy()

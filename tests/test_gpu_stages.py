@@ -84,13 +84,13 @@ def test_bin_labels_keys_order_bitexact(gf, oracle, grid):
     assert_bitexact("sort order", order_g, order_o.astype(np.int32))
 
 
-@pytest.mark.parametrize("tiles_k,lanes", [(1, 0), (2, 0), (1, 1), (2, 1)])
+@pytest.mark.parametrize("tiles_k,lanes", [(1, 0), (2, 0), (1, 1), (2, 1), (1, 2), (2, 2)])
 @pytest.mark.parametrize("transfer", ["flip", "apic"])
 @pytest.mark.parametrize("grid", GRIDS[:2] + [(17, 12, 40)])
 def test_p2g_matches_oracle(gf, oracle, grid, transfer, tiles_k, lanes):
-    """P2G with blocks of 8^3 or 8 x 8 x 16 cells per CTA and either lane
-    mapping (the autotuner's choices; 40 cells along k give an odd tile count,
-    so the last block holds one tile)."""
+    """P2G with blocks of 8^3 or 8 x 8 x 16 cells per CTA and each lane
+    mapping, per-cell register sums included (the autotuner's choices; 40
+    cells along k give an odd tile count, so the last block holds one tile)."""
     import torch
     nx, ny, nz = grid
     s = _mk(gf, grid, transfer=transfer)
@@ -449,3 +449,38 @@ def test_global_pcg_tile_sgs_preconditioner(gf, oracle, grid, refined):
             assert rel_l2(s._p.cpu().numpy(), p64) < 1e-4
         res[sweeps] = info.iters
     assert res[2] < res[1] < res[0], res
+
+
+@pytest.mark.parametrize("kernel_flags", ["global_sgs2", "global_jacobi", "smem"])
+def test_refined_pcg_warm_start_both_kernels(gf, oracle, kernel_flags):
+    """GF_FLAG_WARM_START on the refined PCG: after a solve, a nearby system
+    (the divergence perturbed by 2%) solved from the previous pressure meets
+    the same FP64 stop test relative to ||b||, gives the FP64 answer, and
+    takes fewer iterations than the cold start of the same system."""
+    import torch
+    from gpufluid_b200 import _lib
+    base = {"global_sgs2": _lib.GF_FLAG_GLOBAL_PCG | (2 << _lib.GF_FLAG_SGS_SHIFT),
+            "global_jacobi": _lib.GF_FLAG_GLOBAL_PCG, "smem": 0}[kernel_flags]
+    kernel = 1 if kernel_flags == "smem" else 2
+    s, o = _pressure_case(gf, oracle, (48, 40, 56), seed=17)
+    it = ctypes.c_int32()
+    _call(s, "gf_pressure", ctypes.byref(_params(gf, "pcg_refined", 6000, tol=1e-10, flags=base)),
+          ctypes.byref(it))
+    rng = np.random.default_rng(4)
+    div2 = np.where(o.marker == 1, o.div * (1 + 0.02 * rng.normal(0, 1, o.div.shape)), 0)
+    div2 = div2.astype(np.float32)
+    o.div[...] = div2
+    p64, _, _ = oracle.pcg64(o.marker, o.div, tol=1e-14)
+    iters = {}
+    for warm in (True, False):  # the warm solve first: fields.p holds the last answer
+        s.div.copy_(_t(div2))
+        flags = base | (_lib.GF_FLAG_WARM_START if warm else 0)
+        _call(s, "gf_pressure", ctypes.byref(_params(gf, "pcg_refined", 6000, tol=1e-10,
+                                                     flags=flags)), ctypes.byref(it))
+        torch.cuda.synchronize()
+        info = _stats(s)
+        assert info.kernel == kernel and info.status == 0, (warm, info.kernel, info.status)
+        assert info.relres <= 1e-10, (warm, info.relres)
+        assert rel_l2(s._p.cpu().numpy(), p64) < 1e-6
+        iters[warm] = info.iters
+    assert iters[True] < iters[False], iters
