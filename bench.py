@@ -66,10 +66,12 @@ SPHERE = ((0.7, 0.2, 0.5), 0.12)
 BOX = ((0.0, 0.0, 0.0), (0.4, 0.6, 1.0))
 SGS_SWEEPS = 2  # tile-local symmetric Gauss-Seidel sweeps of the headline solve
 COARSE = True   # plus the block-region coarse correction
+WARM_START = True  # each refined solve starts from the previous substep's pressure
 WORKLOAD = ("APIC dam break + sphere obstacle, 128^3 (dx=1/128), 8 ppc -> 3,969,024 "
             "particles, dt=1/480, pressure: FP32 PCG + FP64 residual replacement to 1e-8, "
             "tile-local symmetric Gauss-Seidel preconditioner (2 sweeps) + block-region "
-            "coarse correction")
+            "coarse correction, each solve started from the previous substep's pressure "
+            "(stop test ||b - Ap|| <= 1e-8 ||b|| as from zero)")
 
 
 def peaks():
@@ -150,12 +152,12 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------- scene
-def make_solver(gf, device, graphs=True, precond="tile_sgs", coarse=COARSE):
+def make_solver(gf, device, graphs=True, precond="tile_sgs", coarse=COARSE, warm=WARM_START):
     from gpufluid_b200 import scene
     s = gf.FlipSolver3D(GRID, GRID, GRID, transfer_mode="apic", flip_blend=0.95,
                         device=device, pressure_tol=TOL, enable_cuda_graphs=graphs,
                         pcg_preconditioner=precond, pcg_sgs_sweeps=SGS_SWEEPS,
-                        pcg_coarse=coarse)
+                        pcg_coarse=coarse, pcg_warm_start=warm)
     s.add_solid_from_sdf(scene.sdf_sphere(s.cell_centers_np(), *SPHERE))
     s.seed_box(*BOX)
     return s
@@ -296,8 +298,10 @@ def fp64_cpu_solve(lab, div, x0=None, tol=1e-13):
 def fp64_error_leg(torch, s, snap0, steps=120, every=20):
     """The 128^3 workload's own protocol: 120 substeps of the refined solve
     from the seeded state; every 20 substeps the float32 pressure is compared
-    with an FP64 solve of the same system on the host CPU."""
+    with an FP64 solve of the same system on the host CPU (the solver's
+    settings as timed, warm start included)."""
     restore(s, snap0)
+    s._p.zero_()  # no previous pressure at the seeded state
     rows = []
     t0 = time.perf_counter()
     for k in range(1, steps + 1):
@@ -792,9 +796,12 @@ def run_ours(args):
         s.step(DT, pressure_iters=MAX_ITERS, pressure_solver="pcg_refined")
     torch.cuda.synchronize()
     snap = snapshot(s)
+    p_snap = s._p.clone()  # the last solve's pressure: the warm start of the next
 
     # ---- plain FP32 PCG from the same state (same 1e-8 target, recursive
-    # residual), with the reference's Jacobi preconditioner
+    # residual), with the reference's Jacobi preconditioner; every comparison
+    # leg starts its solves from zero, as the reference does
+    s.pcg_warm_start = False
     s.pcg_preconditioner = "jacobi"
     s.pcg_coarse = False
     s.step(DT, pressure_iters=MAX_ITERS, pressure_solver="pcg")  # capture its graph
@@ -819,7 +826,22 @@ def run_ours(args):
     refj_err = pressure_error_fp64(torch, s) if check else None
     s.pcg_preconditioner = "tile_sgs"
     s.pcg_coarse = COARSE
+    # ---- the headline solver with every solve started from zero
     restore(s, snap)
+    s.step(DT, pressure_iters=MAX_ITERS, pressure_solver="pcg_refined")  # capture
+    torch.cuda.synchronize()
+    restore(s, snap)
+    barrier()
+    torch.cuda.synchronize()
+    ms_cold, _ = timed_steps(torch, s, args.steps, "pcg_refined")
+    cold_stats = s.pressure_stats()
+    s.pcg_warm_start = WARM_START
+    restore(s, snap)
+    s._p.copy_(p_snap)
+    s.step(DT, pressure_iters=MAX_ITERS, pressure_solver="pcg_refined")  # capture
+    torch.cuda.synchronize()
+    restore(s, snap)
+    s._p.copy_(p_snap)
 
     # ---- refined (the value)
     clocks = ClockSampler(local)
@@ -836,6 +858,7 @@ def run_ours(args):
 
     # ---- per-stage device times and the PCG kernel (live, same workload)
     restore(s, snap)
+    s._p.copy_(p_snap)
     s._prof.enabled = True
     s._L.gf_enable_timing(s._ctx, 1)
     stage, pcg_ms, pcg_b = [], [], []
@@ -931,7 +954,13 @@ def run_ours(args):
                         "true_relres_fp64": ref_true,
                         "pressure_rel_error_vs_fp64": ref_err,
                         "error_vs_fp64_cpu_every_20": fp64_check,
+                        "warm_start": WARM_START,
                         "time_vs_plain": round(ms_ref / ms_plain, 3)},
+            "refined_cold_start": {"ms_per_step": round(ms_cold, 4),
+                                   "substeps_per_s": round(1000.0 / ms_cold, 3),
+                                   "iters_last": cold_stats["iters"],
+                                   "note": "the headline solver with every solve started from "
+                                           "zero (the reference's start)"},
             "refined_jacobi": {"ms_per_step": round(ms_refj, 4), "iters_last": refj_stats["iters"],
                                "pressure_rel_error_vs_fp64": refj_err,
                                "time_vs_plain": round(ms_refj / ms_plain, 3)},

@@ -144,7 +144,8 @@ struct FaceMaps {
 struct Tune {
   int p2g_tiles_k = 1;           // P2G and G2P blocks: 8 x 8 x 8 (1) or 8 x 8 x 16 cells (2)
   int g2p_tiles_k = 1;
-  int p2g_map = 0;               // P2G lanes: runs of particles (0) or one cell each (1)
+  int p2g_map = 2;               // P2G lanes: runs of particles (0), one cell each (1), one
+                                 // cell each summed in registers first (2)
   int g2p_threads = 256;
   int grid_threads = 256;        // forces / divergence / project / sweeps
   int grid_blocks_per_sm = 16;   // cap of their grid-stride launches

@@ -692,10 +692,35 @@ __device__ __forceinline__ float sample3_at(const F &at, float fx, float fy, flo
   return c0 * oz + c1 * sz;
 }
 
+// sample3_at for corners that needed no clamp (i1 = i0 + 1, j1 = j0 + 1,
+// k1 = k0 + 1): corner (di, dj, dk) is element di*si + dj*sj + dk of `p`; the
+// same products and sums in the same order.
+__device__ __forceinline__ float sample3_lin(const float *p, int si, int sj, float fx, float fy,
+                                             float fz, int i0, int j0, int k0) {
+  float sx = clampf(fx - (float)i0, 0.0f, 1.0f);
+  float sy = clampf(fy - (float)j0, 0.0f, 1.0f);
+  float sz = clampf(fz - (float)k0, 0.0f, 1.0f);
+  float c000 = p[0], c100 = p[si];
+  float c010 = p[sj], c110 = p[si + sj];
+  float c001 = p[1], c101 = p[si + 1];
+  float c011 = p[sj + 1], c111 = p[si + sj + 1];
+  float ox = 1.0f - sx, oy = 1.0f - sy, oz = 1.0f - sz;
+  float c00 = c000 * ox + c100 * sx;
+  float c10 = c010 * ox + c110 * sx;
+  float c01 = c001 * ox + c101 * sx;
+  float c11 = c011 * ox + c111 * sx;
+  float c0 = c00 * oy + c10 * sy;
+  float c1 = c01 * oy + c11 * sy;
+  return c0 * oz + c1 * sz;
+}
+
 __device__ __forceinline__ float sample3(const float *__restrict__ f, float fx, float fy,
                                          float fz, int nxm, int nym, int nzm) {
   int i0, j0, k0, i1, j1, k1;
   sample3_index(fx, fy, fz, nxm, nym, nzm, i0, j0, k0, i1, j1, k1);
+  if (i1 == i0 + 1 && j1 == j0 + 1 && k1 == k0 + 1)
+    return sample3_lin(f + ((int64_t)i0 * nym + j0) * nzm + k0, nym * nzm, nzm, fx, fy, fz, i0,
+                       j0, k0);
   return sample3_at(GlobalAt{f, (int64_t)nym * nzm, nzm, (int64_t)nxm * nym * nzm}, fx, fy, fz,
                     i0, j0, k0, i1, j1, k1);
 }
@@ -746,12 +771,68 @@ __device__ __forceinline__ void apic_gather_at(const F &at, float px, float py, 
   vel = acc;
 }
 
+// apic_gather_at when no index needs clamping (every corner inside the
+// component's grid): the corner (di, dj, dk) is element di*si + dj*sj + dk of
+// `p` (the stencil's first corner), and the per-axis face offsets and the
+// products wx * wy are formed once.  Every product and sum is the one
+// apic_gather_at forms, in the same order, so the results are identical;
+// only the index arithmetic (the clamps, one address per corner) is gone.
+__device__ __forceinline__ void apic_gather_lin(const float *p, int si, int sj, int i0, int j0,
+                                                int k0, float px, float py, float pz, float dx,
+                                                float fx, float fy, float fz, int ax, float inv,
+                                                float &vel, float &c0, float &c1, float &c2) {
+  const float sx = fx - (float)i0, sy = fy - (float)j0, sz = fz - (float)k0;
+  const float wx[2] = {1.0f - sx, sx}, wy[2] = {1.0f - sy, sy}, wz[2] = {1.0f - sz, sz};
+  float ox[2], oy[2], oz[2];
+#pragma unroll
+  for (int d = 0; d < 2; ++d) {
+    ox[d] = ax == 0 ? (float)(i0 + d) * dx - px : ((float)(i0 + d) + 0.5f) * dx - px;
+    oy[d] = ax == 1 ? (float)(j0 + d) * dx - py : ((float)(j0 + d) + 0.5f) * dx - py;
+    oz[d] = ax == 2 ? (float)(k0 + d) * dx - pz : ((float)(k0 + d) + 0.5f) * dx - pz;
+  }
+  float acc = 0.0f;
+  c0 = 0.0f;
+  c1 = 0.0f;
+  c2 = 0.0f;
+#pragma unroll
+  for (int di = 0; di < 2; ++di)
+#pragma unroll
+    for (int dj = 0; dj < 2; ++dj) {
+      const float wxy = wx[di] * wy[dj];
+#pragma unroll
+      for (int dk = 0; dk < 2; ++dk) {
+        const float wt = wxy * wz[dk];
+        const float t = wt * p[di * si + dj * sj + dk];
+        acc = acc + t;
+        const float fu = t * inv;
+        c0 = c0 + fu * ox[di];
+        c1 = c1 + fu * oy[dj];
+        c2 = c2 + fu * oz[dk];
+      }
+    }
+  vel = acc;
+}
+
+// True when apic_gather_at's stencil at (fx, fy, fz) needs no clamp.
+__device__ __forceinline__ bool stencil_inside(float fx, float fy, float fz, int snx, int sny,
+                                               int snz, int &i0, int &j0, int &k0) {
+  i0 = __float2int_rz(floorf(fx));
+  j0 = __float2int_rz(floorf(fy));
+  k0 = __float2int_rz(floorf(fz));
+  return i0 >= 0 && i0 < snx - 1 && j0 >= 0 && j0 < sny - 1 && k0 >= 0 && k0 < snz - 1;
+}
+
 __device__ __forceinline__ void apic_gather(const float *__restrict__ f, float px, float py,
                                             float pz, float dx, float fx, float fy, float fz,
                                             int snx, int sny, int snz, int ax, float inv,
                                             float &vel, float &c0, float &c1, float &c2) {
-  apic_gather_at(GlobalAt{f, (int64_t)sny * snz, snz, (int64_t)snx * sny * snz}, px, py, pz, dx,
-                 fx, fy, fz, snx, sny, snz, ax, inv, vel, c0, c1, c2);
+  int i0, j0, k0;
+  if (stencil_inside(fx, fy, fz, snx, sny, snz, i0, j0, k0))
+    apic_gather_lin(f + ((int64_t)i0 * sny + j0) * snz + k0, sny * snz, snz, i0, j0, k0, px, py,
+                    pz, dx, fx, fy, fz, ax, inv, vel, c0, c1, c2);
+  else
+    apic_gather_at(GlobalAt{f, (int64_t)sny * snz, snz, (int64_t)snx * sny * snz}, px, py, pz,
+                   dx, fx, fy, fz, snx, sny, snz, ax, inv, vel, c0, c1, c2);
 }
 
 struct G2PArgs {
@@ -1053,18 +1134,23 @@ __global__ void __launch_bounds__(G2P_TILE_THREADS)
 #pragma unroll
         for (int cc = 0; cc < 3; ++cc) {
           const int snx = nx + (cc == 0), sny = ny + (cc == 1), snz = nz + (cc == 2);
-          const int i0 = __float2int_rz(floorf(fxs[cc])), j0 = __float2int_rz(floorf(fys[cc])),
-                    k0 = __float2int_rz(floorf(fzs[cc]));
+          int i0, j0, k0;
+          const bool inside = stencil_inside(fxs[cc], fys[cc], fzs[cc], snx, sny, snz, i0, j0, k0);
           auto cl = [](int v, int n) { return v < 0 ? 0 : (v > n - 1 ? n - 1 : v); };
-          if (in_box(bx[cc], gbox_ni(cc), cl(i0, snx), cl(i0 + 1, snx), cl(j0, sny),
-                     cl(j0 + 1, sny), cl(k0, snz), cl(k0 + 1, snz)))
+          const int NJ = gbox_nj(cc), NK = gbox_nk(cc, KT);
+          if (inside && in_box(bx[cc], gbox_ni(cc), i0, i0 + 1, j0, j0 + 1, k0, k0 + 1))
+            apic_gather_lin(bx[cc].s + ((i0 - bx[cc].oi) * NJ + (j0 - bx[cc].oj)) * NK +
+                                (k0 - bx[cc].ok),
+                            NJ * NK, NK, i0, j0, k0, px, py, pz, dx, fxs[cc], fys[cc], fzs[cc],
+                            cc, inv, vel3[cc], c[3 * cc], c[3 * cc + 1], c[3 * cc + 2]);
+          else if (in_box(bx[cc], gbox_ni(cc), cl(i0, snx), cl(i0 + 1, snx), cl(j0, sny),
+                          cl(j0 + 1, sny), cl(k0, snz), cl(k0 + 1, snz)))
             apic_gather_at(bx[cc], px, py, pz, dx, fxs[cc], fys[cc], fzs[cc], snx, sny, snz, cc,
                            inv, vel3[cc], c[3 * cc], c[3 * cc + 1], c[3 * cc + 2]);
           else
-            apic_gather_at(GlobalAt{cc == 0 ? a.u : (cc == 1 ? a.v : a.w),
-                                    (int64_t)sny * snz, snz, (int64_t)snx * sny * snz},
-                           px, py, pz, dx, fxs[cc], fys[cc], fzs[cc], snx, sny, snz, cc, inv,
-                           vel3[cc], c[3 * cc], c[3 * cc + 1], c[3 * cc + 2]);
+            apic_gather(cc == 0 ? a.u : (cc == 1 ? a.v : a.w), px, py, pz, dx, fxs[cc], fys[cc],
+                        fzs[cc], snx, sny, snz, cc, inv, vel3[cc], c[3 * cc], c[3 * cc + 1],
+                        c[3 * cc + 2]);
         }
         nu = vel3[0];
         nv = vel3[1];
@@ -1081,7 +1167,13 @@ __global__ void __launch_bounds__(G2P_TILE_THREADS)
           float fx = fxs[cc], fy = fys[cc], fz = fzs[cc];
           int i0, j0, k0, i1, j1, k1;
           sample3_index(fx, fy, fz, snx, sny, snz, i0, j0, k0, i1, j1, k1);
-          if (in_box(bx[cc], gbox_ni(cc), i0, i1, j0, j1, k0, k1)) {
+          const int NJ = gbox_nj(cc), NK = gbox_nk(cc, KT);
+          if (i1 == i0 + 1 && j1 == j0 + 1 && k1 == k0 + 1 &&
+              in_box(bx[cc], gbox_ni(cc), i0, i1, j0, j1, k0, k1)) {
+            const int off = ((i0 - bx[cc].oi) * NJ + (j0 - bx[cc].oj)) * NK + (k0 - bx[cc].ok);
+            pic[cc] = sample3_lin(bx[cc].s + off, NJ * NK, NK, fx, fy, fz, i0, j0, k0);
+            old[cc] = sample3_lin(bx[cc + 3].s + off, NJ * NK, NK, fx, fy, fz, i0, j0, k0);
+          } else if (in_box(bx[cc], gbox_ni(cc), i0, i1, j0, j1, k0, k1)) {
             pic[cc] = sample3_at(bx[cc], fx, fy, fz, i0, j0, k0, i1, j1, k1);
             old[cc] = sample3_at(bx[cc + 3], fx, fy, fz, i0, j0, k0, i1, j1, k1);
           } else {
@@ -1202,14 +1294,14 @@ __device__ __forceinline__ GridArgs grid_view(const BatchArgs &b, const SegRow &
   return a;
 }
 
-template <bool APIC>
-__global__ void __launch_bounds__(256) kb_p2g_tile(BatchArgs b) {
+template <bool APIC, int MAP>
+__global__ void __launch_bounds__(256, MAP == 2 ? GF_P2G_MINB : 1) kb_p2g_tile(BatchArgs b) {
   const int64_t t = blockIdx.x;
   const int s = seg_find(b.sx.tile0, b.sx.n, t);
   const SegRow r = b.sx.row[s];
   P2GArgs a{b.start, b.rec0, b.rec1, b.rec2, b.rec3, b.u + r.fu0, b.v + r.fv0, b.w + r.fw0,
             b.uw + r.fu0, b.vw + r.fv0, b.ww + r.fw0, r.dx, r.nx, r.ny, r.nz, r.nty, r.ntz};
-  p2g_tile_body<APIC, 1>(a, (int)(t - r.tile0), t * TILE_CELLS, 1);
+  p2g_tile_body<APIC, 1, MAP>(a, (int)(t - r.tile0), t * TILE_CELLS, 1);
 }
 
 __global__ void kb_forces(BatchArgs b, int64_t nslot, float gravity) {
@@ -1307,10 +1399,16 @@ int launch_p2g(Ctx *c, int transfer) {
   if (c->p.n > 0 && c->nseg > 0) {
     BatchArgs b = batch_args(c);
     const size_t sm = p2g_smem_bytes(1);
-    if (transfer == GF_APIC)
-      kb_p2g_tile<true><<<c->ntiles, 256, sm, st>>>(b);
-    else
-      kb_p2g_tile<false><<<c->ntiles, 256, sm, st>>>(b);
+    const int map = c->tune.p2g_map;
+    if (transfer == GF_APIC) {
+      if (map == 2) kb_p2g_tile<true, 2><<<c->ntiles, 256, sm, st>>>(b);
+      else if (map == 1) kb_p2g_tile<true, 1><<<c->ntiles, 256, sm, st>>>(b);
+      else kb_p2g_tile<true, 0><<<c->ntiles, 256, sm, st>>>(b);
+    } else {
+      if (map == 2) kb_p2g_tile<false, 2><<<c->ntiles, 256, sm, st>>>(b);
+      else if (map == 1) kb_p2g_tile<false, 1><<<c->ntiles, 256, sm, st>>>(b);
+      else kb_p2g_tile<false, 0><<<c->ntiles, 256, sm, st>>>(b);
+    }
     c->launches++;
   } else if (c->p.n > 0) {
     const int kt = c->tune.p2g_tiles_k == 2 ? 2 : 1;

@@ -7,8 +7,9 @@
 //                               (single grid): blocks of 8 x 8 x 8 cells (1)
 //                               or 8 x 8 x 16 (2); for G2P also 0, the
 //                               unstaged per-particle kernel   (P2G, G2P stage)
-//   p2g_map                     P2G lanes: runs of particles (0) or one cell
-//                               each (1)                            (P2G stage)
+//   p2g_map                     P2G lanes: runs of particles (0), one cell
+//                               each (1), one cell each summed in registers
+//                               first (2)                           (P2G stage)
 //   g2p_threads                 threads per block of the batches' per-particle
 //                               G2P                                 (G2P stage)
 //   grid_threads, blocks_per_sm launch shape of the grid-stride face/cell
@@ -137,9 +138,11 @@ int gf_autotune(void *ctx, const gf_step_params *prm, gf_tune_info *out) {
   float before = 0.f, after = 0.f;
   const int reps = 2;
   if (!e) e = gf::measure(c, snap, prm, 0, reps, &before);
-  // tile shapes of P2G and G2P (single grid), fastest stage time of each
-  if (!e && c->nseg == 0) {
+  // tile shapes of P2G and G2P (single grid) and the P2G lane map (single
+  // grid and batches), fastest stage time of each
+  if (!e) {
     for (int knob = 0; knob < 3 && !e; ++knob) {
+      if (c->nseg > 0 && knob != 1) continue;  // batches: 8^3 P2G tiles, per-particle G2P
       int &v = knob == 0 ? c->tune.p2g_tiles_k : (knob == 1 ? c->tune.p2g_map : c->tune.g2p_tiles_k);
       // P2G blocks 1..2 tiles, lane maps 0..2, G2P 0 (unstaged) ..2 tiles
       const int lo = knob == 0 ? 1 : 0, hi = 2;
