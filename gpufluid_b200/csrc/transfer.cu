@@ -317,6 +317,106 @@ __device__ __forceinline__ void p2g_cell_comp(const P2GArgs &a, T *s_val, T *s_w
       }
 }
 
+// Lane map 3: the cells of map 2, with the particles read from a warp-private
+// shared staging area instead of global memory.  A warp's 32 cells hold one
+// contiguous range of the sorted particles; it is loaded P2G_CH particles at
+// a time with coalesced 16-byte loads (lane i takes particles i, i + 32, ...)
+// into structure-of-arrays fields -- grid coordinates x/dx, velocity, and for
+// APIC the world position and the 3 x 3 C -- and each lane then sums its own
+// cell's particles of the chunk from there.  Reading a cell's particles
+// straight from global memory (map 2) makes every load instruction touch 32
+// different cache lines.
+constexpr int P2G_CH = 128;  // particles per warp and chunk
+__host__ __device__ constexpr int p2g_stage_fields(bool apic) { return apic ? 18 : 6; }
+// field f of staged particle i: s[f * P2G_CH + i]
+//   0..2 x/dx, y/dx, z/dx   3..5 vx, vy, vz   (APIC) 6..8 x, y, z   9..17 C row-major
+template <bool APIC, int KT, int COMP, typename T>
+__device__ __forceinline__ void p2g_cell_comp_staged(const P2GArgs &a, T *s_val, T *s_wt,
+                                                     const float *st, int lo, int cnt,
+                                                     int maxcnt, int ci, int cj, int ck, int I0,
+                                                     int J0, int K0) {
+  constexpr int EX = COMP == 0 ? 2 : 3, EY = COMP == 1 ? 2 : 3, EZ = COMP == 2 ? 2 : 3;
+  constexpr float HX = COMP == 0 ? 0.0f : 0.5f, HY = COMP == 1 ? 0.0f : 0.5f,
+                  HZ = COMP == 2 ? 0.0f : 0.5f;
+  const int xo = ci - (COMP != 0), yo = cj - (COMP != 1), zo = ck - (COMP != 2);
+  const float dx = a.dx;
+  float av[EX * EY * EZ], aw[EX * EY * EZ];
+#pragma unroll
+  for (int m = 0; m < EX * EY * EZ; ++m) av[m] = aw[m] = 0.0f;
+  for (int kp = 0; kp < maxcnt; ++kp) {
+    if (kp >= cnt) continue;
+    const int i = lo + kp;
+    const float fx = st[0 * P2G_CH + i] - HX, fy = st[1 * P2G_CH + i] - HY,
+                fz = st[2 * P2G_CH + i] - HZ;
+    const float vp = st[(3 + COMP) * P2G_CH + i];
+    float px = 0.f, py = 0.f, pz = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
+    if (APIC) {
+      px = st[6 * P2G_CH + i];
+      py = st[7 * P2G_CH + i];
+      pz = st[8 * P2G_CH + i];
+      c0 = st[(9 + 3 * COMP) * P2G_CH + i];
+      c1 = st[(10 + 3 * COMP) * P2G_CH + i];
+      c2 = st[(11 + 3 * COMP) * P2G_CH + i];
+    }
+    const int i0 = __float2int_rz(floorf(fx)), j0 = __float2int_rz(floorf(fy)),
+              k0 = __float2int_rz(floorf(fz));
+    const int rx = i0 - xo, ry = j0 - yo, rz = k0 - zo;
+    if (rx < 0 || rx + 2 > EX || ry < 0 || ry + 2 > EY || rz < 0 || rz + 2 > EZ) {
+      float *gv = COMP == 0 ? a.u : (COMP == 1 ? a.v : a.w);
+      float *gw = COMP == 0 ? a.uw : (COMP == 1 ? a.vw : a.ww);
+      scatter_comp<APIC, KT, T>(s_val, s_wt, COMP, vp, c0, c1, c2, px, py, pz, fx, fy, fz, I0,
+                                J0, K0, a, gv, gw);
+      continue;
+    }
+    const float sx = fx - (float)i0, sy = fy - (float)j0, sz = fz - (float)k0;
+    float wx[EX], wy[EY], wz[EZ], A[EX], B[EY], C[EZ];
+#pragma unroll
+    for (int m = 0; m < EX; ++m) {
+      wx[m] = m == rx ? 1.0f - sx : (m == rx + 1 ? sx : 0.0f);
+      A[m] = APIC ? __fmaf_rn(c0, ((float)(xo + m) + HX) * dx - px, vp) : vp;
+    }
+#pragma unroll
+    for (int m = 0; m < EY; ++m) {
+      wy[m] = m == ry ? 1.0f - sy : (m == ry + 1 ? sy : 0.0f);
+      B[m] = APIC ? c1 * (((float)(yo + m) + HY) * dx - py) : 0.0f;
+    }
+#pragma unroll
+    for (int m = 0; m < EZ; ++m) {
+      wz[m] = m == rz ? 1.0f - sz : (m == rz + 1 ? sz : 0.0f);
+      C[m] = APIC ? c2 * (((float)(zo + m) + HZ) * dx - pz) : 0.0f;
+    }
+#pragma unroll
+    for (int x = 0; x < EX; ++x)
+#pragma unroll
+      for (int y = 0; y < EY; ++y) {
+        const float wxy = wx[x] * wy[y];
+        const float ab = A[x] + B[y];
+#pragma unroll
+        for (int z = 0; z < EZ; ++z) {
+          const int m = (x * EY + y) * EZ + z;
+          const float wt = wxy * wz[z];
+          av[m] = __fmaf_rn(ab + C[z], wt, av[m]);
+          aw[m] += wt;
+        }
+      }
+  }
+  const int ey = COMP == 1 ? BOX_N : BOX_T, ez = p2g_ez(COMP, KT);
+  const int e0 = ((ci - I0) * ey + (cj - J0)) * ez + (ck - K0);
+#pragma unroll
+  for (int x = 0; x < EX; ++x)
+#pragma unroll
+    for (int y = 0; y < EY; ++y)
+#pragma unroll
+      for (int z = 0; z < EZ; ++z) {
+        const int m = (x * EY + y) * EZ + z;
+        if (aw[m] == 0.0f) continue;
+        const int e = e0 + (x * ey + y) * ez + z;
+        if (!GF_IN(e, P2G_BOXK(KT))) continue;
+        atomicAdd(&s_val[e], (T)av[m]);
+        atomicAdd(&s_wt[e], (T)aw[m]);
+      }
+}
+
 // One block's P2G: t is its first tile within the grid (the block's
 // coordinates), key0 the sort key of that tile's first cell (t * 512 for a
 // single grid), ntk (<= KT) the tiles it holds along k, which are consecutive
@@ -348,7 +448,62 @@ __device__ __forceinline__ void p2g_tile_body(const P2GArgs &a, int t, int64_t k
   //     so one instruction's atomics land on nearly consecutive box entries
   //     (few bank conflicts); lanes of emptier cells idle;
   //  2: the cells of 1, each lane summing its cell's particles in registers
-  //     first, one component at a time (p2g_cell_comp).
+  //     first, one component at a time (p2g_cell_comp);
+  //  3: map 2 reading the particles from a warp-private staging area filled
+  //     with coalesced loads (p2g_cell_comp_staged).
+  if (MAP == 3) {
+    const int lane3 = threadIdx.x & 31, warp3 = threadIdx.x >> 5;
+    constexpr int NF = p2g_stage_fields(APIC);
+    float *st = reinterpret_cast<float *>(s_wt + 3 * BK) + warp3 * NF * P2G_CH;
+    const float dx = a.dx;
+    for (int g3 = warp3; g3 < ntk * (TILE_CELLS / 32); g3 += blockDim.x >> 5) {
+      const int cl = g3 * 32 + lane3;
+      const int64_t key = key0 + cl;
+      const int64_t first = a.start[key], end = a.start[key + 1];
+      const int64_t P0 = __shfl_sync(0xffffffffu, first, 0);
+      const int64_t P1 = __shfl_sync(0xffffffffu, end, 31);
+      if (P0 >= P1) continue;
+      const int l = cl & (TILE_CELLS - 1);
+      const int ci = I0 + (l >> 6), cj = J0 + ((l >> 3) & 7),
+                ck = K0 + (cl >> 9) * TILE + (l & 7);
+      for (int64_t c0 = P0; c0 < P1; c0 += P2G_CH) {
+        const int n = (int)(P1 - c0 < P2G_CH ? P1 - c0 : P2G_CH);
+        __syncwarp();
+        for (int i = lane3; i < n; i += 32) {
+          const int64_t q = c0 + i;
+          const float4 r0 = a.rec0[q], r1 = a.rec1[q];
+          st[0 * P2G_CH + i] = __fdiv_rn(r0.x, dx);
+          st[1 * P2G_CH + i] = __fdiv_rn(r0.y, dx);
+          st[2 * P2G_CH + i] = __fdiv_rn(r0.z, dx);
+          st[3 * P2G_CH + i] = r1.x;
+          st[4 * P2G_CH + i] = r1.y;
+          st[5 * P2G_CH + i] = r1.z;
+          if (APIC) {
+            const float4 r2 = a.rec2[q], r3 = a.rec3[q];
+            const float f[12] = {r0.x, r0.y, r0.z, r1.w, r2.x, r2.y,
+                                 r2.z, r2.w, r3.x, r3.y, r3.z, r3.w};
+#pragma unroll
+            for (int m = 0; m < 12; ++m) st[(6 + m) * P2G_CH + i] = f[m];
+          }
+        }
+        __syncwarp();
+        const int64_t lo64 = first > c0 ? first : c0, hi64 = end < c0 + n ? end : c0 + n;
+        const int cnt = hi64 > lo64 ? (int)(hi64 - lo64) : 0;
+        const int lo = (int)(lo64 - c0);
+        const int maxcnt = (int)__reduce_max_sync(0xffffffffu, (unsigned)cnt);
+        if (maxcnt == 0) continue;
+        p2g_cell_comp_staged<APIC, KT, 0, T>(a, s_val, s_wt, st, lo, cnt, maxcnt, ci, cj, ck, I0,
+                                             J0, K0);
+        p2g_cell_comp_staged<APIC, KT, 1, T>(a, s_val + BK, s_wt + BK, st, lo, cnt, maxcnt, ci,
+                                             cj, ck, I0, J0, K0);
+        p2g_cell_comp_staged<APIC, KT, 2, T>(a, s_val + 2 * BK, s_wt + 2 * BK, st, lo, cnt,
+                                             maxcnt, ci, cj, ck, I0, J0, K0);
+      }
+    }
+    __syncthreads();
+    p2g_flush_box<KT, T>(a, s_val, s_wt, I0, J0, K0);
+    return;
+  }
   if (MAP == 2) {
     const int lane2 = threadIdx.x & 31;
     for (int g2 = threadIdx.x >> 5; g2 < ntk * (TILE_CELLS / 32); g2 += blockDim.x >> 5) {
@@ -432,8 +587,11 @@ __device__ __forceinline__ void p2g_tile_body(const P2GArgs &a, int t, int64_t k
   p2g_flush_box<KT, T>(a, s_val, s_wt, I0, J0, K0);
 }
 
-__host__ __device__ constexpr size_t p2g_smem_bytes(int KT) {
-  return 2 * 3 * (size_t)P2G_BOXK(KT) * sizeof(P2G_ACC);
+// Dynamic shared memory of a P2G block: the boxes, and for lane map 3 the
+// staging areas of its 8 warps.
+__host__ __device__ constexpr size_t p2g_smem_bytes(int KT, int map = 0, bool apic = true) {
+  return 2 * 3 * (size_t)P2G_BOXK(KT) * sizeof(P2G_ACC) +
+         (map == 3 ? (size_t)8 * p2g_stage_fields(apic) * P2G_CH * sizeof(float) : 0);
 }
 
 // One CTA per block of KT tiles along k: block b holds tiles (ti, tj, KT*kb
@@ -442,7 +600,7 @@ __host__ __device__ constexpr size_t p2g_smem_bytes(int KT) {
 #define GF_P2G_MINB 2  // resident CTAs per SM the register-summing map is compiled for
 #endif
 template <bool APIC, int KT, int MAP>
-__global__ void __launch_bounds__(256, MAP == 2 ? GF_P2G_MINB : 1) k_p2g_tile(P2GArgs a) {
+__global__ void __launch_bounds__(256, MAP >= 2 ? GF_P2G_MINB : 1) k_p2g_tile(P2GArgs a) {
   const int ntkb = (a.ntz + KT - 1) / KT;
   const int kb = blockIdx.x % ntkb, r = blockIdx.x / ntkb;
   const int t = r * a.ntz + KT * kb;  // r = ti * nty + tj
@@ -1076,14 +1234,25 @@ __global__ void __launch_bounds__(G2P_TILE_THREADS)
       const int ni = gbox_ni(c), nj = gbox_nj(c), nk = gbox_nk(c, KT);
       const int oi = I0 - (c != 0), oj = J0 - (c != 1), ok = c == 2 ? K0 : K0 - 4;
       float *dst = s_box + (q / 3) * SET + gbox_off(c, KT);
-      for (int v = tid; v < ni * nj * nk; v += G2P_TILE_THREADS) {
-        const int bk = v % nk, r = v / nk, bj = r % nj, bi = r / nj;
-        const int gi = oi + bi, gj = oj + bj, gk = ok + bk;
-        float val = 0.f;
-        if (gi >= 0 && gi < snx && gj >= 0 && gj < sny && gk >= 0 && gk < snz &&
-            GF_IN(((int64_t)gi * sny + gj) * snz + gk, (int64_t)snx * sny * snz))
-          val = __ldg(src[q] + ((int64_t)gi * sny + gj) * snz + gk);
-        dst[v] = val;
+      // one thread per row of nk faces along k: the row's address once, then
+      // nk consecutive loads (zero outside the grid)
+      for (int r = tid; r < ni * nj; r += G2P_TILE_THREADS) {
+        const int bj = r % nj, bi = r / nj;
+        const int gi = oi + bi, gj = oj + bj;
+        float *drow = dst + r * nk;
+        if (gi < 0 || gi >= snx || gj < 0 || gj >= sny) {
+#pragma unroll 4
+          for (int bk = 0; bk < nk; ++bk) drow[bk] = 0.f;
+          continue;
+        }
+        const int64_t row = ((int64_t)gi * sny + gj) * snz;
+#pragma unroll 4
+        for (int bk = 0; bk < nk; ++bk) {
+          const int gk = ok + bk;
+          drow[bk] = gk >= 0 && gk < snz && GF_IN(row + gk, (int64_t)snx * sny * snz)
+                         ? __ldg(src[q] + row + gk)
+                         : 0.f;
+        }
       }
     }
   }
@@ -1295,7 +1464,7 @@ __device__ __forceinline__ GridArgs grid_view(const BatchArgs &b, const SegRow &
 }
 
 template <bool APIC, int MAP>
-__global__ void __launch_bounds__(256, MAP == 2 ? GF_P2G_MINB : 1) kb_p2g_tile(BatchArgs b) {
+__global__ void __launch_bounds__(256, MAP >= 2 ? GF_P2G_MINB : 1) kb_p2g_tile(BatchArgs b) {
   const int64_t t = blockIdx.x;
   const int s = seg_find(b.sx.tile0, b.sx.n, t);
   const SegRow r = b.sx.row[s];
@@ -1398,14 +1567,22 @@ int launch_p2g(Ctx *c, int transfer) {
             c->f.uw, c->f.vw, c->f.ww, c->dx, c->nx, c->ny, c->nz, c->nty, c->ntz};
   if (c->p.n > 0 && c->nseg > 0) {
     BatchArgs b = batch_args(c);
-    const size_t sm = p2g_smem_bytes(1);
     const int map = c->tune.p2g_map;
+    const size_t sm = p2g_smem_bytes(1, map, transfer == GF_APIC);
+    auto launch = [&](auto kern) {
+      if (sm > 48 * 1024)
+        cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sm);
+      kern<<<c->ntiles, 256, sm, st>>>(b);
+    };
     if (transfer == GF_APIC) {
-      if (map == 2) kb_p2g_tile<true, 2><<<c->ntiles, 256, sm, st>>>(b);
+      if (map == 3) launch(kb_p2g_tile<true, 3>);
+      else if (map == 2) kb_p2g_tile<true, 2><<<c->ntiles, 256, sm, st>>>(b);
       else if (map == 1) kb_p2g_tile<true, 1><<<c->ntiles, 256, sm, st>>>(b);
       else kb_p2g_tile<true, 0><<<c->ntiles, 256, sm, st>>>(b);
     } else {
-      if (map == 2) kb_p2g_tile<false, 2><<<c->ntiles, 256, sm, st>>>(b);
+      if (map == 3) launch(kb_p2g_tile<false, 3>);
+      else if (map == 2) kb_p2g_tile<false, 2><<<c->ntiles, 256, sm, st>>>(b);
       else if (map == 1) kb_p2g_tile<false, 1><<<c->ntiles, 256, sm, st>>>(b);
       else kb_p2g_tile<false, 0><<<c->ntiles, 256, sm, st>>>(b);
     }
@@ -1413,20 +1590,22 @@ int launch_p2g(Ctx *c, int transfer) {
   } else if (c->p.n > 0) {
     const int kt = c->tune.p2g_tiles_k == 2 ? 2 : 1;
     const unsigned g = (unsigned)(c->ntx * c->nty * ((c->ntz + kt - 1) / kt));
-    const size_t sm = p2g_smem_bytes(kt);
+    const int map = c->tune.p2g_map >= 0 && c->tune.p2g_map <= 3 ? c->tune.p2g_map : 0;
+    const size_t sm = p2g_smem_bytes(kt, map, transfer == GF_APIC);
     auto launch = [&](auto kern) {
       if (sm > 48 * 1024)
         cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sm);
       kern<<<g, 256, sm, st>>>(a);
     };
-    const int map = c->tune.p2g_map >= 1 && c->tune.p2g_map <= 2 ? c->tune.p2g_map : 0;
     if (transfer == GF_APIC) {
-      if (map == 2) kt == 2 ? launch(k_p2g_tile<true, 2, 2>) : launch(k_p2g_tile<true, 1, 2>);
+      if (map == 3) kt == 2 ? launch(k_p2g_tile<true, 2, 3>) : launch(k_p2g_tile<true, 1, 3>);
+      else if (map == 2) kt == 2 ? launch(k_p2g_tile<true, 2, 2>) : launch(k_p2g_tile<true, 1, 2>);
       else if (map) kt == 2 ? launch(k_p2g_tile<true, 2, 1>) : launch(k_p2g_tile<true, 1, 1>);
       else     kt == 2 ? launch(k_p2g_tile<true, 2, 0>) : launch(k_p2g_tile<true, 1, 0>);
     } else {
-      if (map == 2) kt == 2 ? launch(k_p2g_tile<false, 2, 2>) : launch(k_p2g_tile<false, 1, 2>);
+      if (map == 3) kt == 2 ? launch(k_p2g_tile<false, 2, 3>) : launch(k_p2g_tile<false, 1, 3>);
+      else if (map == 2) kt == 2 ? launch(k_p2g_tile<false, 2, 2>) : launch(k_p2g_tile<false, 1, 2>);
       else if (map) kt == 2 ? launch(k_p2g_tile<false, 2, 1>) : launch(k_p2g_tile<false, 1, 1>);
       else     kt == 2 ? launch(k_p2g_tile<false, 2, 0>) : launch(k_p2g_tile<false, 1, 0>);
     }

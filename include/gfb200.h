@@ -449,7 +449,8 @@ typedef struct gf_tune_info {
   int32_t g2p_tiles_k;        /* tile-staged G2P blocks: 8^3 cells (1) or 8 x 8 x 16 (2);
                                  0: one thread per particle, no staged boxes */
   int32_t p2g_map;            /* P2G lanes: runs of a block's particles (0), one cell each (1),
-                                 one cell each summed in registers first (2) */
+                                 one cell each summed in registers first (2), the same
+                                 reading the particles from coalesced shared staging (3) */
 } gf_tune_info;
 int gf_autotune(void *ctx, const gf_step_params *prm, gf_tune_info *out);
 int gf_get_tune(void *ctx, gf_tune_info *out);
