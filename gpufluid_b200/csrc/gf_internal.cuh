@@ -30,12 +30,16 @@ constexpr int TILE = 8;            // tile edge in cells (the reference's BLOCK_
 constexpr int TILE_CELLS = 512;    // cells per tile
 constexpr int MAX_PCG_BLOCKS = 4096;
 constexpr int COARSE_MAXG = 160;  // blocks of the shared-memory PCG, at most
-constexpr int COARSE_K = 4;       // coarse regions per block
-// coarse buffer: rows of B [CMAX][CMAX], then the compact rows of P^T A P
-// (diagonal [CMAX], count [CMAX], values [CMAX][32], columns [CMAX][32])
-constexpr int64_t COARSE_BUF_FLOATS =
-    (int64_t)(COARSE_MAXG * COARSE_K) * (COARSE_MAXG * COARSE_K) + 2 * COARSE_MAXG * COARSE_K +
-    2 * 32 * COARSE_MAXG * COARSE_K;
+// coarse regions (one per active tile of the shared-memory PCG), at most: 14
+// tiles per block; a multiple of 8, so bf16 rows of this stride are 16-byte
+// aligned
+constexpr int COARSE_RMAX = COARSE_MAXG * 14;
+static_assert(COARSE_RMAX % 8 == 0, "coarse row stride");
+// coarse buffer: rows of B = (P^T A P)^-1 as bf16 [RMAX][RMAX], then the rows
+// of P^T A P: diagonal [RMAX] and the six face-neighbour entries [RMAX][6]
+// (floats)
+constexpr int64_t COARSE_B_BYTES = (int64_t)COARSE_RMAX * COARSE_RMAX * 2;
+constexpr int64_t COARSE_BUF_BYTES = COARSE_B_BYTES + (int64_t)COARSE_RMAX * 7 * 4;
 constexpr int TRACE_CAP = 4096;
 
 // Stencil code bits (per compact cell).
@@ -86,8 +90,8 @@ struct PcgSmemArgs {
   double tol2, replace2;
   float sign;
   int sgs_sweeps;             // 0: Jacobi (the reference's); 1-3: tile-local symmetric GS
-  int coarse;                 // coarse regions per block (0: no coarse correction)
-  float *cbuf;                // coarse: rows of B, then the compact rows of P^T A P
+  int coarse;                 // 1: tile coarse correction (one region per active tile)
+  unsigned char *cbuf;        // coarse: bf16 rows of B, then the rows of P^T A P
   int test_stall;             // GF_FLAG_TEST_STALL: the first all-reduce waits for a count
                               // no block publishes, with a short spin limit
   // GF_FLAG_WARM_START (refined solve): start from the dense pressure p0 (the
@@ -192,7 +196,7 @@ struct Ctx {
   double *partials = nullptr;    // [3 * MAX_PCG_BLOCKS]
   unsigned long long *bar_counters = nullptr;  // 8 lines x 16 u64
   float *halo = nullptr;         // [6 * nkeys] halo publication buffers
-  float *coarse_buf = nullptr;   // [COARSE_BUF_FLOATS] coarse operator and inverse rows
+  unsigned char *coarse_buf = nullptr;  // [COARSE_BUF_BYTES] coarse operator and inverse rows
   int32_t *tile_cost = nullptr;  // [ntiles] per-slot PCG work estimate
   long long *trace = nullptr;    // [TRACE_CAP] PCG phase timestamps
   bool trace_on = false;

@@ -37,6 +37,8 @@
 // If the active region holds more than SmemCfg::MAXT tiles per block the
 // kernel sets PcgState::fallback and returns; the global-memory solver (k_pcg
 // in pressure.cu) launched right after it then performs the solve.
+#include <cuda_bf16.h>
+
 #include "gf_internal.cuh"
 
 namespace gf {
@@ -51,11 +53,9 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
 }
 
 constexpr int SM_MAXG = 160;      // blocks (one per SM)
-constexpr int CK = 4;             // coarse sub-regions per block, at most
-constexpr int CMAX = SM_MAXG * CK;  // coarse regions, at most
-constexpr int CCAP = 32;          // off-diagonal entries per coarse row, at most
+constexpr int CRMAX = COARSE_RMAX;  // coarse regions (one per active tile), at most
 constexpr float kCoarseTol2 = 1e-6f;  // squared residual target of the coarse row solves
-static_assert(SM_MAXG == COARSE_MAXG && CK == COARSE_K, "coarse buffer sizing");
+static_assert(SM_MAXG == COARSE_MAXG, "coarse buffer sizing");
 
 struct GridSync {
   double *partials;            // [2][4][G]
@@ -306,8 +306,9 @@ __device__ __forceinline__ void ring_fill_tagged(float *s_zb, const int *s_nbr,
 // solve's accuracy rests on its FP64 residual replacements, not on these.
 constexpr int FAST_WORDS = 4;  // words per block and parity (3 used)
 constexpr int64_t FAST_SLOTS_OFF = 2048;  // in doubles, into the partials buffer
-// tagged coarse sums g_r: [2][CMAX] u64 after the reduction words
+// tagged coarse sums g_t: [2][CRMAX] u64 after the reduction words
 constexpr int64_t COARSE_SLOTS_OFF = FAST_SLOTS_OFF + 2 * 160 * FAST_WORDS;
+static_assert(COARSE_SLOTS_OFF + 2 * CRMAX <= 3 * MAX_PCG_BLOCKS, "partials buffer");
 struct FastSync {
   unsigned long long *slots;  // [2][SM_MAXG][FAST_WORDS], zeroed per solve
   unsigned long long epoch;
@@ -495,11 +496,10 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   __shared__ int s_bounds[SM_MAXG + 1];
   __shared__ Acc sh[36 * 4];
   __shared__ double shd[36 * 4];
-  // coarse correction: region sums g = P^T r gathered from every block, the
-  // block's row of B, region of each face's neighbouring tile
-  __shared__ float s_ep[CK][32];  // warp partials of e_r = B_r . g
-  __shared__ short s_freg[MAXT * 6];
-  __shared__ float s_gw[CK][32];  // warp partials of the regions' residual sums
+  // coarse correction: warp partials of e_t = B_t . g, and of the tiles'
+  // residual sums g_t (16 warps per tile)
+  __shared__ float s_ep[32];
+  __shared__ float s_gw[MAXT * 16];
 
   PcgState *st = a.st;
   const int na = *a.n_active;
@@ -550,207 +550,14 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   const int l = threadIdx.x & 511, tl0 = threadIdx.x >> 9;
   const int pc = pad_of(l);
 
-  // ---- coarse space (a.coarse = K, sub-regions per block): the block's run
-  // of tiles is split into K runs by tile count, and each run's fluid cells
-  // form one region (GR = G K regions); P is their indicator.  Each block
-  // assembles its K rows of A_c = P^T A P (diagonal: sum over the region's
-  // cells of diag - #fluid neighbours in the region; off-diagonal: -#fluid-
-  // fluid faces to each other region), published compactly; then each of its
-  // K warps solves A_c x = e_r for one of its regions r (Jacobi-
-  // preconditioned CG in float32, warm-started from the row solved last
-  // time), which is row r of the symmetric B = A_c^-1.  The preconditioner
-  // becomes M^-1 = M_tile^-1 + P B P^T (additive two-level).  A block whose
-  // solve fails, or whose row has more than CCAP off-diagonal entries,
-  // switches the correction off for the whole solve.  Dynamic shared memory
-  // is free until the tiles load.
-  const int K = (CRS && a.cbuf != nullptr) ? a.coarse : 0;
-  const int GR = G * (K > 0 ? K : 1);
-  bool coarse = K > 0;
-  float *const Bg = a.cbuf;                                   // [GR][GR] rows of B
-  float *const Cdiag = a.cbuf + (int64_t)CMAX * CMAX;         // [GR]
-  int *const Cnnz = reinterpret_cast<int *>(Cdiag + CMAX);    // [GR]
-  float *const Cval = reinterpret_cast<float *>(Cnnz + CMAX); // [GR][CCAP]
-  int *const Ccol = reinterpret_cast<int *>(Cval + CMAX * CCAP);  // [GR][CCAP]
-  if (coarse) {
-    for (int f = threadIdx.x; f < nt * 6; f += blockDim.x) {
-      const int sl = a.nbr[(int64_t)b0 * 6 + f];
-      int r = -1;
-      if (sl >= 0) {  // the block g with bounds[g] <= sl < bounds[g + 1]
-        int lo = 0, hi = G;
-        while (hi - lo > 1) {
-          const int mid = (lo + hi) >> 1;
-          if (s_bounds[mid] <= sl) lo = mid; else hi = mid;
-        }
-        const int ntg = s_bounds[lo + 1] - s_bounds[lo];
-        r = lo * K + (sl - s_bounds[lo]) * K / ntg;
-      }
-      s_freg[f] = (short)r;
-    }
-    float *rows = reinterpret_cast<float *>(smem);  // [K][GR]
-    for (int i = threadIdx.x; i < K * GR; i += blockDim.x) rows[i] = 0.f;
-    __syncthreads();
-    const int I = blockIdx.x;
-    for (int L = threadIdx.x; L < nt * 512; L += blockDim.x) {
-      const uint16_t code = a.code[q0 + L];
-      if (!(code & CODE_FLUID)) continue;
-      const int tl = L >> 9, lc = L & 511;
-      const int li = lc >> 6, lj = (lc >> 3) & 7, lk = lc & 7;
-      const int sub = tl * K / nt, R0 = I * K + sub;
-      int same = 0;
-      for (int dir = 0; dir < 6; ++dir) {
-        if (!(code & (1 << dir))) continue;
-        const bool inside = dir == 0 ? li > 0 : dir == 1 ? li < 7 : dir == 2 ? lj > 0
-                          : dir == 3 ? lj < 7 : dir == 4 ? lk > 0 : lk < 7;
-        const int R = inside ? R0 : (int)s_freg[tl * 6 + dir];
-        if (R == R0 || R < 0) ++same; else atomicAdd(&rows[sub * GR + R], -1.0f);
-      }
-      atomicAdd(&rows[sub * GR + R0], (float)((int)((code >> CODE_DIAG_SHIFT) & 7) - same));
-    }
-    __syncthreads();
-    {  // warp r publishes row I K + r compactly (diagonal 1 for an empty region)
-      const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-      if (wid < K) {
-        const int gr = I * K + wid;
-        const float *row = rows + wid * GR;
-        int n = 0;
-        for (int c0 = 0; c0 < GR; c0 += 32) {
-          const int c = c0 + lane;
-          const float v = c < GR ? row[c] : 0.f;
-          const bool off = v != 0.f && c != gr;
-          const unsigned m = __ballot_sync(0xffffffffu, off);
-          const int k = n + __popc(m & ((1u << lane) - 1u));
-          if (off && k < CCAP) {
-            Cval[gr * CCAP + k] = v;
-            Ccol[gr * CCAP + k] = c;
-          }
-          n += __popc(m);
-        }
-        if (lane == 0) {
-          const float d = row[gr];
-          Cdiag[gr] = d > 0.f ? d : 1.0f;
-          Cnnz[gr] = n < CCAP ? n : CCAP;
-          if (n > CCAP) atomicExch(&st->coarse_off, 1);
-        }
-      }
-    }
-    {
-      double z0[1] = {0.0}, zt[1];
-      if (!grid_allreduce<double, 1>(gs, z0, zt, shd)) return;
-    }
-    // all rows of A_c and K sets of CG vectors in dynamic smem
-    float *sdi = reinterpret_cast<float *>(smem);
-    int *snz = reinterpret_cast<int *>(sdi + CMAX);
-    float *sval = reinterpret_cast<float *>(snz + CMAX);
-    short *scol = reinterpret_cast<short *>(sval + CMAX * CCAP);
-    float *vec = reinterpret_cast<float *>(scol + CMAX * CCAP);  // [K][4][CMAX]
-    for (int i = threadIdx.x; i < GR; i += blockDim.x) {
-      sdi[i] = __ldcg(Cdiag + i);
-      snz[i] = __ldcg(Cnnz + i);
-    }
-    for (int i = threadIdx.x; i < GR * CCAP; i += blockDim.x) {
-      sval[i] = __ldcg(Cval + i);
-      scol[i] = (short)__ldcg(Ccol + i);
-    }
-    __syncthreads();
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    {  // the K systems A_c x = e_{I K + q}, 32 / K warps each, in lockstep:
-       // Jacobi-preconditioned CG, warm-started from last solve's rows
-      const int per = 32 / K;                  // warps per system
-      const int q = wid / per;                 // system of this warp
-      const int nth = per * 32, lt = threadIdx.x - q * nth;
-      const int gr = I * K + q;
-      float *cx = vec + q * 4 * CMAX, *cr = cx + CMAX, *cp = cr + CMAX, *cq = cp + CMAX;
-      float *red = reinterpret_cast<float *>(vec + CK * 4 * CMAX);  // [32 warps][2] partials
-      auto matvec = [&](const float *x, int r) {
-        float acc = sdi[r] * x[r];
-        const int n = snz[r];
-        for (int k = 0; k < n; ++k) acc += sval[r * CCAP + k] * x[scol[r * CCAP + k]];
-        return acc;
-      };
-      // sum of v over the system's threads (all threads call it: a barrier)
-      auto sys_sum = [&](float v0, float v1, float *o0, float *o1) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          v0 += __shfl_xor_sync(0xffffffffu, v0, o);
-          v1 += __shfl_xor_sync(0xffffffffu, v1, o);
-        }
-        if (lane == 0) {
-          red[wid * 2 + 0] = v0;
-          red[wid * 2 + 1] = v1;
-        }
-        __syncthreads();
-        float s0 = 0.f, s1 = 0.f;
-        for (int w = q * per; w < (q + 1) * per; ++w) {
-          s0 += red[w * 2 + 0];
-          s1 += red[w * 2 + 1];
-        }
-        __syncthreads();
-        *o0 = s0;
-        *o1 = s1;
-      };
-      const float *prev = Bg + (int64_t)gr * GR;
-      for (int r = lt; r < GR; r += nth) {
-        const float x0 = __ldcg(prev + r);
-        cx[r] = isfinite(x0) ? x0 : 0.f;
-      }
-      __syncthreads();
-      float rz = 0.f, rr = 0.f;
-      {
-        float a0 = 0.f, a1 = 0.f;
-        for (int r = lt; r < GR; r += nth) {
-          const float b = (r == gr ? 1.f : 0.f) - matvec(cx, r);
-          cr[r] = b;
-          cp[r] = b / sdi[r];
-          a0 += b * cp[r];
-          a1 += b * b;
-        }
-        sys_sum(a0, a1, &rz, &rr);
-      }
-      bool ok = rr <= kCoarseTol2;  // relative to ||e_r|| = 1
-      bool dead = false;
-      for (int it = 0; it < 4 * CMAX; ++it) {
-        if (__syncthreads_and(ok || dead)) break;  // every system converged
-        float pq = 0.f, dummy = 0.f;
-        for (int r = lt; r < GR; r += nth) {
-          const float v = matvec(cp, r);
-          cq[r] = v;
-          pq += cp[r] * v;
-        }
-        sys_sum(pq, 0.f, &pq, &dummy);
-        const bool run = !(ok || dead);
-        if (run && !(pq > 0.f)) dead = true;
-        const float al = (run && !dead) ? rz / pq : 0.f;
-        float a0 = 0.f, a1 = 0.f;
-        for (int r = lt; r < GR; r += nth) {
-          cx[r] += al * cp[r];
-          const float rn = cr[r] - al * cq[r];
-          cr[r] = rn;
-          a0 += rn * rn;
-          a1 += rn * rn / sdi[r];
-        }
-        float rz2;
-        sys_sum(a0, a1, &rr, &rz2);
-        if (run && !dead && rr <= kCoarseTol2) ok = true;
-        const float be = (run && !dead && !ok) ? rz2 / rz : 0.f;
-        if (run && !dead) rz = rz2;
-        for (int r = lt; r < GR; r += nth) cp[r] = cr[r] / sdi[r] + be * cp[r];
-      }
-      bool finite = true;
-      float *out = Bg + (int64_t)gr * GR;
-      for (int r = lt; r < GR; r += nth) {
-        finite &= isfinite(cx[r]);
-        out[r] = cx[r];
-      }
-      if (lt == 0 && (!ok || dead)) atomicExch(&st->coarse_off, 1);
-      if (!finite) atomicExch(&st->coarse_off, 1);
-    }
-    __syncthreads();
-    {
-      double z0[1] = {0.0}, zt[1];
-      if (!grid_allreduce<double, 1>(gs, z0, zt, shd)) return;
-    }
-    coarse = *reinterpret_cast<volatile int *>(&st->coarse_off) == 0;
-  }
+  // ---- coarse correction (GF_FLAG_COARSE): one region per active tile, P
+  // the indicator of each tile's fluid cells, and the preconditioner
+  // M^-1 = M_tile^-1 + P B P^T (additive two-level) with B = (P^T A P)^-1,
+  // whose rows k_coarse_rows / k_coarse_solve computed before this launch (as
+  // bfloat16).  A failed row solve switched the correction off for the solve.
+  const bool coarse = CRS && a.coarse && a.cbuf != nullptr &&
+                      *reinterpret_cast<volatile int *>(&st->coarse_off) == 0;
+  const uint16_t *const Bh = reinterpret_cast<const uint16_t *>(a.cbuf);
 
   for (int i = threadIdx.x; i < nt * 6; i += blockDim.x) s_nbr[i] = a.nbr[(int64_t)b0 * 6 + i];
   for (int i = threadIdx.x; i < nt * 1000; i += blockDim.x) s_zb[i] = 0.f;
@@ -797,8 +604,13 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   // ---- init: r0 = b, z0 = M r0, w0 = A z0; d_{-1} = s_{-1} = 0.  Per-thread
   // masks: fluid (bit j), halo (bit j), neighbour count (3 bits per j).
   unsigned fmask = 0, hmask = 0, dpack = 0;
-  unsigned spack = 0;  // coarse sub-region of the tile of each j (2 bits)
-  float rs[CK] = {0.f, 0.f, 0.f, 0.f};
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // warp partial of the tile's residual sum g_t (a barrier follows before use)
+  auto tile_partial = [&](int tl, float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) s_gw[tl * 16 + (wid & 15)] = v;
+  };
   // warm start (refined only): x64 = the dense p0 at the cell, r = b - A x64
   // in FP64 with the neighbours' p0 read from the dense array (complete and
   // read-only during the solve, so no halo exchange); the stop test stays
@@ -844,21 +656,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
     s_d[L] = 0.f;
     s_s[L] = 0.f;
     if (REF) s_x64[L] = x0;
-    if (CRS && coarse) {
-      const int sub = tl * K / nt;
-      spack |= (unsigned)sub << (2 * j);
-#pragma unroll
-      for (int r = 0; r < CK; ++r) rs[r] += sub == r ? b : 0.f;
-    }
-  }
-  if (CRS && coarse) {  // warp partials of g = P^T r0 for the block's regions
-#pragma unroll
-    for (int r = 0; r < CK; ++r) {
-      float v = rs[r];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-      if ((threadIdx.x & 31) == 0) s_gw[r][threadIdx.x >> 5] = v;
-    }
+    if (CRS && coarse) tile_partial(tl, b);
   }
   __syncthreads();
 
@@ -879,15 +677,6 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   // every solve.  A word is overwritten only after the reduction that
   // follows its reads, so no publication is missed.
   unsigned long long zep = 0;  // z publications, the same sequence in every block
-  auto warp_gsum = [&](float (&v)[CK]) {  // warp partials into s_gw (a barrier follows)
-#pragma unroll
-    for (int r = 0; r < CK; ++r) {
-      float x = v[r];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-      if ((threadIdx.x & 31) == 0) s_gw[r][threadIdx.x >> 5] = x;
-    }
-  };
   unsigned long long *const HZ = reinterpret_cast<unsigned long long *>(a.hr0);
   auto half_sweep = [&](int c) {  // z = (r + in-tile fluid neighbours' z) / D, colour c
     const int k = threadIdx.x & 255;
@@ -924,36 +713,34 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   };
   // Callers have written z = r/D on their fluid cells, zeroed the rings
   // (zero_rings, SGS only) and passed a barrier.
-  // Coarse correction: each block publishes g_I = P^T r (its fluid cells'
-  // residual sum, warp partials in s_gw) as a tagged word before the sweeps
-  // and gathers every block's after them (by then they have arrived), then
-  // adds e_I = B_I . g to its own fluid cells' z, so the halo exchange, the
-  // stencil and the dot products below all see u = z + P e.
+  // Coarse correction: each block publishes its tiles' residual sums g_t as
+  // tagged words before the sweeps and gathers all of them after (by then
+  // they have arrived) into the w array, which is free until the stencil
+  // rebuilds it; then e_t = B_t . g for its tiles (bf16 rows of B streamed
+  // from L2/L1, two or three warps per row, a fixed-order sum) is added to
+  // the z of each tile's fluid cells, so the halo exchange, the stencil and
+  // the dot products below all see u = z + P e.
   unsigned long long gep = 0;  // g publications, the same sequence in every block
   unsigned long long *const GSL =
       reinterpret_cast<unsigned long long *>(a.partials + COARSE_SLOTS_OFF);
   auto precond_exchange = [&]() {
-    if (CRS && coarse && (int)threadIdx.x < K) {  // publish g_r for the block's regions
+    if (CRS && coarse && (int)threadIdx.x < nt) {  // publish g_t for the block's tiles
       float g = 0.f;
-#pragma unroll 8
-      for (int w = 0; w < 32; ++w) g += s_gw[threadIdx.x][w];
-      st_relaxed_u64(GSL + (gep & 1ull) * CMAX + blockIdx.x * K + threadIdx.x,
+#pragma unroll
+      for (int w = 0; w < 16; ++w) g += s_gw[threadIdx.x * 16 + w];
+      st_relaxed_u64(GSL + (gep & 1ull) * CRMAX + b0 + threadIdx.x,
                      ((gep + 1ull) << 32) | __float_as_uint(g));
     }
-    // thread t < GR gathers region t's word and holds B_{I K + r, t}; the
-    // first loads are issued before the last half-sweep, so their latency
-    // hides behind the sweep; a stale word is polled again
-    const unsigned long long *gsrc = GSL + (gep & 1ull) * CMAX;
+    // thread t gathers the words of tiles t, t + 1024, t + 2048; the first
+    // loads are issued before the last half-sweep, so their latency hides
+    // behind it; a stale word is polled again
+    const unsigned long long *gsrc = GSL + (gep & 1ull) * CRMAX;
     const int t = threadIdx.x;
-    unsigned long long gpre = 0;
-    float bpre[CK] = {0.f, 0.f, 0.f, 0.f};
+    unsigned long long gpre[3] = {0ull, 0ull, 0ull};
     auto prefetch = [&]() {
-      if (t < GR) {
-        gpre = ld_relaxed_u64(gsrc + t);
 #pragma unroll
-        for (int r = 0; r < CK; ++r)
-          if (r < K) bpre[r] = __ldcg(a.cbuf + (int64_t)(blockIdx.x * K + r) * GR + t);
-      }
+      for (int k = 0; k < 3; ++k)
+        if (t + k * SM_THREADS < na) gpre[k] = ld_relaxed_u64(gsrc + t + k * SM_THREADS);
     };
     for (int sw = 0; sw < sgs; ++sw) {
       half_sweep(1);
@@ -965,46 +752,56 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
     if (CRS && coarse) {
       if (sgs == 0) prefetch();
       const unsigned long long tag = (gep + 1ull) << 32;
-      float gt = 0.f;
-      if (t < GR) {
-        unsigned long long w = gpre;
-        long long spins = 0;
-        while ((w & 0xffffffff00000000ull) != tag) {
-          w = ld_relaxed_u64(gsrc + t);
-          if ((w & 0xffffffff00000000ull) == tag) break;
-          if (++spins > SM_SPIN_LIMIT) {
-            atomicExch(&st->error, 1);
-            w = 0;
-            break;
+      float *const s_g = s_w;  // [R8]: the gathered g, zero-padded
+      const int R8 = (na + 7) & ~7;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const int sl = t + k * SM_THREADS;
+        if (sl < na) {
+          unsigned long long w = gpre[k];
+          long long spins = 0;
+          while ((w & 0xffffffff00000000ull) != tag) {
+            w = ld_relaxed_u64(gsrc + sl);
+            if ((w & 0xffffffff00000000ull) == tag) break;
+            if (++spins > SM_SPIN_LIMIT) {
+              atomicExch(&st->error, 1);
+              w = 0;
+              break;
+            }
           }
+          s_g[sl] = __uint_as_float((unsigned)w);
+        } else if (sl < R8) {
+          s_g[sl] = 0.f;
         }
-        gt = __uint_as_float((unsigned)w);
       }
       ++gep;
-      // e_r = sum_t B_{I K + r, t} g_t: warp partials, then a fixed-order sum
-#pragma unroll
-      for (int r = 0; r < CK; ++r) {
-        if (r >= K) break;
-        float v = bpre[r] * gt;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-        if ((t & 31) == 0) s_ep[r][t >> 5] = v;
-      }
       __syncthreads();
-      float e[CK] = {0.f, 0.f, 0.f, 0.f};  // every warp sums the 32 partials
-#pragma unroll
-      for (int r = 0; r < CK; ++r) {
-        if (r >= K) break;
-        float x = s_ep[r][t & 31];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-        e[r] = x;
+      // e_t = B_t . g: row b0 + jr is summed by warps jr, jr + nt, ... (the
+      // lanes over 8-column chunks), then the warps' partials in warp order
+      float v = 0.f;
+      if (nt > 0) {
+        const int jr = wid % nt, iw = wid / nt, nw = (31 - jr) / nt + 1;
+        const uint4 *row = reinterpret_cast<const uint4 *>(Bh + (int64_t)(b0 + jr) * CRMAX);
+        for (int ch = iw * 32 + lane; ch < (R8 >> 3); ch += nw * 32) {
+          const uint4 q = __ldg(row + ch);
+          const float *gp = s_g + ch * 8;
+          v += __uint_as_float(q.x << 16) * gp[0] + __uint_as_float(q.x & 0xffff0000u) * gp[1];
+          v += __uint_as_float(q.y << 16) * gp[2] + __uint_as_float(q.y & 0xffff0000u) * gp[3];
+          v += __uint_as_float(q.z << 16) * gp[4] + __uint_as_float(q.z & 0xffff0000u) * gp[5];
+          v += __uint_as_float(q.w << 16) * gp[6] + __uint_as_float(q.w & 0xffff0000u) * gp[7];
+        }
       }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (lane == 0) s_ep[wid] = v;
+      __syncthreads();
 #pragma unroll
       for (int j = 0; j < MAXJ; ++j)
         if ((fmask >> j) & 1) {
-          const int sub = (spack >> (2 * j)) & 3;
-          s_zb[(tl0 + 2 * j) * 1000 + pc] += sub == 0 ? e[0] : sub == 1 ? e[1] : sub == 2 ? e[2] : e[3];
+          const int tl = tl0 + 2 * j;
+          float e = 0.f;
+          for (int w = tl; w < 32; w += nt) e += s_ep[w];
+          s_zb[tl * 1000 + pc] += e;
         }
       __syncthreads();
     }
@@ -1068,29 +865,25 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
 
   for (int it = 0; it < a.max_iter && !done; ++it) {
     const float alphaf = (float)alpha, nalpha = -alphaf, betaf = (float)beta;
-    float rsum[CK] = {0.f, 0.f, 0.f, 0.f};  // g = P^T r of the block's regions
     // ---- own: d = z + beta d; s = w + beta s; x += alpha d; r -= alpha s; z = M r
 #pragma unroll
     for (int j = 0; j < MAXJ; ++j) {
-      if (!((fmask >> j) & 1)) continue;
       const int tl = tl0 + 2 * j, L = tl * 512 + l;
-      float *zp = s_zb + tl * 1000 + pc;
-      const float dn = *zp + betaf * s_d[L];
-      const float sn = s_w[L] + betaf * s_s[L];
-      s_d[L] = dn;
-      s_s[L] = sn;
-      s_x[L] = s_x[L] + alphaf * dn;
-      const float rn = s_r[L] + nalpha * sn;
-      s_r[L] = rn;
-      if (CRS) {
-        const int sub = (spack >> (2 * j)) & 3;
-#pragma unroll
-        for (int r = 0; r < CK; ++r) rsum[r] += sub == r ? rn : 0.f;
+      float rn = 0.f;
+      if ((fmask >> j) & 1) {
+        float *zp = s_zb + tl * 1000 + pc;
+        const float dn = *zp + betaf * s_d[L];
+        const float sn = s_w[L] + betaf * s_s[L];
+        s_d[L] = dn;
+        s_s[L] = sn;
+        s_x[L] = s_x[L] + alphaf * dn;
+        rn = s_r[L] + nalpha * sn;
+        s_r[L] = rn;
+        *zp = SGS ? rn * s_rtab[8 | ((dpack >> (3 * j)) & 7)]
+                  : rn / fmaxf((float)((dpack >> (3 * j)) & 7), 1.0f);
       }
-      *zp = SGS ? rn * s_rtab[8 | ((dpack >> (3 * j)) & 7)]
-                : rn / fmaxf((float)((dpack >> (3 * j)) & 7), 1.0f);
+      if (CRS && coarse && tl < nt) tile_partial(tl, rn);
     }
-    if (CRS && coarse) warp_gsum(rsum);
     if (SGS) zero_rings();
     __syncthreads();
     trace_mark(gs);
@@ -1147,34 +940,29 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       }
       double vr[1] = {0.0};
 #pragma unroll
-      for (int r = 0; r < CK; ++r) rsum[r] = 0.f;
-#pragma unroll
       for (int j = 0; j < MAXJ; ++j) {
-        if (!((fmask >> j) & 1)) continue;
         const int tl = tl0 + 2 * j, L = tl * 512 + l;
-        const uint16_t code = s_code[L];
-        double sum = 0.0;
+        float rf = 0.f;
+        if ((fmask >> j) & 1) {
+          const uint16_t code = s_code[L];
+          double sum = 0.0;
 #pragma unroll
-        for (int dir = 0; dir < 6; ++dir)
-          if (code & (1 << dir)) {
-            int Lnb;
-            int64_t qnb;
-            sum += nb_where(L, dir, b0, b1, s_nbr, Lnb, qnb) ? s_x64[Lnb] : __ldcg(a.x64 + qnb);
-          }
-        const double diag = (double)((code >> CODE_DIAG_SHIFT) & 7);
-        const double res = (double)(a.sign * a.bdiv[q0 + L]) - (diag * s_x64[L] - sum);
-        const float rf = (float)res;
-        s_r[L] = rf;
-        if (CRS) {
-          const int sub = (spack >> (2 * j)) & 3;
-#pragma unroll
-          for (int r = 0; r < CK; ++r) rsum[r] += sub == r ? rf : 0.f;
+          for (int dir = 0; dir < 6; ++dir)
+            if (code & (1 << dir)) {
+              int Lnb;
+              int64_t qnb;
+              sum += nb_where(L, dir, b0, b1, s_nbr, Lnb, qnb) ? s_x64[Lnb] : __ldcg(a.x64 + qnb);
+            }
+          const double diag = (double)((code >> CODE_DIAG_SHIFT) & 7);
+          const double res = (double)(a.sign * a.bdiv[q0 + L]) - (diag * s_x64[L] - sum);
+          rf = (float)res;
+          s_r[L] = rf;
+          s_zb[tl * 1000 + pc] =
+              SGS ? rf * s_rtab[8 | ((code >> CODE_DIAG_SHIFT) & 7)] : rf / diagz_of(code);
+          vr[0] += res * res;
         }
-        s_zb[tl * 1000 + pc] =
-            SGS ? rf * s_rtab[8 | ((code >> CODE_DIAG_SHIFT) & 7)] : rf / diagz_of(code);
-        vr[0] += res * res;
+        if (CRS && coarse && tl < nt) tile_partial(tl, rf);
       }
-      if (CRS && coarse) warp_gsum(rsum);
       if (SGS) zero_rings();
       double tr[1];
       if (!grid_allreduce<double, 1>(gs, vr, tr, shd)) return;
@@ -1251,6 +1039,162 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   }
 }
 
+// ---- set-up of the coarse correction (GF_FLAG_COARSE), before the solve.
+// Row t of A_c = P^T A P for active tile t (one block per tile): the
+// diagonal is the sum over the tile's fluid cells of diag - #fluid neighbours
+// inside the tile, entry (t, nbr[t][dir]) is minus the number of fluid-fluid
+// faces across face dir.  An empty tile gets a unit diagonal (it decouples).
+// Tiles beyond `limit` (more than the shared-memory solver holds) set no rows.
+__global__ void __launch_bounds__(256) k_coarse_rows(const int32_t *__restrict__ n_active,
+                                                     const int32_t *__restrict__ nbr,
+                                                     const uint16_t *__restrict__ code,
+                                                     float *__restrict__ cdiag,
+                                                     float *__restrict__ coff, int limit) {
+  const int na = *n_active;
+  const int s = blockIdx.x;
+  if (na > limit || na > CRMAX || s >= na) return;
+  float v[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // diagonal, then faces 0..5
+  for (int L = threadIdx.x; L < 512; L += blockDim.x) {
+    const uint16_t cd = code[(int64_t)s * 512 + L];
+    if (!(cd & CODE_FLUID)) continue;
+    const int li = L >> 6, lj = (L >> 3) & 7, lk = L & 7;
+    int same = 0;
+#pragma unroll
+    for (int dir = 0; dir < 6; ++dir) {
+      if (!(cd & (1 << dir))) continue;
+      const bool inside = dir == 0 ? li > 0 : dir == 1 ? li < 7 : dir == 2 ? lj > 0
+                        : dir == 3 ? lj < 7 : dir == 4 ? lk > 0 : lk < 7;
+      if (inside) ++same; else v[1 + dir] += 1.f;
+    }
+    v[0] += (float)((int)((cd >> CODE_DIAG_SHIFT) & 7) - same);
+  }
+  __shared__ float red[8][7];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 7; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    if (lane == 0) red[wid][k] = v[k];
+  }
+  __syncthreads();
+  if (threadIdx.x < 7) {
+    float t = 0.f;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w][threadIdx.x];
+    if (threadIdx.x == 0) {
+      cdiag[s] = t > 0.f ? t : 1.0f;
+    } else {
+      const int dir = threadIdx.x - 1;
+      coff[(int64_t)s * 6 + dir] = nbr[(int64_t)s * 6 + dir] >= 0 ? -t : 0.f;
+    }
+  }
+}
+
+// Row r of B = A_c^-1 (one block per active tile r): A_c x = e_r by
+// Jacobi-preconditioned CG in float32 to ||e_r - A_c x|| <= 1e-3 (B only has
+// to be close to the inverse for the correction to work), the vectors in
+// shared memory, the rows of A_c read through the cache.  Written as bfloat16
+// with row stride CRMAX, zero up to the next multiple of 8 columns.  A solve
+// that fails (no convergence, a non-finite value) switches the correction
+// off for the coming solve.
+constexpr int COARSE_SOLVE_THREADS = 256;
+__global__ void __launch_bounds__(COARSE_SOLVE_THREADS)
+    k_coarse_solve(const int32_t *__restrict__ n_active, const int32_t *__restrict__ nbr,
+                   const float *__restrict__ cdiag, const float *__restrict__ coff,
+                   uint16_t *__restrict__ bh, PcgState *st, int limit) {
+  extern __shared__ float cs[];  // x, r, p, q: [4][na]
+  const int na = *n_active;
+  const int rr0 = blockIdx.x;
+  if (na > limit || na > CRMAX || rr0 >= na) return;
+  float *cx = cs, *cr = cs + na, *cp = cr + na, *cq = cp + na;
+  __shared__ float red[COARSE_SOLVE_THREADS / 32][2];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  auto bsum = [&](float a0, float a1, float &o0, float &o1) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+      a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+    }
+    if (lane == 0) {
+      red[wid][0] = a0;
+      red[wid][1] = a1;
+    }
+    __syncthreads();
+    float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+    for (int w = 0; w < COARSE_SOLVE_THREADS / 32; ++w) {
+      s0 += red[w][0];
+      s1 += red[w][1];
+    }
+    __syncthreads();
+    o0 = s0;
+    o1 = s1;
+  };
+  auto matvec = [&](const float *x, int i) {
+    float acc = __ldg(cdiag + i) * x[i];
+#pragma unroll
+    for (int dir = 0; dir < 6; ++dir) {
+      const int j = __ldg(nbr + (int64_t)i * 6 + dir);
+      if (j >= 0 && j < na) acc += __ldg(coff + (int64_t)i * 6 + dir) * x[j];
+    }
+    return acc;
+  };
+  float rz = 0.f, rn2 = 0.f;
+  {
+    float a0 = 0.f, a1 = 0.f;
+    for (int i = threadIdx.x; i < na; i += blockDim.x) {
+      const float b = i == rr0 ? 1.f : 0.f;
+      cx[i] = 0.f;
+      cr[i] = b;
+      cp[i] = b / __ldg(cdiag + i);
+      a0 += b * cp[i];
+      a1 += b * b;
+    }
+    bsum(a0, a1, rz, rn2);
+  }
+  bool ok = false;
+  for (int it = 0; it < 1000; ++it) {
+    float pq, dummy;
+    {
+      float a0 = 0.f;
+      for (int i = threadIdx.x; i < na; i += blockDim.x) {
+        const float v = matvec(cp, i);
+        cq[i] = v;
+        a0 += cp[i] * v;
+      }
+      bsum(a0, 0.f, pq, dummy);
+    }
+    if (!(pq > 0.f)) break;
+    const float al = rz / pq;
+    float a0 = 0.f, a1 = 0.f;
+    for (int i = threadIdx.x; i < na; i += blockDim.x) {
+      cx[i] += al * cp[i];
+      const float rn = cr[i] - al * cq[i];
+      cr[i] = rn;
+      a0 += rn * rn;
+      a1 += rn * rn / __ldg(cdiag + i);
+    }
+    float rz2;
+    bsum(a0, a1, rn2, rz2);
+    if (rn2 <= kCoarseTol2) {
+      ok = true;
+      break;
+    }
+    const float be = rz2 / rz;
+    rz = rz2;
+    for (int i = threadIdx.x; i < na; i += blockDim.x) cp[i] = cr[i] / __ldg(cdiag + i) + be * cp[i];
+    __syncthreads();
+  }
+  bool finite = true;
+  uint16_t *out = bh + (int64_t)rr0 * CRMAX;
+  const int R8 = (na + 7) & ~7;
+  for (int i = threadIdx.x; i < R8; i += blockDim.x) {
+    const float x = i < na ? cx[i] : 0.f;
+    finite &= isfinite(x);
+    out[i] = __bfloat16_as_ushort(__float2bfloat16_rn(x));
+  }
+  if ((threadIdx.x == 0 && !ok) || !finite) atomicExch(&st->coarse_off, 1);
+}
+
 template <typename Acc, bool REF>
 static bool fits_t(Ctx *c) {
   int optin = 0;
@@ -1285,6 +1229,17 @@ static int launch_t(Ctx *c, PcgSmemArgs &a) {
                  "PCG occupancy");
   if (e) return e;
   if (per_sm < 1) return fail(c, GF_CUDA_ERROR, "PCG shared-memory kernel does not fit an SM");
+  if (a.coarse && a.cbuf) {  // rows of A_c, then of B = A_c^-1, for the active tiles
+    const int limit = c->num_sms * SmemCfg<REF>::MAXT;
+    float *cdiag = reinterpret_cast<float *>(a.cbuf + COARSE_B_BYTES);
+    float *coff = cdiag + CRMAX;
+    k_coarse_rows<<<CRMAX, 256, 0, c->stream>>>(a.n_active, a.nbr, a.code, cdiag, coff, limit);
+    const size_t vec = (size_t)4 * CRMAX * sizeof(float);
+    k_coarse_solve<<<CRMAX, COARSE_SOLVE_THREADS, vec, c->stream>>>(
+        a.n_active, a.nbr, cdiag, coff, reinterpret_cast<uint16_t *>(a.cbuf), a.st, limit);
+    c->launches += 2;
+    if ((e = check_launch(c, "coarse correction set-up"))) return e;
+  }
   void *args[] = {&a};
   e = check_cuda(c, cudaLaunchCooperativeKernel((const void *)fn, dim3(c->num_sms),
                                                 dim3(SM_THREADS), args, smem, c->stream),

@@ -1528,11 +1528,7 @@ int pressure_alloc(Ctx *c) {
   if ((e = A((void **)&c->halo, nk * 6 * 4, "alloc halo buffers"))) return e;
   // coarse operator and its inverse (GF_FLAG_COARSE), allocated up front so
   // that solves can be captured in CUDA graphs
-  if ((e = A((void **)&c->coarse_buf, (size_t)COARSE_BUF_FLOATS * 4, "alloc coarse operator")))
-    return e;
-  // the solves warm-start from the previous inverse rows: zero the first
-  if ((e = check_cuda(c, cudaMemset(c->coarse_buf, 0, (size_t)COARSE_BUF_FLOATS * 4),
-                      "zero coarse operator")))
+  if ((e = A((void **)&c->coarse_buf, (size_t)COARSE_BUF_BYTES, "alloc coarse operator")))
     return e;
   if ((e = A((void **)&c->tile_cost, (size_t)c->ntiles * 4, "alloc tile cost"))) return e;
   if ((e = A((void **)&c->health, 8 * 4, "alloc solve health"))) return e;
@@ -1764,9 +1760,9 @@ int launch_pressure(Ctx *c, const gf_step_params *prm) {
         return e;
       // the one-round-trip reduction words of the shared-memory solver
       // ([2][160][4] u64 at 2048 doubles into the partials buffer), then the
-      // tagged coarse sums ([2][640] u64)
+      // tagged coarse sums ([2][COARSE_RMAX] u64)
       if ((e = check_cuda(c, cudaMemsetAsync(c->partials + 2048, 0,
-                                             (2 * 160 * 4 + 2 * COARSE_MAXG * COARSE_K) * 8, st),
+                                             (2 * 160 * 4 + 2 * COARSE_RMAX) * 8, st),
                           "zero reduction words")))
         return e;
       const bool coarse = (prm->flags & GF_FLAG_COARSE) != 0;
@@ -1778,7 +1774,7 @@ int launch_pressure(Ctx *c, const gf_step_params *prm) {
                      (prm->flags & GF_FLAG_TRACE) ? c->trace : nullptr, TRACE_CAP,
                      prm->max_iters, check_every, prm->tol * prm->tol, replace2, sign,
                      (prm->flags & GF_FLAG_SGS_MASK) >> GF_FLAG_SGS_SHIFT,
-                     coarse ? COARSE_K : 0, c->coarse_buf,
+                     coarse ? 1 : 0, c->coarse_buf,
                      (prm->flags & GF_FLAG_TEST_STALL) ? 1 : 0,
                      (refined && (prm->flags & GF_FLAG_WARM_START)) ? 1 : 0, c->f.p,
                      c->tile_list, c->ny, c->nz, c->nty, c->ntz};

@@ -24,8 +24,8 @@ default path):
   1-3) on each 8^3 pressure tile with its neighbours held at zero.  Same
   operator and stop test, about half the iterations.
 * ``pcg_coarse=True`` (new): adds a coarse correction to the shared-memory
-  PCG's preconditioner -- one constant per region, four regions of tiles per
-  solver block -- for fewer iterations again.
+  PCG's preconditioner -- one constant per active 8^3 tile -- for fewer
+  iterations again.
 * ``pcg_warm_start=True`` (new): the refined PCG (either kernel) starts from
   the previous substep's pressure instead of zero (the reference's solves
   start from zero); the stop test stays relative to ||b||.

@@ -104,10 +104,11 @@ typedef struct gf_step_params {
 #define GF_FLAG_SGS_SHIFT 2
 #define GF_FLAG_SGS_MASK 12
 /* flags: add a coarse correction to the shared-memory PCG's preconditioner
- * (no counterpart in the reference): one constant per region (four regions
- * of tiles per solver block), B ~ (P^T A P)^-1 solved at the start of every
- * solve, M^-1 = M_tile^-1 + P B P^T.  Same operator, stop test and answer;
- * fewer iterations.  The global-memory kernel ignores it. */
+ * (no counterpart in the reference): one constant per active 8^3 tile, the
+ * rows of B ~ (P^T A P)^-1 computed (to 1e-3, stored as bfloat16) by two
+ * kernels before every solve, M^-1 = M_tile^-1 + P B P^T.  Same operator,
+ * stop test and answer; fewer iterations.  The global-memory kernel ignores
+ * it. */
 #define GF_FLAG_COARSE 16
 /* flags, test only: the shared-memory PCG's first grid reduction waits for a
  * publication count that no block writes, with a spin limit of 4096 polls
