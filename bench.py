@@ -324,27 +324,23 @@ def fp64_error_leg(torch, s, snap0, steps=120, every=20):
             "checks": rows, "wall_s": round(time.perf_counter() - t0, 1)}
 
 
-def pcg_bytes(st, sgs_sweeps=0, coarse=False) -> float:
-    """Algorithmic bytes of one PCG launch: per fluid cell 14 B of set-up,
-    48 B per iteration (phase A: z, d_old, code in; d_new, Ad out; phase B:
-    d_new, Ad, x, r, code in; x, r, z out), 48 B per FP64 residual
-    replacement (x64, x, code, b in; x64, x, r, z out); 2 B of stencil code
-    per active-tile cell and per phase.  A tile-local symmetric Gauss-Seidel
-    preconditioner adds 12 B per fluid cell per sweep (each half-sweep reads
-    r and writes z on its colour and reads z of the other); the coarse
-    correction adds 8 B per fluid cell per iteration (z read, z + e written)
-    and 2 B of stencil code per active-tile cell for assembling P^T A P."""
-    nf, na = st["n_fluid"], st["n_active_tiles"] * 512
-    it, rep = st["iters"], st["replacements"]
-    per_it = 48 + 12 * sgs_sweeps + (8 if coarse else 0)
-    return float(nf * (14 + per_it * it + 48 * rep) + na * 2 * (1 + 2 * it + (1 if coarse else 0)))
+def pcg_bytes(st) -> float:
+    """Algorithmic bytes of one PCG launch in the survey's accounting, over
+    the cells the solver processes (N = active tiles x 512): 13 N of set-up,
+    47 N per iteration (SpMV and p.Ap; x, r update and r.z; p update) and
+    25 N per FP64 residual replacement.  The preconditioner's own traffic
+    (tile sweeps, coarse correction) is not counted."""
+    N = st["n_active_tiles"] * 512
+    return float(N * (13 + 47 * st["iters"] + 25 * st["replacements"]))
 
 
 def stage_bytes(P, nf, ncell_active, F):
-    """Algorithmic bytes of the other APIC stages at these sizes."""
-    return {"bin_sort": 136 * P + 12 * ncell_active, "p2g": 60 * P + 24 * F,
-            "forces_div": 8 * F + 5 * ncell_active, "project": 8 * F + 5 * ncell_active,
-            "g2p": 12 * P + 4 * F + 64 * P}
+    """Algorithmic bytes of the other APIC stages at these sizes, in the
+    survey's accounting (N = cells the stage processes): sort 136P + 12N,
+    P2G 60P + 4F + 2N, forces/div 8F + 5N, project 8F + 5N, G2P 72P + 4F."""
+    N = ncell_active
+    return {"bin_sort": 136 * P + 12 * N, "p2g": 60 * P + 4 * F + 2 * N,
+            "forces_div": 8 * F + 5 * N, "project": 8 * F + 5 * N, "g2p": 72 * P + 4 * F}
 
 
 # ------------------------------------------------------------- timed loops
@@ -668,11 +664,11 @@ def mesh_leg(torch, s, snap, hbm, reps=5):
 
 
 def stage_bytes_flip(P, ncell_active, F):
-    """Algorithmic bytes of the FLIP (non-APIC) stages: sort 64P + 12N,
-    P2G 24P + 24F (the zeroing of the six P2G face arrays counted as for
-    APIC), forces/div 8F + 5N, project 8F + 5N, G2P 48P + 8F."""
+    """Algorithmic bytes of the FLIP (non-APIC) stages in the survey's
+    accounting: sort 64P + 12N, P2G 24P + 4F + 2N, forces/div 8F + 5N,
+    project 8F + 5N, G2P 48P + 8F."""
     N = ncell_active
-    return {"bin_sort": 64 * P + 12 * N, "p2g": 24 * P + 24 * F,
+    return {"bin_sort": 64 * P + 12 * N, "p2g": 24 * P + 4 * F + 2 * N,
             "forces_div": 8 * F + 5 * N, "project": 8 * F + 5 * N, "g2p": 48 * P + 8 * F}
 
 
@@ -868,7 +864,7 @@ def run_ours(args):
         st = s.pressure_stats()
         stage.append(t)
         pcg_ms.append(t[7])
-        pcg_b.append(pcg_bytes(st, SGS_SWEEPS, COARSE))
+        pcg_b.append(pcg_bytes(st))
     s._L.gf_enable_timing(s._ctx, 0)
     s._prof.enabled = False
     stage_ms = np.mean(np.array(stage), axis=0)
