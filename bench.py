@@ -65,11 +65,11 @@ MAX_ITERS = 4000
 SPHERE = ((0.7, 0.2, 0.5), 0.12)
 BOX = ((0.0, 0.0, 0.0), (0.4, 0.6, 1.0))
 SGS_SWEEPS = 2  # tile-local symmetric Gauss-Seidel sweeps of the headline solve
-COARSE = True   # plus the block-region coarse correction
+COARSE = True   # plus the tile coarse correction (one region per active tile)
 WARM_START = True  # each refined solve starts from the previous substep's pressure
 WORKLOAD = ("APIC dam break + sphere obstacle, 128^3 (dx=1/128), 8 ppc -> 3,969,024 "
             "particles, dt=1/480, pressure: FP32 PCG + FP64 residual replacement to 1e-8, "
-            "tile-local symmetric Gauss-Seidel preconditioner (2 sweeps) + block-region "
+            "tile-local symmetric Gauss-Seidel preconditioner (2 sweeps) + tile "
             "coarse correction, each solve started from the previous substep's pressure "
             "(stop test ||b - Ap|| <= 1e-8 ||b|| as from zero)")
 
@@ -934,7 +934,7 @@ def run_ours(args):
             "config": {"workload": WORKLOAD, "grid": GRID, "particles": P, "transfer": "apic",
                        "dt": DT, "pressure": "pcg_refined", "tol": TOL,
                        "preconditioner": f"tile-local symmetric Gauss-Seidel, {SGS_SWEEPS} sweeps"
-                                         + (", block-region coarse correction" if COARSE else ""),
+                                         + (", tile coarse correction" if COARSE else ""),
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2_policy": "inputs larger than L2: particle state "
                                     f"{P * 64 / 1e6:.0f} MB + MAC grids {F * 4 * 3 / 1e6:.0f} MB "

@@ -65,7 +65,7 @@ class StepParams(ctypes.Structure):
 GF_FLAG_GLOBAL_PCG = 1
 GF_FLAG_TRACE = 2
 GF_FLAG_SGS_SHIFT = 2  # bits 2-3: tile-local symmetric Gauss-Seidel sweeps
-GF_FLAG_COARSE = 16    # block-region coarse correction of the shared-memory PCG
+GF_FLAG_COARSE = 16    # tile coarse correction of the shared-memory PCG
 GF_FLAG_TEST_STALL = 64  # test only: the first grid reduction of the PCG runs out its wait
 GF_FLAG_WARM_START = 128  # refined PCG starts from the previous pressure
 GF_NOALLOC_MAX_CELLS = 2097152

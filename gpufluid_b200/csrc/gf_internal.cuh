@@ -35,11 +35,23 @@ constexpr int COARSE_MAXG = 160;  // blocks of the shared-memory PCG, at most
 // aligned
 constexpr int COARSE_RMAX = COARSE_MAXG * 14;
 static_assert(COARSE_RMAX % 8 == 0, "coarse row stride");
-// coarse buffer: rows of B = (P^T A P)^-1 as bf16 [RMAX][RMAX], then the rows
-// of P^T A P: diagonal [RMAX] and the six face-neighbour entries [RMAX][6]
-// (floats)
+// coarse buffer: two sets of rows of B = (P^T A P)^-1 as bf16 [RMAX][RMAX]
+// (the last solve's and the next), then the rows of P^T A P: diagonal [RMAX]
+// and the six face-neighbour entries [RMAX][6] (floats), the tile of each row
+// of the last B [RMAX] (ints), and CoarseMeta.  The meta and the tile-to-row
+// map of the last B (Ctx::coarse_prev_slot) persist from solve to solve; the
+// device keeps them, so CUDA-graph replays stay consistent.
 constexpr int64_t COARSE_B_BYTES = (int64_t)COARSE_RMAX * COARSE_RMAX * 2;
-constexpr int64_t COARSE_BUF_BYTES = COARSE_B_BYTES + (int64_t)COARSE_RMAX * 7 * 4;
+struct CoarseMeta {
+  int parity;   // which B set holds the last solve's rows
+  int prev_na;  // rows of that B (0: none yet)
+  int pad[2];
+};
+constexpr int64_t COARSE_DIAG_OFF = 2 * COARSE_B_BYTES;
+constexpr int64_t COARSE_OFF_OFF = COARSE_DIAG_OFF + (int64_t)COARSE_RMAX * 4;
+constexpr int64_t COARSE_LIST_OFF = COARSE_OFF_OFF + (int64_t)COARSE_RMAX * 6 * 4;
+constexpr int64_t COARSE_META_OFF = COARSE_LIST_OFF + (int64_t)COARSE_RMAX * 4;
+constexpr int64_t COARSE_BUF_BYTES = COARSE_META_OFF + (int64_t)sizeof(CoarseMeta);
 constexpr int TRACE_CAP = 4096;
 
 // Stencil code bits (per compact cell).
@@ -197,6 +209,7 @@ struct Ctx {
   unsigned long long *bar_counters = nullptr;  // 8 lines x 16 u64
   float *halo = nullptr;         // [6 * nkeys] halo publication buffers
   unsigned char *coarse_buf = nullptr;  // [COARSE_BUF_BYTES] coarse operator and inverse rows
+  int32_t *coarse_prev_slot = nullptr;  // [ntiles] row of each tile in the last B, or -1
   int32_t *tile_cost = nullptr;  // [ntiles] per-slot PCG work estimate
   long long *trace = nullptr;    // [TRACE_CAP] PCG phase timestamps
   bool trace_on = false;

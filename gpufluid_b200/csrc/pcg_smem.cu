@@ -554,10 +554,15 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   // the indicator of each tile's fluid cells, and the preconditioner
   // M^-1 = M_tile^-1 + P B P^T (additive two-level) with B = (P^T A P)^-1,
   // whose rows k_coarse_rows / k_coarse_solve computed before this launch (as
-  // bfloat16).  A failed row solve switched the correction off for the solve.
+  // bfloat16; the set CoarseMeta::parity names).  A failed row solve switched
+  // the correction off for the solve.
   const bool coarse = CRS && a.coarse && a.cbuf != nullptr &&
                       *reinterpret_cast<volatile int *>(&st->coarse_off) == 0;
-  const uint16_t *const Bh = reinterpret_cast<const uint16_t *>(a.cbuf);
+  const uint16_t *const Bh =
+      coarse ? reinterpret_cast<const uint16_t *>(a.cbuf) +
+                   (int64_t)reinterpret_cast<const CoarseMeta *>(a.cbuf + COARSE_META_OFF)->parity *
+                       CRMAX * CRMAX
+             : nullptr;
 
   for (int i = threadIdx.x; i < nt * 6; i += blockDim.x) s_nbr[i] = a.nbr[(int64_t)b0 * 6 + i];
   for (int i = threadIdx.x; i < nt * 1000; i += blockDim.x) s_zb[i] = 0.f;
@@ -742,6 +747,14 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       for (int k = 0; k < 3; ++k)
         if (t + k * SM_THREADS < na) gpre[k] = ld_relaxed_u64(gsrc + t + k * SM_THREADS);
     };
+#ifdef GF_COARSE_PREFETCH
+    if (CRS && coarse && nt > 0) {  // B rows of the apply below into L1
+      const int jr = wid % nt, iw = wid / nt, nw = (31 - jr) / nt + 1;
+      const uint4 *row = reinterpret_cast<const uint4 *>(Bh + (int64_t)(b0 + jr) * CRMAX);
+      for (int ch = iw * 32 + lane; ch < ((na + 7) >> 3); ch += nw * 32)
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(row + ch));
+    }
+#endif
     for (int sw = 0; sw < sgs; ++sw) {
       half_sweep(1);
       __syncthreads();
@@ -1092,19 +1105,32 @@ __global__ void __launch_bounds__(256) k_coarse_rows(const int32_t *__restrict__
 // Row r of B = A_c^-1 (one block per active tile r): A_c x = e_r by
 // Jacobi-preconditioned CG in float32 to ||e_r - A_c x|| <= 1e-3 (B only has
 // to be close to the inverse for the correction to work), the vectors in
-// shared memory, the rows of A_c read through the cache.  Written as bfloat16
-// with row stride CRMAX, zero up to the next multiple of 8 columns.  A solve
-// that fails (no convergence, a non-finite value) switches the correction
-// off for the coming solve.
+// shared memory, the rows of A_c read through the cache.  The solve starts
+// from the last solve's row of the same tile, its columns mapped by tile
+// (zero for tiles that had no row): the fluid moves little from one substep
+// to the next, and a few CG steps instead of ~35 meet the target.  Written as
+// bfloat16 with row stride CRMAX, zero up to the next multiple of 8 columns,
+// into the B set the last solve did not use.  A solve that fails (no
+// convergence, a non-finite value) switches the correction off for the
+// coming solve.
 constexpr int COARSE_SOLVE_THREADS = 256;
+__device__ __forceinline__ float bf16_at(const uint16_t *p, int64_t i) {
+  return __uint_as_float((unsigned)p[i] << 16);
+}
 __global__ void __launch_bounds__(COARSE_SOLVE_THREADS)
-    k_coarse_solve(const int32_t *__restrict__ n_active, const int32_t *__restrict__ nbr,
-                   const float *__restrict__ cdiag, const float *__restrict__ coff,
-                   uint16_t *__restrict__ bh, PcgState *st, int limit) {
+    k_coarse_solve(const int32_t *__restrict__ n_active, const int32_t *__restrict__ tile_list,
+                   const int32_t *__restrict__ nbr, const float *__restrict__ cdiag,
+                   const float *__restrict__ coff, uint16_t *__restrict__ bsets,
+                   const int32_t *__restrict__ prev_slot, const CoarseMeta *meta, PcgState *st,
+                   int limit) {
   extern __shared__ float cs[];  // x, r, p, q: [4][na]
   const int na = *n_active;
   const int rr0 = blockIdx.x;
   if (na > limit || na > CRMAX || rr0 >= na) return;
+  const int par = meta->parity;
+  const uint16_t *bprev = bsets + (int64_t)par * CRMAX * CRMAX;
+  uint16_t *bh = bsets + (int64_t)(par ^ 1) * CRMAX * CRMAX;
+  const int pr = meta->prev_na > 0 ? prev_slot[tile_list[rr0]] : -1;
   float *cx = cs, *cr = cs + na, *cp = cr + na, *cq = cp + na;
   __shared__ float red[COARSE_SOLVE_THREADS / 32][2];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -1138,12 +1164,20 @@ __global__ void __launch_bounds__(COARSE_SOLVE_THREADS)
     }
     return acc;
   };
+  for (int i = threadIdx.x; i < na; i += blockDim.x) {  // the warm start
+    float x0 = 0.f;
+    if (pr >= 0) {
+      const int pc = prev_slot[tile_list[i]];
+      if (pc >= 0) x0 = bf16_at(bprev, (int64_t)pr * CRMAX + pc);
+    }
+    cx[i] = isfinite(x0) ? x0 : 0.f;
+  }
+  __syncthreads();
   float rz = 0.f, rn2 = 0.f;
   {
     float a0 = 0.f, a1 = 0.f;
     for (int i = threadIdx.x; i < na; i += blockDim.x) {
-      const float b = i == rr0 ? 1.f : 0.f;
-      cx[i] = 0.f;
+      const float b = (i == rr0 ? 1.f : 0.f) - matvec(cx, i);
       cr[i] = b;
       cp[i] = b / __ldg(cdiag + i);
       a0 += b * cp[i];
@@ -1151,8 +1185,8 @@ __global__ void __launch_bounds__(COARSE_SOLVE_THREADS)
     }
     bsum(a0, a1, rz, rn2);
   }
-  bool ok = false;
-  for (int it = 0; it < 1000; ++it) {
+  bool ok = rn2 <= kCoarseTol2;
+  for (int it = 0; it < 1000 && !ok; ++it) {
     float pq, dummy;
     {
       float a0 = 0.f;
@@ -1195,6 +1229,37 @@ __global__ void __launch_bounds__(COARSE_SOLVE_THREADS)
   if ((threadIdx.x == 0 && !ok) || !finite) atomicExch(&st->coarse_off, 1);
 }
 
+// After the row solves: the tile-to-row map and the row tiles describe the
+// new B, and the parity names its set.  First the last B's tiles lose their
+// rows, then the new ones get theirs (two launches, so that no block clears
+// an entry another has already set).
+__global__ void k_coarse_commit_clear(const int32_t *__restrict__ n_active,
+                                      const int32_t *__restrict__ prev_list,
+                                      int32_t *__restrict__ prev_slot, const CoarseMeta *meta,
+                                      int limit) {
+  const int na = *n_active;
+  if (na > limit || na > CRMAX) return;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < meta->prev_na;
+       s += gridDim.x * blockDim.x)
+    prev_slot[prev_list[s]] = -1;
+}
+__global__ void k_coarse_commit_set(const int32_t *__restrict__ n_active,
+                                    const int32_t *__restrict__ tile_list,
+                                    int32_t *__restrict__ prev_list,
+                                    int32_t *__restrict__ prev_slot, CoarseMeta *meta, int limit) {
+  const int na = *n_active;
+  if (na > limit || na > CRMAX) return;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < na; s += gridDim.x * blockDim.x) {
+    const int t = tile_list[s];
+    prev_slot[t] = s;
+    prev_list[s] = t;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    meta->prev_na = na;
+    meta->parity ^= 1;
+  }
+}
+
 template <typename Acc, bool REF>
 static bool fits_t(Ctx *c) {
   int optin = 0;
@@ -1231,13 +1296,21 @@ static int launch_t(Ctx *c, PcgSmemArgs &a) {
   if (per_sm < 1) return fail(c, GF_CUDA_ERROR, "PCG shared-memory kernel does not fit an SM");
   if (a.coarse && a.cbuf) {  // rows of A_c, then of B = A_c^-1, for the active tiles
     const int limit = c->num_sms * SmemCfg<REF>::MAXT;
-    float *cdiag = reinterpret_cast<float *>(a.cbuf + COARSE_B_BYTES);
-    float *coff = cdiag + CRMAX;
+    float *cdiag = reinterpret_cast<float *>(a.cbuf + COARSE_DIAG_OFF);
+    float *coff = reinterpret_cast<float *>(a.cbuf + COARSE_OFF_OFF);
+    int32_t *plist = reinterpret_cast<int32_t *>(a.cbuf + COARSE_LIST_OFF);
+    CoarseMeta *meta = reinterpret_cast<CoarseMeta *>(a.cbuf + COARSE_META_OFF);
     k_coarse_rows<<<CRMAX, 256, 0, c->stream>>>(a.n_active, a.nbr, a.code, cdiag, coff, limit);
     const size_t vec = (size_t)4 * CRMAX * sizeof(float);
     k_coarse_solve<<<CRMAX, COARSE_SOLVE_THREADS, vec, c->stream>>>(
-        a.n_active, a.nbr, cdiag, coff, reinterpret_cast<uint16_t *>(a.cbuf), a.st, limit);
-    c->launches += 2;
+        a.n_active, a.tile_list, a.nbr, cdiag, coff, reinterpret_cast<uint16_t *>(a.cbuf),
+        c->coarse_prev_slot, meta, a.st, limit);
+    k_coarse_commit_clear<<<(CRMAX + 255) / 256, 256, 0, c->stream>>>(a.n_active, plist,
+                                                                    c->coarse_prev_slot, meta,
+                                                                    limit);
+    k_coarse_commit_set<<<(CRMAX + 255) / 256, 256, 0, c->stream>>>(
+        a.n_active, a.tile_list, plist, c->coarse_prev_slot, meta, limit);
+    c->launches += 4;
     if ((e = check_launch(c, "coarse correction set-up"))) return e;
   }
   void *args[] = {&a};

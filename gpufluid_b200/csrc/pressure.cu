@@ -1530,6 +1530,14 @@ int pressure_alloc(Ctx *c) {
   // that solves can be captured in CUDA graphs
   if ((e = A((void **)&c->coarse_buf, (size_t)COARSE_BUF_BYTES, "alloc coarse operator")))
     return e;
+  if ((e = A((void **)&c->coarse_prev_slot, (size_t)c->ntiles * 4, "alloc coarse row map")))
+    return e;
+  // no B yet: meta zero, no tile has a row
+  if ((e = check_cuda(c, cudaMemset(c->coarse_buf + COARSE_META_OFF, 0, sizeof(CoarseMeta)),
+                      "zero coarse meta")) ||
+      (e = check_cuda(c, cudaMemset(c->coarse_prev_slot, 0xff, (size_t)c->ntiles * 4),
+                      "clear coarse row map")))
+    return e;
   if ((e = A((void **)&c->tile_cost, (size_t)c->ntiles * 4, "alloc tile cost"))) return e;
   if ((e = A((void **)&c->health, 8 * 4, "alloc solve health"))) return e;
   if ((e = check_cuda(c, cudaMemset(c->health, 0, 8 * 4), "zero solve health"))) return e;
@@ -1545,7 +1553,7 @@ void pressure_free(Ctx *c) {
   void *ps[] = {c->tile_slot, c->tile_list, c->tile_order, c->tile_nbr, c->n_active, c->code, c->bdiv,
                 c->xf, c->r, c->z, c->d0, c->d1, c->Ad, c->x64, c->partials, c->state,
                 c->bar_counters, c->trace, c->halo, c->tile_cost, c->coarse_buf,
-                c->health};
+                c->coarse_prev_slot, c->health};
   for (void *p : ps)
     if (p) cudaFree(p);
   if (c->state_host) cudaFreeHost(c->state_host);
