@@ -22,8 +22,10 @@
 namespace gf {
 
 struct AdjArgs {
-  const float4 *rec0, *rec1;  // sorted inputs of the substep: (x,y,z,pid), (vx,vy,vz,C00)
-  const float4 *rec2, *rec3;  // APIC: (C01,C02,C10,C11), (C12,C20,C21,C22)
+  // sorted inputs of the substep: (x,y,z,pid), then FLIP/PIC (vx,vy,vz,-),
+  // APIC one record per component c: (v_c, C row c) in rec1, rec2, rec3
+  const float4 *rec0, *rec1;
+  const float4 *rec2, *rec3;
   const float *Cbar_out;      // APIC: (n,9) adjoint of the output C, sorted order
   float *Cbar_in;             // APIC: (n,9) adjoint of the input C, storage order
   const int32_t *order;       // storage slot (input order) of each sorted position
@@ -410,8 +412,8 @@ __global__ void k_adj_g2p_apic(AdjArgs a) {
 
 __device__ __forceinline__ void adj_p2g_apic_item(const AdjArgs &a, int64_t q) {
   const float4 r0 = a.rec0[q], r1 = a.rec1[q], r2 = a.rec2[q], r3 = a.rec3[q];
-  const float vel[3] = {r1.x, r1.y, r1.z};
-  const float C[3][3] = {{r1.w, r2.x, r2.y}, {r2.z, r2.w, r3.x}, {r3.y, r3.z, r3.w}};
+  const float vel[3] = {r1.x, r2.x, r3.x};
+  const float C[3][3] = {{r1.y, r1.z, r1.w}, {r2.y, r2.z, r2.w}, {r3.y, r3.z, r3.w}};
   const float p[3] = {r0.x, r0.y, r0.z};
   const float dx = a.dx, inv_dx = 1.0f / dx;
   const float g[3] = {__fdiv_rn(p[0], dx), __fdiv_rn(p[1], dx), __fdiv_rn(p[2], dx)};

@@ -254,11 +254,11 @@ __global__ void k_permute(const int32_t *__restrict__ order, int64_t n,
   b.y = vel[3 * s + 1];
   b.z = vel[3 * s + 2];
   b.w = 0.f;
-  if (C) {
+  if (C) {  // APIC: one record per face component c, (v_c, C row c)
     const float *m = C + 9 * s;
-    b.w = m[0];
-    rec2[d] = make_float4(m[1], m[2], m[3], m[4]);
-    rec3[d] = make_float4(m[5], m[6], m[7], m[8]);
+    rec2[d] = make_float4(b.y, m[3], m[4], m[5]);
+    rec3[d] = make_float4(b.z, m[6], m[7], m[8]);
+    b = make_float4(b.x, m[0], m[1], m[2]);
   }
   rec0[d] = a;
   rec1[d] = b;

@@ -7,8 +7,10 @@
 //    reference's int32 marker;
 //  * particles in the caller's (n,3) AoS buffers hold the state between
 //    substeps; inside a substep they are read from four float4 streams,
-//    sorted by cell:  rec0 = (x, y, z, pid-as-bits)  rec1 = (vx, vy, vz, C00)
-//    rec2 = (C01, C02, C10, C11)  rec3 = (C12, C20, C21, C22)
+//    sorted by cell:  rec0 = (x, y, z, pid-as-bits); FLIP/PIC rec1 = (vx, vy,
+//    vz, 0); APIC one record per face component c: rec1 = (vx, C00, C01, C02),
+//    rec2 = (vy, C10, C11, C12), rec3 = (vz, C20, C21, C22), so that a
+//    component's scatter reads two records
 //    (FLIP/PIC use rec0, rec1 only);
 //  * the pressure solve works on a compact array of active 8x8x8 tiles:
 //    element (slot*512 + ((li*8 + lj)*8 + lk)) is cell (8*ti+li, 8*tj+lj,

@@ -233,26 +233,13 @@ __device__ __forceinline__ void p2g_cell_comp(const P2GArgs &a, T *s_val, T *s_w
     const int64_t q = first + kp;
     const float4 r0 = a.rec0[q];
     float vp, c0 = 0.f, c1 = 0.f, c2 = 0.f;
-    // C rows: (r1.w, r2.x, r2.y) (r2.z, r2.w, r3.x) (r3.y, r3.z, r3.w)
-    if (COMP == 0) {
-      const float4 r1 = a.rec1[q];
-      vp = r1.x;
-      if (APIC) {
-        const float4 r2 = a.rec2[q];
-        c0 = r1.w; c1 = r2.x; c2 = r2.y;
-      }
-    } else if (COMP == 1) {
-      vp = a.rec1[q].y;
-      if (APIC) {
-        const float4 r2 = a.rec2[q], r3 = a.rec3[q];
-        c0 = r2.z; c1 = r2.w; c2 = r3.x;
-      }
+    // APIC: record 1 + c holds (v_c, C row c); FLIP/PIC: record 1 (vx, vy, vz)
+    if (APIC) {
+      const float4 rc = (COMP == 0 ? a.rec1 : (COMP == 1 ? a.rec2 : a.rec3))[q];
+      vp = rc.x; c0 = rc.y; c1 = rc.z; c2 = rc.w;
     } else {
-      vp = a.rec1[q].z;
-      if (APIC) {
-        const float4 r3 = a.rec3[q];
-        c0 = r3.y; c1 = r3.z; c2 = r3.w;
-      }
+      const float4 r1 = a.rec1[q];
+      vp = COMP == 0 ? r1.x : (COMP == 1 ? r1.y : r1.z);
     }
     const float fx = __fdiv_rn(r0.x, dx) - HX, fy = __fdiv_rn(r0.y, dx) - HY,
                 fz = __fdiv_rn(r0.z, dx) - HZ;
@@ -475,15 +462,16 @@ __device__ __forceinline__ void p2g_tile_body(const P2GArgs &a, int t, int64_t k
           st[0 * P2G_CH + i] = __fdiv_rn(r0.x, dx);
           st[1 * P2G_CH + i] = __fdiv_rn(r0.y, dx);
           st[2 * P2G_CH + i] = __fdiv_rn(r0.z, dx);
-          st[3 * P2G_CH + i] = r1.x;
-          st[4 * P2G_CH + i] = r1.y;
-          st[5 * P2G_CH + i] = r1.z;
-          if (APIC) {
+          if (APIC) {  // records 1..3: (v_c, C row c)
             const float4 r2 = a.rec2[q], r3 = a.rec3[q];
-            const float f[12] = {r0.x, r0.y, r0.z, r1.w, r2.x, r2.y,
-                                 r2.z, r2.w, r3.x, r3.y, r3.z, r3.w};
+            const float f[15] = {r1.x, r2.x, r3.x, r0.x, r0.y, r0.z, r1.y, r1.z,
+                                 r1.w, r2.y, r2.z, r2.w, r3.y, r3.z, r3.w};
 #pragma unroll
-            for (int m = 0; m < 12; ++m) st[(6 + m) * P2G_CH + i] = f[m];
+            for (int m = 0; m < 15; ++m) st[(3 + m) * P2G_CH + i] = f[m];
+          } else {
+            st[3 * P2G_CH + i] = r1.x;
+            st[4 * P2G_CH + i] = r1.y;
+            st[5 * P2G_CH + i] = r1.z;
           }
         }
         __syncwarp();
@@ -567,20 +555,22 @@ __device__ __forceinline__ void p2g_tile_body(const P2GArgs &a, int t, int64_t k
     }
     float gx = __fdiv_rn(r0.x, a.dx), gy = __fdiv_rn(r0.y, a.dx), gz = __fdiv_rn(r0.z, a.dx);
     float hx = gx - 0.5f, hy = gy - 0.5f, hz = gz - 0.5f;
-    // C rows: (r1.w, r2.x, r2.y) (r2.z, r2.w, r3.x) (r3.y, r3.z, r3.w)
+    // component c: velocity and C row.  APIC: record 1 + c holds (v_c, C row
+    // c); FLIP/PIC: record 1 holds (vx, vy, vz)
+    const float vc0 = r1.x, vc1 = APIC ? r2.x : r1.y, vc2 = APIC ? r3.x : r1.z;
     T *v0 = s_val, *w0 = s_wt, *v1 = s_val + BK, *w1 = s_wt + BK, *v2 = s_val + 2 * BK,
       *w2 = s_wt + 2 * BK;
-    if (!scatter_comp_fast<APIC, KT, T>(v0, w0, 0, r1.x, r1.w, r2.x, r2.y, r0.x, r0.y, r0.z, gx,
+    if (!scatter_comp_fast<APIC, KT, T>(v0, w0, 0, vc0, r1.y, r1.z, r1.w, r0.x, r0.y, r0.z, gx,
                                         hy, hz, I0, J0, K0, a))
-      scatter_comp<APIC, KT, T>(v0, w0, 0, r1.x, r1.w, r2.x, r2.y, r0.x, r0.y, r0.z, gx, hy, hz,
+      scatter_comp<APIC, KT, T>(v0, w0, 0, vc0, r1.y, r1.z, r1.w, r0.x, r0.y, r0.z, gx, hy, hz,
                                 I0, J0, K0, a, a.u, a.uw);
-    if (!scatter_comp_fast<APIC, KT, T>(v1, w1, 1, r1.y, r2.z, r2.w, r3.x, r0.x, r0.y, r0.z, hx,
+    if (!scatter_comp_fast<APIC, KT, T>(v1, w1, 1, vc1, r2.y, r2.z, r2.w, r0.x, r0.y, r0.z, hx,
                                         gy, hz, I0, J0, K0, a))
-      scatter_comp<APIC, KT, T>(v1, w1, 1, r1.y, r2.z, r2.w, r3.x, r0.x, r0.y, r0.z, hx, gy, hz,
+      scatter_comp<APIC, KT, T>(v1, w1, 1, vc1, r2.y, r2.z, r2.w, r0.x, r0.y, r0.z, hx, gy, hz,
                                 I0, J0, K0, a, a.v, a.vw);
-    if (!scatter_comp_fast<APIC, KT, T>(v2, w2, 2, r1.z, r3.y, r3.z, r3.w, r0.x, r0.y, r0.z, hx,
+    if (!scatter_comp_fast<APIC, KT, T>(v2, w2, 2, vc2, r3.y, r3.z, r3.w, r0.x, r0.y, r0.z, hx,
                                         hy, gz, I0, J0, K0, a))
-      scatter_comp<APIC, KT, T>(v2, w2, 2, r1.z, r3.y, r3.z, r3.w, r0.x, r0.y, r0.z, hx, hy, gz,
+      scatter_comp<APIC, KT, T>(v2, w2, 2, vc2, r3.y, r3.z, r3.w, r0.x, r0.y, r0.z, hx, hy, gz,
                                 I0, J0, K0, a, a.w, a.ww);
   }
   __syncthreads();
