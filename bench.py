@@ -679,7 +679,8 @@ def extra_legs(torch, device, steps=3):
     [.7,1], y in [0,.7]), FLIP 0.97, dt 1/960, refined PCG to 1e-7 (the
     global-memory solver: the active region exceeds the shared-memory one)
     with the tile SGS preconditioner, then warm-started from the previous
-    substep's pressure, and, from the same state, with the reference's Jacobi
+    substep's pressure, then with the coarse correction over cubes of tiles
+    (warm-started, and cold), and, from the same state, with the reference's Jacobi
     preconditioner, and 200 Jacobi sweeps as the plain comparison,
     with per-stage times and the device memory footprint."""
     import gpufluid_b200 as gf
@@ -727,7 +728,18 @@ def extra_legs(torch, device, steps=3):
     s.step(dt, pressure_iters=4000, pressure_solver="pcg_refined")
     ms_warm = timed(s, dt, 4000, "pcg_refined", steps)
     st_warm = s.pressure_stats()
+    # the same substeps with the coarse correction (cubes of tiles), warm
+    # started as above, then cold
+    restore(s, snap)
+    s.pcg_coarse = True
+    s.step(dt, pressure_iters=4000, pressure_solver="pcg_refined")
+    ms_cw = timed(s, dt, 4000, "pcg_refined", steps)
+    st_cw = s.pressure_stats()
+    restore(s, snap)
     s.pcg_warm_start = False
+    ms_cc = timed(s, dt, 4000, "pcg_refined", steps)
+    st_cc = s.pressure_stats()
+    s.pcg_coarse = False
     # the same substeps with the reference's Jacobi preconditioner
     restore(s, snap)
     s.pcg_preconditioner = "jacobi"
@@ -757,6 +769,13 @@ def extra_legs(torch, device, steps=3):
         "refined_warm_start_substeps_per_s": round(1000 / ms_warm, 3),
         "refined_warm_start_iters_last": st_warm["iters"],
         "refined_warm_start_relres_last": st_warm["relres"],
+        "refined_coarse_warm_ms_per_substep": round(ms_cw, 3),
+        "refined_coarse_warm_substeps_per_s": round(1000 / ms_cw, 3),
+        "refined_coarse_warm_iters_last": st_cw["iters"],
+        "refined_coarse_warm_used": st_cw["coarse"],
+        "refined_coarse_ms_per_substep": round(ms_cc, 3),
+        "refined_coarse_iters_last": st_cc["iters"],
+        "refined_coarse_used": st_cc["coarse"],
         "refined_jacobi_precond_ms_per_substep": round(ms_ref_jac, 3),
         "refined_jacobi_precond_iters_last": st_ref_jac["iters"],
         "pcg_kernel": "global-memory" if st_ref["kernel"] == 2 else "shared-memory",

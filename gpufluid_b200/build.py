@@ -11,8 +11,9 @@ bit-for-bit against the CPU oracle (binning, forces/divergence, Jacobi and
 GS-RB sweeps, projection, G2P, region compaction, the mesher, the
 allocation-free Jacobi) are compiled with -fmad=false, so every product and
 sum rounds separately in the reference's float32 operation order.  The
-shared-memory PCG and the adjoint kernels are checked against tolerances (an
-FP64 solve, FP64 gradients), so they are compiled with contraction on.
+shared-memory PCG, the coarse-correction set-up and the adjoint kernels are
+checked against tolerances (an FP64 solve, FP64 gradients), so they are
+compiled with contraction on.
 Kernels in a bit-exact unit that are themselves tolerance-checked (P2G, whose
 float atomics already reorder the sums) use explicit fused multiply-adds.
 """
@@ -37,7 +38,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = [*ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
           "--expt-relaxed-constexpr"]
 # translation units whose results are compared within a tolerance only
-FMA_UNITS = {"pcg_smem.cu", "adjoint.cu"}
+FMA_UNITS = {"pcg_smem.cu", "adjoint.cu", "coarse.cu"}
 
 
 def sources():

@@ -583,7 +583,7 @@ int gf_pressure_stats(void *ctx, gf_pressure_info *info) {
   info->kernel = 0;
   if (c->last_solver == GF_PCG || c->last_solver == GF_PCG_REFINED)
     info->kernel = c->state_host->smem_solver ? 1 : 2;
-  info->coarse = (info->kernel == 1 && c->state_host->coarse_used) ? 1 : 0;
+  info->coarse = (info->kernel != 0 && c->state_host->coarse_used) ? 1 : 0;
   return e;
 }
 

@@ -47,7 +47,39 @@ constexpr int64_t COARSE_B_BYTES = (int64_t)COARSE_RMAX * COARSE_RMAX * 2;
 struct CoarseMeta {
   int parity;   // which B set holds the last solve's rows
   int prev_na;  // rows of that B (0: none yet)
-  int pad[2];
+  int kind;     // COARSE_KIND_* of that B's regions
+  int pad;
+};
+constexpr int COARSE_KIND_TILES = 0;    // one region per active tile (shared-memory PCG)
+constexpr int COARSE_KIND_REGIONS = 1;  // cubes of RegionGrid::ct^3 tiles (global-memory PCG)
+constexpr int COARSE_RG_DENSE_MAX = 8192;  // regions of the cube grid, at most
+
+// The cube grid of the global-memory solver's coarse regions.
+struct RegionGrid {
+  int ct;             // tiles per region edge (a power of two)
+  int nx, ny, nz, n;  // regions per axis, total
+  int ntx, nty, ntz;  // tiles per axis
+  __host__ __device__ int region_of_tile(int t) const {
+    const int ti = t / (nty * ntz), tj = (t / ntz) % nty, tk = t % ntz;
+    return ((ti / ct) * ny + tj / ct) * nz + tk / ct;
+  }
+};
+
+struct PcgState;
+// Arguments of the coarse set-up kernels (coarse.cu).
+struct CoarseSetup {
+  const int32_t *count;  // rows (device)
+  const int32_t *ids;    // region id of each row: tile id or cube index
+  const int32_t *nbr;    // [count][6] neighbouring rows, -1: none
+  float *cdiag, *coff;   // rows of A_c: diagonal [RMAX], faces [RMAX][6]
+  uint16_t *bsets;       // [2][RMAX][RMAX] bf16 rows of B
+  int32_t *prev_slot;    // [ids] row of each id in the last B, or -1
+  int32_t *prev_list;    // [RMAX] id of each row of the last B
+  CoarseMeta *meta;
+  PcgState *st;
+  int limit;             // row counts above this skip the set-up
+  const int *gate;       // nullable: the set-up runs only when *gate != 0
+  int kind;              // COARSE_KIND_*
 };
 constexpr int64_t COARSE_DIAG_OFF = 2 * COARSE_B_BYTES;
 constexpr int64_t COARSE_OFF_OFF = COARSE_DIAG_OFF + (int64_t)COARSE_RMAX * 4;
@@ -82,7 +114,9 @@ struct PcgState {
   int smem_solver; // 1: the last solve ran in the shared-memory solver
   int trace_n;     // globaltimer stamps recorded (diagnostic trace)
   int coarse_off;  // a block's coarse-column solve failed: coarse correction off
-  int coarse_used; // 1: the last shared-memory solve applied the coarse correction
+  int coarse_used; // 1: the last solve applied the coarse correction
+  double rz_part;  // global-memory solver with the coarse correction: r . M_tile r, before
+                   // the coarse term r . P e is added
 };
 
 // Shared-memory-resident PCG (pcg_smem.cu).  Returns GF_OK after enqueuing;
@@ -211,7 +245,11 @@ struct Ctx {
   unsigned long long *bar_counters = nullptr;  // 8 lines x 16 u64
   float *halo = nullptr;         // [6 * nkeys] halo publication buffers
   unsigned char *coarse_buf = nullptr;  // [COARSE_BUF_BYTES] coarse operator and inverse rows
-  int32_t *coarse_prev_slot = nullptr;  // [ntiles] row of each tile in the last B, or -1
+  int32_t *coarse_prev_slot = nullptr;  // [max(ntiles, rg.n)] row of each id in the last B, or -1
+  RegionGrid rg{};                      // coarse regions of the global-memory PCG
+  int32_t *rg_buf = nullptr;            // region flags, slots, list, count, neighbours, tiles
+  float *rg_gt = nullptr;               // [ntiles] residual sum of each tile slot (per iteration)
+  float *rg_e = nullptr;                // [RMAX] coarse correction of each region (per iteration)
   int32_t *tile_cost = nullptr;  // [ntiles] per-slot PCG work estimate
   long long *trace = nullptr;    // [TRACE_CAP] PCG phase timestamps
   bool trace_on = false;
@@ -296,6 +334,16 @@ int bounds_read_pressure(unsigned long long *hits, int *line, int reset);
 // ---- helpers ---------------------------------------------------------------
 int fail(Ctx *c, int status, const std::string &msg);
 int check_cuda(Ctx *c, cudaError_t e, const char *what);
+int coarse_setup_tiles(Ctx *c, const int32_t *n_active, const int32_t *tile_list,
+                       const int32_t *tile_nbr, const uint16_t *code, PcgState *st, int limit);
+int coarse_setup_regions(Ctx *c, PcgState *st, const int *gate);
+// Ctx::rg_buf: region flags and slots [rg.n], the active regions' list
+// [RMAX], their count, neighbours [RMAX][6], tile slots [RMAX][ct^3] and the
+// region of each tile slot [ntiles]
+struct RegionBufs {
+  int32_t *flag, *slot, *list, *count, *nbr, *tiles, *of_slot;
+};
+RegionBufs region_bufs(Ctx *c);
 int check_launch(Ctx *c, const char *what);
 
 __host__ __device__ inline int64_t uidx(int i, int j, int k, int ny, int nz) {

@@ -37,8 +37,6 @@
 // If the active region holds more than SmemCfg::MAXT tiles per block the
 // kernel sets PcgState::fallback and returns; the global-memory solver (k_pcg
 // in pressure.cu) launched right after it then performs the solve.
-#include <cuda_bf16.h>
-
 #include "gf_internal.cuh"
 
 namespace gf {
@@ -54,7 +52,6 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long
 
 constexpr int SM_MAXG = 160;      // blocks (one per SM)
 constexpr int CRMAX = COARSE_RMAX;  // coarse regions (one per active tile), at most
-constexpr float kCoarseTol2 = 1e-6f;  // squared residual target of the coarse row solves
 static_assert(SM_MAXG == COARSE_MAXG, "coarse buffer sizing");
 
 struct GridSync {
@@ -553,7 +550,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   // ---- coarse correction (GF_FLAG_COARSE): one region per active tile, P
   // the indicator of each tile's fluid cells, and the preconditioner
   // M^-1 = M_tile^-1 + P B P^T (additive two-level) with B = (P^T A P)^-1,
-  // whose rows k_coarse_rows / k_coarse_solve computed before this launch (as
+  // whose rows the set-up kernels of coarse.cu computed before this launch (as
   // bfloat16; the set CoarseMeta::parity names).  A failed row solve switched
   // the correction off for the solve.
   const bool coarse = CRS && a.coarse && a.cbuf != nullptr &&
@@ -747,14 +744,6 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       for (int k = 0; k < 3; ++k)
         if (t + k * SM_THREADS < na) gpre[k] = ld_relaxed_u64(gsrc + t + k * SM_THREADS);
     };
-#ifdef GF_COARSE_PREFETCH
-    if (CRS && coarse && nt > 0) {  // B rows of the apply below into L1
-      const int jr = wid % nt, iw = wid / nt, nw = (31 - jr) / nt + 1;
-      const uint4 *row = reinterpret_cast<const uint4 *>(Bh + (int64_t)(b0 + jr) * CRMAX);
-      for (int ch = iw * 32 + lane; ch < ((na + 7) >> 3); ch += nw * 32)
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(row + ch));
-    }
-#endif
     for (int sw = 0; sw < sgs; ++sw) {
       half_sweep(1);
       __syncthreads();
@@ -1052,214 +1041,6 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   }
 }
 
-// ---- set-up of the coarse correction (GF_FLAG_COARSE), before the solve.
-// Row t of A_c = P^T A P for active tile t (one block per tile): the
-// diagonal is the sum over the tile's fluid cells of diag - #fluid neighbours
-// inside the tile, entry (t, nbr[t][dir]) is minus the number of fluid-fluid
-// faces across face dir.  An empty tile gets a unit diagonal (it decouples).
-// Tiles beyond `limit` (more than the shared-memory solver holds) set no rows.
-__global__ void __launch_bounds__(256) k_coarse_rows(const int32_t *__restrict__ n_active,
-                                                     const int32_t *__restrict__ nbr,
-                                                     const uint16_t *__restrict__ code,
-                                                     float *__restrict__ cdiag,
-                                                     float *__restrict__ coff, int limit) {
-  const int na = *n_active;
-  const int s = blockIdx.x;
-  if (na > limit || na > CRMAX || s >= na) return;
-  float v[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // diagonal, then faces 0..5
-  for (int L = threadIdx.x; L < 512; L += blockDim.x) {
-    const uint16_t cd = code[(int64_t)s * 512 + L];
-    if (!(cd & CODE_FLUID)) continue;
-    const int li = L >> 6, lj = (L >> 3) & 7, lk = L & 7;
-    int same = 0;
-#pragma unroll
-    for (int dir = 0; dir < 6; ++dir) {
-      if (!(cd & (1 << dir))) continue;
-      const bool inside = dir == 0 ? li > 0 : dir == 1 ? li < 7 : dir == 2 ? lj > 0
-                        : dir == 3 ? lj < 7 : dir == 4 ? lk > 0 : lk < 7;
-      if (inside) ++same; else v[1 + dir] += 1.f;
-    }
-    v[0] += (float)((int)((cd >> CODE_DIAG_SHIFT) & 7) - same);
-  }
-  __shared__ float red[8][7];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int k = 0; k < 7; ++k) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
-    if (lane == 0) red[wid][k] = v[k];
-  }
-  __syncthreads();
-  if (threadIdx.x < 7) {
-    float t = 0.f;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w][threadIdx.x];
-    if (threadIdx.x == 0) {
-      cdiag[s] = t > 0.f ? t : 1.0f;
-    } else {
-      const int dir = threadIdx.x - 1;
-      coff[(int64_t)s * 6 + dir] = nbr[(int64_t)s * 6 + dir] >= 0 ? -t : 0.f;
-    }
-  }
-}
-
-// Row r of B = A_c^-1 (one block per active tile r): A_c x = e_r by
-// Jacobi-preconditioned CG in float32 to ||e_r - A_c x|| <= 1e-3 (B only has
-// to be close to the inverse for the correction to work), the vectors in
-// shared memory, the rows of A_c read through the cache.  The solve starts
-// from the last solve's row of the same tile, its columns mapped by tile
-// (zero for tiles that had no row): the fluid moves little from one substep
-// to the next, and a few CG steps instead of ~35 meet the target.  Written as
-// bfloat16 with row stride CRMAX, zero up to the next multiple of 8 columns,
-// into the B set the last solve did not use.  A solve that fails (no
-// convergence, a non-finite value) switches the correction off for the
-// coming solve.
-constexpr int COARSE_SOLVE_THREADS = 256;
-__device__ __forceinline__ float bf16_at(const uint16_t *p, int64_t i) {
-  return __uint_as_float((unsigned)p[i] << 16);
-}
-__global__ void __launch_bounds__(COARSE_SOLVE_THREADS)
-    k_coarse_solve(const int32_t *__restrict__ n_active, const int32_t *__restrict__ tile_list,
-                   const int32_t *__restrict__ nbr, const float *__restrict__ cdiag,
-                   const float *__restrict__ coff, uint16_t *__restrict__ bsets,
-                   const int32_t *__restrict__ prev_slot, const CoarseMeta *meta, PcgState *st,
-                   int limit) {
-  extern __shared__ float cs[];  // x, r, p, q: [4][na]
-  const int na = *n_active;
-  const int rr0 = blockIdx.x;
-  if (na > limit || na > CRMAX || rr0 >= na) return;
-  const int par = meta->parity;
-  const uint16_t *bprev = bsets + (int64_t)par * CRMAX * CRMAX;
-  uint16_t *bh = bsets + (int64_t)(par ^ 1) * CRMAX * CRMAX;
-  const int pr = meta->prev_na > 0 ? prev_slot[tile_list[rr0]] : -1;
-  float *cx = cs, *cr = cs + na, *cp = cr + na, *cq = cp + na;
-  __shared__ float red[COARSE_SOLVE_THREADS / 32][2];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  auto bsum = [&](float a0, float a1, float &o0, float &o1) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      a0 += __shfl_xor_sync(0xffffffffu, a0, o);
-      a1 += __shfl_xor_sync(0xffffffffu, a1, o);
-    }
-    if (lane == 0) {
-      red[wid][0] = a0;
-      red[wid][1] = a1;
-    }
-    __syncthreads();
-    float s0 = 0.f, s1 = 0.f;
-#pragma unroll
-    for (int w = 0; w < COARSE_SOLVE_THREADS / 32; ++w) {
-      s0 += red[w][0];
-      s1 += red[w][1];
-    }
-    __syncthreads();
-    o0 = s0;
-    o1 = s1;
-  };
-  auto matvec = [&](const float *x, int i) {
-    float acc = __ldg(cdiag + i) * x[i];
-#pragma unroll
-    for (int dir = 0; dir < 6; ++dir) {
-      const int j = __ldg(nbr + (int64_t)i * 6 + dir);
-      if (j >= 0 && j < na) acc += __ldg(coff + (int64_t)i * 6 + dir) * x[j];
-    }
-    return acc;
-  };
-  for (int i = threadIdx.x; i < na; i += blockDim.x) {  // the warm start
-    float x0 = 0.f;
-    if (pr >= 0) {
-      const int pc = prev_slot[tile_list[i]];
-      if (pc >= 0) x0 = bf16_at(bprev, (int64_t)pr * CRMAX + pc);
-    }
-    cx[i] = isfinite(x0) ? x0 : 0.f;
-  }
-  __syncthreads();
-  float rz = 0.f, rn2 = 0.f;
-  {
-    float a0 = 0.f, a1 = 0.f;
-    for (int i = threadIdx.x; i < na; i += blockDim.x) {
-      const float b = (i == rr0 ? 1.f : 0.f) - matvec(cx, i);
-      cr[i] = b;
-      cp[i] = b / __ldg(cdiag + i);
-      a0 += b * cp[i];
-      a1 += b * b;
-    }
-    bsum(a0, a1, rz, rn2);
-  }
-  bool ok = rn2 <= kCoarseTol2;
-  for (int it = 0; it < 1000 && !ok; ++it) {
-    float pq, dummy;
-    {
-      float a0 = 0.f;
-      for (int i = threadIdx.x; i < na; i += blockDim.x) {
-        const float v = matvec(cp, i);
-        cq[i] = v;
-        a0 += cp[i] * v;
-      }
-      bsum(a0, 0.f, pq, dummy);
-    }
-    if (!(pq > 0.f)) break;
-    const float al = rz / pq;
-    float a0 = 0.f, a1 = 0.f;
-    for (int i = threadIdx.x; i < na; i += blockDim.x) {
-      cx[i] += al * cp[i];
-      const float rn = cr[i] - al * cq[i];
-      cr[i] = rn;
-      a0 += rn * rn;
-      a1 += rn * rn / __ldg(cdiag + i);
-    }
-    float rz2;
-    bsum(a0, a1, rn2, rz2);
-    if (rn2 <= kCoarseTol2) {
-      ok = true;
-      break;
-    }
-    const float be = rz2 / rz;
-    rz = rz2;
-    for (int i = threadIdx.x; i < na; i += blockDim.x) cp[i] = cr[i] / __ldg(cdiag + i) + be * cp[i];
-    __syncthreads();
-  }
-  bool finite = true;
-  uint16_t *out = bh + (int64_t)rr0 * CRMAX;
-  const int R8 = (na + 7) & ~7;
-  for (int i = threadIdx.x; i < R8; i += blockDim.x) {
-    const float x = i < na ? cx[i] : 0.f;
-    finite &= isfinite(x);
-    out[i] = __bfloat16_as_ushort(__float2bfloat16_rn(x));
-  }
-  if ((threadIdx.x == 0 && !ok) || !finite) atomicExch(&st->coarse_off, 1);
-}
-
-// After the row solves: the tile-to-row map and the row tiles describe the
-// new B, and the parity names its set.  First the last B's tiles lose their
-// rows, then the new ones get theirs (two launches, so that no block clears
-// an entry another has already set).
-__global__ void k_coarse_commit_clear(const int32_t *__restrict__ n_active,
-                                      const int32_t *__restrict__ prev_list,
-                                      int32_t *__restrict__ prev_slot, const CoarseMeta *meta,
-                                      int limit) {
-  const int na = *n_active;
-  if (na > limit || na > CRMAX) return;
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < meta->prev_na;
-       s += gridDim.x * blockDim.x)
-    prev_slot[prev_list[s]] = -1;
-}
-__global__ void k_coarse_commit_set(const int32_t *__restrict__ n_active,
-                                    const int32_t *__restrict__ tile_list,
-                                    int32_t *__restrict__ prev_list,
-                                    int32_t *__restrict__ prev_slot, CoarseMeta *meta, int limit) {
-  const int na = *n_active;
-  if (na > limit || na > CRMAX) return;
-  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < na; s += gridDim.x * blockDim.x) {
-    const int t = tile_list[s];
-    prev_slot[t] = s;
-    prev_list[s] = t;
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    meta->prev_na = na;
-    meta->parity ^= 1;
-  }
-}
-
 template <typename Acc, bool REF>
 static bool fits_t(Ctx *c) {
   int optin = 0;
@@ -1295,23 +1076,9 @@ static int launch_t(Ctx *c, PcgSmemArgs &a) {
   if (e) return e;
   if (per_sm < 1) return fail(c, GF_CUDA_ERROR, "PCG shared-memory kernel does not fit an SM");
   if (a.coarse && a.cbuf) {  // rows of A_c, then of B = A_c^-1, for the active tiles
-    const int limit = c->num_sms * SmemCfg<REF>::MAXT;
-    float *cdiag = reinterpret_cast<float *>(a.cbuf + COARSE_DIAG_OFF);
-    float *coff = reinterpret_cast<float *>(a.cbuf + COARSE_OFF_OFF);
-    int32_t *plist = reinterpret_cast<int32_t *>(a.cbuf + COARSE_LIST_OFF);
-    CoarseMeta *meta = reinterpret_cast<CoarseMeta *>(a.cbuf + COARSE_META_OFF);
-    k_coarse_rows<<<CRMAX, 256, 0, c->stream>>>(a.n_active, a.nbr, a.code, cdiag, coff, limit);
-    const size_t vec = (size_t)4 * CRMAX * sizeof(float);
-    k_coarse_solve<<<CRMAX, COARSE_SOLVE_THREADS, vec, c->stream>>>(
-        a.n_active, a.tile_list, a.nbr, cdiag, coff, reinterpret_cast<uint16_t *>(a.cbuf),
-        c->coarse_prev_slot, meta, a.st, limit);
-    k_coarse_commit_clear<<<(CRMAX + 255) / 256, 256, 0, c->stream>>>(a.n_active, plist,
-                                                                    c->coarse_prev_slot, meta,
-                                                                    limit);
-    k_coarse_commit_set<<<(CRMAX + 255) / 256, 256, 0, c->stream>>>(
-        a.n_active, a.tile_list, plist, c->coarse_prev_slot, meta, limit);
-    c->launches += 4;
-    if ((e = check_launch(c, "coarse correction set-up"))) return e;
+    if ((e = coarse_setup_tiles(c, a.n_active, a.tile_list, a.nbr, a.code, a.st,
+                                c->num_sms * SmemCfg<REF>::MAXT)))
+      return e;
   }
   void *args[] = {&a};
   e = check_cuda(c, cudaLaunchCooperativeKernel((const void *)fn, dim3(c->num_sms),

@@ -353,6 +353,14 @@ struct PcgArgs {
   const float *p0;
   const int32_t *tile_list;
   int ny, nz, nty, ntz;
+  // cube-region coarse correction (SGS instantiation; coarse.cu set up its
+  // rows): active regions, the tile slots of each region [RMAX][ct^3], the
+  // region of each tile slot, the tiles' residual sums, the corrections e
+  int coarse;
+  const int32_t *rg_count, *rg_tiles, *rg_of_slot;
+  int rg_nt3;
+  float *rg_gt, *rg_e;
+  const unsigned char *cbuf;
 };
 
 // ---- tile-local symmetric Gauss-Seidel preconditioner of the global-memory
@@ -505,6 +513,80 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
   __shared__ alignas(16) unsigned char sgs_raw[SGS ? sizeof(SgsSmem) : 16];
   SgsSmem &S = *reinterpret_cast<SgsSmem *>(sgs_raw);  // boxes of the SGS instantiation
   const int na = *a.n_active;
+  // cube-region coarse correction (tile SGS only): u = z + P e with
+  // e = B P^T r, B's bf16 rows from the set-up; off when a row solve failed
+  // or the set-up did not run (too many regions)
+  __shared__ float s_g[SGS ? COARSE_RMAX : 1];   // every region's residual sum
+  __shared__ float s_tp[SGS ? SGS_TB * 16 : 1];  // warp partials of the round's tile sums
+  const int nreg = SGS && a.coarse ? *a.rg_count : 0;
+  const bool coarse = SGS && a.coarse && nreg > 0 && nreg <= COARSE_RMAX &&
+                      ld_volatile_i(&a.st->coarse_off) == 0;
+  const uint16_t *Bh = nullptr;
+  if (coarse)
+    Bh = reinterpret_cast<const uint16_t *>(a.cbuf) +
+         (int64_t)reinterpret_cast<const CoarseMeta *>(a.cbuf + COARSE_META_OFF)->parity *
+             COARSE_RMAX * COARSE_RMAX;
+  // tile sums of r over a round's SGS_TB tiles (thread t holds cell t of each)
+  auto tile_sums = [&](int base, const float (&v)[SGS_TB]) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int m = 0; m < SGS_TB; ++m) {
+      float x = v[m];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+      if (lane == 0) s_tp[m * 16 + wid] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < SGS_TB && base + (int)threadIdx.x < na) {
+      float s = 0.f;
+#pragma unroll
+      for (int w = 0; w < 16; ++w) s += s_tp[threadIdx.x * 16 + w];
+      a.rg_gt[base + threadIdx.x] = s;
+    }
+  };
+  // the coarse correction of e = B P^T r after a grid barrier that follows
+  // the tile sums: every block sums all regions' g into shared memory (the
+  // region's tiles in index order), its warps form e for a share of the
+  // regions, and g . e = r . P e rides on one grid reduction whose `fin`
+  // gets the total
+  auto coarse_step = [&](auto fin) -> bool {
+    for (int k = threadIdx.x; k < nreg; k += blockDim.x) {
+      float g = 0.f;
+      for (int j = 0; j < a.rg_nt3; ++j) {
+        const int sl = a.rg_tiles[(int64_t)k * a.rg_nt3 + j];
+        if (sl >= 0) g += __ldcg(a.rg_gt + sl);
+      }
+      s_g[k] = g;
+    }
+    for (int k = nreg + threadIdx.x; k < ((nreg + 7) & ~7); k += blockDim.x) s_g[k] = 0.f;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double ge = 0.0;
+    for (int k = blockIdx.x * nw + wid; k < nreg; k += gridDim.x * nw) {
+      const uint4 *row = reinterpret_cast<const uint4 *>(Bh + (int64_t)k * COARSE_RMAX);
+      float v = 0.f;
+      for (int ch = lane; ch < ((nreg + 7) >> 3); ch += 32) {
+        const uint4 q = __ldg(row + ch);
+        const float *gp = s_g + ch * 8;
+        v += __uint_as_float(q.x << 16) * gp[0] + __uint_as_float(q.x & 0xffff0000u) * gp[1];
+        v += __uint_as_float(q.y << 16) * gp[2] + __uint_as_float(q.y & 0xffff0000u) * gp[3];
+        v += __uint_as_float(q.z << 16) * gp[4] + __uint_as_float(q.z & 0xffff0000u) * gp[5];
+        v += __uint_as_float(q.w << 16) * gp[6] + __uint_as_float(q.w & 0xffff0000u) * gp[7];
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) {
+        a.rg_e[k] = v;
+        ge += (double)s_g[k] * (double)v;
+      }
+    }
+    double w[1] = {ge};
+    return grid_reduce<double, 1>(a, w, fin);
+  };
+  // u = z + e of the cell's region
+  auto ecell = [&](int64_t q) -> float {
+    return coarse ? __ldcg(a.rg_e + a.rg_of_slot[q >> 9]) : 0.0f;
+  };
   if (SGS) {  // the boxes' rings stay zero for the whole solve
     for (int q = threadIdx.x; q < SGS_TB * 1000; q += blockDim.x) S.zb[q] = 0.f;
   }
@@ -571,6 +653,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
           v[0] += (Acc)(bb[m] * z);
           v[1] += (Acc)(bb[m] * bb[m]);
         }
+        if (coarse) tile_sums(base, bb);
         __syncthreads();
       }
     } else {
@@ -597,6 +680,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
     }
     if (!grid_reduce<Acc, 2>(a, v, [&](double *t) {
           st->rz = t[0];
+          st->rz_part = t[0];
           st->r0 = t[1];
           st->rr = t[1];
           st->r_upd2 = t[1];
@@ -615,6 +699,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
           }
         }))
       return;
+    if (coarse && !coarse_step([&](double *t) { st->rz = st->rz_part + t[0]; })) return;
   }
 
   for (int it = 0; it < a.max_iter; ++it) {
@@ -640,13 +725,17 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
           dn[m] = sn[m] = 0.0f;
           if (!(cd[m] & CODE_FLUID)) continue;
           const int64_t q = qb + m * stride;
-          dn[m] = __ldcg(Z + q) + beta * __ldcg(dold + q);
+          const float eq = ecell(q);
+          dn[m] = (__ldcg(Z + q) + eq) + beta * __ldcg(dold + q);
           float s = 0.0f;
 #pragma unroll
           for (int d = 0; d < 6; ++d)
             if (cd[m] & (1 << d)) {
               const int64_t nq = nb_index(q, d, a.nbr);
-              if (GF_IN(nq, total)) s = s + (__ldcg(Z + nq) + beta * __ldcg(dold + nq));
+              if (GF_IN(nq, total)) {
+                const float en = (nq >> 9) == (q >> 9) ? eq : ecell(nq);
+                s = s + ((__ldcg(Z + nq) + en) + beta * __ldcg(dold + nq));
+              }
             }
           sn[m] = s;
         }
@@ -717,6 +806,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
             v[0] += (Acc)(rr[m] * z);
             v[1] += (Acc)(rr[m] * rr[m]);
           }
+          if (coarse) tile_sums(base, rr);
           __syncthreads();
         }
       } else
@@ -771,11 +861,21 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
             }
             if (replace) {
               st->n_replace = -st->n_replace - 1;  // negative: replacement pending
+            } else if (coarse) {
+              st->rz_part = rz_new;  // beta once the coarse term is in
             } else {
               const double rz = st->rz;
               st->beta = (Acc)fabs(rz) < (Acc)1.0e-30 ? 0.0 : (double)((Acc)rz_new / (Acc)rz);
               st->rz = rz_new;
             }
+          }))
+        return;
+      // the coarse term of r . u and beta (not when a replacement recomputes r)
+      if (coarse && !(REF && ld_volatile_i(&st->n_replace) < 0) && !ld_volatile_i(&st->done) &&
+          !coarse_step([&](double *t) {
+            const double rz = st->rz, rz_new = st->rz_part + t[0];
+            st->beta = fabs(rz) < 1.0e-30 ? 0.0 : rz_new / rz;
+            st->rz = rz_new;
           }))
         return;
     }
@@ -828,6 +928,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
             v[1] += (double)(rf[m] * z);
             v[2] += (double)(rf[m] * rf[m]);
           }
+          if (coarse) tile_sums(base, rf);
           __syncthreads();
         }
       } else {
@@ -849,16 +950,29 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs a) {
             st->r_upd2 = t[2];
             st->rr = t[2];
             st->n_replace = -st->n_replace;  // back to a positive count (+1)
-            const double rz = st->rz;
-            st->beta = fabs(rz) < 1.0e-30 ? 0.0 : t[1] / rz;
-            st->rz = t[1];
+            if (coarse) {
+              st->rz_part = t[1];
+            } else {
+              const double rz = st->rz;
+              st->beta = fabs(rz) < 1.0e-30 ? 0.0 : t[1] / rz;
+              st->rz = t[1];
+            }
             if (t[0] <= a.tol2 * st->b2) st->done = 1;
+          }))
+        return;
+      if (coarse && !ld_volatile_i(&st->done) &&
+          !coarse_step([&](double *t) {
+            const double rz = st->rz, rz_new = st->rz_part + t[0];
+            st->beta = fabs(rz) < 1.0e-30 ? 0.0 : rz_new / rz;
+            st->rz = rz_new;
           }))
         return;
     }
   }
-  if (threadIdx.x == 0 && blockIdx.x == 0 && !ld_volatile_i(&st->done))
-    st->status = GF_NOT_CONVERGED;
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    if (!ld_volatile_i(&st->done)) st->status = GF_NOT_CONVERGED;
+    st->coarse_used = coarse ? 1 : 0;
+  }
 }
 
 // ------------------------------------------------------- segmented PCG
@@ -1530,14 +1644,40 @@ int pressure_alloc(Ctx *c) {
   // that solves can be captured in CUDA graphs
   if ((e = A((void **)&c->coarse_buf, (size_t)COARSE_BUF_BYTES, "alloc coarse operator")))
     return e;
-  if ((e = A((void **)&c->coarse_prev_slot, (size_t)c->ntiles * 4, "alloc coarse row map")))
-    return e;
-  // no B yet: meta zero, no tile has a row
+  // the cube regions of the global-memory solver: the smallest power-of-two
+  // edge (in tiles) that keeps the region grid within COARSE_RG_DENSE_MAX
+  {
+    RegionGrid &g = c->rg;
+    g.ntx = c->ntx;
+    g.nty = c->nty;
+    g.ntz = c->ntz;
+    g.ct = 1;
+    for (;;) {
+      g.nx = (g.ntx + g.ct - 1) / g.ct;
+      g.ny = (g.nty + g.ct - 1) / g.ct;
+      g.nz = (g.ntz + g.ct - 1) / g.ct;
+      g.n = g.nx * g.ny * g.nz;
+      if (g.n <= COARSE_RG_DENSE_MAX) break;
+      g.ct *= 2;
+    }
+  }
+  const int64_t nids = c->ntiles > c->rg.n ? c->ntiles : c->rg.n;
+  if ((e = A((void **)&c->coarse_prev_slot, (size_t)nids * 4, "alloc coarse row map"))) return e;
+  // no B yet: meta zero, no id has a row
   if ((e = check_cuda(c, cudaMemset(c->coarse_buf + COARSE_META_OFF, 0, sizeof(CoarseMeta)),
                       "zero coarse meta")) ||
-      (e = check_cuda(c, cudaMemset(c->coarse_prev_slot, 0xff, (size_t)c->ntiles * 4),
+      (e = check_cuda(c, cudaMemset(c->coarse_prev_slot, 0xff, (size_t)nids * 4),
                       "clear coarse row map")))
     return e;
+  {
+    const RegionGrid &g = c->rg;
+    const int64_t ni = 2 * (int64_t)g.n + COARSE_RMAX + 4 + (int64_t)COARSE_RMAX * 6 +
+                       (int64_t)COARSE_RMAX * g.ct * g.ct * g.ct + c->ntiles;
+    if ((e = A((void **)&c->rg_buf, (size_t)ni * 4, "alloc coarse regions")) ||
+        (e = A((void **)&c->rg_gt, (size_t)c->ntiles * 4, "alloc tile residual sums")) ||
+        (e = A((void **)&c->rg_e, (size_t)COARSE_RMAX * 4, "alloc region corrections")))
+      return e;
+  }
   if ((e = A((void **)&c->tile_cost, (size_t)c->ntiles * 4, "alloc tile cost"))) return e;
   if ((e = A((void **)&c->health, 8 * 4, "alloc solve health"))) return e;
   if ((e = check_cuda(c, cudaMemset(c->health, 0, 8 * 4), "zero solve health"))) return e;
@@ -1553,7 +1693,7 @@ void pressure_free(Ctx *c) {
   void *ps[] = {c->tile_slot, c->tile_list, c->tile_order, c->tile_nbr, c->n_active, c->code, c->bdiv,
                 c->xf, c->r, c->z, c->d0, c->d1, c->Ad, c->x64, c->partials, c->state,
                 c->bar_counters, c->trace, c->halo, c->tile_cost, c->coarse_buf,
-                c->coarse_prev_slot, c->health};
+                c->coarse_prev_slot, c->rg_buf, c->rg_gt, c->rg_e, c->health};
   for (void *p : ps)
     if (p) cudaFree(p);
   if (c->state_host) cudaFreeHost(c->state_host);
@@ -1798,6 +1938,22 @@ int launch_pressure(Ctx *c, const gf_step_params *prm) {
                force_global ? 0 : 1, (prm->flags & GF_FLAG_SGS_MASK) >> GF_FLAG_SGS_SHIFT,
                (refined && (prm->flags & GF_FLAG_WARM_START)) ? 1 : 0, c->f.p, c->tile_list,
                c->ny, c->nz, c->nty, c->ntz};
+    // the cube-region coarse correction (tile SGS only): set up for the
+    // global-memory solve, which runs when forced or when the shared-memory
+    // solver defers (the set-up then waits for the same flag)
+    if ((prm->flags & GF_FLAG_COARSE) && pa.sgs > 0) {
+      const RegionBufs rb = region_bufs(c);
+      pa.coarse = 1;
+      pa.rg_count = rb.count;
+      pa.rg_tiles = rb.tiles;
+      pa.rg_of_slot = rb.of_slot;
+      pa.rg_nt3 = c->rg.ct * c->rg.ct * c->rg.ct;
+      pa.rg_gt = c->rg_gt;
+      pa.rg_e = c->rg_e;
+      pa.cbuf = c->coarse_buf;
+      if ((e = coarse_setup_regions(c, c->state, force_global ? nullptr : &c->state->fallback)))
+        return e;
+    }
     if (refined) {
       e = launch_pcg<double, true>(c, pa);
       result64 = c->x64;

@@ -292,20 +292,23 @@ def test_cfg3_256_global_pcg_against_fp64(gf, oracle):
     assert rel < 1e-11, rel  # the reference solve: its error is far below the 1e-5 checked
     fl = lab_dev == 1
     iters = {}
-    for precond in ("jacobi", "tile_sgs"):
-        s.pcg_preconditioner = precond
+    for precond in ("jacobi", "tile_sgs", "tile_sgs+coarse"):
+        s.pcg_preconditioner = precond.split("+")[0]
+        s.pcg_coarse = precond.endswith("coarse")
         prm = s._params(dt, 8000, "pcg_refined")
         _call(s, "gf_pressure", ctypes.byref(prm), None)
         st = s.pressure_stats()
         assert st["kernel"] == 2, st  # the global-memory solver
+        assert st["coarse"] == (1 if s.pcg_coarse else 0), (precond, st)
         assert st["status"] == 0 and st["relres"] <= 1e-7, (precond, st)
         assert st["n_fluid"] > 6_000_000
         p = torch.where(fl, s._p.double(), torch.zeros_like(x64))
         err = float(torch.linalg.vector_norm(p - x64) / torch.linalg.vector_norm(x64))
         assert err < 1e-5, (precond, err)
         iters[precond] = st["iters"]
-    assert iters["tile_sgs"] < iters["jacobi"], iters
+    assert iters["tile_sgs+coarse"] < iters["tile_sgs"] < iters["jacobi"], iters
     s.pcg_preconditioner = "jacobi"
+    s.pcg_coarse = False
     # 20 Jacobi sweeps: bit-exact against the oracle on the same system
     prm = s._params(dt, 20, "jacobi")
     s.div.copy_(div_dev)

@@ -454,6 +454,52 @@ def test_global_pcg_tile_sgs_preconditioner(gf, oracle, grid, refined):
     assert res[2] < res[1] < res[0], res
 
 
+@pytest.mark.parametrize("refined", [True, False])
+@pytest.mark.parametrize("grid", [(48, 40, 56), (80, 80, 80), (128, 128, 128)])
+def test_global_pcg_coarse_correction(gf, oracle, grid, refined):
+    """Coarse correction of the global-memory PCG (GF_FLAG_COARSE with the
+    tile SGS preconditioner; one region per cube of tiles, here one tile per
+    cube): the same FP64 answer as the tile SGS alone, in fewer iterations
+    from 80^3; the 128^3 system is the dam break of the shared-memory test."""
+    import torch
+    from gpufluid_b200 import _lib
+    res = {}
+    base = _lib.GF_FLAG_GLOBAL_PCG | (2 << _lib.GF_FLAG_SGS_SHIFT)
+    for flags in (base, base | _lib.GF_FLAG_COARSE):
+        s, o = _pressure_case(gf, oracle, grid, seed=37)
+        if grid[0] >= 80:
+            lab = s._marker_host.copy()
+            if grid[0] == 128:
+                lab[1:52, 1:77, 1:-1] = 1
+            else:
+                lab[1:-1, 1:64, 1:-1] = 1
+            rng = np.random.default_rng(5)
+            div = np.where(lab == 1, rng.normal(0, 1, lab.shape), 0).astype(np.float32)
+            s._label.copy_(_t(lab.astype(np.uint8)))
+            s.div.copy_(_t(div))
+            o.marker[...] = lab
+            o.div[...] = div
+        prm = _params(gf, "pcg_refined" if refined else "pcg", 6000,
+                      tol=1e-10 if refined else 1e-6, flags=flags)
+        it = ctypes.c_int32()
+        _call(s, "gf_pressure", ctypes.byref(prm), ctypes.byref(it))
+        torch.cuda.synchronize()
+        info = _stats(s)
+        assert info.kernel == 2 and info.status == 0, (flags, info.kernel, info.status)
+        assert info.coarse == (1 if flags & _lib.GF_FLAG_COARSE else 0), flags
+        if not res:
+            p64, _, _ = oracle.pcg64(o.marker, o.div, tol=1e-14)
+        if refined:
+            assert info.relres <= 1e-10, (flags, info.relres)
+            assert rel_l2(s._p.cpu().numpy(), p64) < 1e-6
+        else:
+            assert info.relres <= 1e-6, (flags, info.relres)
+            assert rel_l2(s._p.cpu().numpy(), p64) < 1e-4
+        res[flags] = info.iters
+    if grid[0] >= 80:
+        assert res[base | _lib.GF_FLAG_COARSE] < res[base], res
+
+
 @pytest.mark.parametrize("kernel_flags", ["global_sgs2", "global_jacobi", "smem"])
 def test_refined_pcg_warm_start_both_kernels(gf, oracle, kernel_flags):
     """GF_FLAG_WARM_START on the refined PCG: after a solve, a nearby system
