@@ -10,7 +10,7 @@
 //                   per-key count with warp-aggregated atomics
 //   k_scan_*        exclusive scan of the per-key counts -> start
 //   k_place         slot = start[key] + rank
-//   k_canon         order each cell's segment by particle id
+//   k_canon         order each cell's segment by particle id (rank by count)
 //   k_permute       gather caller AoS buffers into sorted float4 records
 #include "gf_internal.cuh"
 
@@ -30,7 +30,7 @@ __device__ __forceinline__ int clampi(int v, int lo, int hi) {
   return v < lo ? lo : (v > hi ? hi : v);
 }
 
-__global__ void k_bin_keys(const float *__restrict__ pos, int64_t n, float dx, int nx,
+__global__ void k_bin_keys(const float *__restrict__ pos, int64_t n, float dx, float inv, int nx,
                            int ny, int nz, int nty, int ntz, uint8_t *__restrict__ label,
                            int32_t *__restrict__ key, int32_t *__restrict__ rank,
                            int32_t *__restrict__ count, int64_t nkeys) {
@@ -38,10 +38,11 @@ __global__ void k_bin_keys(const float *__restrict__ pos, int64_t n, float dx, i
   unsigned amask = __ballot_sync(0xffffffffu, i < n);
   if (i >= n) return;
   float px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
-  // int(p / dx) with IEEE division and truncation toward zero, then clamped
-  int ci = clampi(__float2int_rz(__fdiv_rn(px, dx)), 0, nx - 1);
-  int cj = clampi(__float2int_rz(__fdiv_rn(py, dx)), 0, ny - 1);
-  int ck = clampi(__float2int_rz(__fdiv_rn(pz, dx)), 0, nz - 1);
+  // int(p / dx) with IEEE division (a product when dx is a power of two) and
+  // truncation toward zero, then clamped
+  int ci = clampi(__float2int_rz(div_dx(px, dx, inv)), 0, nx - 1);
+  int cj = clampi(__float2int_rz(div_dx(py, dx, inv)), 0, ny - 1);
+  int ck = clampi(__float2int_rz(div_dx(pz, dx, inv)), 0, nz - 1);
   int64_t cell = ((int64_t)ci * ny + cj) * nz + ck;
   if (GF_IN(cell, (int64_t)nx * ny * nz) && label[cell] != 2)
     label[cell] = 1;  // benign race: every writer stores 1
@@ -198,52 +199,48 @@ __global__ void k_place(const int32_t *__restrict__ key, const int32_t *__restri
   if (GF_IN(slot, n)) order[slot] = (int32_t)i;
 }
 
-// Sort each multi-particle cell segment of `order` by original particle id.
-constexpr int CANON_LOCAL = 48;
-__global__ void k_canon(const int32_t *__restrict__ count, const int32_t *__restrict__ start,
-                        int64_t nkeys, const int32_t *__restrict__ pid,
-                        int32_t *__restrict__ order, int64_t n) {
-  int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (q >= nkeys) return;
-  int cnt = count[q];
-  if (cnt < 2) return;
-  int s = start[q];
+// Canonical order of each cell segment, by original particle id: slot d of
+// the placement order (k_place, whose order within a cell follows the
+// atomics) moves to s + the number of its cell's particles with a smaller id
+// (ties, which unique ids never have, broken by index, so the result is a
+// permutation whatever the ids).  One thread per slot; its cell's ids are read
+// through the placement order, so a cell of c particles costs c^2 compares
+// spread over c threads.  The result goes to `canon` (the rank array, dead
+// after k_place).
+__global__ void k_canon(const int32_t *__restrict__ key, const int32_t *__restrict__ count,
+                        const int32_t *__restrict__ start, const int32_t *__restrict__ pid,
+                        const int32_t *__restrict__ order, int32_t *__restrict__ canon,
+                        int64_t n, int64_t nkeys) {
+  const int64_t d = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (d >= n) return;
+  const int32_t i = order[d];
+  if (!GF_IN(i, n)) return;
+  const int32_t k = key[i];
+  if (!GF_IN(k, nkeys)) return;
+  const int32_t s = start[k], cnt = count[k];
   if (!GF_IN(s, n) || !GF_IN((int64_t)s + cnt - 1, n)) return;
-  if (cnt <= CANON_LOCAL) {
-    int ids[CANON_LOCAL], idx[CANON_LOCAL];
-    for (int a = 0; a < cnt; ++a) {
-      int o = order[s + a];
-      int id = pid[o];
-      int b = a;
-      while (b > 0 && ids[b - 1] > id) {
-        ids[b] = ids[b - 1];
-        idx[b] = idx[b - 1];
-        --b;
-      }
-      ids[b] = id;
-      idx[b] = o;
-    }
-    for (int a = 0; a < cnt; ++a) order[s + a] = idx[a];
-  } else {  // rare crowded cell: in-place insertion sort in global memory
-    for (int a = 1; a < cnt; ++a) {
-      int o = order[s + a], id = pid[o], b = a;
-      while (b > 0 && pid[order[s + b - 1]] > id) {
-        order[s + b] = order[s + b - 1];
-        --b;
-      }
-      order[s + b] = o;
-    }
+  const int32_t id = pid[i];
+  int32_t r = 0;
+  for (int32_t a = 0; a < cnt; ++a) {
+    const int32_t j = order[s + a];
+    const int32_t pj = pid[j];
+    r += (pj < id || (pj == id && j < i)) ? 1 : 0;
   }
+  canon[s + r] = i;
 }
 
-__global__ void k_permute(const int32_t *__restrict__ order, int64_t n,
+// Sorted float4 records of the canonical order (canon), which also becomes
+// the context's order array for the later stages.
+__global__ void k_permute(const int32_t *__restrict__ canon, int64_t n,
                           const float *__restrict__ pos, const float *__restrict__ vel,
                           const float *__restrict__ C, const int32_t *__restrict__ pid,
                           float4 *__restrict__ rec0, float4 *__restrict__ rec1,
-                          float4 *__restrict__ rec2, float4 *__restrict__ rec3) {
+                          float4 *__restrict__ rec2, float4 *__restrict__ rec3,
+                          int32_t *__restrict__ order) {
   int64_t d = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (d >= n) return;
-  int64_t s = order[d];
+  int64_t s = canon[d];
+  order[d] = (int32_t)s;
   if (!GF_IN(s, n)) return;
   float4 a, b;
   a.x = pos[3 * s];
@@ -286,7 +283,8 @@ int launch_bin(Ctx *c, int transfer) {
                                               c->rank, c->count, c->ncell, c->nkeys);
     c->launches++;
   } else if (n > 0) {
-    k_bin_keys<<<nblk(n, 256), 256, 0, st>>>(c->p.pos, n, c->dx, c->nx, c->ny, c->nz,
+    k_bin_keys<<<nblk(n, 256), 256, 0, st>>>(c->p.pos, n, c->dx, exact_inverse(c->dx), c->nx,
+                                             c->ny, c->nz,
                                              c->nty, c->ntz, c->f.label, c->key, c->rank,
                                              c->count, c->nkeys);
     c->launches++;
@@ -300,11 +298,11 @@ int launch_bin(Ctx *c, int transfer) {
   c->launches += 3;
   if (n > 0) {
     k_place<<<nblk(n, 256), 256, 0, st>>>(c->key, c->rank, c->start, n, c->order);
-    k_canon<<<nblk(c->nkeys, 256), 256, 0, st>>>(c->count, c->start, c->nkeys, c->p.pid,
-                                                 c->order, n);
+    k_canon<<<nblk(n, 256), 256, 0, st>>>(c->key, c->count, c->start, c->p.pid, c->order,
+                                          c->rank, n, c->nkeys);
     const float *Cp = transfer == GF_APIC ? c->p.C : nullptr;
-    k_permute<<<nblk(n, 256), 256, 0, st>>>(c->order, n, c->p.pos, c->p.vel, Cp, c->p.pid,
-                                            c->rec0, c->rec1, c->rec2, c->rec3);
+    k_permute<<<nblk(n, 256), 256, 0, st>>>(c->rank, n, c->p.pos, c->p.vel, Cp, c->p.pid,
+                                            c->rec0, c->rec1, c->rec2, c->rec3, c->order);
     c->launches += 3;
   }
   return check_launch(c, "gf_bin");

@@ -79,10 +79,13 @@ __global__ void __launch_bounds__(256) k_coarse_tile_rows(CoarseSetup a,
 }
 
 // ---- cube regions of CT^3 tiles (the global-memory solver)
-// Flag the regions holding an active tile (the flags were zeroed).
+// Flag the regions holding an active tile.  The flags are zero between
+// set-ups (zeroed at allocation, cleared again by k_region_compact), and
+// neither kernel runs unless the gate (when given) is set.
 __global__ void k_region_flags(const int32_t *__restrict__ n_active,
                                const int32_t *__restrict__ tile_list, RegionGrid g,
-                               int32_t *__restrict__ flag) {
+                               int32_t *__restrict__ flag, const int *gate) {
+  if (gate != nullptr && *gate == 0) return;
   const int na = *n_active;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < na; s += gridDim.x * blockDim.x) {
     const int t = tile_list[s];
@@ -92,13 +95,15 @@ __global__ void k_region_flags(const int32_t *__restrict__ n_active,
 
 // Compact the flagged regions (one block): slot of each region (-1 when not
 // active), region of each slot, their count, and each slot's six
-// neighbouring slots.
+// neighbouring slots; the flags are cleared behind the read.
 __global__ void __launch_bounds__(1024) k_region_compact(RegionGrid g,
-                                                         const int32_t *__restrict__ flag,
+                                                         int32_t *__restrict__ flag,
                                                          int32_t *__restrict__ slot,
                                                          int32_t *__restrict__ list,
                                                          int32_t *__restrict__ count,
-                                                         int32_t *__restrict__ nbr) {
+                                                         int32_t *__restrict__ nbr,
+                                                         const int *gate) {
+  if (gate != nullptr && *gate == 0) return;
   __shared__ int s_base;
   __shared__ int s_warp[32];
   if (threadIdx.x == 0) s_base = 0;
@@ -107,6 +112,7 @@ __global__ void __launch_bounds__(1024) k_region_compact(RegionGrid g,
   for (int r0 = 0; r0 < g.n; r0 += blockDim.x) {
     const int r = r0 + threadIdx.x;
     const int f = r < g.n ? (flag[r] != 0) : 0;
+    if (r < g.n && f) flag[r] = 0;
     const unsigned m = __ballot_sync(0xffffffffu, f);
     if (lane == 0) s_warp[wid] = __popc(m);
     __syncthreads();
@@ -399,10 +405,9 @@ int coarse_setup_regions(Ctx *c, PcgState *st, const int *gate) {
   const RegionBufs b = region_bufs(c);
   int32_t *flag = b.flag, *slot = b.slot, *list = b.list, *count = b.count, *nbr = b.nbr,
           *rtiles = b.tiles;
-  int e = check_cuda(c, cudaMemsetAsync(flag, 0, (size_t)g.n * 4, c->stream), "zero region flags");
-  if (e) return e;
-  k_region_flags<<<c->num_sms * 4, 256, 0, c->stream>>>(c->n_active, c->tile_list, g, flag);
-  k_region_compact<<<1, 1024, 0, c->stream>>>(g, flag, slot, list, count, nbr);
+  k_region_flags<<<c->num_sms * 4, 256, 0, c->stream>>>(c->n_active, c->tile_list, g, flag,
+                                                        gate);
+  k_region_compact<<<1, 1024, 0, c->stream>>>(g, flag, slot, list, count, nbr, gate);
   const CoarseSetup a =
       coarse_args(c, count, list, nbr, st, COARSE_RMAX, gate, COARSE_KIND_REGIONS);
   k_region_rows<<<COARSE_RMAX, 256, 0, c->stream>>>(a, g, c->tile_slot, c->code, rtiles,

@@ -346,6 +346,32 @@ struct RegionBufs {
 RegionBufs region_bufs(Ctx *c);
 int check_launch(Ctx *c, const char *what);
 
+// 1/dx when dx is a power of two, so that x * (1/dx) is x / dx exactly; 0
+// otherwise (the IEEE division is used then).
+__host__ __device__ inline float exact_inverse(float dx) {
+  int e;
+  return (dx > 0.f && frexpf(dx, &e) == 0.5f) ? 1.0f / dx : 0.0f;
+}
+// x / dx rounded as the IEEE division: a product when inv (exact_inverse(dx))
+// is non-zero.
+__device__ __forceinline__ float div_dx(float x, float dx, float inv) {
+  return inv != 0.0f ? x * inv : __fdiv_rn(x, dx);
+}
+
+// Cell (li * 8 + lj) * 8 + lk of colour c ((li + lj + lk) & 1 == c) that
+// thread k (0..255) of a red-black half-sweep updates.  Warp w = k >> 5 takes
+// planes li = (w & 3) + {0, 4}, rows lj = 2 (w >> 2) + {0, 1, 4, 5} and the
+// four cells of the colour in each row, so that in a 10^3 padded box (plane
+// pitch 100, row pitch 10) the warp's 32 cells -- and each of their six
+// neighbours -- fall in 32 distinct shared-memory banks.
+__device__ __forceinline__ int sgs_color_cell(int k, int c) {
+  const int w = k >> 5, ln = k & 31, b = (ln >> 2) & 3;
+  const int li = (w & 3) + 4 * (ln >> 4);
+  const int lj = 2 * (w >> 2) + (b & 1) + 4 * (b >> 1);
+  const int lk = 2 * (ln & 3) + ((li + lj + c) & 1);
+  return (li * 8 + lj) * 8 + lk;
+}
+
 __host__ __device__ inline int64_t uidx(int i, int j, int k, int ny, int nz) {
   return ((int64_t)i * ny + j) * nz + k;
 }

@@ -511,38 +511,52 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   // Phases of an iteration for the trace (block thread 0's view, cycles):
   // 0 own update, 1 SGS sweeps, 2 halo publication + neighbour flags +
   // in-block rings, 3 remote rings, 4 stencil and dot products, 5 grid
-  // all-reduce (with the barrier before it).  s_ph[6] holds the last stamp.
-  __shared__ long long s_ph[7];
+  // all-reduce (with the barrier before it), 6 coarse gather of the tiles'
+  // residual sums (the wait for their publication), 7 coarse e = B g and its
+  // addition to z.  s_ph[8] holds the last stamp.
+  __shared__ long long s_ph[9];
   if (threadIdx.x == 0)
-    for (int k = 0; k < 7; ++k) s_ph[k] = k < 6 ? 0 : clock64();
+    for (int k = 0; k < 9; ++k) s_ph[k] = k < 8 ? 0 : clock64();
   auto phase_mark = [&](int k) {
     if (a.trace && threadIdx.x == 0) {
       const long long now = clock64();
-      s_ph[k] += now - s_ph[6];
-      s_ph[6] = now;
+      s_ph[k] += now - s_ph[8];
+      s_ph[8] = now;
     }
   };
   if (G > SM_MAXG) {
     if (threadIdx.x == 0) atomicExch(&st->error, 1);
     return;
   }
-  unsigned char *pb = smem;
-  double *s_x64 = reinterpret_cast<double *>(pb);
-  if (REF) pb += (size_t)MAXT * 4096;
-  float *s_x = reinterpret_cast<float *>(pb);
-  float *s_r = s_x + MAXT * 512;
-  float *s_d = s_r + MAXT * 512;
-  float *s_s = s_d + MAXT * 512;
-  float *s_w = s_s + MAXT * 512;
-  float *s_zb = s_w + MAXT * 512;  // padded z boxes, 1000 per tile
-  uint16_t *s_code = reinterpret_cast<uint16_t *>(s_zb + MAXT * 1000);
-  uint8_t *s_rdiag = reinterpret_cast<uint8_t *>(s_code + MAXT * 512);  // 384 per tile
-
-  // the z boxes are not yet in use: borrow them for the partition prefix
-  partition_slots(a.tile_cost, na, MAXT, reinterpret_cast<int *>(s_zb), s_bounds);
+  // the per-cell arrays are not yet in use: borrow their memory for the
+  // partition prefix
+  partition_slots(a.tile_cost, na, MAXT, reinterpret_cast<int *>(smem), s_bounds);
   const int b0 = s_bounds[blockIdx.x], b1 = s_bounds[blockIdx.x + 1];
   const int nt = b1 - b0;
   const int64_t q0 = (int64_t)b0 * 512;
+  // per-cell arrays pitched by this block's tile count, so that the memory of
+  // its MAXT - nt unused tiles is one free region at the end (16-byte aligned:
+  // every array's size per tile is a multiple of 16 bytes)
+  unsigned char *pb = smem;
+  double *s_x64 = reinterpret_cast<double *>(pb);
+  if (REF) pb += (size_t)nt * 4096;
+  float *s_x = reinterpret_cast<float *>(pb);
+  float *s_r = s_x + nt * 512;
+  float *s_d = s_r + nt * 512;
+  float *s_s = s_d + nt * 512;
+  float *s_w = s_s + nt * 512;
+  // w doubles as the gathered coarse residual sums (one per active tile,
+  // rounded up to 8), so it spans at least that many floats; the layout still
+  // fits, since a block holding fewer than MAXT tiles has a whole free tile
+  // (over 19 KB) and the sums take at most 160 * 14 floats (8.75 KB)
+  const int wlen = nt * 512 > ((na + 7) & ~7) ? nt * 512 : ((na + 7) & ~7);
+  float *s_zb = s_w + wlen;  // padded z boxes, 1000 per tile
+  uint16_t *s_code = reinterpret_cast<uint16_t *>(s_zb + nt * 1000);
+  uint8_t *s_rdiag = reinterpret_cast<uint8_t *>(s_code + nt * 512);  // 384 per tile
+  unsigned char *const s_free = s_rdiag + nt * 384;
+  const size_t used = (size_t)(s_free - smem);
+  const size_t free_bytes = used < Cfg::BYTES ? Cfg::BYTES - used : 0;
+  static_assert(Cfg::TILE_BYTES % 16 == 0, "free region alignment");
 
   const int l = threadIdx.x & 511, tl0 = threadIdx.x >> 9;
   const int pc = pad_of(l);
@@ -560,6 +574,18 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
                    (int64_t)reinterpret_cast<const CoarseMeta *>(a.cbuf + COARSE_META_OFF)->parity *
                        CRMAX * CRMAX
              : nullptr;
+  // this block's rows of B (R8 bf16 each), copied once into the free region
+  // when they fit, so that e = B g reads shared memory instead of L2
+  const int R8c = (na + 7) & ~7;
+  const bool b_smem = coarse && (size_t)nt * R8c * 2 <= free_bytes;
+  uint4 *const s_B = reinterpret_cast<uint4 *>(s_free);
+  if (b_smem) {
+    const int nch = R8c >> 3;
+    for (int i = threadIdx.x; i < nt * nch; i += blockDim.x) {
+      const int jr = i / nch, ch = i - jr * nch;
+      s_B[i] = __ldg(reinterpret_cast<const uint4 *>(Bh + (int64_t)(b0 + jr) * CRMAX) + ch);
+    }
+  }
 
   for (int i = threadIdx.x; i < nt * 6; i += blockDim.x) s_nbr[i] = a.nbr[(int64_t)b0 * 6 + i];
   for (int i = threadIdx.x; i < nt * 1000; i += blockDim.x) s_zb[i] = 0.f;
@@ -670,9 +696,10 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   // (z = r/D) is the z = r/D every caller writes for all fluid cells; then
   // per sweep black, red.  Callers also zero the boxes' rings, and non-fluid
   // cells hold 0, so a half-sweep is the branch-free six-neighbour sum with a
-  // per-cell factor (0 on non-fluid cells).  It maps thread t to the
-  // (t & 255)-th cell of the colour in tiles (t >> 8) + 4i, so all threads
-  // work.  The result is published on the halo cells as 64-bit words, the
+  // per-cell factor (0 on non-fluid cells).  It maps thread t to cell
+  // sgs_color_cell(t & 255) of the colour (bank-conflict-free in the boxes)
+  // in tiles (t >> 8) + 4i, so all threads work.  The result is published on
+  // the halo cells as 64-bit words, the
   // float's bits under a 32-bit publication count (relaxed stores: the word
   // is its own flag, no fence), and the ring of another block's tile is
   // loaded until the count matches (bounded).  The words are zeroed before
@@ -681,10 +708,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   unsigned long long zep = 0;  // z publications, the same sequence in every block
   unsigned long long *const HZ = reinterpret_cast<unsigned long long *>(a.hr0);
   auto half_sweep = [&](int c) {  // z = (r + in-tile fluid neighbours' z) / D, colour c
-    const int k = threadIdx.x & 255;
-    const int li = k >> 5, lj = (k >> 2) & 7;
-    const int lk = 2 * (k & 3) + ((li + lj + c) & 1);
-    const int lc = (li * 8 + lj) * 8 + lk;
+    const int lc = sgs_color_cell(threadIdx.x & 255, c);
     const int pcc = pad_of(lc);
     for (int tl = threadIdx.x >> 8; tl < nt; tl += 4) {
       const int L = tl * 512 + lc;
@@ -751,6 +775,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       half_sweep(0);
       __syncthreads();
     }
+    phase_mark(1);
     if (CRS && coarse) {
       if (sgs == 0) prefetch();
       const unsigned long long tag = (gep + 1ull) << 32;
@@ -778,36 +803,51 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       }
       ++gep;
       __syncthreads();
+      phase_mark(6);
       // e_t = B_t . g: row b0 + jr is summed by warps jr, jr + nt, ... (the
       // lanes over 8-column chunks), then the warps' partials in warp order
       float v = 0.f;
       if (nt > 0) {
         const int jr = wid % nt, iw = wid / nt, nw = (31 - jr) / nt + 1;
-        const uint4 *row = reinterpret_cast<const uint4 *>(Bh + (int64_t)(b0 + jr) * CRMAX);
-        for (int ch = iw * 32 + lane; ch < (R8 >> 3); ch += nw * 32) {
-          const uint4 q = __ldg(row + ch);
+        const uint4 *row = b_smem ? s_B + jr * (R8 >> 3)
+                                  : reinterpret_cast<const uint4 *>(Bh + (int64_t)(b0 + jr) * CRMAX);
+        auto ldB = [&](int ch) -> uint4 { return b_smem ? row[ch] : __ldg(row + ch); };
+        auto dot8 = [&](const uint4 q, int ch) {
           const float *gp = s_g + ch * 8;
           v += __uint_as_float(q.x << 16) * gp[0] + __uint_as_float(q.x & 0xffff0000u) * gp[1];
           v += __uint_as_float(q.y << 16) * gp[2] + __uint_as_float(q.y & 0xffff0000u) * gp[3];
           v += __uint_as_float(q.z << 16) * gp[4] + __uint_as_float(q.z & 0xffff0000u) * gp[5];
           v += __uint_as_float(q.w << 16) * gp[6] + __uint_as_float(q.w & 0xffff0000u) * gp[7];
+        };
+        // two chunks in flight per lane, so a lane's loads wait one L2 trip
+        const int nch = R8 >> 3, step = nw * 32;
+        int ch = iw * 32 + lane;
+        for (; ch + step < nch; ch += 2 * step) {
+          const uint4 q0 = ldB(ch), q1 = ldB(ch + step);
+          dot8(q0, ch);
+          dot8(q1, ch + step);
         }
+        if (ch < nch) dot8(ldB(ch), ch);
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
       if (lane == 0) s_ep[wid] = v;
       __syncthreads();
+      // lane t < nt of every warp sums e_t from the warps' partials (in warp
+      // order); a thread's tiles tl0 + 2j are the same across its warp, so
+      // each takes its e_t from lane tl by a shuffle
+      float e_lane = 0.f;
+      if (lane < nt)
+        for (int w = lane; w < 32; w += nt) e_lane += s_ep[w];
 #pragma unroll
-      for (int j = 0; j < MAXJ; ++j)
-        if ((fmask >> j) & 1) {
-          const int tl = tl0 + 2 * j;
-          float e = 0.f;
-          for (int w = tl; w < 32; w += nt) e += s_ep[w];
-          s_zb[tl * 1000 + pc] += e;
-        }
+      for (int j = 0; j < MAXJ; ++j) {
+        const int tl = tl0 + 2 * j;
+        const float e = __shfl_sync(0xffffffffu, e_lane, tl & 31);
+        if ((fmask >> j) & 1) s_zb[tl * 1000 + pc] += e;
+      }
       __syncthreads();
     }
-    phase_mark(1);
+    phase_mark(7);
     ++zep;
     const unsigned long long tag = zep << 32;
 #pragma unroll
@@ -1017,12 +1057,12 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       int remote = 0;
       for (int f = 0; f < nt * 6; ++f)
         if (s_nbr[f] >= 0 && !(s_nbr[f] >= b0 && s_nbr[f] < b1)) ++remote;
-      long long *t = gs.trace + a.trace_cap / 2 + 10 * blockIdx.x;
+      long long *t = gs.trace + a.trace_cap / 2 + 12 * blockIdx.x;
       t[0] = gs.busy;
       t[1] = nt;
       t[2] = s_nf;
       t[3] = remote;
-      for (int k = 0; k < 6; ++k) t[4 + k] = s_ph[k];
+      for (int k = 0; k < 8; ++k) t[4 + k] = s_ph[k];
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {

@@ -385,11 +385,9 @@ __device__ __forceinline__ float sgs_factor(unsigned code) {  // 1 / max(D, 1) o
   return (code & CODE_FLUID) ? 1.0f / fmaxf((float)((code >> CODE_DIAG_SHIFT) & 7), 1.0f) : 0.0f;
 }
 // z = (r + the in-tile fluid neighbours' z) / D on colour c of the round's
-// tiles (thread t: the (t & 255)-th cell of the colour in tiles t >> 8, +2).
+// tiles (thread t: cell sgs_color_cell(t & 255, c) in tiles t >> 8, +2).
 __device__ __forceinline__ void sgs_half(SgsSmem &S, int c) {
-  const int k = threadIdx.x & 255;
-  const int li = k >> 5, lj = (k >> 2) & 7, lk = 2 * (k & 3) + ((li + lj + c) & 1);
-  const int lc = (li * 8 + lj) * 8 + lk, pc = tile_pad(lc);
+  const int lc = sgs_color_cell(threadIdx.x & 255, c), pc = tile_pad(lc);
   for (int m = threadIdx.x >> 8; m < SGS_TB; m += PCG_THREADS / 256) {
     float *zp = S.zb + m * 1000 + pc;
     float acc = S.r[m * 512 + lc];
@@ -1674,6 +1672,7 @@ int pressure_alloc(Ctx *c) {
     const int64_t ni = 2 * (int64_t)g.n + COARSE_RMAX + 4 + (int64_t)COARSE_RMAX * 6 +
                        (int64_t)COARSE_RMAX * g.ct * g.ct * g.ct + c->ntiles;
     if ((e = A((void **)&c->rg_buf, (size_t)ni * 4, "alloc coarse regions")) ||
+        (e = check_cuda(c, cudaMemset(c->rg_buf, 0, (size_t)g.n * 4), "zero region flags")) ||
         (e = A((void **)&c->rg_gt, (size_t)c->ntiles * 4, "alloc tile residual sums")) ||
         (e = A((void **)&c->rg_e, (size_t)COARSE_RMAX * 4, "alloc region corrections")))
       return e;

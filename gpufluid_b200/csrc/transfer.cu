@@ -49,7 +49,9 @@ struct P2GArgs {
   float *u, *v, *w, *uw, *vw, *ww;
   float dx;
   int nx, ny, nz, nty, ntz;
+  float inv_dx_exact;  // exact_inverse(dx)
 };
+
 
 // Scatter one face component of one particle into the shared box of `comp`
 // (0 u, 1 v, 2 w).  APIC adds C_row . (x_face - x_p) with world face
@@ -224,7 +226,7 @@ __device__ __forceinline__ void p2g_cell_comp(const P2GArgs &a, T *s_val, T *s_w
   constexpr float HX = COMP == 0 ? 0.0f : 0.5f, HY = COMP == 1 ? 0.0f : 0.5f,
                   HZ = COMP == 2 ? 0.0f : 0.5f;
   const int xo = ci - (COMP != 0), yo = cj - (COMP != 1), zo = ck - (COMP != 2);
-  const float dx = a.dx;
+  const float dx = a.dx, inv = a.inv_dx_exact;
   float av[EX * EY * EZ], aw[EX * EY * EZ];
 #pragma unroll
   for (int m = 0; m < EX * EY * EZ; ++m) av[m] = aw[m] = 0.0f;
@@ -241,8 +243,11 @@ __device__ __forceinline__ void p2g_cell_comp(const P2GArgs &a, T *s_val, T *s_w
       const float4 r1 = a.rec1[q];
       vp = COMP == 0 ? r1.x : (COMP == 1 ? r1.y : r1.z);
     }
-    const float fx = __fdiv_rn(r0.x, dx) - HX, fy = __fdiv_rn(r0.y, dx) - HY,
-                fz = __fdiv_rn(r0.z, dx) - HZ;
+    // x / dx: a product when dx is a power of two (exact), else the division
+    const float gx = div_dx(r0.x, dx, inv);
+    const float gy = div_dx(r0.y, dx, inv);
+    const float gz = div_dx(r0.z, dx, inv);
+    const float fx = gx - HX, fy = gy - HY, fz = gz - HZ;
     const int i0 = __float2int_rz(floorf(fx)), j0 = __float2int_rz(floorf(fy)),
               k0 = __float2int_rz(floorf(fz));
     const int rx = i0 - xo, ry = j0 - yo, rz = k0 - zo;
@@ -270,18 +275,23 @@ __device__ __forceinline__ void p2g_cell_comp(const P2GArgs &a, T *s_val, T *s_w
       wz[m] = m == rz ? 1.0f - sz : (m == rz + 1 ? sz : 0.0f);
       C[m] = APIC ? c2 * (((float)(zo + m) + HZ) * dx - r0.z) : 0.0f;
     }
+    // face (x, y, z) gains (A_x + B_y + C_z) wx wy wz, summed as
+    // (wxy (A_x + B_y)) wz + wxy (C_z wz) with wxy = wx wy, and weight wxy wz
+    float D[EZ];
+#pragma unroll
+    for (int z = 0; z < EZ; ++z) D[z] = C[z] * wz[z];
 #pragma unroll
     for (int x = 0; x < EX; ++x)
 #pragma unroll
       for (int y = 0; y < EY; ++y) {
         const float wxy = wx[x] * wy[y];
-        const float ab = A[x] + B[y];
+        const float P = wxy * (A[x] + B[y]);
 #pragma unroll
         for (int z = 0; z < EZ; ++z) {
           const int m = (x * EY + y) * EZ + z;
-          const float wt = wxy * wz[z];
-          av[m] = __fmaf_rn(ab + C[z], wt, av[m]);
-          aw[m] += wt;
+          av[m] = __fmaf_rn(P, wz[z], av[m]);
+          if (APIC) av[m] = __fmaf_rn(wxy, D[z], av[m]);
+          aw[m] = __fmaf_rn(wxy, wz[z], aw[m]);
         }
       }
   }
@@ -404,6 +414,143 @@ __device__ __forceinline__ void p2g_cell_comp_staged(const P2GArgs &a, T *s_val,
       }
 }
 
+// Lane maps 4 and 5: the cells of map 2, with the particles staged in
+// rounds of up to K (8 or 4) per cell by the whole warp.  In a round, slot s
+// of cell l holds the cell's (K r + s)-th particle; the warp loads the slots
+// in K steps of 32 / K cells, lane j of step t taking slot j % K of cell
+// (32 / K) t + j / K, so a load instruction reads 32 / K runs of K
+// consecutive sorted particles.  Slot s of cell l lives at s * 32 + (l ^
+// (32 / K) s) of each field's plane: a step's stores and a lane's reads of its
+// own cell (all lanes at one slot) both fall in 32 distinct banks.  One face
+// component at a time (its register sums live across the rounds), each
+// staged field being one of: the grid coordinates x/dx, y/dx, z/dx (unshifted),
+// v_c, and for APIC the row c of C.  The APIC offsets are formed in grid units,
+// (face - x/dx) dx, so the world position is not staged.
+template <bool APIC>
+__host__ __device__ constexpr int p2g_round_fields() { return APIC ? 7 : 4; }
+template <int K>
+__device__ __forceinline__ int p2g_round_slot(int cell, int s) {
+  return s * 32 + (cell ^ ((32 / K) * s));
+}
+template <bool APIC, int KT, int COMP, int K, typename T>
+__device__ __forceinline__ void p2g_cell_comp_rounds(const P2GArgs &a, T *s_val, T *s_wt,
+                                                     float *st, int64_t first, int cnt,
+                                                     int maxcnt, int ci, int cj, int ck, int I0,
+                                                     int J0, int K0) {
+  constexpr int EX = COMP == 0 ? 2 : 3, EY = COMP == 1 ? 2 : 3, EZ = COMP == 2 ? 2 : 3;
+  constexpr float HX = COMP == 0 ? 0.0f : 0.5f, HY = COMP == 1 ? 0.0f : 0.5f,
+                  HZ = COMP == 2 ? 0.0f : 0.5f;
+  constexpr int PL = K * 32;  // slots of a field's plane
+  const int lane = threadIdx.x & 31;
+  const int xo = ci - (COMP != 0), yo = cj - (COMP != 1), zo = ck - (COMP != 2);
+  const float dx = a.dx, inv = a.inv_dx_exact;
+  const float4 *recc = APIC ? (COMP == 0 ? a.rec1 : (COMP == 1 ? a.rec2 : a.rec3)) : a.rec1;
+  float av[EX * EY * EZ], aw[EX * EY * EZ];
+#pragma unroll
+  for (int m = 0; m < EX * EY * EZ; ++m) av[m] = aw[m] = 0.0f;
+  for (int kb = 0; kb < maxcnt; kb += K) {
+    __syncwarp();
+    // ---- stage the round: K steps of 32 / K cells
+#pragma unroll
+    for (int t = 0; t < K; ++t) {
+      const int cc = (32 / K) * t + lane / K, s = lane % K;
+      const int64_t fc = __shfl_sync(0xffffffffu, first, cc);
+      const int nc = __shfl_sync(0xffffffffu, cnt, cc);
+      if (kb + s < nc) {
+        const int64_t q = fc + kb + s;
+        const float4 r0 = a.rec0[q], rc = recc[q];
+        const int o = p2g_round_slot<K>(cc, s);
+        st[0 * PL + o] = div_dx(r0.x, dx, inv);
+        st[1 * PL + o] = div_dx(r0.y, dx, inv);
+        st[2 * PL + o] = div_dx(r0.z, dx, inv);
+        if (APIC) {  // record 1 + c: (v_c, C row c)
+          st[3 * PL + o] = rc.x;
+          st[4 * PL + o] = rc.y;
+          st[5 * PL + o] = rc.z;
+          st[6 * PL + o] = rc.w;
+        } else {
+          st[3 * PL + o] = COMP == 0 ? rc.x : (COMP == 1 ? rc.y : rc.z);
+        }
+      }
+    }
+    __syncwarp();
+    // ---- this lane's cell: its particles kb .. kb + K - 1
+#pragma unroll 1
+    for (int s = 0; s < K; ++s) {
+      if (kb + s >= cnt) break;
+      const int o = p2g_round_slot<K>(lane, s);
+      const float gx = st[0 * PL + o], gy = st[1 * PL + o], gz = st[2 * PL + o];
+      const float fx = gx - HX, fy = gy - HY, fz = gz - HZ;
+      const float vp = st[3 * PL + o];
+      float c0 = 0.f, c1 = 0.f, c2 = 0.f;
+      if (APIC) {
+        c0 = st[4 * PL + o];
+        c1 = st[5 * PL + o];
+        c2 = st[6 * PL + o];
+      }
+      const int i0 = __float2int_rz(floorf(fx)), j0 = __float2int_rz(floorf(fy)),
+                k0 = __float2int_rz(floorf(fz));
+      const int rx = i0 - xo, ry = j0 - yo, rz = k0 - zo;
+      if (rx < 0 || rx + 2 > EX || ry < 0 || ry + 2 > EY || rz < 0 || rz + 2 > EZ) {
+        // outside the cell's pattern (a position outside the grid): the
+        // general scatter, with the world position rebuilt from the record
+        const float4 r0 = a.rec0[first + kb + s];
+        float *gv = COMP == 0 ? a.u : (COMP == 1 ? a.v : a.w);
+        float *gw = COMP == 0 ? a.uw : (COMP == 1 ? a.vw : a.ww);
+        scatter_comp<APIC, KT, T>(s_val, s_wt, COMP, vp, c0, c1, c2, r0.x, r0.y, r0.z, fx, fy,
+                                  fz, I0, J0, K0, a, gv, gw);
+        continue;
+      }
+      const float sx = fx - (float)i0, sy = fy - (float)j0, sz = fz - (float)k0;
+      float wx[EX], wy[EY], wz[EZ], A[EX], B[EY], C[EZ];
+#pragma unroll
+      for (int m = 0; m < EX; ++m) {
+        wx[m] = m == rx ? 1.0f - sx : (m == rx + 1 ? sx : 0.0f);
+        A[m] = APIC ? __fmaf_rn(c0, (((float)(xo + m) + HX) - gx) * dx, vp) : vp;
+      }
+#pragma unroll
+      for (int m = 0; m < EY; ++m) {
+        wy[m] = m == ry ? 1.0f - sy : (m == ry + 1 ? sy : 0.0f);
+        B[m] = APIC ? c1 * ((((float)(yo + m) + HY) - gy) * dx) : 0.0f;
+      }
+#pragma unroll
+      for (int m = 0; m < EZ; ++m) {
+        wz[m] = m == rz ? 1.0f - sz : (m == rz + 1 ? sz : 0.0f);
+        C[m] = APIC ? c2 * ((((float)(zo + m) + HZ) - gz) * dx) : 0.0f;
+      }
+#pragma unroll
+      for (int x = 0; x < EX; ++x)
+#pragma unroll
+        for (int y = 0; y < EY; ++y) {
+          const float wxy = wx[x] * wy[y];
+          const float ab = A[x] + B[y];
+#pragma unroll
+          for (int z = 0; z < EZ; ++z) {
+            const int m = (x * EY + y) * EZ + z;
+            const float wt = wxy * wz[z];
+            av[m] = __fmaf_rn(ab + C[z], wt, av[m]);
+            aw[m] += wt;
+          }
+        }
+    }
+  }
+  const int ey = COMP == 1 ? BOX_N : BOX_T, ez = p2g_ez(COMP, KT);
+  const int e0 = ((ci - I0) * ey + (cj - J0)) * ez + (ck - K0);
+#pragma unroll
+  for (int x = 0; x < EX; ++x)
+#pragma unroll
+    for (int y = 0; y < EY; ++y)
+#pragma unroll
+      for (int z = 0; z < EZ; ++z) {
+        const int m = (x * EY + y) * EZ + z;
+        if (aw[m] == 0.0f) continue;
+        const int e = e0 + (x * ey + y) * ez + z;
+        if (!GF_IN(e, P2G_BOXK(KT))) continue;
+        atomicAdd(&s_val[e], (T)av[m]);
+        atomicAdd(&s_wt[e], (T)aw[m]);
+      }
+}
+
 // One block's P2G: t is its first tile within the grid (the block's
 // coordinates), key0 the sort key of that tile's first cell (t * 512 for a
 // single grid), ntk (<= KT) the tiles it holds along k, which are consecutive
@@ -437,7 +584,34 @@ __device__ __forceinline__ void p2g_tile_body(const P2GArgs &a, int t, int64_t k
   //  2: the cells of 1, each lane summing its cell's particles in registers
   //     first, one component at a time (p2g_cell_comp);
   //  3: map 2 reading the particles from a warp-private staging area filled
-  //     with coalesced loads (p2g_cell_comp_staged).
+  //     with coalesced loads (p2g_cell_comp_staged);
+  //  4, 5: map 2 over rounds of 8 or 4 particles per cell, staged by the
+  //     warp in bank-conflict-free slots (p2g_cell_comp_rounds).
+  if (MAP == 4 || MAP == 5) {
+    constexpr int K = MAP == 4 ? 8 : 4;
+    const int lane4 = threadIdx.x & 31, warp4 = threadIdx.x >> 5;
+    float *st = reinterpret_cast<float *>(s_wt + 3 * BK) +
+                warp4 * p2g_round_fields<APIC>() * K * 32;
+    for (int g4 = warp4; g4 < ntk * (TILE_CELLS / 32); g4 += blockDim.x >> 5) {
+      const int cl = g4 * 32 + lane4;
+      const int64_t key = key0 + cl;
+      const int64_t first = a.start[key];
+      const int cnt = (int)(a.start[key + 1] - first);
+      const int maxcnt = (int)__reduce_max_sync(0xffffffffu, (unsigned)cnt);
+      if (maxcnt == 0) continue;
+      const int l = cl & (TILE_CELLS - 1);
+      const int ci = I0 + (l >> 6), cj = J0 + ((l >> 3) & 7), ck = K0 + (cl >> 9) * TILE + (l & 7);
+      p2g_cell_comp_rounds<APIC, KT, 0, K, T>(a, s_val, s_wt, st, first, cnt, maxcnt, ci, cj, ck,
+                                              I0, J0, K0);
+      p2g_cell_comp_rounds<APIC, KT, 1, K, T>(a, s_val + BK, s_wt + BK, st, first, cnt, maxcnt,
+                                              ci, cj, ck, I0, J0, K0);
+      p2g_cell_comp_rounds<APIC, KT, 2, K, T>(a, s_val + 2 * BK, s_wt + 2 * BK, st, first, cnt,
+                                              maxcnt, ci, cj, ck, I0, J0, K0);
+    }
+    __syncthreads();
+    p2g_flush_box<KT, T>(a, s_val, s_wt, I0, J0, K0);
+    return;
+  }
   if (MAP == 3) {
     const int lane3 = threadIdx.x & 31, warp3 = threadIdx.x >> 5;
     constexpr int NF = p2g_stage_fields(APIC);
@@ -459,9 +633,9 @@ __device__ __forceinline__ void p2g_tile_body(const P2GArgs &a, int t, int64_t k
         for (int i = lane3; i < n; i += 32) {
           const int64_t q = c0 + i;
           const float4 r0 = a.rec0[q], r1 = a.rec1[q];
-          st[0 * P2G_CH + i] = __fdiv_rn(r0.x, dx);
-          st[1 * P2G_CH + i] = __fdiv_rn(r0.y, dx);
-          st[2 * P2G_CH + i] = __fdiv_rn(r0.z, dx);
+          st[0 * P2G_CH + i] = div_dx(r0.x, dx, a.inv_dx_exact);
+          st[1 * P2G_CH + i] = div_dx(r0.y, dx, a.inv_dx_exact);
+          st[2 * P2G_CH + i] = div_dx(r0.z, dx, a.inv_dx_exact);
           if (APIC) {  // records 1..3: (v_c, C row c)
             const float4 r2 = a.rec2[q], r3 = a.rec3[q];
             const float f[15] = {r1.x, r2.x, r3.x, r0.x, r0.y, r0.z, r1.y, r1.z,
@@ -553,7 +727,8 @@ __device__ __forceinline__ void p2g_tile_body(const P2GArgs &a, int t, int64_t k
       r2 = a.rec2[q];
       r3 = a.rec3[q];
     }
-    float gx = __fdiv_rn(r0.x, a.dx), gy = __fdiv_rn(r0.y, a.dx), gz = __fdiv_rn(r0.z, a.dx);
+    const float inv = a.inv_dx_exact;
+    float gx = div_dx(r0.x, a.dx, inv), gy = div_dx(r0.y, a.dx, inv), gz = div_dx(r0.z, a.dx, inv);
     float hx = gx - 0.5f, hy = gy - 0.5f, hz = gz - 0.5f;
     // component c: velocity and C row.  APIC: record 1 + c holds (v_c, C row
     // c); FLIP/PIC: record 1 holds (vx, vy, vz)
@@ -581,7 +756,11 @@ __device__ __forceinline__ void p2g_tile_body(const P2GArgs &a, int t, int64_t k
 // staging areas of its 8 warps.
 __host__ __device__ constexpr size_t p2g_smem_bytes(int KT, int map = 0, bool apic = true) {
   return 2 * 3 * (size_t)P2G_BOXK(KT) * sizeof(P2G_ACC) +
-         (map == 3 ? (size_t)8 * p2g_stage_fields(apic) * P2G_CH * sizeof(float) : 0);
+         (map == 3 ? (size_t)8 * p2g_stage_fields(apic) * P2G_CH * sizeof(float) : 0) +
+         (map == 4 || map == 5
+              ? (size_t)8 * (apic ? p2g_round_fields<true>() : p2g_round_fields<false>()) *
+                    (map == 4 ? 8 : 4) * 32 * sizeof(float)
+              : 0);
 }
 
 // One CTA per block of KT tiles along k: block b holds tiles (ti, tj, KT*kb
@@ -991,14 +1170,15 @@ struct G2PArgs {
   int64_t n;
   float dx, dt, flip_blend, dom0, dom1, dom2;
   int nx, ny, nz;
+  float inv_dx_exact;  // exact_inverse(dx)
 };
 
 template <bool APIC>
 __device__ __forceinline__ void g2p_particle(const G2PArgs &a, int64_t q) {
   const float4 r0 = a.rec0[q];
   const float px = r0.x, py = r0.y, pz = r0.z;
-  const float dx = a.dx;
-  float gx = __fdiv_rn(px, dx), gy = __fdiv_rn(py, dx), gz = __fdiv_rn(pz, dx);
+  const float dx = a.dx, idx = a.inv_dx_exact;
+  float gx = div_dx(px, dx, idx), gy = div_dx(py, dx, idx), gz = div_dx(pz, dx, idx);
   float hx = gx - 0.5f, hy = gy - 0.5f, hz = gz - 0.5f;
   float nu, nv, nw;
   if (APIC) {
@@ -1281,7 +1461,8 @@ __global__ void __launch_bounds__(G2P_TILE_THREADS)
       const int64_t q = base + tid;
       const float4 r0 = a.rec0[q];
       const float px = r0.x, py = r0.y, pz = r0.z;
-      float gx = __fdiv_rn(px, dx), gy = __fdiv_rn(py, dx), gz = __fdiv_rn(pz, dx);
+      float gx = div_dx(px, dx, a.inv_dx_exact), gy = div_dx(py, dx, a.inv_dx_exact),
+            gz = div_dx(pz, dx, a.inv_dx_exact);
       float hx = gx - 0.5f, hy = gy - 0.5f, hz = gz - 0.5f;
       float nu, nv, nw;
       if (APIC) {
@@ -1459,7 +1640,8 @@ __global__ void __launch_bounds__(256, MAP >= 2 ? GF_P2G_MINB : 1) kb_p2g_tile(B
   const int s = seg_find(b.sx.tile0, b.sx.n, t);
   const SegRow r = b.sx.row[s];
   P2GArgs a{b.start, b.rec0, b.rec1, b.rec2, b.rec3, b.u + r.fu0, b.v + r.fv0, b.w + r.fw0,
-            b.uw + r.fu0, b.vw + r.fv0, b.ww + r.fw0, r.dx, r.nx, r.ny, r.nz, r.nty, r.ntz};
+            b.uw + r.fu0, b.vw + r.fv0, b.ww + r.fw0, r.dx, r.nx, r.ny, r.nz, r.nty, r.ntz,
+            exact_inverse(r.dx)};
   p2g_tile_body<APIC, 1, MAP>(a, (int)(t - r.tile0), t * TILE_CELLS, 1);
 }
 
@@ -1503,7 +1685,7 @@ __global__ void __launch_bounds__(512) kb_g2p(BatchArgs b) {
   const SegRow r = b.sx.row[s];
   G2PArgs a{b.rec0, b.rec1, b.u + r.fu0, b.v + r.fv0, b.w + r.fw0, b.us + r.fu0,
             b.vs + r.fv0, b.ws + r.fw0, b.pos, b.vel, b.C, b.pid, b.n, r.dx, b.dt,
-            b.flip_blend, r.dom0, r.dom1, r.dom2, r.nx, r.ny, r.nz};
+            b.flip_blend, r.dom0, r.dom1, r.dom2, r.nx, r.ny, r.nz, exact_inverse(r.dx)};
   g2p_particle<APIC>(a, q);
 }
 
@@ -1554,7 +1736,8 @@ int launch_p2g(Ctx *c, int transfer) {
     if (e) return e;
   }
   P2GArgs a{c->start, c->rec0, c->rec1, c->rec2, c->rec3, c->f.u, c->f.v, c->f.w,
-            c->f.uw, c->f.vw, c->f.ww, c->dx, c->nx, c->ny, c->nz, c->nty, c->ntz};
+            c->f.uw, c->f.vw, c->f.ww, c->dx, c->nx, c->ny, c->nz, c->nty, c->ntz,
+            exact_inverse(c->dx)};
   if (c->p.n > 0 && c->nseg > 0) {
     BatchArgs b = batch_args(c);
     const int map = c->tune.p2g_map;
@@ -1566,12 +1749,16 @@ int launch_p2g(Ctx *c, int transfer) {
       kern<<<c->ntiles, 256, sm, st>>>(b);
     };
     if (transfer == GF_APIC) {
-      if (map == 3) launch(kb_p2g_tile<true, 3>);
+      if (map == 5) launch(kb_p2g_tile<true, 5>);
+      else if (map == 4) launch(kb_p2g_tile<true, 4>);
+      else if (map == 3) launch(kb_p2g_tile<true, 3>);
       else if (map == 2) kb_p2g_tile<true, 2><<<c->ntiles, 256, sm, st>>>(b);
       else if (map == 1) kb_p2g_tile<true, 1><<<c->ntiles, 256, sm, st>>>(b);
       else kb_p2g_tile<true, 0><<<c->ntiles, 256, sm, st>>>(b);
     } else {
-      if (map == 3) launch(kb_p2g_tile<false, 3>);
+      if (map == 5) launch(kb_p2g_tile<false, 5>);
+      else if (map == 4) launch(kb_p2g_tile<false, 4>);
+      else if (map == 3) launch(kb_p2g_tile<false, 3>);
       else if (map == 2) kb_p2g_tile<false, 2><<<c->ntiles, 256, sm, st>>>(b);
       else if (map == 1) kb_p2g_tile<false, 1><<<c->ntiles, 256, sm, st>>>(b);
       else kb_p2g_tile<false, 0><<<c->ntiles, 256, sm, st>>>(b);
@@ -1580,7 +1767,7 @@ int launch_p2g(Ctx *c, int transfer) {
   } else if (c->p.n > 0) {
     const int kt = c->tune.p2g_tiles_k == 2 ? 2 : 1;
     const unsigned g = (unsigned)(c->ntx * c->nty * ((c->ntz + kt - 1) / kt));
-    const int map = c->tune.p2g_map >= 0 && c->tune.p2g_map <= 3 ? c->tune.p2g_map : 0;
+    const int map = c->tune.p2g_map >= 0 && c->tune.p2g_map <= 5 ? c->tune.p2g_map : 0;
     const size_t sm = p2g_smem_bytes(kt, map, transfer == GF_APIC);
     auto launch = [&](auto kern) {
       if (sm > 48 * 1024)
@@ -1589,12 +1776,16 @@ int launch_p2g(Ctx *c, int transfer) {
       kern<<<g, 256, sm, st>>>(a);
     };
     if (transfer == GF_APIC) {
-      if (map == 3) kt == 2 ? launch(k_p2g_tile<true, 2, 3>) : launch(k_p2g_tile<true, 1, 3>);
+      if (map == 5) kt == 2 ? launch(k_p2g_tile<true, 2, 5>) : launch(k_p2g_tile<true, 1, 5>);
+      else if (map == 4) kt == 2 ? launch(k_p2g_tile<true, 2, 4>) : launch(k_p2g_tile<true, 1, 4>);
+      else if (map == 3) kt == 2 ? launch(k_p2g_tile<true, 2, 3>) : launch(k_p2g_tile<true, 1, 3>);
       else if (map == 2) kt == 2 ? launch(k_p2g_tile<true, 2, 2>) : launch(k_p2g_tile<true, 1, 2>);
       else if (map) kt == 2 ? launch(k_p2g_tile<true, 2, 1>) : launch(k_p2g_tile<true, 1, 1>);
       else     kt == 2 ? launch(k_p2g_tile<true, 2, 0>) : launch(k_p2g_tile<true, 1, 0>);
     } else {
-      if (map == 3) kt == 2 ? launch(k_p2g_tile<false, 2, 3>) : launch(k_p2g_tile<false, 1, 3>);
+      if (map == 5) kt == 2 ? launch(k_p2g_tile<false, 2, 5>) : launch(k_p2g_tile<false, 1, 5>);
+      else if (map == 4) kt == 2 ? launch(k_p2g_tile<false, 2, 4>) : launch(k_p2g_tile<false, 1, 4>);
+      else if (map == 3) kt == 2 ? launch(k_p2g_tile<false, 2, 3>) : launch(k_p2g_tile<false, 1, 3>);
       else if (map == 2) kt == 2 ? launch(k_p2g_tile<false, 2, 2>) : launch(k_p2g_tile<false, 1, 2>);
       else if (map) kt == 2 ? launch(k_p2g_tile<false, 2, 1>) : launch(k_p2g_tile<false, 1, 1>);
       else     kt == 2 ? launch(k_p2g_tile<false, 2, 0>) : launch(k_p2g_tile<false, 1, 0>);
@@ -1685,7 +1876,7 @@ int launch_g2p(Ctx *c, int transfer, float flip_blend, float dt) {
   }
   G2PArgs a{c->rec0, c->rec1, c->f.u, c->f.v, c->f.w, c->f.us, c->f.vs, c->f.ws,
             c->p.pos, c->p.vel, c->p.C, c->p.pid, c->p.n, c->dx, dt, flip_blend,
-            c->dom[0], c->dom[1], c->dom[2], c->nx, c->ny, c->nz};
+            c->dom[0], c->dom[1], c->dom[2], c->nx, c->ny, c->nz, exact_inverse(c->dx)};
   if (c->tune.g2p_tiles_k == 0) {  // no staging: one thread per particle, L1/L2 gathers
     if (transfer == GF_APIC)
       k_g2p<true><<<g, th, 0, c->stream>>>(a);

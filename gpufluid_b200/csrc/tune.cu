@@ -10,7 +10,8 @@
 //   p2g_map                     P2G lanes: runs of particles (0), one cell
 //                               each (1), one cell each summed in registers
 //                               first (2), the same from coalesced shared
-//                               staging (3)                         (P2G stage)
+//                               staging (3) or from warp-staged rounds of 8
+//                               (4) or 4 (5) particles per cell  (P2G stage)
 //   g2p_threads                 threads per block of the batches' per-particle
 //                               G2P                                 (G2P stage)
 //   grid_threads, blocks_per_sm launch shape of the grid-stride face/cell
@@ -145,8 +146,8 @@ int gf_autotune(void *ctx, const gf_step_params *prm, gf_tune_info *out) {
     for (int knob = 0; knob < 3 && !e; ++knob) {
       if (c->nseg > 0 && knob != 1) continue;  // batches: 8^3 P2G tiles, per-particle G2P
       int &v = knob == 0 ? c->tune.p2g_tiles_k : (knob == 1 ? c->tune.p2g_map : c->tune.g2p_tiles_k);
-      // P2G blocks 1..2 tiles, lane maps 0..3, G2P 0 (unstaged) ..2 tiles
-      const int lo = knob == 0 ? 1 : 0, hi = knob == 1 ? 3 : 2;
+      // P2G blocks 1..2 tiles, lane maps 0..5, G2P 0 (unstaged) ..2 tiles
+      const int lo = knob == 0 ? 1 : 0, hi = knob == 1 ? 5 : 2;
       int best_v = v;
       float best = 3.4e38f;
       for (int x = lo; x <= hi; ++x) {
@@ -234,7 +235,7 @@ int gf_set_tune(void *ctx, const gf_tune_info *in) {
   if (!ok_threads(in->g2p_threads, 512) || !ok_threads(in->grid_threads, 1024) ||
       in->grid_blocks_per_sm < 1 || in->grid_blocks_per_sm > 64 || in->pcg_blocks_per_sm < 0 ||
       in->pcg_blocks_per_sm > 8 || in->p2g_tiles_k < 1 || in->p2g_tiles_k > 2 ||
-      in->g2p_tiles_k < 0 || in->g2p_tiles_k > 2 || in->p2g_map < 0 || in->p2g_map > 3)
+      in->g2p_tiles_k < 0 || in->g2p_tiles_k > 2 || in->p2g_map < 0 || in->p2g_map > 5)
     return gf::fail(c, GF_INVALID_ARG, "gf_set_tune: launch shape out of range");
   c->tune.p2g_tiles_k = in->p2g_tiles_k;
   c->tune.p2g_map = in->p2g_map;

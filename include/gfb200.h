@@ -201,11 +201,13 @@ typedef struct gf_pressure_info {
 } gf_pressure_info;
 /* Copies the trace buffer of the last traced PCG solve (up to cap int64
  * entries: block 0's SM-cycle stamps in the first half, *n of them, then per
- * block ten values: busy cycles outside the all-reduce, tiles owned, fluid
- * cells owned, faces bordering another block's tile, and the cycles of six
+ * block twelve values: busy cycles outside the all-reduce, tiles owned, fluid
+ * cells owned, faces bordering another block's tile, and the cycles of eight
  * iteration phases as block thread 0 sees them -- own update, SGS sweeps,
  * halo publication with the neighbour flags and in-block rings, remote rings,
- * stencil and dot products, grid all-reduce) into host memory; synchronises. */
+ * stencil and dot products, grid all-reduce, the coarse correction's gather
+ * of the tiles' residual sums, its e = B g and addition to z) into host
+ * memory; synchronises. */
 int gf_pcg_trace(void *ctx, int64_t *host, int32_t cap, int32_t *n);
 /* Statistics of the last pressure solve; synchronises. */
 int gf_pressure_stats(void *ctx, gf_pressure_info *info);
@@ -451,7 +453,9 @@ typedef struct gf_tune_info {
                                  0: one thread per particle, no staged boxes */
   int32_t p2g_map;            /* P2G lanes: runs of a block's particles (0), one cell each (1),
                                  one cell each summed in registers first (2), the same
-                                 reading the particles from coalesced shared staging (3) */
+                                 reading the particles from coalesced shared staging (3),
+                                 or from warp-staged rounds of 8 (4) or 4 (5) particles
+                                 per cell */
 } gf_tune_info;
 int gf_autotune(void *ctx, const gf_step_params *prm, gf_tune_info *out);
 int gf_get_tune(void *ctx, gf_tune_info *out);

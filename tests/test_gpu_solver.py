@@ -268,7 +268,7 @@ def test_autotune_tile_shapes_and_state_restored(gf):
         if tune:
             info = s.autotune(1 / 240, 60, "jacobi")
             assert info["p2g_tiles_k"] in (1, 2) and info["g2p_tiles_k"] in (0, 1, 2), info
-            assert info["p2g_map"] in (0, 1, 2, 3), info
+            assert info["p2g_map"] in (0, 1, 2, 3, 4, 5), info
             assert info["step_ms_before"] > 0 and info["step_ms_after"] > 0
             after = s.get_particles()
             assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])

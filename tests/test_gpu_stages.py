@@ -85,7 +85,7 @@ def test_bin_labels_keys_order_bitexact(gf, oracle, grid):
 
 
 @pytest.mark.parametrize("tiles_k,lanes", [(1, 0), (2, 0), (1, 1), (2, 1), (1, 2), (2, 2),
-                                           (1, 3), (2, 3)])
+                                           (1, 3), (2, 3), (1, 4), (2, 4), (1, 5), (2, 5)])
 @pytest.mark.parametrize("transfer", ["flip", "apic"])
 @pytest.mark.parametrize("grid", GRIDS[:2] + [(17, 12, 40)])
 def test_p2g_matches_oracle(gf, oracle, grid, transfer, tiles_k, lanes):
