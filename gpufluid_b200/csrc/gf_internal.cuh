@@ -346,6 +346,50 @@ struct RegionBufs {
 RegionBufs region_bufs(Ctx *c);
 int check_launch(Ctx *c, const char *what);
 
+// Packed float32 pairs (the sm_100 f32x2 instructions): one instruction does
+// the operation on both halves.  mul2 / add2 / sub2 round each half exactly as
+// the scalar IEEE operation (.rn), so a paired product or sum is bit-identical
+// to the two scalar ones; fma2 fuses each half's multiply-add.
+__device__ __forceinline__ unsigned long long f2_bits(const float2 &a) {
+  return reinterpret_cast<const unsigned long long &>(a);
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+  float2 d;
+  asm("mul.rn.f32x2 %0, %1, %2;"
+      : "=l"(reinterpret_cast<unsigned long long &>(d))
+      : "l"(f2_bits(a)), "l"(f2_bits(b)));
+  return d;
+}
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+  float2 d;
+  asm("add.rn.f32x2 %0, %1, %2;"
+      : "=l"(reinterpret_cast<unsigned long long &>(d))
+      : "l"(f2_bits(a)), "l"(f2_bits(b)));
+  return d;
+}
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+  float2 d;
+  asm("sub.rn.f32x2 %0, %1, %2;"
+      : "=l"(reinterpret_cast<unsigned long long &>(d))
+      : "l"(f2_bits(a)), "l"(f2_bits(b)));
+  return d;
+}
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+  float2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;"
+      : "=l"(reinterpret_cast<unsigned long long &>(d))
+      : "l"(f2_bits(a)), "l"(f2_bits(b)), "l"(f2_bits(c)));
+  return d;
+}
+__device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
+// x + y as fma(x, one, y), where `one` is 1 but known only at run time (a
+// launch argument): x * 1 is exact, so the result is the correctly rounded
+// sum of mul2 / add2, yet the compiler cannot merge a paired product that
+// feeds it into a fused multiply-add.  (ptxas contracts mul.rn.f32x2 into a
+// following add.rn.f32x2 even under --fmad=false; bit-exact code forms every
+// paired sum of a product this way.)
+__device__ __forceinline__ float2 sum2(float2 x, float2 one, float2 y) { return fma2(x, one, y); }
+
 // 1/dx when dx is a power of two, so that x * (1/dx) is x / dx exactly; 0
 // otherwise (the IEEE division is used then).
 __host__ __device__ inline float exact_inverse(float dx) {

@@ -227,9 +227,10 @@ __device__ __forceinline__ void p2g_cell_comp(const P2GArgs &a, T *s_val, T *s_w
                   HZ = COMP == 2 ? 0.0f : 0.5f;
   const int xo = ci - (COMP != 0), yo = cj - (COMP != 1), zo = ck - (COMP != 2);
   const float dx = a.dx, inv = a.inv_dx_exact;
-  float av[EX * EY * EZ], aw[EX * EY * EZ];
+  // (value, weight) sums of each face, one f32x2 pair
+  float2 acc[EX * EY * EZ];
 #pragma unroll
-  for (int m = 0; m < EX * EY * EZ; ++m) av[m] = aw[m] = 0.0f;
+  for (int m = 0; m < EX * EY * EZ; ++m) acc[m] = dup2(0.0f);
   for (int kp = 0; kp < maxcnt; ++kp) {
     if (kp >= cnt) continue;
     const int64_t q = first + kp;
@@ -289,9 +290,8 @@ __device__ __forceinline__ void p2g_cell_comp(const P2GArgs &a, T *s_val, T *s_w
 #pragma unroll
         for (int z = 0; z < EZ; ++z) {
           const int m = (x * EY + y) * EZ + z;
-          av[m] = __fmaf_rn(P, wz[z], av[m]);
-          if (APIC) av[m] = __fmaf_rn(wxy, D[z], av[m]);
-          aw[m] = __fmaf_rn(wxy, wz[z], aw[m]);
+          acc[m] = fma2(make_float2(P, wxy), dup2(wz[z]), acc[m]);
+          if (APIC) acc[m].x = __fmaf_rn(wxy, D[z], acc[m].x);
         }
       }
   }
@@ -306,11 +306,11 @@ __device__ __forceinline__ void p2g_cell_comp(const P2GArgs &a, T *s_val, T *s_w
 #pragma unroll
       for (int z = 0; z < EZ; ++z) {
         const int m = (x * EY + y) * EZ + z;
-        if (aw[m] == 0.0f) continue;
+        if (acc[m].y == 0.0f) continue;
         const int e = e0 + (x * ey + y) * ez + z;
         if (!GF_IN(e, P2G_BOXK(KT))) continue;
-        atomicAdd(&s_val[e], (T)av[m]);
-        atomicAdd(&s_wt[e], (T)aw[m]);
+        atomicAdd(&s_val[e], (T)acc[m].x);
+        atomicAdd(&s_wt[e], (T)acc[m].y);
       }
 }
 
@@ -1140,6 +1140,152 @@ __device__ __forceinline__ void apic_gather_lin(const float *p, int si, int sj, 
   vel = acc;
 }
 
+// Stencil of one component for the paired gathers: its first corner in the
+// staged box, the box strides, the first face index per axis and the sample
+// coordinates.
+struct GStencil {
+  const float *p;
+  int si, sj, i0, j0, k0;
+  float fx, fy, fz;
+};
+
+// apic_gather_lin for two components at once (a on the x half of each
+// float32 pair, b on the y half): every product and sum is the one
+// apic_gather_lin forms for that component, in the same order, done by the
+// paired f32x2 instructions (each half rounds as the scalar operation), so
+// both results are identical to two apic_gather_lin calls.  A sum that takes
+// a product is formed as fma(x, one, y) with one == 1 known only at run time
+// (sum2): the compiler contracts a paired product into a paired add even with
+// contraction disabled, which would round the two operations once.
+template <int AXA, int AXB>
+__device__ __forceinline__ void apic_gather_lin_pair(const GStencil &a, const GStencil &b,
+                                                     float px, float py, float pz, float dx,
+                                                     float inv, float one, float2 &vel,
+                                                     float2 &c0, float2 &c1, float2 &c2) {
+  const float2 ONE = dup2(one), NEG = dup2(-one);
+  // s = f - floor(f): the difference as -floor * 1 + f
+  const float2 s_x = fma2(make_float2((float)a.i0, (float)b.i0), NEG, make_float2(a.fx, b.fx));
+  const float2 s_y = fma2(make_float2((float)a.j0, (float)b.j0), NEG, make_float2(a.fy, b.fy));
+  const float2 s_z = fma2(make_float2((float)a.k0, (float)b.k0), NEG, make_float2(a.fz, b.fz));
+  const float2 wx[2] = {sub2(dup2(1.0f), s_x), s_x}, wy[2] = {sub2(dup2(1.0f), s_y), s_y},
+               wz[2] = {sub2(dup2(1.0f), s_z), s_z};
+  // face offsets: (index [+ 0.5]) dx - p; adding 0 to the integer-valued float
+  // is exact, so the component without the half shift keeps its value
+  const float2 hx = make_float2(AXA == 0 ? 0.0f : 0.5f, AXB == 0 ? 0.0f : 0.5f);
+  const float2 hy = make_float2(AXA == 1 ? 0.0f : 0.5f, AXB == 1 ? 0.0f : 0.5f);
+  const float2 hz = make_float2(AXA == 2 ? 0.0f : 0.5f, AXB == 2 ? 0.0f : 0.5f);
+  const float2 DX = dup2(dx);
+  float2 ox[2], oy[2], oz[2];
+#pragma unroll
+  for (int d = 0; d < 2; ++d) {
+    ox[d] = sum2(mul2(add2(make_float2((float)(a.i0 + d), (float)(b.i0 + d)), hx), DX), ONE,
+                 dup2(-px));
+    oy[d] = sum2(mul2(add2(make_float2((float)(a.j0 + d), (float)(b.j0 + d)), hy), DX), ONE,
+                 dup2(-py));
+    oz[d] = sum2(mul2(add2(make_float2((float)(a.k0 + d), (float)(b.k0 + d)), hz), DX), ONE,
+                 dup2(-pz));
+  }
+  const float2 INV = dup2(inv);
+  float2 acc = dup2(0.0f);
+  c0 = c1 = c2 = dup2(0.0f);
+#pragma unroll
+  for (int di = 0; di < 2; ++di)
+#pragma unroll
+    for (int dj = 0; dj < 2; ++dj) {
+      const float2 wxy = mul2(wx[di], wy[dj]);
+#pragma unroll
+      for (int dk = 0; dk < 2; ++dk) {
+        const float2 wt = mul2(wxy, wz[dk]);
+        const float2 val = make_float2(a.p[di * a.si + dj * a.sj + dk],
+                                       b.p[di * b.si + dj * b.sj + dk]);
+        const float2 t = mul2(wt, val);
+        acc = sum2(t, ONE, acc);
+        const float2 fu = mul2(t, INV);
+        c0 = sum2(mul2(fu, ox[di]), ONE, c0);
+        c1 = sum2(mul2(fu, oy[dj]), ONE, c1);
+        c2 = sum2(mul2(fu, oz[dk]), ONE, c2);
+      }
+    }
+  vel = acc;
+}
+
+// apic_gather_lin for one component with its two corners along k paired:
+// the products of both corners are paired f32x2 instructions, and each
+// accumulator adds the dk = 0 term before the dk = 1 term, as
+// apic_gather_lin does, so the results are identical (the paired sum that
+// takes a product is a sum2, as in apic_gather_lin_pair).
+template <int AX>
+__device__ __forceinline__ void apic_gather_lin_k2(const GStencil &g, float px, float py,
+                                                   float pz, float dx, float inv, float one,
+                                                   float &vel, float &c0, float &c1, float &c2) {
+  const float sx = g.fx - (float)g.i0, sy = g.fy - (float)g.j0, sz = g.fz - (float)g.k0;
+  const float wx[2] = {1.0f - sx, sx}, wy[2] = {1.0f - sy, sy};
+  const float2 wz = make_float2(1.0f - sz, sz);
+  float ox[2], oy[2];
+#pragma unroll
+  for (int d = 0; d < 2; ++d) {
+    ox[d] = AX == 0 ? (float)(g.i0 + d) * dx - px : ((float)(g.i0 + d) + 0.5f) * dx - px;
+    oy[d] = AX == 1 ? (float)(g.j0 + d) * dx - py : ((float)(g.j0 + d) + 0.5f) * dx - py;
+  }
+  const float2 oz = sum2(mul2(add2(make_float2((float)g.k0, (float)(g.k0 + 1)),
+                                   dup2(AX == 2 ? 0.0f : 0.5f)),
+                              dup2(dx)),
+                         dup2(one), dup2(-pz));
+  const float2 INV = dup2(inv);
+  float acc = 0.0f;
+  c0 = 0.0f;
+  c1 = 0.0f;
+  c2 = 0.0f;
+#pragma unroll
+  for (int di = 0; di < 2; ++di)
+#pragma unroll
+    for (int dj = 0; dj < 2; ++dj) {
+      const float wxy = wx[di] * wy[dj];
+      const float *q = g.p + di * g.si + dj * g.sj;
+      const float2 wt = mul2(dup2(wxy), wz);
+      const float2 t = mul2(wt, make_float2(q[0], q[1]));
+      const float2 fu = mul2(t, INV);
+      const float2 m0 = mul2(fu, dup2(ox[di])), m1 = mul2(fu, dup2(oy[dj])), m2 = mul2(fu, oz);
+      acc = acc + t.x;
+      c0 = c0 + m0.x;
+      c1 = c1 + m1.x;
+      c2 = c2 + m2.x;
+      acc = acc + t.y;
+      c0 = c0 + m0.y;
+      c1 = c1 + m1.y;
+      c2 = c2 + m2.y;
+    }
+  vel = acc;
+}
+
+// sample3_lin of two arrays that share the stencil (the new and the saved
+// velocity of one component): the weights are formed once and every
+// interpolation step is a paired f32x2 instruction (x half: p, y half: q),
+// each half rounding as sample3_lin's scalar step, so both results are
+// identical to two sample3_lin calls (sums of products are sum2s, as in
+// apic_gather_lin_pair).
+__device__ __forceinline__ float2 sample3_lin_pair(const float *p, const float *q, int si,
+                                                   int sj, float fx, float fy, float fz, int i0,
+                                                   int j0, int k0, float one) {
+  const float sx = clampf(fx - (float)i0, 0.0f, 1.0f);
+  const float sy = clampf(fy - (float)j0, 0.0f, 1.0f);
+  const float sz = clampf(fz - (float)k0, 0.0f, 1.0f);
+  const float2 SX = dup2(sx), SY = dup2(sy), SZ = dup2(sz), ONE = dup2(one);
+  const float2 OX = dup2(1.0f - sx), OY = dup2(1.0f - sy), OZ = dup2(1.0f - sz);
+  const float2 c000 = make_float2(p[0], q[0]), c100 = make_float2(p[si], q[si]);
+  const float2 c010 = make_float2(p[sj], q[sj]), c110 = make_float2(p[si + sj], q[si + sj]);
+  const float2 c001 = make_float2(p[1], q[1]), c101 = make_float2(p[si + 1], q[si + 1]);
+  const float2 c011 = make_float2(p[sj + 1], q[sj + 1]);
+  const float2 c111 = make_float2(p[si + sj + 1], q[si + sj + 1]);
+  const float2 c00 = sum2(mul2(c000, OX), ONE, mul2(c100, SX));
+  const float2 c10 = sum2(mul2(c010, OX), ONE, mul2(c110, SX));
+  const float2 c01 = sum2(mul2(c001, OX), ONE, mul2(c101, SX));
+  const float2 c11 = sum2(mul2(c011, OX), ONE, mul2(c111, SX));
+  const float2 c0 = sum2(mul2(c00, OY), ONE, mul2(c10, SY));
+  const float2 c1 = sum2(mul2(c01, OY), ONE, mul2(c11, SY));
+  return sum2(mul2(c0, OZ), ONE, mul2(c1, SZ));
+}
+
 // True when apic_gather_at's stencil at (fx, fy, fz) needs no clamp.
 __device__ __forceinline__ bool stencil_inside(float fx, float fy, float fz, int snx, int sny,
                                                int snz, int &i0, int &j0, int &k0) {
@@ -1171,6 +1317,7 @@ struct G2PArgs {
   float dx, dt, flip_blend, dom0, dom1, dom2;
   int nx, ny, nz;
   float inv_dx_exact;  // exact_inverse(dx)
+  float one = 1.0f;    // 1, as a launch argument (sum2's multiplier)
 };
 
 template <bool APIC>
@@ -1339,7 +1486,7 @@ __device__ __forceinline__ bool in_box(const BoxAt &b, int ni, int i0, int i1, i
 }
 
 template <int MODE, int KT>
-__global__ void __launch_bounds__(G2P_TILE_THREADS)
+__global__ void __launch_bounds__(G2P_TILE_THREADS, 4)
     k_g2p_tile(const G2PTileArgs ta, const __grid_constant__ FaceMaps fm) {
   constexpr bool APIC = MODE == GF_APIC;
   constexpr int NARR = APIC ? 3 : 6;  // u, v, w (+ us, vs, ws for the FLIP delta)
@@ -1455,6 +1602,8 @@ __global__ void __launch_bounds__(G2P_TILE_THREADS)
   }
   const float dx = a.dx;
   int *s_pid = reinterpret_cast<int *>(s_out + (APIC ? 3840 : 1536));
+  // per-launch constants: 3 / dx^2 of the C rows (one IEEE division), the clamp margin
+  const float inv = __fdiv_rn(3.0f, dx * dx), eps = dx * 1.001f;
   for (int64_t base = b; base < e; base += G2P_TILE_THREADS) {
     const int m = (int)(e - base < G2P_TILE_THREADS ? e - base : G2P_TILE_THREADS);
     if (tid < m) {
@@ -1466,23 +1615,32 @@ __global__ void __launch_bounds__(G2P_TILE_THREADS)
       float hx = gx - 0.5f, hy = gy - 0.5f, hz = gz - 0.5f;
       float nu, nv, nw;
       if (APIC) {
-        float dd = dx * dx;
-        float inv = __fdiv_rn(3.0f, dd);
         float c[9];
         const float fxs[3] = {gx, hx, hx}, fys[3] = {hy, gy, hy}, fzs[3] = {hz, hz, gz};
         float vel3[3];
+        // the common case: every corner inside the grid and the staged box
+        // (the paired gathers); otherwise the clamped gathers of k_g2p
+        GStencil gs[3];
+        bool lin[3];
 #pragma unroll
         for (int cc = 0; cc < 3; ++cc) {
           const int snx = nx + (cc == 0), sny = ny + (cc == 1), snz = nz + (cc == 2);
           int i0, j0, k0;
           const bool inside = stencil_inside(fxs[cc], fys[cc], fzs[cc], snx, sny, snz, i0, j0, k0);
-          auto cl = [](int v, int n) { return v < 0 ? 0 : (v > n - 1 ? n - 1 : v); };
           const int NJ = gbox_nj(cc), NK = gbox_nk(cc, KT);
-          if (inside && in_box(bx[cc], gbox_ni(cc), i0, i0 + 1, j0, j0 + 1, k0, k0 + 1))
-            apic_gather_lin(bx[cc].s + ((i0 - bx[cc].oi) * NJ + (j0 - bx[cc].oj)) * NK +
+          lin[cc] = inside && in_box(bx[cc], gbox_ni(cc), i0, i0 + 1, j0, j0 + 1, k0, k0 + 1);
+          gs[cc] = GStencil{bx[cc].s + ((i0 - bx[cc].oi) * NJ + (j0 - bx[cc].oj)) * NK +
                                 (k0 - bx[cc].ok),
-                            NJ * NK, NK, i0, j0, k0, px, py, pz, dx, fxs[cc], fys[cc], fzs[cc],
-                            cc, inv, vel3[cc], c[3 * cc], c[3 * cc + 1], c[3 * cc + 2]);
+                            NJ * NK, NK, i0, j0, k0, fxs[cc], fys[cc], fzs[cc]};
+        }
+        auto gather_one = [&](int cc) {
+          const int snx = nx + (cc == 0), sny = ny + (cc == 1), snz = nz + (cc == 2);
+          auto cl = [](int v, int n) { return v < 0 ? 0 : (v > n - 1 ? n - 1 : v); };
+          const int i0 = gs[cc].i0, j0 = gs[cc].j0, k0 = gs[cc].k0;
+          if (lin[cc])
+            apic_gather_lin(gs[cc].p, gs[cc].si, gs[cc].sj, i0, j0, k0, px, py, pz, dx,
+                            fxs[cc], fys[cc], fzs[cc], cc, inv, vel3[cc], c[3 * cc],
+                            c[3 * cc + 1], c[3 * cc + 2]);
           else if (in_box(bx[cc], gbox_ni(cc), cl(i0, snx), cl(i0 + 1, snx), cl(j0, sny),
                           cl(j0 + 1, sny), cl(k0, snz), cl(k0 + 1, snz)))
             apic_gather_at(bx[cc], px, py, pz, dx, fxs[cc], fys[cc], fzs[cc], snx, sny, snz, cc,
@@ -1491,7 +1649,23 @@ __global__ void __launch_bounds__(G2P_TILE_THREADS)
             apic_gather(cc == 0 ? a.u : (cc == 1 ? a.v : a.w), px, py, pz, dx, fxs[cc], fys[cc],
                         fzs[cc], snx, sny, snz, cc, inv, vel3[cc], c[3 * cc], c[3 * cc + 1],
                         c[3 * cc + 2]);
+        };
+        if (lin[0] && lin[1]) {
+          float2 v2, c0, c1, c2;
+          apic_gather_lin_pair<0, 1>(gs[0], gs[1], px, py, pz, dx, inv, a.one, v2, c0, c1,
+                                     c2);
+          vel3[0] = v2.x;
+          vel3[1] = v2.y;
+          c[0] = c0.x, c[1] = c1.x, c[2] = c2.x;
+          c[3] = c0.y, c[4] = c1.y, c[5] = c2.y;
+        } else {
+          gather_one(0);
+          gather_one(1);
         }
+        if (lin[2])
+          apic_gather_lin_k2<2>(gs[2], px, py, pz, dx, inv, a.one, vel3[2], c[6], c[7], c[8]);
+        else
+          gather_one(2);
         nu = vel3[0];
         nv = vel3[1];
         nw = vel3[2];
@@ -1511,8 +1685,10 @@ __global__ void __launch_bounds__(G2P_TILE_THREADS)
           if (i1 == i0 + 1 && j1 == j0 + 1 && k1 == k0 + 1 &&
               in_box(bx[cc], gbox_ni(cc), i0, i1, j0, j1, k0, k1)) {
             const int off = ((i0 - bx[cc].oi) * NJ + (j0 - bx[cc].oj)) * NK + (k0 - bx[cc].ok);
-            pic[cc] = sample3_lin(bx[cc].s + off, NJ * NK, NK, fx, fy, fz, i0, j0, k0);
-            old[cc] = sample3_lin(bx[cc + 3].s + off, NJ * NK, NK, fx, fy, fz, i0, j0, k0);
+            const float2 po = sample3_lin_pair(bx[cc].s + off, bx[cc + 3].s + off, NJ * NK, NK,
+                                               fx, fy, fz, i0, j0, k0, a.one);
+            pic[cc] = po.x;
+            old[cc] = po.y;
           } else if (in_box(bx[cc], gbox_ni(cc), i0, i1, j0, j1, k0, k1)) {
             pic[cc] = sample3_at(bx[cc], fx, fy, fz, i0, j0, k0, i1, j1, k1);
             old[cc] = sample3_at(bx[cc + 3], fx, fy, fz, i0, j0, k0, i1, j1, k1);
@@ -1536,7 +1712,6 @@ __global__ void __launch_bounds__(G2P_TILE_THREADS)
       s_out[768 + 3 * tid] = nu;
       s_out[768 + 3 * tid + 1] = nv;
       s_out[768 + 3 * tid + 2] = nw;
-      const float eps = dx * 1.001f;
       s_out[3 * tid] = clampf(px + nu * a.dt, eps, a.dom0 - eps);
       s_out[3 * tid + 1] = clampf(py + nv * a.dt, eps, a.dom1 - eps);
       s_out[3 * tid + 2] = clampf(pz + nw * a.dt, eps, a.dom2 - eps);
