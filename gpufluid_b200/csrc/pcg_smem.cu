@@ -740,12 +740,13 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   // Callers have written z = r/D on their fluid cells, zeroed the rings
   // (zero_rings, SGS only) and passed a barrier.
   // Coarse correction: each block publishes its tiles' residual sums g_t as
-  // tagged words before the sweeps and gathers all of them after (by then
-  // they have arrived) into the w array, which is free until the stencil
-  // rebuilds it; then e_t = B_t . g for its tiles (bf16 rows of B streamed
-  // from L2/L1, two or three warps per row, a fixed-order sum) is added to
-  // the z of each tile's fluid cells, so the halo exchange, the stencil and
-  // the dot products below all see u = z + P e.
+  // tagged words before the sweeps and gathers all of them (inside the last
+  // sweep with two or more sweeps, else after the sweeps) into the w array,
+  // which is free until the stencil rebuilds it; then e_t = B_t . g for its
+  // tiles (bf16 rows of B from shared memory or L2, several warps per row, a
+  // fixed-order sum) is added to the z of each tile's fluid cells after the
+  // sweeps, so the halo exchange, the stencil and the dot products below all
+  // see u = z + P e.
   unsigned long long gep = 0;  // g publications, the same sequence in every block
   unsigned long long *const GSL =
       reinterpret_cast<unsigned long long *>(a.partials + COARSE_SLOTS_OFF);
@@ -758,8 +759,8 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
                      ((gep + 1ull) << 32) | __float_as_uint(g));
     }
     // thread t gathers the words of tiles t, t + 1024, t + 2048; the first
-    // loads are issued before the last half-sweep, so their latency hides
-    // behind it; a stale word is polled again
+    // loads are issued a half-sweep before the words are needed, so their
+    // latency hides behind it; a stale word is polled again
     const unsigned long long *gsrc = GSL + (gep & 1ull) * CRMAX;
     const int t = threadIdx.x;
     unsigned long long gpre[3] = {0ull, 0ull, 0ull};
@@ -768,28 +769,20 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       for (int k = 0; k < 3; ++k)
         if (t + k * SM_THREADS < na) gpre[k] = ld_relaxed_u64(gsrc + t + k * SM_THREADS);
     };
-    for (int sw = 0; sw < sgs; ++sw) {
-      half_sweep(1);
-      __syncthreads();
-      if (CRS && coarse && sw == sgs - 1) prefetch();
-      half_sweep(0);
-      __syncthreads();
-    }
-    phase_mark(1);
-    if (CRS && coarse) {
-      if (sgs == 0) prefetch();
-      const unsigned long long tag = (gep + 1ull) << 32;
-      float *const s_g = s_w;  // [R8]: the gathered g, zero-padded
-      const int R8 = (na + 7) & ~7;
+    const unsigned long long gtag = (gep + 1ull) << 32;
+    float *const s_g = s_w;  // [R8]: the gathered g, zero-padded
+    const int R8 = (na + 7) & ~7;
+    // wait for every tile's g_t word (bounded) and store the sums into s_g
+    auto gather_store = [&]() {
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
         const int sl = t + k * SM_THREADS;
         if (sl < na) {
           unsigned long long w = gpre[k];
           long long spins = 0;
-          while ((w & 0xffffffff00000000ull) != tag) {
+          while ((w & 0xffffffff00000000ull) != gtag) {
             w = ld_relaxed_u64(gsrc + sl);
-            if ((w & 0xffffffff00000000ull) == tag) break;
+            if ((w & 0xffffffff00000000ull) == gtag) break;
             if (++spins > SM_SPIN_LIMIT) {
               atomicExch(&st->error, 1);
               w = 0;
@@ -802,37 +795,86 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
         }
       }
       ++gep;
-      __syncthreads();
-      phase_mark(6);
-      // e_t = B_t . g: row b0 + jr is summed by warps jr, jr + nt, ... (the
-      // lanes over 8-column chunks), then the warps' partials in warp order
-      float v = 0.f;
-      if (nt > 0) {
-        const int jr = wid % nt, iw = wid / nt, nw = (31 - jr) / nt + 1;
-        const uint4 *row = b_smem ? s_B + jr * (R8 >> 3)
-                                  : reinterpret_cast<const uint4 *>(Bh + (int64_t)(b0 + jr) * CRMAX);
-        auto ldB = [&](int ch) -> uint4 { return b_smem ? row[ch] : __ldg(row + ch); };
-        auto dot8 = [&](const uint4 q, int ch) {
-          const float *gp = s_g + ch * 8;
-          v += __uint_as_float(q.x << 16) * gp[0] + __uint_as_float(q.x & 0xffff0000u) * gp[1];
-          v += __uint_as_float(q.y << 16) * gp[2] + __uint_as_float(q.y & 0xffff0000u) * gp[3];
-          v += __uint_as_float(q.z << 16) * gp[4] + __uint_as_float(q.z & 0xffff0000u) * gp[5];
-          v += __uint_as_float(q.w << 16) * gp[6] + __uint_as_float(q.w & 0xffff0000u) * gp[7];
-        };
-        // two chunks in flight per lane, so a lane's loads wait one L2 trip
-        const int nch = R8 >> 3, step = nw * 32;
-        int ch = iw * 32 + lane;
-        for (; ch + step < nch; ch += 2 * step) {
-          const uint4 q0 = ldB(ch), q1 = ldB(ch + step);
-          dot8(q0, ch);
-          dot8(q1, ch + step);
-        }
-        if (ch < nch) dot8(ldB(ch), ch);
+    };
+    // this warp's share of e_t = B_t . g (s_g complete): row b0 + jr is summed
+    // by warps jr, jr + nt, ... (the lanes over 8-column chunks)
+    auto e_chunks = [&](float &v) {
+      if (nt <= 0) return;
+      const int jr = wid % nt, iw = wid / nt, nw = (31 - jr) / nt + 1;
+      const uint4 *row = b_smem ? s_B + jr * (R8 >> 3)
+                                : reinterpret_cast<const uint4 *>(Bh + (int64_t)(b0 + jr) * CRMAX);
+      auto ldB = [&](int ch) -> uint4 { return b_smem ? row[ch] : __ldg(row + ch); };
+      auto dot8 = [&](const uint4 q, int ch) {
+        const float *gp = s_g + ch * 8;
+        v += __uint_as_float(q.x << 16) * gp[0] + __uint_as_float(q.x & 0xffff0000u) * gp[1];
+        v += __uint_as_float(q.y << 16) * gp[2] + __uint_as_float(q.y & 0xffff0000u) * gp[3];
+        v += __uint_as_float(q.z << 16) * gp[4] + __uint_as_float(q.z & 0xffff0000u) * gp[5];
+        v += __uint_as_float(q.w << 16) * gp[6] + __uint_as_float(q.w & 0xffff0000u) * gp[7];
+      };
+      // two chunks in flight per lane, so a lane's loads wait one L2 trip
+      const int nch = R8 >> 3, step = nw * 32;
+      int ch = iw * 32 + lane;
+      for (; ch + step < nch; ch += 2 * step) {
+        const uint4 q0 = ldB(ch), q1 = ldB(ch + step);
+        dot8(q0, ch);
+        dot8(q1, ch + step);
       }
+      if (ch < nch) dot8(ldB(ch), ch);
+    };
+    // the warp's partial of its row, for the sums in warp order below
+    auto e_reduce = [&](float v) {
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
       if (lane == 0) s_ep[wid] = v;
+    };
+    // With two or more sweeps the coarse work rides inside the last sweep (it
+    // does not depend on the sweeps: M^-1 is the sum of the two parts): the g
+    // words are loaded before the last sweep and stored after its first
+    // half-sweep, before that barrier (published all earlier half-sweeps ago,
+    // so the wait is short); the last half-sweep starts with the e = B g
+    // products and ends with their warp sums.  This saves the two block
+    // barriers of the gather and of the products and lets their latency
+    // overlap the sweeps (measured 17.4 -> 16.9 us per iteration at 128^3).
+    const bool early = CRS && coarse && sgs >= 2;
+    if (early) {
+      for (int sw = 0; sw < sgs - 1; ++sw) {
+        half_sweep(1);
+        __syncthreads();
+        if (sw == sgs - 2) prefetch();
+        half_sweep(0);
+        __syncthreads();
+      }
+      half_sweep(1);
+      gather_store();
       __syncthreads();
+      {
+        float ev = 0.f;
+        e_chunks(ev);
+        half_sweep(0);
+        e_reduce(ev);
+        __syncthreads();
+      }
+    } else {
+      for (int sw = 0; sw < sgs; ++sw) {
+        half_sweep(1);
+        __syncthreads();
+        if (CRS && coarse && sw == sgs - 1) prefetch();
+        half_sweep(0);
+        __syncthreads();
+      }
+    }
+    phase_mark(1);
+    if (CRS && coarse) {
+      if (!early) {
+        if (sgs == 0) prefetch();
+        gather_store();
+        __syncthreads();
+        phase_mark(6);
+        float ev = 0.f;
+        e_chunks(ev);
+        e_reduce(ev);
+        __syncthreads();
+      }
       // lane t < nt of every warp sums e_t from the warps' partials (in warp
       // order); a thread's tiles tl0 + 2j are the same across its warp, so
       // each takes its e_t from lane tl by a shuffle
