@@ -1073,9 +1073,15 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
       if (r_true2 <= a.tol2 * b2) done = 1;
     }
     // ---- scalars of the next iteration (Chronopoulos-Gear)
+    // (beta' gamma' / alpha formed as gamma'^2 / (gamma alpha), so that its
+    // division does not wait for beta's: two dependent divisions, not three)
     const Acc gamma_new = tv[0], delta = tv[1];
-    const Acc bnew = fabs((double)gamma) < 1.0e-30 ? (Acc)0 : gamma_new / gamma;
-    const Acc den = delta - (fabs((double)alpha) < 1.0e-30 ? (Acc)0 : bnew * gamma_new / alpha);
+    const bool g_zero = fabs((double)gamma) < 1.0e-30;
+    const Acc bnew = g_zero ? (Acc)0 : gamma_new / gamma;
+    const Acc den = delta - (g_zero || fabs((double)alpha) < 1.0e-30
+                                 ? (Acc)0
+                                 : (Acc)((double)gamma_new * (double)gamma_new /
+                                         ((double)gamma * (double)alpha)));
     alpha = fabs((double)den) < 1.0e-30 ? (Acc)0 : gamma_new / den;
     beta = bnew;
     gamma = gamma_new;

@@ -1376,8 +1376,9 @@ __global__ void __launch_bounds__(512) k_g2p(G2PArgs a) {
 // shared memory first: by TMA (cp.async.bulk.tensor, completion on an
 // mbarrier) for every face array whose layout admits a tensor map, by plain
 // loads for the others.  The gathers then read shared memory, and the
-// outputs (positions, velocities, C, ids; AoS) go through a shared staging
-// buffer so that each warp writes whole cache lines with 16-byte stores.
+// outputs (positions, velocities, C, ids; AoS) go through a per-warp shared
+// staging buffer, so that each warp store instruction writes 32 consecutive
+// floats of one array (no block barrier between rounds).
 // The arithmetic is that of k_g2p, operation for operation.
 //
 // Box of component c (0 u, 1 v, 2 w) at tile origin (I0, J0, K0), in face
@@ -1450,21 +1451,6 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, i
       : "memory");
 }
 
-// Copy n floats from shared memory to global memory: scalar stores up to the
-// first 16-byte boundary of dst, then 16-byte stores, then the scalar tail.
-__device__ __forceinline__ void store_run(float *dst, const float *src, int n) {
-  int head = (int)(((16u - (uint32_t)(reinterpret_cast<uintptr_t>(dst) & 15u)) & 15u) >> 2);
-  if (head > n) head = n;
-  const int tid = threadIdx.x;
-  if (tid < head) dst[tid] = src[tid];
-  const int nv = (n - head) >> 2;
-  float4 *d4 = reinterpret_cast<float4 *>(dst + head);
-  const float *s4 = src + head;
-  for (int v = tid; v < nv; v += G2P_TILE_THREADS)
-    d4[v] = make_float4(s4[4 * v], s4[4 * v + 1], s4[4 * v + 2], s4[4 * v + 3]);
-  for (int q = head + 4 * nv + tid; q < n; q += G2P_TILE_THREADS) dst[q] = src[q];
-}
-
 struct G2PTileArgs {
   G2PArgs g;
   const int32_t *start;
@@ -1490,7 +1476,9 @@ __global__ void __launch_bounds__(G2P_TILE_THREADS, 4)
     k_g2p_tile(const G2PTileArgs ta, const __grid_constant__ FaceMaps fm) {
   constexpr bool APIC = MODE == GF_APIC;
   constexpr int NARR = APIC ? 3 : 6;  // u, v, w (+ us, vs, ws for the FLIP delta)
-  constexpr int OUTF = APIC ? 4096 : 1792;  // staging: pos 768, vel 768, [C 2304], pid 256
+  // output staging, per warp: pos 96, vel 96, [C 288,] pid 32 floats
+  constexpr int PW = APIC ? 512 : 224, OUTF = 8 * PW;
+  static_assert(G2P_TILE_THREADS == 256, "eight warps of staging");
   constexpr int SET = gbox_set(KT);
   extern __shared__ __align__(128) unsigned char g2p_smem[];
   float *s_box = reinterpret_cast<float *>(g2p_smem);  // (NARR / 3) sets of boxes
@@ -1601,7 +1589,9 @@ __global__ void __launch_bounds__(G2P_TILE_THREADS, 4)
                   c == 2 ? K0 : K0 - 4, gbox_nj(c), gbox_nk(c, KT), gbox_vol(c, KT)};
   }
   const float dx = a.dx;
-  int *s_pid = reinterpret_cast<int *>(s_out + (APIC ? 3840 : 1536));
+  const int lane = tid & 31, warp = tid >> 5;
+  float *const ws = s_out + warp * PW;  // this warp's staging
+  int *const wpid = reinterpret_cast<int *>(ws + (APIC ? 480 : 192));
   // per-launch constants: 3 / dx^2 of the C rows (one IEEE division), the clamp margin
   const float inv = __fdiv_rn(3.0f, dx * dx), eps = dx * 1.001f;
   for (int64_t base = b; base < e; base += G2P_TILE_THREADS) {
@@ -1670,7 +1660,7 @@ __global__ void __launch_bounds__(G2P_TILE_THREADS, 4)
         nv = vel3[1];
         nw = vel3[2];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) s_out[1536 + 9 * tid + k] = c[k];
+        for (int k = 0; k < 9; ++k) ws[192 + 9 * lane + k] = c[k];
       } else {
         const float4 r1 = a.rec1[q];
         float pic[3], old[3];
@@ -1709,20 +1699,42 @@ __global__ void __launch_bounds__(G2P_TILE_THREADS, 4)
         nv = a.flip_blend * fv + ob * pic[1];
         nw = a.flip_blend * fw + ob * pic[2];
       }
-      s_out[768 + 3 * tid] = nu;
-      s_out[768 + 3 * tid + 1] = nv;
-      s_out[768 + 3 * tid + 2] = nw;
-      s_out[3 * tid] = clampf(px + nu * a.dt, eps, a.dom0 - eps);
-      s_out[3 * tid + 1] = clampf(py + nv * a.dt, eps, a.dom1 - eps);
-      s_out[3 * tid + 2] = clampf(pz + nw * a.dt, eps, a.dom2 - eps);
-      s_pid[tid] = __float_as_int(r0.w);
+      ws[96 + 3 * lane] = nu;
+      ws[96 + 3 * lane + 1] = nv;
+      ws[96 + 3 * lane + 2] = nw;
+      ws[3 * lane] = clampf(px + nu * a.dt, eps, a.dom0 - eps);
+      ws[3 * lane + 1] = clampf(py + nv * a.dt, eps, a.dom1 - eps);
+      ws[3 * lane + 2] = clampf(pz + nw * a.dt, eps, a.dom2 - eps);
+      wpid[lane] = __float_as_int(r0.w);
     }
-    __syncthreads();
-    store_run(a.pos + 3 * base, s_out, 3 * m);
-    store_run(a.vel + 3 * base, s_out + 768, 3 * m);
-    if (APIC) store_run(a.C + 9 * base, s_out + 1536, 9 * m);
-    store_run(reinterpret_cast<float *>(a.pid + base), reinterpret_cast<const float *>(s_pid), m);
-    __syncthreads();
+    // the warp writes its particles' outputs: each store instruction covers
+    // 32 consecutive floats of one array (whole 128-byte spans)
+    __syncwarp();
+    const int mw = m - warp * 32 < 0 ? 0 : (m - warp * 32 > 32 ? 32 : m - warp * 32);
+    const int64_t wb = base + warp * 32;
+    float *const gp = a.pos + 3 * wb, *const gv = a.vel + 3 * wb;
+    if (mw == 32) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        gp[lane + 32 * k] = ws[lane + 32 * k];
+        gv[lane + 32 * k] = ws[96 + lane + 32 * k];
+      }
+      if (APIC) {
+        float *const gc = a.C + 9 * wb;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) gc[lane + 32 * k] = ws[192 + lane + 32 * k];
+      }
+      a.pid[wb + lane] = wpid[lane];
+    } else if (mw > 0) {
+      for (int k = lane; k < 3 * mw; k += 32) {
+        gp[k] = ws[k];
+        gv[k] = ws[96 + k];
+      }
+      if (APIC)
+        for (int k = lane; k < 9 * mw; k += 32) a.C[9 * wb + k] = ws[192 + k];
+      if (lane < mw) a.pid[wb + lane] = wpid[lane];
+    }
+    __syncwarp();
   }
 }
 
