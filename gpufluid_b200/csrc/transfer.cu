@@ -171,29 +171,30 @@ __device__ __forceinline__ bool scatter_comp_fast(T *s_val, T *s_wt, int comp, f
 
 // Flush a tile's shared box: faces that only this tile's particles reach are
 // stored, the shared halo band is accumulated atomically; exact zeros are
-// skipped (the destination was zeroed before the launch).
-template <int KT, typename T>
-__device__ __forceinline__ void p2g_flush_box(const P2GArgs &a, const T *s_val, const T *s_wt,
-                                              int I0, int J0, int K0) {
-  constexpr int BK = P2G_BOXK(KT);
-  for (int q = threadIdx.x; q < 3 * BK; q += blockDim.x) {
-    int comp = q / BK, e2 = q - comp * BK;
-    int ey = comp == 1 ? BOX_N : BOX_T, ez = p2g_ez(comp, KT);
-    if (e2 >= (comp == 0 ? BOX_N : BOX_T) * ey * ez) continue;  // beyond this component's box
-    float val = (float)s_val[q], wt = (float)s_wt[q];
+// skipped (the destination was zeroed before the launch).  One component at
+// a time, so the box extents are compile-time constants and the entry index
+// splits into (bx, by, bz) by multiplications instead of divisions.
+template <int COMP, int KT, typename T>
+__device__ __forceinline__ void p2g_flush_comp(const P2GArgs &a, const T *s_val, const T *s_wt,
+                                               int I0, int J0, int K0) {
+  constexpr int EX = COMP == 0 ? BOX_N : BOX_T, EY = COMP == 1 ? BOX_N : BOX_T,
+                EZ = p2g_ez(COMP, KT);
+  const int snx = a.nx + (COMP == 0), sny = a.ny + (COMP == 1), snz = a.nz + (COMP == 2);
+  const int ox = COMP == 0 ? I0 : I0 - 1, oy = COMP == 1 ? J0 : J0 - 1,
+            oz = COMP == 2 ? K0 : K0 - 1;
+  float *const gv = COMP == 0 ? a.u : (COMP == 1 ? a.v : a.w);
+  float *const gw = COMP == 0 ? a.uw : (COMP == 1 ? a.vw : a.ww);
+  for (int e2 = threadIdx.x; e2 < EX * EY * EZ; e2 += blockDim.x) {
+    const float val = (float)s_val[e2], wt = (float)s_wt[e2];
     if (val == 0.f && wt == 0.f) continue;
-    int bx = e2 / (ey * ez), by = (e2 / ez) % ey, bz = e2 % ez;
-    int ii = bx + (comp == 0 ? I0 : I0 - 1), jj = by + (comp == 1 ? J0 : J0 - 1),
-        kk = bz + (comp == 2 ? K0 : K0 - 1);
-    int snx = a.nx + (comp == 0), sny = a.ny + (comp == 1), snz = a.nz + (comp == 2);
+    const int bx = e2 / (EY * EZ), by = (e2 / EZ) % EY, bz = e2 % EZ;
+    const int ii = bx + ox, jj = by + oy, kk = bz + oz;
     if (ii < 0 || ii >= snx || jj < 0 || jj >= sny || kk < 0 || kk >= snz) continue;
     // exclusive: every cell that can reach the face lies in this tile
-    bool ex_x = comp == 0 ? (bx >= 1 && bx <= 7) : (bx >= 2 && bx <= 7);
-    bool ex_y = comp == 1 ? (by >= 1 && by <= 7) : (by >= 2 && by <= 7);
-    bool ex_z = comp == 2 ? (bz >= 1 && bz <= 8 * KT - 1) : (bz >= 2 && bz <= 8 * KT - 1);
-    int64_t g = ((int64_t)ii * sny + jj) * snz + kk;
-    float *gv = comp == 0 ? a.u : (comp == 1 ? a.v : a.w);
-    float *gw = comp == 0 ? a.uw : (comp == 1 ? a.vw : a.ww);
+    const bool ex_x = COMP == 0 ? (bx >= 1 && bx <= 7) : (bx >= 2 && bx <= 7);
+    const bool ex_y = COMP == 1 ? (by >= 1 && by <= 7) : (by >= 2 && by <= 7);
+    const bool ex_z = COMP == 2 ? (bz >= 1 && bz <= 8 * KT - 1) : (bz >= 2 && bz <= 8 * KT - 1);
+    const int64_t g = ((int64_t)ii * sny + jj) * snz + kk;
     if (!GF_IN(g, (int64_t)snx * sny * snz)) continue;
     if (ex_x && ex_y && ex_z) {
       gv[g] = val;
@@ -203,6 +204,15 @@ __device__ __forceinline__ void p2g_flush_box(const P2GArgs &a, const T *s_val, 
       atomicAdd(&gw[g], wt);
     }
   }
+}
+
+template <int KT, typename T>
+__device__ __forceinline__ void p2g_flush_box(const P2GArgs &a, const T *s_val, const T *s_wt,
+                                              int I0, int J0, int K0) {
+  constexpr int BK = P2G_BOXK(KT);
+  p2g_flush_comp<0, KT, T>(a, s_val, s_wt, I0, J0, K0);
+  p2g_flush_comp<1, KT, T>(a, s_val + BK, s_wt + BK, I0, J0, K0);
+  p2g_flush_comp<2, KT, T>(a, s_val + 2 * BK, s_wt + 2 * BK, I0, J0, K0);
 }
 
 // Per-cell register accumulation (p2g_map 2), one face component COMP: lane
@@ -564,10 +574,10 @@ __device__ __forceinline__ void p2g_tile_body(const P2GArgs &a, int t, int64_t k
   T *s_wt = s_val + 3 * BK;
   const int64_t b = a.start[key0], e = a.start[key0 + (int64_t)ntk * TILE_CELLS];
   if (b == e) return;
-  for (int q = threadIdx.x; q < 3 * BK; q += blockDim.x) {
-    s_val[q] = (T)0;
-    s_wt[q] = (T)0;
-  }
+  // zero both boxes (contiguous, 16-byte aligned) with 16-byte stores
+  static_assert((2 * 3 * BK * sizeof(T)) % 16 == 0, "P2G box size");
+  for (int q = threadIdx.x; q < (int)(2 * 3 * BK * sizeof(T) / 16); q += blockDim.x)
+    reinterpret_cast<uint4 *>(s_val)[q] = make_uint4(0u, 0u, 0u, 0u);
   __syncthreads();
   const int ti = t / (a.nty * a.ntz), tj = (t / a.ntz) % a.nty, tk = t % a.ntz;
   const int I0 = ti * TILE, J0 = tj * TILE, K0 = tk * TILE;
@@ -1412,8 +1422,8 @@ static_assert(gbox_vol(0) == 1440 && gbox_vol(1) == 1440 && gbox_vol(2) == 1200,
 static_assert(gbox_off(2) == 2880 && gbox_set(1) == GBOX_SET, "box set");
 static_assert(gbox_set(2) == 6368, "box set of 8 x 8 x 16 blocks");
 constexpr int G2P_TILE_THREADS = 256;
-constexpr int G2P_SPLIT_N = 1024;  // particles per CTA (4 rounds of 256)
-constexpr int G2P_SPLITS = 4;      // CTAs per 8^3 tile: 4096 particles at 8 per cell
+constexpr int G2P_SPLIT_N = 2048;  // particles per CTA (8 rounds of 256)
+constexpr int G2P_SPLITS = 2;      // CTAs per 8^3 tile: 4096 particles at 8 per cell
 constexpr long long G2P_WAIT_LIMIT = 1LL << 22;  // try_wait polls before giving up
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
