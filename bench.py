@@ -52,12 +52,12 @@ sys.path.insert(0, ROOT)
 
 METRIC = ("FLIP substeps/s @128³ (refined vs plain FP32 PCG, same residual); fwd+adj/s")
 # DRAM bytes (read + write) of one launch of the shared-memory PCG with the
-# tile SGS preconditioner and the coarse correction (four regions per block) on
-# this workload, from an ncu capture: 9,925,632 read + 741,376 written.  The
-# solve's vectors stay in shared memory; only the input, result, tagged halo
-# and coarse words, the coarse rows and the FP64 replacement steps touch DRAM,
-# far below the algorithmic bytes of a streaming PCG.
-PCG_DRAM_BYTES = 9925632 + 741376
+# tile SGS preconditioner and the coarse correction (one region per active
+# tile) on this workload, from an ncu capture: 12,928,000 read + 791,552
+# written.  The solve's vectors stay in shared memory; only the input, result,
+# tagged halo and coarse words, the coarse rows and the FP64 replacement steps
+# touch DRAM, far below the algorithmic bytes of a streaming PCG.
+PCG_DRAM_BYTES = 12928000 + 791552
 GRID = 128
 DT = 1.0 / 480.0
 TOL = 1e-8
