@@ -639,6 +639,33 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     if (lane == 0) s_gw[tl * 16 + (wid & 15)] = v;
   };
+
+  // the warp partials of all the thread's tiles at once (v[j] for tile tl0 +
+  // 2j, 0 beyond the block's tiles): a butterfly over eight values -- three
+  // exchange levels that halve the values a lane holds, then two plain levels
+  // -- leaves lane L with the warp's sum of value (L >> 2) & 7 after 9
+  // shuffles instead of 5 per tile; lane 4q writes value q
+  auto tile_partials = [&](const float (&v)[MAXJ]) {
+    static_assert(MAXJ <= 8, "eight values per butterfly");
+    float a8[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) a8[q] = q < MAXJ ? v[q < MAXJ ? q : 0] : 0.f;
+    const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+    float w4[4], w2[2];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      w4[q] = (b4 ? a8[4 + q] : a8[q]) +
+              __shfl_xor_sync(0xffffffffu, b4 ? a8[q] : a8[4 + q], 16);
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
+      w2[q] = (b3 ? w4[2 + q] : w4[q]) +
+              __shfl_xor_sync(0xffffffffu, b3 ? w4[q] : w4[2 + q], 8);
+    float y = (b2 ? w2[1] : w2[0]) + __shfl_xor_sync(0xffffffffu, b2 ? w2[0] : w2[1], 4);
+    y += __shfl_xor_sync(0xffffffffu, y, 2);
+    y += __shfl_xor_sync(0xffffffffu, y, 1);
+    const int q = (lane >> 2) & 7, tl = tl0 + 2 * q;
+    if ((lane & 3) == 0 && q < MAXJ && tl < nt) s_gw[tl * 16 + (wid & 15)] = y;
+  };
   // warm start (refined only): x64 = the dense p0 at the cell, r = b - A x64
   // in FP64 with the neighbours' p0 read from the dense array (complete and
   // read-only during the solve, so no halo exchange); the stop test stays
@@ -950,6 +977,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
   for (int it = 0; it < a.max_iter && !done; ++it) {
     const float alphaf = (float)alpha, nalpha = -alphaf, betaf = (float)beta;
     // ---- own: d = z + beta d; s = w + beta s; x += alpha d; r -= alpha s; z = M r
+    float rv[MAXJ];  // new residuals of the thread's cells (0 off the fluid)
 #pragma unroll
     for (int j = 0; j < MAXJ; ++j) {
       const int tl = tl0 + 2 * j, L = tl * 512 + l;
@@ -966,8 +994,9 @@ __global__ void __launch_bounds__(SM_THREADS, 1) k_pcg_smem(PcgSmemArgs a) {
         *zp = SGS ? rn * s_rtab[8 | ((dpack >> (3 * j)) & 7)]
                   : rn / fmaxf((float)((dpack >> (3 * j)) & 7), 1.0f);
       }
-      if (CRS && coarse && tl < nt) tile_partial(tl, rn);
+      rv[j] = rn;
     }
+    if (CRS && coarse) tile_partials(rv);
     if (SGS) zero_rings();
     __syncthreads();
     trace_mark(gs);
