@@ -1817,7 +1817,7 @@ static int launch_pressure_batch(Ctx *c, const gf_step_params *prm) {
     SegPcgArgs pa{c->n_active, c->tile_nbr, c->seg_slot0, c->nseg, c->code, c->bdiv, c->xf,
                   c->r, c->z, c->d0, c->d1, c->Ad, refined ? c->x64 : nullptr, c->partials,
                   (int64_t)c->ntiles + MAX_PCG_BLOCKS, c->seg_state, c->state, nullptr,
-                  nullptr, prm->max_iters, check_every, prm->tol * prm->tol, 1e-4, sign,
+                  nullptr, prm->max_iters, check_every, prm->tol * prm->tol, PCG_REPLACE2, sign,
                   (prm->flags & GF_FLAG_SGS_MASK) >> GF_FLAG_SGS_SHIFT};
     if (refined) {
       e = launch_pcg_seg<double, true>(c, pa);
@@ -1898,7 +1898,7 @@ int launch_pressure(Ctx *c, const gf_step_params *prm) {
       return e;
     const int check_every = prm->check_every > 0 ? prm->check_every : 1;
     const float sign = prm->rhs_sign >= 0 ? 1.0f : -1.0f;
-    const double replace2 = 1e-4;  // replace the residual each time it drops by 100x
+    const double replace2 = PCG_REPLACE2;
     const bool force_global =
         (prm->flags & GF_FLAG_GLOBAL_PCG) != 0 || !pcg_smem_fits(c, refined);
     if (!force_global) {
