@@ -1157,6 +1157,7 @@ struct GStencil {
   const float *p;
   int si, sj, i0, j0, k0;
   float fx, fy, fz;
+  float i0f, j0f, k0f;  // floor(fx), ...: the first face indices as floats (exact)
 };
 
 // apic_gather_lin for two components at once (a on the x half of each
@@ -1173,10 +1174,15 @@ __device__ __forceinline__ void apic_gather_lin_pair(const GStencil &a, const GS
                                                      float inv, float one, float2 &vel,
                                                      float2 &c0, float2 &c1, float2 &c2) {
   const float2 ONE = dup2(one), NEG = dup2(-one);
+  // first face indices as floats: float(floor(f)) is floor(f), and adding 1
+  // to it is exact, so no integer-to-float conversion is needed
+  const float2 I0[2] = {make_float2(a.i0f, b.i0f), add2(make_float2(a.i0f, b.i0f), dup2(1.0f))};
+  const float2 J0[2] = {make_float2(a.j0f, b.j0f), add2(make_float2(a.j0f, b.j0f), dup2(1.0f))};
+  const float2 K0[2] = {make_float2(a.k0f, b.k0f), add2(make_float2(a.k0f, b.k0f), dup2(1.0f))};
   // s = f - floor(f): the difference as -floor * 1 + f
-  const float2 s_x = fma2(make_float2((float)a.i0, (float)b.i0), NEG, make_float2(a.fx, b.fx));
-  const float2 s_y = fma2(make_float2((float)a.j0, (float)b.j0), NEG, make_float2(a.fy, b.fy));
-  const float2 s_z = fma2(make_float2((float)a.k0, (float)b.k0), NEG, make_float2(a.fz, b.fz));
+  const float2 s_x = fma2(I0[0], NEG, make_float2(a.fx, b.fx));
+  const float2 s_y = fma2(J0[0], NEG, make_float2(a.fy, b.fy));
+  const float2 s_z = fma2(K0[0], NEG, make_float2(a.fz, b.fz));
   const float2 wx[2] = {sub2(dup2(1.0f), s_x), s_x}, wy[2] = {sub2(dup2(1.0f), s_y), s_y},
                wz[2] = {sub2(dup2(1.0f), s_z), s_z};
   // face offsets: (index [+ 0.5]) dx - p; adding 0 to the integer-valued float
@@ -1188,12 +1194,9 @@ __device__ __forceinline__ void apic_gather_lin_pair(const GStencil &a, const GS
   float2 ox[2], oy[2], oz[2];
 #pragma unroll
   for (int d = 0; d < 2; ++d) {
-    ox[d] = sum2(mul2(add2(make_float2((float)(a.i0 + d), (float)(b.i0 + d)), hx), DX), ONE,
-                 dup2(-px));
-    oy[d] = sum2(mul2(add2(make_float2((float)(a.j0 + d), (float)(b.j0 + d)), hy), DX), ONE,
-                 dup2(-py));
-    oz[d] = sum2(mul2(add2(make_float2((float)(a.k0 + d), (float)(b.k0 + d)), hz), DX), ONE,
-                 dup2(-pz));
+    ox[d] = sum2(mul2(add2(I0[d], hx), DX), ONE, dup2(-px));
+    oy[d] = sum2(mul2(add2(J0[d], hy), DX), ONE, dup2(-py));
+    oz[d] = sum2(mul2(add2(K0[d], hz), DX), ONE, dup2(-pz));
   }
   const float2 INV = dup2(inv);
   float2 acc = dup2(0.0f);
@@ -1228,16 +1231,17 @@ template <int AX>
 __device__ __forceinline__ void apic_gather_lin_k2(const GStencil &g, float px, float py,
                                                    float pz, float dx, float inv, float one,
                                                    float &vel, float &c0, float &c1, float &c2) {
-  const float sx = g.fx - (float)g.i0, sy = g.fy - (float)g.j0, sz = g.fz - (float)g.k0;
+  const float sx = g.fx - g.i0f, sy = g.fy - g.j0f, sz = g.fz - g.k0f;
   const float wx[2] = {1.0f - sx, sx}, wy[2] = {1.0f - sy, sy};
   const float2 wz = make_float2(1.0f - sz, sz);
   float ox[2], oy[2];
 #pragma unroll
-  for (int d = 0; d < 2; ++d) {
-    ox[d] = AX == 0 ? (float)(g.i0 + d) * dx - px : ((float)(g.i0 + d) + 0.5f) * dx - px;
-    oy[d] = AX == 1 ? (float)(g.j0 + d) * dx - py : ((float)(g.j0 + d) + 0.5f) * dx - py;
+  for (int d = 0; d < 2; ++d) {  // float(i0 + d) as floor + d (exact)
+    const float fi = g.i0f + (float)d, fj = g.j0f + (float)d;
+    ox[d] = AX == 0 ? fi * dx - px : (fi + 0.5f) * dx - px;
+    oy[d] = AX == 1 ? fj * dx - py : (fj + 0.5f) * dx - py;
   }
-  const float2 oz = sum2(mul2(add2(make_float2((float)g.k0, (float)(g.k0 + 1)),
+  const float2 oz = sum2(mul2(add2(make_float2(g.k0f, g.k0f + 1.0f),
                                    dup2(AX == 2 ? 0.0f : 0.5f)),
                               dup2(dx)),
                          dup2(one), dup2(-pz));
@@ -1625,13 +1629,16 @@ __global__ void __launch_bounds__(G2P_TILE_THREADS, 4)
 #pragma unroll
         for (int cc = 0; cc < 3; ++cc) {
           const int snx = nx + (cc == 0), sny = ny + (cc == 1), snz = nz + (cc == 2);
-          int i0, j0, k0;
-          const bool inside = stencil_inside(fxs[cc], fys[cc], fzs[cc], snx, sny, snz, i0, j0, k0);
+          // stencil_inside, keeping the floors as floats for the gathers
+          const float flx = floorf(fxs[cc]), fly = floorf(fys[cc]), flz = floorf(fzs[cc]);
+          const int i0 = __float2int_rz(flx), j0 = __float2int_rz(fly), k0 = __float2int_rz(flz);
+          const bool inside = i0 >= 0 && i0 < snx - 1 && j0 >= 0 && j0 < sny - 1 && k0 >= 0 &&
+                              k0 < snz - 1;
           const int NJ = gbox_nj(cc), NK = gbox_nk(cc, KT);
           lin[cc] = inside && in_box(bx[cc], gbox_ni(cc), i0, i0 + 1, j0, j0 + 1, k0, k0 + 1);
           gs[cc] = GStencil{bx[cc].s + ((i0 - bx[cc].oi) * NJ + (j0 - bx[cc].oj)) * NK +
                                 (k0 - bx[cc].ok),
-                            NJ * NK, NK, i0, j0, k0, fxs[cc], fys[cc], fzs[cc]};
+                            NJ * NK, NK, i0, j0, k0, fxs[cc], fys[cc], fzs[cc], flx, fly, flz};
         }
         auto gather_one = [&](int cc) {
           const int snx = nx + (cc == 0), sny = ny + (cc == 1), snz = nz + (cc == 2);
@@ -1922,15 +1929,39 @@ static inline unsigned grid_for(int64_t n, int threads, int num_sms) {
   return (unsigned)g;
 }
 
+// Zero the six face arrays P2G accumulates into, in one launch (six memsets
+// cost six graph nodes): each array's 16-byte-aligned body with 16-byte
+// stores, its unaligned head and tail with 4-byte stores.
+struct ZeroFaces {
+  float *p[6];
+  int64_t n[6];
+};
+__global__ void k_zero_faces(ZeroFaces z) {
+  const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+#pragma unroll 1
+  for (int q = 0; q < 6; ++q) {
+    float *const p = z.p[q];
+    const int64_t n = z.n[q];
+    int64_t head = (int64_t)(((16u - (uint32_t)(reinterpret_cast<uintptr_t>(p) & 15u)) & 15u) >> 2);
+    if (head > n) head = n;
+    const int64_t nv = (n - head) >> 2;
+    float4 *const v = reinterpret_cast<float4 *>(p + head);
+    for (int64_t i = t0; i < nv; i += stride) v[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (t0 < head) p[t0] = 0.f;
+    for (int64_t i = head + 4 * nv + t0; i < n; i += stride) p[i] = 0.f;
+  }
+}
+
 int launch_p2g(Ctx *c, int transfer) {
   if (!c->bound) return fail(c, GF_INVALID_ARG, "gf_p2g: buffers not bound");
   if (transfer == GF_APIC && !c->p.C) return fail(c, GF_INVALID_ARG, "gf_p2g: APIC needs C");
   cudaStream_t st = c->stream;
-  float *bufs[6] = {c->f.u, c->f.uw, c->f.v, c->f.vw, c->f.w, c->f.ww};
-  int64_t lens[6] = {c->nu, c->nu, c->nv, c->nv, c->nw, c->nw};
-  for (int q = 0; q < 6; ++q) {
-    int e = check_cuda(c, cudaMemsetAsync(bufs[q], 0, lens[q] * 4, st), "memset p2g");
-    if (e) return e;
+  {
+    const ZeroFaces z{{c->f.u, c->f.uw, c->f.v, c->f.vw, c->f.w, c->f.ww},
+                      {c->nu, c->nu, c->nv, c->nv, c->nw, c->nw}};
+    k_zero_faces<<<(unsigned)((c->num_sms > 0 ? c->num_sms : 148) * 4), 512, 0, st>>>(z);
+    c->launches++;
   }
   P2GArgs a{c->start, c->rec0, c->rec1, c->rec2, c->rec3, c->f.u, c->f.v, c->f.w,
             c->f.uw, c->f.vw, c->f.ww, c->dx, c->nx, c->ny, c->nz, c->nty, c->ntz,
