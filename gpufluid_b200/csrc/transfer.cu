@@ -15,10 +15,13 @@
 //                     (:1591-1732) over sorted particles; results go back to
 //                     the caller's AoS buffers in sorted order (pid follows).
 //
-// The library is compiled with -fmad=false: every product and sum rounds
+// This unit is compiled with -fmad=false: every product and sum rounds
 // separately, in the reference's operation order, so that each stage is
 // bit-identical to the CPU oracle when its inputs are.  Only the order of the
-// floating-point atomic sums in P2G differs.
+// floating-point atomic sums in P2G differs (P2G uses explicit fused
+// multiply-adds, its sums being tolerance-checked).  G2P does part of its
+// arithmetic on packed float32 pairs (mul2 / sum2 of gf_internal.cuh), each
+// half rounded as the scalar operation, so it stays bit-identical.
 #include "gf_internal.cuh"
 
 namespace gf {
